@@ -1,0 +1,478 @@
+// Launchers, per-device runtime state and the C ABI of the primitive entry points (include/fls_b200.h).
+#include "fls_b200.h"
+#include "fls_decode.cu"
+#include "fls_runtime.h"
+
+#include <cstdio>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+namespace flsgpu {
+
+// ---------------------------------------------------------------------------------------------------------
+// Kernel families
+// ---------------------------------------------------------------------------------------------------------
+#define FLS_NUM64 64, 0u, 8, 8, 2
+#define FLS_NUM32 32, 0u, 4, 12, 3
+#define FLS_GATHER 32, 8320u, 8, 6, 2
+#define FLS_ANY 64, 8320u, 8, 5, 2
+
+template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES>
+static cudaError_t launch_family(const DecodeArgs& a, cudaStream_t s, int sm_count, int grid_override) {
+	using G            = Geometry<MAXWS, GSTAGE, EMAX, WARPS, STAGES>;
+	auto*       kfn    = k_decode<MAXWS, GSTAGE, EMAX, WARPS, STAGES>;
+	static bool inited = false;
+	if (!inited) {
+		cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, G::kSmem);
+		if (e != cudaSuccess) { return e; }
+		inited = true;
+	}
+	int per_sm = 0;
+	cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, G::kThreads, G::kSmem);
+	if (e != cudaSuccess) { return e; }
+	if (per_sm < 1) { per_sm = 1; }
+	const uint64_t want = (a.n_items + WARPS - 1) / WARPS;
+	uint64_t       grid = static_cast<uint64_t>(sm_count) * per_sm;
+	if (grid_override > 0) { grid = static_cast<uint64_t>(grid_override); }
+	if (want < grid) { grid = want; }
+	if (grid == 0) { return cudaSuccess; }
+	kfn<<<static_cast<unsigned>(grid), G::kThreads, G::kSmem, s>>>(a);
+	++launch_counter();
+	return cudaGetLastError();
+}
+
+uint64_t& launch_counter() {
+	static uint64_t n = 0;
+	return n;
+}
+
+Device* current_device() {
+	static Device     devs[64];
+	static std::mutex mu;
+	int               ord = 0;
+	if (cudaGetDevice(&ord) != cudaSuccess || ord < 0 || ord >= 64) { return nullptr; }
+	std::lock_guard<std::mutex> lk(mu);
+	Device&                     d = devs[ord];
+	if (d.ordinal < 0) {
+		if (cudaDeviceGetAttribute(&d.sm_count, cudaDevAttrMultiProcessorCount, ord) != cudaSuccess) { return nullptr; }
+		if (cudaMalloc(&d.status, sizeof(int)) != cudaSuccess) { return nullptr; }
+		if (cudaMemset(d.status, 0, sizeof(int)) != cudaSuccess) { return nullptr; }
+		d.ordinal = ord;
+	}
+	return &d;
+}
+
+cudaError_t launch_decode(Family fam, const DecodeArgs& args, cudaStream_t stream, int grid_override) {
+	Device* d = current_device();
+	if (!d) { return cudaErrorInitializationError; }
+	DecodeArgs a = args;
+	if (!a.status) { a.status = d->status; }
+	if (a.n_items == 0) { return cudaSuccess; }
+	bool narrow = a.cols == nullptr && a.col0.ws <= 32 && a.col0.e <= 4;
+	switch (fam) {
+	case Family::NUM:
+		return narrow ? launch_family<FLS_NUM32>(a, stream, d->sm_count, grid_override)
+		              : launch_family<FLS_NUM64>(a, stream, d->sm_count, grid_override);
+	case Family::GATHER: return launch_family<FLS_GATHER>(a, stream, d->sm_count, grid_override);
+	default: return launch_family<FLS_ANY>(a, stream, d->sm_count, grid_override);
+	}
+}
+
+void family_geometry(Family fam, int* threads, int* smem, int* ctas_per_sm) {
+	auto fill = [&](int th, int sm, const void* fn) {
+		*threads = th;
+		*smem    = sm;
+		int per  = 0;
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, th, sm);
+		*ctas_per_sm = per;
+	};
+	switch (fam) {
+	case Family::NUM: {
+		using G = Geometry<FLS_NUM64>;
+		fill(G::kThreads, G::kSmem, reinterpret_cast<const void*>(k_decode<FLS_NUM64>));
+		break;
+	}
+	case Family::GATHER: {
+		using G = Geometry<FLS_GATHER>;
+		fill(G::kThreads, G::kSmem, reinterpret_cast<const void*>(k_decode<FLS_GATHER>));
+		break;
+	}
+	default: {
+		using G = Geometry<FLS_ANY>;
+		fill(G::kThreads, G::kSmem, reinterpret_cast<const void*>(k_decode<FLS_ANY>));
+		break;
+	}
+	}
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// Encoder-side kernels (fixtures, trial encodes, benchmark data).  Thread per lane of a vector.
+// ---------------------------------------------------------------------------------------------------------
+__host__ __device__ __forceinline__ uint32_t transposed_index(uint32_t o) {
+	// inverse of original_index: o = 64a + 8b + c  ->  k = a + 16*O[b] + 128*c   (O is an involution)
+	return (o / 64) + 16 * fls_order((o / 8) % 8) + 128 * (o % 8);
+}
+
+template <typename T>
+__global__ void k_permute(const T* __restrict__ in, T* __restrict__ out, uint64_t n_vec, bool to_transposed) {
+	const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	if (i >= n_vec * kVec) { return; }
+	const uint64_t v = i / kVec;
+	const uint32_t k = static_cast<uint32_t>(i % kVec);
+	if (to_transposed) {
+		out[i] = in[v * kVec + original_index(k)];
+	} else {
+		out[v * kVec + original_index(k)] = in[i];
+	}
+}
+
+template <typename T, int W>
+__global__ void k_ffor(const T* __restrict__ in, T* __restrict__ out, const uint8_t* __restrict__ bw,
+                       const T* __restrict__ base, const uint64_t* __restrict__ byte_off, uint64_t n_vec) {
+	// Word-centric packing: word w of lane l gathers every value j whose bits [j*b, (j+1)*b) overlap
+	// [w*W, (w+1)*W).  Inverse of the unpack layout: lane l's word w lives at out[l + L*w].
+	constexpr uint32_t L = 1024 / W;
+	const uint64_t     i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	if (i >= n_vec * L) { return; }
+	const uint64_t v = i / L;
+	const uint32_t l = static_cast<uint32_t>(i % L);
+	const uint32_t b = bw[v];
+	if (b == 0 || b > W) { return; }
+	T* o = reinterpret_cast<T*>(reinterpret_cast<uint8_t*>(out) + (byte_off ? byte_off[v] : v * b * 128ull));
+	const T        bs   = base ? base[v] : T(0);
+	const T*       src  = in + v * kVec;
+	const uint64_t mask = b >= 64 ? ~0ull : ((1ull << b) - 1ull);
+	for (uint32_t w = 0; w < b; ++w) {
+		const uint32_t lo_bit = w * W;
+		const uint32_t j0     = lo_bit / b;
+		const uint32_t j1     = (lo_bit + W - 1) / b;
+		uint64_t       word   = 0;
+		for (uint32_t j = j0; j <= j1 && j < static_cast<uint32_t>(W); ++j) {
+			const uint64_t x  = static_cast<uint64_t>(static_cast<T>(src[l + L * j] - bs)) & mask;
+			const int32_t  sh = static_cast<int32_t>(j * b) - static_cast<int32_t>(lo_bit);
+			if (sh >= 0) {
+				word |= sh >= 64 ? 0ull : (x << sh);
+			} else {
+				word |= (-sh) >= 64 ? 0ull : (x >> (-sh));
+			}
+		}
+		o[l + L * w] = static_cast<T>(word);
+	}
+}
+
+template <typename T, int W>
+__global__ void k_unrsum(const T* __restrict__ in, T* __restrict__ out, uint64_t n_vec) {
+	constexpr uint32_t L = 1024 / W;
+	const uint64_t     i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+	if (i >= n_vec * L) { return; }
+	const uint64_t v = i / L;
+	const uint32_t l = static_cast<uint32_t>(i % L);
+	// lane l covers a contiguous run of original positions; walk it in order
+	uint32_t start;
+	if constexpr (W == 64) {
+		start = l * 64;
+	} else if constexpr (W == 32) {
+		start = (l % 16) * 64 + 32 * (l / 16);
+	} else {
+		start = (l % 16) * 64 + fls_order(l / 16) * 8;
+	}
+	const T* src  = in + v * kVec;
+	T*       dst  = out + v * kVec;
+	T        prev = 0;
+	for (uint32_t p = 0; p < static_cast<uint32_t>(W); ++p) {
+		const uint32_t k = transposed_index(start + p);
+		const T        x = src[k];
+		dst[k]           = p == 0 ? T(0) : static_cast<T>(x - prev);
+		prev             = x;
+	}
+}
+
+template <typename T, int W>
+__global__ void k_analyze(const T* __restrict__ in, uint8_t* __restrict__ bw, T* __restrict__ base, uint64_t n_vec,
+                          bool is_signed) {
+	// one warp per vector
+	const uint64_t v    = static_cast<uint64_t>(blockIdx.x) * (blockDim.x / 32) + threadIdx.x / 32;
+	const uint32_t lane = threadIdx.x & 31u;
+	if (v >= n_vec) { return; }
+	const T* src  = in + v * kVec;
+	const T  flip = is_signed ? static_cast<T>(T(1) << (W - 1)) : T(0);
+	T        mn = static_cast<T>(~T(0)), mx = 0;
+	for (uint32_t k = lane; k < kVec; k += 32) {
+		const T x = static_cast<T>(src[k] ^ flip);
+		mn        = x < mn ? x : mn;
+		mx        = x > mx ? x : mx;
+	}
+	for (int o = 16; o > 0; o >>= 1) {
+		const T a = __shfl_xor_sync(0xFFFFFFFFu, mn, o);
+		const T b = __shfl_xor_sync(0xFFFFFFFFu, mx, o);
+		mn        = a < mn ? a : mn;
+		mx        = b > mx ? b : mx;
+	}
+	if (lane == 0) {
+		const uint64_t d = static_cast<uint64_t>(static_cast<T>(mx - mn));
+		bw[v]            = static_cast<uint8_t>(d == 0 ? 0 : 64 - __clzll(static_cast<long long>(d)));
+		base[v]          = static_cast<T>(mn ^ flip);
+	}
+}
+
+} // namespace flsgpu
+
+// =========================================================================================================
+// C ABI
+// =========================================================================================================
+using namespace flsgpu;
+
+namespace {
+int to_status(cudaError_t e) { return e == cudaSuccess ? FLS_OK : FLS_ERR_CUDA; }
+
+template <int W>
+int run_primitive(const void* in, void* out, const uint8_t* bw, uint8_t bw_const, const void* base,
+                  const void* lane_base, const uint64_t* byte_off, uint64_t n_vec, int order, uint8_t enc,
+                  fls_stream_t stream) {
+	if (n_vec == 0) { return FLS_OK; }
+	if (!in || !out || (order != FLS_TRANSPOSED && order != FLS_ORIGINAL) || n_vec >= (1ull << 32)) {
+		return FLS_ERR_ARG;
+	}
+	if ((reinterpret_cast<uintptr_t>(in) & 3u) != 0 || (reinterpret_cast<uintptr_t>(out) & (W / 8 - 1)) != 0) {
+		return FLS_ERR_ARG;
+	}
+	if (bw_const > W) { return FLS_ERR_BW; }
+	DecodeArgs a {};
+	ColDesc&   c    = a.col0;
+	c.ws            = W;
+	c.e             = W / 8;
+	c.enc           = enc;
+	c.post          = POST_NONE;
+	c.order         = static_cast<uint8_t>(order);
+	c.layout        = LAYOUT_ARRAYS;
+	c.n_vec         = static_cast<uint32_t>(n_vec);
+	c.bw_const      = bw_const;
+	c.packed        = static_cast<const uint8_t*>(in);
+	c.byte_off      = byte_off;
+	c.bw_arr        = bw;
+	c.base_arr      = static_cast<const uint8_t*>(base);
+	c.lane_base_arr = static_cast<const uint8_t*>(lane_base);
+	c.out           = static_cast<uint8_t*>(out);
+	a.n_items       = n_vec;
+	return to_status(launch_decode(Family::NUM, a, static_cast<cudaStream_t>(stream)));
+}
+
+template <typename T>
+int run_permute(const T* in, T* out, uint64_t n_vec, bool to_transposed, fls_stream_t stream) {
+	if (n_vec == 0) { return FLS_OK; }
+	if (!in || !out) { return FLS_ERR_ARG; }
+	const uint64_t n = n_vec * kVec;
+	k_permute<T><<<static_cast<unsigned>((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(in, out, n_vec,
+	                                                                                                    to_transposed);
+	++launch_counter();
+	return to_status(cudaGetLastError());
+}
+
+template <typename T, int W>
+int run_ffor(const T* in, T* out, const uint8_t* bw, const T* base, const uint64_t* off, uint64_t n_vec,
+             fls_stream_t stream) {
+	if (n_vec == 0) { return FLS_OK; }
+	if (!in || !out || !bw) { return FLS_ERR_ARG; }
+	const uint64_t n = n_vec * (1024 / W);
+	k_ffor<T, W><<<static_cast<unsigned>((n + 127) / 128), 128, 0, static_cast<cudaStream_t>(stream)>>>(in, out, bw,
+	                                                                                                   base, off, n_vec);
+	++launch_counter();
+	return to_status(cudaGetLastError());
+}
+
+template <typename T, int W>
+int run_unrsum(const T* in, T* out, uint64_t n_vec, fls_stream_t stream) {
+	if (n_vec == 0) { return FLS_OK; }
+	if (!in || !out || in == out) { return FLS_ERR_ARG; }
+	const uint64_t n = n_vec * (1024 / W);
+	k_unrsum<T, W><<<static_cast<unsigned>((n + 127) / 128), 128, 0, static_cast<cudaStream_t>(stream)>>>(in, out,
+	                                                                                                     n_vec);
+	++launch_counter();
+	return to_status(cudaGetLastError());
+}
+
+template <typename T, int W>
+int run_analyze(const T* in, uint8_t* bw, T* base, uint64_t n_vec, int is_signed, fls_stream_t stream) {
+	if (n_vec == 0) { return FLS_OK; }
+	if (!in || !bw || !base) { return FLS_ERR_ARG; }
+	k_analyze<T, W><<<static_cast<unsigned>((n_vec + 7) / 8), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+	    in, bw, base, n_vec, is_signed != 0);
+	++launch_counter();
+	return to_status(cudaGetLastError());
+}
+} // namespace
+
+extern "C" {
+
+int fls_gpu_status(int reset) {
+	Device* d = current_device();
+	if (!d) { return FLS_ERR_CUDA; }
+	if (cudaDeviceSynchronize() != cudaSuccess) { return FLS_ERR_CUDA; }
+	int h = 0;
+	if (cudaMemcpy(&h, d->status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) { return FLS_ERR_CUDA; }
+	if (reset && cudaMemset(d->status, 0, sizeof(int)) != cudaSuccess) { return FLS_ERR_CUDA; }
+	return h;
+}
+
+uint64_t fls_gpu_launch_count(int reset) {
+	const uint64_t n = launch_counter();
+	if (reset) { launch_counter() = 0; }
+	return n;
+}
+
+#define FLS_PRIM(T, W)                                                                                                \
+	int fls_gpu_unpack_u##W(const T* in, T* out, const uint8_t* bw, const uint64_t* off, uint64_t n, int order,     \
+	                        fls_stream_t s) {                                                                       \
+		if (!bw) { return FLS_ERR_ARG; }                                                                            \
+		return run_primitive<W>(in, out, bw, 0, nullptr, nullptr, off, n, order, ENC_FFOR, s);                      \
+	}                                                                                                               \
+	int fls_gpu_unffor_u##W(const T* in, T* out, const uint8_t* bw, const T* base, const uint64_t* off, uint64_t n, \
+	                        int order, fls_stream_t s) {                                                            \
+		if (!bw || !base) { return FLS_ERR_ARG; }                                                                   \
+		return run_primitive<W>(in, out, bw, 0, base, nullptr, off, n, order, ENC_FFOR, s);                         \
+	}                                                                                                               \
+	int fls_gpu_rsum_u##W(const T* in, T* out, const T* lane_base, uint64_t n, int order, fls_stream_t s) {         \
+		if (!lane_base) { return FLS_ERR_ARG; }                                                                     \
+		return run_primitive<W>(in, out, nullptr, W, nullptr, lane_base, nullptr, n, order, ENC_DELTA, s);          \
+	}                                                                                                               \
+	int fls_gpu_untranspose_i_u##W(const T* in, T* out, uint64_t n, fls_stream_t s) {                               \
+		return run_primitive<W>(in, out, nullptr, W, nullptr, nullptr, nullptr, n, FLS_ORIGINAL, ENC_RAW, s);       \
+	}                                                                                                               \
+	int fls_gpu_transpose_i_u##W(const T* in, T* out, uint64_t n, fls_stream_t s) {                                 \
+		return run_permute<T>(in, out, n, true, s);                                                                 \
+	}                                                                                                               \
+	int fls_gpu_ffor_u##W(const T* in, T* out, const uint8_t* bw, const T* base, const uint64_t* off, uint64_t n,   \
+	                      fls_stream_t s) {                                                                         \
+		return run_ffor<T, W>(in, out, bw, base, off, n, s);                                                        \
+	}
+
+FLS_PRIM(uint8_t, 8)
+FLS_PRIM(uint16_t, 16)
+FLS_PRIM(uint32_t, 32)
+FLS_PRIM(uint64_t, 64)
+
+#define FLS_PRIM2(T, W)                                                                                               \
+	int fls_gpu_unffor_rsum_u##W(const T* in, T* out, const uint8_t* bw, const T* base, const T* lane_base,         \
+	                             const uint64_t* off, uint64_t n, int order, fls_stream_t s) {                      \
+		if (!bw || !base || !lane_base) { return FLS_ERR_ARG; }                                                     \
+		return run_primitive<W>(in, out, bw, 0, base, lane_base, off, n, order, ENC_DELTA, s);                      \
+	}                                                                                                               \
+	int fls_gpu_unrsum_u##W(const T* in, T* out, uint64_t n, fls_stream_t s) { return run_unrsum<T, W>(in, out, n, s); } \
+	int fls_gpu_analyze_u##W(const T* in, uint8_t* bw, T* base, uint64_t n, int sg, fls_stream_t s) {               \
+		return run_analyze<T, W>(in, bw, base, n, sg, s);                                                           \
+	}
+
+FLS_PRIM2(uint16_t, 16)
+FLS_PRIM2(uint32_t, 32)
+FLS_PRIM2(uint64_t, 64)
+
+} // extern "C"
+
+// =========================================================================================================
+// Plans
+// =========================================================================================================
+struct fls_plan {
+	ColDesc*  d_cols   = nullptr;
+	uint32_t* d_queue  = nullptr;
+	uint64_t  n_items  = 0;
+	uint32_t  n_cols   = 0;
+	int       device   = -1;
+	Family    family   = Family::NUM;
+	ColDesc   col0 {};
+};
+
+extern "C" {
+
+int fls_plan_create(const fls_vector_batch* batches, uint32_t n_batches, const uint32_t* d_queue, uint64_t n_items,
+                    fls_plan** out_plan) {
+	if (!out_plan || !batches || n_batches == 0 || n_batches > 256) { return FLS_ERR_ARG; }
+	*out_plan = nullptr;
+	std::unique_ptr<fls_plan> p(new fls_plan());
+	std::vector<ColDesc>     cols(n_batches);
+	uint64_t                 total = 0;
+	for (uint32_t i = 0; i < n_batches; ++i) {
+		const fls_vector_batch& b = batches[i];
+		if (b.width != 8 && b.width != 16 && b.width != 32 && b.width != 64) { return FLS_ERR_ARG; }
+		if (b.encoding > FLS_ENC_DELTA || b.order > FLS_ORIGINAL || !b.d_packed || !b.d_out) { return FLS_ERR_ARG; }
+		if (b.encoding != FLS_ENC_RAW && (!b.d_bw || !b.d_base || !b.d_byte_off)) { return FLS_ERR_ARG; }
+		if (b.encoding == FLS_ENC_DELTA && !b.d_lane_base) { return FLS_ERR_ARG; }
+		if (b.n_vec >= (1u << 24)) { return FLS_ERR_ARG; }
+		ColDesc& c      = cols[i];
+		c               = ColDesc {};
+		c.ws            = b.width;
+		c.e             = b.width / 8;
+		c.enc           = b.encoding;
+		c.post          = POST_NONE;
+		c.order         = b.order;
+		c.layout        = LAYOUT_ARRAYS;
+		c.n_vec         = b.n_vec;
+		c.bw_const      = b.encoding == FLS_ENC_RAW ? b.width : 0;
+		c.packed        = static_cast<const uint8_t*>(b.d_packed);
+		c.byte_off      = b.encoding == FLS_ENC_RAW ? nullptr : b.d_byte_off;
+		c.bw_arr        = b.encoding == FLS_ENC_RAW ? nullptr : b.d_bw;
+		c.base_arr      = static_cast<const uint8_t*>(b.d_base);
+		c.lane_base_arr = static_cast<const uint8_t*>(b.d_lane_base);
+		c.out           = static_cast<uint8_t*>(b.d_out);
+		total += b.n_vec;
+	}
+	if (cudaGetDevice(&p->device) != cudaSuccess) { return FLS_ERR_CUDA; }
+	p->n_cols = n_batches;
+	p->family = Family::NUM;
+	if (n_batches == 1 && d_queue == nullptr) {
+		p->col0    = cols[0];
+		p->n_items = total;
+	} else {
+		std::vector<uint32_t> q;
+		if (d_queue == nullptr) {
+			q.reserve(total);
+			for (uint32_t i = 0; i < n_batches; ++i) {
+				for (uint32_t v = 0; v < cols[i].n_vec; ++v) { q.push_back((i << 24) | v); }
+			}
+			n_items = total;
+		}
+		if (cudaMalloc(&p->d_cols, sizeof(ColDesc) * n_batches) != cudaSuccess) { return FLS_ERR_CUDA; }
+		if (cudaMemcpy(p->d_cols, cols.data(), sizeof(ColDesc) * n_batches, cudaMemcpyHostToDevice) != cudaSuccess) {
+			return FLS_ERR_CUDA;
+		}
+		if (n_items > 0) {
+			if (cudaMalloc(&p->d_queue, sizeof(uint32_t) * n_items) != cudaSuccess) { return FLS_ERR_CUDA; }
+			const cudaError_t e = d_queue ? cudaMemcpy(p->d_queue, d_queue, sizeof(uint32_t) * n_items,
+			                                           cudaMemcpyDeviceToDevice)
+			                              : cudaMemcpy(p->d_queue, q.data(), sizeof(uint32_t) * n_items,
+			                                           cudaMemcpyHostToDevice);
+			if (e != cudaSuccess) { return FLS_ERR_CUDA; }
+		}
+		p->n_items = n_items;
+	}
+	*out_plan = p.release();
+	return FLS_OK;
+}
+
+int fls_plan_decode_grid(const fls_plan* p, int grid, fls_stream_t stream) {
+	if (!p) { return FLS_ERR_ARG; }
+	DecodeArgs a {};
+	a.cols    = p->d_cols;
+	a.queue   = p->d_queue;
+	a.n_items = p->n_items;
+	a.col0    = p->col0;
+	return to_status(launch_decode(p->family, a, static_cast<cudaStream_t>(stream), grid));
+}
+
+int fls_plan_decode(const fls_plan* p, fls_stream_t stream) { return fls_plan_decode_grid(p, 0, stream); }
+
+int fls_plan_destroy(fls_plan* p) {
+	if (!p) { return FLS_OK; }
+	if (p->d_cols) { cudaFree(p->d_cols); }
+	if (p->d_queue) { cudaFree(p->d_queue); }
+	delete p;
+	return FLS_OK;
+}
+
+int fls_plan_geometry(const fls_plan* p, int* threads, int* smem_bytes, int* ctas_per_sm) {
+	if (!p || !threads || !smem_bytes || !ctas_per_sm) { return FLS_ERR_ARG; }
+	family_geometry(p->family, threads, smem_bytes, ctas_per_sm);
+	return FLS_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,460 @@
+// The B200 decode engine: one persistent kernel that walks a queue of (column, vector) work items and decodes
+// each FastLanes vector with one warp.
+//
+//   stage 1  packed words of the vector -> shared memory with a bulk TMA copy (cp.async.bulk + mbarrier),
+//            STAGES vectors ahead of the one being decoded (per-warp ring)
+//   stage 2  bit-unpack + FOR add (+ per-lane running sum for DELTA) in registers, values in run order
+//   stage 3  optional gather: RLE expansion from the run values staged next to the packed words, or a
+//            dictionary lookup
+//   stage 4  store: transposed order straight from registers, original order through a swizzled staging
+//            buffer and row-wise 16-byte stores (every decoded byte crosses HBM exactly once)
+//
+// Reference semantics (cwida/FastLanes): unpack/unffor = primitives/fls_generated/fallback/scalar_aav_uf1/
+// *_unpack_src.cpp:17277 / *_unffor_src.cpp:22971 (u32 dispatch), rsum = *_rsum_src.cpp:100-410,
+// untranspose_i = *_untranspose_src.cpp:4110, RLE expansion = src/cor/lyt/vec.cpp:318-332 (Vec::flatten_to),
+// dictionary gather = include/fls/encoder/assert_eq.hpp:257-400.
+#include "fls_device.cuh"
+#include "fls_plan.h"
+
+namespace flsgpu {
+
+struct Plan {
+	const uint8_t* src;        // packed words of the stream
+	const uint8_t* lane_bases; // ENC_DELTA
+	const uint8_t* gsrc;       // RLE run values
+	const uint8_t* dict;
+	uint8_t*       out;
+	uint64_t       for_base;
+	uint32_t       bytes;  // packed bytes = bw * 128
+	uint32_t       gbytes; // run-value bytes
+	uint32_t       bw;
+	uint32_t       entry_c;
+	uint32_t       n_runs;
+	uint32_t       ghead; // offset of the run values inside the staged (16-byte aligned) copy
+	uint8_t        ws, e, enc, post, order;
+	bool           ok;
+};
+
+__device__ __forceinline__ uint64_t ld_le(const uint8_t* p, uint32_t n) {
+	const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+	if ((a & (n - 1)) == 0) {
+		switch (n) {
+		case 1: return *p;
+		case 2: return *reinterpret_cast<const uint16_t*>(p);
+		case 4: return *reinterpret_cast<const uint32_t*>(p);
+		default: return *reinterpret_cast<const uint64_t*>(p);
+		}
+	}
+	uint64_t x = 0;
+	for (uint32_t i = 0; i < n; ++i) { x |= static_cast<uint64_t>(p[i]) << (8 * i); }
+	return x;
+}
+
+__device__ __forceinline__ uint32_t ep_of(const ColDesc& c, uint32_t v, uint32_t i) {
+	return v == 0 ? 0u : c.ep[(v - 1) * c.arr_c + i];
+}
+
+__device__ __forceinline__ Plan make_plan(const ColDesc& c, uint32_t v) {
+	Plan p;
+	p.ws      = c.ws;
+	p.e       = c.e;
+	p.enc     = c.enc;
+	p.post    = c.post;
+	p.order   = c.order;
+	p.entry_c = c.entry_c;
+	p.dict    = c.dict;
+	p.out     = c.out + static_cast<uint64_t>(v) * kVec * c.e;
+	p.ok      = v < c.n_vec;
+	p.for_base   = 0;
+	p.lane_bases = nullptr;
+	p.gsrc       = nullptr;
+	p.gbytes     = 0;
+	p.n_runs     = 0;
+	p.ghead      = 0;
+	const uint32_t wb = c.ws / 8;
+	if (c.layout == LAYOUT_ARRAYS) {
+		p.bw               = c.bw_arr ? c.bw_arr[v] : c.bw_const;
+		const uint64_t off = c.byte_off ? c.byte_off[v] : static_cast<uint64_t>(v) * c.bw_const * 128u;
+		p.src              = c.packed + off;
+		if (c.base_arr) { p.for_base = ld_le(c.base_arr + static_cast<uint64_t>(v) * wb, wb); }
+		if (c.lane_base_arr) { p.lane_bases = c.lane_base_arr + static_cast<uint64_t>(v) * 128u; }
+	} else {
+		if (c.enc == ENC_RAW) {
+			p.bw = c.ws;
+		} else {
+			const uint32_t obw = ep_of(c, v, c.ib_bw);
+			const uint32_t obs = ep_of(c, v, c.ib_base);
+			if (obw >= c.buf_size[c.ib_bw] || obs + wb > c.buf_size[c.ib_base]) { p.ok = false; }
+			p.bw       = p.ok ? c.buf[c.ib_bw][obw] : 0;
+			p.for_base = p.ok ? ld_le(c.buf[c.ib_base] + obs, wb) : 0;
+		}
+		const uint32_t opk = ep_of(c, v, c.ib_packed);
+		p.src              = c.buf[c.ib_packed] + opk;
+		if (static_cast<uint64_t>(opk) + p.bw * 128ull > c.buf_size[c.ib_packed]) { p.ok = false; }
+		if (c.enc == ENC_DELTA) {
+			const uint32_t olb = ep_of(c, v, c.ib_lane_bases);
+			if (olb + 128ull > c.buf_size[c.ib_lane_bases]) { p.ok = false; }
+			p.lane_bases = c.buf[c.ib_lane_bases] + olb;
+		}
+		if (c.post == POST_RLE || c.post == POST_RLE_DICT) {
+			const uint32_t ov  = ep_of(c, v, c.ib_vals);
+			const uint64_t end = (v + 1 < c.n_vec) ? ep_of(c, v + 1, c.ib_vals) : c.buf_size[c.ib_vals];
+			if (end < ov || end > c.buf_size[c.ib_vals]) { p.ok = false; }
+			p.gsrc   = c.buf[c.ib_vals] + ov;
+			p.gbytes = p.ok ? static_cast<uint32_t>(end - ov) : 0;
+		}
+	}
+	if (p.bw > p.ws) { p.ok = false; }
+	p.bytes = p.ok ? p.bw * 128u : 0u;
+	if (p.post == POST_RLE || p.post == POST_RLE_DICT) {
+		const uint32_t ve = p.post == POST_RLE ? p.e : 4u;
+		if (p.gbytes > kVec * ve) { p.ok = false; }
+		p.n_runs = p.ok ? p.gbytes / ve : 0u;
+		p.ghead  = static_cast<uint32_t>(reinterpret_cast<uintptr_t>(p.gsrc) & 15u);
+	}
+	return p;
+}
+
+// Copy one vector's inputs into its stage and arm the stage's mbarrier.  Called by all 32 lanes with the same
+// plan.  16-byte aligned packed words go through the TMA engine; anything else is copied by the warp.
+// The run values of an RLE vector are fetched as the enclosing 16-byte aligned window (pages are placed
+// with at least 16 bytes of slack on both sides), so they always take the TMA path.
+template <uint32_t GSTAGE>
+__device__ __forceinline__ void issue(const Plan& p, uint8_t* stage, uint8_t* gstage, uint64_t* bar, uint32_t lane) {
+	uint32_t   tx      = 0;
+	const bool tma_pk  = p.ok && p.bytes > 0 && (reinterpret_cast<uintptr_t>(p.src) & 15u) == 0;
+	uint32_t   gwindow = 0;
+	if (GSTAGE > 0 && p.ok && p.gbytes > 0) { gwindow = (p.ghead + p.gbytes + 15u) & ~15u; }
+	if (GSTAGE > 0 && gwindow > GSTAGE) { gwindow = 0; }
+	if (p.ok && p.bytes > 0 && !tma_pk) {
+		if ((reinterpret_cast<uintptr_t>(p.src) & 3u) == 0) {
+			const uint32_t* s = reinterpret_cast<const uint32_t*>(p.src);
+			uint32_t*       d = reinterpret_cast<uint32_t*>(stage);
+			for (uint32_t i = lane; i < p.bytes / 4; i += 32) { d[i] = s[i]; }
+		} else {
+			for (uint32_t i = lane; i < p.bytes; i += 32) { stage[i] = p.src[i]; }
+		}
+	}
+	__syncwarp();
+	if (lane == 0) {
+		if (tma_pk) { tx += p.bytes; }
+		tx += gwindow;
+		mbar_arrive_expect_tx(bar, tx);
+		if (tma_pk) { bulk_g2s(stage, p.src, p.bytes, bar); }
+		if (gwindow) { bulk_g2s(gstage, p.gsrc - p.ghead, gwindow, bar); }
+	}
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// Per-width decode of the staged stream into registers (run order).
+// ---------------------------------------------------------------------------------------------------------
+template <int WS>
+struct StreamT {
+	using T = uint32_t;
+};
+template <>
+struct StreamT<64> {
+	using T = uint64_t;
+};
+
+template <int WS>
+__device__ __forceinline__ void decode_stream(const Plan& p, const uint32_t* S, uint32_t t,
+                                              typename StreamT<WS>::T (&v)[32]) {
+	using T = typename StreamT<WS>::T;
+	if constexpr (WS == 64) {
+		extract_w64(S, t, p.bw, v);
+	} else if constexpr (WS == 32) {
+		extract_w32(S, t, p.bw, v);
+	} else if constexpr (WS == 16) {
+		extract_w16(S, t, p.bw, v);
+	} else {
+		extract_w8(S, t, p.bw, v);
+	}
+	constexpr T wmask = WS == 64 ? ~T(0) : static_cast<T>((1ull << WS) - 1ull);
+	if (p.enc != ENC_RAW) {
+		const T base = static_cast<T>(p.for_base);
+#pragma unroll
+		for (int i = 0; i < 32; ++i) { v[i] = (v[i] + base) & wmask; }
+	}
+	if (p.enc == ENC_DELTA) {
+		// rsum: running sum along each lane in original order, seeded by the lane's base.
+		if constexpr (WS == 32) {
+			T acc = static_cast<T>(ld_le(p.lane_bases + 4 * t, 4));
+#pragma unroll
+			for (int i = 0; i < 32; ++i) {
+				acc += v[i];
+				v[i] = acc;
+			}
+		} else if constexpr (WS == 64) {
+			const uint32_t l   = t & 15u;
+			const uint32_t h   = t >> 4;
+			T              acc = 0;
+#pragma unroll
+			for (int i = 0; i < 32; ++i) {
+				acc += v[i];
+				v[i] = acc;
+			}
+			const T lower = __shfl_sync(0xFFFFFFFFu, acc, l); // total of the lane's first half
+			T       add   = static_cast<T>(ld_le(p.lane_bases + 8 * l, 8));
+			if (h) { add += lower; }
+#pragma unroll
+			for (int i = 0; i < 32; ++i) { v[i] += add; }
+		} else if constexpr (WS == 16) {
+#pragma unroll
+			for (int q = 0; q < 2; ++q) {
+				T acc = static_cast<T>(ld_le(p.lane_bases + 2 * (2 * t + q), 2));
+#pragma unroll
+				for (int i = 0; i < 16; ++i) {
+					acc          = (acc + v[16 * q + i]) & wmask;
+					v[16 * q + i] = acc;
+				}
+			}
+		} else {
+#pragma unroll
+			for (int q = 0; q < 4; ++q) {
+				T acc = p.lane_bases[4 * t + q];
+#pragma unroll
+				for (int i = 0; i < 8; ++i) {
+					acc         = (acc + v[8 * q + i]) & wmask;
+					v[8 * q + i] = acc;
+				}
+			}
+		}
+	}
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// Store of 32 values per thread (run order) for stream width WS and element size E.
+// ---------------------------------------------------------------------------------------------------------
+template <int E>
+struct OutT {
+	using T = uint32_t;
+};
+template <>
+struct OutT<8> {
+	using T = uint64_t;
+};
+
+template <int WS, int E>
+__device__ __forceinline__ void store_vector(const typename OutT<E>::T (&o)[32], uint8_t* out, uint8_t* ost,
+                                             bool original, uint32_t t) {
+	constexpr uint32_t RL = run_len<WS>();
+	constexpr uint32_t RC = run_count<WS>();
+	if (original) {
+#pragma unroll
+		for (uint32_t r = 0; r < RC; ++r) {
+			const uint32_t b0 = run_start<WS>(t, r) * E;
+			if constexpr (RL * E >= 16) {
+				constexpr uint32_t PER = 16 / E; // values per 16-byte chunk
+#pragma unroll
+				for (uint32_t c = 0; c < RL * E / 16; ++c) {
+					uint32_t w[4];
+#pragma unroll
+					for (uint32_t k = 0; k < 4; ++k) {
+						if constexpr (E == 8) {
+							const uint64_t x = o[r * RL + c * PER + k / 2];
+							w[k]             = (k & 1) ? static_cast<uint32_t>(x >> 32) : static_cast<uint32_t>(x);
+						} else if constexpr (E == 4) {
+							w[k] = static_cast<uint32_t>(o[r * RL + c * PER + k]);
+						} else if constexpr (E == 2) {
+							w[k] = (o[r * RL + c * PER + 2 * k] & 0xFFFFu) | (o[r * RL + c * PER + 2 * k + 1] << 16);
+						} else {
+							const uint32_t i0 = r * RL + c * PER + 4 * k;
+							w[k] = (o[i0] & 0xFFu) | ((o[i0 + 1] & 0xFFu) << 8) | ((o[i0 + 2] & 0xFFu) << 16) |
+							       (o[i0 + 3] << 24);
+						}
+					}
+					*reinterpret_cast<uint4*>(ost + stage_off(b0 + 16 * c)) = make_uint4(w[0], w[1], w[2], w[3]);
+				}
+			} else {
+				// WS = 8, E = 1: an 8-byte run
+				const uint32_t i0 = r * RL;
+				const uint32_t lo = (o[i0] & 0xFFu) | ((o[i0 + 1] & 0xFFu) << 8) | ((o[i0 + 2] & 0xFFu) << 16) |
+				                    (o[i0 + 3] << 24);
+				const uint32_t hi = (o[i0 + 4] & 0xFFu) | ((o[i0 + 5] & 0xFFu) << 8) |
+				                    ((o[i0 + 6] & 0xFFu) << 16) | (o[i0 + 7] << 24);
+				*reinterpret_cast<uint2*>(ost + stage_off(b0)) = make_uint2(lo, hi);
+			}
+		}
+		__syncwarp();
+		if ((reinterpret_cast<uintptr_t>(out) & 15u) == 0) {
+#pragma unroll
+			for (uint32_t c = t; c < 64u * E; c += 32) {
+				const uint4 x = *reinterpret_cast<const uint4*>(ost + stage_off(16 * c));
+				*reinterpret_cast<uint4*>(out + 16 * c) = x;
+			}
+		} else {
+			for (uint32_t b = t; b < 1024u * E; b += 32) { out[b] = ost[stage_off(b)]; }
+		}
+		__syncwarp();
+	} else {
+		using OT = typename OutT<E>::T;
+#pragma unroll
+		for (uint32_t p = 0; p < RL; ++p) {
+			if constexpr (RC == 1) {
+				reinterpret_cast<OT*>(out)[run_tpos<WS>(t, 0, p)] = o[p];
+			} else {
+				// the thread's RC lanes are adjacent: one wider store per run position
+				const uint32_t k0 = run_tpos<WS>(t, 0, p);
+#pragma unroll
+				for (uint32_t r = 0; r < RC; ++r) {
+					if constexpr (E == 1) {
+						out[k0 + r] = static_cast<uint8_t>(o[r * RL + p]);
+					} else {
+						reinterpret_cast<OT*>(out)[k0 + r] = static_cast<OT>(o[r * RL + p]);
+					}
+				}
+			}
+		}
+	}
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// Full decode of one staged vector.
+// ---------------------------------------------------------------------------------------------------------
+template <int WS, int E>
+__device__ __forceinline__ void decode_vector(const Plan& p, const uint8_t* stage, const uint8_t* gstage, uint8_t* ost,
+                                              uint32_t t, int* status) {
+	using ST = typename StreamT<WS>::T;
+	using OT = typename OutT<E>::T;
+	ST v[32];
+	decode_stream<WS>(p, reinterpret_cast<const uint32_t*>(stage), t, v);
+	OT o[32];
+	bool bad = false;
+	if (p.post == POST_NONE) {
+#pragma unroll
+		for (int i = 0; i < 32; ++i) { o[i] = static_cast<OT>(v[i]); }
+	} else if (p.post == POST_RLE) {
+		const OT* vals = reinterpret_cast<const OT*>(gstage + p.ghead);
+#pragma unroll
+		for (int i = 0; i < 32; ++i) {
+			const uint32_t idx = static_cast<uint32_t>(v[i]);
+			const bool     in  = idx < p.n_runs;
+			bad |= !in;
+			o[i] = in ? vals[idx] : OT(0);
+		}
+	} else {
+		const OT* dict = reinterpret_cast<const OT*>(p.dict);
+		const uint32_t* codes = reinterpret_cast<const uint32_t*>(gstage + p.ghead);
+#pragma unroll
+		for (int i = 0; i < 32; ++i) {
+			uint32_t code = static_cast<uint32_t>(v[i]);
+			if (p.post == POST_RLE_DICT) {
+				const bool in = code < p.n_runs;
+				bad |= !in;
+				code = in ? codes[code] : 0u;
+			}
+			const bool in = code < p.entry_c;
+			bad |= !in;
+			o[i] = in ? __ldg(dict + code) : OT(0);
+		}
+	}
+	if (__any_sync(0xFFFFFFFFu, bad) && t == 0) { atomicOr(status, STATUS_BAD_INDEX); }
+	store_vector<WS, E>(o, p.out, ost, p.order != 0, t);
+}
+
+__device__ __forceinline__ uint32_t item_col(uint32_t it) { return it >> 24; }
+__device__ __forceinline__ uint32_t item_vec(uint32_t it) { return it & 0xFFFFFFu; }
+
+__device__ __forceinline__ Plan plan_of(const DecodeArgs& a, uint64_t item) {
+	if (a.queue == nullptr) { return make_plan(a.col0, static_cast<uint32_t>(item)); }
+	const uint32_t it = a.queue[item];
+	const ColDesc& c  = a.cols ? a.cols[item_col(it)] : a.col0;
+	return make_plan(c, item_vec(it));
+}
+
+// Kernel family: MAXWS bounds the staged stream (bytes per stage = MAXWS * 128), GSTAGE the run-value window,
+// EMAX the output element size (staging buffer = EMAX * 1024 bytes).
+template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES>
+struct Geometry {
+	static constexpr uint32_t kStage     = MAXWS * 128u;
+	static constexpr uint32_t kOut       = EMAX * 1024u;
+	static constexpr uint32_t kPerWarp   = 64u + STAGES * (kStage + GSTAGE) + kOut;
+	static constexpr uint32_t kSlack     = 256u; // extraction reads one row past the last stage
+	static constexpr uint32_t kSmem      = WARPS * kPerWarp + kSlack;
+	static constexpr int      kThreads   = WARPS * 32;
+};
+
+template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES>
+__global__ void __launch_bounds__(WARPS * 32) k_decode(const DecodeArgs a) {
+	using G = Geometry<MAXWS, GSTAGE, EMAX, WARPS, STAGES>;
+	extern __shared__ __align__(128) uint8_t smem[];
+	const uint32_t lane  = threadIdx.x & 31u;
+	const uint32_t warp  = threadIdx.x >> 5;
+	uint8_t*       wbase = smem + warp * G::kPerWarp;
+	uint64_t*      bars  = reinterpret_cast<uint64_t*>(wbase);
+	uint8_t*       stages = wbase + 64;
+	uint8_t*       ost    = wbase + 64 + STAGES * (G::kStage + GSTAGE);
+
+	if (lane == 0) {
+		for (int s = 0; s < STAGES; ++s) { mbar_init(&bars[s], 1); }
+		fence_mbar_init();
+	}
+	__syncwarp();
+
+	const uint64_t gw = static_cast<uint64_t>(blockIdx.x) * WARPS + warp;
+	const uint64_t nw = static_cast<uint64_t>(gridDim.x) * WARPS;
+	const uint64_t n  = a.n_items;
+
+	auto stage_ptr  = [&](int s) { return stages + s * (G::kStage + GSTAGE); };
+	auto gstage_ptr = [&](int s) { return stages + s * (G::kStage + GSTAGE) + G::kStage; };
+
+	// prologue: fill the ring
+	for (int s = 0; s < STAGES; ++s) {
+		const uint64_t item = gw + s * nw;
+		if (item < n) { issue<GSTAGE>(plan_of(a, item), stage_ptr(s), gstage_ptr(s), &bars[s], lane); }
+	}
+
+	uint32_t k       = 0;
+	bool     aborted = false;
+	for (uint64_t item = gw; item < n; item += nw, ++k) {
+		const int      s      = static_cast<int>(k % STAGES);
+		const uint32_t parity = (k / STAGES) & 1u;
+		const Plan     p      = plan_of(a, item);
+		if (!mbar_wait(&bars[s], parity)) {
+			if (lane == 0) { atomicOr(a.status, STATUS_TIMEOUT); }
+			aborted = true;
+			break;
+		}
+		if (!p.ok) {
+			if (lane == 0) { atomicOr(a.status, p.bw > p.ws ? STATUS_BAD_BW : STATUS_BAD_LAYOUT); }
+		} else {
+			const uint8_t* st = stage_ptr(s);
+			const uint8_t* gs = gstage_ptr(s);
+			if (p.ws == 64) {
+				if constexpr (MAXWS >= 64) { decode_vector<64, 8>(p, st, gs, ost, lane, a.status); }
+			} else if (p.ws == 32) {
+				if constexpr (MAXWS >= 32) {
+					if (p.e == 8) {
+						if constexpr (EMAX >= 8) { decode_vector<32, 8>(p, st, gs, ost, lane, a.status); }
+					} else {
+						decode_vector<32, 4>(p, st, gs, ost, lane, a.status);
+					}
+				}
+			} else if (p.ws == 16) {
+				if (p.e == 8) {
+					if constexpr (EMAX >= 8) { decode_vector<16, 8>(p, st, gs, ost, lane, a.status); }
+				} else if (p.e == 4) {
+					if constexpr (EMAX >= 4) { decode_vector<16, 4>(p, st, gs, ost, lane, a.status); }
+				} else {
+					decode_vector<16, 2>(p, st, gs, ost, lane, a.status);
+				}
+			} else {
+				decode_vector<8, 1>(p, st, gs, ost, lane, a.status);
+			}
+		}
+		__syncwarp();
+		const uint64_t next = item + STAGES * nw;
+		if (next < n) { issue<GSTAGE>(plan_of(a, next), stage_ptr(s), gstage_ptr(s), &bars[s], lane); }
+	}
+	if (aborted) {
+		// Drain: every later stage this warp armed must land before the block's shared memory goes away.
+		for (uint32_t j = k + 1; j < k + STAGES; ++j) {
+			const uint64_t item = gw + static_cast<uint64_t>(j) * nw;
+			if (item >= n) { break; }
+			(void)mbar_wait(&bars[j % STAGES], (j / STAGES) & 1u);
+		}
+	}
+}
+
+} // namespace flsgpu

@@ -1,0 +1,80 @@
+// Column descriptors shared by the host runtime (C++) and the decode kernels (CUDA).
+//
+// A decode launch walks a queue of (column, vector) work items.  Each column says how its 1024-value vectors
+// are stored: either as plain per-vector arrays (the primitive API: packed words + bw + base arrays) or as a
+// FastLanes page (PageHdr + buffer offsets + entry points + buffers, src/cor/eng/compressor.cpp:68-86 and
+// src/cor/lyt/page/page.cpp:63-139 of the reference), and what the decoded stream turns into
+// (plain values, RLE expansion, dictionary gather).
+#pragma once
+
+#include <cstdint>
+
+namespace flsgpu {
+
+enum : uint8_t {
+	ENC_RAW   = 0, // 1024 transposed values stored verbatim (bw = W)
+	ENC_FFOR  = 1, // bit-packed, plus FOR base
+	ENC_DELTA = 2, // bit-packed deltas + FOR base, then per-lane running sum from 128-byte lane bases
+};
+
+enum : uint8_t {
+	POST_NONE     = 0, // output = decoded stream
+	POST_RLE      = 1, // stream is a u16 run index; output = run_values[index]
+	POST_DICT     = 2, // stream is u32 codes; output = dict[code]
+	POST_RLE_DICT = 3, // stream is a u16 run index into u32 codes; output = dict[codes[index]]
+};
+
+enum : uint8_t {
+	LAYOUT_ARRAYS = 0,
+	LAYOUT_PAGE   = 1,
+};
+
+constexpr uint8_t kNoBuf = 0xFF;
+
+struct __align__(16) ColDesc {
+	// what
+	uint8_t  ws;     // stream width in bits: 8, 16, 32, 64
+	uint8_t  e;      // output element size in bytes: 1, 2, 4, 8
+	uint8_t  enc;    // ENC_*
+	uint8_t  post;   // POST_*
+	uint8_t  order;  // 0 transposed (primitive order), 1 original (materialised)
+	uint8_t  layout; // LAYOUT_*
+	uint8_t  arr_c;  // page: number of buffers
+	uint8_t  bw_const;
+	uint32_t n_vec;
+	uint32_t entry_c; // dictionary entries (POST_DICT / POST_RLE_DICT)
+
+	// LAYOUT_PAGE: role -> buffer index (kNoBuf when absent) and resolved buffer starts
+	uint8_t  ib_bw, ib_base, ib_packed, ib_lane_bases, ib_vals, pad0[3];
+	const uint8_t*  buf[6];
+	uint64_t        buf_size[6];
+	const uint32_t* ep; // entry points, (n_vec - 1) x arr_c u32; vector 0 starts at 0 in every buffer
+
+	// LAYOUT_ARRAYS
+	const uint8_t*  packed;     // packed words of all vectors
+	const uint64_t* byte_off;   // per-vector byte offset into packed; null => v * bw_const * 128
+	const uint8_t*  bw_arr;     // per-vector bit width; null => bw_const
+	const uint8_t*  base_arr;   // per-vector FOR base (ws/8 bytes each); null => 0
+	const uint8_t*  lane_base_arr; // per-vector 128-byte lane bases (ENC_DELTA)
+
+	// gathers and output
+	const uint8_t* dict; // POST_DICT: entry_c values of e bytes
+	uint8_t*       out;  // n_vec * 1024 * e bytes
+};
+
+struct DecodeArgs {
+	const ColDesc*  cols;   // device array of columns, or null => use col0
+	const uint32_t* queue;  // device array of (col << 24 | vec) items, or null => items are vectors of col0
+	uint64_t        n_items;
+	int*            status; // device word; kernels OR error bits into it
+	ColDesc         col0;
+};
+
+enum : int {
+	STATUS_TIMEOUT    = 1,  // an mbarrier wait hit its bound
+	STATUS_BAD_BW     = 2,  // bit width above the stream width
+	STATUS_BAD_INDEX  = 4,  // RLE index or dictionary code out of range
+	STATUS_BAD_LAYOUT = 8,  // page buffer reference outside the page
+};
+
+} // namespace flsgpu

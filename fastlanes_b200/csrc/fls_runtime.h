@@ -1,0 +1,35 @@
+// Internal runtime interface between the C++ host code (page walking, column API) and the CUDA launchers.
+#pragma once
+
+#include "fls_plan.h"
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace flsgpu {
+
+enum class Family : int {
+	NUM    = 0, // streams up to 64 bits, no gather (FFOR / DELTA / raw, incl. primitive API)
+	GATHER = 1, // streams up to 32 bits with RLE run values staged and/or a dictionary gather, outputs up to 8 B
+	ANY    = 2, // everything (mixed row-group batches)
+};
+
+// Per-device state: SM count and the library-owned status word.
+struct Device {
+	int  ordinal  = -1;
+	int  sm_count = 0;
+	int* status   = nullptr; // cudaMalloc'd once, 4 bytes
+};
+
+// Returns the state of the current device (initialising it on first use), or nullptr on a CUDA error.
+Device* current_device();
+
+// Launch the persistent decode kernel of the given family.  max_ctas_per_sm caps residency (0 = occupancy).
+cudaError_t launch_decode(Family fam, const DecodeArgs& args, cudaStream_t stream, int grid_override = 0);
+
+// Geometry of a family (threads per CTA, dynamic shared memory per CTA, CTAs resident per SM).
+void family_geometry(Family fam, int* threads, int* smem, int* ctas_per_sm);
+
+// Kernels launched by this library inside the last timed region of a caller (a plain counter; not thread-safe).
+uint64_t& launch_counter();
+
+} // namespace flsgpu

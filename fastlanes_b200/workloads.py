@@ -1,0 +1,138 @@
+"""Seeded synthetic workloads with the shapes of the FastLanes decode benchmarks, encoded on the GPU with this
+library's own encoders (transpose_i -> ffor), so the packed bytes are exactly what the reference's
+generated ffor would produce for the same values.
+
+The reference measures on public datasets (public_bi, NextiaJD, ClickBench) that are not available here;
+these generators stand in for them with the value distributions the benchmark configurations name.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import primitives as P
+from ._lib import check, declare, lib
+
+_p = ctypes.c_void_p
+
+
+class _Batch(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_uint8), ("encoding", ctypes.c_uint8), ("order", ctypes.c_uint8),
+                ("reserved", ctypes.c_uint8), ("n_vec", ctypes.c_uint32), ("d_packed", _p), ("d_byte_off", _p),
+                ("d_bw", _p), ("d_base", _p), ("d_lane_base", _p), ("d_out", _p)]
+
+
+declare("fls_plan_create", ctypes.c_int, [ctypes.POINTER(_Batch), ctypes.c_uint32, _p, ctypes.c_uint64,
+                                          ctypes.POINTER(_p)])
+declare("fls_plan_decode", ctypes.c_int, [_p, _p])
+declare("fls_plan_decode_grid", ctypes.c_int, [_p, ctypes.c_int, _p])
+declare("fls_plan_destroy", ctypes.c_int, [_p])
+declare("fls_plan_geometry", ctypes.c_int, [_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                            ctypes.POINTER(ctypes.c_int)])
+
+_DT = {32: torch.uint32, 64: torch.uint64, 16: torch.uint16, 8: torch.uint8}
+_SIGNED = {32: torch.int32, 64: torch.int64, 16: torch.int16, 8: torch.int8}
+
+
+class FforColumn:
+    """Packed FFOR vectors of one width, device resident: packed bytes, byte offsets, bw, base."""
+
+    def __init__(self, width, packed, byte_off, bw, base, values=None):
+        self.width, self.packed, self.byte_off, self.bw, self.base, self.values = (width, packed, byte_off, bw, base,
+                                                                                   values)
+        self.n_vec = bw.numel()
+
+    @property
+    def packed_bytes(self):
+        return int((self.bw.to(torch.int64) * 128).sum().item())
+
+    def algorithmic_read_bytes(self):
+        """Packed words + per-vector bw byte + FOR base + 8-byte offset."""
+        return self.packed_bytes + self.n_vec * (1 + self.width // 8 + 8)
+
+    def decoded_bytes(self):
+        return self.n_vec * 1024 * self.width // 8
+
+
+def random_ffor_column(width, n_vec, rng, device, keep_values=False):
+    """Vectors whose bit width is uniform in 0..width and whose base is uniform in [0, 2^width - 2^bw];
+    values = base + uniform[0, 2^bw)."""
+    bw = rng.integers(0, width + 1, n_vec)
+    hi = (np.uint64(0) - (np.uint64(1) << bw.astype(np.uint64))) if width == 64 else \
+        ((1 << width) - (1 << bw)).astype(np.uint64)
+    if width == 64:
+        hi = np.where(bw == 64, np.uint64(0), hi)  # 2^64 - 2^64 = 0
+        hi = np.where(bw == 0, np.uint64(np.iinfo(np.uint64).max), hi)
+    base = rng.integers(0, hi, dtype=np.uint64, endpoint=True)
+    g = torch.Generator(device=device)
+    g.manual_seed(int(rng.integers(0, 1 << 62)))
+    bits = torch.randint(-(1 << 63), (1 << 63) - 1, (n_vec, 1024), dtype=torch.int64, device=device, generator=g)
+    bw_t = torch.from_numpy(bw.astype(np.int64)).to(device)
+    mask = torch.where(bw_t >= 64, torch.full_like(bw_t, -1), (torch.ones_like(bw_t) << bw_t.clamp(max=63)) - 1)
+    base_i64 = torch.from_numpy(base.view(np.int64)).to(device)
+    vals = (bits & mask[:, None]) + base_i64[:, None]
+    if width < 64:
+        vals = (vals & ((1 << width) - 1)).to(_SIGNED[width]).view(_DT[width])
+    else:
+        vals = vals.view(torch.uint64)
+    vals = vals.reshape(-1).contiguous()
+    tr = P.transpose_i(vals)
+    bw_d = torch.from_numpy(bw.astype(np.uint8)).to(device)
+    base_d = torch.from_numpy(base.astype(np.uint64)).to(device)
+    if width < 64:
+        base_d = base_d.view(torch.int64).to(_SIGNED[width]).view(_DT[width])
+    else:
+        base_d = base_d.view(torch.uint64)
+    packed, off = P.ffor(tr, bw_d, base_d)
+    return FforColumn(width, packed, off, bw_d, base_d, vals if keep_values else None)
+
+
+class Plan:
+    """A decode plan over several FFOR columns (fls_plan_create / fls_plan_decode)."""
+
+    def __init__(self, columns, outs, order, queue=None):
+        batches = (_Batch * len(columns))()
+        for i, (c, o) in enumerate(zip(columns, outs)):
+            b = batches[i]
+            b.width, b.encoding, b.order, b.n_vec = c.width, 1, order, c.n_vec
+            b.d_packed, b.d_byte_off, b.d_bw, b.d_base = (c.packed.data_ptr(), c.byte_off.data_ptr(),
+                                                          c.bw.data_ptr(), c.base.data_ptr())
+            b.d_lane_base, b.d_out = None, o.data_ptr()
+        self._keep = (columns, outs, queue)
+        h = _p()
+        n_items = queue.numel() if queue is not None else 0
+        check(lib.fls_plan_create(batches, len(columns), queue.data_ptr() if queue is not None else None, n_items,
+                                  ctypes.byref(h)), "fls_plan_create")
+        self.handle = h
+
+    def decode(self, stream=None, grid=0):
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        check(lib.fls_plan_decode_grid(self.handle, grid, s), "fls_plan_decode")
+
+    def geometry(self):
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(lib.fls_plan_geometry(self.handle, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)), "geometry")
+        return a.value, b.value, c.value
+
+    def close(self):
+        if self.handle:
+            lib.fls_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def bw_sweep(n32=65536, n64=32768, seed=0, device="cuda", keep_values=False):
+    """Batched bit-width sweep: 64 Mi u32 + 32 Mi u64 values in 1024-value vectors, per-vector bit width uniform
+    in 0..32 / 0..64, vectors of both widths interleaved in a shuffled work queue."""
+    rng = np.random.default_rng(seed)
+    c32 = random_ffor_column(32, n32, rng, device, keep_values)
+    c64 = random_ffor_column(64, n64, rng, device, keep_values)
+    items = np.concatenate([np.arange(n32, dtype=np.uint32), (1 << 24) | np.arange(n64, dtype=np.uint32)])
+    items = items[rng.permutation(items.size)]
+    queue = torch.from_numpy(items.view(np.int32)).to(device)
+    return [c32, c64], queue

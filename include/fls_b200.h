@@ -1,0 +1,176 @@
+/* fls_b200.h — C ABI of the B200-native FastLanes decode engine.
+ *
+ * Drop-in boundary for the decode path of cwida/FastLanes.  Every entry point below names the reference
+ * interface it replaces (paths are inside the reference project).  All pointers named d_* are device
+ * pointers; calls with an fls_stream_t are asynchronous on that stream (NULL = legacy default stream) and
+ * return a status code for argument errors detected on the host.  Errors found on the device (corrupt
+ * input) are OR-ed into a per-device status word read by fls_gpu_status().
+ *
+ * Vector layout: 1024 values per vector in the FastLanes unified transposed layout
+ *   transposed[k] = original[(k % 16) * 64 + O[(k / 16) % 8] * 8 + k / 128],  O = {0,4,2,6,1,5,3,7}.
+ * order = FLS_TRANSPOSED leaves outputs in that layout (what the reference primitives return);
+ * order = FLS_ORIGINAL also untransposes (what Materializer::Materialize, src/encoder/materializer.cpp:13-21,
+ * returns).
+ */
+#ifndef FLS_B200_H
+#define FLS_B200_H
+
+#include <stdbool.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void* fls_stream_t; /* a cudaStream_t */
+
+enum fls_status_code {
+	FLS_OK              = 0,
+	FLS_ERR_ARG         = -1, /* null pointer, bad size, bad order, misaligned buffer */
+	FLS_ERR_CUDA        = -2, /* a CUDA runtime call failed */
+	FLS_ERR_FORMAT      = -3, /* malformed page / dictionary bytes */
+	FLS_ERR_UNSUPPORTED = -4, /* expression or type outside the decode path */
+	FLS_ERR_BW          = -5, /* bit width above the type width */
+};
+
+enum fls_order_code { FLS_TRANSPOSED = 0, FLS_ORIGINAL = 1 };
+
+/* Device status bits (fls_gpu_status) */
+#define FLS_DEV_TIMEOUT 1
+#define FLS_DEV_BAD_BW 2
+#define FLS_DEV_BAD_INDEX 4
+#define FLS_DEV_BAD_LAYOUT 8
+
+/* Synchronise the current device and return the OR of all device status bits raised since the last reset. */
+int fls_gpu_status(int reset);
+
+/* Number of kernels this library has launched since the last reset (for launch accounting in benchmarks). */
+uint64_t fls_gpu_launch_count(int reset);
+
+/* ---------------------------------------------------------------------------------------------------------
+ * Primitives, batched over n_vec vectors.
+ *   d_bw[v]        bit width of vector v (0..W)
+ *   d_byte_off[v]  byte offset of vector v's packed words inside d_in (NULL: vector v starts at v*bw[v]*128,
+ *                  which is only meaningful when every vector has the same width)
+ *   d_base[v]      FOR base of vector v (unffor)
+ *   d_lane_base    L = 1024/W lane bases per vector, 128 bytes per vector (rsum)
+ * Packed words of a vector start at a 4-byte boundary at least; 16-byte aligned vectors are staged by TMA.
+ * ------------------------------------------------------------------------------------------------------- */
+
+/* replaces generated::unpack::fallback::scalar::unpack (include/fls_gen/unpack/unpack.hpp:6-11) */
+int fls_gpu_unpack_u8(const uint8_t* d_in, uint8_t* d_out, const uint8_t* d_bw, const uint64_t* d_byte_off,
+                      uint64_t n_vec, int order, fls_stream_t stream);
+int fls_gpu_unpack_u16(const uint16_t* d_in, uint16_t* d_out, const uint8_t* d_bw, const uint64_t* d_byte_off,
+                       uint64_t n_vec, int order, fls_stream_t stream);
+int fls_gpu_unpack_u32(const uint32_t* d_in, uint32_t* d_out, const uint8_t* d_bw, const uint64_t* d_byte_off,
+                       uint64_t n_vec, int order, fls_stream_t stream);
+int fls_gpu_unpack_u64(const uint64_t* d_in, uint64_t* d_out, const uint8_t* d_bw, const uint64_t* d_byte_off,
+                       uint64_t n_vec, int order, fls_stream_t stream);
+
+/* replaces generated::unffor::fallback::scalar::unffor (include/fls_gen/unffor/unffor.hpp:6-18) */
+int fls_gpu_unffor_u8(const uint8_t* d_in, uint8_t* d_out, const uint8_t* d_bw, const uint8_t* d_base,
+                      const uint64_t* d_byte_off, uint64_t n_vec, int order, fls_stream_t stream);
+int fls_gpu_unffor_u16(const uint16_t* d_in, uint16_t* d_out, const uint8_t* d_bw, const uint16_t* d_base,
+                       const uint64_t* d_byte_off, uint64_t n_vec, int order, fls_stream_t stream);
+int fls_gpu_unffor_u32(const uint32_t* d_in, uint32_t* d_out, const uint8_t* d_bw, const uint32_t* d_base,
+                       const uint64_t* d_byte_off, uint64_t n_vec, int order, fls_stream_t stream);
+int fls_gpu_unffor_u64(const uint64_t* d_in, uint64_t* d_out, const uint8_t* d_bw, const uint64_t* d_base,
+                       const uint64_t* d_byte_off, uint64_t n_vec, int order, fls_stream_t stream);
+
+/* replaces generated::rsum::fallback::scalar::rsum (include/fls_gen/rsum/rsum.hpp:9-12); d_in holds 1024
+ * transposed deltas per vector */
+int fls_gpu_rsum_u8(const uint8_t* d_in, uint8_t* d_out, const uint8_t* d_lane_base, uint64_t n_vec, int order,
+                    fls_stream_t stream);
+int fls_gpu_rsum_u16(const uint16_t* d_in, uint16_t* d_out, const uint16_t* d_lane_base, uint64_t n_vec,
+                     int order, fls_stream_t stream);
+int fls_gpu_rsum_u32(const uint32_t* d_in, uint32_t* d_out, const uint32_t* d_lane_base, uint64_t n_vec,
+                     int order, fls_stream_t stream);
+int fls_gpu_rsum_u64(const uint64_t* d_in, uint64_t* d_out, const uint64_t* d_lane_base, uint64_t n_vec,
+                     int order, fls_stream_t stream);
+
+/* fused unffor + rsum: the DELTA decode of ffor_decompress + rsum_decompress
+ * (src/cor/prm/ffor/ffor_decompress.cpp:13-32, src/cor/prm/rsum/rsum_decompress.cpp:12-24) */
+int fls_gpu_unffor_rsum_u16(const uint16_t* d_in, uint16_t* d_out, const uint8_t* d_bw, const uint16_t* d_base,
+                            const uint16_t* d_lane_base, const uint64_t* d_byte_off, uint64_t n_vec, int order,
+                            fls_stream_t stream);
+int fls_gpu_unffor_rsum_u32(const uint32_t* d_in, uint32_t* d_out, const uint8_t* d_bw, const uint32_t* d_base,
+                            const uint32_t* d_lane_base, const uint64_t* d_byte_off, uint64_t n_vec, int order,
+                            fls_stream_t stream);
+int fls_gpu_unffor_rsum_u64(const uint64_t* d_in, uint64_t* d_out, const uint8_t* d_bw, const uint64_t* d_base,
+                            const uint64_t* d_lane_base, const uint64_t* d_byte_off, uint64_t n_vec, int order,
+                            fls_stream_t stream);
+
+/* replaces generated::untranspose::fallback::scalar::untranspose_i / _o
+ * (include/fls_gen/untranspose/untranspose.hpp:8-19) */
+int fls_gpu_untranspose_i_u8(const uint8_t* d_in, uint8_t* d_out, uint64_t n_vec, fls_stream_t stream);
+int fls_gpu_untranspose_i_u16(const uint16_t* d_in, uint16_t* d_out, uint64_t n_vec, fls_stream_t stream);
+int fls_gpu_untranspose_i_u32(const uint32_t* d_in, uint32_t* d_out, uint64_t n_vec, fls_stream_t stream);
+int fls_gpu_untranspose_i_u64(const uint64_t* d_in, uint64_t* d_out, uint64_t n_vec, fls_stream_t stream);
+
+/* Encoder side (fixtures, trial encodes): generated::transpose::...::transpose_i
+ * (include/fls_gen/transpose/transpose.hpp:8-19), generated::ffor::...::ffor (include/fls_gen/ffor/ffor.hpp:6-15),
+ * generated::unrsum::...::unrsum (include/fls_gen/unrsum/unrsum.hpp:8-16) and the base/bit-width choice of
+ * ffor_analyze (src/cor/prm/ffor/ffor_analyze.cpp:77-102; exact bit count, signed min/max when is_signed). */
+int fls_gpu_transpose_i_u8(const uint8_t* d_in, uint8_t* d_out, uint64_t n_vec, fls_stream_t stream);
+int fls_gpu_transpose_i_u16(const uint16_t* d_in, uint16_t* d_out, uint64_t n_vec, fls_stream_t stream);
+int fls_gpu_transpose_i_u32(const uint32_t* d_in, uint32_t* d_out, uint64_t n_vec, fls_stream_t stream);
+int fls_gpu_transpose_i_u64(const uint64_t* d_in, uint64_t* d_out, uint64_t n_vec, fls_stream_t stream);
+int fls_gpu_ffor_u8(const uint8_t* d_in, uint8_t* d_out, const uint8_t* d_bw, const uint8_t* d_base,
+                    const uint64_t* d_byte_off, uint64_t n_vec, fls_stream_t stream);
+int fls_gpu_ffor_u16(const uint16_t* d_in, uint16_t* d_out, const uint8_t* d_bw, const uint16_t* d_base,
+                     const uint64_t* d_byte_off, uint64_t n_vec, fls_stream_t stream);
+int fls_gpu_ffor_u32(const uint32_t* d_in, uint32_t* d_out, const uint8_t* d_bw, const uint32_t* d_base,
+                     const uint64_t* d_byte_off, uint64_t n_vec, fls_stream_t stream);
+int fls_gpu_ffor_u64(const uint64_t* d_in, uint64_t* d_out, const uint8_t* d_bw, const uint64_t* d_base,
+                     const uint64_t* d_byte_off, uint64_t n_vec, fls_stream_t stream);
+int fls_gpu_unrsum_u16(const uint16_t* d_in, uint16_t* d_out, uint64_t n_vec, fls_stream_t stream);
+int fls_gpu_unrsum_u32(const uint32_t* d_in, uint32_t* d_out, uint64_t n_vec, fls_stream_t stream);
+int fls_gpu_unrsum_u64(const uint64_t* d_in, uint64_t* d_out, uint64_t n_vec, fls_stream_t stream);
+int fls_gpu_analyze_u16(const uint16_t* d_in, uint8_t* d_bw, uint16_t* d_base, uint64_t n_vec, int is_signed,
+                        fls_stream_t stream);
+int fls_gpu_analyze_u32(const uint32_t* d_in, uint8_t* d_bw, uint32_t* d_base, uint64_t n_vec, int is_signed,
+                        fls_stream_t stream);
+int fls_gpu_analyze_u64(const uint64_t* d_in, uint8_t* d_bw, uint64_t* d_base, uint64_t n_vec, int is_signed,
+                        fls_stream_t stream);
+
+
+/* ---------------------------------------------------------------------------------------------------------
+ * Batched decode plans.  A plan describes many vector batches (any mix of widths and encodings) and the
+ * order in which the persistent decode kernel takes their vectors.  Creating a plan uploads its descriptors
+ * and queue once; fls_plan_decode then only launches (one kernel, capturable in a CUDA graph).
+ * Replaces the per-vector Engine/Exe dispatch (src/cor/eng/executor.cpp:44-53) with a device-side queue of
+ * (batch, vector) work items.
+ * ------------------------------------------------------------------------------------------------------- */
+enum fls_encoding_code { FLS_ENC_RAW = 0, FLS_ENC_FFOR = 1, FLS_ENC_DELTA = 2 };
+
+typedef struct {
+	uint8_t         width;    /* 8, 16, 32 or 64 */
+	uint8_t         encoding; /* fls_encoding_code */
+	uint8_t         order;    /* fls_order_code */
+	uint8_t         reserved;
+	uint32_t        n_vec;
+	const void*     d_packed;    /* packed words of all vectors */
+	const uint64_t* d_byte_off;  /* per-vector byte offset in d_packed */
+	const uint8_t*  d_bw;        /* per-vector bit width (FFOR/DELTA) */
+	const void*     d_base;      /* per-vector FOR base (FFOR/DELTA) */
+	const void*     d_lane_base; /* per-vector 128-byte lane bases (DELTA) */
+	void*           d_out;       /* n_vec * 1024 values */
+} fls_vector_batch;
+
+typedef struct fls_plan fls_plan;
+
+/* d_queue: n_items work items (batch << 24 | vector), NULL = every vector of every batch in batch order.
+ * The queue is copied; the batches' device buffers must outlive the plan. */
+int fls_plan_create(const fls_vector_batch* batches, uint32_t n_batches, const uint32_t* d_queue, uint64_t n_items,
+                    fls_plan** out_plan);
+int fls_plan_decode(const fls_plan* plan, fls_stream_t stream);
+/* Same, with an explicit grid (CTAs); 0 = one wave of resident CTAs. */
+int fls_plan_decode_grid(const fls_plan* plan, int grid, fls_stream_t stream);
+int fls_plan_destroy(fls_plan* plan);
+/* Shape of the kernel a plan launches: threads per CTA, dynamic shared memory, resident CTAs per SM. */
+int fls_plan_geometry(const fls_plan* plan, int* threads, int* smem_bytes, int* ctas_per_sm);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLS_B200_H */

@@ -1,0 +1,144 @@
+"""TEST INFRASTRUCTURE — restatement of the reference's page framing, used as the checker for the GPU
+column decoders.
+
+Page bytes (src/cor/eng/compressor.cpp:68-86, src/cor/lyt/page/page.cpp:63-139,
+src/cor/lyt/page/entry_point.cpp:21-41, include/fls/cor/lyt/page/page_hdr.hpp:8-15):
+    [PageHdr: exp_t u8, var u8, reserved u16, vec_c u16, pad u16]
+    [arr_c x u32: absolute offset of each buffer]
+    [(vec_c - 1) x arr_c x u32: per-vector entry points; vector 0 starts at 0 in every buffer]
+    [buffer 0] ... [buffer arr_c - 1]
+"""
+import struct
+
+import numpy as np
+
+from . import oracle
+
+# (exp_t, var) -> number of buffers, from the compress RPN tables (des_buf_c) of include/fls/cor/exp/*/*_exp.hpp
+ARR_C = {
+    (2, 1): 1,  # UNCOMPRESSED
+    (3, 1): 2,  # BYTE_ARR: bytes, end offsets
+    (4, 1): 3,  # FFOR NO_PATCH: bw, base, packed
+    (5, 1): 4,  # DELTA NO_PATCH: lane bases, bw, base, packed
+    (6, 1): 2,  # RLE UNCOMPRESSED: run values, u16 index
+    (6, 2): 5,  # RLE DELTA_NO_PATCH: run values, lane bases, bw, base, packed (u16 index)
+    (6, 4): 5,  # RLE DELTA_NO_PATCH_REC: as above, run values rec-compressed
+    (7, 1): 2,  # FSST: bytes, end offsets
+    (7, 2): 5,  # FSST DELTA_NO_PATCH: bytes, lane bases, bw, base, packed (u32 end offsets)
+    (8, 1): 1,  # DICT UNCOMPRESSED: u32 codes
+    (8, 2): 3,  # DICT FFOR_NO_PATCH
+    (8, 7): 4,  # DICT DELTA_NO_PATCH
+    (11, 1): 2,  # DICT_RLE UNCOMPRESSED: u32 code runs, u16 index
+    (11, 2): 5,  # DICT_RLE DELTA_NO_PATCH
+    (11, 4): 5,  # DICT_RLE DELTA_NO_PATCH_REC
+}
+
+
+class Page:
+    def __init__(self, b):
+        self.b = np.ascontiguousarray(b, np.uint8)
+        self.exp_t, self.var, _, self.vec_c, _ = struct.unpack("<BBHHH", self.b[:8].tobytes())
+        self.arr_c = ARR_C[(self.exp_t, self.var)]
+        self.off = np.frombuffer(self.b[8:8 + 4 * self.arr_c].tobytes(), np.uint32).astype(np.int64)
+        n_ep = (self.vec_c - 1) * self.arr_c
+        s = 8 + 4 * self.arr_c
+        self.ep = np.frombuffer(self.b[s:s + 4 * n_ep].tobytes(), np.uint32).astype(np.int64).reshape(-1, self.arr_c)
+        ends = list(self.off[1:]) + [self.b.size]
+        self.buf_size = [int(ends[i] - self.off[i]) for i in range(self.arr_c)]
+
+    def ep_of(self, v, i):
+        return 0 if v == 0 else int(self.ep[v - 1, i])
+
+    def vector_slice(self, v, i, size=None):
+        start = self.ep_of(v, i)
+        end = start + size if size is not None else (self.ep_of(v + 1, i) if v + 1 < self.vec_c else self.buf_size[i])
+        return self.b[self.off[i] + start:self.off[i] + end]
+
+
+def parse_page(b):
+    return Page(b)
+
+
+def _le(b, dtype):
+    return np.frombuffer(np.ascontiguousarray(b).tobytes(), dtype)
+
+
+def rec_buffer(b):
+    """HzlDeCmp::decompress_buf (src/cor/eng/hzl_de_cmp.cpp:28-77) for the raw-tail form: rec_hdr
+    {bw u8, pad u8, exc_c u16, base[8]} with bw = 255 holds the byte count in base and the raw bytes after it.
+    Returns (decoded bytes, consumed bytes); FFOR blocks are decoded as 1024-value unffor + exception patch."""
+    out = []
+    pos = 0
+    while True:
+        bw = int(b[pos])
+        exc_c = int(struct.unpack("<H", b[pos + 2:pos + 4].tobytes())[0])
+        base_raw = b[pos + 4:pos + 12]
+        pos += 12
+        if bw == 255:
+            sz = int(struct.unpack("<Q", base_raw.tobytes())[0])
+            out.append(b[pos:pos + sz])
+            pos += sz
+            return np.concatenate(out) if out else np.zeros(0, np.uint8), pos
+        raise NotImplementedError("rec FFOR blocks")
+
+
+STREAM_W = {2: None, 4: None, 5: None}
+
+
+def _stream(pg, v, first, ws, enc, T):
+    """Decode one 1024-value stream of width ws stored from buffer index `first` on; returns transposed."""
+    if enc == "raw":
+        return _le(pg.vector_slice(v, first, 128 * ws), T).copy()
+    if enc == "ffor":
+        bw = int(pg.vector_slice(v, first, 1)[0])
+        base = _le(pg.vector_slice(v, first + 1, ws // 8), T)[0]
+        packed = _le(pg.vector_slice(v, first + 2, bw * 128), T)
+        return oracle.unffor(packed, bw, base, T)
+    lb = _le(pg.vector_slice(v, first, 128), T).copy()
+    bw = int(pg.vector_slice(v, first + 1, 1)[0])
+    base = _le(pg.vector_slice(v, first + 2, ws // 8), T)[0]
+    packed = _le(pg.vector_slice(v, first + 3, bw * 128), T)
+    return oracle.rsum(oracle.unffor(packed, bw, base, T), lb)
+
+
+def decode_int(page, dict_bytes=None, value_dtype=np.uint64):
+    """Materialised (original-order) values of an integer page, as assert_eq.hpp:50-400 reconstructs them."""
+    pg = parse_page(page)
+    VT = np.dtype(value_dtype)
+    W = VT.itemsize * 8
+    dic = None
+    if dict_bytes is not None and len(dict_bytes) > 8:
+        dic = _le(rec_buffer(np.asarray(dict_bytes, np.uint8)[8:])[0], VT)
+    out = np.empty(pg.vec_c * 1024, VT)
+    et, var = pg.exp_t, pg.var
+    rec_vals = None
+    if et in (6, 11) and var == 4:
+        # DELTA_NO_PATCH_REC: buffer 0 (run values) is one rec buffer; entry points index its decoded bytes
+        rec_vals = rec_buffer(pg.b[pg.off[0]:pg.off[0] + pg.buf_size[0]])[0]
+    for v in range(pg.vec_c):
+        if et == 2:
+            tr = _stream(pg, v, 0, W, "raw", VT)
+        elif et == 4:
+            tr = _stream(pg, v, 0, W, "ffor", VT)
+        elif et == 5:
+            tr = _stream(pg, v, 0, W, "delta", VT)
+        elif et in (6, 11):
+            if rec_vals is not None:
+                end = pg.ep_of(v + 1, 0) if v + 1 < pg.vec_c else rec_vals.size
+                vals_buf = rec_vals[pg.ep_of(v, 0):end]
+            else:
+                vals_buf = pg.vector_slice(v, 0)
+            vt = VT if et == 6 else np.dtype(np.uint32)
+            vals = _le(vals_buf, vt)
+            idx = _stream(pg, v, 1, 16, "raw" if var in (1, 3) else "delta", np.uint16)
+            tr = vals[idx.astype(np.int64)]
+            if et == 11:
+                tr = dic[tr.astype(np.int64)]
+        elif et == 8:
+            enc = {1: "raw", 2: "ffor", 7: "delta"}[var]
+            codes = _stream(pg, v, 0, 32, enc, np.uint32)
+            tr = dic[codes.astype(np.int64)]
+        else:
+            raise NotImplementedError((et, var))
+        out[v * 1024:(v + 1) * 1024] = oracle.untranspose_i(np.ascontiguousarray(tr.astype(VT)))
+    return out
