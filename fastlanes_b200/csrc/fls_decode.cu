@@ -115,6 +115,7 @@ __device__ __forceinline__ Plan make_plan(const ColDesc& c, uint32_t v) {
 	return p;
 }
 
+#ifndef FLS_HOST_EMULATION
 // Copy one vector's inputs into its stage and arm the stage's mbarrier.  Called by all 32 lanes with the same
 // plan.  16-byte aligned packed words go through the TMA engine; anything else is copied by the warp.
 // The run values of an RLE vector are fetched as the enclosing 16-byte aligned window (pages are placed
@@ -144,6 +145,8 @@ __device__ __forceinline__ void issue(const Plan& p, uint8_t* stage, uint8_t* gs
 		if (gwindow) { bulk_g2s(gstage, p.gsrc - p.ghead, gwindow, bar); }
 	}
 }
+
+#endif // FLS_HOST_EMULATION
 
 // ---------------------------------------------------------------------------------------------------------
 // Per-width decode of the staged stream into registers (run order).
@@ -234,6 +237,25 @@ template <>
 struct OutT<8> {
 	using T = uint64_t;
 };
+// exact element type of an E-byte output
+template <int E>
+struct ElemT;
+template <>
+struct ElemT<1> {
+	using T = uint8_t;
+};
+template <>
+struct ElemT<2> {
+	using T = uint16_t;
+};
+template <>
+struct ElemT<4> {
+	using T = uint32_t;
+};
+template <>
+struct ElemT<8> {
+	using T = uint64_t;
+};
 
 template <int WS, int E>
 __device__ __forceinline__ void store_vector(const typename OutT<E>::T (&o)[32], uint8_t* out, uint8_t* ost,
@@ -288,23 +310,13 @@ __device__ __forceinline__ void store_vector(const typename OutT<E>::T (&o)[32],
 		}
 		__syncwarp();
 	} else {
-		using OT = typename OutT<E>::T;
+		using ET = typename ElemT<E>::T;
 #pragma unroll
 		for (uint32_t p = 0; p < RL; ++p) {
-			if constexpr (RC == 1) {
-				reinterpret_cast<OT*>(out)[run_tpos<WS>(t, 0, p)] = o[p];
-			} else {
-				// the thread's RC lanes are adjacent: one wider store per run position
-				const uint32_t k0 = run_tpos<WS>(t, 0, p);
+			// the thread's RC lanes are adjacent in the transposed order
+			const uint32_t k0 = run_tpos<WS>(t, 0, p);
 #pragma unroll
-				for (uint32_t r = 0; r < RC; ++r) {
-					if constexpr (E == 1) {
-						out[k0 + r] = static_cast<uint8_t>(o[r * RL + p]);
-					} else {
-						reinterpret_cast<OT*>(out)[k0 + r] = static_cast<OT>(o[r * RL + p]);
-					}
-				}
-			}
+			for (uint32_t r = 0; r < RC; ++r) { reinterpret_cast<ET*>(out)[k0 + r] = static_cast<ET>(o[r * RL + p]); }
 		}
 	}
 }
@@ -353,6 +365,7 @@ __device__ __forceinline__ void decode_vector(const Plan& p, const uint8_t* stag
 	store_vector<WS, E>(o, p.out, ost, p.order != 0, t);
 }
 
+#ifndef FLS_HOST_EMULATION
 __device__ __forceinline__ uint32_t item_col(uint32_t it) { return it >> 24; }
 __device__ __forceinline__ uint32_t item_vec(uint32_t it) { return it & 0xFFFFFFu; }
 
@@ -456,5 +469,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_decode(const DecodeArgs a) {
 		}
 	}
 }
+
+#endif // FLS_HOST_EMULATION
 
 } // namespace flsgpu

@@ -21,6 +21,8 @@ namespace flsgpu {
 
 constexpr uint32_t kVec = 1024;
 
+#ifndef FLS_HOST_EMULATION // the tests compile the pure device logic below as host code; PTX stays here
+
 // ---------------------------------------------------------------------------------------------------------
 // PTX wrappers: mbarrier + bulk (non-tensor) TMA copies global -> shared.  No multicast anywhere.
 // ---------------------------------------------------------------------------------------------------------
@@ -68,6 +70,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 	}
 	return false;
 }
+
+#endif // FLS_HOST_EMULATION
 
 // ---------------------------------------------------------------------------------------------------------
 // Layout helpers

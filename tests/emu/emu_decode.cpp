@@ -1,0 +1,89 @@
+// Warp emulation of the decode engine's device logic (fastlanes_b200/csrc/fls_decode.cu) on the CPU.
+// make_plan / decode_vector run unchanged; one warp = 32 std::threads; "shared memory" is a host buffer the
+// harness fills the way the kernel's bulk copies would.  Used by tests/test_device_logic_emulated.py.
+#define FLS_HOST_EMULATION 1
+#include "fls_decode.cu"
+
+#include <thread>
+#include <vector>
+
+thread_local EmuWarp* g_emu_warp = nullptr;
+thread_local int      g_emu_lane = 0;
+
+using namespace flsgpu;
+
+static void dispatch(const Plan& p, const uint8_t* st, const uint8_t* gs, uint8_t* ost, uint32_t t, int* status) {
+	if (p.ws == 64) {
+		decode_vector<64, 8>(p, st, gs, ost, t, status);
+	} else if (p.ws == 32) {
+		if (p.e == 8) {
+			decode_vector<32, 8>(p, st, gs, ost, t, status);
+		} else {
+			decode_vector<32, 4>(p, st, gs, ost, t, status);
+		}
+	} else if (p.ws == 16) {
+		if (p.e == 8) {
+			decode_vector<16, 8>(p, st, gs, ost, t, status);
+		} else if (p.e == 4) {
+			decode_vector<16, 4>(p, st, gs, ost, t, status);
+		} else {
+			decode_vector<16, 2>(p, st, gs, ost, t, status);
+		}
+	} else {
+		decode_vector<8, 1>(p, st, gs, ost, t, status);
+	}
+}
+
+static int emu_vector(const ColDesc& c, uint32_t v) {
+	const Plan p = make_plan(c, v);
+	if (!p.ok) { return p.bw > p.ws ? STATUS_BAD_BW : STATUS_BAD_LAYOUT; }
+	std::vector<uint8_t> smem(3 * 8448 + 8192, 0xA5);
+	uint8_t*             stage  = smem.data();
+	uint8_t*             gstage = stage + 8448;
+	uint8_t*             ost    = gstage + 8448;
+	if (p.bytes) { std::memcpy(stage, p.src, p.bytes); }
+	if (p.gbytes) {
+		const uint32_t win = (p.ghead + p.gbytes + 15u) & ~15u;
+		std::memcpy(gstage, p.gsrc - p.ghead, win);
+	}
+	int                      status = 0;
+	std::barrier<>           bar(32);
+	EmuWarp                  w {&bar, {}, {}};
+	std::vector<std::thread> th;
+	for (int t = 0; t < 32; ++t) {
+		th.emplace_back([&, t] {
+			g_emu_warp = &w;
+			g_emu_lane = t;
+			dispatch(p, stage, gstage, ost, static_cast<uint32_t>(t), &status);
+		});
+	}
+	for (auto& x : th) { x.join(); }
+	return status;
+}
+
+extern "C" int emu_decode_column(const ColDesc* c) {
+	int st = 0;
+	for (uint32_t v = 0; v < c->n_vec; ++v) { st |= emu_vector(*c, v); }
+	return st;
+}
+
+extern "C" int emu_unffor(int width, int enc, int order, const uint8_t* packed, const uint64_t* byte_off,
+                          const uint8_t* bw, const uint8_t* base, const uint8_t* lane_base, uint64_t n_vec,
+                          uint8_t* out) {
+	ColDesc c {};
+	c.ws            = static_cast<uint8_t>(width);
+	c.e             = static_cast<uint8_t>(width / 8);
+	c.enc           = static_cast<uint8_t>(enc);
+	c.post          = POST_NONE;
+	c.order         = static_cast<uint8_t>(order);
+	c.layout        = LAYOUT_ARRAYS;
+	c.n_vec         = static_cast<uint32_t>(n_vec);
+	c.bw_const      = enc == ENC_RAW ? static_cast<uint8_t>(width) : 0;
+	c.packed        = packed;
+	c.byte_off      = enc == ENC_RAW ? nullptr : byte_off;
+	c.bw_arr        = enc == ENC_RAW ? nullptr : bw;
+	c.base_arr      = base;
+	c.lane_base_arr = lane_base;
+	c.out           = out;
+	return emu_decode_column(&c);
+}

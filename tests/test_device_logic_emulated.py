@@ -1,0 +1,109 @@
+"""The decode engine's device logic (make_plan / decode_vector of fastlanes_b200/csrc/fls_decode.cu), compiled
+as host code and run on an emulated warp (32 threads + barrier), against the CPU oracle.  Catches layout and
+indexing mistakes without a GPU; the same cases run on the B200 in test_primitives_gpu.py."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+from tests.emu import build
+
+TYPES = {8: np.uint8, 16: np.uint16, 32: np.uint32, 64: np.uint64}
+
+
+@pytest.fixture(scope="module")
+def emu():
+    return ctypes.CDLL(build.build())
+
+
+def P(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def batch(w, n_vec, rng):
+    T = TYPES[w]
+    bw = rng.integers(0, w + 1, n_vec).astype(np.uint8)
+    base = rng.integers(0, np.iinfo(T).max, n_vec, dtype=np.uint64, endpoint=True).astype(T)
+    chunks, offs, pos = [], [], 0
+    for v in range(n_vec):
+        b = int(bw[v])
+        x = rng.integers(0, np.iinfo(np.uint64).max, 1024, dtype=np.uint64, endpoint=True)
+        if b < 64:
+            x &= np.uint64((1 << b) - 1)
+        x = (x.astype(T) + base[v]).astype(T)
+        p = oracle.ffor(x, b, base[v]).view(np.uint8)
+        chunks.append(p)
+        offs.append(pos)
+        pos += p.size
+    return np.concatenate(chunks + [np.zeros(256, np.uint8)]), np.array(offs, np.uint64), bw, base
+
+
+def run(emu, w, enc, order, packed, off, bw, base, lane_base, n):
+    out = np.zeros(n * 1024, TYPES[w])
+    st = emu.emu_unffor(w, enc, order, P(packed), P(off), P(bw), P(None if base is None else base.view(np.uint8)),
+                        P(None if lane_base is None else lane_base.view(np.uint8)), ctypes.c_uint64(n), P(out))
+    return out, st
+
+
+@pytest.mark.parametrize("w", [8, 16, 32, 64])
+@pytest.mark.parametrize("order", [0, 1])
+def test_emulated_unffor(emu, w, order):
+    rng = np.random.default_rng(11 + w)
+    n = 24
+    _, _, bw, base = batch(w, n, rng)
+    bw[:2] = [0, w]  # always cover the edge widths
+    packed, off, _, _ = _rebuild(w, bw, base, rng)
+    got, st = run(emu, w, 1, order, packed, off, bw, base, None, n)
+    assert st == 0
+    assert np.array_equal(got, oracle.unffor_batch(packed, off, bw, base, order == 1))
+
+
+def _rebuild(w, bw, base, rng):
+    T = TYPES[w]
+    chunks, offs, pos = [], [], 0
+    for v in range(bw.size):
+        b = int(bw[v])
+        x = rng.integers(0, np.iinfo(np.uint64).max, 1024, dtype=np.uint64, endpoint=True)
+        if b < 64:
+            x &= np.uint64((1 << b) - 1)
+        x = (x.astype(T) + base[v]).astype(T)
+        p = oracle.ffor(x, b, base[v]).view(np.uint8)
+        chunks.append(p)
+        offs.append(pos)
+        pos += p.size
+    return np.concatenate(chunks + [np.zeros(256, np.uint8)]), np.array(offs, np.uint64), bw, base
+
+
+@pytest.mark.parametrize("w", [8, 16, 32, 64])
+@pytest.mark.parametrize("order", [0, 1])
+def test_emulated_rsum_and_delta(emu, w, order):
+    T = TYPES[w]
+    rng = np.random.default_rng(21 + w)
+    n = 12
+    L = 1024 // w
+    lb = rng.integers(0, np.iinfo(np.uint64).max, n * L, dtype=np.uint64, endpoint=True).astype(T)
+    packed, off, bw, base = batch(w, n, rng)
+    got, st = run(emu, w, 2, order, packed, off, bw, base, lb, n)
+    assert st == 0
+    assert np.array_equal(got, oracle.delta_batch(packed, off, bw, base, lb, order == 1))
+
+
+@pytest.mark.parametrize("w", [8, 16, 32, 64])
+def test_emulated_untranspose(emu, w):
+    T = TYPES[w]
+    rng = np.random.default_rng(31 + w)
+    n = 6
+    x = rng.integers(0, np.iinfo(np.uint64).max, n * 1024, dtype=np.uint64, endpoint=True).astype(T)
+    got, st = run(emu, w, 0, 1, x.view(np.uint8), None, None, None, None, n)
+    assert st == 0
+    want = np.concatenate([oracle.untranspose_i(x[v * 1024:(v + 1) * 1024].copy()) for v in range(n)])
+    assert np.array_equal(got, want)
+
+
+def test_emulated_rejects_bit_width_above_type(emu):
+    rng = np.random.default_rng(3)
+    packed, off, bw, base = batch(32, 3, rng)
+    bw[1] = 33
+    _, st = run(emu, 32, 1, 0, packed, off, bw, base, None, 3)
+    assert st & 2
