@@ -3,6 +3,7 @@
 #include "fls_decode.cu"
 #include "fls_runtime.h"
 
+#include <algorithm>
 #include <cstdio>
 #include <memory>
 #include <mutex>
@@ -13,10 +14,10 @@ namespace flsgpu {
 // ---------------------------------------------------------------------------------------------------------
 // Kernel families
 // ---------------------------------------------------------------------------------------------------------
-#define FLS_NUM64 64, 0u, 8, 8, 2
-#define FLS_NUM32 32, 0u, 4, 12, 3
+#define FLS_NUM64 64, 0u, 8, 12, 2
+#define FLS_NUM32 32, 0u, 4, 15, 3
 #define FLS_GATHER 32, 8320u, 8, 6, 2
-#define FLS_ANY 64, 8320u, 8, 5, 2
+#define FLS_ANY 64, 8320u, 8, 6, 2
 
 template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES>
 static cudaError_t launch_family(const DecodeArgs& a, cudaStream_t s, int sm_count, int grid_override) {
@@ -386,6 +387,11 @@ extern "C" {
 
 int fls_plan_create(const fls_vector_batch* batches, uint32_t n_batches, const uint32_t* d_queue, uint64_t n_items,
                     fls_plan** out_plan) {
+	return fls_plan_create_ex(batches, n_batches, d_queue, n_items, 0u, out_plan);
+}
+
+int fls_plan_create_ex(const fls_vector_batch* batches, uint32_t n_batches, const uint32_t* d_queue, uint64_t n_items,
+                       uint32_t flags, fls_plan** out_plan) {
 	if (!out_plan || !batches || n_batches == 0 || n_batches > 256) { return FLS_ERR_ARG; }
 	*out_plan = nullptr;
 	std::unique_ptr<fls_plan> p(new fls_plan());
@@ -430,6 +436,25 @@ int fls_plan_create(const fls_vector_batch* batches, uint32_t n_batches, const u
 				for (uint32_t v = 0; v < cols[i].n_vec; ++v) { q.push_back((i << 24) | v); }
 			}
 			n_items = total;
+		} else {
+			q.resize(n_items);
+			if (n_items && cudaMemcpy(q.data(), d_queue, sizeof(uint32_t) * n_items, cudaMemcpyDeviceToHost) !=
+			                   cudaSuccess) {
+				return FLS_ERR_CUDA;
+			}
+		}
+		for (uint32_t it : q) {
+			if ((it >> 24) >= n_batches || (it & 0xFFFFFFu) >= cols[it >> 24].n_vec) { return FLS_ERR_ARG; }
+		}
+		if (!(flags & FLS_PLAN_KEEP_ORDER)) {
+			// Group the work items by kernel specialisation (stream width, output size, encoding, order) so
+			// that the warps of the persistent kernel run long stretches of one code path; within a group the
+			// queue order is kept.  Outputs do not depend on the order.
+			auto key = [&](uint32_t it) {
+				const ColDesc& c = cols[it >> 24];
+				return (c.ws << 24) | (c.e << 16) | (c.enc << 8) | (c.post << 4) | c.order;
+			};
+			std::stable_sort(q.begin(), q.end(), [&](uint32_t x, uint32_t y) { return key(x) < key(y); });
 		}
 		if (cudaMalloc(&p->d_cols, sizeof(ColDesc) * n_batches) != cudaSuccess) { return FLS_ERR_CUDA; }
 		if (cudaMemcpy(p->d_cols, cols.data(), sizeof(ColDesc) * n_batches, cudaMemcpyHostToDevice) != cudaSuccess) {
@@ -437,10 +462,8 @@ int fls_plan_create(const fls_vector_batch* batches, uint32_t n_batches, const u
 		}
 		if (n_items > 0) {
 			if (cudaMalloc(&p->d_queue, sizeof(uint32_t) * n_items) != cudaSuccess) { return FLS_ERR_CUDA; }
-			const cudaError_t e = d_queue ? cudaMemcpy(p->d_queue, d_queue, sizeof(uint32_t) * n_items,
-			                                           cudaMemcpyDeviceToDevice)
-			                              : cudaMemcpy(p->d_queue, q.data(), sizeof(uint32_t) * n_items,
-			                                           cudaMemcpyHostToDevice);
+			const cudaError_t e =
+			    cudaMemcpy(p->d_queue, q.data(), sizeof(uint32_t) * n_items, cudaMemcpyHostToDevice);
 			if (e != cudaSuccess) { return FLS_ERR_CUDA; }
 		}
 		p->n_items = n_items;

@@ -263,6 +263,7 @@ __device__ __forceinline__ void store_vector(const typename OutT<E>::T (&o)[32],
 	constexpr uint32_t RL = run_len<WS>();
 	constexpr uint32_t RC = run_count<WS>();
 	if (original) {
+		__syncwarp(); // the staging buffer is the stage the packed words were just read from
 #pragma unroll
 		for (uint32_t r = 0; r < RC; ++r) {
 			const uint32_t b0 = run_start<WS>(t, r) * E;
@@ -365,6 +366,65 @@ __device__ __forceinline__ void decode_vector(const Plan& p, const uint8_t* stag
 	store_vector<WS, E>(o, p.out, ost, p.order != 0, t);
 }
 
+// Compact plan kept in shared memory between the lane-parallel metadata fetch and the use of the plan.
+struct __align__(16) PlanS {
+	const uint8_t* src;
+	uint8_t*       out;
+	uint64_t       for_base;
+	const uint8_t* lane_bases;
+	const uint8_t* gsrc;
+	const uint8_t* dict;
+	uint32_t       gbytes;
+	uint32_t       entry_c;
+	uint16_t       bytes;
+	uint8_t        bw, ws, e, enc, post, flags; // flags: bit0 original order, bit1 ok, bit2 valid item
+};
+static_assert(sizeof(PlanS) == 64, "PlanS layout");
+
+__device__ __forceinline__ PlanS pack_plan(const Plan& p, bool valid) {
+	PlanS s;
+	s.src        = p.src;
+	s.out        = p.out;
+	s.for_base   = p.for_base;
+	s.lane_bases = p.lane_bases;
+	s.gsrc       = p.gsrc;
+	s.dict       = p.dict;
+	s.gbytes     = p.gbytes;
+	s.entry_c    = p.entry_c;
+	s.bytes      = static_cast<uint16_t>(p.bytes);
+	s.bw         = static_cast<uint8_t>(p.bw > 255 ? 255 : p.bw);
+	s.ws         = p.ws;
+	s.e          = p.e;
+	s.enc        = p.enc;
+	s.post       = p.post;
+	s.flags      = static_cast<uint8_t>((p.order ? 1 : 0) | (p.ok ? 2 : 0) | (valid ? 4 : 0));
+	return s;
+}
+
+__device__ __forceinline__ Plan unpack_plan(const PlanS& s) {
+	Plan p;
+	p.src        = s.src;
+	p.out        = s.out;
+	p.for_base   = s.for_base;
+	p.lane_bases = s.lane_bases;
+	p.gsrc       = s.gsrc;
+	p.dict       = s.dict;
+	p.gbytes     = s.gbytes;
+	p.entry_c    = s.entry_c;
+	p.bytes      = s.bytes;
+	p.bw         = s.bw;
+	p.ws         = s.ws;
+	p.e          = s.e;
+	p.enc        = s.enc;
+	p.post       = s.post;
+	p.order      = s.flags & 1u;
+	p.ok         = (s.flags & 2u) != 0;
+	const uint32_t ve = p.post == POST_RLE ? p.e : 4u;
+	p.n_runs     = (p.post == POST_RLE || p.post == POST_RLE_DICT) ? p.gbytes / ve : 0u;
+	p.ghead      = static_cast<uint32_t>(reinterpret_cast<uintptr_t>(p.gsrc) & 15u);
+	return p;
+}
+
 #ifndef FLS_HOST_EMULATION
 __device__ __forceinline__ uint32_t item_col(uint32_t it) { return it >> 24; }
 __device__ __forceinline__ uint32_t item_vec(uint32_t it) { return it & 0xFFFFFFu; }
@@ -376,54 +436,105 @@ __device__ __forceinline__ Plan plan_of(const DecodeArgs& a, uint64_t item) {
 	return make_plan(c, item_vec(it));
 }
 
-// Kernel family: MAXWS bounds the staged stream (bytes per stage = MAXWS * 128), GSTAGE the run-value window,
-// EMAX the output element size (staging buffer = EMAX * 1024 bytes).
+// Kernel family: MAXWS bounds the staged stream (MAXWS * 128 bytes), GSTAGE the run-value window, EMAX the
+// output element size.  The original-order staging reuses the stage once its packed words are in registers,
+// so a slot is max(stream, output) bytes plus the run-value window.  Plans of the warp's next 2*PB items
+// live in shared memory (64 bytes each).
 template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES>
 struct Geometry {
-	static constexpr uint32_t kStage     = MAXWS * 128u;
-	static constexpr uint32_t kOut       = EMAX * 1024u;
-	static constexpr uint32_t kPerWarp   = 64u + STAGES * (kStage + GSTAGE) + kOut;
-	static constexpr uint32_t kSlack     = 256u; // extraction reads one row past the last stage
-	static constexpr uint32_t kSmem      = WARPS * kPerWarp + kSlack;
-	static constexpr int      kThreads   = WARPS * 32;
+	static constexpr uint32_t kPB      = 16;
+	static constexpr uint32_t kStage   = MAXWS * 128u;
+	static constexpr uint32_t kOut     = EMAX * 1024u;
+	static constexpr uint32_t kMain    = kStage > kOut ? kStage : kOut;
+	static constexpr uint32_t kSlot    = kMain + GSTAGE;
+	static constexpr uint32_t kPlans   = 2 * kPB * sizeof(PlanS);
+	static constexpr uint32_t kPerWarp = 64u + kPlans + STAGES * kSlot;
+	static constexpr uint32_t kSlack   = 256u; // extraction reads one row past the last stage
+	static constexpr uint32_t kSmem    = WARPS * kPerWarp + kSlack;
+	static constexpr int      kThreads = WARPS * 32;
+	static_assert(STAGES < kPB, "plans must run ahead of the copies");
 };
 
+template <int MAXWS, uint32_t GSTAGE, int EMAX>
+__device__ __forceinline__ void decode_dispatch(const Plan& p, uint8_t* st, const uint8_t* gs, uint32_t lane,
+                                                int* status) {
+	if (p.ws == 64) {
+		if constexpr (MAXWS >= 64) { decode_vector<64, 8>(p, st, gs, st, lane, status); }
+	} else if (p.ws == 32) {
+		if constexpr (MAXWS >= 32) {
+			if (p.e == 8) {
+				if constexpr (EMAX >= 8) { decode_vector<32, 8>(p, st, gs, st, lane, status); }
+			} else {
+				decode_vector<32, 4>(p, st, gs, st, lane, status);
+			}
+		}
+	} else if (p.ws == 16) {
+		if (p.e == 8) {
+			if constexpr (EMAX >= 8) { decode_vector<16, 8>(p, st, gs, st, lane, status); }
+		} else if (p.e == 4) {
+			if constexpr (EMAX >= 4) { decode_vector<16, 4>(p, st, gs, st, lane, status); }
+		} else {
+			decode_vector<16, 2>(p, st, gs, st, lane, status);
+		}
+	} else {
+		decode_vector<8, 1>(p, st, gs, st, lane, status);
+	}
+}
+
 template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES>
-__global__ void __launch_bounds__(WARPS * 32) k_decode(const DecodeArgs a) {
+__global__ void __launch_bounds__(WARPS * 32, 1) k_decode(const DecodeArgs a) {
 	using G = Geometry<MAXWS, GSTAGE, EMAX, WARPS, STAGES>;
+	constexpr uint32_t PB = G::kPB;
 	extern __shared__ __align__(128) uint8_t smem[];
-	const uint32_t lane  = threadIdx.x & 31u;
-	const uint32_t warp  = threadIdx.x >> 5;
-	uint8_t*       wbase = smem + warp * G::kPerWarp;
-	uint64_t*      bars  = reinterpret_cast<uint64_t*>(wbase);
-	uint8_t*       stages = wbase + 64;
-	uint8_t*       ost    = wbase + 64 + STAGES * (G::kStage + GSTAGE);
+	const uint32_t lane   = threadIdx.x & 31u;
+	const uint32_t warp   = threadIdx.x >> 5;
+	uint8_t*       wbase  = smem + warp * G::kPerWarp;
+	uint64_t*      bars   = reinterpret_cast<uint64_t*>(wbase);
+	PlanS*         plans  = reinterpret_cast<PlanS*>(wbase + 64);
+	uint8_t*       stages = wbase + 64 + G::kPlans;
 
 	if (lane == 0) {
 		for (int s = 0; s < STAGES; ++s) { mbar_init(&bars[s], 1); }
 		fence_mbar_init();
 	}
-	__syncwarp();
 
 	const uint64_t gw = static_cast<uint64_t>(blockIdx.x) * WARPS + warp;
 	const uint64_t nw = static_cast<uint64_t>(gridDim.x) * WARPS;
 	const uint64_t n  = a.n_items;
 
-	auto stage_ptr  = [&](int s) { return stages + s * (G::kStage + GSTAGE); };
-	auto gstage_ptr = [&](int s) { return stages + s * (G::kStage + GSTAGE) + G::kStage; };
+	auto stage_ptr  = [&](uint32_t s) { return stages + s * G::kSlot; };
+	auto gstage_ptr = [&](uint32_t s) { return stages + s * G::kSlot + G::kMain; };
+	// Lane-parallel metadata fetch: lane j resolves the plan of the warp's item blk*PB + j.
+	auto fill = [&](uint32_t blk) {
+		if (lane < PB) {
+			const uint64_t k    = static_cast<uint64_t>(blk) * PB + lane;
+			const uint64_t item = gw + k * nw;
+			Plan           p {};
+			const bool     valid = item < n;
+			if (valid) { p = plan_of(a, item); }
+			plans[k % (2 * PB)] = pack_plan(p, valid);
+		}
+	};
+	auto issue_k = [&](uint64_t k, uint32_t s) {
+		const PlanS& ps = plans[k % (2 * PB)];
+		if (ps.flags & 4u) { issue<GSTAGE>(unpack_plan(ps), stage_ptr(s), gstage_ptr(s), &bars[s], lane); }
+	};
 
-	// prologue: fill the ring
-	for (int s = 0; s < STAGES; ++s) {
-		const uint64_t item = gw + s * nw;
-		if (item < n) { issue<GSTAGE>(plan_of(a, item), stage_ptr(s), gstage_ptr(s), &bars[s], lane); }
-	}
+	fill(0);
+	fill(1);
+	__syncwarp();
+	for (uint32_t s = 0; s < STAGES; ++s) { issue_k(s, s); }
 
 	uint32_t k       = 0;
 	bool     aborted = false;
 	for (uint64_t item = gw; item < n; item += nw, ++k) {
-		const int      s      = static_cast<int>(k % STAGES);
+		if (k % PB == 0 && k > 0) {
+			fill(k / PB + 1);
+			__syncwarp();
+		}
+		const uint32_t s      = k % STAGES;
 		const uint32_t parity = (k / STAGES) & 1u;
-		const Plan     p      = plan_of(a, item);
+		const Plan     p      = unpack_plan(plans[k % (2 * PB)]);
 		if (!mbar_wait(&bars[s], parity)) {
 			if (lane == 0) { atomicOr(a.status, STATUS_TIMEOUT); }
 			aborted = true;
@@ -432,33 +543,10 @@ __global__ void __launch_bounds__(WARPS * 32) k_decode(const DecodeArgs a) {
 		if (!p.ok) {
 			if (lane == 0) { atomicOr(a.status, p.bw > p.ws ? STATUS_BAD_BW : STATUS_BAD_LAYOUT); }
 		} else {
-			const uint8_t* st = stage_ptr(s);
-			const uint8_t* gs = gstage_ptr(s);
-			if (p.ws == 64) {
-				if constexpr (MAXWS >= 64) { decode_vector<64, 8>(p, st, gs, ost, lane, a.status); }
-			} else if (p.ws == 32) {
-				if constexpr (MAXWS >= 32) {
-					if (p.e == 8) {
-						if constexpr (EMAX >= 8) { decode_vector<32, 8>(p, st, gs, ost, lane, a.status); }
-					} else {
-						decode_vector<32, 4>(p, st, gs, ost, lane, a.status);
-					}
-				}
-			} else if (p.ws == 16) {
-				if (p.e == 8) {
-					if constexpr (EMAX >= 8) { decode_vector<16, 8>(p, st, gs, ost, lane, a.status); }
-				} else if (p.e == 4) {
-					if constexpr (EMAX >= 4) { decode_vector<16, 4>(p, st, gs, ost, lane, a.status); }
-				} else {
-					decode_vector<16, 2>(p, st, gs, ost, lane, a.status);
-				}
-			} else {
-				decode_vector<8, 1>(p, st, gs, ost, lane, a.status);
-			}
+			decode_dispatch<MAXWS, GSTAGE, EMAX>(p, stage_ptr(s), gstage_ptr(s), lane, a.status);
 		}
 		__syncwarp();
-		const uint64_t next = item + STAGES * nw;
-		if (next < n) { issue<GSTAGE>(plan_of(a, next), stage_ptr(s), gstage_ptr(s), &bars[s], lane); }
+		issue_k(k + STAGES, s);
 	}
 	if (aborted) {
 		// Drain: every later stage this warp armed must land before the block's shared memory goes away.
@@ -469,7 +557,6 @@ __global__ void __launch_bounds__(WARPS * 32) k_decode(const DecodeArgs a) {
 		}
 	}
 }
-
 #endif // FLS_HOST_EMULATION
 
 } // namespace flsgpu

@@ -24,6 +24,8 @@ class _Batch(ctypes.Structure):
 
 declare("fls_plan_create", ctypes.c_int, [ctypes.POINTER(_Batch), ctypes.c_uint32, _p, ctypes.c_uint64,
                                           ctypes.POINTER(_p)])
+declare("fls_plan_create_ex", ctypes.c_int, [ctypes.POINTER(_Batch), ctypes.c_uint32, _p, ctypes.c_uint64,
+                                             ctypes.c_uint32, ctypes.POINTER(_p)])
 declare("fls_plan_decode", ctypes.c_int, [_p, _p])
 declare("fls_plan_decode_grid", ctypes.c_int, [_p, ctypes.c_int, _p])
 declare("fls_plan_destroy", ctypes.c_int, [_p])
@@ -90,7 +92,7 @@ def random_ffor_column(width, n_vec, rng, device, keep_values=False):
 class Plan:
     """A decode plan over several FFOR columns (fls_plan_create / fls_plan_decode)."""
 
-    def __init__(self, columns, outs, order, queue=None):
+    def __init__(self, columns, outs, order, queue=None, keep_order=False):
         batches = (_Batch * len(columns))()
         for i, (c, o) in enumerate(zip(columns, outs)):
             b = batches[i]
@@ -101,8 +103,8 @@ class Plan:
         self._keep = (columns, outs, queue)
         h = _p()
         n_items = queue.numel() if queue is not None else 0
-        check(lib.fls_plan_create(batches, len(columns), queue.data_ptr() if queue is not None else None, n_items,
-                                  ctypes.byref(h)), "fls_plan_create")
+        check(lib.fls_plan_create_ex(batches, len(columns), queue.data_ptr() if queue is not None else None, n_items,
+                                     1 if keep_order else 0, ctypes.byref(h)), "fls_plan_create")
         self.handle = h
 
     def decode(self, stream=None, grid=0):

@@ -163,6 +163,10 @@ typedef struct fls_plan fls_plan;
  * The queue is copied; the batches' device buffers must outlive the plan. */
 int fls_plan_create(const fls_vector_batch* batches, uint32_t n_batches, const uint32_t* d_queue, uint64_t n_items,
                     fls_plan** out_plan);
+/* flags of fls_plan_create_ex; fls_plan_create groups the queue by vector kind (flags = 0) */
+#define FLS_PLAN_KEEP_ORDER 1u /* take the work items exactly in queue order */
+int fls_plan_create_ex(const fls_vector_batch* batches, uint32_t n_batches, const uint32_t* d_queue,
+                       uint64_t n_items, uint32_t flags, fls_plan** out_plan);
 int fls_plan_decode(const fls_plan* plan, fls_stream_t stream);
 /* Same, with an explicit grid (CTAs); 0 = one wave of resident CTAs. */
 int fls_plan_decode_grid(const fls_plan* plan, int grid, fls_stream_t stream);

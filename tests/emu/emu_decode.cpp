@@ -40,7 +40,6 @@ static int emu_vector(const ColDesc& c, uint32_t v) {
 	std::vector<uint8_t> smem(3 * 8448 + 8192, 0xA5);
 	uint8_t*             stage  = smem.data();
 	uint8_t*             gstage = stage + 8448;
-	uint8_t*             ost    = gstage + 8448;
 	if (p.bytes) { std::memcpy(stage, p.src, p.bytes); }
 	if (p.gbytes) {
 		const uint32_t win = (p.ghead + p.gbytes + 15u) & ~15u;
@@ -54,7 +53,7 @@ static int emu_vector(const ColDesc& c, uint32_t v) {
 		th.emplace_back([&, t] {
 			g_emu_warp = &w;
 			g_emu_lane = t;
-			dispatch(p, stage, gstage, ost, static_cast<uint32_t>(t), &status);
+			dispatch(p, stage, gstage, stage, static_cast<uint32_t>(t), &status); // as on the GPU: staging reuses the stage
 		});
 	}
 	for (auto& x : th) { x.join(); }

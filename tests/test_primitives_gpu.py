@@ -168,3 +168,33 @@ def test_bit_width_above_type_width_is_reported_not_decoded(cuda):
     st = P.device_status()
     assert st & 2
     assert P.device_status() == 0
+
+
+@pytest.mark.parametrize("keep_order", [False, True])
+@pytest.mark.parametrize("order", [0, 1])
+def test_plan_mixed_batch_shuffled_queue(cuda, keep_order, order):
+    """One persistent launch over several columns of different widths with a shuffled work queue."""
+    import torch
+
+    from fastlanes_b200 import workloads as W
+
+    rng = np.random.default_rng(900 + order + 2 * keep_order)
+    cols, wants = [], []
+    for w, n in ((32, 300), (64, 200), (16, 100), (8, 50)):
+        packed, offs, bw, base, vals = _batch(w, n, rng)
+        c = W.FforColumn(w, _t(packed, cuda), _t(offs, cuda), _t(bw, cuda), _t(base, cuda))
+        cols.append(c)
+        wants.append(oracle.unffor_batch(packed, offs, bw, base, order == 1))
+    items = np.concatenate([(i << 24) | np.arange(c.n_vec, dtype=np.uint32) for i, c in enumerate(cols)])
+    items = items[rng.permutation(items.size)].astype(np.uint32)
+    queue = torch.from_numpy(items.view(np.int32)).to(cuda)
+    outs = [torch.zeros(c.n_vec * 1024, dtype=W._DT[c.width], device=cuda) for c in cols]
+    plan = W.Plan(cols, outs, order=order, queue=queue, keep_order=keep_order)
+    plan.decode()
+    torch.cuda.synchronize()
+    for o, want in zip(outs, wants):
+        assert np.array_equal(_np(o), want)
+    plan.close()
+    from fastlanes_b200 import primitives as P
+
+    assert P.device_status() == 0
