@@ -5,6 +5,7 @@ package is the Python face of that ABI.
 """
 from . import _lib  # noqa: F401  (raises if the CUDA library is missing)
 from . import primitives  # noqa: F401
+from . import pages  # noqa: F401
 from . import workloads  # noqa: F401
 
-__all__ = ["primitives", "workloads"]
+__all__ = ["pages", "primitives", "workloads"]

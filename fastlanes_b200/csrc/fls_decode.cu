@@ -50,8 +50,11 @@ __device__ __forceinline__ uint64_t ld_le(const uint8_t* p, uint32_t n) {
 	return x;
 }
 
+// Entry points sit at page offset 8 + 4*arr_c; a page may be placed at any byte address (it is placed so that
+// its packed buffer is 16-byte aligned), so they are read alignment-agnostically.
 __device__ __forceinline__ uint32_t ep_of(const ColDesc& c, uint32_t v, uint32_t i) {
-	return v == 0 ? 0u : c.ep[(v - 1) * c.arr_c + i];
+	if (v == 0) { return 0u; }
+	return static_cast<uint32_t>(ld_le(reinterpret_cast<const uint8_t*>(c.ep) + 4ull * ((v - 1) * c.arr_c + i), 4));
 }
 
 __device__ __forceinline__ Plan make_plan(const ColDesc& c, uint32_t v) {
@@ -338,28 +341,28 @@ __device__ __forceinline__ void decode_vector(const Plan& p, const uint8_t* stag
 #pragma unroll
 		for (int i = 0; i < 32; ++i) { o[i] = static_cast<OT>(v[i]); }
 	} else if (p.post == POST_RLE) {
-		const OT* vals = reinterpret_cast<const OT*>(gstage + p.ghead);
+		// run values keep the byte alignment they have inside the page
+		const uint8_t* vals = gstage + p.ghead;
 #pragma unroll
 		for (int i = 0; i < 32; ++i) {
 			const uint32_t idx = static_cast<uint32_t>(v[i]);
 			const bool     in  = idx < p.n_runs;
 			bad |= !in;
-			o[i] = in ? vals[idx] : OT(0);
+			o[i] = in ? static_cast<OT>(ld_le(vals + static_cast<uint64_t>(idx) * E, E)) : OT(0);
 		}
 	} else {
-		const OT* dict = reinterpret_cast<const OT*>(p.dict);
-		const uint32_t* codes = reinterpret_cast<const uint32_t*>(gstage + p.ghead);
+		const uint8_t* codes = gstage + p.ghead;
 #pragma unroll
 		for (int i = 0; i < 32; ++i) {
 			uint32_t code = static_cast<uint32_t>(v[i]);
 			if (p.post == POST_RLE_DICT) {
 				const bool in = code < p.n_runs;
 				bad |= !in;
-				code = in ? codes[code] : 0u;
+				code = in ? static_cast<uint32_t>(ld_le(codes + 4ull * code, 4)) : 0u;
 			}
 			const bool in = code < p.entry_c;
 			bad |= !in;
-			o[i] = in ? __ldg(dict + code) : OT(0);
+			o[i] = in ? static_cast<OT>(ld_le(p.dict + static_cast<uint64_t>(code) * E, E)) : OT(0);
 		}
 	}
 	if (__any_sync(0xFFFFFFFFu, bad) && t == 0) { atomicOr(status, STATUS_BAD_INDEX); }

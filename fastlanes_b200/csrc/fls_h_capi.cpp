@@ -1,0 +1,307 @@
+// The reference's C API (include/fastlanes.h) served by the GPU engine, with host buffers on both sides.
+//
+// encode_from_memory follows the single-column encoder of the reference (src/connection.cpp:150-167,
+// src/encoder/single_col_encoder.cpp:9-34, src/encoder/exp_col_encoder.cpp:40-64): the page of the chosen
+// expression, built from whole 1024-value vectors; the per-vector steps run on the GPU
+//   UNCOMPRESSED (id 0): transpose_i                         -> [values]
+//   FFOR        (id 1): transpose_i, analyze, ffor           -> [bw][base][packed]
+//   DELTA       (id 11): transpose_i, lane bases = row 0, unrsum, analyze, ffor
+//                                                            -> [lane bases][bw][base][packed]
+// (RPN tables include/fls/cor/exp/ffor/ffor_exp.hpp:35-53, include/fls/cor/exp/delta/delta_exp.hpp:39-56;
+// primitives src/cor/prm/{trs,rsum,ffor}/*_compress.cpp, src/cor/prm/ffor/ffor_analyze.cpp:77-102) and the
+// host writes the page framing (src/cor/eng/compressor.cpp:68-86).
+// decode_to_memory places the page in device memory with its packed buffer on a 16-byte boundary, decodes it
+// with the page engine and copies the values back.
+#include "fastlanes.h"
+#include "fls_b200.h"
+#include "fls_page.h"
+#include "fls_runtime.h"
+
+#include <cstring>
+#include <cuda_runtime.h>
+#include <mutex>
+#include <vector>
+
+struct Connection {
+	int magic = 0x464C5342; // "FLSB"
+};
+
+namespace flsgpu {
+namespace {
+
+cudaStream_t api_stream() {
+	static cudaStream_t s[64] {};
+	static std::mutex   mu;
+	int                 d = 0;
+	if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= 64) { return nullptr; }
+	std::lock_guard<std::mutex> lk(mu);
+	if (!s[d]) { cudaStreamCreateWithFlags(&s[d], cudaStreamNonBlocking); }
+	return s[d];
+}
+
+struct DevBuf {
+	void*        p = nullptr;
+	cudaStream_t s = nullptr;
+	explicit DevBuf(cudaStream_t st) : s(st) {}
+	bool alloc(size_t n) { return cudaMallocAsync(&p, n ? n : 16, s) == cudaSuccess; }
+	~DevBuf() {
+		if (p) { cudaFreeAsync(p, s); }
+	}
+	template <class T>
+	T* as() const {
+		return static_cast<T*>(p);
+	}
+};
+
+// Size of a page from its bytes: the last buffer is always the stream's packed (or raw) buffer, so its size is
+// the last vector's entry point plus that vector's packed size.
+int page_size_of(const uint8_t* page, PageInfo* pi, uint64_t* size, int value_width) {
+	int rc = parse_page_header(page, 8 + 4 * 6, pi);
+	if (rc != FLS_OK) { return rc; }
+	const ExprLayout* L    = pi->layout;
+	const uint32_t    last = pi->arr_c - 1;
+	if (pi->vec_c == 0) {
+		*size = pi->off[last];
+		return FLS_OK;
+	}
+	const uint32_t v  = pi->vec_c - 1u;
+	auto           ep = [&](uint32_t vv, uint32_t i) -> uint64_t {
+        if (vv == 0) { return 0; }
+        uint32_t x;
+        std::memcpy(&x, page + pi->ep_off + 4ull * ((vv - 1) * pi->arr_c + i), 4);
+        return x;
+	};
+	const uint32_t ws = L->ws ? L->ws : static_cast<uint32_t>(value_width);
+	uint64_t       part;
+	if (L->enc == ENC_RAW) {
+		part = ws * 128ull;
+	} else {
+		part = page[pi->off[L->ib_bw] + ep(v, L->ib_bw)] * 128ull;
+	}
+	*size = pi->off[last] + ep(v, last) + part;
+	return FLS_OK;
+}
+
+template <class T>
+int encode_t(const T* in, uint64_t n, uint64_t cap, uint8_t* out, uint64_t* out_size, uint64_t* mtd_size, bool sgn,
+             uint8_t expr) {
+	constexpr int      W     = sizeof(T) * 8;
+	constexpr uint32_t L     = 1024 / W;
+	const uint64_t     n_vec = n / 1024;
+	if (n_vec > 0xFFFFu) { return FLS_ERR_ARG; }
+	uint8_t  exp_t, arr_c;
+	switch (expr) {
+	case 0: exp_t = 2, arr_c = 1; break;
+	case 1: exp_t = 4, arr_c = 3; break;
+	case 11: exp_t = 5, arr_c = 4; break;
+	default: return FLS_ERR_UNSUPPORTED;
+	}
+	cudaStream_t s = api_stream();
+	if (!s) { return FLS_ERR_CUDA; }
+	const uint64_t bytes = n_vec * 1024 * sizeof(T);
+	DevBuf         d_in(s), d_tr(s), d_delta(s), d_bw(s), d_base(s), d_off(s), d_packed(s);
+	std::vector<uint8_t>  bw(n_vec);
+	std::vector<T>        base(n_vec);
+	std::vector<uint64_t> off(n_vec);
+	std::vector<T>        lane_bases;
+	uint64_t              packed_total = 0;
+	if (n_vec > 0) {
+		if (!d_in.alloc(bytes) || !d_tr.alloc(bytes)) { return FLS_ERR_CUDA; }
+		cudaMemcpyAsync(d_in.p, in, bytes, cudaMemcpyHostToDevice, s);
+		int rc;
+		if constexpr (W == 64) {
+			rc = fls_gpu_transpose_i_u64(d_in.as<uint64_t>(), d_tr.as<uint64_t>(), n_vec, s);
+		} else {
+			rc = fls_gpu_transpose_i_u32(d_in.as<uint32_t>(), d_tr.as<uint32_t>(), n_vec, s);
+		}
+		if (rc != FLS_OK) { return rc; }
+		if (expr != 0) {
+			const T* src = d_tr.as<T>();
+			if (expr == 11) {
+				lane_bases.resize(n_vec * L);
+				cudaMemcpy2DAsync(lane_bases.data(), 128, d_tr.p, 1024 * sizeof(T), 128, n_vec, cudaMemcpyDeviceToHost,
+				                  s);
+				if (!d_delta.alloc(bytes)) { return FLS_ERR_CUDA; }
+				if constexpr (W == 64) {
+					rc = fls_gpu_unrsum_u64(d_tr.as<uint64_t>(), d_delta.as<uint64_t>(), n_vec, s);
+				} else {
+					rc = fls_gpu_unrsum_u32(d_tr.as<uint32_t>(), d_delta.as<uint32_t>(), n_vec, s);
+				}
+				if (rc != FLS_OK) { return rc; }
+				src = d_delta.as<T>();
+			}
+			if (!d_bw.alloc(n_vec) || !d_base.alloc(n_vec * sizeof(T)) || !d_off.alloc(n_vec * 8)) {
+				return FLS_ERR_CUDA;
+			}
+			if constexpr (W == 64) {
+				rc = fls_gpu_analyze_u64(reinterpret_cast<const uint64_t*>(src), d_bw.as<uint8_t>(),
+				                         d_base.as<uint64_t>(), n_vec, sgn, s);
+			} else {
+				rc = fls_gpu_analyze_u32(reinterpret_cast<const uint32_t*>(src), d_bw.as<uint8_t>(),
+				                         d_base.as<uint32_t>(), n_vec, sgn, s);
+			}
+			if (rc != FLS_OK) { return rc; }
+			cudaMemcpyAsync(bw.data(), d_bw.p, n_vec, cudaMemcpyDeviceToHost, s);
+			cudaMemcpyAsync(base.data(), d_base.p, n_vec * sizeof(T), cudaMemcpyDeviceToHost, s);
+			if (cudaStreamSynchronize(s) != cudaSuccess) { return FLS_ERR_CUDA; }
+			for (uint64_t v = 0; v < n_vec; ++v) {
+				off[v] = packed_total;
+				packed_total += bw[v] * 128ull;
+			}
+			if (!d_packed.alloc(packed_total + 16)) { return FLS_ERR_CUDA; }
+			cudaMemcpyAsync(d_off.p, off.data(), n_vec * 8, cudaMemcpyHostToDevice, s);
+			if constexpr (W == 64) {
+				rc = fls_gpu_ffor_u64(reinterpret_cast<const uint64_t*>(src), d_packed.as<uint64_t>(), d_bw.as<uint8_t>(),
+				                      d_base.as<uint64_t>(), d_off.as<uint64_t>(), n_vec, s);
+			} else {
+				rc = fls_gpu_ffor_u32(reinterpret_cast<const uint32_t*>(src), d_packed.as<uint32_t>(), d_bw.as<uint8_t>(),
+				                      d_base.as<uint32_t>(), d_off.as<uint64_t>(), n_vec, s);
+			}
+			if (rc != FLS_OK) { return rc; }
+		}
+	}
+	// page framing: header, buffer offsets, entry points of vectors 1.., buffers
+	std::vector<uint64_t> buf_len(arr_c);
+	if (expr == 0) {
+		buf_len[0] = bytes;
+	} else {
+		const uint32_t first = expr == 11 ? 1 : 0;
+		if (expr == 11) { buf_len[0] = n_vec * 128; }
+		buf_len[first]     = n_vec;
+		buf_len[first + 1] = n_vec * sizeof(T);
+		buf_len[first + 2] = packed_total;
+	}
+	const uint64_t meta = 8 + 4ull * arr_c + 4ull * arr_c * (n_vec ? n_vec - 1 : 0);
+	uint64_t       total = meta;
+	for (auto b : buf_len) { total += b; }
+	if (out_size) { *out_size = total; }
+	if (mtd_size) { *mtd_size = meta; }
+	if (total > cap || !out) {
+		cudaStreamSynchronize(s);
+		return FLS_ERR_ARG;
+	}
+	uint8_t* p = out;
+	std::memset(p, 0, 8);
+	p[0]                 = exp_t;
+	p[1]                 = 1; // NO_PATCH / UNCOMPRESSED variant
+	const uint16_t vec_c = static_cast<uint16_t>(n_vec);
+	std::memcpy(p + 4, &vec_c, 2);
+	uint64_t boff[4];
+	boff[0] = meta;
+	for (uint32_t i = 1; i < arr_c; ++i) { boff[i] = boff[i - 1] + buf_len[i - 1]; }
+	for (uint32_t i = 0; i < arr_c; ++i) {
+		const uint32_t o = static_cast<uint32_t>(boff[i]);
+		std::memcpy(p + 8 + 4 * i, &o, 4);
+	}
+	uint8_t* ep = p + 8 + 4 * arr_c;
+	for (uint64_t v = 1; v < n_vec; ++v) {
+		uint32_t e[4];
+		if (expr == 0) {
+			e[0] = static_cast<uint32_t>(v * 1024 * sizeof(T));
+		} else {
+			uint32_t j = 0;
+			if (expr == 11) { e[j++] = static_cast<uint32_t>(v * 128); }
+			e[j++] = static_cast<uint32_t>(v);
+			e[j++] = static_cast<uint32_t>(v * sizeof(T));
+			e[j++] = static_cast<uint32_t>(off[v]);
+		}
+		std::memcpy(ep + 4ull * arr_c * (v - 1), e, 4ull * arr_c);
+	}
+	if (n_vec > 0) {
+		if (expr == 0) {
+			cudaMemcpyAsync(p + boff[0], d_tr.p, bytes, cudaMemcpyDeviceToHost, s);
+		} else {
+			const uint32_t first = expr == 11 ? 1 : 0;
+			if (expr == 11) { std::memcpy(p + boff[0], lane_bases.data(), n_vec * 128); }
+			std::memcpy(p + boff[first], bw.data(), n_vec);
+			std::memcpy(p + boff[first + 1], base.data(), n_vec * sizeof(T));
+			cudaMemcpyAsync(p + boff[first + 2], d_packed.p, packed_total, cudaMemcpyDeviceToHost, s);
+		}
+	}
+	return cudaStreamSynchronize(s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
+}
+
+int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_t out_cap, uint8_t dt,
+                     uint64_t* n_values) {
+	const int w = value_width_of(dt);
+	if (!page || w == 0 || dt == DOUBLE) { return FLS_ERR_UNSUPPORTED; }
+	PageInfo pi;
+	uint64_t computed = 0;
+	int      rc       = page_size_of(page, &pi, &computed, w);
+	if (rc != FLS_OK) { return rc; }
+	if (page_size == 0) { page_size = computed; }
+	if (computed > page_size) { return FLS_ERR_FORMAT; }
+	rc = finish_page_info(&pi, page_size);
+	if (rc != FLS_OK) { return rc; }
+	if (pi.layout->post != POST_NONE) { return FLS_ERR_FORMAT; } // the C API carries no dictionary
+	const uint64_t out_bytes = static_cast<uint64_t>(pi.vec_c) * 1024 * (w / 8);
+	if (n_values) { *n_values = static_cast<uint64_t>(pi.vec_c) * 1024; }
+	if (out_cap < out_bytes || !out) { return FLS_ERR_ARG; }
+	if (pi.vec_c == 0) { return FLS_OK; }
+	cudaStream_t s = api_stream();
+	if (!s) { return FLS_ERR_CUDA; }
+	const uint32_t shift = static_cast<uint32_t>((16 - pi.off[pi.layout->ib_packed] % 16) % 16);
+	DevBuf         d_page(s), d_out(s);
+	if (!d_page.alloc(page_size + 32) || !d_out.alloc(out_bytes)) { return FLS_ERR_CUDA; }
+	uint8_t* dp = d_page.as<uint8_t>() + shift;
+	cudaMemcpyAsync(dp, page, page_size, cudaMemcpyHostToDevice, s);
+	fls_page_column c {};
+	c.d_page    = dp;
+	c.page_size = page_size;
+	c.data_type = dt;
+	c.order     = FLS_ORIGINAL;
+	c.d_out     = d_out.p;
+	rc          = fls_gpu_decode_pages(&c, 1, s);
+	if (rc != FLS_OK) { return rc; }
+	cudaMemcpyAsync(out, d_out.p, out_bytes, cudaMemcpyDeviceToHost, s);
+	return cudaStreamSynchronize(s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
+}
+
+} // namespace
+} // namespace flsgpu
+
+using namespace flsgpu;
+
+extern "C" {
+
+connection_cpi* fls_cpi_connection_open() { return new Connection(); }
+
+void fls_cpi_connection_close(connection_cpi* c) { delete c; }
+
+int fls_encode_from_memory_status(void* in, uint64_t n, uint64_t cap, uint8_t* out, uint64_t* out_size,
+                                  uint64_t* mtd_size, enum data_t dt, uint8_t expr) {
+	if (!in && n >= 1024) { return FLS_ERR_ARG; }
+	switch (dt) {
+	case INT64: return encode_t(static_cast<const uint64_t*>(in), n, cap, out, out_size, mtd_size, true, expr);
+	case UINT64: return encode_t(static_cast<const uint64_t*>(in), n, cap, out, out_size, mtd_size, false, expr);
+	case INT32: return encode_t(static_cast<const uint32_t*>(in), n, cap, out, out_size, mtd_size, true, expr);
+	case UINT32: return encode_t(static_cast<const uint32_t*>(in), n, cap, out, out_size, mtd_size, false, expr);
+	default: return FLS_ERR_UNSUPPORTED;
+	}
+}
+
+bool encode_from_memory(void* in, uint64_t n, uint64_t cap, uint8_t* out, uint64_t* out_size, uint64_t* mtd_size,
+                        enum data_t dt, uint8_t expr) {
+	return fls_encode_from_memory_status(in, n, cap, out, out_size, mtd_size, dt, expr) == FLS_OK;
+}
+
+int fls_decode_to_memory_checked(const uint8_t* enc, uint64_t enc_size, void* out, uint64_t out_cap, enum data_t dt,
+                                 uint64_t* n_values) {
+	return decode_host_page(enc, enc_size, out, out_cap, dt, n_values);
+}
+
+void decode_to_memory(uint8_t* enc, void* out, enum data_t dt) {
+	// The reference API passes no sizes: the page size is derived from its own metadata and the caller
+	// provides room for vec_c * 1024 values, as with the reference.
+	(void)decode_host_page(enc, 0, out, ~0ull, dt, nullptr);
+}
+
+int fls_page_placement(const uint8_t* page_prefix, uint64_t prefix_size, uint32_t* shift) {
+	PageInfo pi;
+	const int rc = parse_page_header(page_prefix, prefix_size, &pi);
+	if (rc != FLS_OK) { return rc; }
+	if (shift) { *shift = static_cast<uint32_t>((16 - pi.off[pi.layout->ib_packed] % 16) % 16); }
+	return FLS_OK;
+}
+
+} // extern "C"

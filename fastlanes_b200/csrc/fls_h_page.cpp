@@ -1,0 +1,225 @@
+// Host side of the page path: reading FastLanes page metadata, mapping expressions onto the decode engine's
+// column descriptors, and the reference's C API (include/fastlanes.h).
+//
+// Page bytes (src/cor/eng/compressor.cpp:68-86, src/cor/lyt/page/page.cpp:63-139,
+// src/cor/lyt/page/entry_point.cpp:21-41, include/fls/cor/lyt/page/page_hdr.hpp:8-15):
+//   [PageHdr 8 B: exp_t u8, var u8, reserved u16, vec_c u16, pad u16]
+//   [arr_c x u32 absolute buffer offsets]
+//   [(vec_c - 1) x arr_c x u32 entry points (vector 0 starts every buffer at 0)]
+//   [buffer 0] ... [buffer arr_c - 1]
+// The buffer roles per expression come from the compress RPN tables (include/fls/cor/exp/*/*_exp.hpp) and the
+// compress primitives that fill them (src/cor/prm/{ffor,rsum,rle}/*_compress.cpp, src/cor/lyt/vec.cpp:40-120).
+#include "fastlanes.h"
+#include "fls_b200.h"
+#include "fls_page.h"
+#include "fls_runtime.h"
+
+#include <cstring>
+#include <cuda_runtime.h>
+#include <vector>
+
+namespace flsgpu {
+
+const ExprLayout* expr_layout(uint8_t exp_t, uint8_t var) {
+	// exp_t, var, arr_c, stream width (0 = value width), enc, post, roles: bw, base, packed, lane, vals, rec
+	static const ExprLayout table[] = {
+	    {2, 1, 1, 0, ENC_RAW, POST_NONE, kNoBuf, kNoBuf, 0, kNoBuf, kNoBuf, false},        // UNCOMPRESSED
+	    {4, 1, 3, 0, ENC_FFOR, POST_NONE, 0, 1, 2, kNoBuf, kNoBuf, false},                  // FFOR NO_PATCH
+	    {5, 1, 4, 0, ENC_DELTA, POST_NONE, 1, 2, 3, 0, kNoBuf, false},                      // DELTA NO_PATCH
+	    {6, 1, 2, 16, ENC_RAW, POST_RLE, kNoBuf, kNoBuf, 1, kNoBuf, 0, false},               // RLE UNCOMPRESSED
+	    {6, 2, 5, 16, ENC_DELTA, POST_RLE, 2, 3, 4, 1, 0, false},                            // RLE DELTA_NO_PATCH
+	    {6, 4, 5, 16, ENC_DELTA, POST_RLE, 2, 3, 4, 1, 0, true},                             // RLE DELTA_NO_PATCH_REC
+	    {8, 1, 1, 32, ENC_RAW, POST_DICT, kNoBuf, kNoBuf, 0, kNoBuf, kNoBuf, false},         // DICT UNCOMPRESSED
+	    {8, 2, 3, 32, ENC_FFOR, POST_DICT, 0, 1, 2, kNoBuf, kNoBuf, false},                  // DICT FFOR_NO_PATCH
+	    {8, 7, 4, 32, ENC_DELTA, POST_DICT, 1, 2, 3, 0, kNoBuf, false},                      // DICT DELTA_NO_PATCH
+	    {11, 1, 2, 16, ENC_RAW, POST_RLE_DICT, kNoBuf, kNoBuf, 1, kNoBuf, 0, false},         // DICT_RLE UNCOMPRESSED
+	    {11, 2, 5, 16, ENC_DELTA, POST_RLE_DICT, 2, 3, 4, 1, 0, false},                      // DICT_RLE DELTA_NO_PATCH
+	    {11, 4, 5, 16, ENC_DELTA, POST_RLE_DICT, 2, 3, 4, 1, 0, true},                       // DICT_RLE ..._REC
+	};
+	for (const auto& e : table) {
+		if (e.exp_t == exp_t && e.var == var) { return &e; }
+	}
+	return nullptr;
+}
+
+int value_width_of(uint8_t data_type) {
+	switch (data_type) {
+	case INT64:
+	case UINT64:
+	case DOUBLE: return 64;
+	case INT32:
+	case UINT32: return 32;
+	case INT16:
+	case UINT16: return 16;
+	case INT8:
+	case UINT8: return 8;
+	default: return 0;
+	}
+}
+
+int parse_page_header(const uint8_t* hdr, uint64_t avail, PageInfo* out) {
+	if (avail < 8) { return FLS_ERR_FORMAT; }
+	PageInfo pi {};
+	pi.exp_t = hdr[0];
+	pi.var   = hdr[1];
+	std::memcpy(&pi.vec_c, hdr + 4, 2);
+	pi.layout = expr_layout(pi.exp_t, pi.var);
+	if (!pi.layout) { return FLS_ERR_UNSUPPORTED; }
+	pi.arr_c = pi.layout->arr_c;
+	if (avail < 8ull + 4ull * pi.arr_c) { return FLS_ERR_FORMAT; }
+	for (uint32_t i = 0; i < pi.arr_c; ++i) { std::memcpy(&pi.off[i], hdr + 8 + 4 * i, 4); }
+	pi.ep_off  = 8 + 4 * pi.arr_c;
+	pi.meta_sz = pi.ep_off + 4ull * pi.arr_c * (pi.vec_c ? pi.vec_c - 1 : 0);
+	*out       = pi;
+	return FLS_OK;
+}
+
+int finish_page_info(PageInfo* pi, uint64_t page_size) {
+	if (pi->vec_c == 0) { return FLS_OK; }
+	if (pi->meta_sz > page_size) { return FLS_ERR_FORMAT; }
+	for (uint32_t i = 0; i < pi->arr_c; ++i) {
+		const uint64_t end = (i + 1 < pi->arr_c) ? pi->off[i + 1] : page_size;
+		if (pi->off[i] < pi->meta_sz || pi->off[i] > end || end > page_size) { return FLS_ERR_FORMAT; }
+		pi->size[i] = end - pi->off[i];
+	}
+	return FLS_OK;
+}
+
+int build_page_column(const PageInfo& pi, const uint8_t* d_page, int value_width, const uint8_t* d_dict_vals,
+                      uint32_t dict_entries, int order, uint8_t* d_out, ColDesc* c) {
+	const ExprLayout* L = pi.layout;
+	if (!L || value_width == 0) { return FLS_ERR_UNSUPPORTED; }
+	if (L->rec_vals) { return FLS_ERR_UNSUPPORTED; } // the page-level rec buffer is decoded by the caller
+	*c        = ColDesc {};
+	c->ws     = static_cast<uint8_t>(L->ws ? L->ws : value_width);
+	c->e      = static_cast<uint8_t>(value_width / 8);
+	c->enc    = L->enc;
+	c->post   = L->post;
+	c->order  = static_cast<uint8_t>(order);
+	c->layout = LAYOUT_PAGE;
+	c->arr_c  = static_cast<uint8_t>(pi.arr_c);
+	c->n_vec  = pi.vec_c;
+	c->ib_bw  = L->ib_bw;
+	c->ib_base = L->ib_base;
+	c->ib_packed = L->ib_packed;
+	c->ib_lane_bases = L->ib_lane;
+	c->ib_vals = L->ib_vals;
+	for (uint32_t i = 0; i < pi.arr_c; ++i) {
+		c->buf[i]      = d_page + pi.off[i];
+		c->buf_size[i] = pi.size[i];
+	}
+	c->ep  = reinterpret_cast<const uint32_t*>(d_page + pi.ep_off);
+	c->out = d_out;
+	if (L->post == POST_DICT || L->post == POST_RLE_DICT) {
+		if (!d_dict_vals || dict_entries == 0) { return FLS_ERR_FORMAT; }
+		c->dict    = d_dict_vals;
+		c->entry_c = dict_entries;
+	}
+	return FLS_OK;
+}
+
+int int_dictionary_values(const uint8_t* dict, uint64_t dict_size, int value_width, uint64_t* vals_off,
+                          uint32_t* entries) {
+	// only the first 20 bytes of dict are read; dict_size bounds the values
+	// dict_hdr_t {exp_t u8, emp u8, emp u8, version u8, entry_c u32} (include/fls/cor/lyt/dic/dic.hpp:32-41)
+	// followed by the dictionary values as a rec buffer (src/cor/lyt/dic/dic.cpp:142-144); rec_hdr
+	// {bw u8, pad u8, exc_c u16, base[8]} (include/fls/cor/lyt/rec_hdr.hpp:7-13).  The raw form (bw = 255,
+	// byte count in base) is a zero-copy view; FFOR blocks are not on this path.
+	if (dict_size < 8 + 12) { return FLS_ERR_FORMAT; }
+	uint32_t entry_c = 0;
+	std::memcpy(&entry_c, dict + 4, 4);
+	if (dict[8] != 255) { return FLS_ERR_UNSUPPORTED; }
+	uint64_t raw = 0;
+	std::memcpy(&raw, dict + 12, 8);
+	const uint64_t need = static_cast<uint64_t>(entry_c) * (value_width / 8);
+	if (raw != need || 20 + raw > dict_size) { return FLS_ERR_FORMAT; }
+	*vals_off = 20;
+	*entries  = entry_c;
+	return FLS_OK;
+}
+
+} // namespace flsgpu
+
+#ifndef FLS_HOST_EMULATION
+// =========================================================================================================
+// C ABI: page columns
+// =========================================================================================================
+using namespace flsgpu;
+
+extern "C" {
+
+int fls_page_info(const uint8_t* page_prefix, uint64_t prefix_size, uint32_t* exp_t, uint32_t* var,
+                  uint32_t* vec_c, uint32_t* arr_c, uint64_t* meta_size) {
+	PageInfo pi;
+	const int rc = parse_page_header(page_prefix, prefix_size, &pi);
+	if (rc != FLS_OK) { return rc; }
+	if (exp_t) { *exp_t = pi.exp_t; }
+	if (var) { *var = pi.var; }
+	if (vec_c) { *vec_c = pi.vec_c; }
+	if (arr_c) { *arr_c = pi.arr_c; }
+	if (meta_size) { *meta_size = pi.meta_sz; }
+	return FLS_OK;
+}
+
+int fls_gpu_decode_pages(const fls_page_column* cols, uint32_t n_cols, fls_stream_t stream) {
+	if (!cols || n_cols == 0 || n_cols > 255) { return FLS_ERR_ARG; }
+	std::vector<ColDesc>  descs(n_cols);
+	std::vector<uint32_t> queue;
+	Family                fam   = Family::NUM;
+	bool                  any64 = false;
+	for (uint32_t i = 0; i < n_cols; ++i) {
+		const fls_page_column& pc = cols[i];
+		const int              w  = value_width_of(pc.data_type);
+		if (!pc.d_page || !pc.d_out || w == 0 || pc.order > FLS_ORIGINAL) { return FLS_ERR_ARG; }
+		if ((reinterpret_cast<uintptr_t>(pc.d_out) & 15u) != 0) { return FLS_ERR_ARG; }
+		uint8_t hdr[8 + 4 * 8];
+		const uint64_t take = pc.page_size < sizeof(hdr) ? pc.page_size : sizeof(hdr);
+		if (cudaMemcpy(hdr, pc.d_page, take, cudaMemcpyDeviceToHost) != cudaSuccess) { return FLS_ERR_CUDA; }
+		PageInfo pi;
+		int      rc = parse_page_header(hdr, take, &pi);
+		if (rc == FLS_OK) { rc = finish_page_info(&pi, pc.page_size); }
+		if (rc != FLS_OK) { return rc; }
+		const uint8_t* dvals   = nullptr;
+		uint32_t       entries = 0;
+		if (pi.layout->post == POST_DICT || pi.layout->post == POST_RLE_DICT) {
+			if (!pc.d_dict || pc.dict_size < 20) { return FLS_ERR_FORMAT; }
+			uint8_t dh[20];
+			if (cudaMemcpy(dh, pc.d_dict, 20, cudaMemcpyDeviceToHost) != cudaSuccess) { return FLS_ERR_CUDA; }
+			uint64_t voff = 0;
+			rc            = int_dictionary_values(dh, pc.dict_size, w, &voff, &entries);
+			if (rc != FLS_OK) { return rc; }
+			dvals = pc.d_dict + voff;
+		}
+		rc = build_page_column(pi, pc.d_page, w, dvals, entries, pc.order, static_cast<uint8_t*>(pc.d_out), &descs[i]);
+		if (rc != FLS_OK) { return rc; }
+		if (descs[i].post != POST_NONE) { fam = Family::GATHER; }
+		if (descs[i].ws == 64) { any64 = true; }
+		for (uint32_t v = 0; v < pi.vec_c; ++v) { queue.push_back((i << 24) | v); }
+	}
+	if (fam == Family::GATHER && any64) { fam = Family::ANY; }
+	if (queue.empty()) { return FLS_OK; }
+	cudaStream_t s = static_cast<cudaStream_t>(stream);
+	DecodeArgs   a {};
+	if (n_cols == 1) {
+		a.col0    = descs[0];
+		a.n_items = queue.size();
+		return launch_decode(fam, a, s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
+	}
+	ColDesc*  d_cols  = nullptr;
+	uint32_t* d_queue = nullptr;
+	if (cudaMallocAsync(&d_cols, sizeof(ColDesc) * n_cols, s) != cudaSuccess) { return FLS_ERR_CUDA; }
+	if (cudaMallocAsync(&d_queue, sizeof(uint32_t) * queue.size(), s) != cudaSuccess) { return FLS_ERR_CUDA; }
+	cudaMemcpyAsync(d_cols, descs.data(), sizeof(ColDesc) * n_cols, cudaMemcpyHostToDevice, s);
+	cudaMemcpyAsync(d_queue, queue.data(), sizeof(uint32_t) * queue.size(), cudaMemcpyHostToDevice, s);
+	a.cols    = d_cols;
+	a.queue   = d_queue;
+	a.n_items = queue.size();
+	// copies from pageable host memory are staged before cudaMemcpyAsync returns, so descs/queue may go away
+	const cudaError_t e = launch_decode(fam, a, s);
+	cudaFreeAsync(d_cols, s);
+	cudaFreeAsync(d_queue, s);
+	return e == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
+}
+
+} // extern "C"
+#endif // FLS_HOST_EMULATION

@@ -1,0 +1,37 @@
+// Page metadata and the expression table shared by the host modules.
+#pragma once
+
+#include "fls_plan.h"
+#include <cstdint>
+
+namespace flsgpu {
+
+struct ExprLayout {
+	uint8_t exp_t, var, arr_c;
+	uint8_t ws; // stream width in bits; 0 = the column's value width
+	uint8_t enc, post;
+	uint8_t ib_bw, ib_base, ib_packed, ib_lane, ib_vals;
+	bool    rec_vals; // buffer ib_vals is a rec buffer (..._REC variants)
+};
+
+struct PageInfo {
+	uint8_t           exp_t = 0, var = 0;
+	uint16_t          vec_c = 0;
+	uint32_t          arr_c = 0;
+	uint32_t          off[6] {};
+	uint64_t          size[6] {};
+	uint64_t          ep_off  = 0;
+	uint64_t          meta_sz = 0;
+	const ExprLayout* layout  = nullptr;
+};
+
+const ExprLayout* expr_layout(uint8_t exp_t, uint8_t var);
+int               value_width_of(uint8_t data_type);
+int               parse_page_header(const uint8_t* hdr, uint64_t avail, PageInfo* out);
+int               finish_page_info(PageInfo* pi, uint64_t page_size);
+int build_page_column(const PageInfo& pi, const uint8_t* d_page, int value_width, const uint8_t* d_dict_vals,
+                      uint32_t dict_entries, int order, uint8_t* d_out, ColDesc* c);
+int int_dictionary_values(const uint8_t* dict, uint64_t dict_size, int value_width, uint64_t* vals_off,
+                          uint32_t* entries);
+
+} // namespace flsgpu

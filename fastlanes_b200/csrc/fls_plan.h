@@ -31,7 +31,7 @@ enum : uint8_t {
 
 constexpr uint8_t kNoBuf = 0xFF;
 
-struct __align__(16) ColDesc {
+struct alignas(16) ColDesc {
 	// what
 	uint8_t  ws;     // stream width in bits: 8, 16, 32, 64
 	uint8_t  e;      // output element size in bytes: 1, 2, 4, 8

@@ -1,0 +1,94 @@
+"""Reference page columns and the reference's C API (include/fastlanes.h), on the GPU engine."""
+import ctypes
+
+import numpy as np
+
+from ._lib import FlsError, check, declare
+
+_p = ctypes.c_void_p
+_u64 = ctypes.c_uint64
+
+# data_t values of include/fastlanes.h
+INT64, UINT64, INT32, UINT32, INT16, UINT16 = 5, 9, 4, 8, 3, 7
+DTYPE_OF = {INT64: np.int64, UINT64: np.uint64, INT32: np.int32, UINT32: np.uint32, INT16: np.int16,
+            UINT16: np.uint16}
+
+
+class PageColumn(ctypes.Structure):
+    _fields_ = [("d_page", _p), ("page_size", _u64), ("d_dict", _p), ("dict_size", _u64), ("data_type", ctypes.c_uint8),
+                ("order", ctypes.c_uint8), ("reserved", ctypes.c_uint8 * 6), ("d_out", _p)]
+
+
+_decode_pages = declare("fls_gpu_decode_pages", ctypes.c_int, [ctypes.POINTER(PageColumn), ctypes.c_uint32, _p])
+_page_info = declare("fls_page_info", ctypes.c_int, [_p, _u64, ctypes.POINTER(ctypes.c_uint32),
+                                                     ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32),
+                                                     ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(_u64)])
+_placement = declare("fls_page_placement", ctypes.c_int, [_p, _u64, ctypes.POINTER(ctypes.c_uint32)])
+_enc_status = declare("fls_encode_from_memory_status", ctypes.c_int, [_p, _u64, _u64, _p, ctypes.POINTER(_u64),
+                                                                        ctypes.POINTER(_u64), ctypes.c_uint8,
+                                                                        ctypes.c_uint8])
+_dec_checked = declare("fls_decode_to_memory_checked", ctypes.c_int, [_p, _u64, _p, _u64, ctypes.c_uint8,
+                                                                       ctypes.POINTER(_u64)])
+declare("encode_from_memory", ctypes.c_bool, [_p, _u64, _u64, _p, ctypes.POINTER(_u64), ctypes.POINTER(_u64),
+                                              ctypes.c_uint8, ctypes.c_uint8])
+declare("decode_to_memory", None, [_p, _p, ctypes.c_uint8])
+declare("fls_cpi_connection_open", _p, [])
+declare("fls_cpi_connection_close", None, [_p])
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_p)
+
+
+def page_info(page):
+    page = np.ascontiguousarray(page, np.uint8)
+    e, v, n, a = (ctypes.c_uint32() for _ in range(4))
+    m = _u64()
+    check(_page_info(_ptr(page), page.size, ctypes.byref(e), ctypes.byref(v), ctypes.byref(n), ctypes.byref(a),
+                     ctypes.byref(m)), "page_info")
+    return {"exp_t": e.value, "var": v.value, "vec_c": n.value, "arr_c": a.value, "meta_size": m.value}
+
+
+def placement(page):
+    page = np.ascontiguousarray(page, np.uint8)
+    s = ctypes.c_uint32()
+    check(_placement(_ptr(page), page.size, ctypes.byref(s)), "placement")
+    return s.value
+
+
+def decode_pages(columns, stream=None):
+    """columns: list of dicts with d_page, page_size, d_dict, dict_size, data_type, order, d_out (device ptrs)."""
+    import torch
+
+    arr = (PageColumn * len(columns))()
+    for i, c in enumerate(columns):
+        a = arr[i]
+        a.d_page, a.page_size = c["d_page"], c["page_size"]
+        a.d_dict, a.dict_size = c.get("d_dict"), c.get("dict_size", 0)
+        a.data_type, a.order, a.d_out = c["data_type"], c.get("order", 1), c["d_out"]
+    s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    check(_decode_pages(arr, len(columns), s), "fls_gpu_decode_pages")
+
+
+def encode_from_memory(values, data_type, expr_id, capacity=None):
+    """fastlanes.h encode_from_memory on a host array; returns (page bytes, metadata size)."""
+    values = np.ascontiguousarray(values, DTYPE_OF[data_type])
+    cap = capacity if capacity is not None else values.nbytes * 2 + 65536
+    out = np.zeros(cap, np.uint8)
+    size, mtd = _u64(), _u64()
+    rc = _enc_status(_ptr(values), values.size, cap, _ptr(out), ctypes.byref(size), ctypes.byref(mtd), data_type,
+                     expr_id)
+    if rc != 0:
+        raise FlsError(f"encode_from_memory: {rc}")
+    return out[: size.value].copy(), mtd.value
+
+
+def decode_to_memory(page, data_type, size=None):
+    """fastlanes.h decode_to_memory on host bytes; returns the decoded values (original order)."""
+    page = np.ascontiguousarray(page, np.uint8)
+    info = page_info(page)
+    out = np.zeros(info["vec_c"] * 1024, DTYPE_OF[data_type])
+    n = _u64()
+    check(_dec_checked(_ptr(page), page.size if size is None else size, _ptr(out), out.nbytes, data_type,
+                       ctypes.byref(n)), "decode_to_memory")
+    return out

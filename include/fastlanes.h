@@ -1,0 +1,90 @@
+/* fastlanes.h — the reference's C API (cwida/FastLanes include/fastlanes.h:14-111), served by the B200 engine.
+ *
+ * Same names, argument meaning and enum values as the reference, so a program written against the reference
+ * links against libfls_b200.so unchanged.  encode_from_memory encodes on the GPU and frames the result as a
+ * FastLanes page (bit-identical to the reference's page for the same input); decode_to_memory decodes on the
+ * GPU.  Both take HOST pointers and copy through device memory.  Besides the reference's INT64 expressions
+ * 0 (UNCOMPRESSED), 1 (FFOR) and 11 (DELTA), the engine also accepts UINT32 / INT32 / UINT64 columns with the
+ * same framing (T = the 32/64-bit type).
+ */
+#ifndef FASTLANES_H
+#define FASTLANES_H
+
+#include <stdbool.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* datatype — values of include/fastlanes.h:14-34 */
+enum data_t : uint8_t {
+	INVALID    = 0,
+	DOUBLE     = 1,
+	INT8       = 2,
+	INT16      = 3,
+	INT32      = 4,
+	INT64      = 5,
+	UINT8      = 6,
+	UINT16     = 7,
+	UINT32     = 8,
+	UINT64     = 9,
+	STR        = 10,
+	BOOLEAN    = 11,
+	DATE       = 12,
+	FLOAT      = 13,
+	BYTE_ARRAY = 14,
+	LIST       = 15,
+	STRUCT     = 16,
+	MAP        = 17,
+	FALLBACK   = 18,
+};
+
+/* int64 expression ids — include/fastlanes.h:37-41 */
+enum i64_expr_encoding_t : uint8_t {
+	I64_UNCOMPRESSED   = 0,
+	I64_FFOR_NO_PATCH  = 1,
+	I64_DELTA_NO_PATCH = 11,
+};
+
+/* double expression ids — include/fastlanes.h:44-47 (ALP is outside the decode path of this engine) */
+enum dbl_expr_encoding_t : uint8_t {
+	DBL_UNCOMPRESSED = 0,
+	DBL_ALP          = 1,
+};
+
+typedef struct Connection connection_cpi;
+
+/* include/fastlanes.h:53-54 */
+connection_cpi* fls_cpi_connection_open();
+void            fls_cpi_connection_close(connection_cpi* fls_connection);
+
+/* include/fastlanes.h:72-79: encode in_n_input values (whole 1024-value vectors; a tail of n % 1024 values is
+ * dropped, as the reference's encoder does).  Returns false when the encoded page does not fit in_capacity or
+ * the type / expression is not supported.  out_metadadata_size receives the page's header + offsets + entry
+ * points size. */
+bool encode_from_memory(void*       in_data,
+                        uint64_t    in_n_input,
+                        uint64_t    in_capacity,
+                        uint8_t*    out_encoded_data,
+                        uint64_t*   out_encoded_size,
+                        uint64_t*   out_metadadata_size,
+                        enum data_t in_datatype,
+                        uint8_t     in_expression_type);
+
+/* include/fastlanes.h:84-86: decode a page into vec_c * 1024 values (original order). */
+void decode_to_memory(uint8_t* in_encoded_data, void* out_data, enum data_t in_datatype);
+
+/* Status-returning forms of the two calls above (0 = ok, fls_status_code of fls_b200.h otherwise).
+ * fls_decode_to_memory_checked also bounds the input by in_encoded_size and reports the vector count. */
+int fls_encode_from_memory_status(void* in_data, uint64_t in_n_input, uint64_t in_capacity, uint8_t* out_encoded_data,
+                                  uint64_t* out_encoded_size, uint64_t* out_metadadata_size, enum data_t in_datatype,
+                                  uint8_t in_expression_type);
+int fls_decode_to_memory_checked(const uint8_t* in_encoded_data, uint64_t in_encoded_size, void* out_data,
+                                 uint64_t out_capacity_bytes, enum data_t in_datatype, uint64_t* out_n_values);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FASTLANES_H */

@@ -174,6 +174,35 @@ int fls_plan_destroy(fls_plan* plan);
 /* Shape of the kernel a plan launches: threads per CTA, dynamic shared memory, resident CTAs per SM. */
 int fls_plan_geometry(const fls_plan* plan, int* threads, int* smem_bytes, int* ctas_per_sm);
 
+/* ---------------------------------------------------------------------------------------------------------
+ * Reference page columns on the device.  d_page holds the bytes of one FastLanes page (the data_buf of
+ * ExpColEncoder, src/encoder/exp_col_encoder.cpp:40-64); d_dict the dictionary bytes for DICT / DICT_RLE
+ * expressions.  Replaces TColDecoder::{ExtInitDict, InitDecompress, Decompress} plus the materialisation of
+ * include/fls/encoder/assert_eq.hpp:50-400 for the integer expressions: UNCOMPRESSED, FFOR, DELTA, RLE
+ * (UNCOMPRESSED / DELTA_NO_PATCH), DICT (UNCOMPRESSED / FFOR / DELTA), DICT_RLE (UNCOMPRESSED / DELTA).
+ * d_page may sit at any byte address and d_out must be 16-byte aligned; a packed buffer that starts 16-byte
+ * aligned is staged by TMA (fls_page_placement gives the shift that achieves it), any other by the warp.
+ * Several columns decode in one launch.
+ * ------------------------------------------------------------------------------------------------------- */
+typedef struct {
+	const uint8_t* d_page;
+	uint64_t       page_size;
+	const uint8_t* d_dict; /* NULL unless the expression has a dictionary */
+	uint64_t       dict_size;
+	uint8_t        data_type; /* enum data_t of fastlanes.h: INT64, UINT64, INT32, UINT32, INT16, UINT16 */
+	uint8_t        order;     /* fls_order_code; FLS_ORIGINAL is what the reference materialises */
+	uint8_t        reserved[6];
+	void*          d_out; /* vec_c * 1024 values of data_type */
+} fls_page_column;
+
+/* Header facts of a page from its first bytes (prefix_size >= 8 + 4 * arr_c). */
+int fls_page_info(const uint8_t* page_prefix, uint64_t prefix_size, uint32_t* exp_t, uint32_t* var, uint32_t* vec_c,
+                  uint32_t* arr_c, uint64_t* meta_size);
+/* Byte shift (0..15) to add to a 16-byte aligned device address so that the page's packed buffer lands on a
+ * 16-byte boundary. */
+int fls_page_placement(const uint8_t* page_prefix, uint64_t prefix_size, uint32_t* shift);
+int fls_gpu_decode_pages(const fls_page_column* cols, uint32_t n_cols, fls_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -3,6 +3,8 @@
 // harness fills the way the kernel's bulk copies would.  Used by tests/test_device_logic_emulated.py.
 #define FLS_HOST_EMULATION 1
 #include "fls_decode.cu"
+#include "fls_page.h"
+#include "fls_b200.h"
 
 #include <thread>
 #include <vector>
@@ -84,5 +86,26 @@ extern "C" int emu_unffor(int width, int enc, int order, const uint8_t* packed, 
 	c.base_arr      = base;
 	c.lane_base_arr = lane_base;
 	c.out           = out;
+	return emu_decode_column(&c);
+}
+
+// Decode a reference page (host bytes) with the product's host page code + the emulated device logic.
+extern "C" int emu_decode_page(const uint8_t* page, uint64_t page_size, const uint8_t* dict, uint64_t dict_size,
+                               int value_width, int order, uint8_t* out) {
+	PageInfo pi;
+	int      rc = parse_page_header(page, page_size, &pi);
+	if (rc == FLS_OK) { rc = finish_page_info(&pi, page_size); }
+	if (rc != FLS_OK) { return -1000 + rc; }
+	const uint8_t* dvals   = nullptr;
+	uint32_t       entries = 0;
+	if (pi.layout->post == POST_DICT || pi.layout->post == POST_RLE_DICT) {
+		uint64_t voff = 0;
+		rc            = int_dictionary_values(dict, dict_size, value_width, &voff, &entries);
+		if (rc != FLS_OK) { return -2000 + rc; }
+		dvals = dict + voff;
+	}
+	ColDesc c;
+	rc = build_page_column(pi, page, value_width, dvals, entries, order, out, &c);
+	if (rc != FLS_OK) { return -3000 + rc; }
 	return emu_decode_column(&c);
 }

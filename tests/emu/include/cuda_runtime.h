@@ -13,6 +13,10 @@
 #define __align__(n) __attribute__((aligned(n)))
 #define __restrict__ __restrict
 
+typedef int           cudaError_t;
+typedef struct CUst_* cudaStream_t;
+#define cudaSuccess 0
+
 struct uint2 {
 	uint32_t x, y;
 };

@@ -107,3 +107,33 @@ def test_emulated_rejects_bit_width_above_type(emu):
     bw[1] = 33
     _, st = run(emu, 32, 1, 0, packed, off, bw, base, None, 3)
     assert st & 2
+
+
+@pytest.mark.parametrize("eid", [0, 1, 6, 7, 11, 16, 17, 22])
+@pytest.mark.parametrize("order", [0, 1])
+def test_emulated_reference_int64_pages(emu, col_golden, eid, order):
+    """Reference-encoded int64 pages through the product's host page walker and the emulated warp decode."""
+    page = np.ascontiguousarray(col_golden[f"i64_{eid}_page"])
+    dic = np.ascontiguousarray(col_golden[f"i64_{eid}_dict"])
+    want = col_golden[f"i64_{eid}_input"].view(np.uint64)
+    n = want.size
+    out = np.zeros(n, np.uint64)
+    st = emu.emu_decode_page(P(page), ctypes.c_uint64(page.size), P(dic) if dic.size else None,
+                             ctypes.c_uint64(dic.size), 64, order, P(out))
+    assert st == 0
+    if order == 1:
+        assert np.array_equal(out, want)
+    else:
+        assert np.array_equal(out, np.concatenate([oracle.transpose_i(want[v * 1024:(v + 1) * 1024].copy())
+                                                   for v in range(n // 1024)]))
+
+
+def test_emulated_rejects_dictionary_code_out_of_range(emu, col_golden):
+    page = np.ascontiguousarray(col_golden["i64_17_page"])
+    dic = np.ascontiguousarray(col_golden["i64_17_dict"]).copy()
+    # shrink the dictionary's entry count below the largest code in use
+    dic[4:8] = np.frombuffer(np.uint32(3).tobytes(), np.uint8)
+    dic[12:20] = np.frombuffer(np.uint64(3 * 8).tobytes(), np.uint8)
+    out = np.zeros(3 * 1024, np.uint64)
+    st = emu.emu_decode_page(P(page), ctypes.c_uint64(page.size), P(dic), ctypes.c_uint64(dic.size), 64, 1, P(out))
+    assert st & 4

@@ -1,0 +1,108 @@
+"""GPU decode of reference pages (bytes written by the reference's own encoder) and the fastlanes.h C API."""
+import numpy as np
+import pytest
+
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+INT_IDS = [0, 1, 6, 7, 11, 16, 17, 22]
+
+
+def _dev_bytes(a, dev, shift=0):
+    import torch
+
+    buf = torch.zeros(a.size + 64, dtype=torch.uint8, device=dev)
+    buf[shift:shift + a.size] = torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    return buf, buf.data_ptr() + shift
+
+
+@pytest.mark.parametrize("eid", INT_IDS)
+@pytest.mark.parametrize("shift", [0, 1, 4, 8])
+def test_reference_int64_pages(cuda, col_golden, eid, shift):
+    import torch
+
+    from fastlanes_b200 import pages
+    from fastlanes_b200 import primitives as P
+
+    page = col_golden[f"i64_{eid}_page"]
+    dic = col_golden[f"i64_{eid}_dict"]
+    want = col_golden[f"i64_{eid}_input"]
+    pbuf, pptr = _dev_bytes(page, cuda, shift)
+    dbuf, dptr = _dev_bytes(dic, cuda, (shift * 3) % 8) if dic.size else (None, None)
+    for order in (1, 0):
+        out = torch.zeros(want.size, dtype=torch.int64, device=cuda)
+        pages.decode_pages([dict(d_page=pptr, page_size=page.size, d_dict=dptr, dict_size=dic.size,
+                                 data_type=pages.INT64, order=order, d_out=out.data_ptr())])
+        got = out.cpu().numpy()
+        if order == 1:
+            assert np.array_equal(got, want), (eid, shift)
+        else:
+            tw = np.concatenate([oracle.transpose_i(want[v * 1024:(v + 1) * 1024].view(np.uint64).copy())
+                                 for v in range(want.size // 1024)]).view(np.int64)
+            assert np.array_equal(got, tw), (eid, shift)
+    assert P.device_status() == 0
+
+
+def test_several_pages_one_launch(cuda, col_golden):
+    import torch
+
+    from fastlanes_b200 import pages
+    from fastlanes_b200 import primitives as P
+
+    keep, cols, wants, outs = [], [], [], []
+    for eid in INT_IDS:
+        page, dic, want = col_golden[f"i64_{eid}_page"], col_golden[f"i64_{eid}_dict"], col_golden[f"i64_{eid}_input"]
+        pbuf, pptr = _dev_bytes(page, cuda, eid % 5)
+        dbuf, dptr = _dev_bytes(dic, cuda) if dic.size else (None, None)
+        out = torch.zeros(want.size, dtype=torch.int64, device=cuda)
+        keep += [pbuf, dbuf]
+        outs.append(out)
+        wants.append(want)
+        cols.append(dict(d_page=pptr, page_size=page.size, d_dict=dptr, dict_size=dic.size, data_type=pages.INT64,
+                         order=1, d_out=out.data_ptr()))
+    pages.decode_pages(cols)
+    for o, w in zip(outs, wants):
+        assert np.array_equal(o.cpu().numpy(), w)
+    assert P.device_status() == 0
+
+
+@pytest.mark.parametrize("eid", [0, 1, 11])
+def test_c_api_encode_matches_reference_bytes_and_decodes(cuda, col_golden, eid):
+    """encode_from_memory of the reference's INT64 input reproduces the reference's page byte for byte;
+    decode_to_memory returns the input."""
+    from fastlanes_b200 import pages
+
+    want = col_golden[f"i64_{eid}_input"]
+    page, mtd = pages.encode_from_memory(want, pages.INT64, eid)
+    assert np.array_equal(page, col_golden[f"i64_{eid}_page"])
+    info = pages.page_info(page)
+    assert mtd == info["meta_size"]
+    assert np.array_equal(pages.decode_to_memory(page, pages.INT64), want)
+    assert np.array_equal(pages.decode_to_memory(col_golden[f"i64_{eid}_page"], pages.INT64), want)
+
+
+@pytest.mark.parametrize("dt", ["UINT32", "INT32", "UINT64"])
+@pytest.mark.parametrize("eid", [0, 1, 11])
+def test_c_api_round_trip_other_widths(cuda, dt, eid):
+    from fastlanes_b200 import pages
+
+    code = getattr(pages, dt)
+    T = pages.DTYPE_OF[code]
+    rng = np.random.default_rng(eid + 7 * code)
+    n = 5 * 1024 + 77  # the tail of n % 1024 values is dropped, as in the reference encoder
+    info = np.iinfo(T)
+    if eid == 11:
+        x = (np.cumsum(rng.integers(0, 50, n)) + int(info.min) // 2).astype(T)
+    else:
+        x = rng.integers(int(info.min), int(info.max), n, dtype=np.int64 if T != np.uint64 else np.uint64).astype(T)
+    page, _ = pages.encode_from_memory(x, code, eid)
+    got = pages.decode_to_memory(page, code)
+    assert np.array_equal(got, x[:5 * 1024])
+
+
+def test_c_api_rejects_unknown_expression(cuda):
+    from fastlanes_b200 import _lib, pages
+
+    with pytest.raises(_lib.FlsError):
+        pages.encode_from_memory(np.arange(2048, dtype=np.int64), pages.INT64, 2)
