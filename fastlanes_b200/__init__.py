@@ -6,6 +6,7 @@ package is the Python face of that ABI.
 from . import _lib  # noqa: F401  (raises if the CUDA library is missing)
 from . import primitives  # noqa: F401
 from . import pages  # noqa: F401
+from . import strings  # noqa: F401
 from . import workloads  # noqa: F401
 
-__all__ = ["pages", "primitives", "workloads"]
+__all__ = ["pages", "primitives", "strings", "workloads"]

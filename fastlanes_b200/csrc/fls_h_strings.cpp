@@ -1,0 +1,253 @@
+// Host side of the string path: page and dictionary metadata, FSST symbol-table import, and the string plan
+// (the reference's TColDecoder<str_pt> ExtInitDict + Decompress loop with the materialisation of
+// include/fls/encoder/assert_eq.hpp:166-210 and :257-400).
+#include "fastlanes.h"
+#include "fls_b200.h"
+#include "fls_page.h"
+#include "fls_runtime.h"
+#include "fls_strplan.h"
+
+#include <cstring>
+#include <cuda_runtime.h>
+#include <memory>
+#include <vector>
+
+namespace flsgpu {
+
+// FSST_MAXHEADER (include/fls/cor/prm/fsst/fsst.h:112-114): the dictionary page reserves this many bytes for
+// the exported symbol table whatever its length (src/cor/lyt/dic/dic.cpp:99-101).
+constexpr uint64_t kFsstMaxHeader = 8 + 1 + 8 + 2048 + 1;
+
+// fsst_import (src/cor/prm/fsst/libfsst.cpp:617-657): 8-byte version word (upper 32 bits 20190218), byte 8 the
+// zero-terminated flag, bytes 9..16 the symbol count per length, then the symbol bytes grouped by length in the
+// order 2,3,4,5,6,7,8,1; codes are numbered from the flag upward; unused codes decode to "corrupt" (8 bytes).
+int fsst_import_table(const uint8_t* buf, uint64_t avail, FsstTable* t, uint64_t* used) {
+	if (avail < 17) { return FLS_ERR_FORMAT; }
+	uint64_t version = 0;
+	std::memcpy(&version, buf, 8);
+	if ((version >> 32) != 20190218ull) { return FLS_ERR_FORMAT; }
+	const uint32_t zt = buf[8] & 1u;
+	uint8_t        hist[8];
+	std::memcpy(hist, buf + 9, 8);
+	std::memset(t, 0, sizeof(*t));
+	t->len[0]     = 1;
+	t->sym[0]     = 0;
+	uint32_t code = zt;
+	uint64_t pos  = 17;
+	if (zt) { hist[0] = static_cast<uint8_t>(hist[0] - 1); }
+	for (uint32_t l = 1; l <= 8; ++l) {
+		for (uint32_t i = 0; i < hist[l & 7]; ++i, ++code) {
+			if (code >= 255) { return FLS_ERR_FORMAT; }
+			t->len[code] = static_cast<uint8_t>((l & 7) + 1);
+			t->sym[code] = 0;
+			for (uint32_t j = 0; j < t->len[code]; ++j) {
+				if (pos >= avail) { return FLS_ERR_FORMAT; }
+				t->sym[code] |= static_cast<uint64_t>(buf[pos++]) << (8 * j);
+			}
+		}
+	}
+	while (code < 255) {
+		t->sym[code] = 32774747032022883ull; // "corrupt"
+		t->len[code] = 8;
+		++code;
+	}
+	if (used) { *used = pos; }
+	return FLS_OK;
+}
+
+namespace {
+
+// Row-stream layouts of the string expressions (roles as in the integer table of fls_h_page.cpp; ib_vals of a
+// DICT_RLE page holds the u32 code runs).  kind: STR_*.
+struct StrLayout {
+	uint8_t exp_t, var, arr_c, ws, enc, post, ib_bw, ib_base, ib_packed, ib_lane, ib_vals, kind;
+};
+const StrLayout* str_layout(uint8_t exp_t, uint8_t var) {
+	static const StrLayout t[] = {
+	    {8, 1, 1, 32, ENC_RAW, POST_NONE, kNoBuf, kNoBuf, 0, kNoBuf, kNoBuf, STR_DICT},   // DICT UNCOMPRESSED
+	    {8, 2, 3, 32, ENC_FFOR, POST_NONE, 0, 1, 2, kNoBuf, kNoBuf, STR_DICT},            // DICT FFOR_NO_PATCH
+	    {8, 7, 4, 32, ENC_DELTA, POST_NONE, 1, 2, 3, 0, kNoBuf, STR_DICT},                // DICT DELTA_NO_PATCH
+	    {11, 1, 2, 16, ENC_RAW, POST_RLE, kNoBuf, kNoBuf, 1, kNoBuf, 0, STR_DICT},        // DICT_RLE UNCOMPRESSED
+	    {11, 2, 5, 16, ENC_DELTA, POST_RLE, 2, 3, 4, 1, 0, STR_DICT},                     // DICT_RLE DELTA_NO_PATCH
+	    {7, 1, 2, 32, ENC_RAW, POST_NONE, kNoBuf, kNoBuf, 1, kNoBuf, kNoBuf, STR_FSST},   // FSST
+	    {7, 2, 5, 32, ENC_DELTA, POST_NONE, 2, 3, 4, 1, kNoBuf, STR_FSST},                // FSST DELTA_NO_PATCH
+	    {3, 1, 2, 32, ENC_RAW, POST_NONE, kNoBuf, kNoBuf, 1, kNoBuf, kNoBuf, STR_BYTES},  // BYTE_ARR
+	};
+	for (const auto& e : t) {
+		if (e.exp_t == exp_t && e.var == var) { return &e; }
+	}
+	return nullptr;
+}
+
+template <class T>
+struct DevArr {
+	T* p = nullptr;
+	~DevArr() {
+		if (p) { cudaFree(p); }
+	}
+	bool alloc(size_t n) { return cudaMalloc(&p, (n ? n : 1) * sizeof(T)) == cudaSuccess; }
+};
+
+} // namespace
+} // namespace flsgpu
+
+using namespace flsgpu;
+
+struct fls_string_plan {
+	StrArgs                  args {};
+	DevArr<FsstTable>        table;
+	DevArr<uint32_t>         dict_ends;
+	DevArr<uint8_t>          dict_bytes;
+	DevArr<uint64_t>         vec_total;
+	DevArr<uint64_t>         vec_base;
+	uint32_t                 dyn_smem = 0;
+	int                      grid     = 0;
+	uint64_t                 n_rows   = 0;
+};
+
+extern "C" {
+
+int fls_string_plan_create(const uint8_t* d_page, uint64_t page_size, const uint8_t* d_dict, uint64_t dict_size,
+                           fls_string_plan** out) {
+	if (!out || !d_page) { return FLS_ERR_ARG; }
+	*out = nullptr;
+	Device* dev = current_device();
+	if (!dev) { return FLS_ERR_CUDA; }
+	uint8_t hdr[8 + 4 * 6];
+	const uint64_t take = page_size < sizeof(hdr) ? page_size : sizeof(hdr);
+	if (take < 8 || cudaMemcpy(hdr, d_page, take, cudaMemcpyDeviceToHost) != cudaSuccess) { return FLS_ERR_FORMAT; }
+	const StrLayout* L = str_layout(hdr[0], hdr[1]);
+	if (!L) { return FLS_ERR_UNSUPPORTED; }
+	PageInfo pi {};
+	pi.exp_t = hdr[0];
+	pi.var   = hdr[1];
+	std::memcpy(&pi.vec_c, hdr + 4, 2);
+	pi.arr_c = L->arr_c;
+	if (take < 8ull + 4 * pi.arr_c) { return FLS_ERR_FORMAT; }
+	for (uint32_t i = 0; i < pi.arr_c; ++i) { std::memcpy(&pi.off[i], hdr + 8 + 4 * i, 4); }
+	pi.ep_off  = 8 + 4 * pi.arr_c;
+	pi.meta_sz = pi.ep_off + 4ull * pi.arr_c * (pi.vec_c ? pi.vec_c - 1 : 0);
+	int rc     = finish_page_info(&pi, page_size);
+	if (rc != FLS_OK) { return rc; }
+	std::unique_ptr<fls_string_plan> p(new fls_string_plan());
+	StrArgs&                         a = p->args;
+	ColDesc&                         c = a.col;
+	c        = ColDesc {};
+	c.ws     = L->ws;
+	c.e      = 4;
+	c.enc    = L->enc;
+	c.post   = L->post;
+	c.order  = 1;
+	c.layout = LAYOUT_PAGE;
+	c.arr_c  = static_cast<uint8_t>(pi.arr_c);
+	c.n_vec  = pi.vec_c;
+	c.ib_bw = L->ib_bw, c.ib_base = L->ib_base, c.ib_packed = L->ib_packed, c.ib_lane_bases = L->ib_lane;
+	c.ib_vals = L->ib_vals;
+	for (uint32_t i = 0; i < pi.arr_c; ++i) {
+		c.buf[i]      = d_page + pi.off[i];
+		c.buf_size[i] = pi.size[i];
+	}
+	c.ep      = reinterpret_cast<const uint32_t*>(d_page + pi.ep_off);
+	a.kind    = L->kind;
+	a.status  = dev->status;
+	p->n_rows = static_cast<uint64_t>(pi.vec_c) * 1024;
+	if (!p->vec_total.alloc(pi.vec_c + 1) || !p->vec_base.alloc(pi.vec_c + 1)) { return FLS_ERR_CUDA; }
+	a.vec_total = p->vec_total.p;
+	a.vec_base  = p->vec_base.p;
+	if (!p->table.alloc(1)) { return FLS_ERR_CUDA; }
+	FsstTable tab {};
+	if (L->kind != STR_BYTES) {
+		// DICT: dict_hdr | FSST table slot | entry_c u32 lengths | bytes.  FSST column: dict_hdr | exported table.
+		if (!d_dict || dict_size < 8 + 17) { return FLS_ERR_FORMAT; }
+		const uint64_t head = L->kind == STR_DICT ? 8 + kFsstMaxHeader : dict_size;
+		if (head > dict_size) { return FLS_ERR_FORMAT; }
+		std::vector<uint8_t> h(head);
+		if (cudaMemcpy(h.data(), d_dict, head, cudaMemcpyDeviceToHost) != cudaSuccess) { return FLS_ERR_CUDA; }
+		rc = fsst_import_table(h.data() + 8, head - 8, &tab, nullptr);
+		if (rc != FLS_OK) { return rc; }
+		if (L->kind == STR_DICT) {
+			uint32_t entry_c = 0;
+			std::memcpy(&entry_c, h.data() + 4, 4);
+			const uint64_t lens_off = 8 + kFsstMaxHeader;
+			const uint64_t comp_off = lens_off + 4ull * entry_c;
+			if (entry_c == 0 || comp_off > dict_size) { return FLS_ERR_FORMAT; }
+			const uint64_t comp_size = dict_size - comp_off;
+			const uint64_t cap       = comp_size * 8 + 16;
+			if (!p->dict_ends.alloc(entry_c) || !p->dict_bytes.alloc(cap)) { return FLS_ERR_CUDA; }
+			cudaMemcpy(p->table.p, &tab, sizeof(tab), cudaMemcpyHostToDevice);
+			if (launch_fsst_dict(d_dict + lens_off, d_dict + comp_off, comp_size, entry_c, p->table.p,
+			                     p->dict_ends.p, p->dict_bytes.p, cap, dev->status, nullptr) != cudaSuccess) {
+				return FLS_ERR_CUDA;
+			}
+			uint32_t last = 0;
+			if (cudaMemcpy(&last, p->dict_ends.p + entry_c - 1, 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+				return FLS_ERR_CUDA;
+			}
+			a.entry_c      = entry_c;
+			a.dict_ends    = p->dict_ends.p;
+			a.dict_bytes   = p->dict_bytes.p;
+			a.dict_bytes_n = last;
+		}
+	}
+	if (cudaMemcpy(p->table.p, &tab, sizeof(tab), cudaMemcpyHostToDevice) != cudaSuccess) { return FLS_ERR_CUDA; }
+	a.table = p->table.p;
+	// shared-memory budget of the materialising kernel: per-warp areas + (dictionary bytes and ends if they fit)
+	const uint32_t base     = str_smem_base();
+	const uint64_t dict_sm  = ((a.dict_bytes_n + 15) & ~15ull) + 4ull * a.entry_c;
+	const uint64_t budget   = 220 * 1024;
+	a.dict_in_smem          = a.kind == STR_DICT && base + dict_sm <= budget;
+	p->dyn_smem             = base + (a.dict_in_smem ? static_cast<uint32_t>(dict_sm) : 0u);
+	p->grid                 = dev->sm_count;
+	*out                    = p.release();
+	return FLS_OK;
+}
+
+int fls_string_plan_rows(const fls_string_plan* p, uint64_t* n_rows) {
+	if (!p || !n_rows) { return FLS_ERR_ARG; }
+	*n_rows = p->n_rows;
+	return FLS_OK;
+}
+
+static int run_totals(const fls_string_plan* p, cudaStream_t s) {
+	if (p->args.col.n_vec == 0) { return FLS_OK; }
+	if (launch_str_lengths(p->args, p->grid, s) != cudaSuccess) { return FLS_ERR_CUDA; }
+	if (launch_scan_totals(p->vec_total.p, p->vec_base.p, p->args.col.n_vec, s) != cudaSuccess) { return FLS_ERR_CUDA; }
+	return FLS_OK;
+}
+
+int fls_string_plan_measure(fls_string_plan* p, uint64_t* n_bytes, fls_stream_t stream) {
+	if (!p || !n_bytes) { return FLS_ERR_ARG; }
+	cudaStream_t s  = static_cast<cudaStream_t>(stream);
+	const int    rc = run_totals(p, s);
+	if (rc != FLS_OK) { return rc; }
+	*n_bytes = 0;
+	if (p->args.col.n_vec == 0) { return FLS_OK; }
+	if (cudaMemcpyAsync(n_bytes, p->vec_base.p + p->args.col.n_vec, 8, cudaMemcpyDeviceToHost, s) != cudaSuccess) {
+		return FLS_ERR_CUDA;
+	}
+	return cudaStreamSynchronize(s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
+}
+
+int fls_string_plan_decode(const fls_string_plan* p, uint32_t* d_offsets, uint8_t* d_bytes, uint64_t bytes_cap,
+                           fls_stream_t stream) {
+	if (!p || !d_offsets || (!d_bytes && bytes_cap)) { return FLS_ERR_ARG; }
+	if ((reinterpret_cast<uintptr_t>(d_bytes) & 15u) != 0 || bytes_cap >= (1ull << 32)) { return FLS_ERR_ARG; }
+	cudaStream_t s  = static_cast<cudaStream_t>(stream);
+	int          rc = run_totals(p, s);
+	if (rc != FLS_OK) { return rc; }
+	if (p->args.col.n_vec == 0) {
+		return cudaMemsetAsync(d_offsets, 0, 4, s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
+	}
+	StrArgs a   = p->args;
+	a.offsets   = d_offsets;
+	a.bytes     = d_bytes;
+	a.bytes_cap = bytes_cap;
+	return launch_str_materialize(a, p->grid, p->dyn_smem, s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
+}
+
+int fls_string_plan_destroy(fls_string_plan* p) {
+	delete p;
+	return FLS_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,75 @@
+// String decoding on the B200: FSST symbol tables, dictionary pages and string columns.
+//
+// Reference semantics (cwida/FastLanes):
+//   * FSST decode (include/fls/cor/prm/fsst/fsst.h:152-259): code < 255 emits its symbol (len[code] bytes,
+//     little-endian in a 64-bit word), 255 escapes the next byte.
+//   * string dictionary page (src/cor/lyt/dic/dic.cpp:88-111, src/cor/eng/hzl_de_cmp.cpp:85-117):
+//     dict_hdr_t (8 B) | FSST table (FSST_MAXHEADER = 2066 B slot) | entry_c x u32 compressed lengths |
+//     compressed bytes; entry i decodes from the bytes after entries 0..i-1; UNFSST keeps cumulative END
+//     offsets of the decoded entries.
+//   * DICT / DICT_RLE rows (include/fls/encoder/assert_eq.hpp:257-400): row i is dictionary entry code[i],
+//     codes untransposed (and RLE-expanded for DICT_RLE).
+//   * FSST column (include/fls/encoder/assert_eq.hpp:166-210, src/cor/lyt/vec.cpp:162-207): per vector the
+//     compressed bytes and 1024 cumulative end offsets (transposed); row i decodes bytes [end[i-1], end[i]).
+// Output is Arrow-style: n_rows + 1 u32 offsets and the concatenated bytes.
+#pragma once
+
+#include "fls_device.cuh"
+#include "fls_plan.h"
+#include "fls_strplan.h"
+
+namespace flsgpu {
+
+// Decoded length of one FSST-compressed string.
+__device__ __forceinline__ uint32_t fsst_decoded_len(const uint8_t* len, const uint8_t* in, uint32_t n) {
+	uint32_t out = 0;
+	for (uint32_t i = 0; i < n; ++i) {
+		const uint8_t c = in[i];
+		if (c == 255) {
+			out += 1;
+			++i;
+		} else {
+			out += len[c];
+		}
+	}
+	return out;
+}
+
+// Decode one FSST-compressed string to out (exactly the decoded length is written).
+__device__ __forceinline__ void fsst_decode_to(const uint64_t* sym, const uint8_t* len, const uint8_t* in, uint32_t n,
+                                               uint8_t* out) {
+	uint32_t o = 0;
+	for (uint32_t i = 0; i < n; ++i) {
+		const uint8_t c = in[i];
+		if (c == 255) {
+			if (i + 1 < n) { out[o] = in[i + 1]; }
+			o += 1;
+			++i;
+		} else {
+			const uint64_t s = sym[c];
+			const uint32_t l = len[c];
+			for (uint32_t b = 0; b < l; ++b) { out[o + b] = static_cast<uint8_t>(s >> (8 * b)); }
+			o += l;
+		}
+	}
+}
+
+// Inclusive warp scan (Kogge-Stone over shuffles).
+template <class T>
+__device__ __forceinline__ T warp_inclusive_scan(T x, uint32_t lane) {
+#pragma unroll
+	for (int d = 1; d < 32; d <<= 1) {
+		const T y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+		if (lane >= static_cast<uint32_t>(d)) { x += y; }
+	}
+	return x;
+}
+
+template <class T>
+__device__ __forceinline__ T warp_sum(T x) {
+#pragma unroll
+	for (int d = 16; d > 0; d >>= 1) { x += __shfl_xor_sync(0xFFFFFFFFu, x, d); }
+	return x;
+}
+
+} // namespace flsgpu

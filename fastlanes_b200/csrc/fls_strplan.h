@@ -1,0 +1,47 @@
+// Arguments of the string kernels (shared by the host string plan and fls_k_strings.cu).
+#pragma once
+
+#include "fls_plan.h"
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace flsgpu {
+
+// FSST symbol table as the decoder uses it: symbol c (little-endian) and its length.
+struct FsstTable {
+	uint64_t sym[256];
+	uint8_t  len[256];
+};
+
+enum : uint8_t {
+	STR_DICT  = 0, // rows are dictionary codes (DICT / DICT_RLE pages), dictionary FSST-decoded once per plan
+	STR_FSST  = 1, // rows are FSST-compressed in the page (FSST pages)
+	STR_BYTES = 2, // rows are plain bytes in the page (BYTE_ARR pages)
+};
+
+struct StrArgs {
+	ColDesc          col; // the row stream: codes or cumulative end offsets, page layout
+	uint8_t          kind;
+	bool             dict_in_smem;
+	uint32_t         entry_c;
+	const uint32_t*  dict_ends;
+	const uint8_t*   dict_bytes;
+	uint64_t         dict_bytes_n;
+	const FsstTable* table;
+	uint64_t*        vec_total;
+	const uint64_t*  vec_base;
+	uint32_t*        offsets;
+	uint8_t*         bytes;
+	uint64_t         bytes_cap;
+	int*             status;
+};
+
+cudaError_t launch_fsst_dict(const uint8_t* lens, const uint8_t* comp, uint64_t comp_size, uint32_t entry_c,
+                             const FsstTable* tab, uint32_t* ends, uint8_t* bytes, uint64_t cap, int* status,
+                             cudaStream_t s);
+cudaError_t launch_str_lengths(const StrArgs& a, int grid, cudaStream_t s);
+cudaError_t launch_scan_totals(const uint64_t* total, uint64_t* base, uint64_t n, cudaStream_t s);
+cudaError_t launch_str_materialize(const StrArgs& a, int grid, uint32_t dyn_smem, cudaStream_t s);
+uint32_t    str_smem_base();
+
+} // namespace flsgpu

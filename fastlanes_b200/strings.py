@@ -1,0 +1,56 @@
+"""String columns (DICT / DICT_RLE with FSST dictionaries, FSST, BYTE_ARR pages) decoded on the GPU into
+Arrow-style offsets + bytes (fls_string_plan_* of include/fls_b200.h)."""
+import ctypes
+
+import torch
+
+from ._lib import check, declare
+
+_p = ctypes.c_void_p
+_u64 = ctypes.c_uint64
+
+_create = declare("fls_string_plan_create", ctypes.c_int, [_p, _u64, _p, _u64, ctypes.POINTER(_p)])
+_rows = declare("fls_string_plan_rows", ctypes.c_int, [_p, ctypes.POINTER(_u64)])
+_measure = declare("fls_string_plan_measure", ctypes.c_int, [_p, ctypes.POINTER(_u64), _p])
+_decode = declare("fls_string_plan_decode", ctypes.c_int, [_p, _p, _p, _u64, _p])
+_destroy = declare("fls_string_plan_destroy", ctypes.c_int, [_p])
+
+
+class StringPlan:
+    """Decoder of one string page; the page / dictionary device buffers must outlive it."""
+
+    def __init__(self, d_page, page_size, d_dict=None, dict_size=0):
+        h = _p()
+        check(_create(d_page, page_size, d_dict, dict_size, ctypes.byref(h)), "fls_string_plan_create")
+        self.handle = h
+        n = _u64()
+        check(_rows(h, ctypes.byref(n)), "rows")
+        self.n_rows = n.value
+
+    def measure(self, stream=None):
+        n = _u64()
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        check(_measure(self.handle, ctypes.byref(n), s), "measure")
+        return n.value
+
+    def decode_into(self, offsets, data, stream=None):
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        check(_decode(self.handle, offsets.data_ptr(), data.data_ptr(), data.numel(), s), "decode")
+
+    def decode(self, device="cuda"):
+        n_bytes = self.measure()
+        offsets = torch.empty(self.n_rows + 1, dtype=torch.int32, device=device)
+        data = torch.empty(max(n_bytes, 16), dtype=torch.uint8, device=device)
+        self.decode_into(offsets, data)
+        return offsets, data[:n_bytes]
+
+    def close(self):
+        if self.handle:
+            _destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

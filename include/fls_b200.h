@@ -203,6 +203,25 @@ int fls_page_info(const uint8_t* page_prefix, uint64_t prefix_size, uint32_t* ex
 int fls_page_placement(const uint8_t* page_prefix, uint64_t prefix_size, uint32_t* shift);
 int fls_gpu_decode_pages(const fls_page_column* cols, uint32_t n_cols, fls_stream_t stream);
 
+/* ---------------------------------------------------------------------------------------------------------
+ * String columns.  d_page: a string page (DICT: str expressions 2, 3, 8; DICT_RLE: 15, 16; FSST: 13, 14;
+ * BYTE_ARR: 0 of src/cor/exp_pool.cpp:66-101); d_dict: its dictionary bytes (DICT / DICT_RLE: the FSST-
+ * compressed dictionary page; FSST: the exported symbol table; BYTE_ARR: none).  Creating a plan decodes the
+ * dictionary once on the GPU (TColDecoder::ExtInitDict, src/encoder/col_encoder.cpp:198-201); decoding emits
+ * Arrow-style output: n_rows + 1 u32 offsets and the concatenated bytes, rows in original order
+ * (include/fls/encoder/assert_eq.hpp:166-210, :257-400).  The page and dictionary buffers must outlive the plan.
+ * ------------------------------------------------------------------------------------------------------- */
+typedef struct fls_string_plan fls_string_plan;
+int fls_string_plan_create(const uint8_t* d_page, uint64_t page_size, const uint8_t* d_dict, uint64_t dict_size,
+                           fls_string_plan** out_plan);
+int fls_string_plan_rows(const fls_string_plan* plan, uint64_t* n_rows);
+/* Total decoded bytes (runs the length pass; synchronises the stream). */
+int fls_string_plan_measure(fls_string_plan* plan, uint64_t* n_bytes, fls_stream_t stream);
+/* d_offsets: n_rows + 1 entries; d_bytes: 16-byte aligned, bytes_cap < 4 GiB.  Asynchronous, no allocation. */
+int fls_string_plan_decode(const fls_string_plan* plan, uint32_t* d_offsets, uint8_t* d_bytes, uint64_t bytes_cap,
+                           fls_stream_t stream);
+int fls_string_plan_destroy(fls_string_plan* plan);
+
 #ifdef __cplusplus
 }
 #endif
