@@ -12,6 +12,10 @@
 #include "fls_strings.cuh"
 #include "fls_runtime.h"
 #include "fls_strplan.h"
+#include "fls_b200.h"
+
+#include <cstring>
+#include <mutex>
 
 namespace flsgpu {
 
@@ -381,3 +385,139 @@ cudaError_t launch_str_materialize(const StrArgs& a, int grid, uint32_t dyn_smem
 }
 
 } // namespace flsgpu
+
+// =========================================================================================================
+// Allocation-free decode of FSST / BYTE_ARR string pages (fls_gpu_decode_fsst_page_noalloc).
+//
+// The string plan keeps its scratch (per-vector byte totals and first-byte bases, the FSST table, a status
+// word) in cudaMalloc'd buffers.  This variant keeps the same scratch in one array compiled into the library,
+// so the call allocates nothing; in exchange the page may hold at most kNoAllocMaxVectors vectors.
+// =========================================================================================================
+namespace flsgpu {
+
+constexpr uint32_t kNoAllocMaxVectors = 8192; // 8,388,608 rows per call
+
+struct NoAllocLayout {
+	static constexpr size_t kStatus = 0;                                      // int, OR-ed device status
+	static constexpr size_t kTable  = 256;                                    // FsstTable (2304 B)
+	static constexpr size_t kTotal  = kTable + ((sizeof(FsstTable) + 255) & ~size_t(255));
+	static constexpr size_t kBase   = kTotal + 8 * (kNoAllocMaxVectors + 1);
+	static constexpr size_t kBytes  = kBase + 8 * (kNoAllocMaxVectors + 1);   // 133,376 B in all
+};
+
+// Every GPU that loads the library holds this array until the process exits.
+static __device__ __align__(256) uint8_t g_noalloc_scratch[NoAllocLayout::kBytes];
+
+// Device address of g_noalloc_scratch on the current device, looked up once per device on the first call.
+static uint8_t* noalloc_scratch() {
+	static uint8_t*   addr[64] = {};
+	static std::mutex mu;
+	int               dev      = 0;
+	if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) { return nullptr; }
+	std::lock_guard<std::mutex> lk(mu);
+	if (!addr[dev]) {
+		void* p = nullptr;
+		if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr) { return nullptr; }
+		addr[dev] = static_cast<uint8_t*>(p);
+	}
+	return addr[dev];
+}
+
+int fsst_import_table(const uint8_t* buf, uint64_t avail, FsstTable* t, uint64_t* used);
+
+} // namespace flsgpu
+
+extern "C" int fls_gpu_decode_fsst_page_noalloc(const uint8_t* d_page, uint64_t page_size, const uint8_t* d_dict,
+                                                uint64_t dict_size, uint32_t* d_offsets, uint8_t* d_bytes,
+                                                uint64_t bytes_cap, int* d_status, void* stream) {
+	using namespace flsgpu;
+	if (!d_page || !d_offsets || (!d_bytes && bytes_cap) || (reinterpret_cast<uintptr_t>(d_bytes) & 15u) != 0 ||
+	    bytes_cap >= (1ull << 32)) {
+		return FLS_ERR_ARG;
+	}
+	cudaStream_t s = static_cast<cudaStream_t>(stream);
+	uint8_t      hdr[8 + 4 * 5];
+	const uint64_t take = page_size < sizeof(hdr) ? page_size : sizeof(hdr);
+	if (take < 8 || cudaMemcpy(hdr, d_page, take, cudaMemcpyDeviceToHost) != cudaSuccess) { return FLS_ERR_FORMAT; }
+	uint8_t kind = 0, arr_c = 0, ws = 32, enc = ENC_RAW, ib_packed = 1, ib_bw = kNoBuf, ib_base = kNoBuf,
+	        ib_lane = kNoBuf;
+	if (hdr[0] == 7 && hdr[1] == 1) {
+		kind = STR_FSST, arr_c = 2; // FSST: bytes, end offsets
+	} else if (hdr[0] == 7 && hdr[1] == 2) {
+		kind = STR_FSST, arr_c = 5, enc = ENC_DELTA, ib_packed = 4, ib_bw = 2, ib_base = 3, ib_lane = 1;
+	} else if (hdr[0] == 3 && hdr[1] == 1) {
+		kind = STR_BYTES, arr_c = 2; // BYTE_ARR: bytes, end offsets
+	} else {
+		return FLS_ERR_UNSUPPORTED;
+	}
+	uint16_t vec_c = 0;
+	std::memcpy(&vec_c, hdr + 4, 2);
+	if (vec_c > kNoAllocMaxVectors) { return FLS_ERR_TOO_LARGE; }
+	if (take < 8ull + 4 * arr_c) { return FLS_ERR_FORMAT; }
+	uint32_t off[5];
+	for (uint32_t i = 0; i < arr_c; ++i) { std::memcpy(&off[i], hdr + 8 + 4 * i, 4); }
+	const uint64_t meta = 8 + 4ull * arr_c + 4ull * arr_c * (vec_c ? vec_c - 1 : 0);
+	ColDesc        c {};
+	for (uint32_t i = 0; i < arr_c; ++i) {
+		const uint64_t end = (i + 1 < arr_c) ? off[i + 1] : page_size;
+		if (off[i] < meta || off[i] > end || end > page_size) { return FLS_ERR_FORMAT; }
+		c.buf[i]      = d_page + off[i];
+		c.buf_size[i] = end - off[i];
+	}
+	uint8_t* scratch = noalloc_scratch();
+	if (!scratch) { return FLS_ERR_CUDA; }
+	FsstTable tab {};
+	if (kind == STR_FSST) {
+		// dict_hdr_t followed by the exported symbol table (at most FSST_MAXHEADER = 2066 bytes)
+		uint8_t        h[8 + 2066];
+		const uint64_t n = dict_size < sizeof(h) ? dict_size : sizeof(h);
+		if (!d_dict || n < 8 + 17 || cudaMemcpy(h, d_dict, n, cudaMemcpyDeviceToHost) != cudaSuccess) {
+			return FLS_ERR_FORMAT;
+		}
+		const int rc = fsst_import_table(h + 8, n - 8, &tab, nullptr);
+		if (rc != FLS_OK) { return rc; }
+	}
+	// the table and a zero status are the only scratch contents a call relies on; totals and bases are
+	// rewritten in full by every call
+	if (cudaMemcpyAsync(scratch + NoAllocLayout::kTable, &tab, sizeof(tab), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+	    cudaMemsetAsync(scratch + NoAllocLayout::kStatus, 0, sizeof(int), s) != cudaSuccess) {
+		return FLS_ERR_CUDA;
+	}
+	c.ws            = ws;
+	c.e             = 4;
+	c.enc           = enc;
+	c.post          = POST_NONE;
+	c.order         = 1;
+	c.layout        = LAYOUT_PAGE;
+	c.arr_c         = arr_c;
+	c.n_vec         = vec_c;
+	c.ib_bw         = ib_bw;
+	c.ib_base       = ib_base;
+	c.ib_packed     = ib_packed;
+	c.ib_lane_bases = ib_lane;
+	c.ib_vals       = kNoBuf;
+	c.ep            = reinterpret_cast<const uint32_t*>(d_page + 8 + 4 * arr_c);
+	if (vec_c == 0) { return cudaMemsetAsync(d_offsets, 0, 4, s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA; }
+	StrArgs a {};
+	a.col       = c;
+	a.kind      = kind;
+	a.table     = reinterpret_cast<const FsstTable*>(scratch + NoAllocLayout::kTable);
+	a.vec_total = reinterpret_cast<uint64_t*>(scratch + NoAllocLayout::kTotal);
+	a.vec_base  = reinterpret_cast<const uint64_t*>(scratch + NoAllocLayout::kBase);
+	a.offsets   = d_offsets;
+	a.bytes     = d_bytes;
+	a.bytes_cap = bytes_cap;
+	a.status    = d_status ? d_status : reinterpret_cast<int*>(scratch + NoAllocLayout::kStatus);
+	int sms = 0, dev = 0;
+	if (cudaGetDevice(&dev) != cudaSuccess ||
+	    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) {
+		return FLS_ERR_CUDA;
+	}
+	if (launch_str_lengths(a, sms, s) != cudaSuccess ||
+	    launch_scan_totals(a.vec_total, reinterpret_cast<uint64_t*>(scratch + NoAllocLayout::kBase), vec_c, s) !=
+	        cudaSuccess ||
+	    launch_str_materialize(a, sms, str_smem_base(), s) != cudaSuccess) {
+		return FLS_ERR_CUDA;
+	}
+	return FLS_OK;
+}

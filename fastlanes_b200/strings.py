@@ -14,6 +14,15 @@ _rows = declare("fls_string_plan_rows", ctypes.c_int, [_p, ctypes.POINTER(_u64)]
 _measure = declare("fls_string_plan_measure", ctypes.c_int, [_p, ctypes.POINTER(_u64), _p])
 _decode = declare("fls_string_plan_decode", ctypes.c_int, [_p, _p, _p, _u64, _p])
 _destroy = declare("fls_string_plan_destroy", ctypes.c_int, [_p])
+_noalloc = declare("fls_gpu_decode_fsst_page_noalloc", ctypes.c_int, [_p, _u64, _p, _u64, _p, _p, _u64, _p, _p])
+
+
+def decode_fsst_page_noalloc(d_page, page_size, d_dict, dict_size, offsets, data, status=None, stream=None):
+    """Allocation-free decode of an FSST / BYTE_ARR page into caller-owned offsets (int32, n_rows + 1) and data
+    (uint8) tensors; returns the status code (0 = ok, -6 = page beyond the fixed scratch)."""
+    s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    return _noalloc(d_page, page_size, d_dict, dict_size, offsets.data_ptr(), data.data_ptr(), data.numel(),
+                    status.data_ptr() if status is not None else None, s)
 
 
 class StringPlan:

@@ -31,6 +31,7 @@ enum fls_status_code {
 	FLS_ERR_FORMAT      = -3, /* malformed page / dictionary bytes */
 	FLS_ERR_UNSUPPORTED = -4, /* expression or type outside the decode path */
 	FLS_ERR_BW          = -5, /* bit width above the type width */
+	FLS_ERR_TOO_LARGE   = -6, /* input beyond the fixed scratch of an allocation-free entry point */
 };
 
 enum fls_order_code { FLS_TRANSPOSED = 0, FLS_ORIGINAL = 1 };
@@ -221,6 +222,25 @@ int fls_string_plan_measure(fls_string_plan* plan, uint64_t* n_bytes, fls_stream
 int fls_string_plan_decode(const fls_string_plan* plan, uint32_t* d_offsets, uint8_t* d_bytes, uint64_t bytes_cap,
                            fls_stream_t stream);
 int fls_string_plan_destroy(fls_string_plan* plan);
+
+/* Allocation-free decode of an FSST (str expressions 13, 14) or BYTE_ARR (0) page.  No counterpart in the
+ * reference.  Some callers cannot allocate device memory: an engine whose buffer manager owns all of HBM and
+ * forbids plugins to call cudaMalloc, or a caller on a path where allocating is not allowed.  This call needs no
+ * allocation: its scratch (per-vector byte totals and bases, the FSST table, a status word) is one fixed array
+ * of 133,376 bytes compiled into the library, which every GPU that loads the library holds until the process
+ * exits.  Limits and rules:
+ *   - at most 8192 vectors (8,388,608 rows) per page; larger pages return FLS_ERR_TOO_LARGE before any work;
+ *   - the first call on a device looks up the array's device address (cudaGetSymbolAddress); make that first
+ *     call before any stream capture;
+ *   - all calls share the array, so calls whose work overlaps on the GPU (other streams, other threads) race;
+ *     serialise them;
+ *   - device-detected errors are OR-ed into *d_status when it is given (the caller zeroes it), else into the
+ *     array's own status word, which every call clears.
+ * Inputs and outputs are as for fls_string_plan_decode: d_offsets n_rows + 1 u32, d_bytes 16-byte aligned with
+ * room for the decoded bytes (bytes_cap < 4 GiB); d_dict holds the FSST table bytes for FSST pages. */
+int fls_gpu_decode_fsst_page_noalloc(const uint8_t* d_page, uint64_t page_size, const uint8_t* d_dict,
+                                     uint64_t dict_size, uint32_t* d_offsets, uint8_t* d_bytes, uint64_t bytes_cap,
+                                     int* d_status, fls_stream_t stream);
 
 #ifdef __cplusplus
 }
