@@ -36,6 +36,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
+    ap.add_argument("--skip-legs", action="store_true", help="leave out the other configurations' legs")
     return ap.parse_args()
 
 
@@ -247,6 +248,102 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def device_timed(fn, steps, warm):
+    """Mean device time of fn() in ms: CUDA events on the current stream, synchronised on both sides."""
+    import torch
+
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s = torch.cuda.current_stream()
+    e0.record(s)
+    for _ in range(steps):
+        fn()
+    e1.record(s)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def other_configs(dev, args):
+    """Decode legs of the other benchmark configurations (each bit-exact checked before it is timed)."""
+    import torch
+
+    from fastlanes_b200 import _lib as L
+    from fastlanes_b200 import pages as PG
+    from fastlanes_b200 import primitives as P
+    from fastlanes_b200 import strings as S
+    from fastlanes_b200 import workloads as W
+
+    peak, _ = measured_peak()
+    steps = max(10, min(args.steps // 10, 200))
+    out = {}
+
+    def leg(name, workload, ms, read_b, write_b, n_vals, parity, launches):
+        out[name] = {"workload": workload, "value": round(write_b / (ms * 1e-3) / 1e9, 2), "unit": "GB/s",
+                     "ms_per_step": round(ms, 4), "decoded_values_per_s": round(n_vals / (ms * 1e-3), 1),
+                     "bytes_per_step": read_b + write_b,
+                     "roofline_frac": round((read_b + write_b) / (ms * 1e-3) / 1e9 / peak, 4),
+                     "parity": bool(parity), "gpu_launches_per_step": launches}
+
+    # 1: plain FFOR u32, 1024 vectors at bw 7 (launch-bound on a GPU; the CPU-runnable parity case)
+    base, vals = W.ffor_u32_bw7()
+    tv = P.transpose_i(torch.from_numpy(vals.reshape(-1)).to(dev))
+    bw = torch.full((1024,), 7, dtype=torch.uint8, device=dev)
+    bs = torch.from_numpy(base).to(dev)
+    packed, off = P.ffor(tv, bw, bs)
+    res = P.unffor(packed, bw, bs, off, P.TRANSPOSED)
+    ok = torch.equal(res.view(torch.int32), tv.view(torch.int32))
+    ms = device_timed(lambda: P.unffor(packed, bw, bs, off, P.TRANSPOSED), steps, 3)
+    leg("1_ffor_u32_bw7", "1024 u32 vectors, base~U[0,2^20), bw 7, unpack+unffor (transposed)", ms,
+        1024 * (7 * 128 + 4 + 1 + 8), 1024 * 4096, 1024 * 1024, ok, 1)
+
+    def page_leg(name, workload, values, dtype, expr):
+        page, _ = PG.encode_from_memory(values, dtype, expr)
+        shift = PG.placement(page)
+        buf = torch.zeros(page.size + 64, dtype=torch.uint8, device=dev)
+        buf[shift:shift + page.size] = torch.from_numpy(page).to(dev)
+        o = torch.empty(values.size, dtype=torch.from_numpy(values[:1]).dtype, device=dev)
+        col = [dict(d_page=buf.data_ptr() + shift, page_size=page.size, data_type=dtype, order=1,
+                    d_out=o.data_ptr())]
+        PG.decode_pages(col)
+        ok = np.array_equal(o.cpu().numpy(), values)
+        ms = device_timed(lambda: PG.decode_pages(col), steps, 3)
+        leg(name, workload, ms, page.size, values.nbytes, values.size, ok, 1)
+
+    page_leg("3a_delta_i64", "32Mi sorted int64 timestamps from 1.6e18, geometric(mean 10) gaps, DELTA (id 11)",
+             W.delta_timestamps(), PG.INT64, 11)
+    page_leg("3b_rle_i32", "32Mi int32 run values~U[0,1e6), geometric(mean 8) runs, RLE DELTA_NO_PATCH (id 6)",
+             W.rle_int32(), PG.INT32, 6)
+
+    # 4: DICT + FSST strings, 16Mi rows
+    dbytes, doffs = W.string_dictionary()
+    codes = W.zipf_codes()
+    page, dic = S.encode_string_dict(dbytes, doffs, codes)
+    pb = torch.from_numpy(page).to(dev)
+    db = torch.from_numpy(dic).to(dev)
+    plan = S.StringPlan(pb.data_ptr(), page.size, db.data_ptr(), dic.size)
+    n_bytes = plan.measure()
+    offs_t = torch.empty(plan.n_rows + 1, dtype=torch.int32, device=dev)
+    data_t = torch.empty(n_bytes + 16, dtype=torch.uint8, device=dev)
+    plan.decode_into(offs_t, data_t)
+    lens = np.diff(doffs).astype(np.int64)
+    want_off = np.zeros(codes.size + 1, np.int64)
+    want_off[1:] = np.cumsum(lens[codes])
+    got_off = offs_t.cpu().numpy().astype(np.int64)
+    ok = np.array_equal(got_off, want_off)
+    rng = np.random.default_rng(7)
+    data_h = data_t[:n_bytes].cpu().numpy()
+    for r in rng.integers(0, codes.size, 2000):
+        c = codes[r]
+        ok = ok and np.array_equal(data_h[want_off[r]:want_off[r + 1]], dbytes[int(doffs[c]):int(doffs[c + 1])])
+    ms = device_timed(lambda: plan.decode_into(offs_t, data_t), steps, 3)
+    leg("4_dict_fsst_str", "16Mi rows, 4096-entry FSST dictionary (5-40 B strings), Zipf(1.1) codes at 12 bits",
+        ms, page.size + dic.size, 4 * (codes.size + 1) + n_bytes, codes.size, ok, 3)
+    plan.close()
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -268,6 +365,7 @@ def run_ours(args):
         if not torch.equal(o.view(torch.int64 if c.width == 64 else torch.int32),
                            c.values.view(torch.int64 if c.width == 64 else torch.int32)):
             raise SystemExit("decode mismatch in benchmark self-check")
+        c.values_host = c.values.cpu().numpy()
         c.values = None
     if P.device_status() != 0:
         raise SystemExit("device status error")
@@ -305,41 +403,51 @@ def run_ours(args):
         ms_k, _ = timed(plan_k, max(args.steps // 4, 3), 3)
     clocks = clk.summary()
 
-    # end to end through the public API: host (pinned) -> device copy of the compressed inputs, one decode,
-    # device -> host copy of the decoded values, every step
-    h_in = [(c.packed.cpu().pin_memory(), c.byte_off.cpu().pin_memory(), c.bw.cpu().pin_memory(),
-             c.base.cpu().pin_memory()) for c in cols]
-    h_out = [torch.empty(o.numel(), dtype=o.dtype, pin_memory=True) for o in outs]
-    h2d = sum(sum(t.numel() * t.element_size() for t in hi) for hi in h_in) + queue.numel() * 4
-    h_q = queue.cpu().pin_memory()
-    d2h = sum(o.numel() * o.element_size() for o in outs)
+    # end to end through the reference-facing C API: fastlanes.h decode_to_memory on pages held in pinned host
+    # memory, decoded values written to pinned host memory; the call copies host -> device, decodes and copies
+    # device -> host every step (it is synchronous, so it is timed on the host)
+    import ctypes
+
+    from fastlanes_b200 import _lib as L
+    from fastlanes_b200 import pages as PG
+
+    e2e_pages = []
+    for c in cols:
+        vals = c.values_host
+        per = 32768 if c.width == 32 else c.n_vec  # a page holds at most 65535 vectors
+        for v0 in range(0, c.n_vec, per):
+            chunk = vals[v0 * 1024:(v0 + per) * 1024]
+            page, _ = PG.encode_from_memory(chunk, PG.UINT32 if c.width == 32 else PG.UINT64, 1)
+            hp = torch.empty(page.size, dtype=torch.uint8, pin_memory=True)
+            hp.numpy()[:] = page
+            ho = torch.empty(chunk.size, dtype=workloads._DT[c.width], pin_memory=True)
+            e2e_pages.append((hp, ho, PG.UINT32 if c.width == 32 else PG.UINT64, chunk))
+        c.values_host = None
+    h2d = sum(hp.numel() for hp, _, _, _ in e2e_pages)
+    d2h = sum(ho.numel() * ho.element_size() for _, ho, _, _ in e2e_pages)
 
     def e2e_step():
-        for (hp, ho, hb, hs), c in zip(h_in, cols):
-            c.packed.copy_(hp, non_blocking=True)
-            c.byte_off.copy_(ho, non_blocking=True)
-            c.bw.copy_(hb, non_blocking=True)
-            c.base.copy_(hs, non_blocking=True)
-        queue.copy_(h_q, non_blocking=True)
-        plan_o.decode()
-        for o, ho in zip(outs, h_out):
-            ho.copy_(o, non_blocking=True)
+        for hp, ho, dt, _ in e2e_pages:
+            L.lib.decode_to_memory(hp.data_ptr(), ho.data_ptr(), dt)
 
-    for _ in range(2):
-        e2e_step()
-    torch.cuda.synchronize()
+    e2e_step()
+    for hp, ho, dt, chunk in e2e_pages:
+        if not np.array_equal(ho.numpy().view(chunk.dtype), chunk):
+            raise SystemExit("decode_to_memory mismatch in benchmark self-check")
     e_steps = max(3, min(args.steps, 10))
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
     for _ in range(e_steps):
         e2e_step()
-    ev1.record(stream)
     torch.cuda.synchronize()
-    e_ms = ev0.elapsed_time(ev1) / e_steps
+    e_ms = (time.perf_counter() - t0) * 1e3 / e_steps
     if world > 1:
         t = torch.tensor([e_ms], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e_ms = float(t.item())
+    e2e_pages = None
+
+    legs = other_configs(dev, args) if (rank == 0 and world == 1 and not args.skip_legs) else None
 
     cpu = None
     if rank == 0 and world == 1:
@@ -369,7 +477,10 @@ def run_ours(args):
                          "traffic": (traffic or {}).get("bytes_per_launch")},
             "cpu_baseline": cpu,
             "e2e": {"value": round(write_b * world / (e_ms * 1e-3) / 1e9, 3), "unit": "GB/s",
-                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": round(e_ms, 3)},
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": round(e_ms, 3),
+                    "api": "fastlanes.h decode_to_memory, pinned host pages in, pinned host values out",
+                    "timer": "host clock around the synchronous call"},
+            "configs": legs,
             "clocks": clocks,
             "gpu_launches": int(launches),
         }

@@ -271,6 +271,11 @@ void fls_cpi_connection_close(connection_cpi* c) { delete c; }
 int fls_encode_from_memory_status(void* in, uint64_t n, uint64_t cap, uint8_t* out, uint64_t* out_size,
                                   uint64_t* mtd_size, enum data_t dt, uint8_t expr) {
 	if (!in && n >= 1024) { return FLS_ERR_ARG; }
+	if (expr == 6) { // RLE DELTA_NO_PATCH
+		const int w = value_width_of(dt);
+		if (w != 32 && w != 64) { return FLS_ERR_UNSUPPORTED; }
+		return encode_rle_page(in, n, cap, out, out_size, mtd_size, w);
+	}
 	switch (dt) {
 	case INT64: return encode_t(static_cast<const uint64_t*>(in), n, cap, out, out_size, mtd_size, true, expr);
 	case UINT64: return encode_t(static_cast<const uint64_t*>(in), n, cap, out, out_size, mtd_size, false, expr);

@@ -31,6 +31,9 @@ int               parse_page_header(const uint8_t* hdr, uint64_t avail, PageInfo
 int               finish_page_info(PageInfo* pi, uint64_t page_size);
 int build_page_column(const PageInfo& pi, const uint8_t* d_page, int value_width, const uint8_t* d_dict_vals,
                       uint32_t dict_entries, int order, uint8_t* d_out, ColDesc* c);
+// RLE DELTA_NO_PATCH page (fls_h_encode.cpp) of n values of width 32 or 64 from host memory.
+int encode_rle_page(const void* in, uint64_t n, uint64_t cap, uint8_t* out, uint64_t* out_size, uint64_t* mtd_size,
+                    int width);
 int int_dictionary_values(const uint8_t* dict, uint64_t dict_size, int value_width, uint64_t* vals_off,
                           uint32_t* entries);
 

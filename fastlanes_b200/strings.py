@@ -63,3 +63,46 @@ class StringPlan:
             self.close()
         except Exception:
             pass
+
+
+_fsst_compress = declare("fls_fsst_compress", ctypes.c_int, [_p, _p, _u64, _p, _u64, ctypes.POINTER(_u64), _p, _u64,
+                                                             _p])
+_enc_dict = declare("fls_encode_string_dict", ctypes.c_int, [_p, _p, ctypes.c_uint32, _p, _u64, _p, _u64,
+                                                             ctypes.POINTER(_u64), _p, _u64, ctypes.POINTER(_u64)])
+
+
+def _np_ptr(a):
+    return a.ctypes.data_as(_p)
+
+
+def fsst_compress(byts, offsets):
+    """FSST-compress n strings given as (bytes, offsets[n + 1]) numpy arrays (host only).
+    Returns (table bytes in fsst_export format, compressed bytes, compressed offsets[n + 1])."""
+    import numpy as np
+
+    byts = np.ascontiguousarray(byts, np.uint8)
+    offsets = np.ascontiguousarray(offsets, np.uint64)
+    n = offsets.size - 1
+    table = np.zeros(2100, np.uint8)
+    tl = _u64()
+    comp = np.zeros(2 * byts.size + 16, np.uint8)
+    coffs = np.zeros(n + 1, np.uint64)
+    check(_fsst_compress(_np_ptr(byts), _np_ptr(offsets), n, _np_ptr(table), table.size, ctypes.byref(tl),
+                         _np_ptr(comp), comp.size, _np_ptr(coffs)), "fls_fsst_compress")
+    return table[: tl.value].copy(), comp[: int(coffs[-1])].copy(), coffs
+
+
+def encode_string_dict(dict_bytes, dict_offsets, codes):
+    """String DICT FFOR page of codes into a dictionary; returns (page bytes, dictionary page bytes)."""
+    import numpy as np
+
+    dict_bytes = np.ascontiguousarray(dict_bytes, np.uint8)
+    dict_offsets = np.ascontiguousarray(dict_offsets, np.uint64)
+    codes = np.ascontiguousarray(codes, np.uint32)
+    page = np.zeros(codes.size * 4 + 65536, np.uint8)
+    dic = np.zeros(8 + 2066 + 4 * (dict_offsets.size - 1) + 2 * dict_bytes.size + 64, np.uint8)
+    ps, ds = _u64(), _u64()
+    check(_enc_dict(_np_ptr(dict_bytes), _np_ptr(dict_offsets), dict_offsets.size - 1, _np_ptr(codes), codes.size,
+                    _np_ptr(page), page.size, ctypes.byref(ps), _np_ptr(dic), dic.size, ctypes.byref(ds)),
+          "fls_encode_string_dict")
+    return page[: ps.value].copy(), dic[: ds.value].copy()

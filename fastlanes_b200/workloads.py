@@ -138,3 +138,56 @@ def bw_sweep(n32=65536, n64=32768, seed=0, device="cuda", keep_values=False):
     items = items[rng.permutation(items.size)]
     queue = torch.from_numpy(items.view(np.int32)).to(device)
     return [c32, c64], queue
+
+
+# ---------------------------------------------------------------------------------------------------------------
+# Page workloads (host arrays -> reference-format pages through the engine's own encoders)
+# ---------------------------------------------------------------------------------------------------------------
+def ffor_u32_bw7(n_vec=1024, seed=0):
+    """1024 vectors; per vector base ~ U[0, 2^20), values = base + U[0, 2^7); FOR with the drawn base at bw 7.
+    Returns (packed bytes, byte offsets, bw, base, transposed values) as numpy arrays."""
+    rng = np.random.default_rng(seed)
+    base = rng.integers(0, 1 << 20, n_vec).astype(np.uint32)
+    vals = (rng.integers(0, 1 << 7, (n_vec, 1024)) + base[:, None]).astype(np.uint32)
+    return base, vals
+
+
+def delta_timestamps(n=32 << 20, seed=0):
+    """Sorted int64 timestamps from 1.6e18 with geometric(p = 0.1, support >= 1, mean 10) gaps."""
+    rng = np.random.default_rng(seed)
+    gaps = rng.geometric(0.1, n).astype(np.int64)
+    return (1_600_000_000_000_000_000 + np.cumsum(gaps)).astype(np.int64)
+
+
+def rle_int32(n=32 << 20, seed=0):
+    """int32 run values ~ U[0, 1e6) with geometric(mean 8) run lengths."""
+    rng = np.random.default_rng(seed)
+    runs = rng.geometric(1 / 8, n // 4 + 1024)
+    vals = rng.integers(0, 10**6, runs.size).astype(np.int32)
+    out = np.repeat(vals, runs)
+    return out[:n].copy()
+
+
+def string_dictionary(seed=0, n_dict=4096, n_tokens=256):
+    """n_dict strings of uniform length 5..40 over a 64-symbol alphabet, each made of Zipf(1.2)-chosen tokens
+    out of n_tokens seeded 2..6-byte tokens.  Returns (bytes, offsets[n_dict + 1])."""
+    rng = np.random.default_rng(seed)
+    alphabet = np.frombuffer(b"abcdefghijklmnopqrstuvwxyzABCDEFGHIJKLMNOPQRSTUVWXYZ0123456789-_", np.uint8)
+    tokens = [bytes(alphabet[rng.integers(0, 64, rng.integers(2, 7))]) for _ in range(n_tokens)]
+    picks = (rng.zipf(1.2, n_dict * 64) - 1) % n_tokens
+    out, j = [], 0
+    for _ in range(n_dict):
+        target = int(rng.integers(5, 41))
+        s = b""
+        while len(s) < target:
+            s += tokens[picks[j]]
+            j += 1
+        out.append(s[:target])
+    offs = np.zeros(n_dict + 1, np.uint64)
+    offs[1:] = np.cumsum([len(s) for s in out])
+    return np.frombuffer(b"".join(out), np.uint8).copy(), offs
+
+
+def zipf_codes(n_rows=16 << 20, n_dict=4096, a=1.1, seed=0):
+    rng = np.random.default_rng(seed)
+    return ((rng.zipf(a, n_rows) - 1) % n_dict).astype(np.uint32)

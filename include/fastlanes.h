@@ -4,8 +4,9 @@
  * links against libfls_b200.so unchanged.  encode_from_memory encodes on the GPU and frames the result as a
  * FastLanes page (bit-identical to the reference's page for the same input); decode_to_memory decodes on the
  * GPU.  Both take HOST pointers and copy through device memory.  Besides the reference's INT64 expressions
- * 0 (UNCOMPRESSED), 1 (FFOR) and 11 (DELTA), the engine also accepts UINT32 / INT32 / UINT64 columns with the
- * same framing (T = the 32/64-bit type).
+ * 0 (UNCOMPRESSED), 1 (FFOR) and 11 (DELTA), the engine encodes expression 6 (RLE DELTA_NO_PATCH, the pool
+ * id of src/cor/exp_pool.cpp:31) and accepts UINT32 / INT32 / UINT64 columns with the same framing
+ * (T = the 32/64-bit type).
  */
 #ifndef FASTLANES_H
 #define FASTLANES_H

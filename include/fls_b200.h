@@ -242,6 +242,22 @@ int fls_gpu_decode_fsst_page_noalloc(const uint8_t* d_page, uint64_t page_size, 
                                      uint64_t dict_size, uint32_t* d_offsets, uint8_t* d_bytes, uint64_t bytes_cap,
                                      int* d_status, fls_stream_t stream);
 
+/* ---------------------------------------------------------------------------------------------------------
+ * Encoders for string pages (host memory in and out).
+ * fls_fsst_compress: builds an FSST symbol table over n strings (Arrow offsets, n + 1) and compresses them;
+ *   table_out receives the table in fsst_export's format (src/cor/prm/fsst/libfsst.cpp:581-615, read by
+ *   fsst_import :617-657), comp_offsets (n + 1) the compressed strings' boundaries.
+ * fls_encode_string_dict: a string DICT FFOR_NO_PATCH page (str expression 3, src/cor/exp_pool.cpp:69) of
+ *   n_rows codes into a dictionary of n_dict strings, and its FSST-compressed dictionary page
+ *   (src/cor/lyt/dic/dic.cpp:88-111) with the true compressed length of every entry.
+ * ------------------------------------------------------------------------------------------------------- */
+int fls_fsst_compress(const uint8_t* bytes, const uint64_t* offsets, uint64_t n, uint8_t* table_out,
+                      uint64_t table_cap, uint64_t* table_size, uint8_t* comp_out, uint64_t comp_cap,
+                      uint64_t* comp_offsets);
+int fls_encode_string_dict(const uint8_t* dict_bytes, const uint64_t* dict_offsets, uint32_t n_dict,
+                           const uint32_t* codes, uint64_t n_rows, uint8_t* page_out, uint64_t page_cap,
+                           uint64_t* page_size, uint8_t* dict_out, uint64_t dict_cap, uint64_t* dict_size);
+
 #ifdef __cplusplus
 }
 #endif

@@ -106,3 +106,29 @@ def test_c_api_rejects_unknown_expression(cuda):
 
     with pytest.raises(_lib.FlsError):
         pages.encode_from_memory(np.arange(2048, dtype=np.int64), pages.INT64, 2)
+
+
+def test_c_api_rle_matches_reference_bytes(cuda, col_golden):
+    from fastlanes_b200 import pages
+
+    want = col_golden["i64_6_input"]
+    page, _ = pages.encode_from_memory(want, pages.INT64, 6)
+    assert np.array_equal(page, col_golden["i64_6_page"])
+
+
+@pytest.mark.parametrize("dt", ["UINT32", "INT32", "INT64"])
+def test_rle_round_trip_through_the_page_decoder(cuda, dt):
+    import torch
+
+    from fastlanes_b200 import pages
+
+    code = getattr(pages, dt)
+    T = pages.DTYPE_OF[code]
+    rng = np.random.default_rng(code)
+    runs = rng.geometric(1 / 8, 20000)
+    x = np.repeat(rng.integers(0, 10**6, runs.size), runs)[: 7 * 1024].astype(T)
+    page, _ = pages.encode_from_memory(x, code, 6)
+    pb, pp = _dev_bytes(page, cuda, 2)
+    out = torch.zeros(x.size, dtype=torch.from_numpy(np.zeros(1, T)).dtype, device=cuda)
+    pages.decode_pages([dict(d_page=pp, page_size=page.size, data_type=code, order=1, d_out=out.data_ptr())])
+    assert np.array_equal(out.cpu().numpy(), x)

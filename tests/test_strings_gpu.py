@@ -43,3 +43,25 @@ def test_reference_string_pages(cuda, col_golden, eid, shift):
     assert np.array_equal(offs2.cpu().numpy(), offs.cpu().numpy()) and np.array_equal(data2.cpu().numpy(), want_b)
     plan.close()
     assert P.device_status() == 0
+
+
+def test_string_dict_encoder_round_trip(cuda):
+    """Our DICT + FSST encoder (true entry lengths) decodes back to dict[codes] on the GPU."""
+    from fastlanes_b200 import strings
+    from tests.test_encoders import _strings
+
+    rng = np.random.default_rng(4)
+    dbytes, doffs = _strings(rng, 700)
+    n_dict = doffs.size - 1
+    codes = (rng.zipf(1.1, 9 * 1024) % n_dict).astype(np.uint32)
+    page, dic = strings.encode_string_dict(dbytes, doffs, codes)
+    pb, pp = _dev(page, cuda, 5)
+    db, dp = _dev(dic, cuda, 2)
+    plan = strings.StringPlan(pp, page.size, dp, dic.size)
+    offs, data = plan.decode(cuda)
+    plan.close()
+    want = [dbytes[int(doffs[c]):int(doffs[c + 1])] for c in codes]
+    want_off = np.zeros(codes.size + 1, np.uint64)
+    want_off[1:] = np.cumsum([w.size for w in want])
+    assert np.array_equal(offs.cpu().numpy().astype(np.uint64), want_off)
+    assert np.array_equal(data.cpu().numpy(), np.concatenate(want))
