@@ -33,6 +33,7 @@ struct Plan {
 	uint32_t       ghead; // offset of the run values inside the staged (16-byte aligned) copy
 	uint8_t        ws, e, enc, post, order;
 	bool           ok;
+	bool           lb_exact; // lane bases outside a page: copy exactly 128 bytes, never a window around them
 };
 
 __device__ __forceinline__ uint64_t ld_le(const uint8_t* p, uint32_t n) {
@@ -52,6 +53,32 @@ __device__ __forceinline__ uint64_t ld_le(const uint8_t* p, uint32_t n) {
 
 // Entry points sit at page offset 8 + 4*arr_c; a page may be placed at any byte address (it is placed so that
 // its packed buffer is 16-byte aligned), so they are read alignment-agnostically.
+// Little-endian load of 4 / 8 bytes at any byte address inside a shared-memory staging area that has at least 8
+// readable bytes after it: aligned words joined by funnel shifts instead of byte loads.
+__device__ __forceinline__ uint32_t sld4(const uint8_t* p) {
+	const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+	const uint32_t* w = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+	return (a & 3u) ? __funnelshift_r(w[0], w[1], (a & 3u) * 8u) : w[0];
+}
+__device__ __forceinline__ uint64_t sld8(const uint8_t* p) {
+	const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+	const uint32_t* w = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+	const uint32_t  s = (a & 3u) * 8u;
+	const uint32_t  lo = s ? __funnelshift_r(w[0], w[1], s) : w[0];
+	const uint32_t  hi = s ? __funnelshift_r(w[1], w[2], s) : w[1];
+	return (static_cast<uint64_t>(hi) << 32) | lo;
+}
+template <int E>
+__device__ __forceinline__ uint64_t sld(const uint8_t* p) {
+	if constexpr (E == 8) {
+		return sld8(p);
+	} else if constexpr (E == 4) {
+		return sld4(p);
+	} else {
+		return ld_le(p, E);
+	}
+}
+
 __device__ __forceinline__ uint32_t ep_of(const ColDesc& c, uint32_t v, uint32_t i) {
 	if (v == 0) { return 0u; }
 	return static_cast<uint32_t>(ld_le(reinterpret_cast<const uint8_t*>(c.ep) + 4ull * ((v - 1) * c.arr_c + i), 4));
@@ -68,6 +95,7 @@ __device__ __forceinline__ Plan make_plan(const ColDesc& c, uint32_t v) {
 	p.dict    = c.dict;
 	p.out     = c.out + static_cast<uint64_t>(v) * kVec * c.e;
 	p.ok      = v < c.n_vec;
+	p.lb_exact   = c.layout == LAYOUT_ARRAYS;
 	p.for_base   = 0;
 	p.lane_bases = nullptr;
 	p.gsrc       = nullptr;
@@ -123,9 +151,23 @@ __device__ __forceinline__ Plan make_plan(const ColDesc& c, uint32_t v) {
 // plan.  16-byte aligned packed words go through the TMA engine; anything else is copied by the warp.
 // The run values of an RLE vector are fetched as the enclosing 16-byte aligned window (pages are placed
 // with at least 16 bytes of slack on both sides), so they always take the TMA path.
+// The 128 lane bases of a DELTA vector travel with its packed words: the 16-byte aligned window around them
+// (at most 144 bytes, inside the page) lands in a per-slot area of kLaneWindow bytes.
+constexpr uint32_t kLaneWindow = 256;
+
 template <uint32_t GSTAGE>
-__device__ __forceinline__ void issue(const Plan& p, uint8_t* stage, uint8_t* gstage, uint64_t* bar, uint32_t lane) {
-	uint32_t   tx      = 0;
+__device__ __forceinline__ void issue(const Plan& p, uint8_t* stage, uint8_t* gstage, uint8_t* lbstage, uint64_t* bar,
+                                      uint32_t lane) {
+	uint32_t       tx     = 0;
+	const uint32_t lbhead = static_cast<uint32_t>(reinterpret_cast<uintptr_t>(p.lane_bases) & 15u);
+	// 16-byte aligned lane bases: exactly their 128 bytes by TMA; inside a page: the aligned 144-byte window by
+	// TMA; otherwise (a misaligned caller array) the warp copies the 128 bytes
+	const bool lbtma  = p.ok && p.lane_bases != nullptr && (lbhead == 0 || !p.lb_exact);
+	const bool lbwarp = p.ok && p.lane_bases != nullptr && !lbtma;
+	const uint32_t lbbytes = lbhead ? 144u : 128u;
+	if (lbwarp) {
+		for (uint32_t i = lane; i < 128; i += 32) { lbstage[lbhead + i] = p.lane_bases[i]; }
+	}
 	const bool tma_pk  = p.ok && p.bytes > 0 && (reinterpret_cast<uintptr_t>(p.src) & 15u) == 0;
 	uint32_t   gwindow = 0;
 	if (GSTAGE > 0 && p.ok && p.gbytes > 0) { gwindow = (p.ghead + p.gbytes + 15u) & ~15u; }
@@ -143,9 +185,11 @@ __device__ __forceinline__ void issue(const Plan& p, uint8_t* stage, uint8_t* gs
 	if (lane == 0) {
 		if (tma_pk) { tx += p.bytes; }
 		tx += gwindow;
+		if (lbtma) { tx += lbbytes; }
 		mbar_arrive_expect_tx(bar, tx);
 		if (tma_pk) { bulk_g2s(stage, p.src, p.bytes, bar); }
 		if (gwindow) { bulk_g2s(gstage, p.gsrc - p.ghead, gwindow, bar); }
+		if (lbtma) { bulk_g2s(lbstage, p.lane_bases - lbhead, lbbytes, bar); }
 	}
 }
 
@@ -348,7 +392,7 @@ __device__ __forceinline__ void decode_vector(const Plan& p, const uint8_t* stag
 			const uint32_t idx = static_cast<uint32_t>(v[i]);
 			const bool     in  = idx < p.n_runs;
 			bad |= !in;
-			o[i] = in ? static_cast<OT>(ld_le(vals + static_cast<uint64_t>(idx) * E, E)) : OT(0);
+			o[i] = in ? static_cast<OT>(sld<E>(vals + static_cast<uint64_t>(idx) * E)) : OT(0);
 		}
 	} else {
 		const uint8_t* codes = gstage + p.ghead;
@@ -358,7 +402,7 @@ __device__ __forceinline__ void decode_vector(const Plan& p, const uint8_t* stag
 			if (p.post == POST_RLE_DICT) {
 				const bool in = code < p.n_runs;
 				bad |= !in;
-				code = in ? static_cast<uint32_t>(ld_le(codes + 4ull * code, 4)) : 0u;
+				code = in ? sld4(codes + 4ull * code) : 0u;
 			}
 			const bool in = code < p.entry_c;
 			bad |= !in;
@@ -380,7 +424,7 @@ struct __align__(16) PlanS {
 	uint32_t       gbytes;
 	uint32_t       entry_c;
 	uint16_t       bytes;
-	uint8_t        bw, ws, e, enc, post, flags; // flags: bit0 original order, bit1 ok, bit2 valid item
+	uint8_t        bw, ws, e, enc, post, flags; // flags: bit0 original order, bit1 ok, bit2 valid, bit3 lb_exact
 };
 static_assert(sizeof(PlanS) == 64, "PlanS layout");
 
@@ -400,7 +444,7 @@ __device__ __forceinline__ PlanS pack_plan(const Plan& p, bool valid) {
 	s.e          = p.e;
 	s.enc        = p.enc;
 	s.post       = p.post;
-	s.flags      = static_cast<uint8_t>((p.order ? 1 : 0) | (p.ok ? 2 : 0) | (valid ? 4 : 0));
+	s.flags      = static_cast<uint8_t>((p.order ? 1 : 0) | (p.ok ? 2 : 0) | (valid ? 4 : 0) | (p.lb_exact ? 8 : 0));
 	return s;
 }
 
@@ -422,6 +466,7 @@ __device__ __forceinline__ Plan unpack_plan(const PlanS& s) {
 	p.post       = s.post;
 	p.order      = s.flags & 1u;
 	p.ok         = (s.flags & 2u) != 0;
+	p.lb_exact   = (s.flags & 8u) != 0;
 	const uint32_t ve = p.post == POST_RLE ? p.e : 4u;
 	p.n_runs     = (p.post == POST_RLE || p.post == POST_RLE_DICT) ? p.gbytes / ve : 0u;
 	p.ghead      = static_cast<uint32_t>(reinterpret_cast<uintptr_t>(p.gsrc) & 15u);
@@ -449,7 +494,7 @@ struct Geometry {
 	static constexpr uint32_t kStage   = MAXWS * 128u;
 	static constexpr uint32_t kOut     = EMAX * 1024u;
 	static constexpr uint32_t kMain    = kStage > kOut ? kStage : kOut;
-	static constexpr uint32_t kSlot    = kMain + GSTAGE;
+	static constexpr uint32_t kSlot    = kMain + kLaneWindow + GSTAGE;
 	static constexpr uint32_t kPlans   = 2 * kPB * sizeof(PlanS);
 	static constexpr uint32_t kPerWarp = 64u + kPlans + STAGES * kSlot;
 	static constexpr uint32_t kSlack   = 256u; // extraction reads one row past the last stage
@@ -506,7 +551,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_decode(const DecodeArgs a) {
 	const uint64_t n  = a.n_items;
 
 	auto stage_ptr  = [&](uint32_t s) { return stages + s * G::kSlot; };
-	auto gstage_ptr = [&](uint32_t s) { return stages + s * G::kSlot + G::kMain; };
+	auto lb_ptr     = [&](uint32_t s) { return stages + s * G::kSlot + G::kMain; };
+	auto gstage_ptr = [&](uint32_t s) { return stages + s * G::kSlot + G::kMain + kLaneWindow; };
 	// Lane-parallel metadata fetch: lane j resolves the plan of the warp's item blk*PB + j.
 	auto fill = [&](uint32_t blk) {
 		if (lane < PB) {
@@ -520,7 +566,9 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_decode(const DecodeArgs a) {
 	};
 	auto issue_k = [&](uint64_t k, uint32_t s) {
 		const PlanS& ps = plans[k % (2 * PB)];
-		if (ps.flags & 4u) { issue<GSTAGE>(unpack_plan(ps), stage_ptr(s), gstage_ptr(s), &bars[s], lane); }
+		if (ps.flags & 4u) {
+			issue<GSTAGE>(unpack_plan(ps), stage_ptr(s), gstage_ptr(s), lb_ptr(s), &bars[s], lane);
+		}
 	};
 
 	fill(0);
@@ -537,7 +585,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_decode(const DecodeArgs a) {
 		}
 		const uint32_t s      = k % STAGES;
 		const uint32_t parity = (k / STAGES) & 1u;
-		const Plan     p      = unpack_plan(plans[k % (2 * PB)]);
+		Plan           p      = unpack_plan(plans[k % (2 * PB)]);
 		if (!mbar_wait(&bars[s], parity)) {
 			if (lane == 0) { atomicOr(a.status, STATUS_TIMEOUT); }
 			aborted = true;
@@ -546,6 +594,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_decode(const DecodeArgs a) {
 		if (!p.ok) {
 			if (lane == 0) { atomicOr(a.status, p.bw > p.ws ? STATUS_BAD_BW : STATUS_BAD_LAYOUT); }
 		} else {
+			// the lane bases were staged with the packed words
+			if (p.lane_bases) { p.lane_bases = lb_ptr(s) + (reinterpret_cast<uintptr_t>(p.lane_bases) & 15u); }
 			decode_dispatch<MAXWS, GSTAGE, EMAX>(p, stage_ptr(s), gstage_ptr(s), lane, a.status);
 		}
 		__syncwarp();

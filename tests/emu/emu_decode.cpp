@@ -37,7 +37,7 @@ static void dispatch(const Plan& p, const uint8_t* st, const uint8_t* gs, uint8_
 }
 
 static int emu_vector(const ColDesc& c, uint32_t v) {
-	const Plan p = make_plan(c, v);
+	Plan p = make_plan(c, v);
 	if (!p.ok) { return p.bw > p.ws ? STATUS_BAD_BW : STATUS_BAD_LAYOUT; }
 	std::vector<uint8_t> smem(3 * 8448 + 8192, 0xA5);
 	uint8_t*             stage  = smem.data();
@@ -46,6 +46,18 @@ static int emu_vector(const ColDesc& c, uint32_t v) {
 	if (p.gbytes) {
 		const uint32_t win = (p.ghead + p.gbytes + 15u) & ~15u;
 		std::memcpy(gstage, p.gsrc - p.ghead, win);
+	}
+	std::vector<uint8_t> lbwin(256 + 16, 0xA5);
+	if (p.lane_bases) {
+		// as on the GPU: the 16-byte aligned 144-byte window around the lane bases, staged
+		uint8_t*        lb   = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(lbwin.data()) + 15) & ~uintptr_t(15));
+		const uintptr_t head = reinterpret_cast<uintptr_t>(p.lane_bases) & 15u;
+		if (p.lb_exact || head == 0) {
+			std::memcpy(lb + head, p.lane_bases, 128);
+		} else {
+			std::memcpy(lb, p.lane_bases - head, 144);
+		}
+		p.lane_bases = lb + head;
 	}
 	int                      status = 0;
 	std::barrier<>           bar(32);

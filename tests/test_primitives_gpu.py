@@ -198,3 +198,29 @@ def test_plan_mixed_batch_shuffled_queue(cuda, keep_order, order):
     from fastlanes_b200 import primitives as P
 
     assert P.device_status() == 0
+
+
+@pytest.mark.parametrize("w", [16, 32, 64])
+def test_delta_with_misaligned_lane_bases(cuda, w):
+    """Lane bases that do not start on a 16-byte boundary are copied by the warp, not by a TMA window."""
+    import torch
+
+    from fastlanes_b200 import primitives as P
+
+    T = TYPES[w]
+    rng = np.random.default_rng(600 + w)
+    packed, offs, bw, base, _ = _batch(w, 60, rng)
+    lb = rng.integers(0, np.iinfo(np.uint64).max, 60 * (1024 // w), dtype=np.uint64, endpoint=True).astype(T)
+    raw = torch.zeros(lb.nbytes + 8, dtype=torch.uint8, device=cuda)
+    raw[4:4 + lb.nbytes] = torch.from_numpy(lb.view(np.uint8)).to(cuda)
+    lb_view = raw[4:4 + lb.nbytes]
+    from fastlanes_b200._lib import lib
+
+    out = torch.empty(60 * 1024, dtype=getattr(torch, f"uint{w}"), device=cuda)
+    rc = getattr(lib, f"fls_gpu_unffor_rsum_u{w}")(_t(packed, cuda).data_ptr(), out.data_ptr(), _t(bw, cuda).data_ptr(),
+                                                   _t(base, cuda).data_ptr(), lb_view.data_ptr(),
+                                                   _t(offs, cuda).data_ptr(), 60, 1,
+                                                   torch.cuda.current_stream().cuda_stream)
+    assert rc == 0
+    assert np.array_equal(_np(out), oracle.delta_batch(packed, offs, bw, base, lb, True))
+    assert P.device_status() == 0
