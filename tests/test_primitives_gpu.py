@@ -217,9 +217,9 @@ def test_delta_with_misaligned_lane_bases(cuda, w):
     from fastlanes_b200._lib import lib
 
     out = torch.empty(60 * 1024, dtype=getattr(torch, f"uint{w}"), device=cuda)
-    rc = getattr(lib, f"fls_gpu_unffor_rsum_u{w}")(_t(packed, cuda).data_ptr(), out.data_ptr(), _t(bw, cuda).data_ptr(),
-                                                   _t(base, cuda).data_ptr(), lb_view.data_ptr(),
-                                                   _t(offs, cuda).data_ptr(), 60, 1,
+    keep = [_t(packed, cuda), _t(bw, cuda), _t(base, cuda), _t(offs, cuda)]  # alive until the kernel has run
+    rc = getattr(lib, f"fls_gpu_unffor_rsum_u{w}")(keep[0].data_ptr(), out.data_ptr(), keep[1].data_ptr(),
+                                                   keep[2].data_ptr(), lb_view.data_ptr(), keep[3].data_ptr(), 60, 1,
                                                    torch.cuda.current_stream().cuda_stream)
     assert rc == 0
     assert np.array_equal(_np(out), oracle.delta_batch(packed, offs, bw, base, lb, True))
