@@ -306,10 +306,12 @@ def other_configs(dev, args):
         o = torch.empty(values.size, dtype=torch.from_numpy(values[:1]).dtype, device=dev)
         col = [dict(d_page=buf.data_ptr() + shift, page_size=page.size, data_type=dtype, order=1,
                     d_out=o.data_ptr())]
-        PG.decode_pages(col)
+        plan = PG.PagePlan(col)
+        plan.decode()
         ok = np.array_equal(o.cpu().numpy(), values)
-        ms = device_timed(lambda: PG.decode_pages(col), steps, 3)
+        ms = device_timed(plan.decode, steps, 3)
         leg(name, workload, ms, page.size, values.nbytes, values.size, ok, 1)
+        plan.close()
 
     page_leg("3a_delta_i64", "32Mi sorted int64 timestamps from 1.6e18, geometric(mean 10) gaps, DELTA (id 11)",
              W.delta_timestamps(), PG.INT64, 11)
@@ -320,9 +322,11 @@ def other_configs(dev, args):
     dbytes, doffs = W.string_dictionary()
     codes = W.zipf_codes()
     page, dic = S.encode_string_dict(dbytes, doffs, codes)
-    pb = torch.from_numpy(page).to(dev)
+    shift = PG.placement(page)  # packed codes on a 16-byte boundary
+    pb = torch.zeros(page.size + 64, dtype=torch.uint8, device=dev)
+    pb[shift:shift + page.size] = torch.from_numpy(page).to(dev)
     db = torch.from_numpy(dic).to(dev)
-    plan = S.StringPlan(pb.data_ptr(), page.size, db.data_ptr(), dic.size)
+    plan = S.StringPlan(pb.data_ptr() + shift, page.size, db.data_ptr(), dic.size)
     n_bytes = plan.measure()
     offs_t = torch.empty(plan.n_rows + 1, dtype=torch.int32, device=dev)
     data_t = torch.empty(n_bytes + 16, dtype=torch.uint8, device=dev)

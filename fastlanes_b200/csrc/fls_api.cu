@@ -383,6 +383,37 @@ struct fls_plan {
 	ColDesc   col0 {};
 };
 
+namespace flsgpu {
+int make_plan_object(const std::vector<ColDesc>& descs, const std::vector<uint32_t>& queue, Family fam,
+                     ::fls_plan** out) {
+	std::unique_ptr<fls_plan> p(new fls_plan());
+	if (cudaGetDevice(&p->device) != cudaSuccess) { return FLS_ERR_CUDA; }
+	p->n_cols = static_cast<uint32_t>(descs.size());
+	p->family = fam;
+	if (descs.size() == 1) {
+		// one column: the queue is implicit (vector v = item v)
+		p->col0    = descs[0];
+		p->n_items = queue.size();
+	} else {
+		if (cudaMalloc(&p->d_cols, sizeof(ColDesc) * descs.size()) != cudaSuccess) { return FLS_ERR_CUDA; }
+		if (cudaMemcpy(p->d_cols, descs.data(), sizeof(ColDesc) * descs.size(), cudaMemcpyHostToDevice) !=
+		    cudaSuccess) {
+			return FLS_ERR_CUDA;
+		}
+		if (!queue.empty()) {
+			if (cudaMalloc(&p->d_queue, sizeof(uint32_t) * queue.size()) != cudaSuccess) { return FLS_ERR_CUDA; }
+			if (cudaMemcpy(p->d_queue, queue.data(), sizeof(uint32_t) * queue.size(), cudaMemcpyHostToDevice) !=
+			    cudaSuccess) {
+				return FLS_ERR_CUDA;
+			}
+		}
+		p->n_items = queue.size();
+	}
+	*out = p.release();
+	return FLS_OK;
+}
+} // namespace flsgpu
+
 extern "C" {
 
 int fls_plan_create(const fls_vector_batch* batches, uint32_t n_batches, const uint32_t* d_queue, uint64_t n_items,

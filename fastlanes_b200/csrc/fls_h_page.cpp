@@ -161,18 +161,21 @@ int fls_page_info(const uint8_t* page_prefix, uint64_t prefix_size, uint32_t* ex
 	return FLS_OK;
 }
 
-int fls_gpu_decode_pages(const fls_page_column* cols, uint32_t n_cols, fls_stream_t stream) {
+// Descriptors, work queue and kernel family for a set of page columns (reads each page's header from the
+// device).
+static int describe_pages(const fls_page_column* cols, uint32_t n_cols, std::vector<ColDesc>* descs,
+                          std::vector<uint32_t>* queue, Family* fam_out) {
 	if (!cols || n_cols == 0 || n_cols > 255) { return FLS_ERR_ARG; }
-	std::vector<ColDesc>  descs(n_cols);
-	std::vector<uint32_t> queue;
-	Family                fam   = Family::NUM;
-	bool                  any64 = false;
+	descs->assign(n_cols, ColDesc {});
+	queue->clear();
+	Family fam   = Family::NUM;
+	bool   any64 = false;
 	for (uint32_t i = 0; i < n_cols; ++i) {
 		const fls_page_column& pc = cols[i];
 		const int              w  = value_width_of(pc.data_type);
 		if (!pc.d_page || !pc.d_out || w == 0 || pc.order > FLS_ORIGINAL) { return FLS_ERR_ARG; }
 		if ((reinterpret_cast<uintptr_t>(pc.d_out) & 15u) != 0) { return FLS_ERR_ARG; }
-		uint8_t hdr[8 + 4 * 8];
+		uint8_t        hdr[8 + 4 * 8];
 		const uint64_t take = pc.page_size < sizeof(hdr) ? pc.page_size : sizeof(hdr);
 		if (cudaMemcpy(hdr, pc.d_page, take, cudaMemcpyDeviceToHost) != cudaSuccess) { return FLS_ERR_CUDA; }
 		PageInfo pi;
@@ -190,13 +193,24 @@ int fls_gpu_decode_pages(const fls_page_column* cols, uint32_t n_cols, fls_strea
 			if (rc != FLS_OK) { return rc; }
 			dvals = pc.d_dict + voff;
 		}
-		rc = build_page_column(pi, pc.d_page, w, dvals, entries, pc.order, static_cast<uint8_t*>(pc.d_out), &descs[i]);
+		rc = build_page_column(pi, pc.d_page, w, dvals, entries, pc.order, static_cast<uint8_t*>(pc.d_out),
+		                       &(*descs)[i]);
 		if (rc != FLS_OK) { return rc; }
-		if (descs[i].post != POST_NONE) { fam = Family::GATHER; }
-		if (descs[i].ws == 64) { any64 = true; }
-		for (uint32_t v = 0; v < pi.vec_c; ++v) { queue.push_back((i << 24) | v); }
+		if ((*descs)[i].post != POST_NONE) { fam = Family::GATHER; }
+		if ((*descs)[i].ws == 64) { any64 = true; }
+		for (uint32_t v = 0; v < pi.vec_c; ++v) { queue->push_back((i << 24) | v); }
 	}
 	if (fam == Family::GATHER && any64) { fam = Family::ANY; }
+	*fam_out = fam;
+	return FLS_OK;
+}
+
+int fls_gpu_decode_pages(const fls_page_column* cols, uint32_t n_cols, fls_stream_t stream) {
+	std::vector<ColDesc>  descs;
+	std::vector<uint32_t> queue;
+	Family                fam = Family::NUM;
+	int                   rc  = describe_pages(cols, n_cols, &descs, &queue, &fam);
+	if (rc != FLS_OK) { return rc; }
 	if (queue.empty()) { return FLS_OK; }
 	cudaStream_t s = static_cast<cudaStream_t>(stream);
 	DecodeArgs   a {};
@@ -219,6 +233,17 @@ int fls_gpu_decode_pages(const fls_page_column* cols, uint32_t n_cols, fls_strea
 	cudaFreeAsync(d_cols, s);
 	cudaFreeAsync(d_queue, s);
 	return e == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
+}
+
+int fls_plan_create_pages(const fls_page_column* cols, uint32_t n_cols, fls_plan** out_plan) {
+	if (!out_plan) { return FLS_ERR_ARG; }
+	*out_plan = nullptr;
+	std::vector<ColDesc>  descs;
+	std::vector<uint32_t> queue;
+	Family                fam = Family::NUM;
+	const int             rc  = describe_pages(cols, n_cols, &descs, &queue, &fam);
+	if (rc != FLS_OK) { return rc; }
+	return make_plan_object(descs, queue, fam, out_plan);
 }
 
 } // extern "C"

@@ -83,14 +83,24 @@ __global__ void __launch_bounds__(1024) k_fsst_dict(const uint8_t* lens, const u
 // Per-vector building blocks
 // ---------------------------------------------------------------------------------------------------------
 // Warp copy of n bytes global -> shared (16-byte loads when both sides allow it).
-__device__ __forceinline__ void warp_copy(uint8_t* dst, const uint8_t* src, uint32_t n, uint32_t lane) {
-	if (((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15u) == 0) {
+__device__ __forceinline__ void warp_copy(uint8_t* __restrict__ dst, const uint8_t* __restrict__ src, uint32_t n,
+                                          uint32_t lane) {
+	const uintptr_t al = reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst);
+	if ((al & 15u) == 0) {
+#pragma unroll 4
 		for (uint32_t i = lane * 16; i + 16 <= n; i += 512) {
-			*reinterpret_cast<uint4*>(dst + i) = *reinterpret_cast<const uint4*>(src + i);
+			*reinterpret_cast<uint4*>(dst + i) = __ldg(reinterpret_cast<const uint4*>(src + i));
 		}
 		for (uint32_t i = (n & ~15u) + lane; i < n; i += 32) { dst[i] = src[i]; }
+	} else if ((al & 3u) == 0) {
+#pragma unroll 8
+		for (uint32_t i = lane * 4; i + 4 <= n; i += 128) {
+			*reinterpret_cast<uint32_t*>(dst + i) = __ldg(reinterpret_cast<const uint32_t*>(src + i));
+		}
+		for (uint32_t i = (n & ~3u) + lane; i < n; i += 32) { dst[i] = src[i]; }
 	} else {
-		for (uint32_t i = lane; i < n; i += 32) { dst[i] = src[i]; }
+#pragma unroll 8
+		for (uint32_t i = lane; i < n; i += 32) { dst[i] = __ldg(src + i); }
 	}
 }
 
@@ -240,8 +250,12 @@ __global__ void __launch_bounds__(kStrWarps * 32) k_str_materialize(const StrArg
 	if (a.kind == STR_DICT && a.dict_in_smem) {
 		uint8_t* db = dict_smem;
 		uint32_t* de = reinterpret_cast<uint32_t*>(dict_smem + ((a.dict_bytes_n + 15) & ~15ull));
-		for (uint32_t i = threadIdx.x; i < a.dict_bytes_n; i += blockDim.x) { db[i] = a.dict_bytes[i]; }
-		for (uint32_t i = threadIdx.x; i < a.entry_c; i += blockDim.x) { de[i] = a.dict_ends[i]; }
+		// the decoded dictionary lives in cudaMalloc'd (256-byte aligned) plan buffers
+		const uint32_t nb16 = static_cast<uint32_t>((a.dict_bytes_n + 15) / 16);
+		for (uint32_t i = threadIdx.x; i < nb16; i += blockDim.x) {
+			reinterpret_cast<uint4*>(db)[i] = __ldg(reinterpret_cast<const uint4*>(a.dict_bytes) + i);
+		}
+		for (uint32_t i = threadIdx.x; i < a.entry_c; i += blockDim.x) { de[i] = __ldg(a.dict_ends + i); }
 		dbytes = db;
 		dends  = de;
 	}
@@ -306,19 +320,26 @@ __global__ void __launch_bounds__(kStrWarps * 32) k_str_materialize(const StrArg
 					}
 				}
 				uint32_t r = l;
-				uint8_t  chunk[16];
-				for (uint64_t b = lo; b < hi; ++b, ++rb) {
-					while (rb >= s.rel[r + 1]) { ++r; }
-					const uint32_t code = s.rows[r];
-					chunk[b - q * 16]   = dbytes[dict_start(dends, code) + (rb - s.rel[r])];
+				uint32_t w[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+				for (uint32_t j = 0; j < 16; ++j) {
+					const uint64_t b = q * 16 + j;
+					if (b >= lo && b < hi) {
+						const uint32_t rbj = static_cast<uint32_t>(b - b0);
+						while (rbj >= s.rel[r + 1]) { ++r; }
+						const uint32_t code = s.rows[r];
+						w[j / 4] |= static_cast<uint32_t>(dbytes[dict_start(dends, code) + (rbj - s.rel[r])]) << (8 * (j % 4));
+					}
 				}
 				uint8_t* dst = a.bytes + q * 16;
 				if (lo == q * 16 && hi == q * 16 + 16) {
-					uint4 x;
-					memcpy(&x, chunk, 16);
-					*reinterpret_cast<uint4*>(dst) = x;
+					*reinterpret_cast<uint4*>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
 				} else {
-					for (uint64_t b = lo; b < hi; ++b) { dst[b - q * 16] = chunk[b - q * 16]; }
+#pragma unroll
+					for (uint32_t j = 0; j < 16; ++j) {
+						const uint64_t b = q * 16 + j;
+						if (b >= lo && b < hi) { dst[j] = static_cast<uint8_t>(w[j / 4] >> (8 * (j % 4))); }
+					}
 				}
 			}
 		} else {

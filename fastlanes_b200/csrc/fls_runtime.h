@@ -4,6 +4,9 @@
 #include "fls_plan.h"
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <vector>
+
+struct fls_plan; // the opaque plan of include/fls_b200.h
 
 namespace flsgpu {
 
@@ -28,6 +31,10 @@ cudaError_t launch_decode(Family fam, const DecodeArgs& args, cudaStream_t strea
 
 // Geometry of a family (threads per CTA, dynamic shared memory per CTA, CTAs resident per SM).
 void family_geometry(Family fam, int* threads, int* smem, int* ctas_per_sm);
+
+// Build a plan object from descriptors + queue (uploads both; a single column without a queue stays inline).
+int make_plan_object(const std::vector<ColDesc>& descs, const std::vector<uint32_t>& queue, Family fam,
+                     ::fls_plan** out);
 
 // Kernels launched by this library inside the last timed region of a caller (a plain counter; not thread-safe).
 uint64_t& launch_counter();

@@ -56,6 +56,48 @@ def placement(page):
     return s.value
 
 
+_plan_pages = declare("fls_plan_create_pages", ctypes.c_int, [ctypes.POINTER(PageColumn), ctypes.c_uint32,
+                                                                ctypes.POINTER(_p)])
+_plan_decode = declare("fls_plan_decode", ctypes.c_int, [_p, _p])
+_plan_destroy = declare("fls_plan_destroy", ctypes.c_int, [_p])
+
+
+def _columns(columns):
+    arr = (PageColumn * len(columns))()
+    for i, c in enumerate(columns):
+        a = arr[i]
+        a.d_page, a.page_size = c["d_page"], c["page_size"]
+        a.d_dict, a.dict_size = c.get("d_dict"), c.get("dict_size", 0)
+        a.data_type, a.order, a.d_out = c["data_type"], c.get("order", 1), c["d_out"]
+    return arr
+
+
+class PagePlan:
+    """fls_plan_create_pages: page metadata read once; decode() is one kernel launch."""
+
+    def __init__(self, columns):
+        h = _p()
+        check(_plan_pages(_columns(columns), len(columns), ctypes.byref(h)), "fls_plan_create_pages")
+        self.handle = h
+
+    def decode(self, stream=None):
+        import torch
+
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        check(_plan_decode(self.handle, s), "fls_plan_decode")
+
+    def close(self):
+        if self.handle:
+            _plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def decode_pages(columns, stream=None):
     """columns: list of dicts with d_page, page_size, d_dict, dict_size, data_type, order, d_out (device ptrs)."""
     import torch

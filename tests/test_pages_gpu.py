@@ -132,3 +132,29 @@ def test_rle_round_trip_through_the_page_decoder(cuda, dt):
     out = torch.zeros(x.size, dtype=torch.from_numpy(np.zeros(1, T)).dtype, device=cuda)
     pages.decode_pages([dict(d_page=pp, page_size=page.size, data_type=code, order=1, d_out=out.data_ptr())])
     assert np.array_equal(out.cpu().numpy(), x)
+
+
+def test_page_plan_equals_direct_decode(cuda, col_golden):
+    import torch
+
+    from fastlanes_b200 import pages
+
+    keep, cols, wants, outs = [], [], [], []
+    for eid in INT_IDS:
+        page, dic, want = col_golden[f"i64_{eid}_page"], col_golden[f"i64_{eid}_dict"], col_golden[f"i64_{eid}_input"]
+        pbuf, pptr = _dev_bytes(page, cuda, (eid * 7) % 16)
+        dbuf, dptr = _dev_bytes(dic, cuda) if dic.size else (None, None)
+        out = torch.zeros(want.size, dtype=torch.int64, device=cuda)
+        keep += [pbuf, dbuf]
+        outs.append(out)
+        wants.append(want)
+        cols.append(dict(d_page=pptr, page_size=page.size, d_dict=dptr, dict_size=dic.size, data_type=pages.INT64,
+                         order=1, d_out=out.data_ptr()))
+    plan = pages.PagePlan(cols)
+    for _ in range(2):
+        for o in outs:
+            o.zero_()
+        plan.decode()
+        for o, w in zip(outs, wants):
+            assert np.array_equal(o.cpu().numpy(), w)
+    plan.close()
