@@ -161,10 +161,16 @@ int fls_page_info(const uint8_t* page_prefix, uint64_t prefix_size, uint32_t* ex
 	return FLS_OK;
 }
 
-// Descriptors, work queue and kernel family for a set of page columns (reads each page's header from the
-// device).
+// Descriptors, work queue and kernel family for a set of page columns.  Each page's header (and a dictionary's
+// first 20 bytes) is read from the device in stream order on `stream`, so work queued before on that stream
+// (e.g. the copy that brought the page in) is complete when the header is parsed.
+static int read_on(void* dst, const void* src, size_t n, cudaStream_t stream) {
+	if (cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, stream) != cudaSuccess) { return FLS_ERR_CUDA; }
+	return cudaStreamSynchronize(stream) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
+}
+
 static int describe_pages(const fls_page_column* cols, uint32_t n_cols, std::vector<ColDesc>* descs,
-                          std::vector<uint32_t>* queue, Family* fam_out) {
+                          std::vector<uint32_t>* queue, Family* fam_out, cudaStream_t stream) {
 	if (!cols || n_cols == 0 || n_cols > 255) { return FLS_ERR_ARG; }
 	descs->assign(n_cols, ColDesc {});
 	queue->clear();
@@ -177,7 +183,7 @@ static int describe_pages(const fls_page_column* cols, uint32_t n_cols, std::vec
 		if ((reinterpret_cast<uintptr_t>(pc.d_out) & 15u) != 0) { return FLS_ERR_ARG; }
 		uint8_t        hdr[8 + 4 * 8];
 		const uint64_t take = pc.page_size < sizeof(hdr) ? pc.page_size : sizeof(hdr);
-		if (cudaMemcpy(hdr, pc.d_page, take, cudaMemcpyDeviceToHost) != cudaSuccess) { return FLS_ERR_CUDA; }
+		if (read_on(hdr, pc.d_page, take, stream) != FLS_OK) { return FLS_ERR_CUDA; }
 		PageInfo pi;
 		int      rc = parse_page_header(hdr, take, &pi);
 		if (rc == FLS_OK) { rc = finish_page_info(&pi, pc.page_size); }
@@ -187,7 +193,7 @@ static int describe_pages(const fls_page_column* cols, uint32_t n_cols, std::vec
 		if (pi.layout->post == POST_DICT || pi.layout->post == POST_RLE_DICT) {
 			if (!pc.d_dict || pc.dict_size < 20) { return FLS_ERR_FORMAT; }
 			uint8_t dh[20];
-			if (cudaMemcpy(dh, pc.d_dict, 20, cudaMemcpyDeviceToHost) != cudaSuccess) { return FLS_ERR_CUDA; }
+			if (read_on(dh, pc.d_dict, 20, stream) != FLS_OK) { return FLS_ERR_CUDA; }
 			uint64_t voff = 0;
 			rc            = int_dictionary_values(dh, pc.dict_size, w, &voff, &entries);
 			if (rc != FLS_OK) { return rc; }
@@ -209,10 +215,10 @@ int fls_gpu_decode_pages(const fls_page_column* cols, uint32_t n_cols, fls_strea
 	std::vector<ColDesc>  descs;
 	std::vector<uint32_t> queue;
 	Family                fam = Family::NUM;
-	int                   rc  = describe_pages(cols, n_cols, &descs, &queue, &fam);
+	cudaStream_t          s   = static_cast<cudaStream_t>(stream);
+	int                   rc  = describe_pages(cols, n_cols, &descs, &queue, &fam, s);
 	if (rc != FLS_OK) { return rc; }
 	if (queue.empty()) { return FLS_OK; }
-	cudaStream_t s = static_cast<cudaStream_t>(stream);
 	DecodeArgs   a {};
 	if (n_cols == 1) {
 		a.col0    = descs[0];
@@ -241,7 +247,8 @@ int fls_plan_create_pages(const fls_page_column* cols, uint32_t n_cols, fls_plan
 	std::vector<ColDesc>  descs;
 	std::vector<uint32_t> queue;
 	Family                fam = Family::NUM;
-	const int             rc  = describe_pages(cols, n_cols, &descs, &queue, &fam);
+	// headers are read on the legacy default stream: the pages must be in place (e.g. after a device sync)
+	const int rc = describe_pages(cols, n_cols, &descs, &queue, &fam, nullptr);
 	if (rc != FLS_OK) { return rc; }
 	return make_plan_object(descs, queue, fam, out_plan);
 }

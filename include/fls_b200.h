@@ -203,7 +203,9 @@ int fls_page_info(const uint8_t* page_prefix, uint64_t prefix_size, uint32_t* ex
  * 16-byte boundary. */
 int fls_page_placement(const uint8_t* page_prefix, uint64_t prefix_size, uint32_t* shift);
 int fls_gpu_decode_pages(const fls_page_column* cols, uint32_t n_cols, fls_stream_t stream);
-/* The same decode as a plan: page metadata is read once here; fls_plan_decode then only launches.  Replaces
+/* fls_gpu_decode_pages reads each page header in stream order on `stream` (it synchronises that stream once).
+ * The same decode as a plan: page metadata is read once here (on the legacy default stream, so the pages must
+ * already be in place); fls_plan_decode then only launches.  Replaces
  * the reference's per-vector page walk (Page::InitDecompress + page_params, src/cor/lyt/page/page.cpp:63-139). */
 int fls_plan_create_pages(const fls_page_column* cols, uint32_t n_cols, fls_plan** out_plan);
 
