@@ -191,10 +191,11 @@ int fls_string_plan_create(const uint8_t* d_page, uint64_t page_size, const uint
 	}
 	if (cudaMemcpy(p->table.p, &tab, sizeof(tab), cudaMemcpyHostToDevice) != cudaSuccess) { return FLS_ERR_CUDA; }
 	a.table = p->table.p;
-	// shared-memory budget of the materialising kernel: per-warp areas + (dictionary bytes and ends if they fit)
+	// shared-memory budget of the materialising kernel: per-warp areas + the dictionary bytes if they fit (with
+	// a 4-byte word of slack read by the word copies; the end offsets stay in global memory)
 	const uint32_t base     = str_smem_base();
-	const uint64_t dict_sm  = ((a.dict_bytes_n + 15) & ~15ull) + 4ull * a.entry_c;
-	const uint64_t budget   = 220 * 1024;
+	const uint64_t dict_sm  = (a.dict_bytes_n + 4 + 15) & ~15ull;
+	const uint64_t budget   = 224 * 1024;
 	a.dict_in_smem          = a.kind == STR_DICT && base + dict_sm <= budget;
 	p->dyn_smem             = base + (a.dict_in_smem ? static_cast<uint32_t>(dict_sm) : 0u);
 	p->grid                 = dev->sm_count;

@@ -82,89 +82,8 @@ __global__ void __launch_bounds__(1024) k_fsst_dict(const uint8_t* lens, const u
 // ---------------------------------------------------------------------------------------------------------
 // Per-vector building blocks
 // ---------------------------------------------------------------------------------------------------------
-// Warp copy of n bytes global -> shared (16-byte loads when both sides allow it).
-__device__ __forceinline__ void warp_copy(uint8_t* __restrict__ dst, const uint8_t* __restrict__ src, uint32_t n,
-                                          uint32_t lane) {
-	const uintptr_t al = reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst);
-	if ((al & 15u) == 0) {
-#pragma unroll 4
-		for (uint32_t i = lane * 16; i + 16 <= n; i += 512) {
-			*reinterpret_cast<uint4*>(dst + i) = __ldg(reinterpret_cast<const uint4*>(src + i));
-		}
-		for (uint32_t i = (n & ~15u) + lane; i < n; i += 32) { dst[i] = src[i]; }
-	} else if ((al & 3u) == 0) {
-#pragma unroll 8
-		for (uint32_t i = lane * 4; i + 4 <= n; i += 128) {
-			*reinterpret_cast<uint32_t*>(dst + i) = __ldg(reinterpret_cast<const uint32_t*>(src + i));
-		}
-		for (uint32_t i = (n & ~3u) + lane; i < n; i += 32) { dst[i] = src[i]; }
-	} else {
-#pragma unroll 8
-		for (uint32_t i = lane; i < n; i += 32) { dst[i] = __ldg(src + i); }
-	}
-}
-
-// The 1024 codes (DICT / DICT_RLE) or row end offsets (FSST / BYTE_ARR) of vector v, in ORIGINAL order, into
-// rows[1024].  stage: >= 4096 + 128 bytes, gstage: >= 4096 + 32 bytes (RLE run values window).
-__device__ bool load_rows(const ColDesc& c, uint32_t v, uint8_t* stage, uint8_t* gstage, uint32_t* rows,
-                          uint32_t lane, int* status) {
-	const Plan p = make_plan(c, v);
-	if (!p.ok) {
-		if (lane == 0) { atomicOr(status, p.bw > p.ws ? STATUS_BAD_BW : STATUS_BAD_LAYOUT); }
-		return false;
-	}
-	warp_copy(stage, p.src, p.bytes, lane);
-	if (p.post == POST_RLE && p.gbytes) { warp_copy(gstage, p.gsrc, p.gbytes, lane); }
-	__syncwarp();
-	bool bad = false;
-	if (p.ws == 32) {
-		uint32_t x[32];
-		decode_stream<32>(p, reinterpret_cast<const uint32_t*>(stage), lane, x);
-		const uint32_t r0 = run_start<32>(lane, 0);
-#pragma unroll
-		for (int i = 0; i < 32; ++i) { rows[r0 + i] = x[i]; }
-	} else {
-		uint32_t x[32];
-		decode_stream<16>(p, reinterpret_cast<const uint32_t*>(stage), lane, x);
-#pragma unroll
-		for (int r = 0; r < 2; ++r) {
-			const uint32_t r0 = run_start<16>(lane, r);
-#pragma unroll
-			for (int i = 0; i < 16; ++i) {
-				const uint32_t idx = x[16 * r + i];
-				const bool     in  = idx < p.n_runs;
-				bad |= !in;
-				rows[r0 + i] = in ? static_cast<uint32_t>(ld_le(gstage + 4ull * idx, 4)) : 0u;
-			}
-		}
-	}
-	if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) { atomicOr(status, STATUS_BAD_INDEX); }
-	__syncwarp();
-	return true;
-}
-
 __device__ __forceinline__ uint32_t dict_start(const uint32_t* ends, uint32_t code) {
 	return code == 0 ? 0u : ends[code - 1];
-}
-
-// Decoded length of row r of the vector (rows[] holds codes or end offsets in original order).
-__device__ __forceinline__ uint32_t row_len(const StrArgs& a, const uint32_t* rows, uint32_t r, const uint8_t* vbytes,
-                                            uint32_t vbytes_n, const uint8_t* flen, bool* bad) {
-	if (a.kind == STR_DICT) {
-		const uint32_t code = rows[r];
-		if (code >= a.entry_c) {
-			*bad = true;
-			return 0;
-		}
-		return a.dict_ends[code] - dict_start(a.dict_ends, code);
-	}
-	const uint32_t s = r == 0 ? 0u : rows[r - 1];
-	const uint32_t e = rows[r];
-	if (e < s || e > vbytes_n) {
-		*bad = true;
-		return 0;
-	}
-	return a.kind == STR_BYTES ? e - s : fsst_decoded_len(flen, vbytes + s, e - s);
 }
 
 // bytes of vector v's compressed rows (FSST / BYTE_ARR): buffer 0 of the page at the vector's entry point
@@ -177,50 +96,305 @@ __device__ __forceinline__ const uint8_t* vector_bytes(const ColDesc& c, uint32_
 	return *n ? c.buf[0] + o : c.buf[0];
 }
 
-constexpr int kStrWarps = 6;
-constexpr int kStrWarpSmem = 4096 + 128 + 4096 + 32 + 4096 + 4100 + 12; // stage, gstage, rows, rel
-
-struct StrWarpSmem {
-	uint8_t*  stage;
-	uint8_t*  gstage;
-	uint32_t* rows;
-	uint32_t* rel;
-};
-
-__device__ __forceinline__ StrWarpSmem str_warp_smem(uint8_t* base, uint32_t warp) {
-	uint8_t*    w = base + warp * ((kStrWarpSmem + 15) & ~15);
-	StrWarpSmem s;
-	s.stage  = w;
-	s.gstage = w + 4096 + 128;
-	s.rows   = reinterpret_cast<uint32_t*>(w + 4096 + 128 + 4096 + 32);
-	s.rel    = reinterpret_cast<uint32_t*>(w + 4096 + 128 + 4096 + 32 + 4096);
-	return s;
+// Copy n bytes from src to dst, any alignment of either.  The body moves 4-byte words (funnel shifts of two
+// aligned source words), so the source must stay readable up to the 4-byte word after src + n.
+__device__ __forceinline__ void copy_row(uint8_t* __restrict__ dst, const uint8_t* __restrict__ src, uint32_t n) {
+	uint32_t h = (4u - static_cast<uint32_t>(reinterpret_cast<uintptr_t>(dst) & 3u)) & 3u;
+	h          = h < n ? h : n;
+	for (uint32_t i = 0; i < h; ++i) { dst[i] = src[i]; }
+	dst += h, src += h, n -= h;
+	const uint32_t  sh = 8u * static_cast<uint32_t>(reinterpret_cast<uintptr_t>(src) & 3u);
+	const uint32_t* s  = reinterpret_cast<const uint32_t*>(reinterpret_cast<uintptr_t>(src) & ~uintptr_t(3));
+	uint32_t*       d  = reinterpret_cast<uint32_t*>(dst);
+	const uint32_t  nw = n >> 2;
+	if (nw) {
+		uint32_t w0 = s[0];
+		for (uint32_t i = 0; i < nw; ++i) {
+			const uint32_t w1 = s[i + 1];
+			d[i]              = __funnelshift_r(w0, w1, sh);
+			w0                = w1;
+		}
+	}
+	for (uint32_t i = nw << 2; i < n; ++i) { dst[i] = src[i]; }
 }
 
-__global__ void __launch_bounds__(kStrWarps * 32) k_str_lengths(const StrArgs a) {
+// ---------------------------------------------------------------------------------------------------------
+// Per-warp shared memory of the string kernels
+//   bars    two mbarriers, one per slot
+//   plans   ring of 2 x kStrPB plans (64 B each) of the warp's next vectors, fetched lane-parallel
+//   slot[2] packed codes / end offsets of a vector (TMA) and its lane bases; once decoded, the vector's
+//           1024 codes / end offsets in original order (row r at word r + r / 32: conflict-free both by run
+//           and by row)
+//   window  (materialize only) 4 KB of output bytes starting at a 16-byte aligned output position
+// ---------------------------------------------------------------------------------------------------------
+constexpr int      kStrWarps  = 8;
+constexpr uint32_t kStrPB     = 8;
+constexpr uint32_t kStrStage  = 4096 + 128; // >= 1055 padded row words
+constexpr uint32_t kStrSlot   = kStrStage + kLaneWindow;
+constexpr uint32_t kStrWindow = 4096;
+constexpr uint32_t kStrHead   = 16 + 2 * kStrPB * 64;
+
+enum : int { STR_PASS_LENGTHS = 0, STR_PASS_MATERIALIZE = 1 };
+
+template <int PASS>
+__host__ __device__ constexpr uint32_t str_per_warp() {
+	return kStrHead + 2 * kStrSlot + (PASS == STR_PASS_MATERIALIZE ? kStrWindow : 0u);
+}
+
+__device__ __forceinline__ uint32_t row_word(uint32_t r) { return r + (r >> 5); }
+
+// Codes (or end offsets) of the staged vector, decoded in registers, then written over the stage in original
+// order.  DICT_RLE run values are read from the page directly.
+__device__ __forceinline__ void stage_to_rows(const Plan& p, uint8_t* slot, uint32_t lane, int* status) {
+	uint32_t* rows = reinterpret_cast<uint32_t*>(slot);
+	uint32_t  x[32];
+	bool      bad = false;
+	if (p.ws == 32) {
+		decode_stream<32>(p, reinterpret_cast<const uint32_t*>(slot), lane, x);
+		__syncwarp();
+		const uint32_t r0 = row_word(run_start<32>(lane, 0));
+#pragma unroll
+		for (int i = 0; i < 32; ++i) { rows[r0 + i] = x[i]; }
+	} else {
+		decode_stream<16>(p, reinterpret_cast<const uint32_t*>(slot), lane, x);
+#pragma unroll
+		for (int i = 0; i < 32; ++i) {
+			const bool in = x[i] < p.n_runs;
+			bad |= !in;
+			x[i] = in ? static_cast<uint32_t>(ld_le(p.gsrc + 4ull * x[i], 4)) : 0u;
+		}
+		__syncwarp();
+#pragma unroll
+		for (int r = 0; r < 2; ++r) {
+			const uint32_t r0 = row_word(run_start<16>(lane, r));
+#pragma unroll
+			for (int i = 0; i < 16; ++i) { rows[r0 + i] = x[16 * r + i]; }
+		}
+	}
+	if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) { atomicOr(status, STATUS_BAD_INDEX); }
+	__syncwarp();
+}
+
+// Row 32 * b + lane: its source (dictionary entry or compressed bytes) and decoded length.
+struct RowRef {
+	uint32_t start; // dictionary byte offset (DICT) or compressed byte offset within the vector
+	uint32_t clen;  // compressed length (FSST / BYTE_ARR)
+	uint32_t len;   // decoded length
+};
+
+__device__ __forceinline__ RowRef row_ref(const StrArgs& a, const uint32_t* ends, const uint32_t* rows, uint32_t r,
+                                          const uint8_t* vb, uint32_t vn, const uint8_t* flen, bool* bad) {
+	RowRef f {0, 0, 0};
+	if (a.kind == STR_DICT) {
+		const uint32_t code = rows[row_word(r)];
+		if (code >= a.entry_c) {
+			*bad = true;
+			return f;
+		}
+		f.start = code ? __ldg(ends + code - 1) : 0u;
+		f.len   = __ldg(ends + code) - f.start;
+		return f;
+	}
+	const uint32_t s = r == 0 ? 0u : rows[row_word(r - 1)];
+	const uint32_t e = rows[row_word(r)];
+	if (e < s || e > vn) {
+		*bad = true;
+		return f;
+	}
+	f.start = s;
+	f.clen  = e - s;
+	f.len   = a.kind == STR_BYTES ? f.clen : fsst_decoded_len(flen, vb + s, f.clen);
+	return f;
+}
+
+template <int PASS>
+__global__ void __launch_bounds__(kStrWarps * 32) k_str_pass(const StrArgs a) {
 	extern __shared__ __align__(128) uint8_t smem[];
-	__shared__ uint8_t flen[256];
+	__shared__ uint64_t fsym[256];
+	__shared__ uint8_t  flen[256];
+	const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+	constexpr uint32_t kPerWarp = str_per_warp<PASS>();
+	// decoded dictionary bytes into shared memory when the plan found room for them (the end offsets are read
+	// through the L1 cache)
+	const uint8_t* dbytes = a.dict_bytes;
+	if (PASS == STR_PASS_MATERIALIZE && a.kind == STR_DICT && a.dict_in_smem) {
+		uint8_t* db = smem + kStrWarps * kPerWarp;
+		// the decoded dictionary lives in a cudaMalloc'd (256-byte aligned) buffer with at least 16 bytes of
+		// slack after the last entry
+		const uint32_t nb16 = static_cast<uint32_t>((a.dict_bytes_n + 15) / 16);
+		for (uint32_t i = threadIdx.x; i < nb16; i += blockDim.x) {
+			reinterpret_cast<uint4*>(db)[i] = __ldg(reinterpret_cast<const uint4*>(a.dict_bytes) + i);
+		}
+		dbytes = db;
+	}
 	if (a.kind == STR_FSST) {
-		for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) { flen[i] = a.table->len[i]; }
+		for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) {
+			fsym[i] = a.table->sym[i];
+			flen[i] = a.table->len[i];
+		}
+	}
+	uint8_t*  wbase = smem + warp * kPerWarp;
+	uint64_t* bars  = reinterpret_cast<uint64_t*>(wbase);
+	PlanS*    plans = reinterpret_cast<PlanS*>(wbase + 16);
+	uint8_t*  slots = wbase + kStrHead;
+	uint8_t*  win   = slots + 2 * kStrSlot;
+	if (lane == 0) {
+		mbar_init(&bars[0], 1);
+		mbar_init(&bars[1], 1);
+		fence_mbar_init();
 	}
 	__syncthreads();
-	const uint32_t    lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-	const StrWarpSmem s    = str_warp_smem(smem, warp);
-	const uint64_t    nw   = static_cast<uint64_t>(gridDim.x) * kStrWarps;
-	for (uint64_t v = static_cast<uint64_t>(blockIdx.x) * kStrWarps + warp; v < a.col.n_vec; v += nw) {
-		if (!load_rows(a.col, static_cast<uint32_t>(v), s.stage, s.gstage, s.rows, lane, a.status)) {
-			if (lane == 0) { a.vec_total[v] = 0; }
+
+	const uint64_t gw = static_cast<uint64_t>(blockIdx.x) * kStrWarps + warp;
+	const uint64_t nw = static_cast<uint64_t>(gridDim.x) * kStrWarps;
+	const uint64_t n  = a.col.n_vec;
+	auto fetch_plans = [&](uint32_t blk) {
+		if (lane < kStrPB) {
+			const uint64_t k     = static_cast<uint64_t>(blk) * kStrPB + lane;
+			const uint64_t v     = gw + k * nw;
+			Plan           p {};
+			const bool     valid = v < n;
+			if (valid) { p = make_plan(a.col, static_cast<uint32_t>(v)); }
+			plans[k % (2 * kStrPB)] = pack_plan(p, valid);
+		}
+	};
+	auto issue_k = [&](uint64_t k) {
+		const PlanS& ps = plans[k % (2 * kStrPB)];
+		if (ps.flags & 4u) {
+			uint8_t* sl = slots + (k & 1) * kStrSlot;
+			issue<0>(unpack_plan(ps), sl, nullptr, sl + kStrStage, &bars[k & 1], lane);
+		}
+	};
+	fetch_plans(0);
+	fetch_plans(1);
+	__syncwarp();
+	issue_k(0);
+	issue_k(1);
+
+	uint32_t k = 0;
+	for (uint64_t v = gw; v < n; v += nw, ++k) {
+		if (k % kStrPB == 0 && k > 0) {
+			fetch_plans(k / kStrPB + 1);
+			__syncwarp();
+		}
+		uint8_t* sl = slots + (k & 1) * kStrSlot;
+		Plan     p  = unpack_plan(plans[k % (2 * kStrPB)]);
+		if (!mbar_wait(&bars[k & 1], (k >> 1) & 1u)) {
+			if (lane == 0) { atomicOr(a.status, STATUS_TIMEOUT); }
+			// the other slot may still have a copy in flight: wait for it (bounded) before leaving
+			if (gw + static_cast<uint64_t>(k + 1) * nw < n) { (void)mbar_wait(&bars[(k + 1) & 1], ((k + 1) >> 1) & 1u); }
+			return;
+		}
+		if (!p.ok) {
+			if (lane == 0) {
+				atomicOr(a.status, p.bw > p.ws ? STATUS_BAD_BW : STATUS_BAD_LAYOUT);
+				if (PASS == STR_PASS_LENGTHS) { a.vec_total[v] = 0; }
+			}
+			__syncwarp();
+			issue_k(k + 2);
 			continue;
 		}
-		uint32_t       vn = 0;
-		const uint8_t* vb = a.kind == STR_DICT ? nullptr : vector_bytes(a.col, static_cast<uint32_t>(v), &vn);
-		bool           bad = false;
-		uint64_t       sum = 0;
-		for (uint32_t r = lane; r < kVec; r += 32) { sum += row_len(a, s.rows, r, vb, vn, flen, &bad); }
-		sum = warp_sum(sum);
+		if (p.lane_bases) { p.lane_bases = sl + kStrStage + (reinterpret_cast<uintptr_t>(p.lane_bases) & 15u); }
+		stage_to_rows(p, sl, lane, a.status);
+		const uint32_t* rows = reinterpret_cast<const uint32_t*>(sl);
+		uint32_t        vn   = 0;
+		const uint8_t*  vb   = a.kind == STR_DICT ? nullptr : vector_bytes(a.col, static_cast<uint32_t>(v), &vn);
+		bool            bad  = false;
+		if (PASS == STR_PASS_LENGTHS) {
+			uint32_t sum = 0;
+			for (uint32_t b = 0; b < kVec / 32; ++b) {
+				sum += row_ref(a, a.dict_ends, rows, 32 * b + lane, vb, vn, flen, &bad).len;
+			}
+			sum = warp_sum(sum);
+			if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) { atomicOr(a.status, STATUS_BAD_INDEX); }
+			if (lane == 0) { a.vec_total[v] = sum; }
+			__syncwarp();
+			issue_k(k + 2);
+			continue;
+		}
+		const uint64_t vbase = a.vec_base[v];
+		const uint64_t vend  = a.vec_base[v + 1];
+		if (vend < vbase || vend > a.bytes_cap) {
+			if (lane == 0) { atomicOr(a.status, STATUS_BAD_LAYOUT); }
+			__syncwarp();
+			issue_k(k + 2);
+			continue;
+		}
+		// Rows go to the window in batches of 32 (one row per lane, positions from a warp scan of the lengths);
+		// full 16-byte chunks of the window go out with 16-byte stores, the vector's first and last partial
+		// chunks byte by byte (the neighbouring vectors write the other bytes of those chunks).
+		uint64_t W    = vbase & ~15ull;          // output position of win[0]
+		uint32_t fill = static_cast<uint32_t>(vbase & 15u);
+		uint64_t lo   = vbase;                   // first output byte the window may write
+		auto flush = [&](bool all) {
+			const uint32_t full = fill & ~15u;
+			const uint32_t upto = all ? fill : full;
+			for (uint32_t c = 16 * lane; c < upto; c += 512) {
+				const uint64_t g = W + c;
+				if (g >= lo && c + 16 <= upto) {
+					*reinterpret_cast<uint4*>(a.bytes + g) = *reinterpret_cast<const uint4*>(win + c);
+				} else {
+					for (uint32_t i = 0; i < 16 && c + i < upto; ++i) {
+						if (g + i >= lo) { a.bytes[g + i] = win[c + i]; }
+					}
+				}
+			}
+			__syncwarp();
+			if (!all) {
+				const uint8_t t = lane < (fill & 15u) ? win[full + lane] : 0;
+				__syncwarp();
+				if (lane < (fill & 15u)) { win[lane] = t; }
+				__syncwarp();
+				W += full;
+				fill &= 15u;
+				lo = lo > W ? lo : W;
+			}
+		};
+		uint32_t vpos = 0; // bytes of this vector emitted so far
+		for (uint32_t b = 0; b < kVec / 32; ++b) {
+			const uint32_t r   = 32 * b + lane;
+			const RowRef   f   = row_ref(a, a.dict_ends, rows, r, vb, vn, flen, &bad);
+			const uint32_t inc = warp_inclusive_scan(f.len, lane);
+			const uint32_t o   = vpos + inc - f.len;
+			const uint32_t T   = __shfl_sync(0xFFFFFFFFu, inc, 31);
+			a.offsets[v * kVec + r] = static_cast<uint32_t>(vbase + o);
+			if (fill + T > kStrWindow) { flush(false); }
+			if (fill + T <= kStrWindow) {
+				uint8_t* dst = win + fill + (o - vpos);
+				if (a.kind == STR_DICT) {
+					copy_row(dst, dbytes + f.start, f.len);
+				} else if (a.kind == STR_BYTES) {
+					copy_row(dst, vb + f.start, f.len);
+				} else {
+					fsst_decode_to(fsym, flen, vb + f.start, f.clen, dst);
+				}
+				fill += T;
+			} else {
+				// a batch larger than the window: its rows go straight to global memory, after the window's
+				// pending bytes
+				flush(true);
+				uint8_t* dst = a.bytes + vbase + o;
+				if (a.kind == STR_DICT) {
+					for (uint32_t i = 0; i < f.len; ++i) { dst[i] = dbytes[f.start + i]; }
+				} else if (a.kind == STR_BYTES) {
+					for (uint32_t i = 0; i < f.len; ++i) { dst[i] = vb[f.start + i]; }
+				} else {
+					fsst_decode_to(fsym, flen, vb + f.start, f.clen, dst);
+				}
+				const uint64_t pos = vbase + vpos + T;
+				W    = pos & ~15ull;
+				fill = static_cast<uint32_t>(pos & 15u);
+				lo   = pos;
+			}
+			vpos += T;
+			__syncwarp();
+		}
+		flush(true);
+		if (lane == 0 && v + 1 == n) { a.offsets[n * kVec] = static_cast<uint32_t>(vbase + vpos); }
+		if (vbase + vpos != vend) { bad = true; }
 		if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) { atomicOr(a.status, STATUS_BAD_INDEX); }
-		if (lane == 0) { a.vec_total[v] = sum; }
 		__syncwarp();
+		issue_k(k + 2);
 	}
 }
 
@@ -238,133 +412,10 @@ __global__ void __launch_bounds__(1024) k_scan_totals(const uint64_t* total, uin
 	if (threadIdx.x == 0) { base[n] = carry; }
 }
 
-__global__ void __launch_bounds__(kStrWarps * 32) k_str_materialize(const StrArgs a) {
-	extern __shared__ __align__(128) uint8_t smem[];
-	__shared__ uint64_t fsym[256];
-	__shared__ uint8_t  flen[256];
-	const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-	uint8_t*       dict_smem = smem + kStrWarps * ((kStrWarpSmem + 15) & ~15);
-	// dictionary (bytes, then end offsets) into shared memory when the plan found room for it
-	const uint8_t*  dbytes = a.dict_bytes;
-	const uint32_t* dends  = a.dict_ends;
-	if (a.kind == STR_DICT && a.dict_in_smem) {
-		uint8_t* db = dict_smem;
-		uint32_t* de = reinterpret_cast<uint32_t*>(dict_smem + ((a.dict_bytes_n + 15) & ~15ull));
-		// the decoded dictionary lives in cudaMalloc'd (256-byte aligned) plan buffers
-		const uint32_t nb16 = static_cast<uint32_t>((a.dict_bytes_n + 15) / 16);
-		for (uint32_t i = threadIdx.x; i < nb16; i += blockDim.x) {
-			reinterpret_cast<uint4*>(db)[i] = __ldg(reinterpret_cast<const uint4*>(a.dict_bytes) + i);
-		}
-		for (uint32_t i = threadIdx.x; i < a.entry_c; i += blockDim.x) { de[i] = __ldg(a.dict_ends + i); }
-		dbytes = db;
-		dends  = de;
-	}
-	if (a.kind == STR_FSST) {
-		for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) {
-			fsym[i] = a.table->sym[i];
-			flen[i] = a.table->len[i];
-		}
-	}
-	__syncthreads();
-	StrArgs la = a;
-	la.dict_ends = dends;
-	const StrWarpSmem s  = str_warp_smem(smem, warp);
-	const uint64_t    nw = static_cast<uint64_t>(gridDim.x) * kStrWarps;
-	for (uint64_t v = static_cast<uint64_t>(blockIdx.x) * kStrWarps + warp; v < a.col.n_vec; v += nw) {
-		const uint64_t vbase = a.vec_base[v];
-		if (!load_rows(a.col, static_cast<uint32_t>(v), s.stage, s.gstage, s.rows, lane, a.status)) { continue; }
-		uint32_t       vn = 0;
-		const uint8_t* vb = a.kind == STR_DICT ? nullptr : vector_bytes(a.col, static_cast<uint32_t>(v), &vn);
-		// row lengths of rows 32*lane .. 32*lane+31 (contiguous), local exclusive prefix, warp scan
-		bool     bad = false;
-		uint32_t run = 0;
-		for (uint32_t i = 0; i < 32; ++i) {
-			const uint32_t r = 32 * lane + i;
-			s.rel[r]         = run;
-			run += row_len(la, s.rows, r, vb, vn, flen, &bad);
-		}
-		const uint32_t inc = warp_inclusive_scan(run, lane);
-		const uint32_t exc = inc - run;
-		for (uint32_t i = 0; i < 32; ++i) { s.rel[32 * lane + i] += exc; }
-		if (lane == 31) { s.rel[kVec] = inc; }
-		if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) { atomicOr(a.status, STATUS_BAD_INDEX); }
-		__syncwarp();
-		// Arrow offsets (u32) of the vector's rows, coalesced
-		for (uint32_t r = lane; r < kVec; r += 32) {
-			a.offsets[v * kVec + r] = static_cast<uint32_t>(vbase + s.rel[r]);
-		}
-		const uint32_t total = s.rel[kVec];
-		if (v + 1 == a.col.n_vec && lane == 0) { a.offsets[(v + 1) * kVec] = static_cast<uint32_t>(vbase + total); }
-		if (vbase + total > a.bytes_cap) {
-			if (lane == 0) { atomicOr(a.status, STATUS_BAD_LAYOUT); }
-			__syncwarp();
-			continue;
-		}
-		if (a.kind == STR_DICT) {
-			// 16-byte output chunks aligned in the output buffer; chunks shared with the neighbouring vectors are
-			// written bytewise, the others with one 16-byte store
-			const uint64_t b0 = vbase, b1 = vbase + total;
-			const uint64_t q0 = b0 >> 4, q1 = (b1 + 15) >> 4;
-			for (uint64_t q = q0 + lane; q < q1; q += 32) {
-				const uint64_t lo = q * 16 > b0 ? q * 16 : b0;
-				const uint64_t hi = q * 16 + 16 < b1 ? q * 16 + 16 : b1;
-				uint32_t       rb = static_cast<uint32_t>(lo - b0);
-				// last row whose start <= rb (skips empty rows)
-				uint32_t l = 0, h = kVec;
-				while (h - l > 1) {
-					const uint32_t m = (l + h) >> 1;
-					if (s.rel[m] <= rb) {
-						l = m;
-					} else {
-						h = m;
-					}
-				}
-				uint32_t r = l;
-				uint32_t w[4] = {0u, 0u, 0u, 0u};
-#pragma unroll
-				for (uint32_t j = 0; j < 16; ++j) {
-					const uint64_t b = q * 16 + j;
-					if (b >= lo && b < hi) {
-						const uint32_t rbj = static_cast<uint32_t>(b - b0);
-						while (rbj >= s.rel[r + 1]) { ++r; }
-						const uint32_t code = s.rows[r];
-						w[j / 4] |= static_cast<uint32_t>(dbytes[dict_start(dends, code) + (rbj - s.rel[r])]) << (8 * (j % 4));
-					}
-				}
-				uint8_t* dst = a.bytes + q * 16;
-				if (lo == q * 16 && hi == q * 16 + 16) {
-					*reinterpret_cast<uint4*>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
-				} else {
-#pragma unroll
-					for (uint32_t j = 0; j < 16; ++j) {
-						const uint64_t b = q * 16 + j;
-						if (b >= lo && b < hi) { dst[j] = static_cast<uint8_t>(w[j / 4] >> (8 * (j % 4))); }
-					}
-				}
-			}
-		} else {
-			// FSST / BYTE_ARR: every lane decodes its 32 consecutive rows in place
-			for (uint32_t i = 0; i < 32; ++i) {
-				const uint32_t r  = 32 * lane + i;
-				const uint32_t st = r == 0 ? 0u : s.rows[r - 1];
-				const uint32_t en = s.rows[r];
-				if (en < st || en > vn) { continue; }
-				uint8_t* dst = a.bytes + vbase + s.rel[r];
-				if (a.kind == STR_BYTES) {
-					for (uint32_t b = 0; b < en - st; ++b) { dst[b] = vb[st + b]; }
-				} else {
-					fsst_decode_to(fsym, flen, vb + st, en - st, dst);
-				}
-			}
-		}
-		__syncwarp();
-	}
-}
-
 // ---------------------------------------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------------------------------------
-uint32_t str_smem_base() { return kStrWarps * ((kStrWarpSmem + 15) & ~15) + 64; }
+uint32_t str_smem_base() { return kStrWarps * str_per_warp<STR_PASS_MATERIALIZE>(); }
 
 cudaError_t launch_fsst_dict(const uint8_t* lens, const uint8_t* comp, uint64_t comp_size, uint32_t entry_c,
                              const FsstTable* tab, uint32_t* ends, uint8_t* bytes, uint64_t cap, int* status,
@@ -375,16 +426,38 @@ cudaError_t launch_fsst_dict(const uint8_t* lens, const uint8_t* comp, uint64_t 
 	return cudaGetLastError();
 }
 
-cudaError_t launch_str_lengths(const StrArgs& a, int grid, cudaStream_t s) {
-	const uint32_t smem = kStrWarps * ((kStrWarpSmem + 15) & ~15);
-	static bool    set  = false;
-	if (!set) {
-		cudaFuncSetAttribute(k_str_lengths, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-		set = true;
+// Launch one pass over the column's vectors: every SM holds as many CTAs as its shared memory allows, and no
+// more CTAs than there are vectors for their warps.
+template <int PASS>
+static cudaError_t launch_str_pass(const StrArgs& a, uint32_t dyn_smem, cudaStream_t s) {
+	static std::mutex mu;
+	static uint32_t   set = 0;
+	{
+		std::lock_guard<std::mutex> lk(mu);
+		if (dyn_smem > set) {
+			const cudaError_t e =
+			    cudaFuncSetAttribute(k_str_pass<PASS>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_smem);
+			if (e != cudaSuccess) { return e; }
+			set = dyn_smem;
+		}
 	}
-	k_str_lengths<<<grid, kStrWarps * 32, smem, s>>>(a);
+	Device* dev = current_device();
+	if (!dev) { return cudaErrorUnknown; }
+	int per_sm = 0;
+	cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_str_pass<PASS>, kStrWarps * 32, dyn_smem);
+	if (e != cudaSuccess) { return e; }
+	if (per_sm < 1) { return cudaErrorInvalidConfiguration; }
+	const uint64_t need = (a.col.n_vec + kStrWarps - 1) / kStrWarps;
+	uint64_t       grid = static_cast<uint64_t>(dev->sm_count) * per_sm;
+	grid                = grid < need ? grid : need;
+	if (grid == 0) { return cudaSuccess; }
+	k_str_pass<PASS><<<static_cast<unsigned>(grid), kStrWarps * 32, dyn_smem, s>>>(a);
 	++launch_counter();
 	return cudaGetLastError();
+}
+
+cudaError_t launch_str_lengths(const StrArgs& a, int /*grid*/, cudaStream_t s) {
+	return launch_str_pass<STR_PASS_LENGTHS>(a, kStrWarps * str_per_warp<STR_PASS_LENGTHS>(), s);
 }
 
 cudaError_t launch_scan_totals(const uint64_t* total, uint64_t* base, uint64_t n, cudaStream_t s) {
@@ -393,16 +466,8 @@ cudaError_t launch_scan_totals(const uint64_t* total, uint64_t* base, uint64_t n
 	return cudaGetLastError();
 }
 
-cudaError_t launch_str_materialize(const StrArgs& a, int grid, uint32_t dyn_smem, cudaStream_t s) {
-	static uint32_t set = 0;
-	if (dyn_smem > set) {
-		cudaError_t e = cudaFuncSetAttribute(k_str_materialize, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_smem);
-		if (e != cudaSuccess) { return e; }
-		set = dyn_smem;
-	}
-	k_str_materialize<<<grid, kStrWarps * 32, dyn_smem, s>>>(a);
-	++launch_counter();
-	return cudaGetLastError();
+cudaError_t launch_str_materialize(const StrArgs& a, int /*grid*/, uint32_t dyn_smem, cudaStream_t s) {
+	return launch_str_pass<STR_PASS_MATERIALIZE>(a, dyn_smem, s);
 }
 
 } // namespace flsgpu
