@@ -101,7 +101,7 @@ struct fls_string_plan {
 	DevArr<uint64_t>         vec_total;
 	DevArr<uint64_t>         vec_base;
 	uint32_t                 dyn_smem = 0;
-	int                      grid     = 0;
+	int                      warps    = 0; // warps per CTA of the materialising kernel
 	uint64_t                 n_rows   = 0;
 };
 
@@ -191,14 +191,22 @@ int fls_string_plan_create(const uint8_t* d_page, uint64_t page_size, const uint
 	}
 	if (cudaMemcpy(p->table.p, &tab, sizeof(tab), cudaMemcpyHostToDevice) != cudaSuccess) { return FLS_ERR_CUDA; }
 	a.table = p->table.p;
-	// shared-memory budget of the materialising kernel: per-warp areas + the dictionary bytes if they fit (with
-	// a 4-byte word of slack read by the word copies; the end offsets stay in global memory)
-	const uint32_t base     = str_smem_base();
+	// shared memory of the materialising kernel: per-warp areas + the dictionary bytes (with a 4-byte word of
+	// slack read by the word copies; the end offsets stay in global memory) when at least 8 warps still fit
+	// beside them
+	const uint32_t per_warp = str_smem_per_warp();
 	const uint64_t dict_sm  = (a.dict_bytes_n + 4 + 15) & ~15ull;
 	const uint64_t budget   = 224 * 1024;
-	a.dict_in_smem          = a.kind == STR_DICT && base + dict_sm <= budget;
-	p->dyn_smem             = base + (a.dict_in_smem ? static_cast<uint32_t>(dict_sm) : 0u);
-	p->grid                 = dev->sm_count;
+	p->warps                = kStrMaxWarps;
+	a.dict_in_smem          = false;
+	if (a.kind == STR_DICT && dict_sm < budget) {
+		const uint64_t w = (budget - dict_sm) / per_warp;
+		if (w >= 8) {
+			a.dict_in_smem = true;
+			p->warps       = static_cast<int>(w < kStrMaxWarps ? w : kStrMaxWarps);
+		}
+	}
+	p->dyn_smem = p->warps * per_warp + (a.dict_in_smem ? static_cast<uint32_t>(dict_sm) : 0u);
 	*out                    = p.release();
 	return FLS_OK;
 }
@@ -211,7 +219,7 @@ int fls_string_plan_rows(const fls_string_plan* p, uint64_t* n_rows) {
 
 static int run_totals(const fls_string_plan* p, cudaStream_t s) {
 	if (p->args.col.n_vec == 0) { return FLS_OK; }
-	if (launch_str_lengths(p->args, p->grid, s) != cudaSuccess) { return FLS_ERR_CUDA; }
+	if (launch_str_lengths(p->args, 0, s) != cudaSuccess) { return FLS_ERR_CUDA; }
 	if (launch_scan_totals(p->vec_total.p, p->vec_base.p, p->args.col.n_vec, s) != cudaSuccess) { return FLS_ERR_CUDA; }
 	return FLS_OK;
 }
@@ -243,7 +251,7 @@ int fls_string_plan_decode(const fls_string_plan* p, uint32_t* d_offsets, uint8_
 	a.offsets   = d_offsets;
 	a.bytes     = d_bytes;
 	a.bytes_cap = bytes_cap;
-	return launch_str_materialize(a, p->grid, p->dyn_smem, s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
+	return launch_str_materialize(a, p->warps, p->dyn_smem, s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
 }
 
 int fls_string_plan_destroy(fls_string_plan* p) {

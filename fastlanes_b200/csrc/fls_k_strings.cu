@@ -97,66 +97,83 @@ __device__ __forceinline__ const uint8_t* vector_bytes(const ColDesc& c, uint32_
 }
 
 // Copy n bytes from src to dst, any alignment of either.  The body moves 4-byte words (funnel shifts of two
-// aligned source words), so the source must stay readable up to the 4-byte word after src + n.
+// aligned source words), so the source must stay readable up to the 4-byte word after src + n; the at most
+// three bytes before and after the body are predicated stores.
 __device__ __forceinline__ void copy_row(uint8_t* __restrict__ dst, const uint8_t* __restrict__ src, uint32_t n) {
 	uint32_t h = (4u - static_cast<uint32_t>(reinterpret_cast<uintptr_t>(dst) & 3u)) & 3u;
 	h          = h < n ? h : n;
-	for (uint32_t i = 0; i < h; ++i) { dst[i] = src[i]; }
+#pragma unroll
+	for (uint32_t i = 0; i < 3; ++i) {
+		if (i < h) { dst[i] = src[i]; }
+	}
 	dst += h, src += h, n -= h;
 	const uint32_t  sh = 8u * static_cast<uint32_t>(reinterpret_cast<uintptr_t>(src) & 3u);
 	const uint32_t* s  = reinterpret_cast<const uint32_t*>(reinterpret_cast<uintptr_t>(src) & ~uintptr_t(3));
 	uint32_t*       d  = reinterpret_cast<uint32_t*>(dst);
 	const uint32_t  nw = n >> 2;
-	if (nw) {
-		uint32_t w0 = s[0];
-		for (uint32_t i = 0; i < nw; ++i) {
-			const uint32_t w1 = s[i + 1];
-			d[i]              = __funnelshift_r(w0, w1, sh);
-			w0                = w1;
-		}
+	uint32_t        w0 = s[0];
+	for (uint32_t i = 0; i < nw; ++i) {
+		const uint32_t w1 = s[i + 1];
+		d[i]              = __funnelshift_r(w0, w1, sh);
+		w0                = w1;
 	}
-	for (uint32_t i = nw << 2; i < n; ++i) { dst[i] = src[i]; }
+	const uint32_t t = n & 3u;
+	dst += 4 * nw, src += 4 * nw;
+#pragma unroll
+	for (uint32_t i = 0; i < 3; ++i) {
+		if (i < t) { dst[i] = src[i]; }
+	}
 }
 
 // ---------------------------------------------------------------------------------------------------------
-// Per-warp shared memory of the string kernels
-//   bars    two mbarriers, one per slot
-//   plans   ring of 2 x kStrPB plans (64 B each) of the warp's next vectors, fetched lane-parallel
-//   slot[2] packed codes / end offsets of a vector (TMA) and its lane bases; once decoded, the vector's
-//           1024 codes / end offsets in original order (row r at word r + r / 32: conflict-free both by run
-//           and by row)
+// Per-warp shared memory of the string kernels (warps per CTA chosen at launch)
+//   plans   the next kStrPB plans (64 B each) of the warp's vectors, fetched lane-parallel
+//   rows    the vector's packed codes / end offsets (copied in, with 128 bytes of slack for the extraction),
+//           then, once decoded, its 1024 codes / end offsets in original order (row r at word r + r / 32:
+//           conflict-free both by run and by row)
 //   window  (materialize only) 4 KB of output bytes starting at a 16-byte aligned output position
+// The work per vector (1024 row copies) is long next to the latency of its loads, so the packed words are
+// read synchronously: occupancy, not prefetch depth, is what hides latency here.
 // ---------------------------------------------------------------------------------------------------------
-constexpr int      kStrWarps  = 8;
-constexpr uint32_t kStrPB     = 8;
-constexpr uint32_t kStrStage  = 4096 + 128; // >= 1055 padded row words
-constexpr uint32_t kStrSlot   = kStrStage + kLaneWindow;
-constexpr uint32_t kStrWindow = 4096;
-constexpr uint32_t kStrHead   = 16 + 2 * kStrPB * 64;
+constexpr uint32_t kStrPB      = 8;
+constexpr uint32_t kStrRows    = 4096 + 128; // >= 1055 padded row words, >= 128 * (32 + 1) staged bytes
+constexpr uint32_t kStrWindow  = 4096;
 
 enum : int { STR_PASS_LENGTHS = 0, STR_PASS_MATERIALIZE = 1 };
 
-template <int PASS>
-__host__ __device__ constexpr uint32_t str_per_warp() {
-	return kStrHead + 2 * kStrSlot + (PASS == STR_PASS_MATERIALIZE ? kStrWindow : 0u);
+__host__ __device__ constexpr uint32_t str_per_warp(int pass) {
+	return kStrPB * 64 + kStrRows + (pass == STR_PASS_MATERIALIZE ? kStrWindow : 0u);
 }
 
 __device__ __forceinline__ uint32_t row_word(uint32_t r) { return r + (r >> 5); }
 
-// Codes (or end offsets) of the staged vector, decoded in registers, then written over the stage in original
-// order.  DICT_RLE run values are read from the page directly.
-__device__ __forceinline__ void stage_to_rows(const Plan& p, uint8_t* slot, uint32_t lane, int* status) {
-	uint32_t* rows = reinterpret_cast<uint32_t*>(slot);
+// Codes (or end offsets) of the vector into rows[] in original order.  DICT_RLE run values are read from the
+// page directly.
+__device__ __forceinline__ void load_rows(const Plan& p, uint8_t* buf, uint32_t lane, int* status) {
+	const uintptr_t al = reinterpret_cast<uintptr_t>(p.src);
+	if ((al & 15u) == 0) {
+		const uint4* s = reinterpret_cast<const uint4*>(p.src);
+		uint4*       d = reinterpret_cast<uint4*>(buf);
+		for (uint32_t i = lane; i < p.bytes / 16; i += 32) { d[i] = __ldg(s + i); }
+	} else if ((al & 3u) == 0) {
+		const uint32_t* s = reinterpret_cast<const uint32_t*>(p.src);
+		uint32_t*       d = reinterpret_cast<uint32_t*>(buf);
+		for (uint32_t i = lane; i < p.bytes / 4; i += 32) { d[i] = __ldg(s + i); }
+	} else {
+		for (uint32_t i = lane; i < p.bytes; i += 32) { buf[i] = __ldg(p.src + i); }
+	}
+	__syncwarp();
+	uint32_t* rows = reinterpret_cast<uint32_t*>(buf);
 	uint32_t  x[32];
 	bool      bad = false;
 	if (p.ws == 32) {
-		decode_stream<32>(p, reinterpret_cast<const uint32_t*>(slot), lane, x);
+		decode_stream<32>(p, reinterpret_cast<const uint32_t*>(buf), lane, x);
 		__syncwarp();
 		const uint32_t r0 = row_word(run_start<32>(lane, 0));
 #pragma unroll
 		for (int i = 0; i < 32; ++i) { rows[r0 + i] = x[i]; }
 	} else {
-		decode_stream<16>(p, reinterpret_cast<const uint32_t*>(slot), lane, x);
+		decode_stream<16>(p, reinterpret_cast<const uint32_t*>(buf), lane, x);
 #pragma unroll
 		for (int i = 0; i < 32; ++i) {
 			const bool in = x[i] < p.n_runs;
@@ -175,226 +192,195 @@ __device__ __forceinline__ void stage_to_rows(const Plan& p, uint8_t* slot, uint
 	__syncwarp();
 }
 
-// Row 32 * b + lane: its source (dictionary entry or compressed bytes) and decoded length.
+// Row r of the vector: its source (dictionary entry or compressed bytes) and decoded length.
 struct RowRef {
 	uint32_t start; // dictionary byte offset (DICT) or compressed byte offset within the vector
 	uint32_t clen;  // compressed length (FSST / BYTE_ARR)
 	uint32_t len;   // decoded length
 };
 
-__device__ __forceinline__ RowRef row_ref(const StrArgs& a, const uint32_t* ends, const uint32_t* rows, uint32_t r,
-                                          const uint8_t* vb, uint32_t vn, const uint8_t* flen, bool* bad) {
+template <int KIND>
+__device__ __forceinline__ RowRef row_ref(const StrArgs& a, const uint32_t* rows, uint32_t r, const uint8_t* vb,
+                                          uint32_t vn, const uint8_t* flen, bool* bad) {
 	RowRef f {0, 0, 0};
-	if (a.kind == STR_DICT) {
+	if constexpr (KIND == STR_DICT) {
 		const uint32_t code = rows[row_word(r)];
 		if (code >= a.entry_c) {
 			*bad = true;
 			return f;
 		}
-		f.start = code ? __ldg(ends + code - 1) : 0u;
-		f.len   = __ldg(ends + code) - f.start;
+		f.start = code ? __ldg(a.dict_ends + code - 1) : 0u;
+		f.len   = __ldg(a.dict_ends + code) - f.start;
+		return f;
+	} else {
+		const uint32_t s = r == 0 ? 0u : rows[row_word(r - 1)];
+		const uint32_t e = rows[row_word(r)];
+		if (e < s || e > vn) {
+			*bad = true;
+			return f;
+		}
+		f.start = s;
+		f.clen  = e - s;
+		f.len   = KIND == STR_BYTES ? f.clen : fsst_decoded_len(flen, vb + s, f.clen);
 		return f;
 	}
-	const uint32_t s = r == 0 ? 0u : rows[row_word(r - 1)];
-	const uint32_t e = rows[row_word(r)];
-	if (e < s || e > vn) {
-		*bad = true;
-		return f;
-	}
-	f.start = s;
-	f.clen  = e - s;
-	f.len   = a.kind == STR_BYTES ? f.clen : fsst_decoded_len(flen, vb + s, f.clen);
-	return f;
 }
 
-template <int PASS>
-__global__ void __launch_bounds__(kStrWarps * 32) k_str_pass(const StrArgs a) {
+template <int KIND>
+__device__ __forceinline__ void emit_row(uint8_t* dst, const RowRef& f, const uint8_t* dict, const uint8_t* vb,
+                                         const uint64_t* fsym, const uint8_t* flen) {
+	if constexpr (KIND == STR_DICT) {
+		copy_row(dst, dict + f.start, f.len);
+	} else if constexpr (KIND == STR_BYTES) {
+		copy_row(dst, vb + f.start, f.len);
+	} else {
+		fsst_decode_to(fsym, flen, vb + f.start, f.clen, dst);
+	}
+}
+
+// One pass over the column's vectors, warp per vector.  LENGTHS: per-vector decoded byte totals.  MATERIALIZE:
+// Arrow offsets and bytes, at the first output byte of every vector computed from the totals.  DSMEM: the
+// decoded dictionary is copied to shared memory (after the per-warp areas) at CTA start.
+template <int PASS, int KIND, bool DSMEM>
+__global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a) {
 	extern __shared__ __align__(128) uint8_t smem[];
-	__shared__ uint64_t fsym[256];
-	__shared__ uint8_t  flen[256];
-	const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-	constexpr uint32_t kPerWarp = str_per_warp<PASS>();
-	// decoded dictionary bytes into shared memory when the plan found room for them (the end offsets are read
-	// through the L1 cache)
-	const uint8_t* dbytes = a.dict_bytes;
-	if (PASS == STR_PASS_MATERIALIZE && a.kind == STR_DICT && a.dict_in_smem) {
-		uint8_t* db = smem + kStrWarps * kPerWarp;
+	__shared__ uint64_t fsym[KIND == STR_FSST ? 256 : 1];
+	__shared__ uint8_t  flen[KIND == STR_FSST ? 256 : 1];
+	const uint32_t     lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+	constexpr uint32_t kPerWarp = str_per_warp(PASS);
+	const uint8_t*     dict     = a.dict_bytes;
+	if constexpr (PASS == STR_PASS_MATERIALIZE && KIND == STR_DICT && DSMEM) {
+		uint8_t* db = smem + nwarps * kPerWarp;
 		// the decoded dictionary lives in a cudaMalloc'd (256-byte aligned) buffer with at least 16 bytes of
 		// slack after the last entry
 		const uint32_t nb16 = static_cast<uint32_t>((a.dict_bytes_n + 15) / 16);
 		for (uint32_t i = threadIdx.x; i < nb16; i += blockDim.x) {
 			reinterpret_cast<uint4*>(db)[i] = __ldg(reinterpret_cast<const uint4*>(a.dict_bytes) + i);
 		}
-		dbytes = db;
+		dict = db;
 	}
-	if (a.kind == STR_FSST) {
+	if constexpr (KIND == STR_FSST) {
 		for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) {
 			fsym[i] = a.table->sym[i];
 			flen[i] = a.table->len[i];
 		}
 	}
-	uint8_t*  wbase = smem + warp * kPerWarp;
-	uint64_t* bars  = reinterpret_cast<uint64_t*>(wbase);
-	PlanS*    plans = reinterpret_cast<PlanS*>(wbase + 16);
-	uint8_t*  slots = wbase + kStrHead;
-	uint8_t*  win   = slots + 2 * kStrSlot;
-	if (lane == 0) {
-		mbar_init(&bars[0], 1);
-		mbar_init(&bars[1], 1);
-		fence_mbar_init();
-	}
+	uint8_t* wbase = smem + warp * kPerWarp;
+	PlanS*   plans = reinterpret_cast<PlanS*>(wbase);
+	uint8_t* buf   = wbase + kStrPB * 64;
+	uint8_t* win   = buf + kStrRows;
 	__syncthreads();
 
-	const uint64_t gw = static_cast<uint64_t>(blockIdx.x) * kStrWarps + warp;
-	const uint64_t nw = static_cast<uint64_t>(gridDim.x) * kStrWarps;
+	const uint64_t gw = static_cast<uint64_t>(blockIdx.x) * nwarps + warp;
+	const uint64_t nw = static_cast<uint64_t>(gridDim.x) * nwarps;
 	const uint64_t n  = a.col.n_vec;
-	auto fetch_plans = [&](uint32_t blk) {
-		if (lane < kStrPB) {
-			const uint64_t k     = static_cast<uint64_t>(blk) * kStrPB + lane;
-			const uint64_t v     = gw + k * nw;
-			Plan           p {};
-			const bool     valid = v < n;
-			if (valid) { p = make_plan(a.col, static_cast<uint32_t>(v)); }
-			plans[k % (2 * kStrPB)] = pack_plan(p, valid);
-		}
-	};
-	auto issue_k = [&](uint64_t k) {
-		const PlanS& ps = plans[k % (2 * kStrPB)];
-		if (ps.flags & 4u) {
-			uint8_t* sl = slots + (k & 1) * kStrSlot;
-			issue<0>(unpack_plan(ps), sl, nullptr, sl + kStrStage, &bars[k & 1], lane);
-		}
-	};
-	fetch_plans(0);
-	fetch_plans(1);
-	__syncwarp();
-	issue_k(0);
-	issue_k(1);
-
-	uint32_t k = 0;
+	uint32_t       k  = 0;
 	for (uint64_t v = gw; v < n; v += nw, ++k) {
-		if (k % kStrPB == 0 && k > 0) {
-			fetch_plans(k / kStrPB + 1);
+		if (k % kStrPB == 0) {
+			if (lane < kStrPB) {
+				const uint64_t u = v + lane * nw;
+				Plan           q {};
+				if (u < n) { q = make_plan(a.col, static_cast<uint32_t>(u)); }
+				plans[lane] = pack_plan(q, u < n);
+			}
 			__syncwarp();
 		}
-		uint8_t* sl = slots + (k & 1) * kStrSlot;
-		Plan     p  = unpack_plan(plans[k % (2 * kStrPB)]);
-		if (!mbar_wait(&bars[k & 1], (k >> 1) & 1u)) {
-			if (lane == 0) { atomicOr(a.status, STATUS_TIMEOUT); }
-			// the other slot may still have a copy in flight: wait for it (bounded) before leaving
-			if (gw + static_cast<uint64_t>(k + 1) * nw < n) { (void)mbar_wait(&bars[(k + 1) & 1], ((k + 1) >> 1) & 1u); }
-			return;
-		}
+		const Plan p = unpack_plan(plans[k % kStrPB]);
 		if (!p.ok) {
 			if (lane == 0) {
 				atomicOr(a.status, p.bw > p.ws ? STATUS_BAD_BW : STATUS_BAD_LAYOUT);
 				if (PASS == STR_PASS_LENGTHS) { a.vec_total[v] = 0; }
 			}
-			__syncwarp();
-			issue_k(k + 2);
 			continue;
 		}
-		if (p.lane_bases) { p.lane_bases = sl + kStrStage + (reinterpret_cast<uintptr_t>(p.lane_bases) & 15u); }
-		stage_to_rows(p, sl, lane, a.status);
-		const uint32_t* rows = reinterpret_cast<const uint32_t*>(sl);
+		load_rows(p, buf, lane, a.status);
+		const uint32_t* rows = reinterpret_cast<const uint32_t*>(buf);
 		uint32_t        vn   = 0;
-		const uint8_t*  vb   = a.kind == STR_DICT ? nullptr : vector_bytes(a.col, static_cast<uint32_t>(v), &vn);
+		const uint8_t*  vb   = KIND == STR_DICT ? nullptr : vector_bytes(a.col, static_cast<uint32_t>(v), &vn);
 		bool            bad  = false;
-		if (PASS == STR_PASS_LENGTHS) {
+		if constexpr (PASS == STR_PASS_LENGTHS) {
 			uint32_t sum = 0;
-			for (uint32_t b = 0; b < kVec / 32; ++b) {
-				sum += row_ref(a, a.dict_ends, rows, 32 * b + lane, vb, vn, flen, &bad).len;
-			}
+			for (uint32_t b = 0; b < kVec / 32; ++b) { sum += row_ref<KIND>(a, rows, 32 * b + lane, vb, vn, flen, &bad).len; }
 			sum = warp_sum(sum);
 			if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) { atomicOr(a.status, STATUS_BAD_INDEX); }
 			if (lane == 0) { a.vec_total[v] = sum; }
 			__syncwarp();
-			issue_k(k + 2);
 			continue;
-		}
-		const uint64_t vbase = a.vec_base[v];
-		const uint64_t vend  = a.vec_base[v + 1];
-		if (vend < vbase || vend > a.bytes_cap) {
-			if (lane == 0) { atomicOr(a.status, STATUS_BAD_LAYOUT); }
-			__syncwarp();
-			issue_k(k + 2);
-			continue;
-		}
-		// Rows go to the window in batches of 32 (one row per lane, positions from a warp scan of the lengths);
-		// full 16-byte chunks of the window go out with 16-byte stores, the vector's first and last partial
-		// chunks byte by byte (the neighbouring vectors write the other bytes of those chunks).
-		uint64_t W    = vbase & ~15ull;          // output position of win[0]
-		uint32_t fill = static_cast<uint32_t>(vbase & 15u);
-		uint64_t lo   = vbase;                   // first output byte the window may write
-		auto flush = [&](bool all) {
-			const uint32_t full = fill & ~15u;
-			const uint32_t upto = all ? fill : full;
-			for (uint32_t c = 16 * lane; c < upto; c += 512) {
-				const uint64_t g = W + c;
-				if (g >= lo && c + 16 <= upto) {
-					*reinterpret_cast<uint4*>(a.bytes + g) = *reinterpret_cast<const uint4*>(win + c);
-				} else {
-					for (uint32_t i = 0; i < 16 && c + i < upto; ++i) {
-						if (g + i >= lo) { a.bytes[g + i] = win[c + i]; }
+		} else {
+			const uint64_t vbase = a.vec_base[v];
+			const uint64_t vend  = a.vec_base[v + 1];
+			if (vend < vbase || vend > a.bytes_cap) {
+				if (lane == 0) { atomicOr(a.status, STATUS_BAD_LAYOUT); }
+				__syncwarp();
+				continue;
+			}
+			// Rows go to the window in batches of 32 (one row per lane, positions from a warp scan of the
+			// lengths); full 16-byte chunks of the window go out with 16-byte stores, the vector's first and last
+			// partial chunks byte by byte (the neighbouring vectors write the other bytes of those chunks).
+			uint64_t W    = vbase & ~15ull; // output position of win[0]
+			uint32_t fill = static_cast<uint32_t>(vbase & 15u);
+			uint64_t lo   = vbase; // first output byte the window may write
+			auto flush = [&](bool all) {
+				const uint32_t full = fill & ~15u;
+				const uint32_t upto = all ? fill : full;
+				for (uint32_t c = 16 * lane; c < upto; c += 512) {
+					const uint64_t g = W + c;
+					if (g >= lo && c + 16 <= upto) {
+						*reinterpret_cast<uint4*>(a.bytes + g) = *reinterpret_cast<const uint4*>(win + c);
+					} else {
+						for (uint32_t i = 0; i < 16 && c + i < upto; ++i) {
+							if (g + i >= lo) { a.bytes[g + i] = win[c + i]; }
+						}
 					}
 				}
-			}
-			__syncwarp();
-			if (!all) {
-				const uint8_t t = lane < (fill & 15u) ? win[full + lane] : 0;
 				__syncwarp();
-				if (lane < (fill & 15u)) { win[lane] = t; }
+				if (!all) {
+					const uint8_t t = lane < (fill & 15u) ? win[full + lane] : 0;
+					__syncwarp();
+					if (lane < (fill & 15u)) { win[lane] = t; }
+					__syncwarp();
+					W += full;
+					fill &= 15u;
+					lo = lo > W ? lo : W;
+				}
+			};
+			uint32_t vpos = 0; // bytes of this vector emitted so far
+			for (uint32_t b = 0; b < kVec / 32; ++b) {
+				const uint32_t r   = 32 * b + lane;
+				const RowRef   f   = row_ref<KIND>(a, rows, r, vb, vn, flen, &bad);
+				const uint32_t inc = warp_inclusive_scan(f.len, lane);
+				const uint32_t o   = vpos + inc - f.len;
+				const uint32_t T   = __shfl_sync(0xFFFFFFFFu, inc, 31);
+				a.offsets[v * kVec + r] = static_cast<uint32_t>(vbase + o);
+				if (fill + T > kStrWindow) { flush(false); }
+				if (fill + T <= kStrWindow) {
+					emit_row<KIND>(win + fill + (o - vpos), f, dict, vb, fsym, flen);
+					fill += T;
+				} else {
+					// a batch larger than the window: its rows go straight to global memory, after the window's
+					// pending bytes
+					flush(true);
+					uint8_t* dst = a.bytes + vbase + o;
+					if constexpr (KIND == STR_FSST) {
+						fsst_decode_to(fsym, flen, vb + f.start, f.clen, dst);
+					} else {
+						const uint8_t* src = KIND == STR_DICT ? dict + f.start : vb + f.start;
+						for (uint32_t i = 0; i < f.len; ++i) { dst[i] = src[i]; }
+					}
+					const uint64_t pos = vbase + vpos + T;
+					W    = pos & ~15ull;
+					fill = static_cast<uint32_t>(pos & 15u);
+					lo   = pos;
+				}
+				vpos += T;
 				__syncwarp();
-				W += full;
-				fill &= 15u;
-				lo = lo > W ? lo : W;
 			}
-		};
-		uint32_t vpos = 0; // bytes of this vector emitted so far
-		for (uint32_t b = 0; b < kVec / 32; ++b) {
-			const uint32_t r   = 32 * b + lane;
-			const RowRef   f   = row_ref(a, a.dict_ends, rows, r, vb, vn, flen, &bad);
-			const uint32_t inc = warp_inclusive_scan(f.len, lane);
-			const uint32_t o   = vpos + inc - f.len;
-			const uint32_t T   = __shfl_sync(0xFFFFFFFFu, inc, 31);
-			a.offsets[v * kVec + r] = static_cast<uint32_t>(vbase + o);
-			if (fill + T > kStrWindow) { flush(false); }
-			if (fill + T <= kStrWindow) {
-				uint8_t* dst = win + fill + (o - vpos);
-				if (a.kind == STR_DICT) {
-					copy_row(dst, dbytes + f.start, f.len);
-				} else if (a.kind == STR_BYTES) {
-					copy_row(dst, vb + f.start, f.len);
-				} else {
-					fsst_decode_to(fsym, flen, vb + f.start, f.clen, dst);
-				}
-				fill += T;
-			} else {
-				// a batch larger than the window: its rows go straight to global memory, after the window's
-				// pending bytes
-				flush(true);
-				uint8_t* dst = a.bytes + vbase + o;
-				if (a.kind == STR_DICT) {
-					for (uint32_t i = 0; i < f.len; ++i) { dst[i] = dbytes[f.start + i]; }
-				} else if (a.kind == STR_BYTES) {
-					for (uint32_t i = 0; i < f.len; ++i) { dst[i] = vb[f.start + i]; }
-				} else {
-					fsst_decode_to(fsym, flen, vb + f.start, f.clen, dst);
-				}
-				const uint64_t pos = vbase + vpos + T;
-				W    = pos & ~15ull;
-				fill = static_cast<uint32_t>(pos & 15u);
-				lo   = pos;
-			}
-			vpos += T;
+			flush(true);
+			if (lane == 0 && v + 1 == n) { a.offsets[n * kVec] = static_cast<uint32_t>(vbase + vpos); }
+			if (vbase + vpos != vend) { bad = true; }
+			if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) { atomicOr(a.status, STATUS_BAD_INDEX); }
 			__syncwarp();
 		}
-		flush(true);
-		if (lane == 0 && v + 1 == n) { a.offsets[n * kVec] = static_cast<uint32_t>(vbase + vpos); }
-		if (vbase + vpos != vend) { bad = true; }
-		if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) { atomicOr(a.status, STATUS_BAD_INDEX); }
-		__syncwarp();
-		issue_k(k + 2);
 	}
 }
 
@@ -415,7 +401,7 @@ __global__ void __launch_bounds__(1024) k_scan_totals(const uint64_t* total, uin
 // ---------------------------------------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------------------------------------
-uint32_t str_smem_base() { return kStrWarps * str_per_warp<STR_PASS_MATERIALIZE>(); }
+uint32_t str_smem_per_warp() { return str_per_warp(STR_PASS_MATERIALIZE); }
 
 cudaError_t launch_fsst_dict(const uint8_t* lens, const uint8_t* comp, uint64_t comp_size, uint32_t entry_c,
                              const FsstTable* tab, uint32_t* ends, uint8_t* bytes, uint64_t cap, int* status,
@@ -426,38 +412,44 @@ cudaError_t launch_fsst_dict(const uint8_t* lens, const uint8_t* comp, uint64_t 
 	return cudaGetLastError();
 }
 
-// Launch one pass over the column's vectors: every SM holds as many CTAs as its shared memory allows, and no
-// more CTAs than there are vectors for their warps.
-template <int PASS>
-static cudaError_t launch_str_pass(const StrArgs& a, uint32_t dyn_smem, cudaStream_t s) {
+// Launch one pass over the column's vectors with `warps` warps per CTA and as many CTAs per SM as shared
+// memory allows (no more CTAs than there are vectors for their warps).
+template <int PASS, int KIND, bool DSMEM>
+static cudaError_t launch_str_kernel(const StrArgs& a, int warps, uint32_t dyn_smem, cudaStream_t s) {
+	auto* const       fn = k_str_pass<PASS, KIND, DSMEM>;
 	static std::mutex mu;
 	static uint32_t   set = 0;
 	{
 		std::lock_guard<std::mutex> lk(mu);
 		if (dyn_smem > set) {
-			const cudaError_t e =
-			    cudaFuncSetAttribute(k_str_pass<PASS>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_smem);
+			const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_smem);
 			if (e != cudaSuccess) { return e; }
 			set = dyn_smem;
 		}
 	}
 	Device* dev = current_device();
 	if (!dev) { return cudaErrorUnknown; }
-	int per_sm = 0;
-	cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_str_pass<PASS>, kStrWarps * 32, dyn_smem);
+	int         per_sm = 0;
+	cudaError_t e      = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, warps * 32, dyn_smem);
 	if (e != cudaSuccess) { return e; }
 	if (per_sm < 1) { return cudaErrorInvalidConfiguration; }
-	const uint64_t need = (a.col.n_vec + kStrWarps - 1) / kStrWarps;
+	const uint64_t need = (a.col.n_vec + warps - 1) / warps;
 	uint64_t       grid = static_cast<uint64_t>(dev->sm_count) * per_sm;
 	grid                = grid < need ? grid : need;
 	if (grid == 0) { return cudaSuccess; }
-	k_str_pass<PASS><<<static_cast<unsigned>(grid), kStrWarps * 32, dyn_smem, s>>>(a);
+	fn<<<static_cast<unsigned>(grid), warps * 32, dyn_smem, s>>>(a);
 	++launch_counter();
 	return cudaGetLastError();
 }
 
 cudaError_t launch_str_lengths(const StrArgs& a, int /*grid*/, cudaStream_t s) {
-	return launch_str_pass<STR_PASS_LENGTHS>(a, kStrWarps * str_per_warp<STR_PASS_LENGTHS>(), s);
+	constexpr int    w    = kStrMaxWarps;
+	constexpr uint32_t sm = w * str_per_warp(STR_PASS_LENGTHS);
+	switch (a.kind) {
+	case STR_DICT: return launch_str_kernel<STR_PASS_LENGTHS, STR_DICT, false>(a, w, sm, s);
+	case STR_FSST: return launch_str_kernel<STR_PASS_LENGTHS, STR_FSST, false>(a, w, sm, s);
+	default: return launch_str_kernel<STR_PASS_LENGTHS, STR_BYTES, false>(a, w, sm, s);
+	}
 }
 
 cudaError_t launch_scan_totals(const uint64_t* total, uint64_t* base, uint64_t n, cudaStream_t s) {
@@ -466,8 +458,14 @@ cudaError_t launch_scan_totals(const uint64_t* total, uint64_t* base, uint64_t n
 	return cudaGetLastError();
 }
 
-cudaError_t launch_str_materialize(const StrArgs& a, int /*grid*/, uint32_t dyn_smem, cudaStream_t s) {
-	return launch_str_pass<STR_PASS_MATERIALIZE>(a, dyn_smem, s);
+cudaError_t launch_str_materialize(const StrArgs& a, int warps, uint32_t dyn_smem, cudaStream_t s) {
+	switch (a.kind) {
+	case STR_DICT:
+		return a.dict_in_smem ? launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, true>(a, warps, dyn_smem, s)
+		                      : launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, false>(a, warps, dyn_smem, s);
+	case STR_FSST: return launch_str_kernel<STR_PASS_MATERIALIZE, STR_FSST, false>(a, warps, dyn_smem, s);
+	default: return launch_str_kernel<STR_PASS_MATERIALIZE, STR_BYTES, false>(a, warps, dyn_smem, s);
+	}
 }
 
 } // namespace flsgpu
@@ -602,7 +600,7 @@ extern "C" int fls_gpu_decode_fsst_page_noalloc(const uint8_t* d_page, uint64_t 
 	if (launch_str_lengths(a, sms, s) != cudaSuccess ||
 	    launch_scan_totals(a.vec_total, reinterpret_cast<uint64_t*>(scratch + NoAllocLayout::kBase), vec_c, s) !=
 	        cudaSuccess ||
-	    launch_str_materialize(a, sms, str_smem_base(), s) != cudaSuccess) {
+	    launch_str_materialize(a, kStrMaxWarps, kStrMaxWarps * str_smem_per_warp(), s) != cudaSuccess) {
 		return FLS_ERR_CUDA;
 	}
 	return FLS_OK;

@@ -19,6 +19,8 @@ enum : uint8_t {
 	STR_BYTES = 2, // rows are plain bytes in the page (BYTE_ARR pages)
 };
 
+constexpr int kStrMaxWarps = 16; // warps per CTA of the string kernels
+
 struct StrArgs {
 	ColDesc          col; // the row stream: codes or cumulative end offsets, page layout
 	uint8_t          kind;
@@ -41,7 +43,9 @@ cudaError_t launch_fsst_dict(const uint8_t* lens, const uint8_t* comp, uint64_t 
                              cudaStream_t s);
 cudaError_t launch_str_lengths(const StrArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_scan_totals(const uint64_t* total, uint64_t* base, uint64_t n, cudaStream_t s);
-cudaError_t launch_str_materialize(const StrArgs& a, int grid, uint32_t dyn_smem, cudaStream_t s);
-uint32_t    str_smem_base();
+// warps: warps per CTA (at most kStrMaxWarps); dyn_smem: warps * str_smem_per_warp() plus the dictionary
+// bytes when a.dict_in_smem
+cudaError_t launch_str_materialize(const StrArgs& a, int warps, uint32_t dyn_smem, cudaStream_t s);
+uint32_t    str_smem_per_warp();
 
 } // namespace flsgpu
