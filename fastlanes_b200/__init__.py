@@ -7,6 +7,7 @@ from . import _lib  # noqa: F401  (raises if the CUDA library is missing)
 from . import primitives  # noqa: F401
 from . import pages  # noqa: F401
 from . import strings  # noqa: F401
+from . import select  # noqa: F401
 from . import workloads  # noqa: F401
 
-__all__ = ["pages", "primitives", "strings", "workloads"]
+__all__ = ["pages", "primitives", "select", "strings", "workloads"]

@@ -191,3 +191,71 @@ def string_dictionary(seed=0, n_dict=4096, n_tokens=256):
 def zipf_codes(n_rows=16 << 20, n_dict=4096, a=1.1, seed=0):
     rng = np.random.default_rng(seed)
     return ((rng.zipf(a, n_rows) - 1) % n_dict).astype(np.uint32)
+
+
+# ---- integer columns for expression selection ------------------------------------------------------------
+SELECTION_FAMILIES = ("for_u32", "for_i64", "delta_i64", "rle", "dict_i32", "dict_rle", "noise")
+
+
+def _zipf_codes(n, d, a, g, device):
+    """n codes over d entries with P(k) proportional to 1 / (k + 1)^a (inverse CDF)."""
+    k = torch.arange(1, d + 1, dtype=torch.float64, device=device)
+    cdf = torch.cumsum(k.pow(-a), 0)
+    cdf /= cdf[-1].clone()
+    u = torch.rand(n, generator=g, device=device, dtype=torch.float64)
+    return torch.searchsorted(cdf, u).clamp_(max=d - 1)
+
+
+def _runs(n, mean, g, device):
+    """Run id of each of n positions, run lengths geometric with the given mean."""
+    m = int(n / mean * 2) + 16
+    lens = torch.empty(m, device=device, dtype=torch.float64).geometric_(1.0 / mean, generator=g).long()
+    ends = torch.cumsum(lens, 0)
+    pos = torch.arange(n, device=device, dtype=torch.int64)
+    return torch.searchsorted(ends, pos, right=True)
+
+
+def selection_column(rng, n_vec, device="cuda", family=None):
+    """One seeded integer column of n_vec vectors from a family of the mixed row-group workload, with random
+    parameters: FOR u32 / i64 (random bit width), sorted i64 timestamps (geometric gaps), runs (geometric
+    lengths, mean 2..64), low-cardinality int32 dictionaries (16..65,536 entries, Zipf 0.8..1.5), the same with
+    runs, and incompressible noise.  Returns (tensor, is_signed): int32 / int64 on `device`."""
+    fam = family or SELECTION_FAMILIES[rng.choice(len(SELECTION_FAMILIES), p=(.2, .2, .15, .15, .15, .1, .05))]
+    g = torch.Generator(device=device)
+    g.manual_seed(int(rng.integers(0, 2 ** 62)))
+    n = n_vec * 1024
+    if fam == "for_u32":
+        bw = int(rng.integers(0, 33))
+        base = int(rng.integers(0, 2 ** 32 - 2 ** bw + 1))
+        v = torch.randint(0, 2 ** bw, (n,), generator=g, device=device, dtype=torch.int64) + base
+        return v.to(torch.int32), False
+    if fam == "for_i64":
+        bw = int(rng.integers(0, 63))
+        base = int(rng.integers(-2 ** 62, 2 ** 62 - 2 ** bw + 1))
+        return torch.randint(0, 2 ** bw, (n,), generator=g, device=device, dtype=torch.int64) + base, True
+    if fam == "delta_i64":
+        mean = float(np.exp(rng.uniform(0, np.log(4096))))
+        gaps = torch.empty(n, device=device, dtype=torch.float64).geometric_(1.0 / max(mean, 1.0), generator=g)
+        t0 = 1_600_000_000_000_000_000 + int(rng.integers(0, 2 ** 40))
+        return torch.cumsum(gaps.long() - 1, 0) + t0, True
+    if fam == "rle":
+        wide = bool(rng.integers(0, 2))
+        run = _runs(n, float(rng.uniform(2, 64)), g, device)
+        bw = int(rng.integers(1, 41 if wide else 32))
+        vals = torch.randint(0, 2 ** bw, (int(run[-1]) + 1,), generator=g, device=device, dtype=torch.int64)
+        v = vals[run]
+        return (v, True) if wide else (v.to(torch.int32), False)
+    if fam in ("dict_i32", "dict_rle"):
+        d = int(np.exp(rng.uniform(np.log(16), np.log(65536))))
+        bw = int(rng.integers(8, 32))
+        dic = torch.randint(-2 ** bw, 2 ** bw, (d,), generator=g, device=device, dtype=torch.int64)
+        a = float(rng.uniform(0.8, 1.5))
+        if fam == "dict_i32":
+            codes = _zipf_codes(n, d, a, g, device)
+        else:
+            run = _runs(n, float(rng.uniform(2, 64)), g, device)
+            codes = _zipf_codes(int(run[-1]) + 1, d, a, g, device)[run]
+        return dic[codes].to(torch.int32), True
+    wide = bool(rng.integers(0, 2))
+    v = torch.randint(-2 ** 62, 2 ** 62, (n,), generator=g, device=device, dtype=torch.int64) * 2 + 1
+    return (v, True) if wide else (v.to(torch.int32), False)
