@@ -380,16 +380,18 @@ struct fls_plan {
 	uint32_t  n_cols   = 0;
 	int       device   = -1;
 	Family    family   = Family::NUM;
+	uint32_t  col_shift = 24;
 	ColDesc   col0 {};
 };
 
 namespace flsgpu {
 int make_plan_object(const std::vector<ColDesc>& descs, const std::vector<uint32_t>& queue, Family fam,
-                     ::fls_plan** out) {
+                     uint32_t col_shift, ::fls_plan** out) {
 	std::unique_ptr<fls_plan> p(new fls_plan());
 	if (cudaGetDevice(&p->device) != cudaSuccess) { return FLS_ERR_CUDA; }
-	p->n_cols = static_cast<uint32_t>(descs.size());
-	p->family = fam;
+	p->n_cols    = static_cast<uint32_t>(descs.size());
+	p->family    = fam;
+	p->col_shift = col_shift;
 	if (descs.size() == 1) {
 		// one column: the queue is implicit (vector v = item v)
 		p->col0    = descs[0];
@@ -508,8 +510,9 @@ int fls_plan_decode_grid(const fls_plan* p, int grid, fls_stream_t stream) {
 	DecodeArgs a {};
 	a.cols    = p->d_cols;
 	a.queue   = p->d_queue;
-	a.n_items = p->n_items;
-	a.col0    = p->col0;
+	a.n_items   = p->n_items;
+	a.col_shift = p->col_shift;
+	a.col0      = p->col0;
 	return to_status(launch_decode(p->family, a, static_cast<cudaStream_t>(stream), grid));
 }
 

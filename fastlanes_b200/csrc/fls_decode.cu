@@ -474,14 +474,14 @@ __device__ __forceinline__ Plan unpack_plan(const PlanS& s) {
 }
 
 #ifndef FLS_HOST_EMULATION
-__device__ __forceinline__ uint32_t item_col(uint32_t it) { return it >> 24; }
-__device__ __forceinline__ uint32_t item_vec(uint32_t it) { return it & 0xFFFFFFu; }
+__device__ __forceinline__ uint32_t item_col(uint32_t it, uint32_t shift) { return it >> shift; }
+__device__ __forceinline__ uint32_t item_vec(uint32_t it, uint32_t shift) { return it & ((1u << shift) - 1u); }
 
 __device__ __forceinline__ Plan plan_of(const DecodeArgs& a, uint64_t item) {
 	if (a.queue == nullptr) { return make_plan(a.col0, static_cast<uint32_t>(item)); }
 	const uint32_t it = a.queue[item];
-	const ColDesc& c  = a.cols ? a.cols[item_col(it)] : a.col0;
-	return make_plan(c, item_vec(it));
+	const ColDesc& c  = a.cols ? a.cols[item_col(it, a.col_shift)] : a.col0;
+	return make_plan(c, item_vec(it, a.col_shift));
 }
 
 // Kernel family: MAXWS bounds the staged stream (MAXWS * 128 bytes), GSTAGE the run-value window, EMAX the

@@ -349,4 +349,58 @@ int fls_encode_string_dict(const uint8_t* dict_bytes, const uint64_t* dict_offse
 	return FLS_OK;
 }
 
+int fls_encode_int_dict(const void* in, uint64_t n, int width, int rle, uint8_t* page_out, uint64_t page_cap,
+                        uint64_t* page_size, uint8_t* dict_out, uint64_t dict_cap, uint64_t* dict_size) {
+	if (!in || !page_size || !dict_size || (width != 32 && width != 64)) { return FLS_ERR_ARG; }
+	n = n / 1024 * 1024;
+	// dictionary in first-occurrence order (src/cor/lyt/dic/dic_fac.cpp:19-40)
+	std::vector<uint32_t> codes(n);
+	std::vector<uint64_t> entries;
+	{
+		std::unordered_map<uint64_t, uint32_t> idx;
+		idx.reserve(n / 4 + 16);
+		for (uint64_t i = 0; i < n; ++i) {
+			const uint64_t x = width == 64 ? static_cast<const uint64_t*>(in)[i] : static_cast<const uint32_t*>(in)[i];
+			auto           r = idx.emplace(x, static_cast<uint32_t>(entries.size()));
+			if (r.second) { entries.push_back(x); }
+			codes[i] = r.first->second;
+		}
+	}
+	const uint64_t sz    = width / 8;
+	const uint64_t raw   = entries.size() * sz;
+	const uint64_t dsize = 8 + 12 + raw;
+	*dict_size           = dsize;
+	if (!dict_out || dsize > dict_cap) { return FLS_ERR_ARG; }
+	// dict_hdr_t (include/fls/cor/lyt/dic/dic.hpp:32-41), then a rec buffer holding the entries raw: rec_hdr
+	// {bw 255, pad, exc_c 0, base = byte count} (include/fls/cor/lyt/rec_hdr.hpp:7-13)
+	std::memset(dict_out, 0, 20);
+	dict_out[0]             = 8; // DICT
+	const uint32_t entry_c  = static_cast<uint32_t>(entries.size());
+	std::memcpy(dict_out + 4, &entry_c, 4);
+	dict_out[8] = 255;
+	std::memcpy(dict_out + 12, &raw, 8);
+	for (uint64_t e = 0; e < entries.size(); ++e) {
+		if (width == 64) {
+			std::memcpy(dict_out + 20 + 8 * e, &entries[e], 8);
+		} else {
+			const uint32_t x = static_cast<uint32_t>(entries[e]);
+			std::memcpy(dict_out + 20 + 4 * e, &x, 4);
+		}
+	}
+	uint64_t mtd = 0;
+	int      rc;
+	if (rle) {
+		// DICT_RLE DELTA_NO_PATCH: the RLE page layout over the u32 codes
+		rc = encode_rle_page(codes.data(), n, page_cap, page_out, page_size, &mtd, 32);
+		if (rc != FLS_OK) { return rc; }
+		page_out[0] = 11; // DICT_RLE, variant 2 kept
+	} else {
+		rc = fls_encode_from_memory_status(codes.data(), n, page_cap, page_out, page_size, &mtd, UINT32, 1);
+		if (rc != FLS_OK) { return rc; }
+		page_out[0] = 8; // DICT
+		page_out[1] = 2; // FFOR_NO_PATCH
+	}
+	return FLS_OK;
+}
+
 } // extern "C"

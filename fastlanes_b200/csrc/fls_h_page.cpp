@@ -14,6 +14,7 @@
 #include "fls_page.h"
 #include "fls_runtime.h"
 
+#include <algorithm>
 #include <cstring>
 #include <cuda_runtime.h>
 #include <vector>
@@ -169,9 +170,12 @@ static int read_on(void* dst, const void* src, size_t n, cudaStream_t stream) {
 	return cudaStreamSynchronize(stream) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
 }
 
+// Work items of page plans: (column << kPageShift | vector); a page holds at most 65,535 vectors.
+constexpr uint32_t kPageShift = 16;
+
 static int describe_pages(const fls_page_column* cols, uint32_t n_cols, std::vector<ColDesc>* descs,
                           std::vector<uint32_t>* queue, Family* fam_out, cudaStream_t stream) {
-	if (!cols || n_cols == 0 || n_cols > 255) { return FLS_ERR_ARG; }
+	if (!cols || n_cols == 0 || n_cols > 65535) { return FLS_ERR_ARG; }
 	descs->assign(n_cols, ColDesc {});
 	queue->clear();
 	Family fam   = Family::NUM;
@@ -204,7 +208,16 @@ static int describe_pages(const fls_page_column* cols, uint32_t n_cols, std::vec
 		if (rc != FLS_OK) { return rc; }
 		if ((*descs)[i].post != POST_NONE) { fam = Family::GATHER; }
 		if ((*descs)[i].ws == 64) { any64 = true; }
-		for (uint32_t v = 0; v < pi.vec_c; ++v) { queue->push_back((i << 24) | v); }
+		for (uint32_t v = 0; v < pi.vec_c; ++v) { queue->push_back((i << kPageShift) | v); }
+	}
+	// group the work items by kernel specialisation so that warps run long stretches of one code path (the
+	// outputs do not depend on the order)
+	auto key = [&](uint32_t it) {
+		const ColDesc& c = (*descs)[it >> kPageShift];
+		return (c.ws << 24) | (c.e << 16) | (c.enc << 8) | (c.post << 4) | c.order;
+	};
+	if (n_cols > 1) {
+		std::stable_sort(queue->begin(), queue->end(), [&](uint32_t x, uint32_t y) { return key(x) < key(y); });
 	}
 	if (fam == Family::GATHER && any64) { fam = Family::ANY; }
 	*fam_out = fam;
@@ -220,6 +233,7 @@ int fls_gpu_decode_pages(const fls_page_column* cols, uint32_t n_cols, fls_strea
 	if (rc != FLS_OK) { return rc; }
 	if (queue.empty()) { return FLS_OK; }
 	DecodeArgs   a {};
+	a.col_shift = kPageShift;
 	if (n_cols == 1) {
 		a.col0    = descs[0];
 		a.n_items = queue.size();
@@ -250,7 +264,7 @@ int fls_plan_create_pages(const fls_page_column* cols, uint32_t n_cols, fls_plan
 	// headers are read on the legacy default stream: the pages must be in place (e.g. after a device sync)
 	const int rc = describe_pages(cols, n_cols, &descs, &queue, &fam, nullptr);
 	if (rc != FLS_OK) { return rc; }
-	return make_plan_object(descs, queue, fam, out_plan);
+	return make_plan_object(descs, queue, fam, kPageShift, out_plan);
 }
 
 } // extern "C"

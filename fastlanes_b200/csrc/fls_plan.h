@@ -64,9 +64,10 @@ struct alignas(16) ColDesc {
 
 struct DecodeArgs {
 	const ColDesc*  cols;   // device array of columns, or null => use col0
-	const uint32_t* queue;  // device array of (col << 24 | vec) items, or null => items are vectors of col0
+	const uint32_t* queue;  // device array of (col << col_shift | vec) items, or null => vectors of col0
 	uint64_t        n_items;
-	int*            status; // device word; kernels OR error bits into it
+	int*            status;    // device word; kernels OR error bits into it
+	uint32_t        col_shift; // 24 for batch plans (256 batches), 16 for page plans (65,535 pages)
 	ColDesc         col0;
 };
 

@@ -32,9 +32,10 @@ cudaError_t launch_decode(Family fam, const DecodeArgs& args, cudaStream_t strea
 // Geometry of a family (threads per CTA, dynamic shared memory per CTA, CTAs resident per SM).
 void family_geometry(Family fam, int* threads, int* smem, int* ctas_per_sm);
 
-// Build a plan object from descriptors + queue (uploads both; a single column without a queue stays inline).
+// Build a plan object from descriptors + queue of (col << col_shift | vec) items (uploads both; a single column
+// without a queue stays inline).
 int make_plan_object(const std::vector<ColDesc>& descs, const std::vector<uint32_t>& queue, Family fam,
-                     ::fls_plan** out);
+                     uint32_t col_shift, ::fls_plan** out);
 
 // Kernels launched by this library inside the last timed region of a caller (a plain counter; not thread-safe).
 uint64_t& launch_counter();

@@ -125,6 +125,26 @@ def encode_from_memory(values, data_type, expr_id, capacity=None):
     return out[: size.value].copy(), mtd.value
 
 
+_enc_int_dict = declare("fls_encode_int_dict", ctypes.c_int, [_p, _u64, ctypes.c_int, ctypes.c_int, _p, _u64,
+                                                            ctypes.POINTER(_u64), _p, _u64, ctypes.POINTER(_u64)])
+
+
+def encode_int_dict(values, rle=False):
+    """DICT (exp 8 var 2) or DICT_RLE (exp 11 var 2) pages of an integer host array (32 / 64-bit, whole
+    vectors); returns (codes page, dictionary page)."""
+    values = np.ascontiguousarray(values)
+    w = values.dtype.itemsize * 8
+    cap = values.size * 4 * 2 + 65536
+    dcap = values.nbytes + 64
+    page, dic = np.zeros(cap, np.uint8), np.zeros(dcap, np.uint8)
+    ps, ds = _u64(), _u64()
+    rc = _enc_int_dict(_ptr(values), values.size, w, 1 if rle else 0, _ptr(page), cap, ctypes.byref(ps), _ptr(dic),
+                       dcap, ctypes.byref(ds))
+    if rc != 0:
+        raise FlsError(f"encode_int_dict: {rc}")
+    return page[: ps.value].copy(), dic[: ds.value].copy()
+
+
 def decode_to_memory(page, data_type, size=None):
     """fastlanes.h decode_to_memory on host bytes; returns the decoded values (original order)."""
     page = np.ascontiguousarray(page, np.uint8)

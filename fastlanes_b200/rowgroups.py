@@ -1,0 +1,93 @@
+"""Row groups of integer columns: every (column, row-group) chunk encoded with its own expression (chosen by
+``select``), the pages placed in one device buffer, and all chunks decoded by one persistent launch.
+
+Reference shape: a row group's columns each hold one expression per row group (include/fls/footer/
+rowgroup_footer.hpp:23-75, src/reader/reader.cpp:19-61 reads them back chunk by chunk through the
+Engine); here the reader is one page plan whose work queue spans every vector of every chunk.
+"""
+import numpy as np
+import torch
+
+from . import pages as PG
+from .select import POOL_IDS
+
+_DT = {(4, True): PG.INT32, (4, False): PG.UINT32, (8, True): PG.INT64, (8, False): PG.UINT64}
+_UNSIGNED = {4: np.uint32, 8: np.uint64}
+
+
+def encode_chunk(values, signed, candidate):
+    """Pages of one chunk (host array of whole vectors) under selection candidate 0..5; returns
+    (page, dictionary page or None)."""
+    x = values if signed else values.view(_UNSIGNED[values.dtype.itemsize])
+    if candidate <= 3:
+        page, _ = PG.encode_from_memory(x, _DT[(values.dtype.itemsize, signed)], POOL_IDS[candidate])
+        return page, None
+    return PG.encode_int_dict(x, rle=candidate == 5)
+
+
+class RowGroupSet:
+    """Encoded chunks of a set of columns and their decoder.
+
+    columns: list of (int32 / int64 tensor, is_signed); chunks: (col, first vector, vector count) arrays;
+    choice: candidate per chunk.  The pages live in one device buffer, each at a 16-byte aligned offset
+    (fls_page_placement), the dictionaries in another; outputs are one tensor per column (original order)."""
+
+    def __init__(self, columns, chunks, choice, device="cuda"):
+        col, first, count = chunks
+        choice = np.asarray(choice)
+        host = [t.cpu().numpy() for t, _ in columns]
+        self.signed = [s for _, s in columns]
+        pages, dicts, self.page_bytes, self.dict_bytes = [], [], 0, 0
+        for c in range(len(col)):
+            x = host[col[c]][int(first[c]) * 1024:(int(first[c]) + int(count[c])) * 1024]
+            p, d = encode_chunk(x, self.signed[col[c]], int(choice[c]))
+            pages.append(p)
+            dicts.append(d)
+            self.page_bytes += p.size
+            self.dict_bytes += 0 if d is None else d.size
+        # one buffer for the pages (each placed so its packed words start 16-byte aligned), one for dictionaries
+        pos, blob, off = 64, [], []
+        for p in pages:
+            shift = PG.placement(p)
+            start = (pos + 15) // 16 * 16 + shift
+            blob.append((start, p))
+            off.append(start)
+            pos = start + p.size + 16
+        buf = np.zeros(pos + 64, np.uint8)
+        for start, p in blob:
+            buf[start:start + p.size] = p
+        dpos, dblob, doff = 0, [], []
+        for d in dicts:
+            if d is None:
+                doff.append(None)
+                continue
+            start = (dpos + 15) // 16 * 16
+            dblob.append((start, d))
+            doff.append(start)
+            dpos = start + d.size
+        dbuf = np.zeros(max(dpos, 16) + 16, np.uint8)
+        for start, d in dblob:
+            dbuf[start:start + d.size] = d
+        self.d_pages = torch.from_numpy(buf).to(device)
+        self.d_dicts = torch.from_numpy(dbuf).to(device)
+        self.outputs = [torch.empty_like(t, device=device) for t, _ in columns]
+        base, dbase = self.d_pages.data_ptr(), self.d_dicts.data_ptr()
+        self.columns = []
+        for c in range(len(col)):
+            t = self.outputs[col[c]]
+            self.columns.append(dict(
+                d_page=base + off[c], page_size=pages[c].size,
+                d_dict=(dbase + doff[c]) if doff[c] is not None else None,
+                dict_size=0 if dicts[c] is None else dicts[c].size,
+                data_type=_DT[(t.element_size(), self.signed[col[c]])], order=1,
+                d_out=t.data_ptr() + int(first[c]) * 1024 * t.element_size()))
+        self.plan = PG.PagePlan(self.columns)
+        self.values = sum(t.numel() for t in self.outputs)
+        self.value_bytes = sum(t.numel() * t.element_size() for t in self.outputs)
+
+    def decode(self, stream=None):
+        """All chunks of all columns: one persistent kernel launch."""
+        self.plan.decode(stream)
+
+    def close(self):
+        self.plan.close()

@@ -117,12 +117,15 @@ class SelectionPlan:
         return choice, conf, nf.value
 
     def close(self):
-        if self.handle:
+        if getattr(self, "handle", None) and _plan_destroy is not None:
             _plan_destroy(self.handle)
             self.handle = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown: the library may already be gone
+            pass
 
 
 # ---- the MLP ----------------------------------------------------------------------------------------------

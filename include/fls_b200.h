@@ -263,6 +263,14 @@ int fls_encode_string_dict(const uint8_t* dict_bytes, const uint64_t* dict_offse
                            const uint32_t* codes, uint64_t n_rows, uint8_t* page_out, uint64_t page_cap,
                            uint64_t* page_size, uint8_t* dict_out, uint64_t dict_cap, uint64_t* dict_size);
 
+/* DICT / DICT_RLE encoding of an integer column of width 32 or 64 (host memory, whole vectors of n): the
+ * dictionary page (dict_hdr_t + a rec buffer holding the entries raw, first-occurrence order as
+ * src/cor/lyt/dic/dic_fac.cpp:19-40 assigns them) and the codes page, DICT FFOR_NO_PATCH (exp 8 var 2, int
+ * pool id 17) or with rle = 1 DICT_RLE DELTA_NO_PATCH (exp 11 var 2: the RLE layout over u32 run codes; the
+ * int pool's id 27 additionally packs the run codes).  *page_size / *dict_size receive the sizes. */
+int fls_encode_int_dict(const void* in, uint64_t n, int width, int rle, uint8_t* page_out, uint64_t page_cap,
+                        uint64_t* page_size, uint8_t* dict_out, uint64_t dict_cap, uint64_t* dict_size);
+
 #ifdef __cplusplus
 }
 #endif

@@ -100,6 +100,33 @@ def test_wizard_sizes_equal_encoded_page_sizes(cuda):
     plan.close()
 
 
+def test_dictionary_candidates_equal_encoded_sizes_and_round_trip(cuda):
+    """Candidates 4 / 5 are exactly the int DICT / DICT_RLE pages fls_encode_int_dict writes (codes page +
+    dictionary page), and those pages decode back to the column."""
+    import torch
+
+    from fastlanes_b200 import pages as PG
+    from fastlanes_b200 import select as S
+
+    dcols, hcols = _cols(4, n_vec=3, fams=("dict_i32", "dict_rle", "rle", "for_i64"), reps=1)
+    plan = S.SelectionPlan(dcols, 3)
+    sizes = plan.wizard()[0].cpu().numpy()
+    dt = {(8, True): PG.INT64, (8, False): PG.UINT64, (4, True): PG.INT32, (4, False): PG.UINT32}
+    for c, (x, sgn) in enumerate(hcols):
+        for cand, rle in ((4, False), (5, True)):
+            page, dic = PG.encode_int_dict(x, rle=rle)
+            assert page.size + dic.size == sizes[c, cand], (c, cand)
+            dp = torch.from_numpy(np.concatenate([page, np.zeros(64, np.uint8)])).cuda()
+            dd = torch.from_numpy(dic).cuda()
+            out = torch.empty(x.size, dtype=torch.from_numpy(x[:1]).dtype, device="cuda")
+            PG.decode_pages([dict(d_page=dp.data_ptr(), page_size=page.size, d_dict=dd.data_ptr(),
+                                  dict_size=dic.size, data_type=dt[(x.dtype.itemsize, sgn)], order=1,
+                                  d_out=out.data_ptr())])
+            torch.cuda.synchronize()
+            assert np.array_equal(out.cpu().numpy(), x), (c, cand)
+    plan.close()
+
+
 def test_features_match_oracle(cuda):
     from fastlanes_b200 import select as S
 
@@ -206,4 +233,26 @@ def test_learned_selection_after_training(cuda):
     choice_fb, _, nfb = plan.learned(params, stride=8, threshold=1.01)
     assert nfb == plan.n_chunks
     assert torch.equal(choice_fb, best)
+    plan.close()
+
+
+def test_rowgroups_every_candidate_in_one_launch(cuda):
+    """Chunks encoded with every candidate (chosen at random per chunk) decode bit-exactly through one page
+    plan spanning all chunks of all columns."""
+    import torch
+
+    from fastlanes_b200 import rowgroups as RG
+    from fastlanes_b200 import select as S
+
+    dcols, _ = _cols(7, n_vec=6, reps=1)
+    plan = S.SelectionPlan(dcols, 2)
+    rng = np.random.default_rng(0)
+    choice = rng.integers(0, S.K, plan.n_chunks)
+    choice[:S.K] = np.arange(S.K)
+    rg = RG.RowGroupSet(dcols, plan.chunks(), choice)
+    rg.decode()
+    torch.cuda.synchronize()
+    for o, (t, _) in zip(rg.outputs, dcols):
+        assert torch.equal(o, t)
+    rg.close()
     plan.close()
