@@ -17,6 +17,7 @@
 #include "fls_page.h"
 #include "fls_runtime.h"
 
+#include <algorithm>
 #include <cstring>
 #include <cuda_runtime.h>
 #include <mutex>
@@ -221,6 +222,39 @@ int encode_t(const T* in, uint64_t n, uint64_t cap, uint8_t* out, uint64_t* out_
 	return cudaStreamSynchronize(s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
 }
 
+// The three streams of the host decode pipeline of the current device: copies in, decode, copies out.
+struct HostPipe {
+	cudaStream_t in = nullptr, dec = nullptr, out = nullptr;
+};
+HostPipe* host_pipe() {
+	static HostPipe   p[64];
+	static std::mutex mu;
+	int               d = 0;
+	if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= 64) { return nullptr; }
+	std::lock_guard<std::mutex> lk(mu);
+	HostPipe&                   h = p[d];
+	if (!h.in) {
+		if (cudaStreamCreateWithFlags(&h.in, cudaStreamNonBlocking) != cudaSuccess ||
+		    cudaStreamCreateWithFlags(&h.dec, cudaStreamNonBlocking) != cudaSuccess ||
+		    cudaStreamCreateWithFlags(&h.out, cudaStreamNonBlocking) != cudaSuccess) {
+			h.in = nullptr;
+			return nullptr;
+		}
+		// this process's stream-ordered allocations keep their memory between calls instead of returning it
+		// at every synchronisation (a call maps its staging buffers once, not on every page)
+		cudaMemPool_t pool = nullptr;
+		uint64_t      keep = ~0ull;
+		if (cudaDeviceGetDefaultMemPool(&pool, d) == cudaSuccess) {
+			cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+		}
+	}
+	return &h;
+}
+
+// Decode a page held in host memory into host memory.  The header is parsed from the host copy; the vectors
+// go through in chunks of about 8 MB of output: each chunk's slice of every page buffer is copied in on one
+// stream, decoded on a second (a queue of the chunk's vector ids) and copied out on a third, so the copies in
+// both directions and the kernels overlap (with pinned host buffers).
 int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_t out_cap, uint8_t dt,
                      uint64_t* n_values) {
 	const int w = value_width_of(dt);
@@ -233,28 +267,87 @@ int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_
 	if (computed > page_size) { return FLS_ERR_FORMAT; }
 	rc = finish_page_info(&pi, page_size);
 	if (rc != FLS_OK) { return rc; }
-	if (pi.layout->post != POST_NONE) { return FLS_ERR_FORMAT; } // the C API carries no dictionary
-	const uint64_t out_bytes = static_cast<uint64_t>(pi.vec_c) * 1024 * (w / 8);
+	// the C API carries no dictionary
+	if (pi.layout->post == POST_DICT || pi.layout->post == POST_RLE_DICT) { return FLS_ERR_FORMAT; }
+	const uint64_t sz        = static_cast<uint64_t>(w / 8);
+	const uint64_t out_bytes = static_cast<uint64_t>(pi.vec_c) * 1024 * sz;
 	if (n_values) { *n_values = static_cast<uint64_t>(pi.vec_c) * 1024; }
 	if (out_cap < out_bytes || !out) { return FLS_ERR_ARG; }
 	if (pi.vec_c == 0) { return FLS_OK; }
-	cudaStream_t s = api_stream();
-	if (!s) { return FLS_ERR_CUDA; }
+	HostPipe* hp = host_pipe();
+	if (!hp) { return FLS_ERR_CUDA; }
 	const uint32_t shift = static_cast<uint32_t>((16 - pi.off[pi.layout->ib_packed] % 16) % 16);
-	DevBuf         d_page(s), d_out(s);
-	if (!d_page.alloc(page_size + 32) || !d_out.alloc(out_bytes)) { return FLS_ERR_CUDA; }
+	DevBuf         d_page(hp->in), d_out(hp->in), d_queue(hp->in);
+	if (!d_page.alloc(page_size + 32) || !d_out.alloc(out_bytes) || !d_queue.alloc(4ull * pi.vec_c)) {
+		return FLS_ERR_CUDA;
+	}
 	uint8_t* dp = d_page.as<uint8_t>() + shift;
-	cudaMemcpyAsync(dp, page, page_size, cudaMemcpyHostToDevice, s);
-	fls_page_column c {};
-	c.d_page    = dp;
-	c.page_size = page_size;
-	c.data_type = dt;
-	c.order     = FLS_ORIGINAL;
-	c.d_out     = d_out.p;
-	rc          = fls_gpu_decode_pages(&c, 1, s);
+	ColDesc  c {};
+	rc = build_page_column(pi, dp, w, nullptr, 0, FLS_ORIGINAL, d_out.as<uint8_t>(), &c);
 	if (rc != FLS_OK) { return rc; }
-	cudaMemcpyAsync(out, d_out.p, out_bytes, cudaMemcpyDeviceToHost, s);
-	return cudaStreamSynchronize(s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
+	// work items: vector ids (the single column is the plan's inline column)
+	std::vector<uint32_t> ids(pi.vec_c);
+	for (uint32_t v = 0; v < pi.vec_c; ++v) { ids[v] = v; }
+	auto ep = [&](uint32_t v, uint32_t b) -> uint64_t {
+		if (v == 0) { return 0; }
+		uint32_t x;
+		std::memcpy(&x, page + pi.ep_off + 4ull * ((v - 1) * pi.arr_c + b), 4);
+		return x;
+	};
+	const uint64_t chunk_vec = std::max<uint64_t>(1, (8ull << 20) / (1024 * sz));
+	const uint32_t n_chunks  = static_cast<uint32_t>((pi.vec_c + chunk_vec - 1) / chunk_vec);
+	std::vector<cudaEvent_t> ev(2 * n_chunks, nullptr);
+	for (auto& e : ev) {
+		if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) { return FLS_ERR_CUDA; }
+	}
+	struct EvGuard {
+		std::vector<cudaEvent_t>& ev;
+		~EvGuard() {
+			for (auto e : ev) {
+				if (e) { cudaEventDestroy(e); }
+			}
+		}
+	} guard {ev};
+	const Family fam = pi.layout->post == POST_NONE ? Family::NUM : Family::GATHER;
+	// page header, buffer offsets and entry points first, with the queue
+	if (cudaMemcpyAsync(dp, page, pi.meta_sz, cudaMemcpyHostToDevice, hp->in) != cudaSuccess ||
+	    cudaMemcpyAsync(d_queue.p, ids.data(), 4ull * pi.vec_c, cudaMemcpyHostToDevice, hp->in) != cudaSuccess) {
+		return FLS_ERR_CUDA;
+	}
+	for (uint32_t k = 0; k < n_chunks; ++k) {
+		const uint32_t v0 = static_cast<uint32_t>(k * chunk_vec);
+		const uint32_t v1 = static_cast<uint32_t>(std::min<uint64_t>(pi.vec_c, v0 + chunk_vec));
+		for (uint32_t b = 0; b < pi.arr_c; ++b) {
+			const uint64_t lo = pi.off[b] + ep(v0, b);
+			const uint64_t hi = v1 < pi.vec_c ? pi.off[b] + ep(v1, b) : pi.off[b] + pi.size[b];
+			if (hi > lo && hi <= page_size &&
+			    cudaMemcpyAsync(dp + lo, page + lo, hi - lo, cudaMemcpyHostToDevice, hp->in) != cudaSuccess) {
+				return FLS_ERR_CUDA;
+			}
+		}
+		if (cudaEventRecord(ev[2 * k], hp->in) != cudaSuccess || cudaStreamWaitEvent(hp->dec, ev[2 * k], 0) != cudaSuccess) {
+			return FLS_ERR_CUDA;
+		}
+		DecodeArgs a {};
+		a.col0      = c;
+		a.queue     = d_queue.as<uint32_t>() + v0;
+		a.n_items   = v1 - v0;
+		a.col_shift = 16;
+		if (launch_decode(fam, a, hp->dec) != cudaSuccess) { return FLS_ERR_CUDA; }
+		if (cudaEventRecord(ev[2 * k + 1], hp->dec) != cudaSuccess ||
+		    cudaStreamWaitEvent(hp->out, ev[2 * k + 1], 0) != cudaSuccess) {
+			return FLS_ERR_CUDA;
+		}
+		const uint64_t o0 = static_cast<uint64_t>(v0) * 1024 * sz, ob = static_cast<uint64_t>(v1 - v0) * 1024 * sz;
+		if (cudaMemcpyAsync(static_cast<uint8_t*>(out) + o0, d_out.as<uint8_t>() + o0, ob, cudaMemcpyDeviceToHost,
+		                    hp->out) != cudaSuccess) {
+			return FLS_ERR_CUDA;
+		}
+	}
+	// the buffers are freed on the copy-in stream: order it after the copies out
+	const bool ok = cudaEventRecord(ev[0], hp->out) == cudaSuccess && cudaStreamWaitEvent(hp->in, ev[0], 0) == cudaSuccess &&
+	                cudaStreamSynchronize(hp->out) == cudaSuccess;
+	return ok ? FLS_OK : FLS_ERR_CUDA;
 }
 
 } // namespace

@@ -158,3 +158,29 @@ def test_page_plan_equals_direct_decode(cuda, col_golden):
         for o, w in zip(outs, wants):
             assert np.array_equal(o.cpu().numpy(), w)
     plan.close()
+
+
+@pytest.mark.parametrize("expr", [1, 11, 6])
+def test_c_api_decode_pipelines_large_pages(cuda, expr):
+    """decode_to_memory of a page spanning several pipeline chunks (u64: 1024 vectors per chunk; 3000 vectors
+    leave a partial last chunk), from pinned and from pageable host memory."""
+    import torch
+
+    from fastlanes_b200 import pages
+
+    rng = np.random.default_rng(expr)
+    if expr == 6:
+        runs = rng.geometric(1 / 24, 200000)
+        x = np.repeat(rng.integers(-10**12, 10**12, runs.size), runs)[: 3000 * 1024].astype(np.int64)
+    elif expr == 11:
+        x = (1_600_000_000_000_000_000 + np.cumsum(rng.geometric(0.1, 3000 * 1024))).astype(np.int64)
+    else:
+        x = rng.integers(-2**40, 2**40, 3000 * 1024).astype(np.int64)
+    page, _ = pages.encode_from_memory(x, pages.INT64, expr)
+    assert np.array_equal(pages.decode_to_memory(page, pages.INT64), x)
+    hp = torch.from_numpy(page).pin_memory()
+    ho = torch.zeros(x.size, dtype=torch.int64).pin_memory()
+    from fastlanes_b200 import _lib
+
+    _lib.lib.decode_to_memory(hp.data_ptr(), ho.data_ptr(), pages.INT64)
+    assert np.array_equal(ho.numpy(), x)
