@@ -72,6 +72,7 @@ cudaError_t launch_decode(Family fam, const DecodeArgs& args, cudaStream_t strea
 	if (a.n_items == 0) { return cudaSuccess; }
 	bool narrow = a.cols == nullptr && a.col0.ws <= 32 && a.col0.e <= 4;
 	switch (fam) {
+	case Family::NUM_NARROW: return launch_family<FLS_NUM32>(a, stream, d->sm_count, grid_override);
 	case Family::NUM:
 		return narrow ? launch_family<FLS_NUM32>(a, stream, d->sm_count, grid_override)
 		              : launch_family<FLS_NUM64>(a, stream, d->sm_count, grid_override);
@@ -89,6 +90,11 @@ void family_geometry(Family fam, int* threads, int* smem, int* ctas_per_sm) {
 		*ctas_per_sm = per;
 	};
 	switch (fam) {
+	case Family::NUM_NARROW: {
+		using G = Geometry<FLS_NUM32>;
+		fill(G::kThreads, G::kSmem, reinterpret_cast<const void*>(k_decode<FLS_NUM32>));
+		break;
+	}
 	case Family::NUM: {
 		using G = Geometry<FLS_NUM64>;
 		fill(G::kThreads, G::kSmem, reinterpret_cast<const void*>(k_decode<FLS_NUM64>));
@@ -382,6 +388,9 @@ struct fls_plan {
 	Family    family   = Family::NUM;
 	uint32_t  col_shift = 24;
 	ColDesc   col0 {};
+	// items [0, split) decode with `family`, items [split, n_items) with fam_b (0: one launch)
+	uint64_t  split = 0;
+	Family    fam_b = Family::GATHER;
 };
 
 namespace flsgpu {
@@ -392,6 +401,31 @@ int make_plan_object(const std::vector<ColDesc>& descs, const std::vector<uint32
 	p->n_cols    = static_cast<uint32_t>(descs.size());
 	p->family    = fam;
 	p->col_shift = col_shift;
+	if (descs.size() > 1 && !queue.empty()) {
+		// a queue ordered family-major (plain streams first, then gathers) decodes as up to two launches, each
+		// on the kernel specialised for its items, instead of one launch of the catch-all kernel
+		auto     col   = [&](uint32_t it) -> const ColDesc& { return descs[it >> col_shift]; };
+		uint64_t split = 0;
+		while (split < queue.size() && col(queue[split]).post == POST_NONE) { ++split; }
+		bool ordered = true, narrow = true;
+		for (uint64_t i = 0; i < queue.size(); ++i) {
+			const ColDesc& c = col(queue[i]);
+			if ((i < split) != (c.post == POST_NONE)) { ordered = false; }
+			if (i < split && (c.ws > 32 || c.e > 4)) { narrow = false; }
+		}
+		if (ordered) {
+			const Family num = narrow ? Family::NUM_NARROW : Family::NUM;
+			if (split == queue.size()) {
+				p->family = num;
+			} else if (split == 0) {
+				p->family = Family::GATHER;
+			} else {
+				p->family = num;
+				p->fam_b  = Family::GATHER;
+				p->split  = split;
+			}
+		}
+	}
 	if (descs.size() == 1) {
 		// one column: the queue is implicit (vector v = item v)
 		p->col0    = descs[0];
@@ -513,7 +547,13 @@ int fls_plan_decode_grid(const fls_plan* p, int grid, fls_stream_t stream) {
 	a.n_items   = p->n_items;
 	a.col_shift = p->col_shift;
 	a.col0      = p->col0;
-	return to_status(launch_decode(p->family, a, static_cast<cudaStream_t>(stream), grid));
+	if (p->split == 0) { return to_status(launch_decode(p->family, a, static_cast<cudaStream_t>(stream), grid)); }
+	DecodeArgs b = a;
+	a.n_items    = p->split;
+	b.queue      = p->d_queue + p->split;
+	b.n_items    = p->n_items - p->split;
+	const int rc = to_status(launch_decode(p->family, a, static_cast<cudaStream_t>(stream), grid));
+	return rc != FLS_OK ? rc : to_status(launch_decode(p->fam_b, b, static_cast<cudaStream_t>(stream), grid));
 }
 
 int fls_plan_decode(const fls_plan* p, fls_stream_t stream) { return fls_plan_decode_grid(p, 0, stream); }

@@ -212,9 +212,11 @@ static int describe_pages(const fls_page_column* cols, uint32_t n_cols, std::vec
 	}
 	// group the work items by kernel specialisation so that warps run long stretches of one code path (the
 	// outputs do not depend on the order)
+	// family-major: plain streams first, then gathers (a plan then launches each family's own kernel)
 	auto key = [&](uint32_t it) {
 		const ColDesc& c = (*descs)[it >> kPageShift];
-		return (c.ws << 24) | (c.e << 16) | (c.enc << 8) | (c.post << 4) | c.order;
+		return ((c.post != POST_NONE ? 1u : 0u) << 31) | (static_cast<uint32_t>(c.ws) << 24) | (c.e << 16) |
+		       (c.enc << 8) | (c.post << 4) | c.order;
 	};
 	if (n_cols > 1) {
 		std::stable_sort(queue->begin(), queue->end(), [&](uint32_t x, uint32_t y) { return key(x) < key(y); });

@@ -11,9 +11,10 @@ struct fls_plan; // the opaque plan of include/fls_b200.h
 namespace flsgpu {
 
 enum class Family : int {
-	NUM    = 0, // streams up to 64 bits, no gather (FFOR / DELTA / raw, incl. primitive API)
-	GATHER = 1, // streams up to 32 bits with RLE run values staged and/or a dictionary gather, outputs up to 8 B
-	ANY    = 2, // everything (mixed row-group batches)
+	NUM        = 0, // streams up to 64 bits, no gather (FFOR / DELTA / raw, incl. primitive API)
+	GATHER     = 1, // streams up to 32 bits with RLE run values staged and/or a dictionary gather, outputs up to 8 B
+	ANY        = 2, // everything
+	NUM_NARROW = 3, // NUM with every stream and output at most 32 bits
 };
 
 // Per-device state: SM count and the library-owned status word.
