@@ -16,7 +16,8 @@ namespace flsgpu {
 // ---------------------------------------------------------------------------------------------------------
 #define FLS_NUM64 64, 0u, 8, 12, 2
 #define FLS_NUM32 32, 0u, 4, 15, 3
-#define FLS_GATHER 32, 8320u, 8, 6, 2
+#define FLS_GATHER 32, 0u, 8, 10, 2
+#define FLS_GATHER32 32, 0u, 4, 12, 2
 #define FLS_ANY 64, 8320u, 8, 6, 2
 
 template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES>
@@ -77,6 +78,7 @@ cudaError_t launch_decode(Family fam, const DecodeArgs& args, cudaStream_t strea
 		return narrow ? launch_family<FLS_NUM32>(a, stream, d->sm_count, grid_override)
 		              : launch_family<FLS_NUM64>(a, stream, d->sm_count, grid_override);
 	case Family::GATHER: return launch_family<FLS_GATHER>(a, stream, d->sm_count, grid_override);
+	case Family::GATHER_NARROW: return launch_family<FLS_GATHER32>(a, stream, d->sm_count, grid_override);
 	default: return launch_family<FLS_ANY>(a, stream, d->sm_count, grid_override);
 	}
 }
@@ -103,6 +105,11 @@ void family_geometry(Family fam, int* threads, int* smem, int* ctas_per_sm) {
 	case Family::GATHER: {
 		using G = Geometry<FLS_GATHER>;
 		fill(G::kThreads, G::kSmem, reinterpret_cast<const void*>(k_decode<FLS_GATHER>));
+		break;
+	}
+	case Family::GATHER_NARROW: {
+		using G = Geometry<FLS_GATHER32>;
+		fill(G::kThreads, G::kSmem, reinterpret_cast<const void*>(k_decode<FLS_GATHER32>));
 		break;
 	}
 	default: {
@@ -394,6 +401,39 @@ struct fls_plan {
 };
 
 namespace flsgpu {
+bool plan_segments(const std::vector<ColDesc>& descs, const std::vector<uint32_t>& queue, uint32_t col_shift,
+                   Family* fam_a, uint64_t* split, Family* fam_b) {
+	// a queue ordered family-major decodes as up to two launches, each on the kernel specialised for its
+	// items, instead of one launch of the catch-all kernel
+	auto     col = [&](uint32_t it) -> const ColDesc& { return descs.size() == 1 ? descs[0] : descs[it >> col_shift]; };
+	uint64_t s   = 0;
+	while (s < queue.size() && col(queue[s]).post == POST_NONE) { ++s; }
+	bool narrow_num = true, narrow_gather = true;
+	for (uint64_t i = 0; i < queue.size(); ++i) {
+		const ColDesc& c = col(queue[i]);
+		if ((i < s) != (c.post == POST_NONE)) {
+			*fam_a = Family::ANY;
+			*split = 0;
+			return false;
+		}
+		if (i < s && (c.ws > 32 || c.e > 4)) { narrow_num = false; }
+		if (i >= s && (c.ws > 32 || c.e > 4)) { narrow_gather = false; }
+	}
+	const Family num    = narrow_num ? Family::NUM_NARROW : Family::NUM;
+	const Family gather = narrow_gather ? Family::GATHER_NARROW : Family::GATHER;
+	*split              = 0;
+	if (s == queue.size()) {
+		*fam_a = num;
+	} else if (s == 0) {
+		*fam_a = gather;
+	} else {
+		*fam_a = num;
+		*fam_b = gather;
+		*split = s;
+	}
+	return true;
+}
+
 int make_plan_object(const std::vector<ColDesc>& descs, const std::vector<uint32_t>& queue, Family fam,
                      uint32_t col_shift, ::fls_plan** out) {
 	std::unique_ptr<fls_plan> p(new fls_plan());
@@ -401,29 +441,13 @@ int make_plan_object(const std::vector<ColDesc>& descs, const std::vector<uint32
 	p->n_cols    = static_cast<uint32_t>(descs.size());
 	p->family    = fam;
 	p->col_shift = col_shift;
-	if (descs.size() > 1 && !queue.empty()) {
-		// a queue ordered family-major (plain streams first, then gathers) decodes as up to two launches, each
-		// on the kernel specialised for its items, instead of one launch of the catch-all kernel
-		auto     col   = [&](uint32_t it) -> const ColDesc& { return descs[it >> col_shift]; };
+	if (!queue.empty()) {
+		Family   a = fam, b = Family::GATHER;
 		uint64_t split = 0;
-		while (split < queue.size() && col(queue[split]).post == POST_NONE) { ++split; }
-		bool ordered = true, narrow = true;
-		for (uint64_t i = 0; i < queue.size(); ++i) {
-			const ColDesc& c = col(queue[i]);
-			if ((i < split) != (c.post == POST_NONE)) { ordered = false; }
-			if (i < split && (c.ws > 32 || c.e > 4)) { narrow = false; }
-		}
-		if (ordered) {
-			const Family num = narrow ? Family::NUM_NARROW : Family::NUM;
-			if (split == queue.size()) {
-				p->family = num;
-			} else if (split == 0) {
-				p->family = Family::GATHER;
-			} else {
-				p->family = num;
-				p->fam_b  = Family::GATHER;
-				p->split  = split;
-			}
+		if (plan_segments(descs, queue, col_shift, &a, &split, &b)) {
+			p->family = a;
+			p->fam_b  = b;
+			p->split  = split;
 		}
 	}
 	if (descs.size() == 1) {

@@ -46,6 +46,10 @@ __device__ __forceinline__ uint64_t ld_le(const uint8_t* p, uint32_t n) {
 		default: return *reinterpret_cast<const uint64_t*>(p);
 		}
 	}
+	if (n == 8 && (a & 3u) == 0) {
+		const uint32_t* w = reinterpret_cast<const uint32_t*>(p);
+		return static_cast<uint64_t>(w[0]) | (static_cast<uint64_t>(w[1]) << 32);
+	}
 	uint64_t x = 0;
 	for (uint32_t i = 0; i < n; ++i) { x |= static_cast<uint64_t>(p[i]) << (8 * i); }
 	return x;
@@ -190,6 +194,8 @@ __device__ __forceinline__ void issue(const Plan& p, uint8_t* stage, uint8_t* gs
 		if (tma_pk) { bulk_g2s(stage, p.src, p.bytes, bar); }
 		if (gwindow) { bulk_g2s(gstage, p.gsrc - p.ghead, gwindow, bar); }
 		if (lbtma) { bulk_g2s(lbstage, p.lane_bases - lbhead, lbbytes, bar); }
+		// without a staging area the run values are gathered from global memory: start them towards L2 now
+		if (GSTAGE == 0 && p.ok && p.gbytes > 0) { bulk_prefetch_l2(p.gsrc - p.ghead, (p.ghead + p.gbytes + 15u) & ~15u); }
 	}
 }
 
@@ -372,7 +378,8 @@ __device__ __forceinline__ void store_vector(const typename OutT<E>::T (&o)[32],
 // ---------------------------------------------------------------------------------------------------------
 // Full decode of one staged vector.
 // ---------------------------------------------------------------------------------------------------------
-template <int WS, int E>
+// GSMEM: RLE run values / run codes staged in shared memory at gstage + ghead (else read from p.gsrc).
+template <int WS, int E, bool GSMEM = true>
 __device__ __forceinline__ void decode_vector(const Plan& p, const uint8_t* stage, const uint8_t* gstage, uint8_t* ost,
                                               uint32_t t, int* status) {
 	using ST = typename StreamT<WS>::T;
@@ -386,23 +393,25 @@ __device__ __forceinline__ void decode_vector(const Plan& p, const uint8_t* stag
 		for (int i = 0; i < 32; ++i) { o[i] = static_cast<OT>(v[i]); }
 	} else if (p.post == POST_RLE) {
 		// run values keep the byte alignment they have inside the page
-		const uint8_t* vals = gstage + p.ghead;
+		const uint8_t* vals = GSMEM ? gstage + p.ghead : p.gsrc;
 #pragma unroll
 		for (int i = 0; i < 32; ++i) {
 			const uint32_t idx = static_cast<uint32_t>(v[i]);
 			const bool     in  = idx < p.n_runs;
 			bad |= !in;
-			o[i] = in ? static_cast<OT>(sld<E>(vals + static_cast<uint64_t>(idx) * E)) : OT(0);
+			const uint8_t* a = vals + static_cast<uint64_t>(idx) * E;
+			o[i]             = !in ? OT(0) : GSMEM ? static_cast<OT>(sld<E>(a)) : static_cast<OT>(ld_le(a, E));
 		}
 	} else {
-		const uint8_t* codes = gstage + p.ghead;
+		const uint8_t* codes = GSMEM ? gstage + p.ghead : p.gsrc;
 #pragma unroll
 		for (int i = 0; i < 32; ++i) {
 			uint32_t code = static_cast<uint32_t>(v[i]);
 			if (p.post == POST_RLE_DICT) {
-				const bool in = code < p.n_runs;
+				const bool     in = code < p.n_runs;
+				const uint8_t* a  = codes + 4ull * code;
 				bad |= !in;
-				code = in ? sld4(codes + 4ull * code) : 0u;
+				code = !in ? 0u : GSMEM ? sld4(a) : static_cast<uint32_t>(ld_le(a, 4));
 			}
 			const bool in = code < p.entry_c;
 			bad |= !in;
@@ -507,25 +516,25 @@ template <int MAXWS, uint32_t GSTAGE, int EMAX>
 __device__ __forceinline__ void decode_dispatch(const Plan& p, uint8_t* st, const uint8_t* gs, uint32_t lane,
                                                 int* status) {
 	if (p.ws == 64) {
-		if constexpr (MAXWS >= 64) { decode_vector<64, 8>(p, st, gs, st, lane, status); }
+		if constexpr (MAXWS >= 64) { decode_vector<64, 8, (GSTAGE > 0)>(p, st, gs, st, lane, status); }
 	} else if (p.ws == 32) {
 		if constexpr (MAXWS >= 32) {
 			if (p.e == 8) {
-				if constexpr (EMAX >= 8) { decode_vector<32, 8>(p, st, gs, st, lane, status); }
+				if constexpr (EMAX >= 8) { decode_vector<32, 8, (GSTAGE > 0)>(p, st, gs, st, lane, status); }
 			} else {
-				decode_vector<32, 4>(p, st, gs, st, lane, status);
+				decode_vector<32, 4, (GSTAGE > 0)>(p, st, gs, st, lane, status);
 			}
 		}
 	} else if (p.ws == 16) {
 		if (p.e == 8) {
-			if constexpr (EMAX >= 8) { decode_vector<16, 8>(p, st, gs, st, lane, status); }
+			if constexpr (EMAX >= 8) { decode_vector<16, 8, (GSTAGE > 0)>(p, st, gs, st, lane, status); }
 		} else if (p.e == 4) {
-			if constexpr (EMAX >= 4) { decode_vector<16, 4>(p, st, gs, st, lane, status); }
+			if constexpr (EMAX >= 4) { decode_vector<16, 4, (GSTAGE > 0)>(p, st, gs, st, lane, status); }
 		} else {
-			decode_vector<16, 2>(p, st, gs, st, lane, status);
+			decode_vector<16, 2, (GSTAGE > 0)>(p, st, gs, st, lane, status);
 		}
 	} else {
-		decode_vector<8, 1>(p, st, gs, st, lane, status);
+		decode_vector<8, 1, (GSTAGE > 0)>(p, st, gs, st, lane, status);
 	}
 }
 

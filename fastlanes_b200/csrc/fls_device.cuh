@@ -48,6 +48,11 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 	             : "memory");
 }
 
+// Bulk prefetch of a global range into L2 (no completion, no shared memory); 16-byte aligned start and size.
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
+	asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 	uint32_t ok;
 	asm volatile(

@@ -308,7 +308,9 @@ int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_
 			}
 		}
 	} guard {ev};
-	const Family fam = pi.layout->post == POST_NONE ? Family::NUM : Family::GATHER;
+	const Family fam = pi.layout->post == POST_NONE ? Family::NUM
+	                   : c.e <= 4                   ? Family::GATHER_NARROW
+	                                                : Family::GATHER;
 	// page header, buffer offsets and entry points first, with the queue
 	if (cudaMemcpyAsync(dp, page, pi.meta_sz, cudaMemcpyHostToDevice, hp->in) != cudaSuccess ||
 	    cudaMemcpyAsync(d_queue.p, ids.data(), 4ull * pi.vec_c, cudaMemcpyHostToDevice, hp->in) != cudaSuccess) {

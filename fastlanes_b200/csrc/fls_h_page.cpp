@@ -236,10 +236,13 @@ int fls_gpu_decode_pages(const fls_page_column* cols, uint32_t n_cols, fls_strea
 	if (queue.empty()) { return FLS_OK; }
 	DecodeArgs   a {};
 	a.col_shift = kPageShift;
+	Family   fa = fam, fb = Family::GATHER;
+	uint64_t split = 0;
+	plan_segments(descs, queue, kPageShift, &fa, &split, &fb);
 	if (n_cols == 1) {
 		a.col0    = descs[0];
 		a.n_items = queue.size();
-		return launch_decode(fam, a, s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
+		return launch_decode(fa, a, s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
 	}
 	ColDesc*  d_cols  = nullptr;
 	uint32_t* d_queue = nullptr;
@@ -249,9 +252,14 @@ int fls_gpu_decode_pages(const fls_page_column* cols, uint32_t n_cols, fls_strea
 	cudaMemcpyAsync(d_queue, queue.data(), sizeof(uint32_t) * queue.size(), cudaMemcpyHostToDevice, s);
 	a.cols    = d_cols;
 	a.queue   = d_queue;
-	a.n_items = queue.size();
+	a.n_items = split ? split : queue.size();
 	// copies from pageable host memory are staged before cudaMemcpyAsync returns, so descs/queue may go away
-	const cudaError_t e = launch_decode(fam, a, s);
+	cudaError_t e = launch_decode(fa, a, s);
+	if (e == cudaSuccess && split) {
+		a.queue   = d_queue + split;
+		a.n_items = queue.size() - split;
+		e         = launch_decode(fb, a, s);
+	}
 	cudaFreeAsync(d_cols, s);
 	cudaFreeAsync(d_queue, s);
 	return e == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;

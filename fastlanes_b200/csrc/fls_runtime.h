@@ -13,8 +13,9 @@ namespace flsgpu {
 enum class Family : int {
 	NUM        = 0, // streams up to 64 bits, no gather (FFOR / DELTA / raw, incl. primitive API)
 	GATHER     = 1, // streams up to 32 bits with RLE run values staged and/or a dictionary gather, outputs up to 8 B
-	ANY        = 2, // everything
-	NUM_NARROW = 3, // NUM with every stream and output at most 32 bits
+	ANY           = 2, // everything
+	NUM_NARROW    = 3, // NUM with every stream and output at most 32 bits
+	GATHER_NARROW = 4, // GATHER with outputs of at most 4 bytes
 };
 
 // Per-device state: SM count and the library-owned status word.
@@ -32,6 +33,12 @@ cudaError_t launch_decode(Family fam, const DecodeArgs& args, cudaStream_t strea
 
 // Geometry of a family (threads per CTA, dynamic shared memory per CTA, CTAs resident per SM).
 void family_geometry(Family fam, int* threads, int* smem, int* ctas_per_sm);
+
+// Kernel families for a queue: when the items are ordered family-major (plain streams first, then gathers),
+// items [0, *split) run on *fam_a and [*split, n) on *fam_b (*split = 0: all on *fam_a).  Returns false (and
+// Family::ANY) for an unordered queue.
+bool plan_segments(const std::vector<ColDesc>& descs, const std::vector<uint32_t>& queue, uint32_t col_shift,
+                   Family* fam_a, uint64_t* split, Family* fam_b);
 
 // Build a plan object from descriptors + queue of (col << col_shift | vec) items (uploads both; a single column
 // without a queue stays inline).
