@@ -11,6 +11,23 @@ import torch
 from . import pages as PG
 from .select import POOL_IDS
 
+
+def shard_chunks(chunk_bytes, world_size):
+    """Contiguous chunk ranges [begin, end) for each of world_size ranks with about equal bytes each (chunks are
+    independent, so ranks decode their ranges with no exchange).  Every rank computes the same split."""
+    w = np.asarray(chunk_bytes, np.float64)
+    if world_size < 1:
+        raise ValueError("world_size must be positive")
+    prefix = np.concatenate([[0.0], np.cumsum(w)])
+    total = prefix[-1]
+    cuts = [0]
+    for r in range(1, world_size):
+        # first boundary at or after r / world_size of the bytes, never before the previous cut
+        cuts.append(max(cuts[-1], int(np.searchsorted(prefix, total * r / world_size, side="left"))))
+    cuts.append(len(w))
+    return [(cuts[r], cuts[r + 1]) for r in range(world_size)]
+
+
 _DT = {(4, True): PG.INT32, (4, False): PG.UINT32, (8, True): PG.INT64, (8, False): PG.UINT64}
 _UNSIGNED = {4: np.uint32, 8: np.uint64}
 
@@ -32,9 +49,12 @@ class RowGroupSet:
     choice: candidate per chunk.  The pages live in one device buffer, each at a 16-byte aligned offset
     (fls_page_placement), the dictionaries in another; outputs are one tensor per column (original order)."""
 
-    def __init__(self, columns, chunks, choice, device="cuda"):
+    def __init__(self, columns, chunks, choice, device="cuda", chunk_range=None):
         col, first, count = chunks
         choice = np.asarray(choice)
+        if chunk_range is not None:  # one rank's share (shard_chunks): only these chunks are encoded and decoded
+            b, e = chunk_range
+            col, first, count, choice = col[b:e], first[b:e], count[b:e], choice[b:e]
         host = [t.cpu().numpy() for t, _ in columns]
         self.signed = [s for _, s in columns]
         pages, dicts, self.page_bytes, self.dict_bytes = [], [], 0, 0
@@ -81,13 +101,16 @@ class RowGroupSet:
                 dict_size=0 if dicts[c] is None else dicts[c].size,
                 data_type=_DT[(t.element_size(), self.signed[col[c]])], order=1,
                 d_out=t.data_ptr() + int(first[c]) * 1024 * t.element_size()))
-        self.plan = PG.PagePlan(self.columns)
-        self.values = sum(t.numel() for t in self.outputs)
-        self.value_bytes = sum(t.numel() * t.element_size() for t in self.outputs)
+        self.plan = PG.PagePlan(self.columns) if len(col) else None
+        self.values = int(sum(int(n) * 1024 for n in count))
+        self.value_bytes = int(sum(int(count[c]) * 1024 * self.outputs[col[c]].element_size() for c in range(len(col))))
 
     def decode(self, stream=None):
-        """All chunks of all columns: one persistent kernel launch."""
+        """Every chunk of the set: one plan, one persistent launch per kernel family present."""
+        if self.plan is None:
+            return
         self.plan.decode(stream)
 
     def close(self):
-        self.plan.close()
+        if self.plan is not None:
+            self.plan.close()
