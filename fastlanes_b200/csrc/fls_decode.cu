@@ -394,16 +394,30 @@ __device__ __forceinline__ void decode_vector(const Plan& p, const uint8_t* stag
 	} else if (p.post == POST_RLE) {
 		// run values keep the byte alignment they have inside the page
 		const uint8_t* vals = GSMEM ? gstage + p.ghead : p.gsrc;
+		if (!GSMEM && (reinterpret_cast<uintptr_t>(vals) & (E - 1)) == 0) {
+			// naturally aligned run values (the usual case): plain loads, no per-value alignment test
+			using VT        = typename ElemT<E>::T;
+			const VT* tvals = reinterpret_cast<const VT*>(vals);
 #pragma unroll
-		for (int i = 0; i < 32; ++i) {
-			const uint32_t idx = static_cast<uint32_t>(v[i]);
-			const bool     in  = idx < p.n_runs;
-			bad |= !in;
-			const uint8_t* a = vals + static_cast<uint64_t>(idx) * E;
-			o[i]             = !in ? OT(0) : GSMEM ? static_cast<OT>(sld<E>(a)) : static_cast<OT>(ld_le(a, E));
+			for (int i = 0; i < 32; ++i) {
+				const uint32_t idx = static_cast<uint32_t>(v[i]);
+				const bool     in  = idx < p.n_runs;
+				bad |= !in;
+				o[i] = in ? static_cast<OT>(tvals[idx]) : OT(0);
+			}
+		} else {
+#pragma unroll
+			for (int i = 0; i < 32; ++i) {
+				const uint32_t idx = static_cast<uint32_t>(v[i]);
+				const bool     in  = idx < p.n_runs;
+				bad |= !in;
+				const uint8_t* a = vals + static_cast<uint64_t>(idx) * E;
+				o[i] = !in ? OT(0) : GSMEM ? static_cast<OT>(sld<E>(a)) : static_cast<OT>(ld_le(a, E));
+			}
 		}
 	} else {
-		const uint8_t* codes = GSMEM ? gstage + p.ghead : p.gsrc;
+		const uint8_t* codes        = GSMEM ? gstage + p.ghead : p.gsrc;
+		const bool     dict_aligned = (reinterpret_cast<uintptr_t>(p.dict) & (E - 1)) == 0;
 #pragma unroll
 		for (int i = 0; i < 32; ++i) {
 			uint32_t code = static_cast<uint32_t>(v[i]);
@@ -415,7 +429,9 @@ __device__ __forceinline__ void decode_vector(const Plan& p, const uint8_t* stag
 			}
 			const bool in = code < p.entry_c;
 			bad |= !in;
-			o[i] = in ? static_cast<OT>(ld_le(p.dict + static_cast<uint64_t>(code) * E, E)) : OT(0);
+			const uint8_t* a = p.dict + static_cast<uint64_t>(code) * E;
+			o[i] = !in ? OT(0) : dict_aligned ? static_cast<OT>(*reinterpret_cast<const typename ElemT<E>::T*>(a))
+			                                  : static_cast<OT>(ld_le(a, E));
 		}
 	}
 	if (__any_sync(0xFFFFFFFFu, bad) && t == 0) { atomicOr(status, STATUS_BAD_INDEX); }
