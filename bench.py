@@ -309,8 +309,13 @@ def other_configs(dev, args):
         plan = PG.PagePlan(col)
         plan.decode()
         ok = np.array_equal(o.cpu().numpy(), values)
+        tuned = plan.autotune()
+        o.zero_()
+        plan.decode()
+        ok = ok and np.array_equal(o.cpu().numpy(), values)
         ms = device_timed(plan.decode, steps, 3)
         leg(name, workload, ms, page.size, values.nbytes, values.size, ok, 1)
+        out[name]["autotuned"] = tuned
         plan.close()
 
     page_leg("3a_delta_i64", "32Mi sorted int64 timestamps from 1.6e18, geometric(mean 10) gaps, DELTA (id 11)",
@@ -390,7 +395,10 @@ def mixed_rowgroups(dev, peak, steps):
     loss = SL.ratio_loss(sizes, choice)
     agree = float((choice == best).float().mean())
     rg = RG.RowGroupSet(cols, plan.chunks(), choice.cpu().numpy(), dev)
-    rg.decode()
+    tuned = rg.autotune()
+    for o in rg.outputs:
+        o.zero_()
+    rg.decode()  # graph replay of the plan's launches
     torch.cuda.synchronize()
     ok = all(torch.equal(o, t) for o, (t, _) in zip(rg.outputs, cols))
     ms = device_timed(rg.decode, steps, 3)
@@ -402,7 +410,7 @@ def mixed_rowgroups(dev, peak, steps):
         "value": round(write_b / (ms * 1e-3) / 1e9, 2), "unit": "GB/s", "ms_per_step": round(ms, 4),
         "decoded_values_per_s": round(rg.values / (ms * 1e-3), 1), "bytes_per_step": read_b + write_b,
         "roofline_frac": round((read_b + write_b) / (ms * 1e-3) / 1e9 / peak, 4), "parity": bool(ok),
-        "gpu_launches_per_step": 1,
+        "gpu_launches_per_step": len(tuned), "graph_launches_per_step": 1, "autotuned": tuned,
         "selection": {
             "learned_ms": round(ms_sel, 3), "wizard_ms": round(ms_wiz, 3), "speedup": round(ms_wiz / ms_sel, 1),
             "ratio_loss_pct": round(loss * 100, 4), "agreement_with_wizard": round(agree, 4),
@@ -444,6 +452,8 @@ def run_ours(args):
         c.values = None
     if P.device_status() != 0:
         raise SystemExit("device status error")
+    # the plans' geometry (warps per CTA x staging depth) picked by the autotuner on this data
+    tuned = {"transposed": plan_t.autotune(), "original": plan_o.autotune()}
 
     read_b = sum(c.algorithmic_read_bytes() for c in cols) + queue.numel() * 4
     write_b = sum(c.decoded_bytes() for c in cols)
@@ -539,7 +549,8 @@ def run_ours(args):
             "vs_baseline": None, "dtype": "u32+u64", "data": "synthetic (seeded; values base+U[0,2^bw))",
             "config": {"workload": WORKLOAD, "vectors": N32 + N64, "values": n_vals, "order": "transposed",
                        "queue": "shuffled; planner groups items by vector width (data untouched)",
-                       "l2": "inputs and outputs larger than L2, no flush", "parallelism": f"replicas{world}"},
+                       "l2": "inputs and outputs larger than L2, no flush", "parallelism": f"replicas{world}",
+                       "autotuned": tuned},
             "decoded_values_per_s": round(n_vals * world / (ms_t * 1e-3), 1),
             "queue_as_shuffled": {"ms_per_step": round(ms_k, 4),
                                   "value": round(write_b * world / (ms_k * 1e-3) / 1e9, 2), "unit": "GB/s",

@@ -14,16 +14,17 @@ namespace flsgpu {
 // ---------------------------------------------------------------------------------------------------------
 // Kernel families
 // ---------------------------------------------------------------------------------------------------------
-#define FLS_NUM64 64, 0u, 8, 12, 2
-#define FLS_NUM32 32, 0u, 4, 15, 3
-#define FLS_GATHER 32, 0u, 8, 10, 2
-#define FLS_GATHER32 32, 0u, 4, 12, 2
-#define FLS_ANY 64, 8320u, 8, 6, 2
+// <max stream width, run-value staging bytes, max output bytes, warps per CTA, staging depth, gathers>
+#define FLS_NUM64 64, 0u, 8, 12, 2, false
+#define FLS_NUM32 32, 0u, 4, 15, 3, false
+#define FLS_GATHER 32, 0u, 8, 10, 2, true
+#define FLS_GATHER32 32, 0u, 4, 12, 2, true
+#define FLS_ANY 64, 8320u, 8, 6, 2, true
 
-template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES>
+template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES, bool GATHER>
 static cudaError_t launch_family(const DecodeArgs& a, cudaStream_t s, int sm_count, int grid_override) {
-	using G            = Geometry<MAXWS, GSTAGE, EMAX, WARPS, STAGES>;
-	auto*       kfn    = k_decode<MAXWS, GSTAGE, EMAX, WARPS, STAGES>;
+	using G            = Geometry<MAXWS, GSTAGE, EMAX, WARPS, STAGES, GATHER>;
+	auto*       kfn    = k_decode<MAXWS, GSTAGE, EMAX, WARPS, STAGES, GATHER>;
 	static bool inited = false;
 	if (!inited) {
 		cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, G::kSmem);
@@ -49,6 +50,68 @@ uint64_t& launch_counter() {
 	return n;
 }
 
+// ---------------------------------------------------------------------------------------------------------
+// Geometry variants of every family (warps per CTA x staging depth); variant 0 is the default, the others are
+// what fls_plan_autotune chooses from on the plan's own data.
+// ---------------------------------------------------------------------------------------------------------
+struct Variant {
+	const char* name;
+	cudaError_t (*launch)(const DecodeArgs&, cudaStream_t, int, int);
+	const void* kernel;
+	int         threads, smem;
+};
+
+template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES, bool GATHER>
+static cudaError_t launch_variant(const DecodeArgs& a, cudaStream_t s, int sms, int grid) {
+	return launch_family<MAXWS, GSTAGE, EMAX, WARPS, STAGES, GATHER>(a, s, sms, grid);
+}
+
+#define FLS_VARIANT(label, ...)                                                                                   \
+	Variant {                                                                                                     \
+		label, launch_variant<__VA_ARGS__>, reinterpret_cast<const void*>(k_decode<__VA_ARGS__>),                 \
+		    Geometry<__VA_ARGS__>::kThreads, static_cast<int>(Geometry<__VA_ARGS__>::kSmem)                       \
+	}
+
+static const Variant kNum64[]    = {FLS_VARIANT("num64 12x2", FLS_NUM64),
+                                    FLS_VARIANT("num64 8x3", 64, 0u, 8, 8, 3, false),
+                                    FLS_VARIANT("num64 10x2", 64, 0u, 8, 10, 2, false)};
+static const Variant kNum32[]    = {FLS_VARIANT("num32 15x3", FLS_NUM32),
+                                    FLS_VARIANT("num32 16x2", 32, 0u, 4, 16, 2, false),
+                                    FLS_VARIANT("num32 10x4", 32, 0u, 4, 10, 4, false)};
+static const Variant kGather[]   = {FLS_VARIANT("gather 10x2", FLS_GATHER),
+                                    FLS_VARIANT("gather 8x3", 32, 0u, 8, 8, 3, true),
+                                    FLS_VARIANT("gather 12x2", 32, 0u, 8, 12, 2, true)};
+static const Variant kGather32[] = {FLS_VARIANT("gather32 12x2", FLS_GATHER32),
+                                    FLS_VARIANT("gather32 12x3", 32, 0u, 4, 12, 3, true),
+                                    FLS_VARIANT("gather32 16x2", 32, 0u, 4, 16, 2, true)};
+static const Variant kAny[]      = {FLS_VARIANT("any 6x2", FLS_ANY)};
+
+// The variants of a family; a NUM launch without a column array whose column is narrow runs the NUM32 kernels.
+static const Variant* family_variants(Family fam, const DecodeArgs& a, int* n) {
+	const bool narrow = a.cols == nullptr && a.col0.ws <= 32 && a.col0.e <= 4;
+	switch (fam) {
+	case Family::NUM_NARROW: *n = 3; return kNum32;
+	case Family::NUM:
+		*n = 3;
+		return narrow ? kNum32 : kNum64;
+	case Family::GATHER: *n = 3; return kGather;
+	case Family::GATHER_NARROW: *n = 3; return kGather32;
+	default: *n = 1; return kAny;
+	}
+}
+
+int family_variant_count(Family fam, const DecodeArgs& a) {
+	int n = 0;
+	family_variants(fam, a, &n);
+	return n;
+}
+
+const char* family_variant_name(Family fam, const DecodeArgs& a, int variant) {
+	int            n = 0;
+	const Variant* v = family_variants(fam, a, &n);
+	return (variant >= 0 && variant < n) ? v[variant].name : "";
+}
+
 Device* current_device() {
 	static Device     devs[64];
 	static std::mutex mu;
@@ -65,59 +128,27 @@ Device* current_device() {
 	return &d;
 }
 
-cudaError_t launch_decode(Family fam, const DecodeArgs& args, cudaStream_t stream, int grid_override) {
+cudaError_t launch_decode(Family fam, const DecodeArgs& args, cudaStream_t stream, int grid_override, int variant) {
 	Device* d = current_device();
 	if (!d) { return cudaErrorInitializationError; }
 	DecodeArgs a = args;
 	if (!a.status) { a.status = d->status; }
 	if (a.n_items == 0) { return cudaSuccess; }
-	bool narrow = a.cols == nullptr && a.col0.ws <= 32 && a.col0.e <= 4;
-	switch (fam) {
-	case Family::NUM_NARROW: return launch_family<FLS_NUM32>(a, stream, d->sm_count, grid_override);
-	case Family::NUM:
-		return narrow ? launch_family<FLS_NUM32>(a, stream, d->sm_count, grid_override)
-		              : launch_family<FLS_NUM64>(a, stream, d->sm_count, grid_override);
-	case Family::GATHER: return launch_family<FLS_GATHER>(a, stream, d->sm_count, grid_override);
-	case Family::GATHER_NARROW: return launch_family<FLS_GATHER32>(a, stream, d->sm_count, grid_override);
-	default: return launch_family<FLS_ANY>(a, stream, d->sm_count, grid_override);
-	}
+	int            n = 0;
+	const Variant* v = family_variants(fam, a, &n);
+	if (variant < 0 || variant >= n) { variant = 0; }
+	return v[variant].launch(a, stream, d->sm_count, grid_override);
 }
 
-void family_geometry(Family fam, int* threads, int* smem, int* ctas_per_sm) {
-	auto fill = [&](int th, int sm, const void* fn) {
-		*threads = th;
-		*smem    = sm;
-		int per  = 0;
-		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, th, sm);
-		*ctas_per_sm = per;
-	};
-	switch (fam) {
-	case Family::NUM_NARROW: {
-		using G = Geometry<FLS_NUM32>;
-		fill(G::kThreads, G::kSmem, reinterpret_cast<const void*>(k_decode<FLS_NUM32>));
-		break;
-	}
-	case Family::NUM: {
-		using G = Geometry<FLS_NUM64>;
-		fill(G::kThreads, G::kSmem, reinterpret_cast<const void*>(k_decode<FLS_NUM64>));
-		break;
-	}
-	case Family::GATHER: {
-		using G = Geometry<FLS_GATHER>;
-		fill(G::kThreads, G::kSmem, reinterpret_cast<const void*>(k_decode<FLS_GATHER>));
-		break;
-	}
-	case Family::GATHER_NARROW: {
-		using G = Geometry<FLS_GATHER32>;
-		fill(G::kThreads, G::kSmem, reinterpret_cast<const void*>(k_decode<FLS_GATHER32>));
-		break;
-	}
-	default: {
-		using G = Geometry<FLS_ANY>;
-		fill(G::kThreads, G::kSmem, reinterpret_cast<const void*>(k_decode<FLS_ANY>));
-		break;
-	}
-	}
+void family_geometry(Family fam, const DecodeArgs& a, int variant, int* threads, int* smem, int* ctas_per_sm) {
+	int            n = 0;
+	const Variant* v = family_variants(fam, a, &n);
+	if (variant < 0 || variant >= n) { variant = 0; }
+	*threads = v[variant].threads;
+	*smem    = v[variant].smem;
+	int per  = 0;
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, v[variant].kernel, *threads, *smem);
+	*ctas_per_sm = per;
 }
 
 // ---------------------------------------------------------------------------------------------------------
@@ -398,6 +429,9 @@ struct fls_plan {
 	// items [0, split) decode with `family`, items [split, n_items) with fam_b (0: one launch)
 	uint64_t  split = 0;
 	Family    fam_b = Family::GATHER;
+	int       variant[2] {0, 0};     // geometry variant of each segment (fls_plan_autotune)
+	cudaGraphExec_t graph = nullptr; // the segments' launches, captured by fls_plan_decode_graph
+	cudaStream_t    graph_stream = nullptr;
 };
 
 namespace flsgpu {
@@ -563,27 +597,130 @@ int fls_plan_create_ex(const fls_vector_batch* batches, uint32_t n_batches, cons
 	return FLS_OK;
 }
 
+namespace {
+
+// The launch arguments of segment `seg` (0 or 1) of a plan; false when the plan has no such segment.
+bool segment_args(const fls_plan* p, int seg, DecodeArgs* a, Family* fam) {
+	DecodeArgs x {};
+	x.cols      = p->d_cols;
+	x.queue     = p->d_queue;
+	x.col_shift = p->col_shift;
+	x.col0      = p->col0;
+	if (seg == 0) {
+		x.n_items = p->split ? p->split : p->n_items;
+		*fam      = p->family;
+	} else {
+		if (p->split == 0) { return false; }
+		x.queue   = p->d_queue + p->split;
+		x.n_items = p->n_items - p->split;
+		*fam      = p->fam_b;
+	}
+	*a = x;
+	return true;
+}
+
+int launch_segments(const fls_plan* p, int grid, cudaStream_t s) {
+	for (int seg = 0; seg < 2; ++seg) {
+		DecodeArgs a;
+		Family     fam;
+		if (!segment_args(p, seg, &a, &fam)) { break; }
+		const int rc = to_status(launch_decode(fam, a, s, grid, p->variant[seg]));
+		if (rc != FLS_OK) { return rc; }
+	}
+	return FLS_OK;
+}
+
+void drop_graph(fls_plan* p) {
+	if (p->graph) {
+		cudaGraphExecDestroy(p->graph);
+		p->graph = nullptr;
+	}
+}
+
+} // namespace
+
 int fls_plan_decode_grid(const fls_plan* p, int grid, fls_stream_t stream) {
 	if (!p) { return FLS_ERR_ARG; }
-	DecodeArgs a {};
-	a.cols    = p->d_cols;
-	a.queue   = p->d_queue;
-	a.n_items   = p->n_items;
-	a.col_shift = p->col_shift;
-	a.col0      = p->col0;
-	if (p->split == 0) { return to_status(launch_decode(p->family, a, static_cast<cudaStream_t>(stream), grid)); }
-	DecodeArgs b = a;
-	a.n_items    = p->split;
-	b.queue      = p->d_queue + p->split;
-	b.n_items    = p->n_items - p->split;
-	const int rc = to_status(launch_decode(p->family, a, static_cast<cudaStream_t>(stream), grid));
-	return rc != FLS_OK ? rc : to_status(launch_decode(p->fam_b, b, static_cast<cudaStream_t>(stream), grid));
+	return launch_segments(p, grid, static_cast<cudaStream_t>(stream));
 }
 
 int fls_plan_decode(const fls_plan* p, fls_stream_t stream) { return fls_plan_decode_grid(p, 0, stream); }
 
+int fls_plan_decode_graph(fls_plan* p, fls_stream_t stream) {
+	if (!p) { return FLS_ERR_ARG; }
+	if (!p->graph) {
+		// capture on a private stream (the legacy default stream cannot be captured); relaxed mode, since the
+		// first launch of a kernel family sets its shared-memory attribute
+		cudaStream_t cs = nullptr;
+		if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) { return FLS_ERR_CUDA; }
+		cudaGraph_t g  = nullptr;
+		int         rc = FLS_OK;
+		if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+			rc = FLS_ERR_CUDA;
+		} else {
+			const uint64_t launches = launch_counter();
+			rc                      = launch_segments(p, 0, cs);
+			launch_counter()        = launches;
+			if (cudaStreamEndCapture(cs, &g) != cudaSuccess && rc == FLS_OK) { rc = FLS_ERR_CUDA; }
+		}
+		if (rc == FLS_OK && (!g || cudaGraphInstantiate(&p->graph, g, 0) != cudaSuccess)) { rc = FLS_ERR_CUDA; }
+		if (g) { cudaGraphDestroy(g); }
+		cudaStreamDestroy(cs);
+		if (rc != FLS_OK) { return rc; }
+	}
+	if (cudaGraphLaunch(p->graph, static_cast<cudaStream_t>(stream)) != cudaSuccess) { return FLS_ERR_CUDA; }
+	launch_counter() += p->split ? 2 : 1;
+	return FLS_OK;
+}
+
+int fls_plan_autotune(fls_plan* p, int reps, fls_stream_t stream) {
+	if (!p || reps < 1) { return FLS_ERR_ARG; }
+	cudaStream_t s  = static_cast<cudaStream_t>(stream);
+	cudaEvent_t  e0 = nullptr, e1 = nullptr;
+	if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) { return FLS_ERR_CUDA; }
+	int rc = FLS_OK;
+	for (int seg = 0; seg < 2 && rc == FLS_OK; ++seg) {
+		DecodeArgs a;
+		Family     fam;
+		if (!segment_args(p, seg, &a, &fam)) { break; }
+		const int n    = family_variant_count(fam, a);
+		float     best = 0.0f;
+		int       pick = 0;
+		for (int v = 0; v < n && rc == FLS_OK; ++v) {
+			// one untimed launch (first use sets the kernel's attributes), then `reps` timed ones
+			rc = to_status(launch_decode(fam, a, s, 0, v));
+			if (rc != FLS_OK) { break; }
+			cudaEventRecord(e0, s);
+			for (int r = 0; r < reps && rc == FLS_OK; ++r) { rc = to_status(launch_decode(fam, a, s, 0, v)); }
+			cudaEventRecord(e1, s);
+			float ms = 0.0f;
+			if (rc == FLS_OK && (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)) {
+				rc = FLS_ERR_CUDA;
+			}
+			if (rc == FLS_OK && (v == 0 || ms < best)) {
+				best = ms;
+				pick = v;
+			}
+		}
+		p->variant[seg] = pick;
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	drop_graph(p);
+	return rc;
+}
+
+const char* fls_plan_variant_name(const fls_plan* p, int segment) {
+	if (!p || segment < 0 || segment > 1) { return ""; }
+	DecodeArgs a;
+	Family     fam;
+	if (!segment_args(p, segment, &a, &fam)) { return ""; }
+	return family_variant_name(fam, a, p->variant[segment]);
+}
+
 int fls_plan_destroy(fls_plan* p) {
 	if (!p) { return FLS_OK; }
+	drop_graph(p);
 	if (p->d_cols) { cudaFree(p->d_cols); }
 	if (p->d_queue) { cudaFree(p->d_queue); }
 	delete p;
@@ -592,7 +729,10 @@ int fls_plan_destroy(fls_plan* p) {
 
 int fls_plan_geometry(const fls_plan* p, int* threads, int* smem_bytes, int* ctas_per_sm) {
 	if (!p || !threads || !smem_bytes || !ctas_per_sm) { return FLS_ERR_ARG; }
-	family_geometry(p->family, threads, smem_bytes, ctas_per_sm);
+	DecodeArgs a;
+	Family     fam;
+	segment_args(p, 0, &a, &fam);
+	family_geometry(fam, a, p->variant[0], threads, smem_bytes, ctas_per_sm);
 	return FLS_OK;
 }
 

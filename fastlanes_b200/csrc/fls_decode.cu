@@ -379,7 +379,9 @@ __device__ __forceinline__ void store_vector(const typename OutT<E>::T (&o)[32],
 // Full decode of one staged vector.
 // ---------------------------------------------------------------------------------------------------------
 // GSMEM: RLE run values / run codes staged in shared memory at gstage + ghead (else read from p.gsrc).
-template <int WS, int E, bool GSMEM = true>
+// GATHER: the kernel handles RLE / DICT items (plain-stream kernels leave the gather code out and flag such an
+// item as a layout error).
+template <int WS, int E, bool GSMEM = true, bool GATHER = true>
 __device__ __forceinline__ void decode_vector(const Plan& p, const uint8_t* stage, const uint8_t* gstage, uint8_t* ost,
                                               uint32_t t, int* status) {
 	using ST = typename StreamT<WS>::T;
@@ -388,9 +390,10 @@ __device__ __forceinline__ void decode_vector(const Plan& p, const uint8_t* stag
 	decode_stream<WS>(p, reinterpret_cast<const uint32_t*>(stage), t, v);
 	OT o[32];
 	bool bad = false;
-	if (p.post == POST_NONE) {
+	if (!GATHER || p.post == POST_NONE) {
 #pragma unroll
 		for (int i = 0; i < 32; ++i) { o[i] = static_cast<OT>(v[i]); }
+		if (!GATHER && p.post != POST_NONE && t == 0) { atomicOr(status, STATUS_BAD_LAYOUT); }
 	} else if (p.post == POST_RLE) {
 		// run values keep the byte alignment they have inside the page
 		const uint8_t* vals = GSMEM ? gstage + p.ghead : p.gsrc;
@@ -513,7 +516,7 @@ __device__ __forceinline__ Plan plan_of(const DecodeArgs& a, uint64_t item) {
 // output element size.  The original-order staging reuses the stage once its packed words are in registers,
 // so a slot is max(stream, output) bytes plus the run-value window.  Plans of the warp's next 2*PB items
 // live in shared memory (64 bytes each).
-template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES>
+template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES, bool GATHER = true>
 struct Geometry {
 	static constexpr uint32_t kPB      = 16;
 	static constexpr uint32_t kStage   = MAXWS * 128u;
@@ -526,37 +529,38 @@ struct Geometry {
 	static constexpr uint32_t kSmem    = WARPS * kPerWarp + kSlack;
 	static constexpr int      kThreads = WARPS * 32;
 	static_assert(STAGES < kPB, "plans must run ahead of the copies");
+	static_assert(kSmem <= 232448u, "at most 227 KB of shared memory per CTA");
 };
 
-template <int MAXWS, uint32_t GSTAGE, int EMAX>
+template <int MAXWS, uint32_t GSTAGE, int EMAX, bool GATHER>
 __device__ __forceinline__ void decode_dispatch(const Plan& p, uint8_t* st, const uint8_t* gs, uint32_t lane,
                                                 int* status) {
 	if (p.ws == 64) {
-		if constexpr (MAXWS >= 64) { decode_vector<64, 8, (GSTAGE > 0)>(p, st, gs, st, lane, status); }
+		if constexpr (MAXWS >= 64) { decode_vector<64, 8, (GSTAGE > 0), GATHER>(p, st, gs, st, lane, status); }
 	} else if (p.ws == 32) {
 		if constexpr (MAXWS >= 32) {
 			if (p.e == 8) {
-				if constexpr (EMAX >= 8) { decode_vector<32, 8, (GSTAGE > 0)>(p, st, gs, st, lane, status); }
+				if constexpr (EMAX >= 8) { decode_vector<32, 8, (GSTAGE > 0), GATHER>(p, st, gs, st, lane, status); }
 			} else {
-				decode_vector<32, 4, (GSTAGE > 0)>(p, st, gs, st, lane, status);
+				decode_vector<32, 4, (GSTAGE > 0), GATHER>(p, st, gs, st, lane, status);
 			}
 		}
 	} else if (p.ws == 16) {
 		if (p.e == 8) {
-			if constexpr (EMAX >= 8) { decode_vector<16, 8, (GSTAGE > 0)>(p, st, gs, st, lane, status); }
+			if constexpr (EMAX >= 8) { decode_vector<16, 8, (GSTAGE > 0), GATHER>(p, st, gs, st, lane, status); }
 		} else if (p.e == 4) {
-			if constexpr (EMAX >= 4) { decode_vector<16, 4, (GSTAGE > 0)>(p, st, gs, st, lane, status); }
+			if constexpr (EMAX >= 4) { decode_vector<16, 4, (GSTAGE > 0), GATHER>(p, st, gs, st, lane, status); }
 		} else {
-			decode_vector<16, 2, (GSTAGE > 0)>(p, st, gs, st, lane, status);
+			decode_vector<16, 2, (GSTAGE > 0), GATHER>(p, st, gs, st, lane, status);
 		}
 	} else {
-		decode_vector<8, 1, (GSTAGE > 0)>(p, st, gs, st, lane, status);
+		decode_vector<8, 1, (GSTAGE > 0), GATHER>(p, st, gs, st, lane, status);
 	}
 }
 
-template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES>
+template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES, bool GATHER>
 __global__ void __launch_bounds__(WARPS * 32, 1) k_decode(const DecodeArgs a) {
-	using G = Geometry<MAXWS, GSTAGE, EMAX, WARPS, STAGES>;
+	using G = Geometry<MAXWS, GSTAGE, EMAX, WARPS, STAGES, GATHER>;
 	constexpr uint32_t PB = G::kPB;
 	extern __shared__ __align__(128) uint8_t smem[];
 	const uint32_t lane   = threadIdx.x & 31u;
@@ -621,7 +625,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_decode(const DecodeArgs a) {
 		} else {
 			// the lane bases were staged with the packed words
 			if (p.lane_bases) { p.lane_bases = lb_ptr(s) + (reinterpret_cast<uintptr_t>(p.lane_bases) & 15u); }
-			decode_dispatch<MAXWS, GSTAGE, EMAX>(p, stage_ptr(s), gstage_ptr(s), lane, a.status);
+			decode_dispatch<MAXWS, GSTAGE, EMAX, GATHER>(p, stage_ptr(s), gstage_ptr(s), lane, a.status);
 		}
 		__syncwarp();
 		issue_k(k + STAGES, s);

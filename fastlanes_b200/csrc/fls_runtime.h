@@ -28,11 +28,16 @@ struct Device {
 // Returns the state of the current device (initialising it on first use), or nullptr on a CUDA error.
 Device* current_device();
 
-// Launch the persistent decode kernel of the given family.  max_ctas_per_sm caps residency (0 = occupancy).
-cudaError_t launch_decode(Family fam, const DecodeArgs& args, cudaStream_t stream, int grid_override = 0);
+// Launch the persistent decode kernel of the given family in geometry variant `variant` (0 = the default;
+// grid_override 0 = one wave of resident CTAs).
+cudaError_t launch_decode(Family fam, const DecodeArgs& args, cudaStream_t stream, int grid_override = 0,
+                          int variant = 0);
+int         family_variant_count(Family fam, const DecodeArgs& args);
+const char* family_variant_name(Family fam, const DecodeArgs& args, int variant);
 
-// Geometry of a family (threads per CTA, dynamic shared memory per CTA, CTAs resident per SM).
-void family_geometry(Family fam, int* threads, int* smem, int* ctas_per_sm);
+// Geometry of a family variant for these launch arguments (threads per CTA, dynamic shared memory per CTA,
+// CTAs resident per SM).
+void family_geometry(Family fam, const DecodeArgs& args, int variant, int* threads, int* smem, int* ctas_per_sm);
 
 // Kernel families for a queue: when the items are ordered family-major (plain streams first, then gathers),
 // items [0, *split) run on *fam_a and [*split, n) on *fam_b (*split = 0: all on *fam_a).  Returns false (and

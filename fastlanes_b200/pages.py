@@ -60,6 +60,9 @@ _plan_pages = declare("fls_plan_create_pages", ctypes.c_int, [ctypes.POINTER(Pag
                                                                 ctypes.POINTER(_p)])
 _plan_decode = declare("fls_plan_decode", ctypes.c_int, [_p, _p])
 _plan_destroy = declare("fls_plan_destroy", ctypes.c_int, [_p])
+_plan_autotune = declare("fls_plan_autotune", ctypes.c_int, [_p, ctypes.c_int, _p])
+_plan_variant = declare("fls_plan_variant_name", ctypes.c_char_p, [_p, ctypes.c_int])
+_plan_graph = declare("fls_plan_decode_graph", ctypes.c_int, [_p, _p])
 
 
 def _columns(columns):
@@ -85,6 +88,21 @@ class PagePlan:
 
         s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
         check(_plan_decode(self.handle, s), "fls_plan_decode")
+
+    def decode_graph(self, stream=None):
+        """The plan's launches captured once in a CUDA graph, replayed on the stream."""
+        import torch
+
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        check(_plan_graph(self.handle, s), "fls_plan_decode_graph")
+
+    def autotune(self, reps=3, stream=None):
+        """Pick the fastest geometry variant per launch segment (runs decodes); returns the variants' names."""
+        import torch
+
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        check(_plan_autotune(self.handle, reps, s), "fls_plan_autotune")
+        return [n for n in (_plan_variant(self.handle, i).decode() for i in (0, 1)) if n]
 
     def close(self):
         if self.handle:

@@ -105,11 +105,19 @@ class RowGroupSet:
         self.values = int(sum(int(n) * 1024 for n in count))
         self.value_bytes = int(sum(int(count[c]) * 1024 * self.outputs[col[c]].element_size() for c in range(len(col))))
 
-    def decode(self, stream=None):
-        """Every chunk of the set: one plan, one persistent launch per kernel family present."""
+    def decode(self, stream=None, graph=True):
+        """Every chunk of the set: one plan, one persistent launch per kernel family present, replayed from a
+        CUDA graph (graph=False launches directly)."""
         if self.plan is None:
             return
-        self.plan.decode(stream)
+        if graph:
+            self.plan.decode_graph(stream)
+        else:
+            self.plan.decode(stream)
+
+    def autotune(self, reps=3):
+        """Geometry variants chosen on this set's own data (see PagePlan.autotune)."""
+        return self.plan.autotune(reps) if self.plan is not None else []
 
     def close(self):
         if self.plan is not None:

@@ -29,6 +29,9 @@ declare("fls_plan_create_ex", ctypes.c_int, [ctypes.POINTER(_Batch), ctypes.c_ui
 declare("fls_plan_decode", ctypes.c_int, [_p, _p])
 declare("fls_plan_decode_grid", ctypes.c_int, [_p, ctypes.c_int, _p])
 declare("fls_plan_destroy", ctypes.c_int, [_p])
+declare("fls_plan_autotune", ctypes.c_int, [_p, ctypes.c_int, _p])
+declare("fls_plan_variant_name", ctypes.c_char_p, [_p, ctypes.c_int])
+declare("fls_plan_decode_graph", ctypes.c_int, [_p, _p])
 declare("fls_plan_geometry", ctypes.c_int, [_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                             ctypes.POINTER(ctypes.c_int)])
 
@@ -110,6 +113,16 @@ class Plan:
     def decode(self, stream=None, grid=0):
         s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
         check(lib.fls_plan_decode_grid(self.handle, grid, s), "fls_plan_decode")
+
+    def decode_graph(self, stream=None):
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        check(lib.fls_plan_decode_graph(self.handle, s), "fls_plan_decode_graph")
+
+    def autotune(self, reps=3, stream=None):
+        """Pick the fastest geometry variant per launch segment (runs decodes); returns the variants' names."""
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        check(lib.fls_plan_autotune(self.handle, reps, s), "fls_plan_autotune")
+        return [n for n in (lib.fls_plan_variant_name(self.handle, i).decode() for i in (0, 1)) if n]
 
     def geometry(self):
         a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

@@ -172,8 +172,18 @@ int fls_plan_decode(const fls_plan* plan, fls_stream_t stream);
 /* Same, with an explicit grid (CTAs); 0 = one wave of resident CTAs. */
 int fls_plan_decode_grid(const fls_plan* plan, int grid, fls_stream_t stream);
 int fls_plan_destroy(fls_plan* plan);
-/* Shape of the kernel a plan launches: threads per CTA, dynamic shared memory, resident CTAs per SM. */
+/* Shape of the kernel a plan launches (its first segment): threads per CTA, dynamic shared memory, resident CTAs
+ * per SM. */
 int fls_plan_geometry(const fls_plan* plan, int* threads, int* smem_bytes, int* ctas_per_sm);
+/* Autotuner (no reference counterpart): times every geometry variant (warps per CTA x TMA staging depth, hence
+ * vectors per warp) of the plan's kernel families on the plan's own data, `reps` launches each, and keeps the
+ * fastest per launch segment.  Runs decodes (the outputs are written).  Synchronous. */
+int fls_plan_autotune(fls_plan* plan, int reps, fls_stream_t stream);
+/* Name of the variant segment 0 / 1 of the plan launches ("" when the plan has no such segment). */
+const char* fls_plan_variant_name(const fls_plan* plan, int segment);
+/* fls_plan_decode through a CUDA graph: the plan's launches (one per kernel family its queue holds) are
+ * captured once, on the first call or the first after fls_plan_autotune, and replayed on `stream`. */
+int fls_plan_decode_graph(fls_plan* plan, fls_stream_t stream);
 
 /* ---------------------------------------------------------------------------------------------------------
  * Reference page columns on the device.  d_page holds the bytes of one FastLanes page (the data_buf of

@@ -184,3 +184,32 @@ def test_c_api_decode_pipelines_large_pages(cuda, expr):
 
     _lib.lib.decode_to_memory(hp.data_ptr(), ho.data_ptr(), pages.INT64)
     assert np.array_equal(ho.numpy(), x)
+
+
+def test_plan_autotune_and_graph_replay(cuda):
+    """The autotuner picks a variant per launch segment without changing results; graph replays of a plan with
+    a plain and a gather segment equal direct launches."""
+    import torch
+
+    from fastlanes_b200 import rowgroups as RG
+    from fastlanes_b200 import select as S
+    from fastlanes_b200 import workloads as W
+
+    rng = np.random.default_rng(3)
+    cols = [W.selection_column(rng, 6, "cuda", f) for f in ("for_i64", "rle", "dict_i32", "delta_i64", "for_u32")]
+    plan = S.SelectionPlan(cols, 3)
+    _, best, _ = plan.wizard()
+    choice = best.cpu().numpy()
+    choice[0], choice[2] = 1, 2  # make sure both kernel families are present
+    rg = RG.RowGroupSet(cols, plan.chunks(), choice)
+    names = rg.autotune(2)
+    assert len(names) == 2 and all(names)
+    for graph in (False, True, True):
+        for o in rg.outputs:
+            o.zero_()
+        rg.decode(graph=graph)
+        torch.cuda.synchronize()
+        for o, (t, _) in zip(rg.outputs, cols):
+            assert torch.equal(o, t)
+    rg.close()
+    plan.close()
