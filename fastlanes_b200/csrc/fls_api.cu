@@ -25,16 +25,21 @@ template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES, bool GATH
 static cudaError_t launch_family(const DecodeArgs& a, cudaStream_t s, int sm_count, int grid_override) {
 	using G            = Geometry<MAXWS, GSTAGE, EMAX, WARPS, STAGES, GATHER>;
 	auto*       kfn    = k_decode<MAXWS, GSTAGE, EMAX, WARPS, STAGES, GATHER>;
-	static bool inited = false;
-	if (!inited) {
+	// per device: the shared-memory attribute is set and the occupancy queried once
+	static int        occupancy[64] {};
+	static std::mutex mu;
+	int               dev = 0;
+	if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) { return cudaErrorInvalidDevice; }
+	int per_sm = occupancy[dev];
+	if (per_sm == 0) {
+		std::lock_guard<std::mutex> lk(mu);
 		cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, G::kSmem);
 		if (e != cudaSuccess) { return e; }
-		inited = true;
+		e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, G::kThreads, G::kSmem);
+		if (e != cudaSuccess) { return e; }
+		per_sm          = per_sm < 1 ? 1 : per_sm;
+		occupancy[dev] = per_sm;
 	}
-	int per_sm = 0;
-	cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, G::kThreads, G::kSmem);
-	if (e != cudaSuccess) { return e; }
-	if (per_sm < 1) { per_sm = 1; }
 	const uint64_t want = (a.n_items + WARPS - 1) / WARPS;
 	uint64_t       grid = static_cast<uint64_t>(sm_count) * per_sm;
 	if (grid_override > 0) { grid = static_cast<uint64_t>(grid_override); }

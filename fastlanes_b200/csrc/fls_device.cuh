@@ -159,6 +159,21 @@ __device__ __forceinline__ void extract_w64(const uint32_t* __restrict__ S, uint
 	const uint32_t mlo   = static_cast<uint32_t>(mask);
 	const uint32_t mhi   = static_cast<uint32_t>(mask >> 32);
 	const uint2*   S2    = reinterpret_cast<const uint2*>(S);
+	if (bw <= 32) {
+		// a value of at most 32 bits lies in two adjacent 32-bit halves of the lane's 64-bit words: half-word
+		// index 2w (+1 when s >= 32) of word w = b >> 6, i.e. half h2 = b >> 5 of the lane
+#pragma unroll
+		for (uint32_t m = 0; m < 32; ++m) {
+			const uint32_t j  = 2 * m + h;
+			const uint32_t b  = j * bw;
+			const uint32_t h2 = b >> 5;
+			const uint32_t lo = S[2 * (l + 16 * (h2 >> 1)) + (h2 & 1u)];
+			const uint32_t h3 = h2 + 1;
+			const uint32_t hi = S[2 * (l + 16 * (h3 >> 1)) + (h3 & 1u)];
+			v[run32_pos(m)]   = __funnelshift_r(lo, hi, b & 31u) & mlo;
+		}
+		return;
+	}
 #pragma unroll
 	for (uint32_t m = 0; m < 32; ++m) {
 		const uint32_t j   = 2 * m + h;

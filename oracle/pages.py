@@ -22,6 +22,7 @@ ARR_C = {
     (5, 1): 4,  # DELTA NO_PATCH: lane bases, bw, base, packed
     (6, 1): 2,  # RLE UNCOMPRESSED: run values, u16 index
     (6, 2): 5,  # RLE DELTA_NO_PATCH: run values, lane bases, bw, base, packed (u16 index)
+    (6, 3): 2,  # RLE UNCOMPRESSED_REC: run values rec-compressed, raw u16 index
     (6, 4): 5,  # RLE DELTA_NO_PATCH_REC: as above, run values rec-compressed
     (7, 1): 2,  # FSST: bytes, end offsets
     (7, 2): 5,  # FSST DELTA_NO_PATCH: bytes, lane bases, bw, base, packed (u32 end offsets)
@@ -30,6 +31,7 @@ ARR_C = {
     (8, 7): 4,  # DICT DELTA_NO_PATCH
     (11, 1): 2,  # DICT_RLE UNCOMPRESSED: u32 code runs, u16 index
     (11, 2): 5,  # DICT_RLE DELTA_NO_PATCH
+    (11, 3): 2,  # DICT_RLE UNCOMPRESSED_REC
     (11, 4): 5,  # DICT_RLE DELTA_NO_PATCH_REC
 }
 
@@ -63,10 +65,12 @@ def _le(b, dtype):
     return np.frombuffer(np.ascontiguousarray(b).tobytes(), dtype)
 
 
-def rec_buffer(b):
-    """HzlDeCmp::decompress_buf (src/cor/eng/hzl_de_cmp.cpp:28-77) for the raw-tail form: rec_hdr
-    {bw u8, pad u8, exc_c u16, base[8]} with bw = 255 holds the byte count in base and the raw bytes after it.
-    Returns (decoded bytes, consumed bytes); FFOR blocks are decoded as 1024-value unffor + exception patch."""
+def rec_buffer(b, elem=np.uint64):
+    """HzlDeCmp::decompress_buf (src/cor/eng/hzl_de_cmp.cpp:28-77): a chain of blocks, each a rec_hdr
+    {bw u8, pad u8, exc_c u16, base[8]}; bw = 255 ends the chain with base = byte count of raw bytes, any other
+    bw is an FFOR block of 1024 values of the buffer's element type followed by its exceptions
+    (hzl_cmp.cpp:43-127 writes them): uint64 for 64-bit values and dictionary entries, idx_t = uint32
+    (include/fls/common/alias.hpp:17) for DICT_RLE run codes.  Returns (decoded bytes, consumed bytes)."""
     out = []
     pos = 0
     while True:
@@ -79,7 +83,19 @@ def rec_buffer(b):
             out.append(b[pos:pos + sz])
             pos += sz
             return np.concatenate(out) if out else np.zeros(0, np.uint8), pos
-        raise NotImplementedError("rec FFOR blocks")
+        # an FFOR block of 1024 values (generated unffor keeps positions), then exc_c u16 positions and exc_c
+        # values patched over the unpacked ones
+        et = np.dtype(elem)
+        base = np.frombuffer(base_raw.tobytes()[:et.itemsize], et)[0]
+        packed = np.frombuffer(b[pos:pos + bw * 128].tobytes(), et)
+        vals = oracle.unffor(packed, bw, base, et.type)
+        pos += bw * 128
+        exc_pos = np.frombuffer(b[pos:pos + 2 * exc_c].tobytes(), np.uint16)
+        pos += 2 * exc_c
+        exc_val = np.frombuffer(b[pos:pos + et.itemsize * exc_c].tobytes(), et)
+        pos += et.itemsize * exc_c
+        vals[exc_pos.astype(np.int64)] = exc_val
+        out.append(np.frombuffer(vals.tobytes(), np.uint8))
 
 
 STREAM_W = {2: None, 4: None, 5: None}
@@ -108,13 +124,15 @@ def decode_int(page, dict_bytes=None, value_dtype=np.uint64):
     W = VT.itemsize * 8
     dic = None
     if dict_bytes is not None and len(dict_bytes) > 8:
-        dic = _le(rec_buffer(np.asarray(dict_bytes, np.uint8)[8:])[0], VT)
+        dic = _le(rec_buffer(np.asarray(dict_bytes, np.uint8)[8:], np.uint64 if W == 64 else np.uint32)[0], VT)
     out = np.empty(pg.vec_c * 1024, VT)
     et, var = pg.exp_t, pg.var
     rec_vals = None
-    if et in (6, 11) and var == 4:
-        # DELTA_NO_PATCH_REC: buffer 0 (run values) is one rec buffer; entry points index its decoded bytes
-        rec_vals = rec_buffer(pg.b[pg.off[0]:pg.off[0] + pg.buf_size[0]])[0]
+    if et in (6, 11) and var in (3, 4):
+        # UNCOMPRESSED_REC / DELTA_NO_PATCH_REC: buffer 0 (run values / run codes) is one rec buffer; entry
+        # points index its decoded bytes
+        ve = np.uint32 if et == 11 or W == 32 else np.uint64
+        rec_vals = rec_buffer(pg.b[pg.off[0]:pg.off[0] + pg.buf_size[0]], ve)[0]
     for v in range(pg.vec_c):
         if et == 2:
             tr = _stream(pg, v, 0, W, "raw", VT)

@@ -16,6 +16,9 @@ primitives.npz
 columns.npz
     * small seeded columns encoded by the reference's column encoder (ExpColEncoder, verify on) for the
       expressions on the decode path, with the reference decoder's materialised output.
+
+The reference's FSST table export leaves its last byte uninitialised for some tables (str_13_dict differs
+in that byte from run to run); a regenerated file keeps the committed bytes of every existing array.
 """
 import ctypes
 import hashlib
@@ -33,6 +36,9 @@ TYPES = {8: np.uint8, 16: np.uint16, 32: np.uint32, 64: np.uint64}
 
 # Expressions of src/cor/exp_pool.cpp on the integer / string decode path.
 I64_IDS = [0, 1, 6, 7, 11, 16, 17, 22, 27]
+# The same expressions on columns large enough that the reference's rec compression (hzl_cmp.cpp:43-127)
+# writes FFOR blocks with exceptions, not only a raw tail: dictionaries of ~3000 entries, ~2000 runs.
+REC_IDS = [8, 9, 16, 17, 22, 27]
 STR_IDS = [0, 2, 3, 8, 13, 14, 15, 16]
 
 
@@ -110,6 +116,18 @@ def i64_column(eid, rng, n):
     return rng.integers(-(1 << 62), 1 << 62, n).astype(np.int64)
 
 
+def rec_column(eid, rng, n):
+    if eid in (16, 17, 22):
+        return (rng.integers(0, 3000, n) * 7919 - 5000).astype(np.int64)
+    runs = rng.geometric(1 / 2, n)
+    if eid == 27:
+        return np.repeat(rng.integers(0, 40, runs.size) * 1000 + 3, runs)[:n].astype(np.int64)
+    # a few far-off run values become the FFOR blocks' exceptions
+    vals = rng.integers(0, 10**6, runs.size)
+    vals[rng.integers(0, runs.size, 8)] = rng.integers(-(1 << 60), 1 << 60, 8)
+    return np.repeat(vals, runs)[:n].astype(np.int64)
+
+
 def str_column(eid, rng, n):
     alphabet = np.frombuffer(b"abcdefghijklmnopqrstuvwxyzABCDEFGHIJKLMNOPQRSTUVWXYZ0123456789-_", np.uint8)
     tokens = [bytes(alphabet[rng.integers(0, 64, rng.integers(2, 7))]) for _ in range(64)]
@@ -145,6 +163,22 @@ def columns(ref):
         res[f"i64_{eid}_page"] = page[: ps.value].copy()
         res[f"i64_{eid}_dict"] = dic[: ds.value].copy()
         # the reference decoder reproduces the input for every int64 expression (asserted above)
+    for eid in REC_IDS:
+        rng = np.random.default_rng(3000 + eid)
+        m = 4 * 1024
+        col = rec_column(eid, rng, m)
+        page, dic = np.zeros(cap, np.uint8), np.zeros(cap, np.uint8)
+        ps, ds = ctypes.c_uint64(), ctypes.c_uint64()
+        rc = ref.ref_encode_i64(ptr(col), ctypes.c_uint64(m), ctypes.c_uint8(eid), 1, ptr(page), ctypes.c_uint64(cap),
+                                ctypes.byref(ps), ptr(dic), ctypes.c_uint64(cap), ctypes.byref(ds))
+        assert rc == 0, (eid, rc)
+        out = np.zeros(m, np.int64)
+        nv = ctypes.c_uint64()
+        rc = ref.ref_decode_i64(ptr(page), ptr(dic), ds, ptr(out), ctypes.c_uint64(m // 1024), ctypes.byref(nv))
+        assert rc == 0 and np.array_equal(out, col), (eid, rc)
+        res[f"i64rec_{eid}_input"] = col
+        res[f"i64rec_{eid}_page"] = page[: ps.value].copy()
+        res[f"i64rec_{eid}_dict"] = dic[: ds.value].copy()
     for eid in STR_IDS:
         rng = np.random.default_rng(2000 + eid)
         byts, offs = str_column(eid, rng, n)
@@ -173,7 +207,12 @@ def columns(ref):
 def main():
     ref = ctypes.CDLL(os.path.join(REPO, "oracle/_ref/libfls_ref.so"))
     np.savez_compressed(os.path.join(HERE, "primitives.npz"), **primitives(ref))
-    np.savez_compressed(os.path.join(HERE, "columns.npz"), **columns(ref))
+    cols = columns(ref)
+    old = os.path.join(HERE, "columns.npz")
+    if os.path.exists(old):
+        prev = np.load(old)
+        cols.update({k: prev[k] for k in prev.files if k in cols})
+    np.savez_compressed(old, **cols)
     for f in ("primitives.npz", "columns.npz"):
         print(f, os.path.getsize(os.path.join(HERE, f)))
 

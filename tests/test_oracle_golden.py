@@ -110,3 +110,17 @@ def test_page_oracle_decodes_reference_int64_pages(col_golden, eid):
     dic = col_golden[f"i64_{eid}_dict"]
     got = pages.decode_int(page, dic if dic.size else None, np.uint64).view(np.int64)
     assert np.array_equal(got, col_golden[f"i64_{eid}_input"])
+
+
+@pytest.mark.parametrize("eid", [8, 9, 16, 17, 22, 27])
+def test_page_oracle_decodes_reference_rec_pages(col_golden, eid):
+    """Reference pages whose rec buffers hold FFOR blocks with exceptions (large dictionaries, many runs)."""
+    from oracle import pages
+
+    page = col_golden[f"i64rec_{eid}_page"]
+    dic = col_golden[f"i64rec_{eid}_dict"]
+    got = pages.decode_int(page, dic if dic.size else None, np.uint64).view(np.int64)
+    assert np.array_equal(got, col_golden[f"i64rec_{eid}_input"])
+    # the fixtures do exercise FFOR rec blocks
+    buf = dic[8:] if eid in (16, 17, 22) else page[pages.parse_page(page).off[0]:]
+    assert buf[0] != 255
