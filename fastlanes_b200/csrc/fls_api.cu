@@ -435,11 +435,16 @@ struct fls_plan {
 	uint64_t  split = 0;
 	Family    fam_b = Family::GATHER;
 	int       variant[2] {0, 0};     // geometry variant of each segment (fls_plan_autotune)
+	std::vector<void*> owned;        // device buffers decoded for the plan (rec buffers)
 	cudaGraphExec_t graph = nullptr; // the segments' launches, captured by fls_plan_decode_graph
 	cudaStream_t    graph_stream = nullptr;
 };
 
 namespace flsgpu {
+void plan_adopt(::fls_plan* plan, std::vector<void*>&& buffers) {
+	for (void* b : buffers) { plan->owned.push_back(b); }
+}
+
 bool plan_segments(const std::vector<ColDesc>& descs, const std::vector<uint32_t>& queue, uint32_t col_shift,
                    Family* fam_a, uint64_t* split, Family* fam_b) {
 	// a queue ordered family-major decodes as up to two launches, each on the kernel specialised for its
@@ -726,6 +731,7 @@ const char* fls_plan_variant_name(const fls_plan* p, int segment) {
 int fls_plan_destroy(fls_plan* p) {
 	if (!p) { return FLS_OK; }
 	drop_graph(p);
+	for (void* b : p->owned) { cudaFree(b); }
 	if (p->d_cols) { cudaFree(p->d_cols); }
 	if (p->d_queue) { cudaFree(p->d_queue); }
 	delete p;

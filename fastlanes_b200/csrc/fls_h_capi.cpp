@@ -15,6 +15,7 @@
 #include "fastlanes.h"
 #include "fls_b200.h"
 #include "fls_page.h"
+#include "fls_rec.h"
 #include "fls_runtime.h"
 
 #include <algorithm>
@@ -282,8 +283,24 @@ int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_
 		return FLS_ERR_CUDA;
 	}
 	uint8_t* dp = d_page.as<uint8_t>() + shift;
-	ColDesc  c {};
-	rc = build_page_column(pi, dp, w, nullptr, 0, FLS_ORIGINAL, d_out.as<uint8_t>(), &c);
+	// _REC variants: the rec-compressed value buffer goes over whole and is decoded first (on the copy stream,
+	// so every chunk's decode is ordered after it)
+	const int rec_b = pi.layout->rec_vals ? pi.layout->ib_vals : -1;
+	DevBuf    d_rec(hp->in);
+	uint64_t  rec_n = 0;
+	if (rec_b >= 0) {
+		if (cudaMemcpyAsync(dp + pi.off[rec_b], page + pi.off[rec_b], pi.size[rec_b], cudaMemcpyHostToDevice, hp->in) !=
+		    cudaSuccess) {
+			return FLS_ERR_CUDA;
+		}
+		uint8_t*       rb = nullptr;
+		const uint32_t eb = pi.layout->post == POST_RLE_DICT ? 4u : static_cast<uint32_t>(w / 8);
+		rc                = rec_decode(dp + pi.off[rec_b], page + pi.off[rec_b], pi.size[rec_b], eb, &rb, &rec_n, hp->in);
+		d_rec.p           = rb;
+		if (rc != FLS_OK) { return rc; }
+	}
+	ColDesc c {};
+	rc = build_page_column(pi, dp, w, nullptr, 0, FLS_ORIGINAL, d_out.as<uint8_t>(), &c, d_rec.as<uint8_t>(), rec_n);
 	if (rc != FLS_OK) { return rc; }
 	// work items: vector ids (the single column is the plan's inline column)
 	std::vector<uint32_t> ids(pi.vec_c);
@@ -320,6 +337,7 @@ int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_
 		const uint32_t v0 = static_cast<uint32_t>(k * chunk_vec);
 		const uint32_t v1 = static_cast<uint32_t>(std::min<uint64_t>(pi.vec_c, v0 + chunk_vec));
 		for (uint32_t b = 0; b < pi.arr_c; ++b) {
+			if (static_cast<int>(b) == rec_b) { continue; } // already in place (and decoded)
 			const uint64_t lo = pi.off[b] + ep(v0, b);
 			const uint64_t hi = v1 < pi.vec_c ? pi.off[b] + ep(v1, b) : pi.off[b] + pi.size[b];
 			if (hi > lo && hi <= page_size &&

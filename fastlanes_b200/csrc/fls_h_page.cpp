@@ -12,6 +12,7 @@
 #include "fastlanes.h"
 #include "fls_b200.h"
 #include "fls_page.h"
+#include "fls_rec.h"
 #include "fls_runtime.h"
 
 #include <algorithm>
@@ -29,12 +30,14 @@ const ExprLayout* expr_layout(uint8_t exp_t, uint8_t var) {
 	    {5, 1, 4, 0, ENC_DELTA, POST_NONE, 1, 2, 3, 0, kNoBuf, false},                      // DELTA NO_PATCH
 	    {6, 1, 2, 16, ENC_RAW, POST_RLE, kNoBuf, kNoBuf, 1, kNoBuf, 0, false},               // RLE UNCOMPRESSED
 	    {6, 2, 5, 16, ENC_DELTA, POST_RLE, 2, 3, 4, 1, 0, false},                            // RLE DELTA_NO_PATCH
+	    {6, 3, 2, 16, ENC_RAW, POST_RLE, kNoBuf, kNoBuf, 1, kNoBuf, 0, true},                // RLE UNCOMPRESSED_REC
 	    {6, 4, 5, 16, ENC_DELTA, POST_RLE, 2, 3, 4, 1, 0, true},                             // RLE DELTA_NO_PATCH_REC
 	    {8, 1, 1, 32, ENC_RAW, POST_DICT, kNoBuf, kNoBuf, 0, kNoBuf, kNoBuf, false},         // DICT UNCOMPRESSED
 	    {8, 2, 3, 32, ENC_FFOR, POST_DICT, 0, 1, 2, kNoBuf, kNoBuf, false},                  // DICT FFOR_NO_PATCH
 	    {8, 7, 4, 32, ENC_DELTA, POST_DICT, 1, 2, 3, 0, kNoBuf, false},                      // DICT DELTA_NO_PATCH
 	    {11, 1, 2, 16, ENC_RAW, POST_RLE_DICT, kNoBuf, kNoBuf, 1, kNoBuf, 0, false},         // DICT_RLE UNCOMPRESSED
 	    {11, 2, 5, 16, ENC_DELTA, POST_RLE_DICT, 2, 3, 4, 1, 0, false},                      // DICT_RLE DELTA_NO_PATCH
+	    {11, 3, 2, 16, ENC_RAW, POST_RLE_DICT, kNoBuf, kNoBuf, 1, kNoBuf, 0, true},          // DICT_RLE UNCOMPRESSED_REC
 	    {11, 4, 5, 16, ENC_DELTA, POST_RLE_DICT, 2, 3, 4, 1, 0, true},                       // DICT_RLE ..._REC
 	};
 	for (const auto& e : table) {
@@ -87,10 +90,12 @@ int finish_page_info(PageInfo* pi, uint64_t page_size) {
 }
 
 int build_page_column(const PageInfo& pi, const uint8_t* d_page, int value_width, const uint8_t* d_dict_vals,
-                      uint32_t dict_entries, int order, uint8_t* d_out, ColDesc* c) {
+                      uint32_t dict_entries, int order, uint8_t* d_out, ColDesc* c, const uint8_t* d_vals_decoded,
+                      uint64_t vals_decoded_size) {
 	const ExprLayout* L = pi.layout;
 	if (!L || value_width == 0) { return FLS_ERR_UNSUPPORTED; }
-	if (L->rec_vals) { return FLS_ERR_UNSUPPORTED; } // the page-level rec buffer is decoded by the caller
+	// the page-level rec buffer of the _REC variants is decoded by the caller (rec_decode)
+	if (L->rec_vals && !d_vals_decoded) { return FLS_ERR_UNSUPPORTED; }
 	*c        = ColDesc {};
 	c->ws     = static_cast<uint8_t>(L->ws ? L->ws : value_width);
 	c->e      = static_cast<uint8_t>(value_width / 8);
@@ -108,6 +113,10 @@ int build_page_column(const PageInfo& pi, const uint8_t* d_page, int value_width
 	for (uint32_t i = 0; i < pi.arr_c; ++i) {
 		c->buf[i]      = d_page + pi.off[i];
 		c->buf_size[i] = pi.size[i];
+	}
+	if (L->rec_vals) {
+		c->buf[L->ib_vals]      = d_vals_decoded;
+		c->buf_size[L->ib_vals] = vals_decoded_size;
 	}
 	c->ep  = reinterpret_cast<const uint32_t*>(d_page + pi.ep_off);
 	c->out = d_out;
@@ -173,8 +182,27 @@ static int read_on(void* dst, const void* src, size_t n, cudaStream_t stream) {
 // Work items of page plans: (column << kPageShift | vector); a page holds at most 65,535 vectors.
 constexpr uint32_t kPageShift = 16;
 
+// Element bytes of a layout's rec-compressed value buffer: run codes are idx_t = uint32, run values the
+// column's values.
+static uint32_t rec_elem_bytes(const ExprLayout* L, int value_width) {
+	return L->post == POST_RLE_DICT ? 4u : static_cast<uint32_t>(value_width / 8);
+}
+
+// Rec buffer at d_src (device, size bytes) decoded into a new device buffer, appended to *owned.
+static int decode_rec_on(const uint8_t* d_src, uint64_t size, uint32_t eb, std::vector<void*>* owned,
+                         const uint8_t** out, uint64_t* out_size, cudaStream_t stream) {
+	std::vector<uint8_t> h(size);
+	if (size && read_on(h.data(), d_src, size, stream) != FLS_OK) { return FLS_ERR_CUDA; }
+	uint8_t*  buf = nullptr;
+	const int rc  = rec_decode(d_src, h.data(), size, eb, &buf, out_size, stream);
+	if (buf) { owned->push_back(buf); }
+	*out = buf;
+	return rc;
+}
+
 static int describe_pages(const fls_page_column* cols, uint32_t n_cols, std::vector<ColDesc>* descs,
-                          std::vector<uint32_t>* queue, Family* fam_out, cudaStream_t stream) {
+                          std::vector<uint32_t>* queue, Family* fam_out, cudaStream_t stream,
+                          std::vector<void*>* owned) {
 	if (!cols || n_cols == 0 || n_cols > 65535) { return FLS_ERR_ARG; }
 	descs->assign(n_cols, ColDesc {});
 	queue->clear();
@@ -198,13 +226,31 @@ static int describe_pages(const fls_page_column* cols, uint32_t n_cols, std::vec
 			if (!pc.d_dict || pc.dict_size < 20) { return FLS_ERR_FORMAT; }
 			uint8_t dh[20];
 			if (read_on(dh, pc.d_dict, 20, stream) != FLS_OK) { return FLS_ERR_CUDA; }
-			uint64_t voff = 0;
-			rc            = int_dictionary_values(dh, pc.dict_size, w, &voff, &entries);
+			if (dh[8] == 255) {
+				uint64_t voff = 0;
+				rc            = int_dictionary_values(dh, pc.dict_size, w, &voff, &entries);
+				if (rc != FLS_OK) { return rc; }
+				dvals = pc.d_dict + voff;
+			} else {
+				// entries FFOR-packed in rec blocks (dictionaries of 1024 entries and more)
+				std::memcpy(&entries, dh + 4, 4);
+				uint64_t n = 0;
+				rc         = decode_rec_on(pc.d_dict + 8, pc.dict_size - 8, static_cast<uint32_t>(w / 8), owned, &dvals,
+				                           &n, stream);
+				if (rc != FLS_OK) { return rc; }
+				if (n < static_cast<uint64_t>(entries) * (w / 8)) { return FLS_ERR_FORMAT; }
+			}
+		}
+		const uint8_t* rvals = nullptr;
+		uint64_t       rsize = 0;
+		if (pi.layout->rec_vals) {
+			const uint32_t b = pi.layout->ib_vals;
+			rc = decode_rec_on(pc.d_page + pi.off[b], pi.size[b], rec_elem_bytes(pi.layout, w), owned, &rvals, &rsize,
+			                   stream);
 			if (rc != FLS_OK) { return rc; }
-			dvals = pc.d_dict + voff;
 		}
 		rc = build_page_column(pi, pc.d_page, w, dvals, entries, pc.order, static_cast<uint8_t*>(pc.d_out),
-		                       &(*descs)[i]);
+		                       &(*descs)[i], rvals, rsize);
 		if (rc != FLS_OK) { return rc; }
 		if ((*descs)[i].post != POST_NONE) { fam = Family::GATHER; }
 		if ((*descs)[i].ws == 64) { any64 = true; }
@@ -231,7 +277,15 @@ int fls_gpu_decode_pages(const fls_page_column* cols, uint32_t n_cols, fls_strea
 	std::vector<uint32_t> queue;
 	Family                fam = Family::NUM;
 	cudaStream_t          s   = static_cast<cudaStream_t>(stream);
-	int                   rc  = describe_pages(cols, n_cols, &descs, &queue, &fam, s);
+	std::vector<void*>    owned;
+	struct Free {
+		std::vector<void*>& v;
+		cudaStream_t        s;
+		~Free() {
+			for (void* p : v) { cudaFreeAsync(p, s); }
+		}
+	} free_owned {owned, s};
+	int rc = describe_pages(cols, n_cols, &descs, &queue, &fam, s, &owned);
 	if (rc != FLS_OK) { return rc; }
 	if (queue.empty()) { return FLS_OK; }
 	DecodeArgs   a {};
@@ -272,9 +326,16 @@ int fls_plan_create_pages(const fls_page_column* cols, uint32_t n_cols, fls_plan
 	std::vector<uint32_t> queue;
 	Family                fam = Family::NUM;
 	// headers are read on the legacy default stream: the pages must be in place (e.g. after a device sync)
-	const int rc = describe_pages(cols, n_cols, &descs, &queue, &fam, nullptr);
-	if (rc != FLS_OK) { return rc; }
-	return make_plan_object(descs, queue, fam, kPageShift, out_plan);
+	std::vector<void*> owned;
+	int                rc = describe_pages(cols, n_cols, &descs, &queue, &fam, nullptr, &owned);
+	if (rc == FLS_OK) { rc = make_plan_object(descs, queue, fam, kPageShift, out_plan); }
+	if (rc == FLS_OK) {
+		plan_adopt(*out_plan, std::move(owned)); // decoded rec buffers live as long as the plan
+	} else {
+		cudaDeviceSynchronize();
+		for (void* p : owned) { cudaFree(p); }
+	}
+	return rc;
 }
 
 } // extern "C"

@@ -29,8 +29,10 @@ const ExprLayout* expr_layout(uint8_t exp_t, uint8_t var);
 int               value_width_of(uint8_t data_type);
 int               parse_page_header(const uint8_t* hdr, uint64_t avail, PageInfo* out);
 int               finish_page_info(PageInfo* pi, uint64_t page_size);
+// d_vals_decoded / vals_decoded_size: for the _REC layouts, the decoded rec buffer that replaces buffer ib_vals.
 int build_page_column(const PageInfo& pi, const uint8_t* d_page, int value_width, const uint8_t* d_dict_vals,
-                      uint32_t dict_entries, int order, uint8_t* d_out, ColDesc* c);
+                      uint32_t dict_entries, int order, uint8_t* d_out, ColDesc* c,
+                      const uint8_t* d_vals_decoded = nullptr, uint64_t vals_decoded_size = 0);
 // RLE DELTA_NO_PATCH page (fls_h_encode.cpp) of n values of width 32 or 64 from host memory.
 int encode_rle_page(const void* in, uint64_t n, uint64_t cap, uint8_t* out, uint64_t* out_size, uint64_t* mtd_size,
                     int width);

@@ -50,6 +50,9 @@ bool plan_segments(const std::vector<ColDesc>& descs, const std::vector<uint32_t
 int make_plan_object(const std::vector<ColDesc>& descs, const std::vector<uint32_t>& queue, Family fam,
                      uint32_t col_shift, ::fls_plan** out);
 
+// Hand device buffers to a plan: freed when the plan is destroyed.
+void plan_adopt(::fls_plan* plan, std::vector<void*>&& buffers);
+
 // Kernels launched by this library inside the last timed region of a caller (a plain counter; not thread-safe).
 uint64_t& launch_counter();
 

@@ -213,3 +213,32 @@ def test_plan_autotune_and_graph_replay(cuda):
             assert torch.equal(o, t)
     rg.close()
     plan.close()
+
+
+@pytest.mark.parametrize("eid", [8, 9, 16, 17, 22, 27])
+@pytest.mark.parametrize("shift", [0, 3, 8])
+def test_reference_rec_pages(cuda, col_golden, eid, shift):
+    """Reference pages whose rec buffers (dictionary entries, run values, run codes) hold FFOR blocks with
+    exceptions: decoded on the GPU one-shot and through a page plan, equal to the reference's input."""
+    import torch
+
+    from fastlanes_b200 import pages
+
+    page, dic, want = (col_golden[f"i64rec_{eid}_{k}"] for k in ("page", "dict", "input"))
+    pbuf, pptr = _dev_bytes(page, cuda, shift)
+    col = dict(d_page=pptr, page_size=page.size, data_type=pages.INT64, order=1)
+    if dic.size:
+        dbuf, dptr = _dev_bytes(dic, cuda, 5)
+        col.update(d_dict=dptr, dict_size=dic.size)
+    out = torch.zeros(want.size, dtype=torch.int64, device=cuda)
+    pages.decode_pages([dict(col, d_out=out.data_ptr())])
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), want)
+    out.zero_()
+    plan = pages.PagePlan([dict(col, d_out=out.data_ptr())])
+    plan.decode()
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), want)
+    plan.close()
+    if not dic.size:
+        assert np.array_equal(pages.decode_to_memory(page, pages.INT64), want)
