@@ -54,7 +54,7 @@ def case_strings(a):
     return f"strings rows={a.rows} bytes={n} ms={ms:.4f}"
 
 
-def _page_case(values, dtype, expr, reps, name):
+def _page_case(values, dtype, expr, reps, name, autotune=False):
     from . import pages as PG
 
     page, _ = PG.encode_from_memory(values, dtype, expr)
@@ -67,23 +67,24 @@ def _page_case(values, dtype, expr, reps, name):
     plan.decode()
     if not np.array_equal(out.cpu().numpy(), values):
         raise SystemExit(f"{name}: mismatch")
+    tuned = plan.autotune() if autotune else []
     ms = _timed(plan.decode, reps)
     plan.close()
-    return f"{name} values={values.size} page={page.size} ms={ms:.4f}"
+    return f"{name} values={values.size} page={page.size} variants={tuned} ms={ms:.4f}"
 
 
 def case_rle(a):
     from . import pages as PG
     from . import workloads as W
 
-    return _page_case(W.rle_int32(a.values), PG.INT32, 6, a.reps, "rle")
+    return _page_case(W.rle_int32(a.values), PG.INT32, 6, a.reps, "rle", a.autotune)
 
 
 def case_delta(a):
     from . import pages as PG
     from . import workloads as W
 
-    return _page_case(W.delta_timestamps(a.values), PG.INT64, 11, a.reps, "delta")
+    return _page_case(W.delta_timestamps(a.values), PG.INT64, 11, a.reps, "delta", a.autotune)
 
 
 def _columns(a):
@@ -105,6 +106,8 @@ def case_mixed(a):
     torch.cuda.synchronize()
     if not all(torch.equal(o, t) for o, (t, _) in zip(rg.outputs, cols)):
         raise SystemExit("mixed: mismatch")
+    if a.autotune:
+        rg.autotune()
     ms = _timed(rg.decode, a.reps)
     res = f"mixed chunks={plan.n_chunks} values={rg.values} read={rg.page_bytes + rg.dict_bytes} ms={ms:.4f}"
     rg.close()
@@ -137,6 +140,7 @@ def main(argv=None):
     ap.add_argument("--values", type=int, default=16 << 20)
     ap.add_argument("--columns", type=int, default=32)
     ap.add_argument("--max-vectors", type=int, default=1024)
+    ap.add_argument("--autotune", action="store_true", help="pick the plan's geometry variants first (as bench.py)")
     a = ap.parse_args(argv)
     print(CASES[a.case](a))
     return 0
