@@ -20,6 +20,14 @@ ARR_C = {
     (3, 1): 2,  # BYTE_ARR: bytes, end offsets
     (4, 1): 3,  # FFOR NO_PATCH: bw, base, packed
     (5, 1): 4,  # DELTA NO_PATCH: lane bases, bw, base, packed
+    (4, 2): 5,  # FFOR LL_PATCH: exceptions, (exc_c, first position), bw, base, packed
+    (4, 3): 5,  # FFOR S_PATCH: exceptions, (exc_c, positions), bw, base, packed
+    (4, 4): 5,  # FFOR B_PATCH: exceptions, 1024-bit position bitmap, bw, base, packed
+    (4, 5): 5,  # FFOR S_PATCH_REC: as S_PATCH, exceptions rec-compressed
+    (5, 2): 6,  # DELTA LL_PATCH: lane bases, then as FFOR LL_PATCH
+    (5, 3): 6,  # DELTA S_PATCH
+    (5, 4): 6,  # DELTA B_PATCH
+    (5, 5): 6,  # DELTA B_PATCH_REC: as B_PATCH, exceptions rec-compressed
     (6, 1): 2,  # RLE UNCOMPRESSED: run values, u16 index
     (6, 2): 5,  # RLE DELTA_NO_PATCH: run values, lane bases, bw, base, packed (u16 index)
     (6, 3): 2,  # RLE UNCOMPRESSED_REC: run values rec-compressed, raw u16 index
@@ -117,6 +125,56 @@ def _stream(pg, v, first, ws, enc, T):
     return oracle.rsum(oracle.unffor(packed, bw, base, T), lb)
 
 
+# (exp_t, var) of the patched FFOR / DELTA variants -> patch kind, exceptions rec-compressed
+PATCHED = {(4, 2): ("ll", False), (4, 3): ("s", False), (4, 4): ("b", False), (4, 5): ("s", True),
+           (5, 2): ("ll", False), (5, 3): ("s", False), (5, 4): ("b", False), (5, 5): ("b", True)}
+
+
+def _patch(vals, kind, exc_bytes, side, base, T):
+    """One vector's patch over its unpacked values (transposed positions), after unffor:
+    s  (src/cor/prm/patch/s_patch/s_patch_decompress.cpp): side = exc_c u16, then exc_c u16 positions;
+    b  (b_patch_decompress.cpp, patch.cpp:71-83): side = 16 uint64 bitmap words, exceptions in bit order;
+    ll (ll_patch_decompress.cpp): side = exc_c u16, first position u16; the packed value at an exception is
+       the distance to the next one minus one (offset = out[cur] - base + 1 in the type)."""
+    T = np.dtype(T)
+    exc = np.frombuffer(exc_bytes.tobytes(), T)
+    if kind == "s":
+        sel = np.frombuffer(side.tobytes()[: 2 * (1 + int(np.frombuffer(side.tobytes()[:2], np.uint16)[0]))], np.uint16)
+        c = int(sel[0])
+        vals[sel[1:1 + c].astype(np.int64)] = exc[:c]
+    elif kind == "b":
+        pos = np.flatnonzero(np.unpackbits(np.asarray(side[:128], np.uint8), bitorder="little"))
+        vals[pos] = exc[:pos.size]
+    else:
+        c, first = struct.unpack("<HH", side[:4].tobytes())
+        mask = (1 << (T.itemsize * 8)) - 1
+        cur = int(first)
+        for i in range(c):
+            off = (int(vals[cur]) - int(base) + 1) & mask
+            vals[cur] = exc[i]
+            cur = (cur + off) & mask
+    return vals
+
+
+def _patched_stream(pg, v, T, rec_exc):
+    """Unpacked, patched and (DELTA) rsum-ed values of vector v of a patched FFOR / DELTA page (transposed)."""
+    kind, _ = PATCHED[(pg.exp_t, pg.var)]
+    first = 1 if pg.exp_t == 5 else 0
+    ws = np.dtype(T).itemsize * 8
+    bw = int(pg.vector_slice(v, first + 2, 1)[0])
+    base = _le(pg.vector_slice(v, first + 3, ws // 8), T)[0]
+    vals = oracle.unffor(_le(pg.vector_slice(v, first + 4, bw * 128), T), bw, base, T)
+    if rec_exc is not None:
+        end = pg.ep_of(v + 1, first) if v + 1 < pg.vec_c else rec_exc.size
+        exc = rec_exc[pg.ep_of(v, first):end]
+    else:
+        exc = pg.vector_slice(v, first)
+    vals = _patch(vals, kind, exc, pg.vector_slice(v, first + 1), base, T)
+    if pg.exp_t == 5:
+        vals = oracle.rsum(vals, _le(pg.vector_slice(v, 0, 128), T).copy())
+    return vals
+
+
 def decode_int(page, dict_bytes=None, value_dtype=np.uint64):
     """Materialised (original-order) values of an integer page, as assert_eq.hpp:50-400 reconstructs them."""
     pg = parse_page(page)
@@ -133,8 +191,14 @@ def decode_int(page, dict_bytes=None, value_dtype=np.uint64):
         # points index its decoded bytes
         ve = np.uint32 if et == 11 or W == 32 else np.uint64
         rec_vals = rec_buffer(pg.b[pg.off[0]:pg.off[0] + pg.buf_size[0]], ve)[0]
+    rec_exc = None
+    if (et, var) in PATCHED and PATCHED[(et, var)][1]:
+        b = 1 if et == 5 else 0
+        rec_exc = rec_buffer(pg.b[pg.off[b]:pg.off[b] + pg.buf_size[b]], np.uint64 if W == 64 else np.uint32)[0]
     for v in range(pg.vec_c):
-        if et == 2:
+        if (et, var) in PATCHED:
+            tr = _patched_stream(pg, v, VT, rec_exc)
+        elif et == 2:
             tr = _stream(pg, v, 0, W, "raw", VT)
         elif et == 4:
             tr = _stream(pg, v, 0, W, "ffor", VT)

@@ -39,6 +39,8 @@ I64_IDS = [0, 1, 6, 7, 11, 16, 17, 22, 27]
 # The same expressions on columns large enough that the reference's rec compression (hzl_cmp.cpp:43-127)
 # writes FFOR blocks with exceptions, not only a raw tail: dictionaries of ~3000 entries, ~2000 runs.
 REC_IDS = [8, 9, 16, 17, 22, 27]
+# Patched FFOR / DELTA (src/cor/prm/patch/*) on columns with ~3% outliers / outlying gaps.
+PATCH_IDS = [2, 3, 4, 5, 12, 13, 14, 15]
 STR_IDS = [0, 2, 3, 8, 13, 14, 15, 16]
 
 
@@ -128,6 +130,18 @@ def rec_column(eid, rng, n):
     return np.repeat(vals, runs)[:n].astype(np.int64)
 
 
+def patch_column(eid, rng, n):
+    if eid <= 5:
+        x = (rng.integers(0, 1 << 10, n) + 5000).astype(np.int64)
+        out = rng.random(n) < 0.03
+        x[out] = rng.integers(-(1 << 40), 1 << 40, out.sum())
+        return x
+    gaps = rng.geometric(0.1, n)
+    big = rng.random(n) < 0.03
+    gaps[big] = rng.integers(1 << 20, 1 << 30, big.sum())
+    return (1_600_000_000_000_000_000 + np.cumsum(gaps)).astype(np.int64)
+
+
 def str_column(eid, rng, n):
     alphabet = np.frombuffer(b"abcdefghijklmnopqrstuvwxyzABCDEFGHIJKLMNOPQRSTUVWXYZ0123456789-_", np.uint8)
     tokens = [bytes(alphabet[rng.integers(0, 64, rng.integers(2, 7))]) for _ in range(64)]
@@ -179,6 +193,16 @@ def columns(ref):
         res[f"i64rec_{eid}_input"] = col
         res[f"i64rec_{eid}_page"] = page[: ps.value].copy()
         res[f"i64rec_{eid}_dict"] = dic[: ds.value].copy()
+    for eid in PATCH_IDS:
+        rng = np.random.default_rng(4000 + eid)
+        col = patch_column(eid, rng, n)
+        page, dic = np.zeros(cap, np.uint8), np.zeros(cap, np.uint8)
+        ps, ds = ctypes.c_uint64(), ctypes.c_uint64()
+        rc = ref.ref_encode_i64(ptr(col), ctypes.c_uint64(n), ctypes.c_uint8(eid), 1, ptr(page), ctypes.c_uint64(cap),
+                                ctypes.byref(ps), ptr(dic), ctypes.c_uint64(cap), ctypes.byref(ds))
+        assert rc == 0, (eid, rc)
+        res[f"i64patch_{eid}_input"] = col
+        res[f"i64patch_{eid}_page"] = page[: ps.value].copy()
     for eid in STR_IDS:
         rng = np.random.default_rng(2000 + eid)
         byts, offs = str_column(eid, rng, n)

@@ -124,3 +124,13 @@ def test_page_oracle_decodes_reference_rec_pages(col_golden, eid):
     # the fixtures do exercise FFOR rec blocks
     buf = dic[8:] if eid in (16, 17, 22) else page[pages.parse_page(page).off[0]:]
     assert buf[0] != 255
+
+
+@pytest.mark.parametrize("eid", [2, 3, 4, 5, 12, 13, 14, 15])
+def test_page_oracle_decodes_reference_patched_pages(col_golden, eid):
+    """Patched FFOR / DELTA pages of the reference (S / B / LL patches, rec-compressed exceptions)."""
+    from oracle import pages
+
+    page = col_golden[f"i64patch_{eid}_page"]
+    got = pages.decode_int(page, None, np.uint64).view(np.int64)
+    assert np.array_equal(got, col_golden[f"i64patch_{eid}_input"])
