@@ -14,17 +14,18 @@ namespace flsgpu {
 // ---------------------------------------------------------------------------------------------------------
 // Kernel families
 // ---------------------------------------------------------------------------------------------------------
-// <max stream width, run-value staging bytes, max output bytes, warps per CTA, staging depth, gathers>
-#define FLS_NUM64 64, 0u, 8, 12, 2, false
-#define FLS_NUM32 32, 0u, 4, 15, 3, false
-#define FLS_GATHER 32, 0u, 8, 10, 2, true
-#define FLS_GATHER32 32, 0u, 4, 12, 2, true
-#define FLS_ANY 64, 8320u, 8, 6, 2, true
+// <max stream width, run-value staging bytes, max output bytes, warps per CTA, staging depth, item kinds>
+#define FLS_NUM64 64, 0u, 8, 12, 2, KIND_PLAIN
+#define FLS_NUM32 32, 0u, 4, 15, 3, KIND_PLAIN
+#define FLS_NUMPATCH 64, 0u, 8, 12, 2, KIND_PATCH
+#define FLS_GATHER 32, 0u, 8, 10, 2, KIND_GATHER
+#define FLS_GATHER32 32, 0u, 4, 12, 2, KIND_GATHER
+#define FLS_ANY 64, 8320u, 8, 6, 2, KIND_ALL
 
-template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES, bool GATHER>
+template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES, int KIND>
 static cudaError_t launch_family(const DecodeArgs& a, cudaStream_t s, int sm_count, int grid_override) {
-	using G            = Geometry<MAXWS, GSTAGE, EMAX, WARPS, STAGES, GATHER>;
-	auto*       kfn    = k_decode<MAXWS, GSTAGE, EMAX, WARPS, STAGES, GATHER>;
+	using G            = Geometry<MAXWS, GSTAGE, EMAX, WARPS, STAGES, KIND>;
+	auto*       kfn    = k_decode<MAXWS, GSTAGE, EMAX, WARPS, STAGES, KIND>;
 	// per device: the shared-memory attribute is set and the occupancy queried once
 	static int        occupancy[64] {};
 	static std::mutex mu;
@@ -66,9 +67,9 @@ struct Variant {
 	int         threads, smem;
 };
 
-template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES, bool GATHER>
+template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES, int KIND>
 static cudaError_t launch_variant(const DecodeArgs& a, cudaStream_t s, int sms, int grid) {
-	return launch_family<MAXWS, GSTAGE, EMAX, WARPS, STAGES, GATHER>(a, s, sms, grid);
+	return launch_family<MAXWS, GSTAGE, EMAX, WARPS, STAGES, KIND>(a, s, sms, grid);
 }
 
 #define FLS_VARIANT(label, ...)                                                                                   \
@@ -78,17 +79,19 @@ static cudaError_t launch_variant(const DecodeArgs& a, cudaStream_t s, int sms, 
 	}
 
 static const Variant kNum64[]    = {FLS_VARIANT("num64 12x2", FLS_NUM64),
-                                    FLS_VARIANT("num64 8x3", 64, 0u, 8, 8, 3, false),
-                                    FLS_VARIANT("num64 10x2", 64, 0u, 8, 10, 2, false)};
+                                    FLS_VARIANT("num64 8x3", 64, 0u, 8, 8, 3, KIND_PLAIN),
+                                    FLS_VARIANT("num64 10x2", 64, 0u, 8, 10, 2, KIND_PLAIN)};
 static const Variant kNum32[]    = {FLS_VARIANT("num32 15x3", FLS_NUM32),
-                                    FLS_VARIANT("num32 16x2", 32, 0u, 4, 16, 2, false),
-                                    FLS_VARIANT("num32 10x4", 32, 0u, 4, 10, 4, false)};
+                                    FLS_VARIANT("num32 16x2", 32, 0u, 4, 16, 2, KIND_PLAIN),
+                                    FLS_VARIANT("num32 10x4", 32, 0u, 4, 10, 4, KIND_PLAIN)};
+static const Variant kNumPatch[] = {FLS_VARIANT("numpatch 12x2", FLS_NUMPATCH),
+                                    FLS_VARIANT("numpatch 8x3", 64, 0u, 8, 8, 3, KIND_PATCH)};
 static const Variant kGather[]   = {FLS_VARIANT("gather 10x2", FLS_GATHER),
-                                    FLS_VARIANT("gather 8x3", 32, 0u, 8, 8, 3, true),
-                                    FLS_VARIANT("gather 12x2", 32, 0u, 8, 12, 2, true)};
+                                    FLS_VARIANT("gather 8x3", 32, 0u, 8, 8, 3, KIND_GATHER),
+                                    FLS_VARIANT("gather 12x2", 32, 0u, 8, 12, 2, KIND_GATHER)};
 static const Variant kGather32[] = {FLS_VARIANT("gather32 12x2", FLS_GATHER32),
-                                    FLS_VARIANT("gather32 12x3", 32, 0u, 4, 12, 3, true),
-                                    FLS_VARIANT("gather32 16x2", 32, 0u, 4, 16, 2, true)};
+                                    FLS_VARIANT("gather32 12x3", 32, 0u, 4, 12, 3, KIND_GATHER),
+                                    FLS_VARIANT("gather32 16x2", 32, 0u, 4, 16, 2, KIND_GATHER)};
 static const Variant kAny[]      = {FLS_VARIANT("any 6x2", FLS_ANY)};
 
 // The variants of a family; a NUM launch without a column array whose column is narrow runs the NUM32 kernels.
@@ -99,6 +102,7 @@ static const Variant* family_variants(Family fam, const DecodeArgs& a, int* n) {
 	case Family::NUM:
 		*n = 3;
 		return narrow ? kNum32 : kNum64;
+	case Family::NUM_PATCH: *n = 2; return kNumPatch;
 	case Family::GATHER: *n = 3; return kGather;
 	case Family::GATHER_NARROW: *n = 3; return kGather32;
 	default: *n = 1; return kAny;
@@ -431,10 +435,11 @@ struct fls_plan {
 	Family    family   = Family::NUM;
 	uint32_t  col_shift = 24;
 	ColDesc   col0 {};
-	// items [0, split) decode with `family`, items [split, n_items) with fam_b (0: one launch)
-	uint64_t  split = 0;
-	Family    fam_b = Family::GATHER;
-	int       variant[2] {0, 0};     // geometry variant of each segment (fls_plan_autotune)
+	// launch segments: items [seg_begin[i], seg_begin[i + 1]) of the queue on family seg_fam[i]
+	int       n_seg = 1;
+	uint64_t  seg_begin[kMaxSegments + 1] {};
+	Family    seg_fam[kMaxSegments] {};
+	int       variant[kMaxSegments] {}; // geometry variant of each segment (fls_plan_autotune)
 	std::vector<void*> owned;        // device buffers decoded for the plan (rec buffers)
 	cudaGraphExec_t graph = nullptr; // the segments' launches, captured by fls_plan_decode_graph
 	cudaStream_t    graph_stream = nullptr;
@@ -446,35 +451,41 @@ void plan_adopt(::fls_plan* plan, std::vector<void*>&& buffers) {
 }
 
 bool plan_segments(const std::vector<ColDesc>& descs, const std::vector<uint32_t>& queue, uint32_t col_shift,
-                   Family* fam_a, uint64_t* split, Family* fam_b) {
-	// a queue ordered family-major decodes as up to two launches, each on the kernel specialised for its
-	// items, instead of one launch of the catch-all kernel
-	auto     col = [&](uint32_t it) -> const ColDesc& { return descs.size() == 1 ? descs[0] : descs[it >> col_shift]; };
-	uint64_t s   = 0;
-	while (s < queue.size() && col(queue[s]).post == POST_NONE) { ++s; }
-	bool narrow_num = true, narrow_gather = true;
+                   Segments* out) {
+	// a queue ordered by item class (plain streams, patched streams, gathers) decodes as one launch per class
+	// present, each on the kernel specialised for it, instead of one launch of the catch-all kernel
+	auto col   = [&](uint32_t it) -> const ColDesc& { return descs.size() == 1 ? descs[0] : descs[it >> col_shift]; };
+	auto klass = [](const ColDesc& c) { return post_is_gather(c.post) ? 2 : post_is_patch(c.post) ? 1 : 0; };
+	bool narrow[3] = {true, true, true};
+	int  last      = -1;
+	Segments s {};
 	for (uint64_t i = 0; i < queue.size(); ++i) {
 		const ColDesc& c = col(queue[i]);
-		if ((i < s) != (c.post == POST_NONE)) {
-			*fam_a = Family::ANY;
-			*split = 0;
+		const int      k = klass(c);
+		if (k < last) {
+			*out         = Segments {};
+			out->n       = 1;
+			out->fam[0]  = Family::ANY;
+			out->begin[1] = queue.size();
 			return false;
 		}
-		if (i < s && (c.ws > 32 || c.e > 4)) { narrow_num = false; }
-		if (i >= s && (c.ws > 32 || c.e > 4)) { narrow_gather = false; }
+		if (k != last) {
+			s.begin[s.n] = i;
+			s.klass[s.n] = k;
+			++s.n;
+			last = k;
+		}
+		if (c.ws > 32 || c.e > 4) { narrow[k] = false; }
 	}
-	const Family num    = narrow_num ? Family::NUM_NARROW : Family::NUM;
-	const Family gather = narrow_gather ? Family::GATHER_NARROW : Family::GATHER;
-	*split              = 0;
-	if (s == queue.size()) {
-		*fam_a = num;
-	} else if (s == 0) {
-		*fam_a = gather;
-	} else {
-		*fam_a = num;
-		*fam_b = gather;
-		*split = s;
+	s.begin[s.n] = queue.size();
+	for (int i = 0; i < s.n; ++i) {
+		switch (s.klass[i]) {
+		case 0: s.fam[i] = narrow[0] ? Family::NUM_NARROW : Family::NUM; break;
+		case 1: s.fam[i] = Family::NUM_PATCH; break;
+		default: s.fam[i] = narrow[2] ? Family::GATHER_NARROW : Family::GATHER; break;
+		}
 	}
+	*out = s;
 	return true;
 }
 
@@ -485,13 +496,17 @@ int make_plan_object(const std::vector<ColDesc>& descs, const std::vector<uint32
 	p->n_cols    = static_cast<uint32_t>(descs.size());
 	p->family    = fam;
 	p->col_shift = col_shift;
+	p->seg_fam[0]   = fam;
+	p->seg_begin[1] = queue.size();
 	if (!queue.empty()) {
-		Family   a = fam, b = Family::GATHER;
-		uint64_t split = 0;
-		if (plan_segments(descs, queue, col_shift, &a, &split, &b)) {
-			p->family = a;
-			p->fam_b  = b;
-			p->split  = split;
+		Segments sg;
+		if (plan_segments(descs, queue, col_shift, &sg)) {
+			p->n_seg = sg.n;
+			for (int i = 0; i < sg.n; ++i) {
+				p->seg_begin[i] = sg.begin[i];
+				p->seg_fam[i]   = sg.fam[i];
+			}
+			p->seg_begin[sg.n] = sg.begin[sg.n];
 		}
 	}
 	if (descs.size() == 1) {
@@ -611,26 +626,20 @@ namespace {
 
 // The launch arguments of segment `seg` (0 or 1) of a plan; false when the plan has no such segment.
 bool segment_args(const fls_plan* p, int seg, DecodeArgs* a, Family* fam) {
+	if (seg < 0 || seg >= p->n_seg) { return false; }
 	DecodeArgs x {};
 	x.cols      = p->d_cols;
-	x.queue     = p->d_queue;
+	x.queue     = p->d_queue ? p->d_queue + p->seg_begin[seg] : nullptr;
 	x.col_shift = p->col_shift;
 	x.col0      = p->col0;
-	if (seg == 0) {
-		x.n_items = p->split ? p->split : p->n_items;
-		*fam      = p->family;
-	} else {
-		if (p->split == 0) { return false; }
-		x.queue   = p->d_queue + p->split;
-		x.n_items = p->n_items - p->split;
-		*fam      = p->fam_b;
-	}
-	*a = x;
+	x.n_items   = p->n_seg == 1 ? p->n_items : p->seg_begin[seg + 1] - p->seg_begin[seg];
+	*fam        = p->seg_fam[seg];
+	*a          = x;
 	return true;
 }
 
 int launch_segments(const fls_plan* p, int grid, cudaStream_t s) {
-	for (int seg = 0; seg < 2; ++seg) {
+	for (int seg = 0; seg < p->n_seg; ++seg) {
 		DecodeArgs a;
 		Family     fam;
 		if (!segment_args(p, seg, &a, &fam)) { break; }
@@ -679,7 +688,7 @@ int fls_plan_decode_graph(fls_plan* p, fls_stream_t stream) {
 		if (rc != FLS_OK) { return rc; }
 	}
 	if (cudaGraphLaunch(p->graph, static_cast<cudaStream_t>(stream)) != cudaSuccess) { return FLS_ERR_CUDA; }
-	launch_counter() += p->split ? 2 : 1;
+	launch_counter() += static_cast<uint64_t>(p->n_seg);
 	return FLS_OK;
 }
 
@@ -689,7 +698,7 @@ int fls_plan_autotune(fls_plan* p, int reps, fls_stream_t stream) {
 	cudaEvent_t  e0 = nullptr, e1 = nullptr;
 	if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) { return FLS_ERR_CUDA; }
 	int rc = FLS_OK;
-	for (int seg = 0; seg < 2 && rc == FLS_OK; ++seg) {
+	for (int seg = 0; seg < p->n_seg && rc == FLS_OK; ++seg) {
 		DecodeArgs a;
 		Family     fam;
 		if (!segment_args(p, seg, &a, &fam)) { break; }
@@ -721,7 +730,7 @@ int fls_plan_autotune(fls_plan* p, int reps, fls_stream_t stream) {
 }
 
 const char* fls_plan_variant_name(const fls_plan* p, int segment) {
-	if (!p || segment < 0 || segment > 1) { return ""; }
+	if (!p || segment < 0 || segment >= kMaxSegments) { return ""; }
 	DecodeArgs a;
 	Family     fam;
 	if (!segment_args(p, segment, &a, &fam)) { return ""; }
@@ -740,8 +749,8 @@ int fls_plan_destroy(fls_plan* p) {
 
 int fls_plan_geometry(const fls_plan* p, int* threads, int* smem_bytes, int* ctas_per_sm) {
 	if (!p || !threads || !smem_bytes || !ctas_per_sm) { return FLS_ERR_ARG; }
-	DecodeArgs a;
-	Family     fam;
+	DecodeArgs a {};
+	Family     fam = Family::NUM;
 	segment_args(p, 0, &a, &fam);
 	family_geometry(fam, a, p->variant[0], threads, smem_bytes, ctas_per_sm);
 	return FLS_OK;

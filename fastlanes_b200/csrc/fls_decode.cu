@@ -131,6 +131,17 @@ __device__ __forceinline__ Plan make_plan(const ColDesc& c, uint32_t v) {
 			if (olb + 128ull > c.buf_size[c.ib_lane_bases]) { p.ok = false; }
 			p.lane_bases = c.buf[c.ib_lane_bases] + olb;
 		}
+		if (post_is_patch(c.post)) {
+			// exceptions (gsrc, gbytes) and their positions / bitmap / chain head (dict, entry_c bytes)
+			const uint32_t oe = ep_of(c, v, c.ib_exc), os = ep_of(c, v, c.ib_side);
+			const uint64_t ee = (v + 1 < c.n_vec) ? ep_of(c, v + 1, c.ib_exc) : c.buf_size[c.ib_exc];
+			const uint64_t es = (v + 1 < c.n_vec) ? ep_of(c, v + 1, c.ib_side) : c.buf_size[c.ib_side];
+			if (ee < oe || ee > c.buf_size[c.ib_exc] || es < os || es > c.buf_size[c.ib_side]) { p.ok = false; }
+			p.gsrc    = c.buf[c.ib_exc] + oe;
+			p.gbytes  = p.ok ? static_cast<uint32_t>(ee - oe) : 0u;
+			p.dict    = c.buf[c.ib_side] + os;
+			p.entry_c = p.ok ? static_cast<uint32_t>(es - os) : 0u;
+		}
 		if (c.post == POST_RLE || c.post == POST_RLE_DICT) {
 			const uint32_t ov  = ep_of(c, v, c.ib_vals);
 			const uint64_t end = (v + 1 < c.n_vec) ? ep_of(c, v + 1, c.ib_vals) : c.buf_size[c.ib_vals];
@@ -213,9 +224,77 @@ struct StreamT<64> {
 	using T = uint64_t;
 };
 
+// Patch one vector's unpacked values (after the FOR add, before rsum) through `scratch` (1024 values in
+// transposed order; the stage the packed words came from, free once they are in registers).  Exceptions are
+// at p.gsrc (p.gbytes bytes), their positions / bitmap / chain head at p.dict (p.entry_c bytes).
 template <int WS>
+__device__ __forceinline__ void apply_patch(const Plan& p, typename StreamT<WS>::T (&v)[32], uint8_t* scratch,
+                                            uint32_t t, int* status) {
+	using T = typename StreamT<WS>::T;
+	if constexpr (WS == 32 || WS == 64) {
+		T*             s   = reinterpret_cast<T*>(scratch);
+		const uint32_t n_e = p.gbytes / sizeof(T);
+		__syncwarp();
+#pragma unroll
+		for (int q = 0; q < 32; ++q) { s[run_tpos<WS>(t, 0, q)] = v[q]; }
+		__syncwarp();
+		bool bad = false;
+		if (p.post == POST_PATCH_S) {
+			const uint32_t c = p.entry_c >= 2 ? static_cast<uint32_t>(ld_le(p.dict, 2)) : 0u;
+			bad              = p.entry_c < 2 || 2u + 2u * c > p.entry_c || c > n_e;
+			for (uint32_t i = t; !bad && i < c; i += 32) {
+				const uint32_t pos = static_cast<uint32_t>(ld_le(p.dict + 2 + 2 * i, 2));
+				if (pos < kVec) { s[pos] = static_cast<T>(ld_le(p.gsrc + static_cast<uint64_t>(i) * sizeof(T), sizeof(T))); }
+			}
+		} else if (p.post == POST_PATCH_B) {
+			// 16 bitmap words, one per lane 0..15; exceptions follow the set bits in ascending order
+			bad              = p.entry_c < 128;
+			const uint64_t w = (!bad && t < 16) ? ld_le(p.dict + 8 * t, 8) : 0ull;
+			const uint32_t c   = static_cast<uint32_t>(__popcll(w));
+			uint32_t       inc = c; // inclusive warp scan of the per-word counts
+#pragma unroll
+			for (uint32_t d = 1; d < 32; d <<= 1) {
+				const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, inc, d);
+				if (t >= d) { inc += y; }
+			}
+			const uint32_t i0  = inc - c;
+			const uint32_t tot = __shfl_sync(0xFFFFFFFFu, inc, 31);
+			bad |= tot > n_e;
+			uint64_t rest = bad ? 0ull : w;
+			for (uint32_t k = 0; rest != 0; ++k) {
+				const uint32_t r = __ffsll(static_cast<long long>(rest)) - 1;
+				rest &= rest - 1;
+				s[64 * t + r] = static_cast<T>(ld_le(p.gsrc + static_cast<uint64_t>(i0 + k) * sizeof(T), sizeof(T)));
+			}
+		} else if (t == 0) {
+			// LL: the packed value at an exception is the distance to the next one minus one
+			const uint32_t c     = p.entry_c >= 4 ? static_cast<uint32_t>(ld_le(p.dict, 2)) : 0u;
+			uint64_t       cur   = p.entry_c >= 4 ? ld_le(p.dict + 2, 2) : 0u;
+			const T        base  = static_cast<T>(p.for_base);
+			bad                  = p.entry_c < 4 || c > n_e;
+			for (uint32_t i = 0; !bad && i < c; ++i) {
+				if (cur >= kVec) {
+					bad = true;
+					break;
+				}
+				const T off = static_cast<T>(s[cur] - base + T(1));
+				s[cur]      = static_cast<T>(ld_le(p.gsrc + static_cast<uint64_t>(i) * sizeof(T), sizeof(T)));
+				cur += static_cast<uint64_t>(off);
+			}
+		}
+		if (__any_sync(0xFFFFFFFFu, bad) && t == 0) { atomicOr(status, STATUS_BAD_INDEX); }
+		__syncwarp();
+#pragma unroll
+		for (int q = 0; q < 32; ++q) { v[q] = s[run_tpos<WS>(t, 0, q)]; }
+		__syncwarp();
+	}
+}
+
+// PATCH: the kernel may meet patched items (plain-stream kernels and the catch-all one; gather kernels never do)
+template <int WS, bool PATCH = true>
 __device__ __forceinline__ void decode_stream(const Plan& p, const uint32_t* S, uint32_t t,
-                                              typename StreamT<WS>::T (&v)[32]) {
+                                              typename StreamT<WS>::T (&v)[32], uint8_t* scratch = nullptr,
+                                              int* status = nullptr) {
 	using T = typename StreamT<WS>::T;
 	if constexpr (WS == 64) {
 		extract_w64(S, t, p.bw, v);
@@ -231,6 +310,9 @@ __device__ __forceinline__ void decode_stream(const Plan& p, const uint32_t* S, 
 		const T base = static_cast<T>(p.for_base);
 #pragma unroll
 		for (int i = 0; i < 32; ++i) { v[i] = (v[i] + base) & wmask; }
+	}
+	if constexpr (PATCH) {
+		if (scratch && post_is_patch(p.post)) { apply_patch<WS>(p, v, scratch, t, status); }
 	}
 	if (p.enc == ENC_DELTA) {
 		// rsum: running sum along each lane in original order, seeded by the lane's base.
@@ -379,21 +461,26 @@ __device__ __forceinline__ void store_vector(const typename OutT<E>::T (&o)[32],
 // Full decode of one staged vector.
 // ---------------------------------------------------------------------------------------------------------
 // GSMEM: RLE run values / run codes staged in shared memory at gstage + ghead (else read from p.gsrc).
-// GATHER: the kernel handles RLE / DICT items (plain-stream kernels leave the gather code out and flag such an
-// item as a layout error).
-template <int WS, int E, bool GSMEM = true, bool GATHER = true>
+// KIND: bit 0 = the kernel handles RLE / DICT gathers, bit 1 = patched FFOR / DELTA items; a kernel that meets
+// an item outside its kind flags a layout error (plans never route one there).
+enum : int { KIND_PLAIN = 0, KIND_GATHER = 1, KIND_PATCH = 2, KIND_ALL = 3 };
+
+template <int WS, int E, bool GSMEM = true, int KIND = KIND_ALL>
 __device__ __forceinline__ void decode_vector(const Plan& p, const uint8_t* stage, const uint8_t* gstage, uint8_t* ost,
                                               uint32_t t, int* status) {
 	using ST = typename StreamT<WS>::T;
 	using OT = typename OutT<E>::T;
 	ST v[32];
-	decode_stream<WS>(p, reinterpret_cast<const uint32_t*>(stage), t, v);
+	constexpr bool GATHER = (KIND & KIND_GATHER) != 0;
+	constexpr bool PATCH  = (KIND & KIND_PATCH) != 0;
+	decode_stream<WS, PATCH>(p, reinterpret_cast<const uint32_t*>(stage), t, v, ost, status);
+	if (!PATCH && post_is_patch(p.post) && t == 0) { atomicOr(status, STATUS_BAD_LAYOUT); }
 	OT o[32];
 	bool bad = false;
-	if (!GATHER || p.post == POST_NONE) {
+	if (!GATHER || !post_is_gather(p.post)) {
 #pragma unroll
 		for (int i = 0; i < 32; ++i) { o[i] = static_cast<OT>(v[i]); }
-		if (!GATHER && p.post != POST_NONE && t == 0) { atomicOr(status, STATUS_BAD_LAYOUT); }
+		if (!GATHER && post_is_gather(p.post) && t == 0) { atomicOr(status, STATUS_BAD_LAYOUT); }
 	} else if (p.post == POST_RLE) {
 		// run values keep the byte alignment they have inside the page
 		const uint8_t* vals = GSMEM ? gstage + p.ghead : p.gsrc;
@@ -516,7 +603,7 @@ __device__ __forceinline__ Plan plan_of(const DecodeArgs& a, uint64_t item) {
 // output element size.  The original-order staging reuses the stage once its packed words are in registers,
 // so a slot is max(stream, output) bytes plus the run-value window.  Plans of the warp's next 2*PB items
 // live in shared memory (64 bytes each).
-template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES, bool GATHER = true>
+template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES, int KIND = KIND_ALL>
 struct Geometry {
 	static constexpr uint32_t kPB      = 16;
 	static constexpr uint32_t kStage   = MAXWS * 128u;
@@ -532,35 +619,35 @@ struct Geometry {
 	static_assert(kSmem <= 232448u, "at most 227 KB of shared memory per CTA");
 };
 
-template <int MAXWS, uint32_t GSTAGE, int EMAX, bool GATHER>
+template <int MAXWS, uint32_t GSTAGE, int EMAX, int KIND>
 __device__ __forceinline__ void decode_dispatch(const Plan& p, uint8_t* st, const uint8_t* gs, uint32_t lane,
                                                 int* status) {
 	if (p.ws == 64) {
-		if constexpr (MAXWS >= 64) { decode_vector<64, 8, (GSTAGE > 0), GATHER>(p, st, gs, st, lane, status); }
+		if constexpr (MAXWS >= 64) { decode_vector<64, 8, (GSTAGE > 0), KIND>(p, st, gs, st, lane, status); }
 	} else if (p.ws == 32) {
 		if constexpr (MAXWS >= 32) {
 			if (p.e == 8) {
-				if constexpr (EMAX >= 8) { decode_vector<32, 8, (GSTAGE > 0), GATHER>(p, st, gs, st, lane, status); }
+				if constexpr (EMAX >= 8) { decode_vector<32, 8, (GSTAGE > 0), KIND>(p, st, gs, st, lane, status); }
 			} else {
-				decode_vector<32, 4, (GSTAGE > 0), GATHER>(p, st, gs, st, lane, status);
+				decode_vector<32, 4, (GSTAGE > 0), KIND>(p, st, gs, st, lane, status);
 			}
 		}
 	} else if (p.ws == 16) {
 		if (p.e == 8) {
-			if constexpr (EMAX >= 8) { decode_vector<16, 8, (GSTAGE > 0), GATHER>(p, st, gs, st, lane, status); }
+			if constexpr (EMAX >= 8) { decode_vector<16, 8, (GSTAGE > 0), KIND>(p, st, gs, st, lane, status); }
 		} else if (p.e == 4) {
-			if constexpr (EMAX >= 4) { decode_vector<16, 4, (GSTAGE > 0), GATHER>(p, st, gs, st, lane, status); }
+			if constexpr (EMAX >= 4) { decode_vector<16, 4, (GSTAGE > 0), KIND>(p, st, gs, st, lane, status); }
 		} else {
-			decode_vector<16, 2, (GSTAGE > 0), GATHER>(p, st, gs, st, lane, status);
+			decode_vector<16, 2, (GSTAGE > 0), KIND>(p, st, gs, st, lane, status);
 		}
 	} else {
-		decode_vector<8, 1, (GSTAGE > 0), GATHER>(p, st, gs, st, lane, status);
+		decode_vector<8, 1, (GSTAGE > 0), KIND>(p, st, gs, st, lane, status);
 	}
 }
 
-template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES, bool GATHER>
+template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES, int KIND>
 __global__ void __launch_bounds__(WARPS * 32, 1) k_decode(const DecodeArgs a) {
-	using G = Geometry<MAXWS, GSTAGE, EMAX, WARPS, STAGES, GATHER>;
+	using G = Geometry<MAXWS, GSTAGE, EMAX, WARPS, STAGES, KIND>;
 	constexpr uint32_t PB = G::kPB;
 	extern __shared__ __align__(128) uint8_t smem[];
 	const uint32_t lane   = threadIdx.x & 31u;
@@ -625,7 +712,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_decode(const DecodeArgs a) {
 		} else {
 			// the lane bases were staged with the packed words
 			if (p.lane_bases) { p.lane_bases = lb_ptr(s) + (reinterpret_cast<uintptr_t>(p.lane_bases) & 15u); }
-			decode_dispatch<MAXWS, GSTAGE, EMAX, GATHER>(p, stage_ptr(s), gstage_ptr(s), lane, a.status);
+			decode_dispatch<MAXWS, GSTAGE, EMAX, KIND>(p, stage_ptr(s), gstage_ptr(s), lane, a.status);
 		}
 		__syncwarp();
 		issue_k(k + STAGES, s);

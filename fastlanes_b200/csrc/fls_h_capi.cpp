@@ -285,7 +285,7 @@ int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_
 	uint8_t* dp = d_page.as<uint8_t>() + shift;
 	// _REC variants: the rec-compressed value buffer goes over whole and is decoded first (on the copy stream,
 	// so every chunk's decode is ordered after it)
-	const int rec_b = pi.layout->rec_vals ? pi.layout->ib_vals : -1;
+	const int rec_b = pi.layout->ib_rec != kNoBuf ? pi.layout->ib_rec : -1;
 	DevBuf    d_rec(hp->in);
 	uint64_t  rec_n = 0;
 	if (rec_b >= 0) {
@@ -325,9 +325,10 @@ int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_
 			}
 		}
 	} guard {ev};
-	const Family fam = pi.layout->post == POST_NONE ? Family::NUM
-	                   : c.e <= 4                   ? Family::GATHER_NARROW
-	                                                : Family::GATHER;
+	const Family fam = post_is_patch(pi.layout->post)    ? Family::NUM_PATCH
+	                   : !post_is_gather(pi.layout->post) ? Family::NUM
+	                   : c.e <= 4                         ? Family::GATHER_NARROW
+	                                                      : Family::GATHER;
 	// page header, buffer offsets and entry points first, with the queue
 	if (cudaMemcpyAsync(dp, page, pi.meta_sz, cudaMemcpyHostToDevice, hp->in) != cudaSuccess ||
 	    cudaMemcpyAsync(d_queue.p, ids.data(), 4ull * pi.vec_c, cudaMemcpyHostToDevice, hp->in) != cudaSuccess) {

@@ -23,22 +23,32 @@
 namespace flsgpu {
 
 const ExprLayout* expr_layout(uint8_t exp_t, uint8_t var) {
-	// exp_t, var, arr_c, stream width (0 = value width), enc, post, roles: bw, base, packed, lane, vals, rec
+	// exp_t, var, arr_c, stream width (0 = value width), enc, post, roles: bw, base, packed, lane, vals, rec buffer,
+	// exceptions, positions
+	constexpr uint8_t N = kNoBuf;
 	static const ExprLayout table[] = {
-	    {2, 1, 1, 0, ENC_RAW, POST_NONE, kNoBuf, kNoBuf, 0, kNoBuf, kNoBuf, false},        // UNCOMPRESSED
-	    {4, 1, 3, 0, ENC_FFOR, POST_NONE, 0, 1, 2, kNoBuf, kNoBuf, false},                  // FFOR NO_PATCH
-	    {5, 1, 4, 0, ENC_DELTA, POST_NONE, 1, 2, 3, 0, kNoBuf, false},                      // DELTA NO_PATCH
-	    {6, 1, 2, 16, ENC_RAW, POST_RLE, kNoBuf, kNoBuf, 1, kNoBuf, 0, false},               // RLE UNCOMPRESSED
-	    {6, 2, 5, 16, ENC_DELTA, POST_RLE, 2, 3, 4, 1, 0, false},                            // RLE DELTA_NO_PATCH
-	    {6, 3, 2, 16, ENC_RAW, POST_RLE, kNoBuf, kNoBuf, 1, kNoBuf, 0, true},                // RLE UNCOMPRESSED_REC
-	    {6, 4, 5, 16, ENC_DELTA, POST_RLE, 2, 3, 4, 1, 0, true},                             // RLE DELTA_NO_PATCH_REC
-	    {8, 1, 1, 32, ENC_RAW, POST_DICT, kNoBuf, kNoBuf, 0, kNoBuf, kNoBuf, false},         // DICT UNCOMPRESSED
-	    {8, 2, 3, 32, ENC_FFOR, POST_DICT, 0, 1, 2, kNoBuf, kNoBuf, false},                  // DICT FFOR_NO_PATCH
-	    {8, 7, 4, 32, ENC_DELTA, POST_DICT, 1, 2, 3, 0, kNoBuf, false},                      // DICT DELTA_NO_PATCH
-	    {11, 1, 2, 16, ENC_RAW, POST_RLE_DICT, kNoBuf, kNoBuf, 1, kNoBuf, 0, false},         // DICT_RLE UNCOMPRESSED
-	    {11, 2, 5, 16, ENC_DELTA, POST_RLE_DICT, 2, 3, 4, 1, 0, false},                      // DICT_RLE DELTA_NO_PATCH
-	    {11, 3, 2, 16, ENC_RAW, POST_RLE_DICT, kNoBuf, kNoBuf, 1, kNoBuf, 0, true},          // DICT_RLE UNCOMPRESSED_REC
-	    {11, 4, 5, 16, ENC_DELTA, POST_RLE_DICT, 2, 3, 4, 1, 0, true},                       // DICT_RLE ..._REC
+	    {2, 1, 1, 0, ENC_RAW, POST_NONE, N, N, 0, N, N, N, N, N},                     // UNCOMPRESSED
+	    {4, 1, 3, 0, ENC_FFOR, POST_NONE, 0, 1, 2, N, N, N, N, N},                    // FFOR NO_PATCH
+	    {4, 2, 5, 0, ENC_FFOR, POST_PATCH_LL, 2, 3, 4, N, N, N, 0, 1},                // FFOR LL_PATCH
+	    {4, 3, 5, 0, ENC_FFOR, POST_PATCH_S, 2, 3, 4, N, N, N, 0, 1},                 // FFOR S_PATCH
+	    {4, 4, 5, 0, ENC_FFOR, POST_PATCH_B, 2, 3, 4, N, N, N, 0, 1},                 // FFOR B_PATCH
+	    {4, 5, 5, 0, ENC_FFOR, POST_PATCH_S, 2, 3, 4, N, N, 0, 0, 1},                 // FFOR S_PATCH_REC
+	    {5, 1, 4, 0, ENC_DELTA, POST_NONE, 1, 2, 3, 0, N, N, N, N},                   // DELTA NO_PATCH
+	    {5, 2, 6, 0, ENC_DELTA, POST_PATCH_LL, 3, 4, 5, 0, N, N, 1, 2},               // DELTA LL_PATCH
+	    {5, 3, 6, 0, ENC_DELTA, POST_PATCH_S, 3, 4, 5, 0, N, N, 1, 2},                // DELTA S_PATCH
+	    {5, 4, 6, 0, ENC_DELTA, POST_PATCH_B, 3, 4, 5, 0, N, N, 1, 2},                // DELTA B_PATCH
+	    {5, 5, 6, 0, ENC_DELTA, POST_PATCH_B, 3, 4, 5, 0, N, 1, 1, 2},                // DELTA B_PATCH_REC
+	    {6, 1, 2, 16, ENC_RAW, POST_RLE, N, N, 1, N, 0, N, N, N},                     // RLE UNCOMPRESSED
+	    {6, 2, 5, 16, ENC_DELTA, POST_RLE, 2, 3, 4, 1, 0, N, N, N},                   // RLE DELTA_NO_PATCH
+	    {6, 3, 2, 16, ENC_RAW, POST_RLE, N, N, 1, N, 0, 0, N, N},                     // RLE UNCOMPRESSED_REC
+	    {6, 4, 5, 16, ENC_DELTA, POST_RLE, 2, 3, 4, 1, 0, 0, N, N},                   // RLE DELTA_NO_PATCH_REC
+	    {8, 1, 1, 32, ENC_RAW, POST_DICT, N, N, 0, N, N, N, N, N},                    // DICT UNCOMPRESSED
+	    {8, 2, 3, 32, ENC_FFOR, POST_DICT, 0, 1, 2, N, N, N, N, N},                   // DICT FFOR_NO_PATCH
+	    {8, 7, 4, 32, ENC_DELTA, POST_DICT, 1, 2, 3, 0, N, N, N, N},                  // DICT DELTA_NO_PATCH
+	    {11, 1, 2, 16, ENC_RAW, POST_RLE_DICT, N, N, 1, N, 0, N, N, N},               // DICT_RLE UNCOMPRESSED
+	    {11, 2, 5, 16, ENC_DELTA, POST_RLE_DICT, 2, 3, 4, 1, 0, N, N, N},             // DICT_RLE DELTA_NO_PATCH
+	    {11, 3, 2, 16, ENC_RAW, POST_RLE_DICT, N, N, 1, N, 0, 0, N, N},               // DICT_RLE UNCOMPRESSED_REC
+	    {11, 4, 5, 16, ENC_DELTA, POST_RLE_DICT, 2, 3, 4, 1, 0, 0, N, N},             // DICT_RLE ..._REC
 	};
 	for (const auto& e : table) {
 		if (e.exp_t == exp_t && e.var == var) { return &e; }
@@ -95,7 +105,7 @@ int build_page_column(const PageInfo& pi, const uint8_t* d_page, int value_width
 	const ExprLayout* L = pi.layout;
 	if (!L || value_width == 0) { return FLS_ERR_UNSUPPORTED; }
 	// the page-level rec buffer of the _REC variants is decoded by the caller (rec_decode)
-	if (L->rec_vals && !d_vals_decoded) { return FLS_ERR_UNSUPPORTED; }
+	if (L->ib_rec != kNoBuf && !d_vals_decoded) { return FLS_ERR_UNSUPPORTED; }
 	*c        = ColDesc {};
 	c->ws     = static_cast<uint8_t>(L->ws ? L->ws : value_width);
 	c->e      = static_cast<uint8_t>(value_width / 8);
@@ -110,13 +120,15 @@ int build_page_column(const PageInfo& pi, const uint8_t* d_page, int value_width
 	c->ib_packed = L->ib_packed;
 	c->ib_lane_bases = L->ib_lane;
 	c->ib_vals = L->ib_vals;
+	c->ib_exc  = L->ib_exc;
+	c->ib_side = L->ib_side;
 	for (uint32_t i = 0; i < pi.arr_c; ++i) {
 		c->buf[i]      = d_page + pi.off[i];
 		c->buf_size[i] = pi.size[i];
 	}
-	if (L->rec_vals) {
-		c->buf[L->ib_vals]      = d_vals_decoded;
-		c->buf_size[L->ib_vals] = vals_decoded_size;
+	if (L->ib_rec != kNoBuf) {
+		c->buf[L->ib_rec]      = d_vals_decoded;
+		c->buf_size[L->ib_rec] = vals_decoded_size;
 	}
 	c->ep  = reinterpret_cast<const uint32_t*>(d_page + pi.ep_off);
 	c->out = d_out;
@@ -182,8 +194,8 @@ static int read_on(void* dst, const void* src, size_t n, cudaStream_t stream) {
 // Work items of page plans: (column << kPageShift | vector); a page holds at most 65,535 vectors.
 constexpr uint32_t kPageShift = 16;
 
-// Element bytes of a layout's rec-compressed value buffer: run codes are idx_t = uint32, run values the
-// column's values.
+// Element bytes of a layout's rec-compressed buffer: run codes are idx_t = uint32, run values and exceptions
+// the column's values.
 static uint32_t rec_elem_bytes(const ExprLayout* L, int value_width) {
 	return L->post == POST_RLE_DICT ? 4u : static_cast<uint32_t>(value_width / 8);
 }
@@ -243,8 +255,8 @@ static int describe_pages(const fls_page_column* cols, uint32_t n_cols, std::vec
 		}
 		const uint8_t* rvals = nullptr;
 		uint64_t       rsize = 0;
-		if (pi.layout->rec_vals) {
-			const uint32_t b = pi.layout->ib_vals;
+		if (pi.layout->ib_rec != kNoBuf) {
+			const uint32_t b = pi.layout->ib_rec;
 			rc = decode_rec_on(pc.d_page + pi.off[b], pi.size[b], rec_elem_bytes(pi.layout, w), owned, &rvals, &rsize,
 			                   stream);
 			if (rc != FLS_OK) { return rc; }
@@ -252,16 +264,17 @@ static int describe_pages(const fls_page_column* cols, uint32_t n_cols, std::vec
 		rc = build_page_column(pi, pc.d_page, w, dvals, entries, pc.order, static_cast<uint8_t*>(pc.d_out),
 		                       &(*descs)[i], rvals, rsize);
 		if (rc != FLS_OK) { return rc; }
-		if ((*descs)[i].post != POST_NONE) { fam = Family::GATHER; }
+		if (post_is_gather((*descs)[i].post)) { fam = Family::GATHER; }
 		if ((*descs)[i].ws == 64) { any64 = true; }
 		for (uint32_t v = 0; v < pi.vec_c; ++v) { queue->push_back((i << kPageShift) | v); }
 	}
 	// group the work items by kernel specialisation so that warps run long stretches of one code path (the
 	// outputs do not depend on the order)
-	// family-major: plain streams first, then gathers (a plan then launches each family's own kernel)
+	// class-major: plain streams, patched streams, gathers (a plan then launches each class's own kernel)
 	auto key = [&](uint32_t it) {
 		const ColDesc& c = (*descs)[it >> kPageShift];
-		return ((c.post != POST_NONE ? 1u : 0u) << 31) | (static_cast<uint32_t>(c.ws) << 24) | (c.e << 16) |
+		const uint32_t klass = post_is_gather(c.post) ? 2u : post_is_patch(c.post) ? 1u : 0u;
+		return (klass << 30) | (static_cast<uint32_t>(c.ws) << 23) | (c.e << 16) |
 		       (c.enc << 8) | (c.post << 4) | c.order;
 	};
 	if (n_cols > 1) {
@@ -288,15 +301,14 @@ int fls_gpu_decode_pages(const fls_page_column* cols, uint32_t n_cols, fls_strea
 	int rc = describe_pages(cols, n_cols, &descs, &queue, &fam, s, &owned);
 	if (rc != FLS_OK) { return rc; }
 	if (queue.empty()) { return FLS_OK; }
-	DecodeArgs   a {};
+	DecodeArgs a {};
 	a.col_shift = kPageShift;
-	Family   fa = fam, fb = Family::GATHER;
-	uint64_t split = 0;
-	plan_segments(descs, queue, kPageShift, &fa, &split, &fb);
+	Segments sg; // the queue is class-ordered above; an unordered one would run on the catch-all kernel
+	plan_segments(descs, queue, kPageShift, &sg);
 	if (n_cols == 1) {
 		a.col0    = descs[0];
 		a.n_items = queue.size();
-		return launch_decode(fa, a, s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
+		return launch_decode(sg.fam[0], a, s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
 	}
 	ColDesc*  d_cols  = nullptr;
 	uint32_t* d_queue = nullptr;
@@ -304,15 +316,13 @@ int fls_gpu_decode_pages(const fls_page_column* cols, uint32_t n_cols, fls_strea
 	if (cudaMallocAsync(&d_queue, sizeof(uint32_t) * queue.size(), s) != cudaSuccess) { return FLS_ERR_CUDA; }
 	cudaMemcpyAsync(d_cols, descs.data(), sizeof(ColDesc) * n_cols, cudaMemcpyHostToDevice, s);
 	cudaMemcpyAsync(d_queue, queue.data(), sizeof(uint32_t) * queue.size(), cudaMemcpyHostToDevice, s);
-	a.cols    = d_cols;
-	a.queue   = d_queue;
-	a.n_items = split ? split : queue.size();
+	a.cols = d_cols;
 	// copies from pageable host memory are staged before cudaMemcpyAsync returns, so descs/queue may go away
-	cudaError_t e = launch_decode(fa, a, s);
-	if (e == cudaSuccess && split) {
-		a.queue   = d_queue + split;
-		a.n_items = queue.size() - split;
-		e         = launch_decode(fb, a, s);
+	cudaError_t e = cudaSuccess;
+	for (int i = 0; i < sg.n && e == cudaSuccess; ++i) {
+		a.queue   = d_queue + sg.begin[i];
+		a.n_items = sg.begin[i + 1] - sg.begin[i];
+		e         = launch_decode(sg.fam[i], a, s);
 	}
 	cudaFreeAsync(d_cols, s);
 	cudaFreeAsync(d_queue, s);

@@ -11,7 +11,8 @@ struct ExprLayout {
 	uint8_t ws; // stream width in bits; 0 = the column's value width
 	uint8_t enc, post;
 	uint8_t ib_bw, ib_base, ib_packed, ib_lane, ib_vals;
-	bool    rec_vals; // buffer ib_vals is a rec buffer (..._REC variants)
+	uint8_t ib_rec;          // the rec-compressed buffer of the ..._REC variants (kNoBuf: none)
+	uint8_t ib_exc, ib_side; // patched variants: exception values, positions / bitmap / chain head
 };
 
 struct PageInfo {

@@ -22,7 +22,22 @@ enum : uint8_t {
 	POST_RLE      = 1, // stream is a u16 run index; output = run_values[index]
 	POST_DICT     = 2, // stream is u32 codes; output = dict[code]
 	POST_RLE_DICT = 3, // stream is a u16 run index into u32 codes; output = dict[codes[index]]
+	// patched FFOR / DELTA: the unpacked values (transposed positions) are patched before rsum
+	// (src/cor/prm/patch/*_decompress.cpp)
+	POST_PATCH_S  = 4, // exceptions + (exc_c u16, exc_c u16 positions)
+	POST_PATCH_B  = 5, // exceptions + 1024-bit position bitmap (16 u64 words), exceptions in bit order
+	POST_PATCH_LL = 6, // exceptions + (exc_c u16, first position u16); gaps chained through the packed values
 };
+
+// RLE / DICT gathers read a second array per value (gather kernels); patches stay in the plain kernels.
+#ifdef __CUDACC__
+__host__ __device__
+#endif
+constexpr bool post_is_gather(uint32_t post) { return post >= POST_RLE && post <= POST_RLE_DICT; }
+#ifdef __CUDACC__
+__host__ __device__
+#endif
+constexpr bool post_is_patch(uint32_t post) { return post >= POST_PATCH_S && post <= POST_PATCH_LL; }
 
 enum : uint8_t {
 	LAYOUT_ARRAYS = 0,
@@ -45,7 +60,9 @@ struct alignas(16) ColDesc {
 	uint32_t entry_c; // dictionary entries (POST_DICT / POST_RLE_DICT)
 
 	// LAYOUT_PAGE: role -> buffer index (kNoBuf when absent) and resolved buffer starts
-	uint8_t  ib_bw, ib_base, ib_packed, ib_lane_bases, ib_vals, pad0[3];
+	uint8_t  ib_bw, ib_base, ib_packed, ib_lane_bases, ib_vals;
+	uint8_t  ib_exc, ib_side; // patched variants: exception values, positions / bitmap / chain head
+	uint8_t  pad0;
 	const uint8_t*  buf[6];
 	uint64_t        buf_size[6];
 	const uint32_t* ep; // entry points, (n_vec - 1) x arr_c u32; vector 0 starts at 0 in every buffer

@@ -16,6 +16,16 @@ enum class Family : int {
 	ANY           = 2, // everything
 	NUM_NARROW    = 3, // NUM with every stream and output at most 32 bits
 	GATHER_NARROW = 4, // GATHER with outputs of at most 4 bytes
+	NUM_PATCH     = 5, // NUM items with patches (S / B / LL) applied before rsum
+};
+
+// Launch segments of a queue ordered by item class (plain, patched, gather): at most one per class.
+constexpr int kMaxSegments = 3;
+struct Segments {
+	int      n = 0;
+	uint64_t begin[kMaxSegments + 1] {};
+	int      klass[kMaxSegments] {};
+	Family   fam[kMaxSegments] {};
 };
 
 // Per-device state: SM count and the library-owned status word.
@@ -39,11 +49,10 @@ const char* family_variant_name(Family fam, const DecodeArgs& args, int variant)
 // CTAs resident per SM).
 void family_geometry(Family fam, const DecodeArgs& args, int variant, int* threads, int* smem, int* ctas_per_sm);
 
-// Kernel families for a queue: when the items are ordered family-major (plain streams first, then gathers),
-// items [0, *split) run on *fam_a and [*split, n) on *fam_b (*split = 0: all on *fam_a).  Returns false (and
-// Family::ANY) for an unordered queue.
+// Kernel families for a queue of (col << col_shift | vec) items ordered by class (plain streams, patched
+// streams, gathers): one segment per class present.  Returns false (one ANY segment) for an unordered queue.
 bool plan_segments(const std::vector<ColDesc>& descs, const std::vector<uint32_t>& queue, uint32_t col_shift,
-                   Family* fam_a, uint64_t* split, Family* fam_b);
+                   Segments* out);
 
 // Build a plan object from descriptors + queue of (col << col_shift | vec) items (uploads both; a single column
 // without a queue stays inline).

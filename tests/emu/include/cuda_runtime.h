@@ -57,6 +57,16 @@ T __shfl_sync(unsigned, T v, int src) {
 	__syncwarp();
 	return r;
 }
+template <class T>
+T __shfl_up_sync(unsigned, T v, unsigned d) {
+	g_emu_warp->xch[g_emu_lane] = static_cast<uint64_t>(v);
+	__syncwarp();
+	const T r = g_emu_lane >= static_cast<int>(d) ? static_cast<T>(g_emu_warp->xch[g_emu_lane - d]) : v;
+	__syncwarp();
+	return r;
+}
+inline int __popcll(unsigned long long x) { return __builtin_popcountll(x); }
+inline int __ffsll(long long x) { return __builtin_ffsll(x); }
 inline bool __any_sync(unsigned, bool p) {
 	g_emu_warp->vote[g_emu_lane] = p ? 1 : 0;
 	__syncwarp();

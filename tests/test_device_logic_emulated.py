@@ -137,3 +137,20 @@ def test_emulated_rejects_dictionary_code_out_of_range(emu, col_golden):
     out = np.zeros(3 * 1024, np.uint64)
     st = emu.emu_decode_page(P(page), ctypes.c_uint64(page.size), P(dic), ctypes.c_uint64(dic.size), 64, 1, P(out))
     assert st & 4
+
+
+@pytest.mark.parametrize("eid", [2, 4, 5, 12, 13, 14])
+@pytest.mark.parametrize("order", [0, 1])
+def test_emulated_reference_patched_pages(emu, col_golden, eid, order):
+    """Patched FFOR / DELTA pages of the reference (S / B / LL patches) through the device decode logic."""
+    page = col_golden[f"i64patch_{eid}_page"]
+    want = col_golden[f"i64patch_{eid}_input"]
+    out = np.zeros(want.size, np.int64)
+    st = emu.emu_decode_page(P(page), ctypes.c_uint64(page.size), None, ctypes.c_uint64(0), 64, order, P(out))
+    assert st == 0, st
+    if order == 1:
+        assert np.array_equal(out, want)
+    else:
+        tw = np.concatenate([oracle.transpose_i(want.view(np.uint64)[v * 1024:(v + 1) * 1024]) for v in
+                             range(want.size // 1024)]).view(np.int64)
+        assert np.array_equal(out, tw)

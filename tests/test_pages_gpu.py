@@ -242,3 +242,33 @@ def test_reference_rec_pages(cuda, col_golden, eid, shift):
     plan.close()
     if not dic.size:
         assert np.array_equal(pages.decode_to_memory(page, pages.INT64), want)
+
+
+@pytest.mark.parametrize("eid", [2, 3, 4, 5, 12, 13, 14, 15])
+@pytest.mark.parametrize("shift", [0, 5])
+def test_reference_patched_pages(cuda, col_golden, eid, shift):
+    """Patched FFOR / DELTA pages of the reference (S / B / LL patches, rec-compressed exceptions) decode
+    bit-exactly one-shot, through a page plan (both orders) and through decode_to_memory."""
+    import torch
+
+    from fastlanes_b200 import pages
+
+    page, want = col_golden[f"i64patch_{eid}_page"], col_golden[f"i64patch_{eid}_input"]
+    pbuf, pptr = _dev_bytes(page, cuda, shift)
+    out = torch.zeros(want.size, dtype=torch.int64, device=cuda)
+    pages.decode_pages([dict(d_page=pptr, page_size=page.size, data_type=pages.INT64, order=1, d_out=out.data_ptr())])
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), want)
+    for order in (0, 1):
+        out.zero_()
+        plan = pages.PagePlan([dict(d_page=pptr, page_size=page.size, data_type=pages.INT64, order=order,
+                                    d_out=out.data_ptr())])
+        plan.decode()
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        if order == 0:
+            got = np.concatenate([oracle.untranspose_i(got[v * 1024:(v + 1) * 1024].view(np.uint64).copy())
+                                  for v in range(want.size // 1024)]).view(np.int64)
+        assert np.array_equal(got, want), order
+        plan.close()
+    assert np.array_equal(pages.decode_to_memory(page, pages.INT64), want)
