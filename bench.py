@@ -359,9 +359,11 @@ def other_configs(dev, args):
 
 
 def mixed_rowgroups(dev, peak, steps):
-    """Mixed row groups: the learned selector trained on wizard-labelled vectors, selection timed against the
-    exact-size GPU wizard on 256 integer columns, every chunk encoded with its choice, all chunks decoded by one
-    persistent launch (bit-exact checked before timing)."""
+    """Mixed row groups: 256 columns of 64 Ki..4 Mi values, types uniform over FOR / delta / RLE / int32
+    dictionary / FSST strings.  The learned selector (trained here on wizard-labelled vectors) chooses every
+    integer chunk's expression, timed against the exact-size GPU wizard; string columns are DICT pages over
+    FSST dictionaries.  Every chunk of every column decodes from one CUDA graph (the integer plan's launches
+    and the string plans'), bit-exact checked before timing."""
     import time
 
     import torch
@@ -391,7 +393,7 @@ def mixed_rowgroups(dev, peak, steps):
     hist = SL.train(params, feat, y, epochs=10, batch=1024, lr=2e-3)
     t_train = time.perf_counter() - t0
     rng = np.random.default_rng(1)
-    cols = [W.selection_column(rng, int(rng.integers(64, 4097)), str(dev)) for _ in range(256)]
+    cols, str_cols = W.mixed_rowgroup_columns(rng, 256, str(dev))
     plan = SL.SelectionPlan(cols)
     stride, thr = 8, 0.7
     ms_wiz, (sizes, best, _) = host_timed(plan.wizard)
@@ -399,26 +401,47 @@ def mixed_rowgroups(dev, peak, steps):
     loss = SL.ratio_loss(sizes, choice)
     agree = float((choice == best).float().mean())
     rg = RG.RowGroupSet(cols, plan.chunks(), choice.cpu().numpy(), dev)
+    ss = RG.StringColumnSet(str_cols, dev)
     tuned = rg.autotune()
     for o in rg.outputs:
         o.zero_()
-    rg.decode()  # graph replay of the plan's launches
+    rg.decode(graph=False)
+    ss.decode()
     torch.cuda.synchronize()
-    ok = all(torch.equal(o, t) for o, (t, _) in zip(rg.outputs, cols))
-    ms = device_timed(rg.decode, steps, 3)
-    read_b, write_b = rg.page_bytes + rg.dict_bytes, rg.value_bytes
+    ok = all(torch.equal(o, t) for o, (t, _) in zip(rg.outputs, cols)) and ss.check(str_cols)
+    # one graph: the integer plan's segments and every string column's lengths / scan / materialize launches
+    graph = torch.cuda.CUDAGraph()
+    side = [torch.cuda.Stream() for _ in range(8)]
+    with torch.cuda.graph(graph):
+        ss.decode(side)  # the string columns on eight branches of the graph
+        rg.decode(graph=False)
+    graph.replay()
+    torch.cuda.synchronize()
+    ok = ok and all(torch.equal(o, t) for o, (t, _) in zip(rg.outputs, cols)) and ss.check(str_cols, 64, 9)
+    ms = device_timed(graph.replay, steps, 3)
+    read_b = rg.page_bytes + rg.dict_bytes + ss.page_bytes + ss.dict_bytes
+    write_b = rg.value_bytes + ss.value_bytes
+    n_vals = rg.values + ss.rows
     res = {
-        "workload": (f"256 integer columns of U[64Ki,4Mi] values ({rg.values} values, {len(plan.chunks()[0])} "
-                     "64Ki-row chunks; FOR u32/i64, sorted i64 delta, RLE, int32 Zipf dictionaries, dictionary "
-                     "runs, noise), every chunk encoded with the learned choice, decoded by one page plan"),
+        "workload": (f"256 columns of U[64Ki,4Mi] values, types uniform over FOR u32/i64, sorted i64 delta, RLE, "
+                     f"int32 Zipf dictionaries, FSST strings ({len(cols)} integer columns, {rg.values} values, "
+                     f"{plan.n_chunks} 64Ki-row chunks; {len(str_cols)} string columns, {ss.rows} rows); integer "
+                     "chunks encoded with the learned choice, strings as DICT over FSST dictionaries; one CUDA "
+                     "graph decodes everything"),
         "value": round(write_b / (ms * 1e-3) / 1e9, 2), "unit": "GB/s", "ms_per_step": round(ms, 4),
-        "decoded_values_per_s": round(rg.values / (ms * 1e-3), 1), "bytes_per_step": read_b + write_b,
+        "decoded_values_per_s": round(n_vals / (ms * 1e-3), 1), "bytes_per_step": read_b + write_b,
         "roofline_frac": round((read_b + write_b) / (ms * 1e-3) / 1e9 / peak, 4), "parity": bool(ok),
-        "gpu_launches_per_step": len(tuned), "graph_launches_per_step": 1, "autotuned": tuned,
+        "gpu_launches_per_step": len(tuned) + 3 * len(str_cols), "graph_launches_per_step": 1, "autotuned": tuned,
+        "graph": "integer plan segments + the string columns' launches on eight parallel branches",
+        "integer_part": {"values": rg.values, "read_bytes": rg.page_bytes + rg.dict_bytes,
+                         "written_bytes": rg.value_bytes},
+        "string_part": {"rows": ss.rows, "read_bytes": ss.page_bytes + ss.dict_bytes, "written_bytes": ss.value_bytes,
+                        "expression": "DICT FFOR_NO_PATCH over an FSST dictionary (string pool id 3), not selected"},
         "selection": {
             "learned_ms": round(ms_sel, 3), "wizard_ms": round(ms_wiz, 3), "speedup": round(ms_wiz / ms_sel, 1),
             "ratio_loss_pct": round(loss * 100, 4), "agreement_with_wizard": round(agree, 4),
             "wizard_fallback_chunks": int(n_fb), "sample_stride": stride, "confidence_threshold": thr,
+            "columns": "the integer columns",
             "timer": "host clock around the synchronous call (its launches and syncs included)",
             "candidates": dict(zip(SL.CANDIDATES, np.bincount(choice.cpu().numpy(), minlength=SL.K).tolist())),
             "training": {"vectors": int(feat.shape[0]), "label_s": round(t_label, 2), "train_s": round(t_train, 2),
@@ -426,6 +449,8 @@ def mixed_rowgroups(dev, peak, steps):
                          "last_loss": round(float(hist[-50:].mean()), 4)},
         },
     }
+    del graph
+    ss.close()
     rg.close()
     plan.close()
     return res

@@ -5,9 +5,10 @@
 //   k_str_lengths    warp per vector: the vector's 1024 codes (or row end offsets) in original order, the
 //                    decoded length of every row, the vector total.
 //   k_scan_totals    exclusive scan of the vector totals (one CTA): the first output byte of every vector.
-//   k_str_materialize warp per vector: Arrow offsets of its rows and their bytes.  DICT rows are gathered from
-//                    the decoded dictionary (held in shared memory when it fits) in aligned 16-byte output
-//                    chunks; FSST / BYTE_ARR rows decode straight from the page.
+//   k_str_materialize warp per vector: Arrow offsets of its rows and their bytes, 32 rows at a time (one per
+//                    lane) into a per-warp shared-memory window that leaves in coalesced 16-byte stores.  DICT
+//                    rows are copied from the decoded dictionary (held in shared memory when it fits), BYTE_ARR
+//                    rows from the page, FSST rows decode from the page.
 #include "fls_decode.cu"
 #include "fls_strings.cuh"
 #include "fls_runtime.h"
@@ -96,33 +97,41 @@ __device__ __forceinline__ const uint8_t* vector_bytes(const ColDesc& c, uint32_
 	return *n ? c.buf[0] + o : c.buf[0];
 }
 
-// Copy n bytes from src to dst, any alignment of either.  The body moves 4-byte words (funnel shifts of two
-// aligned source words), so the source must stay readable up to the 4-byte word after src + n; the at most
-// three bytes before and after the body are predicated stores.
-__device__ __forceinline__ void copy_row(uint8_t* __restrict__ dst, const uint8_t* __restrict__ src, uint32_t n) {
-	uint32_t h = (4u - static_cast<uint32_t>(reinterpret_cast<uintptr_t>(dst) & 3u)) & 3u;
-	h          = h < n ? h : n;
-#pragma unroll
-	for (uint32_t i = 0; i < 3; ++i) {
-		if (i < h) { dst[i] = src[i]; }
+// OR the n bytes at src into the window at byte offset d, whose bytes there are zero.  Window words wholly
+// inside the row are plain stores; the first and last (shared with the neighbouring rows, which other lanes
+// may be writing at the same time) are atomic ORs of the row's bytes.  Only the aligned source words that hold
+// bytes of [src, src + n) are read.
+__device__ __forceinline__ void or_row(uint32_t* __restrict__ win, uint32_t d, const uint8_t* __restrict__ src,
+                                       uint32_t n) {
+	if (n == 0) { return; }
+	const uintptr_t sa   = reinterpret_cast<uintptr_t>(src);
+	const uintptr_t a    = sa - (d & 3u); // source address of the byte that lands on window byte 4 * (d / 4)
+	const uint32_t  sh   = 8u * static_cast<uint32_t>(a & 3u);
+	const uint32_t* s    = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+	const uint32_t* s_lo = reinterpret_cast<const uint32_t*>(sa & ~uintptr_t(3));
+	const uint32_t* s_hi = reinterpret_cast<const uint32_t*>((sa + n - 1) & ~uintptr_t(3));
+	const uint32_t  k0 = d >> 2, k1 = (d + n - 1) >> 2;
+	const uint32_t  hm = 0xFFFFFFFFu << (8u * (d & 3u));
+	const uint32_t  tm = 0xFFFFFFFFu >> (8u * (3u - ((d + n - 1) & 3u)));
+	// a clamped word only feeds bytes outside the row, which the masks drop
+	uint32_t w0 = *(s < s_lo ? s_lo : s);
+	uint32_t w1 = *(s + 1 > s_hi ? s_hi : s + 1);
+	if (k0 == k1) {
+		atomicOr(win + k0, __funnelshift_r(w0, w1, sh) & hm & tm);
+		return;
 	}
-	dst += h, src += h, n -= h;
-	const uint32_t  sh = 8u * static_cast<uint32_t>(reinterpret_cast<uintptr_t>(src) & 3u);
-	const uint32_t* s  = reinterpret_cast<const uint32_t*>(reinterpret_cast<uintptr_t>(src) & ~uintptr_t(3));
-	uint32_t*       d  = reinterpret_cast<uint32_t*>(dst);
-	const uint32_t  nw = n >> 2;
-	uint32_t        w0 = s[0];
-	for (uint32_t i = 0; i < nw; ++i) {
-		const uint32_t w1 = s[i + 1];
-		d[i]              = __funnelshift_r(w0, w1, sh);
-		w0                = w1;
+	atomicOr(win + k0, __funnelshift_r(w0, w1, sh) & hm);
+	const uint32_t m = k1 - k0; // words k0 + 1 .. k1 - 1 are whole row words
+	uint32_t       j = 1;
+#pragma unroll 4
+	for (; j < m; ++j) {
+		w0              = w1;
+		w1              = s[j + 1];
+		win[k0 + j]     = __funnelshift_r(w0, w1, sh);
 	}
-	const uint32_t t = n & 3u;
-	dst += 4 * nw, src += 4 * nw;
-#pragma unroll
-	for (uint32_t i = 0; i < 3; ++i) {
-		if (i < t) { dst[i] = src[i]; }
-	}
+	w0 = w1;
+	w1 = *(s + m + 1 > s_hi ? s_hi : s + m + 1);
+	atomicOr(win + k1, __funnelshift_r(w0, w1, sh) & tm);
 }
 
 // ---------------------------------------------------------------------------------------------------------
@@ -131,7 +140,8 @@ __device__ __forceinline__ void copy_row(uint8_t* __restrict__ dst, const uint8_
 //   rows    the vector's packed codes / end offsets (copied in, with 128 bytes of slack for the extraction),
 //           then, once decoded, its 1024 codes / end offsets in original order (row r at word r + r / 32:
 //           conflict-free both by run and by row)
-//   window  (materialize only) 4 KB of output bytes starting at a 16-byte aligned output position
+//   window  (materialize only) 4 KB of output bytes starting at a 16-byte aligned output position; for the
+//           copied kinds (DICT, BYTE_ARR) its bytes past the filled part are kept zero, so rows are OR-ed in
 // The work per vector (1024 row copies) is long next to the latency of its loads, so the packed words are
 // read synchronously: occupancy, not prefetch depth, is what hides latency here.
 // ---------------------------------------------------------------------------------------------------------
@@ -200,8 +210,8 @@ struct RowRef {
 };
 
 template <int KIND>
-__device__ __forceinline__ RowRef row_ref(const StrArgs& a, const uint32_t* rows, uint32_t r, const uint8_t* vb,
-                                          uint32_t vn, const uint8_t* flen, bool* bad) {
+__device__ __forceinline__ RowRef row_ref(const StrArgs& a, const uint32_t* ends, const uint32_t* rows, uint32_t r,
+                                          const uint8_t* vb, uint32_t vn, const uint8_t* flen, bool* bad) {
 	RowRef f {0, 0, 0};
 	if constexpr (KIND == STR_DICT) {
 		const uint32_t code = rows[row_word(r)];
@@ -209,8 +219,8 @@ __device__ __forceinline__ RowRef row_ref(const StrArgs& a, const uint32_t* rows
 			*bad = true;
 			return f;
 		}
-		f.start = code ? __ldg(a.dict_ends + code - 1) : 0u;
-		f.len   = __ldg(a.dict_ends + code) - f.start;
+		f.start = code ? ends[code - 1] : 0u;
+		f.len   = ends[code] - f.start;
 		return f;
 	} else {
 		const uint32_t s = r == 0 ? 0u : rows[row_word(r - 1)];
@@ -226,22 +236,14 @@ __device__ __forceinline__ RowRef row_ref(const StrArgs& a, const uint32_t* rows
 	}
 }
 
-template <int KIND>
-__device__ __forceinline__ void emit_row(uint8_t* dst, const RowRef& f, const uint8_t* dict, const uint8_t* vb,
-                                         const uint64_t* fsym, const uint8_t* flen) {
-	if constexpr (KIND == STR_DICT) {
-		copy_row(dst, dict + f.start, f.len);
-	} else if constexpr (KIND == STR_BYTES) {
-		copy_row(dst, vb + f.start, f.len);
-	} else {
-		fsst_decode_to(fsym, flen, vb + f.start, f.clen, dst);
-	}
-}
 
 // One pass over the column's vectors, warp per vector.  LENGTHS: per-vector decoded byte totals.  MATERIALIZE:
-// Arrow offsets and bytes, at the first output byte of every vector computed from the totals.  DSMEM: the
-// decoded dictionary is copied to shared memory (after the per-warp areas) at CTA start.
-template <int PASS, int KIND, bool DSMEM>
+// Arrow offsets and bytes, at the first output byte of every vector computed from the totals.  SM (DICT only):
+// SM_ENDS copies the dictionary end offsets to shared memory (after the per-warp areas) at CTA start,
+// SM_BYTES the decoded dictionary bytes too (after the end offsets).
+enum : int { SM_NONE = 0, SM_ENDS = 1, SM_BYTES = 3 };
+
+template <int PASS, int KIND, int SM>
 __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a) {
 	extern __shared__ __align__(128) uint8_t smem[];
 	__shared__ uint64_t fsym[KIND == STR_FSST ? 256 : 1];
@@ -249,8 +251,14 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 	const uint32_t     lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
 	constexpr uint32_t kPerWarp = str_per_warp(PASS);
 	const uint8_t*     dict     = a.dict_bytes;
-	if constexpr (PASS == STR_PASS_MATERIALIZE && KIND == STR_DICT && DSMEM) {
-		uint8_t* db = smem + nwarps * kPerWarp;
+	const uint32_t*    ends     = a.dict_ends;
+	if constexpr (KIND == STR_DICT && (SM & SM_ENDS)) {
+		uint32_t* es = reinterpret_cast<uint32_t*>(smem + nwarps * kPerWarp);
+		for (uint32_t i = threadIdx.x; i < a.entry_c; i += blockDim.x) { es[i] = __ldg(a.dict_ends + i); }
+		ends = es;
+	}
+	if constexpr (PASS == STR_PASS_MATERIALIZE && KIND == STR_DICT && SM == SM_BYTES) {
+		uint8_t* db = smem + nwarps * kPerWarp + str_ends_smem(a);
 		// the decoded dictionary lives in a cudaMalloc'd (256-byte aligned) buffer with at least 16 bytes of
 		// slack after the last entry
 		const uint32_t nb16 = static_cast<uint32_t>((a.dict_bytes_n + 15) / 16);
@@ -269,6 +277,10 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 	PlanS*   plans = reinterpret_cast<PlanS*>(wbase);
 	uint8_t* buf   = wbase + kStrPB * 64;
 	uint8_t* win   = buf + kStrRows;
+	constexpr bool kOr = PASS == STR_PASS_MATERIALIZE && KIND != STR_FSST;
+	if constexpr (kOr) {
+		for (uint32_t i = lane; i < kStrWindow / 16; i += 32) { reinterpret_cast<uint4*>(win)[i] = make_uint4(0, 0, 0, 0); }
+	}
 	__syncthreads();
 
 	const uint64_t gw = static_cast<uint64_t>(blockIdx.x) * nwarps + warp;
@@ -300,7 +312,7 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 		bool            bad  = false;
 		if constexpr (PASS == STR_PASS_LENGTHS) {
 			uint32_t sum = 0;
-			for (uint32_t b = 0; b < kVec / 32; ++b) { sum += row_ref<KIND>(a, rows, 32 * b + lane, vb, vn, flen, &bad).len; }
+			for (uint32_t b = 0; b < kVec / 32; ++b) { sum += row_ref<KIND>(a, ends, rows, 32 * b + lane, vb, vn, flen, &bad).len; }
 			sum = warp_sum(sum);
 			if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) { atomicOr(a.status, STATUS_BAD_INDEX); }
 			if (lane == 0) { a.vec_total[v] = sum; }
@@ -332,29 +344,47 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 							if (g + i >= lo) { a.bytes[g + i] = win[c + i]; }
 						}
 					}
+					if constexpr (kOr) { *reinterpret_cast<uint4*>(win + c) = make_uint4(0, 0, 0, 0); }
 				}
 				__syncwarp();
 				if (!all) {
-					const uint8_t t = lane < (fill & 15u) ? win[full + lane] : 0;
-					__syncwarp();
-					if (lane < (fill & 15u)) { win[lane] = t; }
+					// the partial chunk [full, fill) moves to the window start
+					if constexpr (kOr) {
+						if (lane == 0 && full != 0 && (fill & 15u) != 0) {
+							*reinterpret_cast<uint4*>(win) = *reinterpret_cast<const uint4*>(win + full);
+							*reinterpret_cast<uint4*>(win + full) = make_uint4(0, 0, 0, 0);
+						}
+					} else {
+						const uint8_t t = lane < (fill & 15u) ? win[full + lane] : 0;
+						__syncwarp();
+						if (lane < (fill & 15u)) { win[lane] = t; }
+					}
 					__syncwarp();
 					W += full;
 					fill &= 15u;
 					lo = lo > W ? lo : W;
 				}
 			};
-			uint32_t vpos = 0; // bytes of this vector emitted so far
+			uint32_t  vpos = 0; // bytes of this vector emitted so far
+			uint32_t* offs = a.offsets + v * kVec + lane;
+			// the next batch's row is looked up while the current one is copied
+			RowRef next = row_ref<KIND>(a, ends, rows, lane, vb, vn, flen, &bad);
 			for (uint32_t b = 0; b < kVec / 32; ++b) {
-				const uint32_t r   = 32 * b + lane;
-				const RowRef   f   = row_ref<KIND>(a, rows, r, vb, vn, flen, &bad);
+				const uint32_t r = 32 * b + lane;
+				const RowRef   f = next;
+				if (b + 1 < kVec / 32) { next = row_ref<KIND>(a, ends, rows, r + 32, vb, vn, flen, &bad); }
 				const uint32_t inc = warp_inclusive_scan(f.len, lane);
 				const uint32_t o   = vpos + inc - f.len;
 				const uint32_t T   = __shfl_sync(0xFFFFFFFFu, inc, 31);
-				a.offsets[v * kVec + r] = static_cast<uint32_t>(vbase + o);
+				offs[32 * b] = static_cast<uint32_t>(vbase + o);
 				if (fill + T > kStrWindow) { flush(false); }
 				if (fill + T <= kStrWindow) {
-					emit_row<KIND>(win + fill + (o - vpos), f, dict, vb, fsym, flen);
+					if constexpr (kOr) {
+						or_row(reinterpret_cast<uint32_t*>(win), fill + (o - vpos),
+						       KIND == STR_DICT ? dict + f.start : vb + f.start, f.len);
+					} else {
+						fsst_decode_to(fsym, flen, vb + f.start, f.clen, win + fill + (o - vpos));
+					}
 					fill += T;
 				} else {
 					// a batch larger than the window: its rows go straight to global memory, after the window's
@@ -414,9 +444,9 @@ cudaError_t launch_fsst_dict(const uint8_t* lens, const uint8_t* comp, uint64_t 
 
 // Launch one pass over the column's vectors with `warps` warps per CTA and as many CTAs per SM as shared
 // memory allows (no more CTAs than there are vectors for their warps).
-template <int PASS, int KIND, bool DSMEM>
+template <int PASS, int KIND, int SM>
 static cudaError_t launch_str_kernel(const StrArgs& a, int warps, uint32_t dyn_smem, cudaStream_t s) {
-	auto* const       fn = k_str_pass<PASS, KIND, DSMEM>;
+	auto* const       fn = k_str_pass<PASS, KIND, SM>;
 	static std::mutex mu;
 	static uint32_t   set = 0;
 	{
@@ -443,12 +473,14 @@ static cudaError_t launch_str_kernel(const StrArgs& a, int warps, uint32_t dyn_s
 }
 
 cudaError_t launch_str_lengths(const StrArgs& a, int /*grid*/, cudaStream_t s) {
-	constexpr int    w    = kStrMaxWarps;
+	constexpr int      w  = kStrMaxWarps;
 	constexpr uint32_t sm = w * str_per_warp(STR_PASS_LENGTHS);
 	switch (a.kind) {
-	case STR_DICT: return launch_str_kernel<STR_PASS_LENGTHS, STR_DICT, false>(a, w, sm, s);
-	case STR_FSST: return launch_str_kernel<STR_PASS_LENGTHS, STR_FSST, false>(a, w, sm, s);
-	default: return launch_str_kernel<STR_PASS_LENGTHS, STR_BYTES, false>(a, w, sm, s);
+	case STR_DICT:
+		return a.ends_in_smem ? launch_str_kernel<STR_PASS_LENGTHS, STR_DICT, SM_ENDS>(a, w, sm + str_ends_smem(a), s)
+		                      : launch_str_kernel<STR_PASS_LENGTHS, STR_DICT, SM_NONE>(a, w, sm, s);
+	case STR_FSST: return launch_str_kernel<STR_PASS_LENGTHS, STR_FSST, SM_NONE>(a, w, sm, s);
+	default: return launch_str_kernel<STR_PASS_LENGTHS, STR_BYTES, SM_NONE>(a, w, sm, s);
 	}
 }
 
@@ -461,10 +493,11 @@ cudaError_t launch_scan_totals(const uint64_t* total, uint64_t* base, uint64_t n
 cudaError_t launch_str_materialize(const StrArgs& a, int warps, uint32_t dyn_smem, cudaStream_t s) {
 	switch (a.kind) {
 	case STR_DICT:
-		return a.dict_in_smem ? launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, true>(a, warps, dyn_smem, s)
-		                      : launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, false>(a, warps, dyn_smem, s);
-	case STR_FSST: return launch_str_kernel<STR_PASS_MATERIALIZE, STR_FSST, false>(a, warps, dyn_smem, s);
-	default: return launch_str_kernel<STR_PASS_MATERIALIZE, STR_BYTES, false>(a, warps, dyn_smem, s);
+		if (a.dict_in_smem) { return launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, SM_BYTES>(a, warps, dyn_smem, s); }
+		return a.ends_in_smem ? launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, SM_ENDS>(a, warps, dyn_smem, s)
+		                      : launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, SM_NONE>(a, warps, dyn_smem, s);
+	case STR_FSST: return launch_str_kernel<STR_PASS_MATERIALIZE, STR_FSST, SM_NONE>(a, warps, dyn_smem, s);
+	default: return launch_str_kernel<STR_PASS_MATERIALIZE, STR_BYTES, SM_NONE>(a, warps, dyn_smem, s);
 	}
 }
 

@@ -272,3 +272,28 @@ def selection_column(rng, n_vec, device="cuda", family=None):
     wide = bool(rng.integers(0, 2))
     v = torch.randint(-2 ** 62, 2 ** 62, (n,), generator=g, device=device, dtype=torch.int64) * 2 + 1
     return (v, True) if wide else (v.to(torch.int32), False)
+
+
+# ---- the mixed row-group workload ------------------------------------------------------------------------
+MIXED_KINDS = ("for", "delta", "rle", "dict", "strings")
+
+
+def mixed_rowgroup_columns(rng, n_cols=256, device="cuda", min_vec=64, max_vec=4096):
+    """Columns of uneven lengths (U[min_vec, max_vec] vectors, i.e. 64 Ki..4 Mi values) whose types are drawn
+    uniformly from: u32 / i64 FOR with a random bit width; sorted i64 timestamps; runs (geometric mean 2..64);
+    low-cardinality int32 Zipf dictionaries (16..65,536 entries, Zipf 0.8..1.5); FSST-able strings (a
+    4096-entry dictionary of 5..40-byte token strings, Zipf(1.1) codes).  Returns (integer columns as
+    (tensor, is_signed), string columns as (dictionary bytes, offsets, codes))."""
+    ints, strs = [], []
+    for _ in range(n_cols):
+        kind = MIXED_KINDS[rng.integers(0, len(MIXED_KINDS))]
+        n_vec = int(rng.integers(min_vec, max_vec + 1))
+        if kind == "strings":
+            seed = int(rng.integers(0, 2 ** 31))
+            dbytes, doffs = string_dictionary(seed=seed)
+            strs.append((dbytes, doffs, zipf_codes(n_vec * 1024, seed=seed + 1)))
+            continue
+        fam = {"for": ("for_u32", "for_i64")[rng.integers(0, 2)], "delta": "delta_i64", "rle": "rle",
+               "dict": "dict_i32"}[kind]
+        ints.append(selection_column(rng, n_vec, device, fam))
+    return ints, strs

@@ -65,3 +65,39 @@ def test_string_dict_encoder_round_trip(cuda):
     want_off[1:] = np.cumsum([w.size for w in want])
     assert np.array_equal(offs.cpu().numpy().astype(np.uint64), want_off)
     assert np.array_equal(data.cpu().numpy(), np.concatenate(want))
+
+
+def _mixed_length_dictionary(rng, n):
+    """n entries: 10 % empty, 20 % of 1-3 bytes, 50 % of 4-40, 20 % of 41-300 (every byte value)."""
+    kind = rng.choice(4, n, p=[0.1, 0.2, 0.5, 0.2])
+    lo = np.array([0, 1, 4, 41])[kind]
+    hi = np.array([0, 3, 40, 300])[kind]
+    lens = rng.integers(lo, hi + 1)
+    offs = np.zeros(n + 1, np.uint64)
+    offs[1:] = np.cumsum(lens)
+    return rng.integers(0, 256, int(offs[-1]), dtype=np.uint8), offs
+
+
+@pytest.mark.parametrize("n_dict", [600, 12000, 20000])
+def test_string_dict_shared_memory_modes(cuda, n_dict):
+    """DICT rows of every length class, with the dictionary bytes and end offsets in shared memory (600
+    entries), only the end offsets there (12000: the bytes do not fit beside the warps), or neither (20000:
+    80 KB of end offsets).  Batches of 32 long rows exceed the per-warp window."""
+    from fastlanes_b200 import strings
+
+    rng = np.random.default_rng(n_dict)
+    dbytes, doffs = _mixed_length_dictionary(rng, n_dict)
+    codes = rng.integers(0, n_dict, 37 * 1024).astype(np.uint32)  # the encoder takes whole vectors
+    codes[5 * 1024:6 * 1024] = int(np.argmax(np.diff(doffs)))  # a vector of the longest entry only
+    page, dic = strings.encode_string_dict(dbytes, doffs, codes)
+    pb, pp = _dev(page, cuda, 1)
+    db, dp = _dev(dic, cuda, 0)
+    plan = strings.StringPlan(pp, page.size, dp, dic.size)
+    offs, data = plan.decode(cuda)
+    plan.close()
+    lens = np.diff(doffs).astype(np.int64)
+    want_off = np.zeros(codes.size + 1, np.int64)
+    want_off[1:] = np.cumsum(lens[codes])
+    assert np.array_equal(offs.cpu().numpy().astype(np.int64), want_off)
+    idx = np.concatenate([np.arange(int(doffs[c]), int(doffs[c + 1])) for c in codes])
+    assert np.array_equal(data.cpu().numpy(), dbytes[idx])
