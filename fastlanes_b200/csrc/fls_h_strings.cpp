@@ -191,24 +191,21 @@ int fls_string_plan_create(const uint8_t* d_page, uint64_t page_size, const uint
 	}
 	if (cudaMemcpy(p->table.p, &tab, sizeof(tab), cudaMemcpyHostToDevice) != cudaSuccess) { return FLS_ERR_CUDA; }
 	a.table = p->table.p;
-	// shared memory of the string kernels: per-warp areas, then the dictionary end offsets (both passes, up to
-	// 64 KB of them), then the decoded dictionary bytes (materialising pass) when at least 8 warps still fit
-	// beside them
+	// shared memory of the string kernels: the lengths pass keeps the dictionary end offsets there (up to 64 KB
+	// of them) after its per-warp areas; the materialising pass the decoded dictionary bytes (its end offsets are
+	// looked up a batch ahead from global memory) when at least 8 warps still fit beside them
 	const uint32_t per_warp = str_smem_per_warp();
 	const uint64_t budget   = 224 * 1024;
-	a.ends_in_smem          = a.kind == STR_DICT && str_ends_smem(a) <= kStrEndsSmemMax;
-	const uint64_t ends_sm  = a.ends_in_smem ? str_ends_smem(a) : 0;
 	const uint64_t dict_sm  = (a.dict_bytes_n + 15) & ~15ull;
-	p->warps                = kStrMaxWarps;
+	a.ends_in_smem          = a.kind == STR_DICT && str_ends_smem(a) <= kStrEndsSmemMax;
 	a.dict_in_smem          = false;
-	if (a.ends_in_smem && ends_sm + dict_sm < budget) {
-		const uint64_t w = (budget - ends_sm - dict_sm) / per_warp;
-		if (w >= 8) {
-			a.dict_in_smem = true;
-			p->warps       = static_cast<int>(w < kStrMaxWarps ? w : kStrMaxWarps);
-		}
+	uint64_t w              = budget / per_warp;
+	if (a.kind == STR_DICT && dict_sm < budget && (budget - dict_sm) / per_warp >= 8) {
+		a.dict_in_smem = true;
+		w              = (budget - dict_sm) / per_warp;
 	}
-	p->dyn_smem = static_cast<uint32_t>(p->warps * per_warp + ends_sm + (a.dict_in_smem ? dict_sm : 0u));
+	p->warps    = static_cast<int>(w < kStrMaxWarps ? w : kStrMaxWarps);
+	p->dyn_smem = static_cast<uint32_t>(p->warps * per_warp + (a.dict_in_smem ? dict_sm : 0u));
 	*out                    = p.release();
 	return FLS_OK;
 }

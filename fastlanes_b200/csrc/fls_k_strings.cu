@@ -140,14 +140,14 @@ __device__ __forceinline__ void or_row(uint32_t* __restrict__ win, uint32_t d, c
 //   rows    the vector's packed codes / end offsets (copied in, with 128 bytes of slack for the extraction),
 //           then, once decoded, its 1024 codes / end offsets in original order (row r at word r + r / 32:
 //           conflict-free both by run and by row)
-//   window  (materialize only) 4 KB of output bytes starting at a 16-byte aligned output position; for the
+//   window  (materialize only) 2 KB of output bytes starting at a 16-byte aligned output position; for the
 //           copied kinds (DICT, BYTE_ARR) its bytes past the filled part are kept zero, so rows are OR-ed in
 // The work per vector (1024 row copies) is long next to the latency of its loads, so the packed words are
 // read synchronously: occupancy, not prefetch depth, is what hides latency here.
 // ---------------------------------------------------------------------------------------------------------
-constexpr uint32_t kStrPB      = 8;
+constexpr uint32_t kStrPB      = 4;
 constexpr uint32_t kStrRows    = 4096 + 128; // >= 1055 padded row words, >= 128 * (32 + 1) staged bytes
-constexpr uint32_t kStrWindow  = 4096;
+constexpr uint32_t kStrWindow  = 2048;
 
 enum : int { STR_PASS_LENGTHS = 0, STR_PASS_MATERIALIZE = 1 };
 
@@ -239,9 +239,9 @@ __device__ __forceinline__ RowRef row_ref(const StrArgs& a, const uint32_t* ends
 
 // One pass over the column's vectors, warp per vector.  LENGTHS: per-vector decoded byte totals.  MATERIALIZE:
 // Arrow offsets and bytes, at the first output byte of every vector computed from the totals.  SM (DICT only):
-// SM_ENDS copies the dictionary end offsets to shared memory (after the per-warp areas) at CTA start,
-// SM_BYTES the decoded dictionary bytes too (after the end offsets).
-enum : int { SM_NONE = 0, SM_ENDS = 1, SM_BYTES = 3 };
+// SM_ENDS (lengths pass) copies the dictionary end offsets to shared memory (after the per-warp areas) at CTA
+// start, SM_BYTES (materialising pass) the decoded dictionary bytes.
+enum : int { SM_NONE = 0, SM_ENDS = 1, SM_BYTES = 2 };
 
 template <int PASS, int KIND, int SM>
 __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a) {
@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 		ends = es;
 	}
 	if constexpr (PASS == STR_PASS_MATERIALIZE && KIND == STR_DICT && SM == SM_BYTES) {
-		uint8_t* db = smem + nwarps * kPerWarp + str_ends_smem(a);
+		uint8_t* db = smem + nwarps * kPerWarp;
 		// the decoded dictionary lives in a cudaMalloc'd (256-byte aligned) buffer with at least 16 bytes of
 		// slack after the last entry
 		const uint32_t nb16 = static_cast<uint32_t>((a.dict_bytes_n + 15) / 16);
@@ -473,7 +473,7 @@ static cudaError_t launch_str_kernel(const StrArgs& a, int warps, uint32_t dyn_s
 }
 
 cudaError_t launch_str_lengths(const StrArgs& a, int /*grid*/, cudaStream_t s) {
-	constexpr int      w  = kStrMaxWarps;
+	constexpr int      w  = kStrLenWarps;
 	constexpr uint32_t sm = w * str_per_warp(STR_PASS_LENGTHS);
 	switch (a.kind) {
 	case STR_DICT:
@@ -493,8 +493,7 @@ cudaError_t launch_scan_totals(const uint64_t* total, uint64_t* base, uint64_t n
 cudaError_t launch_str_materialize(const StrArgs& a, int warps, uint32_t dyn_smem, cudaStream_t s) {
 	switch (a.kind) {
 	case STR_DICT:
-		if (a.dict_in_smem) { return launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, SM_BYTES>(a, warps, dyn_smem, s); }
-		return a.ends_in_smem ? launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, SM_ENDS>(a, warps, dyn_smem, s)
+		return a.dict_in_smem ? launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, SM_BYTES>(a, warps, dyn_smem, s)
 		                      : launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, SM_NONE>(a, warps, dyn_smem, s);
 	case STR_FSST: return launch_str_kernel<STR_PASS_MATERIALIZE, STR_FSST, SM_NONE>(a, warps, dyn_smem, s);
 	default: return launch_str_kernel<STR_PASS_MATERIALIZE, STR_BYTES, SM_NONE>(a, warps, dyn_smem, s);
@@ -633,7 +632,7 @@ extern "C" int fls_gpu_decode_fsst_page_noalloc(const uint8_t* d_page, uint64_t 
 	if (launch_str_lengths(a, sms, s) != cudaSuccess ||
 	    launch_scan_totals(a.vec_total, reinterpret_cast<uint64_t*>(scratch + NoAllocLayout::kBase), vec_c, s) !=
 	        cudaSuccess ||
-	    launch_str_materialize(a, kStrMaxWarps, kStrMaxWarps * str_smem_per_warp(), s) != cudaSuccess) {
+	    launch_str_materialize(a, kStrLenWarps, kStrLenWarps * str_smem_per_warp(), s) != cudaSuccess) {
 		return FLS_ERR_CUDA;
 	}
 	return FLS_OK;

@@ -19,14 +19,15 @@ enum : uint8_t {
 	STR_BYTES = 2, // rows are plain bytes in the page (BYTE_ARR pages)
 };
 
-constexpr int      kStrMaxWarps   = 16;        // warps per CTA of the string kernels
+constexpr int      kStrMaxWarps   = 32;        // warps per CTA of the string kernels (at most)
+constexpr int      kStrLenWarps   = 16;        // warps per CTA of the lengths pass
 constexpr uint32_t kStrEndsSmemMax = 64 * 1024; // largest dictionary end-offset array copied to shared memory
 
 struct StrArgs {
 	ColDesc          col; // the row stream: codes or cumulative end offsets, page layout
 	uint8_t          kind;
-	bool             dict_in_smem; // materialise: decoded dictionary bytes (and end offsets) in shared memory
-	bool             ends_in_smem; // both passes: dictionary end offsets in shared memory
+	bool             dict_in_smem; // materialising pass: decoded dictionary bytes in shared memory
+	bool             ends_in_smem; // lengths pass: dictionary end offsets in shared memory
 	uint32_t         entry_c;
 	const uint32_t*  dict_ends;
 	const uint8_t*   dict_bytes;
@@ -45,8 +46,8 @@ cudaError_t launch_fsst_dict(const uint8_t* lens, const uint8_t* comp, uint64_t 
                              cudaStream_t s);
 cudaError_t launch_str_lengths(const StrArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_scan_totals(const uint64_t* total, uint64_t* base, uint64_t n, cudaStream_t s);
-// warps: warps per CTA (at most kStrMaxWarps); dyn_smem: warps * str_smem_per_warp() plus str_ends_smem(a)
-// when a.ends_in_smem plus the 16-byte rounded dictionary bytes when a.dict_in_smem
+// warps: warps per CTA (at most kStrMaxWarps); dyn_smem: warps * str_smem_per_warp() plus the 16-byte rounded
+// dictionary bytes when a.dict_in_smem
 cudaError_t launch_str_materialize(const StrArgs& a, int warps, uint32_t dyn_smem, cudaStream_t s);
 uint32_t    str_smem_per_warp();
 // shared-memory bytes of the dictionary end offsets (16-byte rounded)
