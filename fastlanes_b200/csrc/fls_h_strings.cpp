@@ -194,7 +194,17 @@ int fls_string_plan_create(const uint8_t* d_page, uint64_t page_size, const uint
 	// shared memory of the string kernels: the lengths pass keeps the dictionary end offsets there (up to 64 KB
 	// of them) after its per-warp areas; the materialising pass the decoded dictionary bytes (its end offsets are
 	// looked up a batch ahead from global memory) when at least 8 warps still fit beside them
-	const uint32_t per_warp = str_smem_per_warp();
+	// 16-bit code rows: fewer than 65535 entries and at most 2 KB of packed codes per vector (16-bit lanes, or
+	// bit widths up to 16 in every vector)
+	a.rows16 = a.kind == STR_DICT && a.entry_c < 0xFFFFu && (c.ws == 16 || c.enc != ENC_RAW);
+	if (a.rows16 && c.ws == 32) {
+		std::vector<uint8_t> bw(c.buf_size[c.ib_bw]);
+		if (!bw.empty() && cudaMemcpy(bw.data(), c.buf[c.ib_bw], bw.size(), cudaMemcpyDeviceToHost) != cudaSuccess) {
+			return FLS_ERR_CUDA;
+		}
+		for (const uint8_t w : bw) { a.rows16 = a.rows16 && w <= 16; }
+	}
+	const uint32_t per_warp = str_smem_per_warp(a.rows16);
 	const uint64_t budget   = 224 * 1024;
 	const uint64_t dict_sm  = (a.dict_bytes_n + 15) & ~15ull;
 	a.ends_in_smem          = a.kind == STR_DICT && str_ends_smem(a) <= kStrEndsSmemMax;

@@ -139,7 +139,9 @@ __device__ __forceinline__ void or_row(uint32_t* __restrict__ win, uint32_t d, c
 //   plans   the next kStrPB plans (64 B each) of the warp's vectors, fetched lane-parallel
 //   rows    the vector's packed codes / end offsets (copied in, with 128 bytes of slack for the extraction),
 //           then, once decoded, its 1024 codes / end offsets in original order (row r at word r + r / 32:
-//           conflict-free both by run and by row)
+//           conflict-free both by run and by row).  Dictionaries of fewer than 65535 entries keep their codes
+//           as 16-bit values (row r at half-word r + 2 * (r / 32), as conflict-free) in half the space: their
+//           packed codes are at most 16 bits wide
 //   window  (materialize only) 2 KB of output bytes starting at a 16-byte aligned output position; for the
 //           copied kinds (DICT, BYTE_ARR) its bytes past the filled part are kept zero, so rows are OR-ed in
 // The work per vector (1024 row copies) is long next to the latency of its loads, so the packed words are
@@ -147,19 +149,48 @@ __device__ __forceinline__ void or_row(uint32_t* __restrict__ win, uint32_t d, c
 // ---------------------------------------------------------------------------------------------------------
 constexpr uint32_t kStrPB      = 4;
 constexpr uint32_t kStrRows    = 4096 + 128; // >= 1055 padded row words, >= 128 * (32 + 1) staged bytes
+constexpr uint32_t kStrRows16  = 2048 + 128; // >= 1086 padded 16-bit rows, >= 128 * (16 + 1) staged bytes
 constexpr uint32_t kStrWindow  = 2048;
 
 enum : int { STR_PASS_LENGTHS = 0, STR_PASS_MATERIALIZE = 1 };
 
-__host__ __device__ constexpr uint32_t str_per_warp(int pass) {
-	return kStrPB * 64 + kStrRows + (pass == STR_PASS_MATERIALIZE ? kStrWindow : 0u);
+__host__ __device__ constexpr uint32_t str_rows_bytes(bool r16) { return r16 ? kStrRows16 : kStrRows; }
+
+__host__ __device__ constexpr uint32_t str_per_warp(int pass, bool r16) {
+	return kStrPB * 64 + str_rows_bytes(r16) + (pass == STR_PASS_MATERIALIZE ? kStrWindow : 0u);
 }
 
 __device__ __forceinline__ uint32_t row_word(uint32_t r) { return r + (r >> 5); }
+__device__ __forceinline__ uint32_t row_half(uint32_t r) { return r + 2 * (r >> 5); }
 
-// Codes (or end offsets) of the vector into rows[] in original order.  DICT_RLE run values are read from the
-// page directly.
-__device__ __forceinline__ void load_rows(const Plan& p, uint8_t* buf, uint32_t lane, int* status) {
+// row r of the decoded rows in buf (32- or 16-bit layout)
+template <bool R16>
+__device__ __forceinline__ uint32_t row_at(const uint8_t* buf, uint32_t r) {
+	if constexpr (R16) {
+		return reinterpret_cast<const uint16_t*>(buf)[row_half(r)];
+	} else {
+		return reinterpret_cast<const uint32_t*>(buf)[row_word(r)];
+	}
+}
+
+template <bool R16>
+__device__ __forceinline__ void set_row(uint8_t* buf, uint32_t r, uint32_t x) {
+	if constexpr (R16) {
+		// codes past 16 bits become 0xFFFF, which is out of range for every 16-bit dictionary
+		reinterpret_cast<uint16_t*>(buf)[row_half(r)] = static_cast<uint16_t>(x < 0xFFFFu ? x : 0xFFFFu);
+	} else {
+		reinterpret_cast<uint32_t*>(buf)[row_word(r)] = x;
+	}
+}
+
+// Codes (or end offsets) of the vector into rows in original order.  DICT_RLE run values are read from the
+// page directly.  False (status set) when the packed codes do not fit the 16-bit layout's staging space.
+template <bool R16>
+__device__ __forceinline__ bool load_rows(const Plan& p, uint8_t* buf, uint32_t lane, int* status) {
+	if (R16 && p.bytes + 128 > kStrRows16) {
+		if (lane == 0) { atomicOr(status, STATUS_BAD_LAYOUT); }
+		return false;
+	}
 	const uintptr_t al = reinterpret_cast<uintptr_t>(p.src);
 	if ((al & 15u) == 0) {
 		const uint4* s = reinterpret_cast<const uint4*>(p.src);
@@ -173,15 +204,14 @@ __device__ __forceinline__ void load_rows(const Plan& p, uint8_t* buf, uint32_t 
 		for (uint32_t i = lane; i < p.bytes; i += 32) { buf[i] = __ldg(p.src + i); }
 	}
 	__syncwarp();
-	uint32_t* rows = reinterpret_cast<uint32_t*>(buf);
-	uint32_t  x[32];
-	bool      bad = false;
+	uint32_t x[32];
+	bool     bad = false;
 	if (p.ws == 32) {
 		decode_stream<32>(p, reinterpret_cast<const uint32_t*>(buf), lane, x);
 		__syncwarp();
-		const uint32_t r0 = row_word(run_start<32>(lane, 0));
+		const uint32_t r0 = run_start<32>(lane, 0);
 #pragma unroll
-		for (int i = 0; i < 32; ++i) { rows[r0 + i] = x[i]; }
+		for (int i = 0; i < 32; ++i) { set_row<R16>(buf, r0 + i, x[i]); }
 	} else {
 		decode_stream<16>(p, reinterpret_cast<const uint32_t*>(buf), lane, x);
 #pragma unroll
@@ -193,13 +223,14 @@ __device__ __forceinline__ void load_rows(const Plan& p, uint8_t* buf, uint32_t 
 		__syncwarp();
 #pragma unroll
 		for (int r = 0; r < 2; ++r) {
-			const uint32_t r0 = row_word(run_start<16>(lane, r));
+			const uint32_t r0 = run_start<16>(lane, r);
 #pragma unroll
-			for (int i = 0; i < 16; ++i) { rows[r0 + i] = x[16 * r + i]; }
+			for (int i = 0; i < 16; ++i) { set_row<R16>(buf, r0 + i, x[16 * r + i]); }
 		}
 	}
 	if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) { atomicOr(status, STATUS_BAD_INDEX); }
 	__syncwarp();
+	return true;
 }
 
 // Row r of the vector: its source (dictionary entry or compressed bytes) and decoded length.
@@ -209,12 +240,12 @@ struct RowRef {
 	uint32_t len;   // decoded length
 };
 
-template <int KIND>
-__device__ __forceinline__ RowRef row_ref(const StrArgs& a, const uint32_t* ends, const uint32_t* rows, uint32_t r,
+template <int KIND, bool R16>
+__device__ __forceinline__ RowRef row_ref(const StrArgs& a, const uint32_t* ends, const uint8_t* rows, uint32_t r,
                                           const uint8_t* vb, uint32_t vn, const uint8_t* flen, bool* bad) {
 	RowRef f {0, 0, 0};
 	if constexpr (KIND == STR_DICT) {
-		const uint32_t code = rows[row_word(r)];
+		const uint32_t code = row_at<R16>(rows, r);
 		if (code >= a.entry_c) {
 			*bad = true;
 			return f;
@@ -223,8 +254,8 @@ __device__ __forceinline__ RowRef row_ref(const StrArgs& a, const uint32_t* ends
 		f.len   = ends[code] - f.start;
 		return f;
 	} else {
-		const uint32_t s = r == 0 ? 0u : rows[row_word(r - 1)];
-		const uint32_t e = rows[row_word(r)];
+		const uint32_t s = r == 0 ? 0u : row_at<R16>(rows, r - 1);
+		const uint32_t e = row_at<R16>(rows, r);
 		if (e < s || e > vn) {
 			*bad = true;
 			return f;
@@ -243,13 +274,13 @@ __device__ __forceinline__ RowRef row_ref(const StrArgs& a, const uint32_t* ends
 // start, SM_BYTES (materialising pass) the decoded dictionary bytes.
 enum : int { SM_NONE = 0, SM_ENDS = 1, SM_BYTES = 2 };
 
-template <int PASS, int KIND, int SM>
+template <int PASS, int KIND, int SM, bool R16>
 __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a) {
 	extern __shared__ __align__(128) uint8_t smem[];
 	__shared__ uint64_t fsym[KIND == STR_FSST ? 256 : 1];
 	__shared__ uint8_t  flen[KIND == STR_FSST ? 256 : 1];
 	const uint32_t     lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-	constexpr uint32_t kPerWarp = str_per_warp(PASS);
+	constexpr uint32_t kPerWarp = str_per_warp(PASS, R16);
 	const uint8_t*     dict     = a.dict_bytes;
 	const uint32_t*    ends     = a.dict_ends;
 	if constexpr (KIND == STR_DICT && (SM & SM_ENDS)) {
@@ -276,7 +307,7 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 	uint8_t* wbase = smem + warp * kPerWarp;
 	PlanS*   plans = reinterpret_cast<PlanS*>(wbase);
 	uint8_t* buf   = wbase + kStrPB * 64;
-	uint8_t* win   = buf + kStrRows;
+	uint8_t* win   = buf + str_rows_bytes(R16);
 	constexpr bool kOr = PASS == STR_PASS_MATERIALIZE && KIND != STR_FSST;
 	if constexpr (kOr) {
 		for (uint32_t i = lane; i < kStrWindow / 16; i += 32) { reinterpret_cast<uint4*>(win)[i] = make_uint4(0, 0, 0, 0); }
@@ -305,14 +336,18 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 			}
 			continue;
 		}
-		load_rows(p, buf, lane, a.status);
-		const uint32_t* rows = reinterpret_cast<const uint32_t*>(buf);
+		if (!load_rows<R16>(p, buf, lane, a.status)) {
+			if (PASS == STR_PASS_LENGTHS && lane == 0) { a.vec_total[v] = 0; }
+			__syncwarp();
+			continue;
+		}
+		const uint8_t* rows = buf;
 		uint32_t        vn   = 0;
 		const uint8_t*  vb   = KIND == STR_DICT ? nullptr : vector_bytes(a.col, static_cast<uint32_t>(v), &vn);
 		bool            bad  = false;
 		if constexpr (PASS == STR_PASS_LENGTHS) {
 			uint32_t sum = 0;
-			for (uint32_t b = 0; b < kVec / 32; ++b) { sum += row_ref<KIND>(a, ends, rows, 32 * b + lane, vb, vn, flen, &bad).len; }
+			for (uint32_t b = 0; b < kVec / 32; ++b) { sum += row_ref<KIND, R16>(a, ends, rows, 32 * b + lane, vb, vn, flen, &bad).len; }
 			sum = warp_sum(sum);
 			if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) { atomicOr(a.status, STATUS_BAD_INDEX); }
 			if (lane == 0) { a.vec_total[v] = sum; }
@@ -368,11 +403,11 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 			uint32_t  vpos = 0; // bytes of this vector emitted so far
 			uint32_t* offs = a.offsets + v * kVec + lane;
 			// the next batch's row is looked up while the current one is copied
-			RowRef next = row_ref<KIND>(a, ends, rows, lane, vb, vn, flen, &bad);
+			RowRef next = row_ref<KIND, R16>(a, ends, rows, lane, vb, vn, flen, &bad);
 			for (uint32_t b = 0; b < kVec / 32; ++b) {
 				const uint32_t r = 32 * b + lane;
 				const RowRef   f = next;
-				if (b + 1 < kVec / 32) { next = row_ref<KIND>(a, ends, rows, r + 32, vb, vn, flen, &bad); }
+				if (b + 1 < kVec / 32) { next = row_ref<KIND, R16>(a, ends, rows, r + 32, vb, vn, flen, &bad); }
 				const uint32_t inc = warp_inclusive_scan(f.len, lane);
 				const uint32_t o   = vpos + inc - f.len;
 				const uint32_t T   = __shfl_sync(0xFFFFFFFFu, inc, 31);
@@ -431,7 +466,7 @@ __global__ void __launch_bounds__(1024) k_scan_totals(const uint64_t* total, uin
 // ---------------------------------------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------------------------------------
-uint32_t str_smem_per_warp() { return str_per_warp(STR_PASS_MATERIALIZE); }
+uint32_t str_smem_per_warp(bool rows16) { return str_per_warp(STR_PASS_MATERIALIZE, rows16); }
 
 cudaError_t launch_fsst_dict(const uint8_t* lens, const uint8_t* comp, uint64_t comp_size, uint32_t entry_c,
                              const FsstTable* tab, uint32_t* ends, uint8_t* bytes, uint64_t cap, int* status,
@@ -444,9 +479,9 @@ cudaError_t launch_fsst_dict(const uint8_t* lens, const uint8_t* comp, uint64_t 
 
 // Launch one pass over the column's vectors with `warps` warps per CTA and as many CTAs per SM as shared
 // memory allows (no more CTAs than there are vectors for their warps).
-template <int PASS, int KIND, int SM>
+template <int PASS, int KIND, int SM, bool R16 = false>
 static cudaError_t launch_str_kernel(const StrArgs& a, int warps, uint32_t dyn_smem, cudaStream_t s) {
-	auto* const       fn = k_str_pass<PASS, KIND, SM>;
+	auto* const       fn = k_str_pass<PASS, KIND, SM, R16>;
 	static std::mutex mu;
 	static uint32_t   set = 0;
 	{
@@ -474,9 +509,13 @@ static cudaError_t launch_str_kernel(const StrArgs& a, int warps, uint32_t dyn_s
 
 cudaError_t launch_str_lengths(const StrArgs& a, int /*grid*/, cudaStream_t s) {
 	constexpr int      w  = kStrLenWarps;
-	constexpr uint32_t sm = w * str_per_warp(STR_PASS_LENGTHS);
+	const uint32_t     sm = w * str_per_warp(STR_PASS_LENGTHS, a.rows16);
 	switch (a.kind) {
 	case STR_DICT:
+		if (a.rows16) {
+			return a.ends_in_smem ? launch_str_kernel<STR_PASS_LENGTHS, STR_DICT, SM_ENDS, true>(a, w, sm + str_ends_smem(a), s)
+			                      : launch_str_kernel<STR_PASS_LENGTHS, STR_DICT, SM_NONE, true>(a, w, sm, s);
+		}
 		return a.ends_in_smem ? launch_str_kernel<STR_PASS_LENGTHS, STR_DICT, SM_ENDS>(a, w, sm + str_ends_smem(a), s)
 		                      : launch_str_kernel<STR_PASS_LENGTHS, STR_DICT, SM_NONE>(a, w, sm, s);
 	case STR_FSST: return launch_str_kernel<STR_PASS_LENGTHS, STR_FSST, SM_NONE>(a, w, sm, s);
@@ -493,6 +532,10 @@ cudaError_t launch_scan_totals(const uint64_t* total, uint64_t* base, uint64_t n
 cudaError_t launch_str_materialize(const StrArgs& a, int warps, uint32_t dyn_smem, cudaStream_t s) {
 	switch (a.kind) {
 	case STR_DICT:
+		if (a.rows16) {
+			return a.dict_in_smem ? launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, SM_BYTES, true>(a, warps, dyn_smem, s)
+			                      : launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, SM_NONE, true>(a, warps, dyn_smem, s);
+		}
 		return a.dict_in_smem ? launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, SM_BYTES>(a, warps, dyn_smem, s)
 		                      : launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, SM_NONE>(a, warps, dyn_smem, s);
 	case STR_FSST: return launch_str_kernel<STR_PASS_MATERIALIZE, STR_FSST, SM_NONE>(a, warps, dyn_smem, s);
@@ -632,7 +675,7 @@ extern "C" int fls_gpu_decode_fsst_page_noalloc(const uint8_t* d_page, uint64_t 
 	if (launch_str_lengths(a, sms, s) != cudaSuccess ||
 	    launch_scan_totals(a.vec_total, reinterpret_cast<uint64_t*>(scratch + NoAllocLayout::kBase), vec_c, s) !=
 	        cudaSuccess ||
-	    launch_str_materialize(a, kStrLenWarps, kStrLenWarps * str_smem_per_warp(), s) != cudaSuccess) {
+	    launch_str_materialize(a, kStrLenWarps, kStrLenWarps * str_smem_per_warp(false), s) != cudaSuccess) {
 		return FLS_ERR_CUDA;
 	}
 	return FLS_OK;

@@ -28,6 +28,7 @@ struct StrArgs {
 	uint8_t          kind;
 	bool             dict_in_smem; // materialising pass: decoded dictionary bytes in shared memory
 	bool             ends_in_smem; // lengths pass: dictionary end offsets in shared memory
+	bool             rows16;       // DICT with fewer than 65535 entries: codes kept as 16-bit rows
 	uint32_t         entry_c;
 	const uint32_t*  dict_ends;
 	const uint8_t*   dict_bytes;
@@ -46,10 +47,10 @@ cudaError_t launch_fsst_dict(const uint8_t* lens, const uint8_t* comp, uint64_t 
                              cudaStream_t s);
 cudaError_t launch_str_lengths(const StrArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_scan_totals(const uint64_t* total, uint64_t* base, uint64_t n, cudaStream_t s);
-// warps: warps per CTA (at most kStrMaxWarps); dyn_smem: warps * str_smem_per_warp() plus the 16-byte rounded
-// dictionary bytes when a.dict_in_smem
+// warps: warps per CTA (at most kStrMaxWarps); dyn_smem: warps * str_smem_per_warp(a.rows16) plus the
+// 16-byte rounded dictionary bytes when a.dict_in_smem
 cudaError_t launch_str_materialize(const StrArgs& a, int warps, uint32_t dyn_smem, cudaStream_t s);
-uint32_t    str_smem_per_warp();
+uint32_t    str_smem_per_warp(bool rows16);
 // shared-memory bytes of the dictionary end offsets (16-byte rounded)
 __host__ __device__ inline uint32_t str_ends_smem(const StrArgs& a) { return (a.entry_c * 4u + 15u) & ~15u; }
 

@@ -78,11 +78,12 @@ def _mixed_length_dictionary(rng, n):
     return rng.integers(0, 256, int(offs[-1]), dtype=np.uint8), offs
 
 
-@pytest.mark.parametrize("n_dict", [600, 12000, 20000])
+@pytest.mark.parametrize("n_dict", [600, 12000, 20000, 70000])
 def test_string_dict_shared_memory_modes(cuda, n_dict):
-    """DICT rows of every length class, with the dictionary bytes and end offsets in shared memory (600
-    entries), only the end offsets there (12000: the bytes do not fit beside the warps), or neither (20000:
-    80 KB of end offsets).  Batches of 32 long rows exceed the per-warp window."""
+    """DICT rows of every length class: the decoded dictionary in shared memory for the materialising pass
+    (600 entries) or not (the larger ones), its end offsets in shared memory for the lengths pass (up to
+    12000) or not (20000: 80 KB of them); 16-bit code rows below 65535 entries, 32-bit ones at 70000.  Batches
+    of 32 long rows exceed the per-warp window."""
     from fastlanes_b200 import strings
 
     rng = np.random.default_rng(n_dict)
