@@ -21,6 +21,7 @@ namespace flsgpu {
 #define FLS_GATHER 32, 0u, 8, 10, 2, KIND_GATHER
 #define FLS_GATHER32 32, 0u, 4, 12, 2, KIND_GATHER
 #define FLS_ANY 64, 8320u, 8, 6, 2, KIND_ALL
+#define FLS_FILTER 64, 8320u, 8, 6, 2, (KIND_ALL | KIND_FILTER)
 
 template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES, int KIND>
 static cudaError_t launch_family(const DecodeArgs& a, cudaStream_t s, int sm_count, int grid_override) {
@@ -93,6 +94,7 @@ static const Variant kGather32[] = {FLS_VARIANT("gather32 12x2", FLS_GATHER32),
                                     FLS_VARIANT("gather32 12x3", 32, 0u, 4, 12, 3, KIND_GATHER),
                                     FLS_VARIANT("gather32 16x2", 32, 0u, 4, 16, 2, KIND_GATHER)};
 static const Variant kAny[]      = {FLS_VARIANT("any 6x2", FLS_ANY)};
+static const Variant kFilter[]   = {FLS_VARIANT("filter 6x2", FLS_FILTER)};
 
 // The variants of a family; a NUM launch without a column array whose column is narrow runs the NUM32 kernels.
 static const Variant* family_variants(Family fam, const DecodeArgs& a, int* n) {
@@ -105,6 +107,7 @@ static const Variant* family_variants(Family fam, const DecodeArgs& a, int* n) {
 	case Family::NUM_PATCH: *n = 2; return kNumPatch;
 	case Family::GATHER: *n = 3; return kGather;
 	case Family::GATHER_NARROW: *n = 3; return kGather32;
+	case Family::FILTER: *n = 1; return kFilter;
 	default: *n = 1; return kAny;
 	}
 }
@@ -441,6 +444,7 @@ struct fls_plan {
 	Family    seg_fam[kMaxSegments] {};
 	int       variant[kMaxSegments] {}; // geometry variant of each segment (fls_plan_autotune)
 	std::vector<void*> owned;        // device buffers decoded for the plan (rec buffers)
+	Pred               pred {};      // filter plans: the predicate of their FILTER launch
 	cudaGraphExec_t graph = nullptr; // the segments' launches, captured by fls_plan_decode_graph
 	cudaStream_t    graph_stream = nullptr;
 };
@@ -448,6 +452,17 @@ struct fls_plan {
 namespace flsgpu {
 void plan_adopt(::fls_plan* plan, std::vector<void*>&& buffers) {
 	for (void* b : buffers) { plan->owned.push_back(b); }
+}
+
+void plan_set_filter(::fls_plan* plan, const Pred& pred) {
+	// one launch of the catch-all kernel in its filter form, whatever the item classes
+	plan->pred         = pred;
+	plan->family       = Family::FILTER;
+	plan->n_seg        = 1;
+	plan->seg_fam[0]   = Family::FILTER;
+	plan->seg_begin[0] = 0;
+	plan->seg_begin[1] = plan->n_items;
+	plan->variant[0]   = 0;
 }
 
 bool plan_segments(const std::vector<ColDesc>& descs, const std::vector<uint32_t>& queue, uint32_t col_shift,
@@ -633,6 +648,7 @@ bool segment_args(const fls_plan* p, int seg, DecodeArgs* a, Family* fam) {
 	x.col_shift = p->col_shift;
 	x.col0      = p->col0;
 	x.n_items   = p->n_seg == 1 ? p->n_items : p->seg_begin[seg + 1] - p->seg_begin[seg];
+	x.pred      = p->pred;
 	*fam        = p->seg_fam[seg];
 	*a          = x;
 	return true;

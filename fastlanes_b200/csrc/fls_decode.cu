@@ -32,6 +32,7 @@ struct Plan {
 	uint32_t       n_runs;
 	uint32_t       ghead; // offset of the run values inside the staged (16-byte aligned) copy
 	uint8_t        ws, e, enc, post, order;
+	uint8_t        cmp; // OUT_BITMAP_* of filter plans, else OUT_VALUES
 	bool           ok;
 	bool           lb_exact; // lane bases outside a page: copy exactly 128 bytes, never a window around them
 };
@@ -97,7 +98,8 @@ __device__ __forceinline__ Plan make_plan(const ColDesc& c, uint32_t v) {
 	p.order   = c.order;
 	p.entry_c = c.entry_c;
 	p.dict    = c.dict;
-	p.out     = c.out + static_cast<uint64_t>(v) * kVec * c.e;
+	p.cmp     = c.out_mode;
+	p.out     = c.out + static_cast<uint64_t>(v) * (c.out_mode != OUT_VALUES ? 128u : kVec * c.e);
 	p.ok      = v < c.n_vec;
 	p.lb_exact   = c.layout == LAYOUT_ARRAYS;
 	p.for_base   = 0;
@@ -458,16 +460,86 @@ __device__ __forceinline__ void store_vector(const typename OutT<E>::T (&o)[32],
 }
 
 // ---------------------------------------------------------------------------------------------------------
+// Predicate of 32 values per thread (run order) into the vector's 1024-bit bitmap at out (predicate pushdown:
+// the decoded values never leave the registers).  Bit i of the bitmap is value i of the vector in the plan's
+// order (original or transposed).  bm: 128 bytes of free shared memory (the stage).
+// ---------------------------------------------------------------------------------------------------------
+template <int E>
+__device__ __forceinline__ bool pred_holds(uint64_t x, bool sgn, const Pred& pr) {
+	if constexpr (E < 8) { x &= (1ull << (8 * E)) - 1; }
+	bool lt, eq;
+	if (sgn) {
+		const int64_t xs = E == 1 ? static_cast<int64_t>(static_cast<int8_t>(x))
+		                 : E == 2 ? static_cast<int64_t>(static_cast<int16_t>(x))
+		                 : E == 4 ? static_cast<int64_t>(static_cast<int32_t>(x))
+		                          : static_cast<int64_t>(x);
+		lt = xs < static_cast<int64_t>(pr.value);
+		eq = xs == static_cast<int64_t>(pr.value);
+	} else {
+		lt = x < pr.value;
+		eq = x == pr.value;
+	}
+	switch (pr.op) {
+	case PRED_EQ: return eq;
+	case PRED_NE: return !eq;
+	case PRED_LT: return lt;
+	case PRED_LE: return lt || eq;
+	case PRED_GT: return !lt && !eq;
+	default: return !lt;
+	}
+}
+
+template <int WS, int E>
+__device__ __forceinline__ void filter_vector(const typename OutT<E>::T (&o)[32], const Plan& p, uint8_t* ost,
+                                              uint32_t t, const Pred& pr) {
+	constexpr uint32_t RL  = run_len<WS>();
+	constexpr uint32_t RC  = run_count<WS>();
+	uint32_t*          bm  = reinterpret_cast<uint32_t*>(ost);
+	const bool         sgn = p.cmp == OUT_BITMAP_S;
+	__syncwarp(); // the stage was just read into registers
+	bm[t] = 0;
+	__syncwarp();
+	if (p.order) {
+		// a run is RL consecutive values of the original order starting at a multiple of 8
+#pragma unroll
+		for (uint32_t r = 0; r < RC; ++r) {
+			uint32_t m = 0;
+#pragma unroll
+			for (uint32_t j = 0; j < RL; ++j) { m |= static_cast<uint32_t>(pred_holds<E>(o[r * RL + j], sgn, pr)) << j; }
+			const uint32_t s  = run_start<WS>(t, r);
+			const uint64_t mm = static_cast<uint64_t>(m) << (s & 31u);
+			if (static_cast<uint32_t>(mm)) { atomicOr(bm + s / 32, static_cast<uint32_t>(mm)); }
+			if (mm >> 32) { atomicOr(bm + s / 32 + 1, static_cast<uint32_t>(mm >> 32)); }
+		}
+	} else {
+#pragma unroll
+		for (uint32_t r = 0; r < RC; ++r) {
+#pragma unroll
+			for (uint32_t j = 0; j < RL; ++j) {
+				if (pred_holds<E>(o[r * RL + j], sgn, pr)) {
+					const uint32_t k = run_tpos<WS>(t, r, j);
+					atomicOr(bm + k / 32, 1u << (k & 31u));
+				}
+			}
+		}
+	}
+	__syncwarp();
+	reinterpret_cast<uint32_t*>(p.out)[t] = bm[t];
+	__syncwarp();
+}
+
+// ---------------------------------------------------------------------------------------------------------
 // Full decode of one staged vector.
 // ---------------------------------------------------------------------------------------------------------
 // GSMEM: RLE run values / run codes staged in shared memory at gstage + ghead (else read from p.gsrc).
 // KIND: bit 0 = the kernel handles RLE / DICT gathers, bit 1 = patched FFOR / DELTA items; a kernel that meets
-// an item outside its kind flags a layout error (plans never route one there).
-enum : int { KIND_PLAIN = 0, KIND_GATHER = 1, KIND_PATCH = 2, KIND_ALL = 3 };
+// an item outside its kind flags a layout error (plans never route one there).  Bit 2 (KIND_FILTER): the
+// vector's predicate bitmap is written instead of its values.
+enum : int { KIND_PLAIN = 0, KIND_GATHER = 1, KIND_PATCH = 2, KIND_ALL = 3, KIND_FILTER = 4 };
 
 template <int WS, int E, bool GSMEM = true, int KIND = KIND_ALL>
 __device__ __forceinline__ void decode_vector(const Plan& p, const uint8_t* stage, const uint8_t* gstage, uint8_t* ost,
-                                              uint32_t t, int* status) {
+                                              uint32_t t, int* status, const Pred& pr = Pred {}) {
 	using ST = typename StreamT<WS>::T;
 	using OT = typename OutT<E>::T;
 	ST v[32];
@@ -525,7 +597,11 @@ __device__ __forceinline__ void decode_vector(const Plan& p, const uint8_t* stag
 		}
 	}
 	if (__any_sync(0xFFFFFFFFu, bad) && t == 0) { atomicOr(status, STATUS_BAD_INDEX); }
-	store_vector<WS, E>(o, p.out, ost, p.order != 0, t);
+	if constexpr ((KIND & KIND_FILTER) != 0) {
+		filter_vector<WS, E>(o, p, ost, t, pr);
+	} else {
+		store_vector<WS, E>(o, p.out, ost, p.order != 0, t);
+	}
 }
 
 // Compact plan kept in shared memory between the lane-parallel metadata fetch and the use of the plan.
@@ -539,7 +615,8 @@ struct __align__(16) PlanS {
 	uint32_t       gbytes;
 	uint32_t       entry_c;
 	uint16_t       bytes;
-	uint8_t        bw, ws, e, enc, post, flags; // flags: bit0 original order, bit1 ok, bit2 valid, bit3 lb_exact
+	uint8_t        bw, ws, e, enc, post, flags; // flags: bit0 original order, bit1 ok, bit2 valid, bit3 lb_exact,
+	                                            // bits 4-5 cmp
 };
 static_assert(sizeof(PlanS) == 64, "PlanS layout");
 
@@ -559,7 +636,8 @@ __device__ __forceinline__ PlanS pack_plan(const Plan& p, bool valid) {
 	s.e          = p.e;
 	s.enc        = p.enc;
 	s.post       = p.post;
-	s.flags      = static_cast<uint8_t>((p.order ? 1 : 0) | (p.ok ? 2 : 0) | (valid ? 4 : 0) | (p.lb_exact ? 8 : 0));
+	s.flags      = static_cast<uint8_t>((p.order ? 1 : 0) | (p.ok ? 2 : 0) | (valid ? 4 : 0) | (p.lb_exact ? 8 : 0) |
+	                                    ((p.cmp & 3u) << 4));
 	return s;
 }
 
@@ -582,6 +660,7 @@ __device__ __forceinline__ Plan unpack_plan(const PlanS& s) {
 	p.order      = s.flags & 1u;
 	p.ok         = (s.flags & 2u) != 0;
 	p.lb_exact   = (s.flags & 8u) != 0;
+	p.cmp        = (s.flags >> 4) & 3u;
 	const uint32_t ve = p.post == POST_RLE ? p.e : 4u;
 	p.n_runs     = (p.post == POST_RLE || p.post == POST_RLE_DICT) ? p.gbytes / ve : 0u;
 	p.ghead      = static_cast<uint32_t>(reinterpret_cast<uintptr_t>(p.gsrc) & 15u);
@@ -621,27 +700,27 @@ struct Geometry {
 
 template <int MAXWS, uint32_t GSTAGE, int EMAX, int KIND>
 __device__ __forceinline__ void decode_dispatch(const Plan& p, uint8_t* st, const uint8_t* gs, uint32_t lane,
-                                                int* status) {
+                                                int* status, const Pred& pr) {
 	if (p.ws == 64) {
-		if constexpr (MAXWS >= 64) { decode_vector<64, 8, (GSTAGE > 0), KIND>(p, st, gs, st, lane, status); }
+		if constexpr (MAXWS >= 64) { decode_vector<64, 8, (GSTAGE > 0), KIND>(p, st, gs, st, lane, status, pr); }
 	} else if (p.ws == 32) {
 		if constexpr (MAXWS >= 32) {
 			if (p.e == 8) {
-				if constexpr (EMAX >= 8) { decode_vector<32, 8, (GSTAGE > 0), KIND>(p, st, gs, st, lane, status); }
+				if constexpr (EMAX >= 8) { decode_vector<32, 8, (GSTAGE > 0), KIND>(p, st, gs, st, lane, status, pr); }
 			} else {
-				decode_vector<32, 4, (GSTAGE > 0), KIND>(p, st, gs, st, lane, status);
+				decode_vector<32, 4, (GSTAGE > 0), KIND>(p, st, gs, st, lane, status, pr);
 			}
 		}
 	} else if (p.ws == 16) {
 		if (p.e == 8) {
-			if constexpr (EMAX >= 8) { decode_vector<16, 8, (GSTAGE > 0), KIND>(p, st, gs, st, lane, status); }
+			if constexpr (EMAX >= 8) { decode_vector<16, 8, (GSTAGE > 0), KIND>(p, st, gs, st, lane, status, pr); }
 		} else if (p.e == 4) {
-			if constexpr (EMAX >= 4) { decode_vector<16, 4, (GSTAGE > 0), KIND>(p, st, gs, st, lane, status); }
+			if constexpr (EMAX >= 4) { decode_vector<16, 4, (GSTAGE > 0), KIND>(p, st, gs, st, lane, status, pr); }
 		} else {
-			decode_vector<16, 2, (GSTAGE > 0), KIND>(p, st, gs, st, lane, status);
+			decode_vector<16, 2, (GSTAGE > 0), KIND>(p, st, gs, st, lane, status, pr);
 		}
 	} else {
-		decode_vector<8, 1, (GSTAGE > 0), KIND>(p, st, gs, st, lane, status);
+		decode_vector<8, 1, (GSTAGE > 0), KIND>(p, st, gs, st, lane, status, pr);
 	}
 }
 
@@ -712,7 +791,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_decode(const DecodeArgs a) {
 		} else {
 			// the lane bases were staged with the packed words
 			if (p.lane_bases) { p.lane_bases = lb_ptr(s) + (reinterpret_cast<uintptr_t>(p.lane_bases) & 15u); }
-			decode_dispatch<MAXWS, GSTAGE, EMAX, KIND>(p, stage_ptr(s), gstage_ptr(s), lane, a.status);
+			decode_dispatch<MAXWS, GSTAGE, EMAX, KIND>(p, stage_ptr(s), gstage_ptr(s), lane, a.status, a.pred);
 		}
 		__syncwarp();
 		issue_k(k + STAGES, s);

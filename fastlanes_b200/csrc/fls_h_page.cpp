@@ -329,6 +329,38 @@ int fls_gpu_decode_pages(const fls_page_column* cols, uint32_t n_cols, fls_strea
 	return e == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
 }
 
+int fls_plan_create_filter(const fls_page_column* cols, uint32_t n_cols, const fls_predicate* pred,
+                           fls_plan** out_plan) {
+	if (!out_plan || !pred || pred->op > FLS_PRED_GE) { return FLS_ERR_ARG; }
+	*out_plan = nullptr;
+	for (uint32_t i = 0; cols && i < n_cols; ++i) {
+		if (cols[i].data_type == DOUBLE) { return FLS_ERR_UNSUPPORTED; }
+	}
+	std::vector<ColDesc>  descs;
+	std::vector<uint32_t> queue;
+	Family                fam = Family::NUM;
+	std::vector<void*>    owned;
+	int                   rc = describe_pages(cols, n_cols, &descs, &queue, &fam, nullptr, &owned);
+	if (rc == FLS_OK) {
+		for (uint32_t i = 0; i < n_cols; ++i) {
+			const uint8_t t = cols[i].data_type;
+			descs[i].out_mode = (t == INT8 || t == INT16 || t == INT32 || t == INT64) ? OUT_BITMAP_S : OUT_BITMAP_U;
+		}
+		rc = make_plan_object(descs, queue, fam, kPageShift, out_plan);
+	}
+	if (rc == FLS_OK) {
+		plan_adopt(*out_plan, std::move(owned));
+		Pred p {};
+		p.op    = pred->op;
+		p.value = static_cast<uint64_t>(pred->value);
+		plan_set_filter(*out_plan, p);
+	} else {
+		cudaDeviceSynchronize();
+		for (void* p : owned) { cudaFree(p); }
+	}
+	return rc;
+}
+
 int fls_plan_create_pages(const fls_page_column* cols, uint32_t n_cols, fls_plan** out_plan) {
 	if (!out_plan) { return FLS_ERR_ARG; }
 	*out_plan = nullptr;

@@ -62,7 +62,7 @@ struct alignas(16) ColDesc {
 	// LAYOUT_PAGE: role -> buffer index (kNoBuf when absent) and resolved buffer starts
 	uint8_t  ib_bw, ib_base, ib_packed, ib_lane_bases, ib_vals;
 	uint8_t  ib_exc, ib_side; // patched variants: exception values, positions / bitmap / chain head
-	uint8_t  pad0;
+	uint8_t  out_mode;        // OUT_VALUES, or OUT_BITMAP_*: `out` takes one 1024-bit predicate bitmap per vector
 	const uint8_t*  buf[6];
 	uint64_t        buf_size[6];
 	const uint32_t* ep; // entry points, (n_vec - 1) x arr_c u32; vector 0 starts at 0 in every buffer
@@ -76,7 +76,22 @@ struct alignas(16) ColDesc {
 
 	// gathers and output
 	const uint8_t* dict; // POST_DICT: entry_c values of e bytes
-	uint8_t*       out;  // n_vec * 1024 * e bytes
+	uint8_t*       out;  // n_vec * 1024 * e bytes (OUT_VALUES) or n_vec * 128 bytes (bitmaps)
+};
+
+enum : uint8_t {
+	OUT_VALUES   = 0,
+	OUT_BITMAP_U = 1, // bitmap of `value OP constant`, values compared as unsigned e-byte integers
+	OUT_BITMAP_S = 2, // the same, values compared as signed (two's complement) e-byte integers
+};
+
+// Predicate of a filter launch: value OP constant, the constant widened to 64 bits (sign-extended for signed
+// columns).  Mirrors the reference's predicate primitives (src/primitive/predicate/equal.cpp).
+enum : uint32_t { PRED_EQ = 0, PRED_NE = 1, PRED_LT = 2, PRED_LE = 3, PRED_GT = 4, PRED_GE = 5 };
+struct Pred {
+	uint64_t value;
+	uint32_t op;
+	uint32_t pad;
 };
 
 struct DecodeArgs {
@@ -86,6 +101,7 @@ struct DecodeArgs {
 	int*            status;    // device word; kernels OR error bits into it
 	uint32_t        col_shift; // 24 for batch plans (256 batches), 16 for page plans (65,535 pages)
 	ColDesc         col0;
+	Pred            pred; // filter launches (KIND_FILTER kernels) only
 };
 
 enum : int {

@@ -116,6 +116,60 @@ class PagePlan:
             pass
 
 
+# ---- predicate pushdown (src/primitive/predicate/equal.cpp of the reference) ------------------------------
+PRED_EQ, PRED_NE, PRED_LT, PRED_LE, PRED_GT, PRED_GE = range(6)
+BITMAP_AND, BITMAP_OR, BITMAP_ANDNOT = range(3)
+
+
+class Predicate(ctypes.Structure):
+    _fields_ = [("op", ctypes.c_uint8), ("reserved", ctypes.c_uint8 * 7), ("value", ctypes.c_int64)]
+
+
+_plan_filter = declare("fls_plan_create_filter", ctypes.c_int, [ctypes.POINTER(PageColumn), ctypes.c_uint32,
+                                                                  ctypes.POINTER(Predicate), ctypes.POINTER(_p)])
+_to_selection = declare("fls_gpu_bitmap_to_selection", ctypes.c_int, [_p, _u64, _p, _p, _p])
+_combine = declare("fls_gpu_bitmap_combine", ctypes.c_int, [_p, _p, _p, _u64, ctypes.c_int, _p])
+_sel_and = declare("fls_gpu_selection_and", ctypes.c_int, [_p, _p, _p, _p, _p, _p, _u64, _p])
+
+
+def _stream(stream):
+    import torch
+
+    return stream if stream is not None else torch.cuda.current_stream().cuda_stream
+
+
+class FilterPlan(PagePlan):
+    """fls_plan_create_filter: `column OP value` over page columns; each column's d_out receives vec_c * 128
+    bytes (one 1024-bit bitmap per vector, bit i = value i in the column's order).  decode() evaluates.  The
+    value is compared with every value widened to 64 bits (sign-extended for signed types); an unsigned
+    column's constant is given as its uint64 bits or any Python int that wraps to them."""
+
+    def __init__(self, columns, op, value):
+        pr = Predicate()
+        pr.op = op
+        v = int(value) & (2**64 - 1)
+        pr.value = v - 2**64 if v >= 2**63 else v
+        h = _p()
+        check(_plan_filter(_columns(columns), len(columns), ctypes.byref(pr), ctypes.byref(h)),
+              "fls_plan_create_filter")
+        self.handle = h
+
+
+def bitmap_to_selection(d_bitmaps, n_vec, d_idx, d_count, stream=None):
+    """SelectionDS idx_arr / n_selected_values per vector (u16) from bitmaps (device pointers)."""
+    check(_to_selection(d_bitmaps, n_vec, d_idx, d_count, _stream(stream)), "fls_gpu_bitmap_to_selection")
+
+
+def bitmap_combine(d_a, d_b, d_out, n_vec, op, stream=None):
+    check(_combine(d_a, d_b, d_out, n_vec, op, _stream(stream)), "fls_gpu_bitmap_combine")
+
+
+def selection_and(d_idx0, d_count0, d_idx1, d_count1, d_idx_out, d_count_out, n_vec, stream=None):
+    """and_selection_ds_func per vector on index lists (device pointers)."""
+    check(_sel_and(d_idx0, d_count0, d_idx1, d_count1, d_idx_out, d_count_out, n_vec, _stream(stream)),
+          "fls_gpu_selection_and")
+
+
 def decode_pages(columns, stream=None):
     """columns: list of dicts with d_page, page_size, d_dict, dict_size, data_type, order, d_out (device ptrs)."""
     import torch

@@ -220,6 +220,51 @@ int fls_gpu_decode_pages(const fls_page_column* cols, uint32_t n_cols, fls_strea
 int fls_plan_create_pages(const fls_page_column* cols, uint32_t n_cols, fls_plan** out_plan);
 
 /* ---------------------------------------------------------------------------------------------------------
+ * Predicate pushdown on compressed columns.  Replaces the reference's per-vector predicate primitives on
+ * decoded i64 vectors (src/primitive/predicate/equal.cpp:9-99: eq_vector_constant_func, ge_tvec_cvec,
+ * lessthan_func, behind predicate_eq_vector_constant_i64 / predicate_GT_i64 / predicate_LE_i64 of
+ * include/fls/expression/predicate_operator.hpp:7-112) and and_selection_ds_func (equal.cpp:100-119), for every
+ * integer expression and type the page decoder handles.  The values are decoded in registers and never
+ * written: each vector yields a 1024-bit bitmap (16 u64 words, the layout of SelectionDS::bitmap,
+ * include/fls/expression/selection_ds.hpp:27), bit i = value i of the vector in the column's order.  Note the
+ * reference's operators: predicate_GT_i64 computes `>`, predicate_LE_i64 computes `<` (lessthan_func).
+ * ------------------------------------------------------------------------------------------------------- */
+#define FLS_PRED_EQ 0 /* value == constant */
+#define FLS_PRED_NE 1
+#define FLS_PRED_LT 2 /* value <  constant (the reference's predicate_LE_i64 / lessthan_func) */
+#define FLS_PRED_LE 3
+#define FLS_PRED_GT 4 /* value >  constant (the reference's predicate_GT_i64 / ge_tvec_cvec) */
+#define FLS_PRED_GE 5
+typedef struct {
+	uint8_t op; /* FLS_PRED_* */
+	uint8_t reserved[7];
+	int64_t value; /* the constant; compared with each value widened to 64 bits: sign-extended for the signed
+	                  data types (value read as int64), zero-extended for the unsigned ones (value read as its
+	                  uint64 bits) */
+} fls_predicate;
+/* A filter plan over page columns (as fls_plan_create_pages; DOUBLE columns are refused): cols[i].d_out
+ * receives vec_c * 128 bytes, one bitmap per vector; fls_plan_decode / fls_plan_decode_graph evaluate. */
+int fls_plan_create_filter(const fls_page_column* cols, uint32_t n_cols, const fls_predicate* pred,
+                           fls_plan** out_plan);
+/* SelectionDS::idx_arr / n_selected_values per vector from bitmaps (equal.cpp:12-28, the index form):
+ * d_idx: n_vec * 1024 u16 positions in ascending order (entries past the count are left as they are),
+ * d_count: n_vec u16.  Asynchronous. */
+int fls_gpu_bitmap_to_selection(const uint64_t* d_bitmaps, uint64_t n_vec, uint16_t* d_idx, uint16_t* d_count,
+                                fls_stream_t stream);
+#define FLS_BITMAP_AND 0
+#define FLS_BITMAP_OR 1
+#define FLS_BITMAP_ANDNOT 2 /* a & ~b */
+/* Word-wise combination of n_vec bitmaps (d_out may alias an input). */
+int fls_gpu_bitmap_combine(const uint64_t* d_a, const uint64_t* d_b, uint64_t* d_out, uint64_t n_vec, int op,
+                           fls_stream_t stream);
+/* and_selection_ds_func (equal.cpp:100-119) per vector: the positions present in both index lists (each
+ * ascending, positions < 1024), ascending.  Lists of d_count0 / d_count1 entries at d_idx0 / d_idx1 + 1024 * v;
+ * an out-of-range position or count sets FLS_DEV_BAD_INDEX (fls_gpu_status). */
+int fls_gpu_selection_and(const uint16_t* d_idx0, const uint16_t* d_count0, const uint16_t* d_idx1,
+                          const uint16_t* d_count1, uint16_t* d_idx_out, uint16_t* d_count_out, uint64_t n_vec,
+                          fls_stream_t stream);
+
+/* ---------------------------------------------------------------------------------------------------------
  * String columns.  d_page: a string page (DICT: str expressions 2, 3, 8; DICT_RLE: 15, 16; FSST: 13, 14;
  * BYTE_ARR: 0 of src/cor/exp_pool.cpp:66-101); d_dict: its dictionary bytes (DICT / DICT_RLE: the FSST-
  * compressed dictionary page; FSST: the exported symbol table; BYTE_ARR: none).  Creating a plan decodes the

@@ -28,6 +28,9 @@
 #include "fls_gen/unpack/unpack.hpp"
 #include "fls_gen/unrsum/unrsum.hpp"
 #include "fls_gen/untranspose/untranspose.hpp"
+#include "fls/expression/logical_expression.hpp"
+#include "fls/expression/selection_ds.hpp"
+#include "fls/primitive/predicate/equal.hpp"
 #include <cstring>
 #include <exception>
 #include <string>
@@ -303,6 +306,41 @@ int64_t ref_fsst_decompress(const uint8_t* table, uint64_t in_len, const uint8_t
 	fsst_decoder_t d;
 	if (fsst_import(&d, const_cast<unsigned char*>(table)) == 0) { return -1; }
 	return static_cast<int64_t>(fsst_decompress(&d, in_len, const_cast<unsigned char*>(in), cap, out));
+}
+
+/* SelectionDS only keeps a reference to its LogicalExpr, which the predicate primitives never touch; the
+ * reference defines no constructible LogicalExpr (src/expression/logical_expression.cpp has its member
+ * definitions commented out), so the reference is bound to inert storage. */
+static const LogicalExpr& no_expr() {
+	alignas(LogicalExpr) static unsigned char raw[sizeof(LogicalExpr)] = {};
+	return *reinterpret_cast<const LogicalExpr*>(raw);
+}
+
+/* The reference's predicate primitives on one decoded i64 vector (src/primitive/predicate/equal.cpp): op 0
+ * eq_vector_constant_func (==), 1 ge_tvec_cvec (>), 2 lessthan_func (<).  The selected positions go to idx
+ * (1024 u16); returns their count. */
+int ref_predicate_i64(int op, const int64_t* vec, int64_t value, uint16_t* idx) {
+	SelectionDS ds(no_expr());
+	switch (op) {
+	case 0: eq_vector_constant_func<i64_pt>(vec, value, ds); break;
+	case 1: ge_tvec_cvec<i64_pt>(vec, &value, ds); break;
+	case 2: lessthan_func<i64_pt>(vec, value, ds); break;
+	default: return -1;
+	}
+	std::memcpy(idx, ds.idx_arr.data(), 1024 * sizeof(uint16_t));
+	return ds.n_selected_values;
+}
+
+/* and_selection_ds_func (equal.cpp:100-119) of two index lists; returns the output count. */
+int ref_selection_and(const uint16_t* i0, int n0, const uint16_t* i1, int n1, uint16_t* out) {
+	SelectionDS a(no_expr()), b(no_expr()), c(no_expr());
+	std::memcpy(a.idx_arr.data(), i0, sizeof(uint16_t) * n0);
+	std::memcpy(b.idx_arr.data(), i1, sizeof(uint16_t) * n1);
+	a.n_selected_values = static_cast<vec_idx_t>(n0);
+	b.n_selected_values = static_cast<vec_idx_t>(n1);
+	and_selection_ds_func(a, b, c);
+	std::memcpy(out, c.idx_arr.data(), 1024 * sizeof(uint16_t));
+	return c.n_selected_values;
 }
 
 } // extern "C"

@@ -14,29 +14,31 @@ thread_local int      g_emu_lane = 0;
 
 using namespace flsgpu;
 
-static void dispatch(const Plan& p, const uint8_t* st, const uint8_t* gs, uint8_t* ost, uint32_t t, int* status) {
+template <int K = KIND_ALL>
+static void dispatch(const Plan& p, const uint8_t* st, const uint8_t* gs, uint8_t* ost, uint32_t t, int* status,
+                     const Pred& pr = Pred {}) {
 	if (p.ws == 64) {
-		decode_vector<64, 8>(p, st, gs, ost, t, status);
+		decode_vector<64, 8, true, K>(p, st, gs, ost, t, status, pr);
 	} else if (p.ws == 32) {
 		if (p.e == 8) {
-			decode_vector<32, 8>(p, st, gs, ost, t, status);
+			decode_vector<32, 8, true, K>(p, st, gs, ost, t, status, pr);
 		} else {
-			decode_vector<32, 4>(p, st, gs, ost, t, status);
+			decode_vector<32, 4, true, K>(p, st, gs, ost, t, status, pr);
 		}
 	} else if (p.ws == 16) {
 		if (p.e == 8) {
-			decode_vector<16, 8>(p, st, gs, ost, t, status);
+			decode_vector<16, 8, true, K>(p, st, gs, ost, t, status, pr);
 		} else if (p.e == 4) {
-			decode_vector<16, 4>(p, st, gs, ost, t, status);
+			decode_vector<16, 4, true, K>(p, st, gs, ost, t, status, pr);
 		} else {
-			decode_vector<16, 2>(p, st, gs, ost, t, status);
+			decode_vector<16, 2, true, K>(p, st, gs, ost, t, status, pr);
 		}
 	} else {
-		decode_vector<8, 1>(p, st, gs, ost, t, status);
+		decode_vector<8, 1, true, K>(p, st, gs, ost, t, status, pr);
 	}
 }
 
-static int emu_vector(const ColDesc& c, uint32_t v) {
+static int emu_vector(const ColDesc& c, uint32_t v, const Pred* filter = nullptr) {
 	Plan p = make_plan(c, v);
 	if (!p.ok) { return p.bw > p.ws ? STATUS_BAD_BW : STATUS_BAD_LAYOUT; }
 	std::vector<uint8_t> smem(3 * 8448 + 8192, 0xA5);
@@ -67,7 +69,12 @@ static int emu_vector(const ColDesc& c, uint32_t v) {
 		th.emplace_back([&, t] {
 			g_emu_warp = &w;
 			g_emu_lane = t;
-			dispatch(p, stage, gstage, stage, static_cast<uint32_t>(t), &status); // as on the GPU: staging reuses the stage
+			// as on the GPU: staging reuses the stage
+			if (filter) {
+				dispatch<KIND_ALL | KIND_FILTER>(p, stage, gstage, stage, static_cast<uint32_t>(t), &status, *filter);
+			} else {
+				dispatch(p, stage, gstage, stage, static_cast<uint32_t>(t), &status);
+			}
 		});
 	}
 	for (auto& x : th) { x.join(); }
@@ -101,9 +108,17 @@ extern "C" int emu_unffor(int width, int enc, int order, const uint8_t* packed, 
 	return emu_decode_column(&c);
 }
 
-// Decode a reference page (host bytes) with the product's host page code + the emulated device logic.
+// Decode a reference page (host bytes) with the product's host page code + the emulated device logic; with
+// cmp != OUT_VALUES, the filter form: out receives one 128-byte bitmap of `value op constant` per vector.
+extern "C" int emu_filter_page(const uint8_t* page, uint64_t page_size, const uint8_t* dict, uint64_t dict_size,
+                               int value_width, int order, int cmp, uint32_t op, uint64_t value, uint8_t* out);
 extern "C" int emu_decode_page(const uint8_t* page, uint64_t page_size, const uint8_t* dict, uint64_t dict_size,
                                int value_width, int order, uint8_t* out) {
+	return emu_filter_page(page, page_size, dict, dict_size, value_width, order, OUT_VALUES, 0, 0, out);
+}
+
+extern "C" int emu_filter_page(const uint8_t* page, uint64_t page_size, const uint8_t* dict, uint64_t dict_size,
+                               int value_width, int order, int cmp, uint32_t op, uint64_t value, uint8_t* out) {
 	PageInfo pi;
 	int      rc = parse_page_header(page, page_size, &pi);
 	if (rc == FLS_OK) { rc = finish_page_info(&pi, page_size); }
@@ -119,5 +134,12 @@ extern "C" int emu_decode_page(const uint8_t* page, uint64_t page_size, const ui
 	ColDesc c;
 	rc = build_page_column(pi, page, value_width, dvals, entries, order, out, &c);
 	if (rc != FLS_OK) { return -3000 + rc; }
-	return emu_decode_column(&c);
+	if (cmp == OUT_VALUES) { return emu_decode_column(&c); }
+	c.out_mode = static_cast<uint8_t>(cmp);
+	Pred pr {};
+	pr.op    = op;
+	pr.value = value;
+	int st   = 0;
+	for (uint32_t v = 0; v < c.n_vec; ++v) { st |= emu_vector(c, v, &pr); }
+	return st;
 }

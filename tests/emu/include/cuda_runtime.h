@@ -76,6 +76,7 @@ inline bool __any_sync(unsigned, bool p) {
 	return r;
 }
 inline int atomicOr(int* a, int v) { return __atomic_fetch_or(a, v, __ATOMIC_SEQ_CST); }
+inline unsigned atomicOr(unsigned* a, unsigned v) { return __atomic_fetch_or(a, v, __ATOMIC_SEQ_CST); }
 template <class T>
 T __ldg(const T* p) {
 	return *p;
