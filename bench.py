@@ -321,6 +321,22 @@ def other_configs(dev, args):
         leg(name, workload, ms, page.size, values.nbytes, values.size, ok, 1)
         out[name]["autotuned"] = tuned
         plan.close()
+        # predicate pushdown on the same page: value > median, one 1024-bit bitmap per vector, values never
+        # written (bytes = page read + bitmaps written)
+        c = int(np.median(values))
+        bm = torch.empty(values.size // 8, dtype=torch.uint8, device=dev)
+        fplan = PG.FilterPlan([dict(col[0], d_out=bm.data_ptr())], PG.PRED_GT, c)
+        fplan.decode()
+        want_bm = np.packbits((values > c).astype(np.uint8).reshape(-1, 1024), axis=1, bitorder="little")
+        fok = np.array_equal(bm.cpu().numpy().reshape(-1, 128), want_bm)
+        fms = device_timed(fplan.decode, steps, 3)
+        fplan.close()
+        leg(name + "_filter", f"x > {c} over the same page (filter plan: bitmaps only)", fms, page.size,
+            values.size // 8, values.size, fok, 1)
+        out[name + "_filter"]["decode_ms_per_step"] = round(ms, 4)
+        # value: the column's decoded bytes per second it filters (the same unit as the decode leg); the
+        # roofline fraction counts the bytes it moves (page + bitmaps)
+        out[name + "_filter"]["value"] = round(values.nbytes / (fms * 1e-3) / 1e9, 2)
 
     page_leg("3a_delta_i64", "32Mi sorted int64 timestamps from 1.6e18, geometric(mean 10) gaps, DELTA (id 11)",
              W.delta_timestamps(), PG.INT64, 11)

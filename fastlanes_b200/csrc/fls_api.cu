@@ -21,7 +21,6 @@ namespace flsgpu {
 #define FLS_GATHER 32, 0u, 8, 10, 2, KIND_GATHER
 #define FLS_GATHER32 32, 0u, 4, 12, 2, KIND_GATHER
 #define FLS_ANY 64, 8320u, 8, 6, 2, KIND_ALL
-#define FLS_FILTER 64, 8320u, 8, 6, 2, (KIND_ALL | KIND_FILTER)
 
 template <int MAXWS, uint32_t GSTAGE, int EMAX, int WARPS, int STAGES, int KIND>
 static cudaError_t launch_family(const DecodeArgs& a, cudaStream_t s, int sm_count, int grid_override) {
@@ -94,11 +93,28 @@ static const Variant kGather32[] = {FLS_VARIANT("gather32 12x2", FLS_GATHER32),
                                     FLS_VARIANT("gather32 12x3", 32, 0u, 4, 12, 3, KIND_GATHER),
                                     FLS_VARIANT("gather32 16x2", 32, 0u, 4, 16, 2, KIND_GATHER)};
 static const Variant kAny[]      = {FLS_VARIANT("any 6x2", FLS_ANY)};
-static const Variant kFilter[]   = {FLS_VARIANT("filter 6x2", FLS_FILTER)};
+// filter launches (predicate bitmaps instead of values): the same geometries in their KIND_FILTER form
+static const Variant kFNum64[]    = {FLS_VARIANT("filter num64 12x2", 64, 0u, 8, 12, 2, KIND_PLAIN | KIND_FILTER)};
+static const Variant kFNum32[]    = {FLS_VARIANT("filter num32 15x3", 32, 0u, 4, 15, 3, KIND_PLAIN | KIND_FILTER)};
+static const Variant kFNumPatch[] = {FLS_VARIANT("filter numpatch 12x2", 64, 0u, 8, 12, 2, KIND_PATCH | KIND_FILTER)};
+static const Variant kFGather[]   = {FLS_VARIANT("filter gather 10x2", 32, 0u, 8, 10, 2, KIND_GATHER | KIND_FILTER)};
+static const Variant kFGather32[] = {FLS_VARIANT("filter gather32 16x2", 32, 0u, 4, 16, 2, KIND_GATHER | KIND_FILTER)};
+static const Variant kFAny[]      = {FLS_VARIANT("filter any 6x2", 64, 8320u, 8, 6, 2, KIND_ALL | KIND_FILTER)};
 
 // The variants of a family; a NUM launch without a column array whose column is narrow runs the NUM32 kernels.
 static const Variant* family_variants(Family fam, const DecodeArgs& a, int* n) {
 	const bool narrow = a.cols == nullptr && a.col0.ws <= 32 && a.col0.e <= 4;
+	if (a.pred.active) {
+		*n = 1;
+		switch (fam) {
+		case Family::NUM_NARROW: return kFNum32;
+		case Family::NUM: return narrow ? kFNum32 : kFNum64;
+		case Family::NUM_PATCH: return kFNumPatch;
+		case Family::GATHER: return kFGather;
+		case Family::GATHER_NARROW: return kFGather32;
+		default: return kFAny;
+		}
+	}
 	switch (fam) {
 	case Family::NUM_NARROW: *n = 3; return kNum32;
 	case Family::NUM:
@@ -107,7 +123,6 @@ static const Variant* family_variants(Family fam, const DecodeArgs& a, int* n) {
 	case Family::NUM_PATCH: *n = 2; return kNumPatch;
 	case Family::GATHER: *n = 3; return kGather;
 	case Family::GATHER_NARROW: *n = 3; return kGather32;
-	case Family::FILTER: *n = 1; return kFilter;
 	default: *n = 1; return kAny;
 	}
 }
@@ -455,14 +470,9 @@ void plan_adopt(::fls_plan* plan, std::vector<void*>&& buffers) {
 }
 
 void plan_set_filter(::fls_plan* plan, const Pred& pred) {
-	// one launch of the catch-all kernel in its filter form, whatever the item classes
-	plan->pred         = pred;
-	plan->family       = Family::FILTER;
-	plan->n_seg        = 1;
-	plan->seg_fam[0]   = Family::FILTER;
-	plan->seg_begin[0] = 0;
-	plan->seg_begin[1] = plan->n_items;
-	plan->variant[0]   = 0;
+	// the plan's segments run the filter form of their families
+	plan->pred        = pred;
+	plan->pred.active = 1;
 }
 
 bool plan_segments(const std::vector<ColDesc>& descs, const std::vector<uint32_t>& queue, uint32_t col_shift,

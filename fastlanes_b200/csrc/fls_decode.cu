@@ -462,69 +462,127 @@ __device__ __forceinline__ void store_vector(const typename OutT<E>::T (&o)[32],
 // ---------------------------------------------------------------------------------------------------------
 // Predicate of 32 values per thread (run order) into the vector's 1024-bit bitmap at out (predicate pushdown:
 // the decoded values never leave the registers).  Bit i of the bitmap is value i of the vector in the plan's
-// order (original or transposed).  bm: 128 bytes of free shared memory (the stage).
+// order (original or transposed).
 // ---------------------------------------------------------------------------------------------------------
+// The predicate for E-byte values: the classes (below / equal / above the constant) it accepts, and the
+// constant in the values' own width when it lies inside their range (else every value is in one class).
 template <int E>
-__device__ __forceinline__ bool pred_holds(uint64_t x, bool sgn, const Pred& pr) {
-	if constexpr (E < 8) { x &= (1ull << (8 * E)) - 1; }
-	bool lt, eq;
-	if (sgn) {
-		const int64_t xs = E == 1 ? static_cast<int64_t>(static_cast<int8_t>(x))
-		                 : E == 2 ? static_cast<int64_t>(static_cast<int16_t>(x))
-		                 : E == 4 ? static_cast<int64_t>(static_cast<int32_t>(x))
-		                          : static_cast<int64_t>(x);
-		lt = xs < static_cast<int64_t>(pr.value);
-		eq = xs == static_cast<int64_t>(pr.value);
-	} else {
-		lt = x < pr.value;
-		eq = x == pr.value;
+struct PredE {
+	using T = typename OutT<E>::T;
+	uint32_t accept; // bit 0: value < constant, bit 1: ==, bit 2: >
+	uint32_t fixed;  // 0: compare; else the class bit of every value (constant outside the values' range)
+	bool     sgn;
+	T        c;
+
+	__device__ __forceinline__ PredE(const Pred& pr, bool is_signed) : sgn(is_signed) {
+		// accepted classes of EQ NE LT LE GT GE: 2, 5, 1, 3, 4, 6 (one nibble each)
+		accept = (0x643152u >> (4 * (pr.op < 6 ? pr.op : 0))) & 7u;
+		fixed  = 0;
+		if constexpr (E == 8) {
+			c = pr.value;
+		} else {
+			const int64_t v = static_cast<int64_t>(pr.value);
+			if (sgn) {
+				const int64_t lo = -(1ll << (8 * E - 1)), hi = (1ll << (8 * E - 1)) - 1;
+				fixed            = v < lo ? 4u : v > hi ? 1u : 0u; // below the range: every value is above it
+			} else {
+				const uint64_t hi = (1ull << (8 * E)) - 1;
+				fixed             = pr.value > hi ? 1u : 0u;
+			}
+			c = static_cast<T>(pr.value);
+		}
 	}
-	switch (pr.op) {
-	case PRED_EQ: return eq;
-	case PRED_NE: return !eq;
-	case PRED_LT: return lt;
-	case PRED_LE: return lt || eq;
-	case PRED_GT: return !lt && !eq;
-	default: return !lt;
+	// class bit of x: 1 below, 2 equal, 4 above the constant
+	__device__ __forceinline__ uint32_t cls(T x) const {
+		if constexpr (E == 8) {
+			const bool lt = sgn ? static_cast<int64_t>(x) < static_cast<int64_t>(c) : x < c;
+			return x == c ? 2u : lt ? 1u : 4u;
+		} else {
+			if (fixed) { return fixed; }
+			constexpr uint32_t sh = 32 - 8 * E;
+			const uint32_t     xu = static_cast<uint32_t>(x) << sh; // the value's E bytes at the top
+			const uint32_t     cu = static_cast<uint32_t>(c) << sh;
+			const bool lt = sgn ? static_cast<int32_t>(xu) < static_cast<int32_t>(cu) : xu < cu;
+			return xu == cu ? 2u : lt ? 1u : 4u;
+		}
 	}
+	__device__ __forceinline__ bool operator()(T x) const { return (cls(x) & accept) != 0; }
+};
+
+// 16 bits to the even bits of a word
+__device__ __forceinline__ uint32_t spread16(uint32_t x) {
+	x = (x | (x << 8)) & 0x00FF00FFu;
+	x = (x | (x << 4)) & 0x0F0F0F0Fu;
+	x = (x | (x << 2)) & 0x33333333u;
+	return (x | (x << 1)) & 0x55555555u;
 }
 
 template <int WS, int E>
 __device__ __forceinline__ void filter_vector(const typename OutT<E>::T (&o)[32], const Plan& p, uint8_t* ost,
                                               uint32_t t, const Pred& pr) {
-	constexpr uint32_t RL  = run_len<WS>();
-	constexpr uint32_t RC  = run_count<WS>();
-	uint32_t*          bm  = reinterpret_cast<uint32_t*>(ost);
-	const bool         sgn = p.cmp == OUT_BITMAP_S;
-	__syncwarp(); // the stage was just read into registers
-	bm[t] = 0;
-	__syncwarp();
+	constexpr uint32_t RL = run_len<WS>();
+	constexpr uint32_t RC = run_count<WS>();
+	const PredE<E>     holds(pr, p.cmp == OUT_BITMAP_S);
+	uint32_t*          out  = reinterpret_cast<uint32_t*>(p.out);
+	uint32_t           mine = 0; // bitmap word t
 	if (p.order) {
-		// a run is RL consecutive values of the original order starting at a multiple of 8
+		if constexpr (RL == 32) {
+			// the thread's run is one aligned bitmap word
 #pragma unroll
-		for (uint32_t r = 0; r < RC; ++r) {
-			uint32_t m = 0;
+			for (uint32_t j = 0; j < 32; ++j) { mine |= static_cast<uint32_t>(holds(o[j])) << j; }
+			out[run_start<WS>(t, 0) / 32] = mine;
+			return;
+		} else {
+			// runs of RL (16 or 8) values start at multiples of 8: every bitmap byte belongs to one run
+			__syncwarp(); // the stage was just read into registers
 #pragma unroll
-			for (uint32_t j = 0; j < RL; ++j) { m |= static_cast<uint32_t>(pred_holds<E>(o[r * RL + j], sgn, pr)) << j; }
-			const uint32_t s  = run_start<WS>(t, r);
-			const uint64_t mm = static_cast<uint64_t>(m) << (s & 31u);
-			if (static_cast<uint32_t>(mm)) { atomicOr(bm + s / 32, static_cast<uint32_t>(mm)); }
-			if (mm >> 32) { atomicOr(bm + s / 32 + 1, static_cast<uint32_t>(mm >> 32)); }
+			for (uint32_t r = 0; r < RC; ++r) {
+				uint32_t m = 0;
+#pragma unroll
+				for (uint32_t j = 0; j < RL; ++j) { m |= static_cast<uint32_t>(holds(o[r * RL + j])) << j; }
+				const uint32_t s = run_start<WS>(t, r) / 8;
+#pragma unroll
+				for (uint32_t b = 0; b < RL / 8; ++b) { ost[s + b] = static_cast<uint8_t>(m >> (8 * b)); }
+			}
+			__syncwarp();
+			mine = reinterpret_cast<const uint32_t*>(ost)[t];
+		}
+	} else if constexpr (WS == 32 || WS == 64) {
+		// run position j of every thread lands on bit t of bitmap word run32_val(j)
+#pragma unroll
+		for (uint32_t j = 0; j < 32; ++j) {
+			const uint32_t b = __ballot_sync(0xFFFFFFFFu, holds(o[j]));
+			if (run32_val(j) == t) { mine = b; }
+		}
+	} else if constexpr (WS == 16) {
+		// run position j of the thread's two lanes: bits 2t and 2t + 1 of the 64 at 64 * run16_val(j)
+#pragma unroll
+		for (uint32_t j = 0; j < 16; ++j) {
+			const uint32_t b0 = __ballot_sync(0xFFFFFFFFu, holds(o[j]));
+			const uint32_t b1 = __ballot_sync(0xFFFFFFFFu, holds(o[16 + j]));
+			const uint32_t g  = 2 * run16_val(j);
+			if (t == g) { mine = spread16(b0 & 0xFFFFu) | (spread16(b1 & 0xFFFFu) << 1); }
+			if (t == g + 1) { mine = spread16(b0 >> 16) | (spread16(b1 >> 16) << 1); }
 		}
 	} else {
+		uint32_t* bm = reinterpret_cast<uint32_t*>(ost);
+		__syncwarp();
+		bm[t] = 0;
+		__syncwarp();
 #pragma unroll
 		for (uint32_t r = 0; r < RC; ++r) {
 #pragma unroll
 			for (uint32_t j = 0; j < RL; ++j) {
-				if (pred_holds<E>(o[r * RL + j], sgn, pr)) {
+				if (holds(o[r * RL + j])) {
 					const uint32_t k = run_tpos<WS>(t, r, j);
 					atomicOr(bm + k / 32, 1u << (k & 31u));
 				}
 			}
 		}
+		__syncwarp();
+		mine = bm[t];
 	}
-	__syncwarp();
-	reinterpret_cast<uint32_t*>(p.out)[t] = bm[t];
+	out[t] = mine;
 	__syncwarp();
 }
 

@@ -91,7 +91,7 @@ enum : uint32_t { PRED_EQ = 0, PRED_NE = 1, PRED_LT = 2, PRED_LE = 3, PRED_GT = 
 struct Pred {
 	uint64_t value;
 	uint32_t op;
-	uint32_t pad;
+	uint32_t active; // nonzero: the launch is a filter (KIND_FILTER kernels of the segment's family)
 };
 
 struct DecodeArgs {

@@ -17,7 +17,6 @@ enum class Family : int {
 	NUM_NARROW    = 3, // NUM with every stream and output at most 32 bits
 	GATHER_NARROW = 4, // GATHER with outputs of at most 4 bytes
 	NUM_PATCH     = 5, // NUM items with patches (S / B / LL) applied before rsum
-	FILTER        = 6, // every item kind, writing predicate bitmaps instead of values (filter plans)
 };
 
 // Launch segments of a queue ordered by item class (plain, patched, gather): at most one per class.
@@ -62,8 +61,8 @@ int make_plan_object(const std::vector<ColDesc>& descs, const std::vector<uint32
 
 // Hand device buffers to a plan: freed when the plan is destroyed.
 void plan_adopt(::fls_plan* plan, std::vector<void*>&& buffers);
-// Turn a page plan into a filter plan: one FILTER launch evaluating `pred` (its columns' descriptors carry
-// OUT_BITMAP_* and bitmap outputs).
+// Turn a page plan into a filter plan: its launches evaluate `pred` with the KIND_FILTER form of each segment's
+// kernel family (its columns' descriptors carry OUT_BITMAP_* and bitmap outputs).
 void plan_set_filter(::fls_plan* plan, const Pred& pred);
 
 // Kernels launched by this library inside the last timed region of a caller (a plain counter; not thread-safe).

@@ -5,6 +5,7 @@
     python -m fastlanes_b200.profile_cases delta --values 16777216 --reps 3
     python -m fastlanes_b200.profile_cases mixed --columns 32 --reps 3
     python -m fastlanes_b200.profile_cases select --columns 32 --reps 3
+    python -m fastlanes_b200.profile_cases filter --values 16777216 --reps 3
 
 Each case builds its input, decodes (or selects) once and checks the result, then repeats the call `reps`
 times, and prints one line with the mean time of the repeats (CUDA events; not a benchmark number).
@@ -87,6 +88,29 @@ def case_delta(a):
     return _page_case(W.delta_timestamps(a.values), PG.INT64, 11, a.reps, "delta", a.autotune)
 
 
+def case_filter(a):
+    """Filter plan (predicate pushdown) on the DELTA page of `values` sorted int64 timestamps: x > median."""
+    from . import pages as PG
+    from . import workloads as W
+
+    values = W.delta_timestamps(a.values)
+    page, _ = PG.encode_from_memory(values, PG.INT64, 11)
+    shift = PG.placement(page)
+    buf = torch.zeros(page.size + 64, dtype=torch.uint8, device="cuda")
+    buf[shift:shift + page.size] = torch.from_numpy(page).cuda()
+    c = int(np.median(values))
+    bm = torch.empty(values.size // 8, dtype=torch.uint8, device="cuda")
+    plan = PG.FilterPlan([dict(d_page=buf.data_ptr() + shift, page_size=page.size, data_type=PG.INT64, order=1,
+                               d_out=bm.data_ptr())], PG.PRED_GT, c)
+    plan.decode()
+    want = np.packbits((values > c).astype(np.uint8).reshape(-1, 1024), axis=1, bitorder="little")
+    if not np.array_equal(bm.cpu().numpy().reshape(-1, 128), want):
+        raise SystemExit("filter: mismatch")
+    ms = _timed(plan.decode, a.reps)
+    plan.close()
+    return f"filter values={values.size} page={page.size} ms={ms:.4f}"
+
+
 def _columns(a):
     from . import workloads as W
 
@@ -130,7 +154,8 @@ def case_select(a):
     return res
 
 
-CASES = {"strings": case_strings, "rle": case_rle, "delta": case_delta, "mixed": case_mixed, "select": case_select}
+CASES = {"strings": case_strings, "rle": case_rle, "delta": case_delta, "mixed": case_mixed, "select": case_select,
+         "filter": case_filter}
 
 
 def main(argv=None):

@@ -75,6 +75,14 @@ inline bool __any_sync(unsigned, bool p) {
 	__syncwarp();
 	return r;
 }
+inline unsigned __ballot_sync(unsigned, bool p) {
+	g_emu_warp->vote[g_emu_lane] = p ? 1 : 0;
+	__syncwarp();
+	unsigned r = 0;
+	for (int i = 0; i < 32; ++i) { r |= (g_emu_warp->vote[i] ? 1u : 0u) << i; }
+	__syncwarp();
+	return r;
+}
 inline int atomicOr(int* a, int v) { return __atomic_fetch_or(a, v, __ATOMIC_SEQ_CST); }
 inline unsigned atomicOr(unsigned* a, unsigned v) { return __atomic_fetch_or(a, v, __ATOMIC_SEQ_CST); }
 template <class T>
