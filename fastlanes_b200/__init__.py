@@ -9,5 +9,6 @@ from . import pages  # noqa: F401
 from . import strings  # noqa: F401
 from . import select  # noqa: F401
 from . import workloads  # noqa: F401
+from . import files  # noqa: F401
 
-__all__ = ["pages", "primitives", "select", "strings", "workloads"]
+__all__ = ["files", "pages", "primitives", "select", "strings", "workloads"]

@@ -265,6 +265,31 @@ int fls_gpu_selection_and(const uint16_t* d_idx0, const uint16_t* d_count0, cons
                           fls_stream_t stream);
 
 /* ---------------------------------------------------------------------------------------------------------
+ * Files: the reference's file pair data.fls + footer.json, written by Connection::to_fls (src/connection.cpp:
+ * 102-128) and opened by Connection::read_fls / Reader (src/reader/reader.cpp:19-61), read into device memory.
+ * Footer keys as src/json/fls_json.cpp:30-62 writes them.  The reference stores values only for its
+ * ZERO_COPY columns (n_vec * 1024 raw values at col_ofs); for CONSTANT / EQUAL columns it keeps neither the
+ * constant nor the equal column's index, so they report FLS_FILE_NO_DATA.  Page columns (FLS_FILE_PAGES) are
+ * this library's extension of the same container: a "pages" list of row-group chunks of reference page bytes
+ * ({"ofs", "size", "dict_ofs", "dict_size", "n_vec"}), decoded on the GPU.
+ * ------------------------------------------------------------------------------------------------------- */
+#define FLS_FILE_ZERO_COPY 1
+#define FLS_FILE_PAGES 2
+#define FLS_FILE_NO_DATA 3
+typedef struct fls_file fls_file;
+/* Parses dir/footer.json and checks the column ranges against dir/data.fls (host only, no GPU work). */
+int fls_file_open(const char* dir, fls_file** out_file);
+int fls_file_shape(const fls_file* file, uint32_t* n_cols, uint64_t* n_vec);
+/* data_type: enum data_t of fastlanes.h; kind: FLS_FILE_*; n_values: values a read writes (0 for NO_DATA). */
+int fls_file_column(const fls_file* file, uint32_t col, uint8_t* data_type, uint8_t* kind, uint64_t* n_values);
+/* Reads columns cols[0..n) into d_outs[i] (n_values values each, original order, 16-byte aligned): the file's
+ * bytes stream through two pinned bounce buffers (the read of one overlapping the copy out of the other);
+ * ZERO_COPY columns land directly in their outputs, the chunks of every page column are staged and decoded by
+ * one page decode.  FLS_ERR_UNSUPPORTED for a NO_DATA column.  Synchronous. */
+int fls_file_read(fls_file* file, const uint32_t* cols, uint32_t n, void* const* d_outs, fls_stream_t stream);
+int fls_file_close(fls_file* file);
+
+/* ---------------------------------------------------------------------------------------------------------
  * String columns.  d_page: a string page (DICT: str expressions 2, 3, 8; DICT_RLE: 15, 16; FSST: 13, 14;
  * BYTE_ARR: 0 of src/cor/exp_pool.cpp:66-101); d_dict: its dictionary bytes (DICT / DICT_RLE: the FSST-
  * compressed dictionary page; FSST: the exported symbol table; BYTE_ARR: none).  Creating a plan decodes the

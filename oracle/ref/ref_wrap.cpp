@@ -28,6 +28,7 @@
 #include "fls_gen/unpack/unpack.hpp"
 #include "fls_gen/unrsum/unrsum.hpp"
 #include "fls_gen/untranspose/untranspose.hpp"
+#include "fls/connection.hpp"
 #include "fls/expression/logical_expression.hpp"
 #include "fls/expression/selection_ds.hpp"
 #include "fls/primitive/predicate/equal.hpp"
@@ -306,6 +307,16 @@ int64_t ref_fsst_decompress(const uint8_t* table, uint64_t in_len, const uint8_t
 	fsst_decoder_t d;
 	if (fsst_import(&d, const_cast<unsigned char*>(table)) == 0) { return -1; }
 	return static_cast<int64_t>(fsst_decompress(&d, in_len, const_cast<unsigned char*>(in), cap, out));
+}
+
+/* Connection::read(dir).to_fls(out) (src/connection.cpp:25-56, :102-128): a CSV + schema.json directory to the
+ * reference's file pair data.fls + footer.json.  Returns 0, or -1 when the reference throws. */
+int ref_csv_to_fls(const char* in_dir, const char* out_dir) {
+	try {
+		fastlanes::Connection conn;
+		conn.read(std::filesystem::path(in_dir)).to_fls(std::filesystem::path(out_dir));
+		return 0;
+	} catch (const std::exception&) { return -1; }
 }
 
 /* SelectionDS only keeps a reference to its LogicalExpr, which the predicate primitives never touch; the
