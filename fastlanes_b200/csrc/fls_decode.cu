@@ -656,7 +656,13 @@ __device__ __forceinline__ void decode_vector(const Plan& p, const uint8_t* stag
 	}
 	if (__any_sync(0xFFFFFFFFu, bad) && t == 0) { atomicOr(status, STATUS_BAD_INDEX); }
 	if constexpr ((KIND & KIND_FILTER) != 0) {
-		filter_vector<WS, E>(o, p, ost, t, pr);
+		bool values = false;
+		if constexpr ((KIND & KIND_PATCH) != 0) {
+			// an intermediate stream of a filter plan (a DICT page's patched codes, a patched item)
+			values = p.cmp == OUT_VALUES;
+			if (values) { store_vector<WS, E>(o, p.out, ost, p.order != 0, t); }
+		}
+		if (!values) { filter_vector<WS, E>(o, p, ost, t, pr); }
 	} else {
 		store_vector<WS, E>(o, p.out, ost, p.order != 0, t);
 	}

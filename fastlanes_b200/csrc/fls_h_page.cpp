@@ -27,28 +27,37 @@ const ExprLayout* expr_layout(uint8_t exp_t, uint8_t var) {
 	// exceptions, positions
 	constexpr uint8_t N = kNoBuf;
 	static const ExprLayout table[] = {
-	    {2, 1, 1, 0, ENC_RAW, POST_NONE, N, N, 0, N, N, N, N, N},                     // UNCOMPRESSED
-	    {4, 1, 3, 0, ENC_FFOR, POST_NONE, 0, 1, 2, N, N, N, N, N},                    // FFOR NO_PATCH
-	    {4, 2, 5, 0, ENC_FFOR, POST_PATCH_LL, 2, 3, 4, N, N, N, 0, 1},                // FFOR LL_PATCH
-	    {4, 3, 5, 0, ENC_FFOR, POST_PATCH_S, 2, 3, 4, N, N, N, 0, 1},                 // FFOR S_PATCH
-	    {4, 4, 5, 0, ENC_FFOR, POST_PATCH_B, 2, 3, 4, N, N, N, 0, 1},                 // FFOR B_PATCH
-	    {4, 5, 5, 0, ENC_FFOR, POST_PATCH_S, 2, 3, 4, N, N, 0, 0, 1},                 // FFOR S_PATCH_REC
-	    {5, 1, 4, 0, ENC_DELTA, POST_NONE, 1, 2, 3, 0, N, N, N, N},                   // DELTA NO_PATCH
-	    {5, 2, 6, 0, ENC_DELTA, POST_PATCH_LL, 3, 4, 5, 0, N, N, 1, 2},               // DELTA LL_PATCH
-	    {5, 3, 6, 0, ENC_DELTA, POST_PATCH_S, 3, 4, 5, 0, N, N, 1, 2},                // DELTA S_PATCH
-	    {5, 4, 6, 0, ENC_DELTA, POST_PATCH_B, 3, 4, 5, 0, N, N, 1, 2},                // DELTA B_PATCH
-	    {5, 5, 6, 0, ENC_DELTA, POST_PATCH_B, 3, 4, 5, 0, N, 1, 1, 2},                // DELTA B_PATCH_REC
-	    {6, 1, 2, 16, ENC_RAW, POST_RLE, N, N, 1, N, 0, N, N, N},                     // RLE UNCOMPRESSED
-	    {6, 2, 5, 16, ENC_DELTA, POST_RLE, 2, 3, 4, 1, 0, N, N, N},                   // RLE DELTA_NO_PATCH
-	    {6, 3, 2, 16, ENC_RAW, POST_RLE, N, N, 1, N, 0, 0, N, N},                     // RLE UNCOMPRESSED_REC
-	    {6, 4, 5, 16, ENC_DELTA, POST_RLE, 2, 3, 4, 1, 0, 0, N, N},                   // RLE DELTA_NO_PATCH_REC
-	    {8, 1, 1, 32, ENC_RAW, POST_DICT, N, N, 0, N, N, N, N, N},                    // DICT UNCOMPRESSED
-	    {8, 2, 3, 32, ENC_FFOR, POST_DICT, 0, 1, 2, N, N, N, N, N},                   // DICT FFOR_NO_PATCH
-	    {8, 7, 4, 32, ENC_DELTA, POST_DICT, 1, 2, 3, 0, N, N, N, N},                  // DICT DELTA_NO_PATCH
-	    {11, 1, 2, 16, ENC_RAW, POST_RLE_DICT, N, N, 1, N, 0, N, N, N},               // DICT_RLE UNCOMPRESSED
-	    {11, 2, 5, 16, ENC_DELTA, POST_RLE_DICT, 2, 3, 4, 1, 0, N, N, N},             // DICT_RLE DELTA_NO_PATCH
-	    {11, 3, 2, 16, ENC_RAW, POST_RLE_DICT, N, N, 1, N, 0, 0, N, N},               // DICT_RLE UNCOMPRESSED_REC
-	    {11, 4, 5, 16, ENC_DELTA, POST_RLE_DICT, 2, 3, 4, 1, 0, 0, N, N},             // DICT_RLE ..._REC
+	    {2, 1, 1, 0, ENC_RAW, POST_NONE, N, N, 0, N, N, N, N, N, 0},                     // UNCOMPRESSED
+	    {4, 1, 3, 0, ENC_FFOR, POST_NONE, 0, 1, 2, N, N, N, N, N, 0},                    // FFOR NO_PATCH
+	    {4, 2, 5, 0, ENC_FFOR, POST_PATCH_LL, 2, 3, 4, N, N, N, 0, 1, 0},                // FFOR LL_PATCH
+	    {4, 3, 5, 0, ENC_FFOR, POST_PATCH_S, 2, 3, 4, N, N, N, 0, 1, 0},                 // FFOR S_PATCH
+	    {4, 4, 5, 0, ENC_FFOR, POST_PATCH_B, 2, 3, 4, N, N, N, 0, 1, 0},                 // FFOR B_PATCH
+	    {4, 5, 5, 0, ENC_FFOR, POST_PATCH_S, 2, 3, 4, N, N, 0, 0, 1, 0},                 // FFOR S_PATCH_REC
+	    {5, 1, 4, 0, ENC_DELTA, POST_NONE, 1, 2, 3, 0, N, N, N, N, 0},                   // DELTA NO_PATCH
+	    {5, 2, 6, 0, ENC_DELTA, POST_PATCH_LL, 3, 4, 5, 0, N, N, 1, 2, 0},               // DELTA LL_PATCH
+	    {5, 3, 6, 0, ENC_DELTA, POST_PATCH_S, 3, 4, 5, 0, N, N, 1, 2, 0},                // DELTA S_PATCH
+	    {5, 4, 6, 0, ENC_DELTA, POST_PATCH_B, 3, 4, 5, 0, N, N, 1, 2, 0},                // DELTA B_PATCH
+	    {5, 5, 6, 0, ENC_DELTA, POST_PATCH_B, 3, 4, 5, 0, N, 1, 1, 2, 0},                // DELTA B_PATCH_REC
+	    {6, 1, 2, 16, ENC_RAW, POST_RLE, N, N, 1, N, 0, N, N, N, 0},                     // RLE UNCOMPRESSED
+	    {6, 2, 5, 16, ENC_DELTA, POST_RLE, 2, 3, 4, 1, 0, N, N, N, 0},                   // RLE DELTA_NO_PATCH
+	    {6, 3, 2, 16, ENC_RAW, POST_RLE, N, N, 1, N, 0, 0, N, N, 0},                     // RLE UNCOMPRESSED_REC
+	    {6, 4, 5, 16, ENC_DELTA, POST_RLE, 2, 3, 4, 1, 0, 0, N, N, 0},                   // RLE DELTA_NO_PATCH_REC
+	    {8, 1, 1, 32, ENC_RAW, POST_DICT, N, N, 0, N, N, N, N, N, 0},                    // DICT UNCOMPRESSED
+	    {8, 2, 3, 32, ENC_FFOR, POST_DICT, 0, 1, 2, N, N, N, N, N, 0},                   // DICT FFOR_NO_PATCH
+	    {8, 7, 4, 32, ENC_DELTA, POST_DICT, 1, 2, 3, 0, N, N, N, N, 0},                  // DICT DELTA_NO_PATCH
+	    // DICT with patched codes (dict_exp.hpp:31-41): the code stream laid out as the patched FFOR / DELTA pages
+	    {8, 3, 5, 32, ENC_FFOR, POST_PATCH_LL, 2, 3, 4, N, N, N, 0, 1, 1},            // DICT FFOR_LL_PATCH
+	    {8, 4, 5, 32, ENC_FFOR, POST_PATCH_S, 2, 3, 4, N, N, N, 0, 1, 1},             // DICT FFOR_S_PATCH
+	    {8, 5, 5, 32, ENC_FFOR, POST_PATCH_B, 2, 3, 4, N, N, N, 0, 1, 1},             // DICT FFOR_B_PATCH
+	    {8, 6, 5, 32, ENC_FFOR, POST_PATCH_S, 2, 3, 4, N, N, 0, 0, 1, 1},             // DICT FFOR_S_PATCH_REC
+	    {8, 8, 6, 32, ENC_DELTA, POST_PATCH_LL, 3, 4, 5, 0, N, N, 1, 2, 1},           // DICT DELTA_LL_PATCH
+	    {8, 9, 6, 32, ENC_DELTA, POST_PATCH_S, 3, 4, 5, 0, N, N, 1, 2, 1},            // DICT DELTA_S_PATCH
+	    {8, 10, 6, 32, ENC_DELTA, POST_PATCH_B, 3, 4, 5, 0, N, N, 1, 2, 1},           // DICT DELTA_B_PATCH
+	    {8, 11, 6, 32, ENC_DELTA, POST_PATCH_B, 3, 4, 5, 0, N, 1, 1, 2, 1},           // DICT DELTA_B_PATCH_REC
+	    {11, 1, 2, 16, ENC_RAW, POST_RLE_DICT, N, N, 1, N, 0, N, N, N, 0},               // DICT_RLE UNCOMPRESSED
+	    {11, 2, 5, 16, ENC_DELTA, POST_RLE_DICT, 2, 3, 4, 1, 0, N, N, N, 0},             // DICT_RLE DELTA_NO_PATCH
+	    {11, 3, 2, 16, ENC_RAW, POST_RLE_DICT, N, N, 1, N, 0, 0, N, N, 0},               // DICT_RLE UNCOMPRESSED_REC
+	    {11, 4, 5, 16, ENC_DELTA, POST_RLE_DICT, 2, 3, 4, 1, 0, 0, N, N, 0},             // DICT_RLE ..._REC
 	};
 	for (const auto& e : table) {
 		if (e.exp_t == exp_t && e.var == var) { return &e; }
@@ -197,7 +206,7 @@ constexpr uint32_t kPageShift = 16;
 // Element bytes of a layout's rec-compressed buffer: run codes are idx_t = uint32, run values and exceptions
 // the column's values.
 static uint32_t rec_elem_bytes(const ExprLayout* L, int value_width) {
-	return L->post == POST_RLE_DICT ? 4u : static_cast<uint32_t>(value_width / 8);
+	return (L->post == POST_RLE_DICT || L->dict_codes) ? 4u : static_cast<uint32_t>(value_width / 8);
 }
 
 // Rec buffer at d_src (device, size bytes) decoded into a new device buffer, appended to *owned.
@@ -212,11 +221,17 @@ static int decode_rec_on(const uint8_t* d_src, uint64_t size, uint32_t eb, std::
 	return rc;
 }
 
+// col_desc (optional) receives, per column, the index of the descriptor that writes the column's output.  A
+// DICT page with patched codes takes two descriptors: its patched code stream decoded into a buffer of the
+// plan (in `owned`; a patched item, so it runs in an earlier launch segment than the gathers), then a raw
+// 32-bit stream of those codes gathered from the dictionary.
 static int describe_pages(const fls_page_column* cols, uint32_t n_cols, std::vector<ColDesc>* descs,
                           std::vector<uint32_t>* queue, Family* fam_out, cudaStream_t stream,
-                          std::vector<void*>* owned) {
+                          std::vector<void*>* owned, std::vector<uint32_t>* col_desc = nullptr) {
 	if (!cols || n_cols == 0 || n_cols > 65535) { return FLS_ERR_ARG; }
-	descs->assign(n_cols, ColDesc {});
+	descs->clear();
+	descs->reserve(n_cols);
+	if (col_desc) { col_desc->assign(n_cols, 0); }
 	queue->clear();
 	Family fam   = Family::NUM;
 	bool   any64 = false;
@@ -234,7 +249,7 @@ static int describe_pages(const fls_page_column* cols, uint32_t n_cols, std::vec
 		if (rc != FLS_OK) { return rc; }
 		const uint8_t* dvals   = nullptr;
 		uint32_t       entries = 0;
-		if (pi.layout->post == POST_DICT || pi.layout->post == POST_RLE_DICT) {
+		if (pi.layout->post == POST_DICT || pi.layout->post == POST_RLE_DICT || pi.layout->dict_codes) {
 			if (!pc.d_dict || pc.dict_size < 20) { return FLS_ERR_FORMAT; }
 			uint8_t dh[20];
 			if (read_on(dh, pc.d_dict, 20, stream) != FLS_OK) { return FLS_ERR_CUDA; }
@@ -261,12 +276,52 @@ static int describe_pages(const fls_page_column* cols, uint32_t n_cols, std::vec
 			                   stream);
 			if (rc != FLS_OK) { return rc; }
 		}
-		rc = build_page_column(pi, pc.d_page, w, dvals, entries, pc.order, static_cast<uint8_t*>(pc.d_out),
-		                       &(*descs)[i], rvals, rsize);
+		if (descs->size() + (pi.layout->dict_codes ? 2 : 1) > 65535) { return FLS_ERR_ARG; }
+		if (pi.layout->dict_codes) {
+			if (entries == 0 || !dvals) { return FLS_ERR_FORMAT; }
+			uint8_t* codes = nullptr;
+			if (pi.vec_c &&
+			    cudaMallocAsync(reinterpret_cast<void**>(&codes), static_cast<uint64_t>(pi.vec_c) * 1024 * 4, stream) !=
+			        cudaSuccess) {
+				return FLS_ERR_CUDA;
+			}
+			if (codes) { owned->push_back(codes); }
+			ColDesc a {};
+			rc = build_page_column(pi, pc.d_page, 32, nullptr, 0, FLS_TRANSPOSED, codes, &a, rvals, rsize);
+			if (rc != FLS_OK) { return rc; }
+			ColDesc g {};
+			g.ws       = 32;
+			g.e        = static_cast<uint8_t>(w / 8);
+			g.enc      = ENC_RAW;
+			g.post     = POST_DICT;
+			g.order    = pc.order;
+			g.layout   = LAYOUT_ARRAYS;
+			g.n_vec    = pi.vec_c;
+			g.bw_const = 32;
+			g.packed   = codes;
+			g.dict     = dvals;
+			g.entry_c  = entries;
+			g.out      = static_cast<uint8_t*>(pc.d_out);
+			const uint32_t ia = static_cast<uint32_t>(descs->size());
+			descs->push_back(a);
+			descs->push_back(g);
+			for (uint32_t v = 0; v < pi.vec_c; ++v) { queue->push_back((ia << kPageShift) | v); }
+			for (uint32_t v = 0; v < pi.vec_c; ++v) { queue->push_back(((ia + 1) << kPageShift) | v); }
+			if (col_desc) { (*col_desc)[i] = ia + 1; }
+			fam = Family::GATHER;
+			if (g.e == 8) { any64 = true; }
+			continue;
+		}
+		ColDesc d {};
+		rc = build_page_column(pi, pc.d_page, w, dvals, entries, pc.order, static_cast<uint8_t*>(pc.d_out), &d, rvals,
+		                       rsize);
 		if (rc != FLS_OK) { return rc; }
-		if (post_is_gather((*descs)[i].post)) { fam = Family::GATHER; }
-		if ((*descs)[i].ws == 64) { any64 = true; }
-		for (uint32_t v = 0; v < pi.vec_c; ++v) { queue->push_back((i << kPageShift) | v); }
+		if (post_is_gather(d.post)) { fam = Family::GATHER; }
+		if (d.ws == 64) { any64 = true; }
+		const uint32_t id = static_cast<uint32_t>(descs->size());
+		descs->push_back(d);
+		for (uint32_t v = 0; v < pi.vec_c; ++v) { queue->push_back((id << kPageShift) | v); }
+		if (col_desc) { (*col_desc)[i] = id; }
 	}
 	// group the work items by kernel specialisation so that warps run long stretches of one code path (the
 	// outputs do not depend on the order)
@@ -277,7 +332,7 @@ static int describe_pages(const fls_page_column* cols, uint32_t n_cols, std::vec
 		return (klass << 30) | (static_cast<uint32_t>(c.ws) << 23) | (c.e << 16) |
 		       (c.enc << 8) | (c.post << 4) | c.order;
 	};
-	if (n_cols > 1) {
+	if (descs->size() > 1) {
 		std::stable_sort(queue->begin(), queue->end(), [&](uint32_t x, uint32_t y) { return key(x) < key(y); });
 	}
 	if (fam == Family::GATHER && any64) { fam = Family::ANY; }
@@ -305,16 +360,16 @@ int fls_gpu_decode_pages(const fls_page_column* cols, uint32_t n_cols, fls_strea
 	a.col_shift = kPageShift;
 	Segments sg; // the queue is class-ordered above; an unordered one would run on the catch-all kernel
 	plan_segments(descs, queue, kPageShift, &sg);
-	if (n_cols == 1) {
+	if (descs.size() == 1) {
 		a.col0    = descs[0];
 		a.n_items = queue.size();
 		return launch_decode(sg.fam[0], a, s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
 	}
 	ColDesc*  d_cols  = nullptr;
 	uint32_t* d_queue = nullptr;
-	if (cudaMallocAsync(&d_cols, sizeof(ColDesc) * n_cols, s) != cudaSuccess) { return FLS_ERR_CUDA; }
+	if (cudaMallocAsync(&d_cols, sizeof(ColDesc) * descs.size(), s) != cudaSuccess) { return FLS_ERR_CUDA; }
 	if (cudaMallocAsync(&d_queue, sizeof(uint32_t) * queue.size(), s) != cudaSuccess) { return FLS_ERR_CUDA; }
-	cudaMemcpyAsync(d_cols, descs.data(), sizeof(ColDesc) * n_cols, cudaMemcpyHostToDevice, s);
+	cudaMemcpyAsync(d_cols, descs.data(), sizeof(ColDesc) * descs.size(), cudaMemcpyHostToDevice, s);
 	cudaMemcpyAsync(d_queue, queue.data(), sizeof(uint32_t) * queue.size(), cudaMemcpyHostToDevice, s);
 	a.cols = d_cols;
 	// copies from pageable host memory are staged before cudaMemcpyAsync returns, so descs/queue may go away
@@ -340,11 +395,15 @@ int fls_plan_create_filter(const fls_page_column* cols, uint32_t n_cols, const f
 	std::vector<uint32_t> queue;
 	Family                fam = Family::NUM;
 	std::vector<void*>    owned;
-	int                   rc = describe_pages(cols, n_cols, &descs, &queue, &fam, nullptr, &owned);
+	std::vector<uint32_t> col_desc;
+	int                   rc = describe_pages(cols, n_cols, &descs, &queue, &fam, nullptr, &owned, &col_desc);
 	if (rc == FLS_OK) {
+		// the descriptor that writes each column's output evaluates the predicate (a DICT page's patched code
+		// stream, decoded first, still writes its codes)
 		for (uint32_t i = 0; i < n_cols; ++i) {
 			const uint8_t t = cols[i].data_type;
-			descs[i].out_mode = (t == INT8 || t == INT16 || t == INT32 || t == INT64) ? OUT_BITMAP_S : OUT_BITMAP_U;
+			descs[col_desc[i]].out_mode =
+			    (t == INT8 || t == INT16 || t == INT32 || t == INT64) ? OUT_BITMAP_S : OUT_BITMAP_U;
 		}
 		rc = make_plan_object(descs, queue, fam, kPageShift, out_plan);
 	}

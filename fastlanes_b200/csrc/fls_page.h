@@ -13,6 +13,7 @@ struct ExprLayout {
 	uint8_t ib_bw, ib_base, ib_packed, ib_lane, ib_vals;
 	uint8_t ib_rec;          // the rec-compressed buffer of the ..._REC variants (kNoBuf: none)
 	uint8_t ib_exc, ib_side; // patched variants: exception values, positions / bitmap / chain head
+	uint8_t dict_codes;      // 1: the patched stream is u32 dictionary codes, gathered from the dictionary after
 };
 
 struct PageInfo {

@@ -37,6 +37,14 @@ ARR_C = {
     (8, 1): 1,  # DICT UNCOMPRESSED: u32 codes
     (8, 2): 3,  # DICT FFOR_NO_PATCH
     (8, 7): 4,  # DICT DELTA_NO_PATCH
+    (8, 3): 5,  # DICT FFOR_LL_PATCH: u32 codes as FFOR LL_PATCH (dict_exp.hpp:62-75)
+    (8, 4): 5,  # DICT FFOR_S_PATCH
+    (8, 5): 5,  # DICT FFOR_B_PATCH
+    (8, 6): 5,  # DICT FFOR_S_PATCH_REC
+    (8, 8): 6,  # DICT DELTA_LL_PATCH: u32 codes as DELTA LL_PATCH
+    (8, 9): 6,  # DICT DELTA_S_PATCH
+    (8, 10): 6,  # DICT DELTA_B_PATCH
+    (8, 11): 6,  # DICT DELTA_B_PATCH_REC
     (11, 1): 2,  # DICT_RLE UNCOMPRESSED: u32 code runs, u16 index
     (11, 2): 5,  # DICT_RLE DELTA_NO_PATCH
     (11, 3): 2,  # DICT_RLE UNCOMPRESSED_REC
@@ -128,6 +136,11 @@ def _stream(pg, v, first, ws, enc, T):
 # (exp_t, var) of the patched FFOR / DELTA variants -> patch kind, exceptions rec-compressed
 PATCHED = {(4, 2): ("ll", False), (4, 3): ("s", False), (4, 4): ("b", False), (4, 5): ("s", True),
            (5, 2): ("ll", False), (5, 3): ("s", False), (5, 4): ("b", False), (5, 5): ("b", True)}
+# DICT with patched u32 codes (dict_exp.hpp:31-41, FFOR_* and DELTA_* variants) -> patch kind, rec exceptions,
+# delta-coded
+DICT_PATCHED = {(8, 3): ("ll", False, False), (8, 4): ("s", False, False), (8, 5): ("b", False, False),
+                (8, 6): ("s", True, False), (8, 8): ("ll", False, True), (8, 9): ("s", False, True),
+                (8, 10): ("b", False, True), (8, 11): ("b", True, True)}
 
 
 def _patch(vals, kind, exc_bytes, side, base, T):
@@ -156,10 +169,13 @@ def _patch(vals, kind, exc_bytes, side, base, T):
     return vals
 
 
-def _patched_stream(pg, v, T, rec_exc):
-    """Unpacked, patched and (DELTA) rsum-ed values of vector v of a patched FFOR / DELTA page (transposed)."""
-    kind, _ = PATCHED[(pg.exp_t, pg.var)]
-    first = 1 if pg.exp_t == 5 else 0
+def _patched_stream(pg, v, T, rec_exc, kind=None, delta=None):
+    """Unpacked, patched and (DELTA) rsum-ed values of vector v of a patched FFOR / DELTA page (transposed);
+    kind / delta given for the DICT pages' patched code streams."""
+    if kind is None:
+        kind, _ = PATCHED[(pg.exp_t, pg.var)]
+        delta = pg.exp_t == 5
+    first = 1 if delta else 0
     ws = np.dtype(T).itemsize * 8
     bw = int(pg.vector_slice(v, first + 2, 1)[0])
     base = _le(pg.vector_slice(v, first + 3, ws // 8), T)[0]
@@ -170,7 +186,7 @@ def _patched_stream(pg, v, T, rec_exc):
     else:
         exc = pg.vector_slice(v, first)
     vals = _patch(vals, kind, exc, pg.vector_slice(v, first + 1), base, T)
-    if pg.exp_t == 5:
+    if delta:
         vals = oracle.rsum(vals, _le(pg.vector_slice(v, 0, 128), T).copy())
     return vals
 
@@ -195,6 +211,9 @@ def decode_int(page, dict_bytes=None, value_dtype=np.uint64):
     if (et, var) in PATCHED and PATCHED[(et, var)][1]:
         b = 1 if et == 5 else 0
         rec_exc = rec_buffer(pg.b[pg.off[b]:pg.off[b] + pg.buf_size[b]], np.uint64 if W == 64 else np.uint32)[0]
+    if (et, var) in DICT_PATCHED and DICT_PATCHED[(et, var)][1]:
+        b = 1 if DICT_PATCHED[(et, var)][2] else 0
+        rec_exc = rec_buffer(pg.b[pg.off[b]:pg.off[b] + pg.buf_size[b]], np.uint32)[0]  # the codes' type
     for v in range(pg.vec_c):
         if (et, var) in PATCHED:
             tr = _patched_stream(pg, v, VT, rec_exc)
@@ -216,6 +235,10 @@ def decode_int(page, dict_bytes=None, value_dtype=np.uint64):
             tr = vals[idx.astype(np.int64)]
             if et == 11:
                 tr = dic[tr.astype(np.int64)]
+        elif (et, var) in DICT_PATCHED:
+            kind, _, delta = DICT_PATCHED[(et, var)]
+            codes = _patched_stream(pg, v, np.uint32, rec_exc, kind, delta)
+            tr = dic[codes.astype(np.int64)]
         elif et == 8:
             enc = {1: "raw", 2: "ffor", 7: "delta"}[var]
             codes = _stream(pg, v, 0, 32, enc, np.uint32)

@@ -41,6 +41,10 @@ I64_IDS = [0, 1, 6, 7, 11, 16, 17, 22, 27]
 REC_IDS = [8, 9, 16, 17, 22, 27]
 # Patched FFOR / DELTA (src/cor/prm/patch/*) on columns with ~3% outliers / outlying gaps.
 PATCH_IDS = [2, 3, 4, 5, 12, 13, 14, 15]
+# DICT with patched FFOR / DELTA codes (dict_exp.hpp FFOR_*_PATCH, DELTA_*_PATCH): ~97 % of the rows take one of
+# 16 values, the rest ~2000 rare ones, so the rare values' codes (assigned in first-occurrence order) are the
+# patches' exceptions.
+DPATCH_IDS = [18, 19, 20, 21, 22, 23, 24, 25, 26]
 STR_IDS = [0, 2, 3, 8, 13, 14, 15, 16]
 
 
@@ -142,6 +146,15 @@ def patch_column(eid, rng, n):
     return (1_600_000_000_000_000_000 + np.cumsum(gaps)).astype(np.int64)
 
 
+def dpatch_column(eid, rng, n):
+    common = rng.integers(-(1 << 40), 1 << 40, 16)
+    rare = rng.integers(-(1 << 40), 1 << 40, 4000)
+    x = common[rng.integers(0, 16, n)]
+    out = rng.random(n) < 0.03
+    x[out] = rare[rng.integers(0, rare.size, out.sum())]
+    return x.astype(np.int64)
+
+
 def str_column(eid, rng, n):
     alphabet = np.frombuffer(b"abcdefghijklmnopqrstuvwxyzABCDEFGHIJKLMNOPQRSTUVWXYZ0123456789-_", np.uint8)
     tokens = [bytes(alphabet[rng.integers(0, 64, rng.integers(2, 7))]) for _ in range(64)]
@@ -203,6 +216,18 @@ def columns(ref):
         assert rc == 0, (eid, rc)
         res[f"i64patch_{eid}_input"] = col
         res[f"i64patch_{eid}_page"] = page[: ps.value].copy()
+    for eid in DPATCH_IDS:
+        rng = np.random.default_rng(5000 + eid)
+        m = 4 * 1024
+        col = dpatch_column(eid, rng, m)
+        page, dic = np.zeros(cap, np.uint8), np.zeros(cap, np.uint8)
+        ps, ds = ctypes.c_uint64(), ctypes.c_uint64()
+        rc = ref.ref_encode_i64(ptr(col), ctypes.c_uint64(m), ctypes.c_uint8(eid), 1, ptr(page), ctypes.c_uint64(cap),
+                                ctypes.byref(ps), ptr(dic), ctypes.c_uint64(cap), ctypes.byref(ds))
+        assert rc == 0, (eid, rc)
+        res[f"i64dpatch_{eid}_input"] = col
+        res[f"i64dpatch_{eid}_page"] = page[: ps.value].copy()
+        res[f"i64dpatch_{eid}_dict"] = dic[: ds.value].copy()
     for eid in STR_IDS:
         rng = np.random.default_rng(2000 + eid)
         byts, offs = str_column(eid, rng, n)

@@ -11,7 +11,7 @@ from oracle import predicate as PR
 pytestmark = pytest.mark.gpu
 
 KEYS = [f"i64_{e}" for e in (0, 1, 6, 7, 11, 16, 17, 22, 27)] + [f"i64patch_{e}" for e in (2, 3, 4, 5, 12, 13, 14, 15)] \
-    + [f"i64rec_{e}" for e in (8, 9, 16, 17, 22, 27)]
+    + [f"i64rec_{e}" for e in (8, 9, 16, 17, 22, 27)] + [f"i64dpatch_{e}" for e in (18, 20, 21, 23, 26)]
 
 
 def _dev_bytes(a, dev, shift=0):

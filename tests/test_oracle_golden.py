@@ -134,3 +134,13 @@ def test_page_oracle_decodes_reference_patched_pages(col_golden, eid):
     page = col_golden[f"i64patch_{eid}_page"]
     got = pages.decode_int(page, None, np.uint64).view(np.int64)
     assert np.array_equal(got, col_golden[f"i64patch_{eid}_input"])
+
+
+@pytest.mark.parametrize("eid", [18, 19, 20, 21, 22, 23, 24, 25, 26])
+def test_page_oracle_decodes_reference_patched_dict_pages(col_golden, eid):
+    """DICT pages whose u32 codes are patched FFOR / DELTA streams (pool ids 18-26), then gathered."""
+    from oracle import pages
+
+    page, dic = col_golden[f"i64dpatch_{eid}_page"], col_golden[f"i64dpatch_{eid}_dict"]
+    got = pages.decode_int(page, dic, np.uint64).view(np.int64)
+    assert np.array_equal(got, col_golden[f"i64dpatch_{eid}_input"])

@@ -272,3 +272,54 @@ def test_reference_patched_pages(cuda, col_golden, eid, shift):
         assert np.array_equal(got, want), order
         plan.close()
     assert np.array_equal(pages.decode_to_memory(page, pages.INT64), want)
+
+
+@pytest.mark.parametrize("eid", [18, 19, 20, 21, 23, 24, 25, 26])
+@pytest.mark.parametrize("shift", [0, 7])
+def test_reference_patched_dict_pages(cuda, col_golden, eid, shift):
+    """DICT pages of the reference whose u32 codes are patched FFOR / DELTA streams (pool ids 18-26): the
+    patched codes decode into a plan-owned buffer, then a gather launch reads the dictionary; one-shot, through
+    a page plan in both orders, and next to other pages in one plan."""
+    import torch
+
+    from fastlanes_b200 import pages
+    from fastlanes_b200 import primitives as P
+
+    page, dic, want = (col_golden[f"i64dpatch_{eid}_{k}"] for k in ("page", "dict", "input"))
+    pbuf, pptr = _dev_bytes(page, cuda, shift)
+    dbuf, dptr = _dev_bytes(dic, cuda, 3)
+    col = dict(d_page=pptr, page_size=page.size, d_dict=dptr, dict_size=dic.size, data_type=pages.INT64)
+    out = torch.zeros(want.size, dtype=torch.int64, device=cuda)
+    pages.decode_pages([dict(col, order=1, d_out=out.data_ptr())])
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), want)
+    for order in (0, 1):
+        out.zero_()
+        plan = pages.PagePlan([dict(col, order=order, d_out=out.data_ptr())])
+        plan.decode()
+        plan.decode()  # replays reuse the plan's code buffer
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        if order == 0:
+            got = np.concatenate([oracle.untranspose_i(got[v * 1024:(v + 1) * 1024].view(np.uint64).copy())
+                                  for v in range(want.size // 1024)]).view(np.int64)
+        assert np.array_equal(got, want), order
+        plan.close()
+    # with a plain and an RLE page in the same plan
+    other = [col_golden["i64_1_page"], col_golden["i64_6_page"]]
+    keep, cols, outs = [], [dict(col, order=1, d_out=out.data_ptr())], [out]
+    for pg in other:
+        b, p = _dev_bytes(pg, cuda, 5)
+        o = torch.zeros(3 * 1024, dtype=torch.int64, device=cuda)
+        keep.append(b)
+        outs.append(o)
+        cols.append(dict(d_page=p, page_size=pg.size, data_type=pages.INT64, order=1, d_out=o.data_ptr()))
+    out.zero_()
+    plan = pages.PagePlan(cols)
+    plan.decode_graph()
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), want)
+    assert np.array_equal(outs[1].cpu().numpy(), col_golden["i64_1_input"])
+    assert np.array_equal(outs[2].cpu().numpy(), col_golden["i64_6_input"])
+    plan.close()
+    assert P.device_status() == 0
