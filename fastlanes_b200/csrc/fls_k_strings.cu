@@ -97,25 +97,26 @@ __device__ __forceinline__ const uint8_t* vector_bytes(const ColDesc& c, uint32_
 	return *n ? c.buf[0] + o : c.buf[0];
 }
 
-// OR the n bytes at src into the window at byte offset d, whose bytes there are zero.  Window words wholly
-// inside the row are plain stores; the first and last (shared with the neighbouring rows, which other lanes
-// may be writing at the same time) are atomic ORs of the row's bytes.  Only the aligned source words that hold
-// bytes of [src, src + n) are read.
-__device__ __forceinline__ void or_row(uint32_t* __restrict__ win, uint32_t d, const uint8_t* __restrict__ src,
-                                       uint32_t n) {
+// OR the n bytes at byte offset `start` of the 4-byte aligned word array `base` into the window at byte offset
+// d, whose bytes there are zero.  Window words wholly inside the row are plain stores; the first and last
+// (shared with the neighbouring rows, which other lanes may be writing at the same time) are atomic ORs of the
+// row's bytes.  Only the source words that hold bytes of the row are read.
+__device__ __forceinline__ void or_row(uint32_t* __restrict__ win, uint32_t d, const uint32_t* __restrict__ base,
+                                       uint32_t start, uint32_t n) {
+	// the row is bytes [start, start + n) of the word array `base`; word indices (not pointers) keep the array's
+	// address space (shared memory for a dictionary held there)
 	if (n == 0) { return; }
-	const uintptr_t sa   = reinterpret_cast<uintptr_t>(src);
-	const uintptr_t a    = sa - (d & 3u); // source address of the byte that lands on window byte 4 * (d / 4)
-	const uint32_t  sh   = 8u * static_cast<uint32_t>(a & 3u);
-	const uint32_t* s    = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
-	const uint32_t* s_lo = reinterpret_cast<const uint32_t*>(sa & ~uintptr_t(3));
-	const uint32_t* s_hi = reinterpret_cast<const uint32_t*>((sa + n - 1) & ~uintptr_t(3));
-	const uint32_t  k0 = d >> 2, k1 = (d + n - 1) >> 2;
-	const uint32_t  hm = 0xFFFFFFFFu << (8u * (d & 3u));
-	const uint32_t  tm = 0xFFFFFFFFu >> (8u * (3u - ((d + n - 1) & 3u)));
+	const int32_t  a    = static_cast<int32_t>(start) - static_cast<int32_t>(d & 3u); // lands on window byte 4*(d/4)
+	const uint32_t sh   = 8u * (static_cast<uint32_t>(a) & 3u);
+	const int32_t  s    = a >> 2;
+	const int32_t  s_lo = static_cast<int32_t>(start >> 2);
+	const int32_t  s_hi = static_cast<int32_t>((start + n - 1) >> 2);
+	const uint32_t k0 = d >> 2, k1 = (d + n - 1) >> 2;
+	const uint32_t hm = 0xFFFFFFFFu << (8u * (d & 3u));
+	const uint32_t tm = 0xFFFFFFFFu >> (8u * (3u - ((d + n - 1) & 3u)));
 	// a clamped word only feeds bytes outside the row, which the masks drop
-	uint32_t w0 = *(s < s_lo ? s_lo : s);
-	uint32_t w1 = *(s + 1 > s_hi ? s_hi : s + 1);
+	uint32_t w0 = base[s < s_lo ? s_lo : s];
+	uint32_t w1 = base[s + 1 > s_hi ? s_hi : s + 1];
 	if (k0 == k1) {
 		atomicOr(win + k0, __funnelshift_r(w0, w1, sh) & hm & tm);
 		return;
@@ -125,12 +126,13 @@ __device__ __forceinline__ void or_row(uint32_t* __restrict__ win, uint32_t d, c
 	uint32_t       j = 1;
 #pragma unroll 4
 	for (; j < m; ++j) {
-		w0              = w1;
-		w1              = s[j + 1];
-		win[k0 + j]     = __funnelshift_r(w0, w1, sh);
+		w0          = w1;
+		w1          = base[s + static_cast<int32_t>(j) + 1];
+		win[k0 + j] = __funnelshift_r(w0, w1, sh);
 	}
-	w0 = w1;
-	w1 = *(s + m + 1 > s_hi ? s_hi : s + m + 1);
+	w0                = w1;
+	const int32_t lst = s + static_cast<int32_t>(m) + 1;
+	w1                = base[lst > s_hi ? s_hi : lst];
 	atomicOr(win + k1, __funnelshift_r(w0, w1, sh) & tm);
 }
 
@@ -415,8 +417,16 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 				if (fill + T > kStrWindow) { flush(false); }
 				if (fill + T <= kStrWindow) {
 					if constexpr (kOr) {
-						or_row(reinterpret_cast<uint32_t*>(win), fill + (o - vpos),
-						       KIND == STR_DICT ? dict + f.start : vb + f.start, f.len);
+						if constexpr (KIND == STR_DICT) {
+							// the decoded dictionary starts 16-byte aligned (shared or global memory)
+							or_row(reinterpret_cast<uint32_t*>(win), fill + (o - vpos),
+							       reinterpret_cast<const uint32_t*>(dict), f.start, f.len);
+						} else {
+							const uintptr_t va = reinterpret_cast<uintptr_t>(vb);
+							or_row(reinterpret_cast<uint32_t*>(win), fill + (o - vpos),
+							       reinterpret_cast<const uint32_t*>(va & ~uintptr_t(3)),
+							       f.start + static_cast<uint32_t>(va & 3u), f.len);
+						}
 					} else {
 						fsst_decode_to(fsym, flen, vb + f.start, f.clen, win + fill + (o - vpos));
 					}
