@@ -196,6 +196,17 @@ __device__ __forceinline__ void extract_w64(const uint32_t* __restrict__ S, uint
 // W = 16: v[16*q + p] is run position p of lane 2t+q.
 __device__ __forceinline__ void extract_w16(const uint32_t* __restrict__ S, uint32_t t, uint32_t bw,
                                             uint32_t (&v)[32]) {
+	if (bw <= 1) {
+		// every value of the thread's two lanes is one bit of its first packed word (RLE run-index deltas
+		// are 0 or 1, so every RLE and DICT_RLE vector takes this path)
+		const uint32_t lo = bw ? S[t] : 0u;
+#pragma unroll
+		for (uint32_t j = 0; j < 16; ++j) {
+			v[run16_pos(j)]      = (lo >> j) & 1u;
+			v[16 + run16_pos(j)] = (lo >> (16 + j)) & 1u;
+		}
+		return;
+	}
 	const uint32_t mask = bw >= 16 ? 0xFFFFu : ((1u << bw) - 1u);
 #pragma unroll
 	for (uint32_t j = 0; j < 16; ++j) {
