@@ -299,8 +299,23 @@ int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_
 		d_rec.p           = rb;
 		if (rc != FLS_OK) { return rc; }
 	}
+	// REC2: the u16 rsum bases are a second rec buffer
+	const int rec2_b = pi.layout->ib_rec2 != kNoBuf ? pi.layout->ib_rec2 : -1;
+	DevBuf    d_rec2(hp->in);
+	uint64_t  rec2_n = 0;
+	if (rec2_b >= 0) {
+		if (cudaMemcpyAsync(dp + pi.off[rec2_b], page + pi.off[rec2_b], pi.size[rec2_b], cudaMemcpyHostToDevice,
+		                    hp->in) != cudaSuccess) {
+			return FLS_ERR_CUDA;
+		}
+		uint8_t* rb = nullptr;
+		rc          = rec_decode(dp + pi.off[rec2_b], page + pi.off[rec2_b], pi.size[rec2_b], 2u, &rb, &rec2_n, hp->in);
+		d_rec2.p    = rb;
+		if (rc != FLS_OK) { return rc; }
+	}
 	ColDesc c {};
-	rc = build_page_column(pi, dp, w, nullptr, 0, FLS_ORIGINAL, d_out.as<uint8_t>(), &c, d_rec.as<uint8_t>(), rec_n);
+	rc = build_page_column(pi, dp, w, nullptr, 0, FLS_ORIGINAL, d_out.as<uint8_t>(), &c, d_rec.as<uint8_t>(), rec_n,
+	                       d_rec2.as<uint8_t>(), rec2_n);
 	if (rc != FLS_OK) { return rc; }
 	// work items: vector ids (the single column is the plan's inline column)
 	std::vector<uint32_t> ids(pi.vec_c);

@@ -42,6 +42,7 @@ const ExprLayout* expr_layout(uint8_t exp_t, uint8_t var) {
 	    {6, 2, 5, 16, ENC_DELTA, POST_RLE, 2, 3, 4, 1, 0, N, N, N, 0},                   // RLE DELTA_NO_PATCH
 	    {6, 3, 2, 16, ENC_RAW, POST_RLE, N, N, 1, N, 0, 0, N, N, 0},                     // RLE UNCOMPRESSED_REC
 	    {6, 4, 5, 16, ENC_DELTA, POST_RLE, 2, 3, 4, 1, 0, 0, N, N, 0},                   // RLE DELTA_NO_PATCH_REC
+	    {6, 5, 5, 16, ENC_DELTA, POST_RLE, 2, 3, 4, 1, 0, 0, N, N, 0, 1},                // RLE DELTA_NO_PATCH_REC2
 	    {8, 1, 1, 32, ENC_RAW, POST_DICT, N, N, 0, N, N, N, N, N, 0},                    // DICT UNCOMPRESSED
 	    {8, 2, 3, 32, ENC_FFOR, POST_DICT, 0, 1, 2, N, N, N, N, N, 0},                   // DICT FFOR_NO_PATCH
 	    {8, 7, 4, 32, ENC_DELTA, POST_DICT, 1, 2, 3, 0, N, N, N, N, 0},                  // DICT DELTA_NO_PATCH
@@ -59,8 +60,11 @@ const ExprLayout* expr_layout(uint8_t exp_t, uint8_t var) {
 	    {11, 3, 2, 16, ENC_RAW, POST_RLE_DICT, N, N, 1, N, 0, 0, N, N, 0},               // DICT_RLE UNCOMPRESSED_REC
 	    {11, 4, 5, 16, ENC_DELTA, POST_RLE_DICT, 2, 3, 4, 1, 0, 0, N, N, 0},             // DICT_RLE ..._REC
 	};
+	// DICT_FRQ (exp_t 9) pages are DICT pages: dict_frq_exp derives dict_exp (dict_exp.hpp:208), only the
+	// dictionary's order differs (frequency instead of first occurrence)
+	const uint8_t et = exp_t == 9 ? 8 : exp_t;
 	for (const auto& e : table) {
-		if (e.exp_t == exp_t && e.var == var) { return &e; }
+		if (e.exp_t == et && e.var == var) { return &e; }
 	}
 	return nullptr;
 }
@@ -110,11 +114,12 @@ int finish_page_info(PageInfo* pi, uint64_t page_size) {
 
 int build_page_column(const PageInfo& pi, const uint8_t* d_page, int value_width, const uint8_t* d_dict_vals,
                       uint32_t dict_entries, int order, uint8_t* d_out, ColDesc* c, const uint8_t* d_vals_decoded,
-                      uint64_t vals_decoded_size) {
+                      uint64_t vals_decoded_size, const uint8_t* d_rec2, uint64_t rec2_size) {
 	const ExprLayout* L = pi.layout;
 	if (!L || value_width == 0) { return FLS_ERR_UNSUPPORTED; }
 	// the page-level rec buffer of the _REC variants is decoded by the caller (rec_decode)
 	if (L->ib_rec != kNoBuf && !d_vals_decoded) { return FLS_ERR_UNSUPPORTED; }
+	if (L->ib_rec2 != kNoBuf && !d_rec2) { return FLS_ERR_UNSUPPORTED; }
 	*c        = ColDesc {};
 	c->ws     = static_cast<uint8_t>(L->ws ? L->ws : value_width);
 	c->e      = static_cast<uint8_t>(value_width / 8);
@@ -138,6 +143,10 @@ int build_page_column(const PageInfo& pi, const uint8_t* d_page, int value_width
 	if (L->ib_rec != kNoBuf) {
 		c->buf[L->ib_rec]      = d_vals_decoded;
 		c->buf_size[L->ib_rec] = vals_decoded_size;
+	}
+	if (L->ib_rec2 != kNoBuf) {
+		c->buf[L->ib_rec2]      = d_rec2;
+		c->buf_size[L->ib_rec2] = rec2_size;
 	}
 	c->ep  = reinterpret_cast<const uint32_t*>(d_page + pi.ep_off);
 	c->out = d_out;
@@ -312,9 +321,17 @@ static int describe_pages(const fls_page_column* cols, uint32_t n_cols, std::vec
 			if (g.e == 8) { any64 = true; }
 			continue;
 		}
+		const uint8_t* r2      = nullptr;
+		uint64_t       r2_size = 0;
+		if (pi.layout->ib_rec2 != kNoBuf) {
+			// REC2: the rsum bases (u16) are a rec buffer too
+			const uint32_t b = pi.layout->ib_rec2;
+			rc = decode_rec_on(pc.d_page + pi.off[b], pi.size[b], 2u, owned, &r2, &r2_size, stream);
+			if (rc != FLS_OK) { return rc; }
+		}
 		ColDesc d {};
 		rc = build_page_column(pi, pc.d_page, w, dvals, entries, pc.order, static_cast<uint8_t*>(pc.d_out), &d, rvals,
-		                       rsize);
+		                       rsize, r2, r2_size);
 		if (rc != FLS_OK) { return rc; }
 		if (post_is_gather(d.post)) { fam = Family::GATHER; }
 		if (d.ws == 64) { any64 = true; }

@@ -60,7 +60,7 @@ bool rec_is_raw(const uint8_t* h, uint64_t size, uint64_t* raw_off, uint64_t* ra
 
 int rec_decode(const uint8_t* d_src, const uint8_t* h_src, uint64_t size, uint32_t eb, uint8_t** d_out,
                uint64_t* out_size, cudaStream_t s) {
-	if ((eb != 4 && eb != 8) || !d_out || !out_size) { return FLS_ERR_ARG; }
+	if ((eb != 2 && eb != 4 && eb != 8) || !d_out || !out_size) { return FLS_ERR_ARG; }
 	Walk w;
 	int  rc = walk(h_src, size, eb, &w);
 	if (rc != FLS_OK) { return rc; }
@@ -91,8 +91,10 @@ int rec_decode(const uint8_t* d_src, const uint8_t* h_src, uint64_t size, uint32
 		if (ok) {
 			rc = eb == 8 ? fls_gpu_unffor_u64(reinterpret_cast<const uint64_t*>(base_ptr), reinterpret_cast<uint64_t*>(*d_out),
 			                                  d_bw, reinterpret_cast<const uint64_t*>(d_base), d_off, nb, FLS_TRANSPOSED, s)
-			             : fls_gpu_unffor_u32(reinterpret_cast<const uint32_t*>(base_ptr), reinterpret_cast<uint32_t*>(*d_out),
-			                                  d_bw, reinterpret_cast<const uint32_t*>(d_base), d_off, nb, FLS_TRANSPOSED, s);
+			     : eb == 4 ? fls_gpu_unffor_u32(reinterpret_cast<const uint32_t*>(base_ptr), reinterpret_cast<uint32_t*>(*d_out),
+			                                  d_bw, reinterpret_cast<const uint32_t*>(d_base), d_off, nb, FLS_TRANSPOSED, s)
+			               : fls_gpu_unffor_u16(reinterpret_cast<const uint16_t*>(base_ptr), reinterpret_cast<uint16_t*>(*d_out),
+			                                  d_bw, reinterpret_cast<const uint16_t*>(d_base), d_off, nb, FLS_TRANSPOSED, s);
 			ok = rc == FLS_OK && launch_rec_patch(d_src, d_exc, static_cast<uint32_t>(nb), eb, *d_out, s) == cudaSuccess;
 		}
 		cudaFreeAsync(tmp, s);

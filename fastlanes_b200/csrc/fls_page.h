@@ -14,6 +14,7 @@ struct ExprLayout {
 	uint8_t ib_rec;          // the rec-compressed buffer of the ..._REC variants (kNoBuf: none)
 	uint8_t ib_exc, ib_side; // patched variants: exception values, positions / bitmap / chain head
 	uint8_t dict_codes;      // 1: the patched stream is u32 dictionary codes, gathered from the dictionary after
+	uint8_t ib_rec2 = kNoBuf; // a second rec-compressed buffer (RLE REC2: the u16 rsum bases)
 };
 
 struct PageInfo {
@@ -31,10 +32,12 @@ const ExprLayout* expr_layout(uint8_t exp_t, uint8_t var);
 int               value_width_of(uint8_t data_type);
 int               parse_page_header(const uint8_t* hdr, uint64_t avail, PageInfo* out);
 int               finish_page_info(PageInfo* pi, uint64_t page_size);
-// d_vals_decoded / vals_decoded_size: for the _REC layouts, the decoded rec buffer that replaces buffer ib_vals.
+// d_vals_decoded / vals_decoded_size: for the _REC layouts, the decoded rec buffer that replaces buffer ib_rec;
+// d_rec2 / rec2_size: the decoded second rec buffer (ib_rec2) of the REC2 layout.
 int build_page_column(const PageInfo& pi, const uint8_t* d_page, int value_width, const uint8_t* d_dict_vals,
                       uint32_t dict_entries, int order, uint8_t* d_out, ColDesc* c,
-                      const uint8_t* d_vals_decoded = nullptr, uint64_t vals_decoded_size = 0);
+                      const uint8_t* d_vals_decoded = nullptr, uint64_t vals_decoded_size = 0,
+                      const uint8_t* d_rec2 = nullptr, uint64_t rec2_size = 0);
 // RLE DELTA_NO_PATCH page (fls_h_encode.cpp) of n values of width 32 or 64 from host memory.
 int encode_rle_page(const void* in, uint64_t n, uint64_t cap, uint8_t* out, uint64_t* out_size, uint64_t* mtd_size,
                     int width);

@@ -32,6 +32,7 @@ ARR_C = {
     (6, 2): 5,  # RLE DELTA_NO_PATCH: run values, lane bases, bw, base, packed (u16 index)
     (6, 3): 2,  # RLE UNCOMPRESSED_REC: run values rec-compressed, raw u16 index
     (6, 4): 5,  # RLE DELTA_NO_PATCH_REC: as above, run values rec-compressed
+    (6, 5): 5,  # RLE DELTA_NO_PATCH_REC2: run values and the u16 rsum bases rec-compressed (rle_exp.hpp:99-110)
     (7, 1): 2,  # FSST: bytes, end offsets
     (7, 2): 5,  # FSST DELTA_NO_PATCH: bytes, lane bases, bw, base, packed (u32 end offsets)
     (8, 1): 1,  # DICT UNCOMPRESSED: u32 codes
@@ -50,6 +51,9 @@ ARR_C = {
     (11, 3): 2,  # DICT_RLE UNCOMPRESSED_REC
     (11, 4): 5,  # DICT_RLE DELTA_NO_PATCH_REC
 }
+# DICT_FRQ (exp_t 9) pages are DICT pages (dict_frq_exp derives dict_exp, dict_exp.hpp:208): same variants and
+# buffers, the dictionary built in frequency order
+ARR_C.update({(9, var): n for (et, var), n in list(ARR_C.items()) if et == 8})
 
 
 class Page:
@@ -117,8 +121,9 @@ def rec_buffer(b, elem=np.uint64):
 STREAM_W = {2: None, 4: None, 5: None}
 
 
-def _stream(pg, v, first, ws, enc, T):
-    """Decode one 1024-value stream of width ws stored from buffer index `first` on; returns transposed."""
+def _stream(pg, v, first, ws, enc, T, lane_bases=None):
+    """Decode one 1024-value stream of width ws stored from buffer index `first` on; returns transposed.
+    lane_bases: a DELTA stream's decoded rsum bases (rec-compressed buffer), indexed by the entry points."""
     if enc == "raw":
         return _le(pg.vector_slice(v, first, 128 * ws), T).copy()
     if enc == "ffor":
@@ -126,7 +131,10 @@ def _stream(pg, v, first, ws, enc, T):
         base = _le(pg.vector_slice(v, first + 1, ws // 8), T)[0]
         packed = _le(pg.vector_slice(v, first + 2, bw * 128), T)
         return oracle.unffor(packed, bw, base, T)
-    lb = _le(pg.vector_slice(v, first, 128), T).copy()
+    if lane_bases is not None:
+        lb = _le(lane_bases[pg.ep_of(v, first):pg.ep_of(v, first) + 128], T).copy()
+    else:
+        lb = _le(pg.vector_slice(v, first, 128), T).copy()
     bw = int(pg.vector_slice(v, first + 1, 1)[0])
     base = _le(pg.vector_slice(v, first + 2, ws // 8), T)[0]
     packed = _le(pg.vector_slice(v, first + 3, bw * 128), T)
@@ -200,9 +208,12 @@ def decode_int(page, dict_bytes=None, value_dtype=np.uint64):
     if dict_bytes is not None and len(dict_bytes) > 8:
         dic = _le(rec_buffer(np.asarray(dict_bytes, np.uint8)[8:], np.uint64 if W == 64 else np.uint32)[0], VT)
     out = np.empty(pg.vec_c * 1024, VT)
-    et, var = pg.exp_t, pg.var
+    et, var = (8 if pg.exp_t == 9 else pg.exp_t), pg.var
     rec_vals = None
-    if et in (6, 11) and var in (3, 4):
+    rec_lb = None
+    if (et, var) == (6, 5):
+        rec_lb = rec_buffer(pg.b[pg.off[1]:pg.off[1] + pg.buf_size[1]], np.uint16)[0]
+    if et in (6, 11) and var in (3, 4) or (et, var) == (6, 5):
         # UNCOMPRESSED_REC / DELTA_NO_PATCH_REC: buffer 0 (run values / run codes) is one rec buffer; entry
         # points index its decoded bytes
         ve = np.uint32 if et == 11 or W == 32 else np.uint64
@@ -231,7 +242,7 @@ def decode_int(page, dict_bytes=None, value_dtype=np.uint64):
                 vals_buf = pg.vector_slice(v, 0)
             vt = VT if et == 6 else np.dtype(np.uint32)
             vals = _le(vals_buf, vt)
-            idx = _stream(pg, v, 1, 16, "raw" if var in (1, 3) else "delta", np.uint16)
+            idx = _stream(pg, v, 1, 16, "raw" if var in (1, 3) else "delta", np.uint16, rec_lb)
             tr = vals[idx.astype(np.int64)]
             if et == 11:
                 tr = dic[tr.astype(np.int64)]

@@ -38,13 +38,16 @@ TYPES = {8: np.uint8, 16: np.uint16, 32: np.uint32, 64: np.uint64}
 I64_IDS = [0, 1, 6, 7, 11, 16, 17, 22, 27]
 # The same expressions on columns large enough that the reference's rec compression (hzl_cmp.cpp:43-127)
 # writes FFOR blocks with exceptions, not only a raw tail: dictionaries of ~3000 entries, ~2000 runs.
-REC_IDS = [8, 9, 16, 17, 22, 27]
+REC_IDS = [8, 9, 10, 16, 17, 22, 27]
 # Patched FFOR / DELTA (src/cor/prm/patch/*) on columns with ~3% outliers / outlying gaps.
 PATCH_IDS = [2, 3, 4, 5, 12, 13, 14, 15]
 # DICT with patched FFOR / DELTA codes (dict_exp.hpp FFOR_*_PATCH, DELTA_*_PATCH): ~97 % of the rows take one of
 # 16 values, the rest ~2000 rare ones, so the rare values' codes (assigned in first-occurrence order) are the
 # patches' exceptions.
 DPATCH_IDS = [18, 19, 20, 21, 22, 23, 24, 25, 26]
+# DICT_FRQ (exp_t 9): the DICT expressions (dict_frq_exp derives dict_exp, dict_exp.hpp:208) over a dictionary
+# built in frequency order; the same columns as the patched DICT ones.
+FRQ_IDS = [28, 29, 30, 31, 32, 33, 34, 35, 36, 37, 38]
 STR_IDS = [0, 2, 3, 8, 13, 14, 15, 16]
 
 
@@ -192,7 +195,8 @@ def columns(ref):
         # the reference decoder reproduces the input for every int64 expression (asserted above)
     for eid in REC_IDS:
         rng = np.random.default_rng(3000 + eid)
-        m = 4 * 1024
+        # REC2 (id 10) also rec-compresses the u16 rsum bases (64 per vector): 20 vectors give one FFOR block
+        m = (20 if eid == 10 else 4) * 1024
         col = rec_column(eid, rng, m)
         page, dic = np.zeros(cap, np.uint8), np.zeros(cap, np.uint8)
         ps, ds = ctypes.c_uint64(), ctypes.c_uint64()
@@ -228,6 +232,18 @@ def columns(ref):
         res[f"i64dpatch_{eid}_input"] = col
         res[f"i64dpatch_{eid}_page"] = page[: ps.value].copy()
         res[f"i64dpatch_{eid}_dict"] = dic[: ds.value].copy()
+    for eid in FRQ_IDS:
+        rng = np.random.default_rng(6000 + eid)
+        m = 4 * 1024
+        col = dpatch_column(eid, rng, m)
+        page, dic = np.zeros(cap, np.uint8), np.zeros(cap, np.uint8)
+        ps, ds = ctypes.c_uint64(), ctypes.c_uint64()
+        rc = ref.ref_encode_i64(ptr(col), ctypes.c_uint64(m), ctypes.c_uint8(eid), 1, ptr(page), ctypes.c_uint64(cap),
+                                ctypes.byref(ps), ptr(dic), ctypes.c_uint64(cap), ctypes.byref(ds))
+        assert rc == 0, (eid, rc)
+        res[f"i64frq_{eid}_input"] = col
+        res[f"i64frq_{eid}_page"] = page[: ps.value].copy()
+        res[f"i64frq_{eid}_dict"] = dic[: ds.value].copy()
     for eid in STR_IDS:
         rng = np.random.default_rng(2000 + eid)
         byts, offs = str_column(eid, rng, n)

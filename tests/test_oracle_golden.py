@@ -112,7 +112,7 @@ def test_page_oracle_decodes_reference_int64_pages(col_golden, eid):
     assert np.array_equal(got, col_golden[f"i64_{eid}_input"])
 
 
-@pytest.mark.parametrize("eid", [8, 9, 16, 17, 22, 27])
+@pytest.mark.parametrize("eid", [8, 9, 10, 16, 17, 22, 27])
 def test_page_oracle_decodes_reference_rec_pages(col_golden, eid):
     """Reference pages whose rec buffers hold FFOR blocks with exceptions (large dictionaries, many runs)."""
     from oracle import pages
@@ -144,3 +144,13 @@ def test_page_oracle_decodes_reference_patched_dict_pages(col_golden, eid):
     page, dic = col_golden[f"i64dpatch_{eid}_page"], col_golden[f"i64dpatch_{eid}_dict"]
     got = pages.decode_int(page, dic, np.uint64).view(np.int64)
     assert np.array_equal(got, col_golden[f"i64dpatch_{eid}_input"])
+
+
+@pytest.mark.parametrize("eid", list(range(28, 39)))
+def test_page_oracle_decodes_reference_dict_frq_pages(col_golden, eid):
+    """DICT_FRQ pages (pool ids 28-38, exp_t 9): DICT pages over a frequency-ordered dictionary."""
+    from oracle import pages
+
+    page, dic = col_golden[f"i64frq_{eid}_page"], col_golden[f"i64frq_{eid}_dict"]
+    got = pages.decode_int(page, dic, np.uint64).view(np.int64)
+    assert np.array_equal(got, col_golden[f"i64frq_{eid}_input"])

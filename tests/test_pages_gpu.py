@@ -215,7 +215,7 @@ def test_plan_autotune_and_graph_replay(cuda):
     plan.close()
 
 
-@pytest.mark.parametrize("eid", [8, 9, 16, 17, 22, 27])
+@pytest.mark.parametrize("eid", [8, 9, 10, 16, 17, 22, 27])
 @pytest.mark.parametrize("shift", [0, 3, 8])
 def test_reference_rec_pages(cuda, col_golden, eid, shift):
     """Reference pages whose rec buffers (dictionary entries, run values, run codes) hold FFOR blocks with
@@ -274,7 +274,8 @@ def test_reference_patched_pages(cuda, col_golden, eid, shift):
     assert np.array_equal(pages.decode_to_memory(page, pages.INT64), want)
 
 
-@pytest.mark.parametrize("eid", [18, 19, 20, 21, 23, 24, 25, 26])
+@pytest.mark.parametrize("eid", [18, 19, 20, 21, 23, 24, 25, 26, "frq_28", "frq_29", "frq_30", "frq_31", "frq_32",
+                                 "frq_33", "frq_34", "frq_35", "frq_36", "frq_37", "frq_38"])
 @pytest.mark.parametrize("shift", [0, 7])
 def test_reference_patched_dict_pages(cuda, col_golden, eid, shift):
     """DICT pages of the reference whose u32 codes are patched FFOR / DELTA streams (pool ids 18-26): the
@@ -285,7 +286,8 @@ def test_reference_patched_dict_pages(cuda, col_golden, eid, shift):
     from fastlanes_b200 import pages
     from fastlanes_b200 import primitives as P
 
-    page, dic, want = (col_golden[f"i64dpatch_{eid}_{k}"] for k in ("page", "dict", "input"))
+    key = f"i64{eid}" if isinstance(eid, str) else f"i64dpatch_{eid}"  # DICT_FRQ (ids 28-38): DICT pages
+    page, dic, want = (col_golden[f"{key}_{k}"] for k in ("page", "dict", "input"))
     pbuf, pptr = _dev_bytes(page, cuda, shift)
     dbuf, dptr = _dev_bytes(dic, cuda, 3)
     col = dict(d_page=pptr, page_size=page.size, d_dict=dptr, dict_size=dic.size, data_type=pages.INT64)
