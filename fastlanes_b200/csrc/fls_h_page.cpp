@@ -234,6 +234,44 @@ static int decode_rec_on(const uint8_t* d_src, uint64_t size, uint32_t eb, std::
 // DICT page with patched codes takes two descriptors: its patched code stream decoded into a buffer of the
 // plan (in `owned`; a patched item, so it runs in an earlier launch segment than the gathers), then a raw
 // 32-bit stream of those codes gathered from the dictionary.
+extern "C++" {
+namespace flsgpu {
+int decode_patched_codes(const uint8_t* d_page, uint64_t page_size, uint32_t* d_codes, cudaStream_t stream) {
+	uint8_t        hdr[8 + 4 * 8];
+	const uint64_t take = page_size < sizeof(hdr) ? page_size : sizeof(hdr);
+	if (read_on(hdr, d_page, take, stream) != FLS_OK) { return FLS_ERR_CUDA; }
+	PageInfo pi;
+	int      rc = parse_page_header(hdr, take, &pi);
+	if (rc == FLS_OK) { rc = finish_page_info(&pi, page_size); }
+	if (rc != FLS_OK) { return rc; }
+	if (!pi.layout->dict_codes) { return FLS_ERR_UNSUPPORTED; }
+	if (pi.vec_c == 0) { return FLS_OK; }
+	std::vector<void*> owned;
+	const uint8_t*     rvals = nullptr;
+	uint64_t           rsize = 0;
+	if (pi.layout->ib_rec != kNoBuf) {
+		const uint32_t b = pi.layout->ib_rec;
+		rc               = decode_rec_on(d_page + pi.off[b], pi.size[b], 4u, &owned, &rvals, &rsize, stream);
+	}
+	ColDesc c {};
+	if (rc == FLS_OK) {
+		rc = build_page_column(pi, d_page, 32, nullptr, 0, FLS_TRANSPOSED, reinterpret_cast<uint8_t*>(d_codes), &c,
+		                       rvals, rsize);
+	}
+	if (rc == FLS_OK) {
+		DecodeArgs a {};
+		a.col0      = c;
+		a.n_items   = pi.vec_c;
+		a.col_shift = kPageShift;
+		if (launch_decode(Family::NUM_PATCH, a, stream) != cudaSuccess) { rc = FLS_ERR_CUDA; }
+	}
+	if (cudaStreamSynchronize(stream) != cudaSuccess && rc == FLS_OK) { rc = FLS_ERR_CUDA; }
+	for (void* p : owned) { cudaFree(p); }
+	return rc;
+}
+} // namespace flsgpu
+} // extern "C++"
+
 static int describe_pages(const fls_page_column* cols, uint32_t n_cols, std::vector<ColDesc>* descs,
                           std::vector<uint32_t>* queue, Family* fam_out, cudaStream_t stream,
                           std::vector<void*>* owned, std::vector<uint32_t>* col_desc = nullptr) {

@@ -59,19 +59,33 @@ namespace {
 
 // Row-stream layouts of the string expressions (roles as in the integer table of fls_h_page.cpp; ib_vals of a
 // DICT_RLE page holds the u32 code runs).  kind: STR_*.
+// patched: the DICT page's codes are a patched FFOR / DELTA stream, decoded once at plan creation
+// (decode_patched_codes) and then read as an UNCOMPRESSED code stream.
 struct StrLayout {
 	uint8_t exp_t, var, arr_c, ws, enc, post, ib_bw, ib_base, ib_packed, ib_lane, ib_vals, kind;
+	uint8_t patched = 0;
 };
 const StrLayout* str_layout(uint8_t exp_t, uint8_t var) {
+	// DICT_FRQ (exp_t 9) pages are DICT pages over a frequency-ordered dictionary (dict_exp.hpp:208)
+	exp_t = exp_t == 9 ? 8 : exp_t;
 	static const StrLayout t[] = {
 	    {8, 1, 1, 32, ENC_RAW, POST_NONE, kNoBuf, kNoBuf, 0, kNoBuf, kNoBuf, STR_DICT},   // DICT UNCOMPRESSED
 	    {8, 2, 3, 32, ENC_FFOR, POST_NONE, 0, 1, 2, kNoBuf, kNoBuf, STR_DICT},            // DICT FFOR_NO_PATCH
 	    {8, 7, 4, 32, ENC_DELTA, POST_NONE, 1, 2, 3, 0, kNoBuf, STR_DICT},                // DICT DELTA_NO_PATCH
+	    {8, 3, 5, 32, ENC_RAW, POST_NONE, kNoBuf, kNoBuf, 0, kNoBuf, kNoBuf, STR_DICT, 1}, // DICT FFOR_LL_PATCH
+	    {8, 4, 5, 32, ENC_RAW, POST_NONE, kNoBuf, kNoBuf, 0, kNoBuf, kNoBuf, STR_DICT, 1}, // DICT FFOR_S_PATCH
+	    {8, 5, 5, 32, ENC_RAW, POST_NONE, kNoBuf, kNoBuf, 0, kNoBuf, kNoBuf, STR_DICT, 1}, // DICT FFOR_B_PATCH
+	    {8, 6, 5, 32, ENC_RAW, POST_NONE, kNoBuf, kNoBuf, 0, kNoBuf, kNoBuf, STR_DICT, 1}, // DICT FFOR_S_PATCH_REC
+	    {8, 8, 6, 32, ENC_RAW, POST_NONE, kNoBuf, kNoBuf, 0, kNoBuf, kNoBuf, STR_DICT, 1}, // DICT DELTA_LL_PATCH
+	    {8, 9, 6, 32, ENC_RAW, POST_NONE, kNoBuf, kNoBuf, 0, kNoBuf, kNoBuf, STR_DICT, 1}, // DICT DELTA_S_PATCH
+	    {8, 10, 6, 32, ENC_RAW, POST_NONE, kNoBuf, kNoBuf, 0, kNoBuf, kNoBuf, STR_DICT, 1}, // DICT DELTA_B_PATCH
+	    {8, 11, 6, 32, ENC_RAW, POST_NONE, kNoBuf, kNoBuf, 0, kNoBuf, kNoBuf, STR_DICT, 1}, // ..._B_PATCH_REC
 	    {11, 1, 2, 16, ENC_RAW, POST_RLE, kNoBuf, kNoBuf, 1, kNoBuf, 0, STR_DICT},        // DICT_RLE UNCOMPRESSED
 	    {11, 2, 5, 16, ENC_DELTA, POST_RLE, 2, 3, 4, 1, 0, STR_DICT},                     // DICT_RLE DELTA_NO_PATCH
 	    {7, 1, 2, 32, ENC_RAW, POST_NONE, kNoBuf, kNoBuf, 1, kNoBuf, kNoBuf, STR_FSST},   // FSST
 	    {7, 2, 5, 32, ENC_DELTA, POST_NONE, 2, 3, 4, 1, kNoBuf, STR_FSST},                // FSST DELTA_NO_PATCH
 	    {3, 1, 2, 32, ENC_RAW, POST_NONE, kNoBuf, kNoBuf, 1, kNoBuf, kNoBuf, STR_BYTES},  // BYTE_ARR
+	    {3, 2, 5, 32, ENC_DELTA, POST_NONE, 2, 3, 4, 1, kNoBuf, STR_BYTES},               // BYTE_ARR DELTA_NO_PATCH
 	};
 	for (const auto& e : t) {
 		if (e.exp_t == exp_t && e.var == var) { return &e; }
@@ -100,6 +114,7 @@ struct fls_string_plan {
 	DevArr<uint8_t>          dict_bytes;
 	DevArr<uint64_t>         vec_total;
 	DevArr<uint64_t>         vec_base;
+	DevArr<uint32_t>         codes; // patched DICT pages: their decoded code stream
 	uint32_t                 dyn_smem = 0;
 	int                      warps    = 0; // warps per CTA of the materialising kernel
 	uint64_t                 n_rows   = 0;
@@ -148,6 +163,22 @@ int fls_string_plan_create(const uint8_t* d_page, uint64_t page_size, const uint
 		c.buf_size[i] = pi.size[i];
 	}
 	c.ep      = reinterpret_cast<const uint32_t*>(d_page + pi.ep_off);
+	if (L->patched) {
+		// decoded once here; the string kernels then read a raw 32-bit code stream
+		if (!p->codes.alloc(static_cast<size_t>(pi.vec_c) * 1024)) { return FLS_ERR_CUDA; }
+		rc = decode_patched_codes(d_page, page_size, p->codes.p, nullptr);
+		if (rc != FLS_OK) { return rc; }
+		c          = ColDesc {};
+		c.ws       = 32;
+		c.e        = 4;
+		c.enc      = ENC_RAW;
+		c.post     = POST_NONE;
+		c.order    = 1;
+		c.layout   = LAYOUT_ARRAYS;
+		c.n_vec    = pi.vec_c;
+		c.bw_const = 32;
+		c.packed   = reinterpret_cast<const uint8_t*>(p->codes.p);
+	}
 	a.kind    = L->kind;
 	a.status  = dev->status;
 	p->n_rows = static_cast<uint64_t>(pi.vec_c) * 1024;

@@ -2,6 +2,7 @@
 #pragma once
 
 #include "fls_plan.h"
+#include <cuda_runtime.h>
 #include <cstdint>
 
 namespace flsgpu {
@@ -38,6 +39,10 @@ int build_page_column(const PageInfo& pi, const uint8_t* d_page, int value_width
                       uint32_t dict_entries, int order, uint8_t* d_out, ColDesc* c,
                       const uint8_t* d_vals_decoded = nullptr, uint64_t vals_decoded_size = 0,
                       const uint8_t* d_rec2 = nullptr, uint64_t rec2_size = 0);
+// The u32 code stream of a DICT / DICT_FRQ page whose codes are patched FFOR / DELTA streams (page bytes in
+// device memory) decoded into d_codes (vec_c * 1024 u32, transposed order, as an UNCOMPRESSED page stores
+// them), exceptions rec-decoded first where the variant compresses them.  Synchronises `stream`.
+int decode_patched_codes(const uint8_t* d_page, uint64_t page_size, uint32_t* d_codes, cudaStream_t stream);
 // RLE DELTA_NO_PATCH page (fls_h_encode.cpp) of n values of width 32 or 64 from host memory.
 int encode_rle_page(const void* in, uint64_t n, uint64_t cap, uint8_t* out, uint64_t* out_size, uint64_t* mtd_size,
                     int width);

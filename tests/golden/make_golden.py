@@ -49,6 +49,10 @@ DPATCH_IDS = [18, 19, 20, 21, 22, 23, 24, 25, 26]
 # built in frequency order; the same columns as the patched DICT ones.
 FRQ_IDS = [28, 29, 30, 31, 32, 33, 34, 35, 36, 37, 38]
 STR_IDS = [0, 2, 3, 8, 13, 14, 15, 16]
+# the rest of the string pool (src/cor/exp_pool.cpp:70-99) but FSST12: BYTE_ARR DELTA_NO_PATCH (1), DICT with
+# patched codes (4-7, 9-12) and DICT_FRQ (17-27), the dictionary ones on columns whose rare strings' codes
+# become the patches' exceptions
+STR_MORE_IDS = [1, 4, 5, 6, 7, 9, 10, 11, 12] + list(range(17, 28))
 
 
 def ptr(a):
@@ -165,6 +169,11 @@ def str_column(eid, rng, n):
     if eid in (15, 16):
         runs = rng.geometric(1 / 5, n)
         col = [distinct[k] for k in np.repeat(rng.integers(0, 300, runs.size), runs)[:n]]
+    elif eid in STR_MORE_IDS and eid != 1:
+        k = rng.integers(0, 16, n)
+        rare = rng.random(n) < 0.03
+        k[rare] = rng.integers(16, 300, rare.sum())
+        col = [distinct[x] for x in k]
     else:
         col = [distinct[k] for k in rng.integers(0, 300, n)]
     offs = np.zeros(n + 1, np.uint64)
@@ -244,8 +253,8 @@ def columns(ref):
         res[f"i64frq_{eid}_input"] = col
         res[f"i64frq_{eid}_page"] = page[: ps.value].copy()
         res[f"i64frq_{eid}_dict"] = dic[: ds.value].copy()
-    for eid in STR_IDS:
-        rng = np.random.default_rng(2000 + eid)
+    for eid in STR_IDS + STR_MORE_IDS:
+        rng = np.random.default_rng(2000 + eid if eid in STR_IDS else 7000 + eid)
         byts, offs = str_column(eid, rng, n)
         page, dic = np.zeros(cap, np.uint8), np.zeros(cap, np.uint8)
         ps, ds = ctypes.c_uint64(), ctypes.c_uint64()

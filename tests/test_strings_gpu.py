@@ -6,6 +6,8 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 STR_IDS = [0, 2, 3, 8, 13, 14, 15, 16]
+# the rest of the string pool but FSST12: BYTE_ARR DELTA (1), DICT with patched codes (4-7, 9-12), DICT_FRQ (17-27)
+STR_MORE_IDS = [1, 4, 5, 6, 7, 9, 10, 11, 12] + list(range(17, 28))
 
 
 def _dev(a, dev, shift=0):
@@ -23,7 +25,7 @@ def _expected(g, eid):
     return g[f"str_{eid}_input_offsets"], g[f"str_{eid}_input_bytes"]
 
 
-@pytest.mark.parametrize("eid", STR_IDS)
+@pytest.mark.parametrize("eid", STR_IDS + STR_MORE_IDS)
 @pytest.mark.parametrize("shift", [0, 3])
 def test_reference_string_pages(cuda, col_golden, eid, shift):
     from fastlanes_b200 import primitives as P
