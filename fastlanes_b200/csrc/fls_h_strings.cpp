@@ -55,6 +55,37 @@ int fsst_import_table(const uint8_t* buf, uint64_t avail, FsstTable* t, uint64_t
 	return FLS_OK;
 }
 
+// fsst12_import (src/cor/prm/fsst12/libfsst12.cpp:363-389): 8-byte version word (upper 32 bits 20190218),
+// lenHisto (8 u16 symbol counts) at byte 8, from byte 24 every symbol as its length byte and that many
+// little-endian bytes; codes past the symbol count decode as the 8 bytes "corrupt".  Symbol lengths above 8 and
+// more than 4096 symbols (which the reference would write past its table for) are format errors.
+int fsst12_import_table(const uint8_t* buf, uint64_t avail, Fsst12Table* t, uint64_t* used) {
+	if (avail < 24) { return FLS_ERR_FORMAT; }
+	uint64_t version = 0;
+	std::memcpy(&version, buf, 8);
+	if ((version >> 32) != 20190218ull) { return FLS_ERR_FORMAT; }
+	uint16_t hist[8];
+	std::memcpy(hist, buf + 8, 16);
+	uint32_t count = 0;
+	for (const uint16_t h : hist) { count += h; }
+	if (count > 4096) { return FLS_ERR_FORMAT; }
+	std::memset(t, 0, sizeof(*t));
+	uint64_t pos = 24;
+	for (uint32_t code = 0; code < count; ++code) {
+		if (pos >= avail) { return FLS_ERR_FORMAT; }
+		const uint32_t l = buf[pos++];
+		if (l > 8 || pos + l > avail) { return FLS_ERR_FORMAT; }
+		t->len[code] = static_cast<uint8_t>(l);
+		for (uint32_t j = 0; j < l; ++j) { t->sym[code] |= static_cast<uint64_t>(buf[pos++]) << (8 * j); }
+	}
+	for (uint32_t code = count; code < 4096; ++code) {
+		t->sym[code] = 32774747032022883ull; // "corrupt"
+		t->len[code] = 8;
+	}
+	if (used) { *used = pos; }
+	return FLS_OK;
+}
+
 namespace {
 
 // Row-stream layouts of the string expressions (roles as in the integer table of fls_h_page.cpp; ib_vals of a
@@ -84,6 +115,8 @@ const StrLayout* str_layout(uint8_t exp_t, uint8_t var) {
 	    {11, 2, 5, 16, ENC_DELTA, POST_RLE, 2, 3, 4, 1, 0, STR_DICT},                     // DICT_RLE DELTA_NO_PATCH
 	    {7, 1, 2, 32, ENC_RAW, POST_NONE, kNoBuf, kNoBuf, 1, kNoBuf, kNoBuf, STR_FSST},   // FSST
 	    {7, 2, 5, 32, ENC_DELTA, POST_NONE, 2, 3, 4, 1, kNoBuf, STR_FSST},                // FSST DELTA_NO_PATCH
+	    {20, 1, 2, 32, ENC_RAW, POST_NONE, kNoBuf, kNoBuf, 1, kNoBuf, kNoBuf, STR_FSST12}, // FSST12
+	    {20, 2, 5, 32, ENC_DELTA, POST_NONE, 2, 3, 4, 1, kNoBuf, STR_FSST12},              // FSST12 DELTA_NO_PATCH
 	    {3, 1, 2, 32, ENC_RAW, POST_NONE, kNoBuf, kNoBuf, 1, kNoBuf, kNoBuf, STR_BYTES},  // BYTE_ARR
 	    {3, 2, 5, 32, ENC_DELTA, POST_NONE, 2, 3, 4, 1, kNoBuf, STR_BYTES},               // BYTE_ARR DELTA_NO_PATCH
 	};
@@ -110,6 +143,7 @@ using namespace flsgpu;
 struct fls_string_plan {
 	StrArgs                  args {};
 	DevArr<FsstTable>        table;
+	DevArr<Fsst12Table>      table12;
 	DevArr<uint32_t>         dict_ends;
 	DevArr<uint8_t>          dict_bytes;
 	DevArr<uint64_t>         vec_total;
@@ -187,7 +221,21 @@ int fls_string_plan_create(const uint8_t* d_page, uint64_t page_size, const uint
 	a.vec_base  = p->vec_base.p;
 	if (!p->table.alloc(1)) { return FLS_ERR_CUDA; }
 	FsstTable tab {};
-	if (L->kind != STR_BYTES) {
+	if (L->kind == STR_FSST12) {
+		// dict_hdr | exported FSST12 table (at most FSST12_MAXHEADER = 36888 bytes)
+		if (!d_dict || dict_size < 8 + 24) { return FLS_ERR_FORMAT; }
+		const uint64_t       head = dict_size < 8 + 36888 ? dict_size : 8 + 36888;
+		std::vector<uint8_t> h(head);
+		if (cudaMemcpy(h.data(), d_dict, head, cudaMemcpyDeviceToHost) != cudaSuccess) { return FLS_ERR_CUDA; }
+		std::unique_ptr<Fsst12Table> t12(new Fsst12Table());
+		rc = fsst12_import_table(h.data() + 8, head - 8, t12.get(), nullptr);
+		if (rc != FLS_OK) { return rc; }
+		if (!p->table12.alloc(1) ||
+		    cudaMemcpy(p->table12.p, t12.get(), sizeof(Fsst12Table), cudaMemcpyHostToDevice) != cudaSuccess) {
+			return FLS_ERR_CUDA;
+		}
+		a.table12 = p->table12.p;
+	} else if (L->kind != STR_BYTES) {
 		// DICT: dict_hdr | FSST table slot | entry_c u32 lengths | bytes.  FSST column: dict_hdr | exported table.
 		if (!d_dict || dict_size < 8 + 17) { return FLS_ERR_FORMAT; }
 		const uint64_t head = L->kind == STR_DICT ? 8 + kFsstMaxHeader : dict_size;
@@ -236,7 +284,7 @@ int fls_string_plan_create(const uint8_t* d_page, uint64_t page_size, const uint
 		for (const uint8_t w : bw) { a.rows16 = a.rows16 && w <= 16; }
 	}
 	const uint32_t per_warp = str_smem_per_warp(a.rows16);
-	const uint64_t budget   = 224 * 1024;
+	const uint64_t budget   = 224 * 1024 - (a.kind == STR_FSST12 ? kStrFsst12Smem : 0u);
 	const uint64_t dict_sm  = (a.dict_bytes_n + 15) & ~15ull;
 	a.ends_in_smem          = a.kind == STR_DICT && str_ends_smem(a) <= kStrEndsSmemMax;
 	a.dict_in_smem          = false;

@@ -8,7 +8,8 @@
 //   k_str_materialize warp per vector: Arrow offsets of its rows and their bytes, 32 rows at a time (one per
 //                    lane) into a per-warp shared-memory window that leaves in coalesced 16-byte stores.  DICT
 //                    rows are copied from the decoded dictionary (held in shared memory when it fits), BYTE_ARR
-//                    rows from the page, FSST rows decode from the page.
+//                    rows from the page, FSST and FSST12 rows decode from the page (symbol table in shared
+//                    memory: 2.3 KB for FSST, 36 KB for FSST12).
 #include "fls_decode.cu"
 #include "fls_strings.cuh"
 #include "fls_runtime.h"
@@ -264,7 +265,13 @@ __device__ __forceinline__ RowRef row_ref(const StrArgs& a, const uint32_t* ends
 		}
 		f.start = s;
 		f.clen  = e - s;
-		f.len   = KIND == STR_BYTES ? f.clen : fsst_decoded_len(flen, vb + s, f.clen);
+		if constexpr (KIND == STR_BYTES) {
+			f.len = f.clen;
+		} else if constexpr (KIND == STR_FSST12) {
+			f.len = fsst12_decoded_len(flen, vb + s, f.clen);
+		} else {
+			f.len = fsst_decoded_len(flen, vb + s, f.clen);
+		}
 		return f;
 	}
 }
@@ -279,8 +286,9 @@ enum : int { SM_NONE = 0, SM_ENDS = 1, SM_BYTES = 2 };
 template <int PASS, int KIND, int SM, bool R16>
 __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a) {
 	extern __shared__ __align__(128) uint8_t smem[];
-	__shared__ uint64_t fsym[KIND == STR_FSST ? 256 : 1];
-	__shared__ uint8_t  flen[KIND == STR_FSST ? 256 : 1];
+	constexpr uint32_t  kSyms = KIND == STR_FSST ? 256 : KIND == STR_FSST12 ? 4096 : 1;
+	__shared__ uint64_t fsym[kSyms];
+	__shared__ uint8_t  flen[kSyms];
 	const uint32_t     lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
 	constexpr uint32_t kPerWarp = str_per_warp(PASS, R16);
 	const uint8_t*     dict     = a.dict_bytes;
@@ -306,11 +314,17 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 			flen[i] = a.table->len[i];
 		}
 	}
+	if constexpr (KIND == STR_FSST12) {
+		for (uint32_t i = threadIdx.x; i < 4096; i += blockDim.x) { fsym[i] = __ldg(a.table12->sym + i); }
+		for (uint32_t i = threadIdx.x; i < 4096 / 16; i += blockDim.x) {
+			reinterpret_cast<uint4*>(flen)[i] = __ldg(reinterpret_cast<const uint4*>(a.table12->len) + i);
+		}
+	}
 	uint8_t* wbase = smem + warp * kPerWarp;
 	PlanS*   plans = reinterpret_cast<PlanS*>(wbase);
 	uint8_t* buf   = wbase + kStrPB * 64;
 	uint8_t* win   = buf + str_rows_bytes(R16);
-	constexpr bool kOr = PASS == STR_PASS_MATERIALIZE && KIND != STR_FSST;
+	constexpr bool kOr = PASS == STR_PASS_MATERIALIZE && KIND != STR_FSST && KIND != STR_FSST12;
 	if constexpr (kOr) {
 		for (uint32_t i = lane; i < kStrWindow / 16; i += 32) { reinterpret_cast<uint4*>(win)[i] = make_uint4(0, 0, 0, 0); }
 	}
@@ -427,6 +441,8 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 							       reinterpret_cast<const uint32_t*>(va & ~uintptr_t(3)),
 							       f.start + static_cast<uint32_t>(va & 3u), f.len);
 						}
+					} else if constexpr (KIND == STR_FSST12) {
+						fsst12_decode_to(fsym, flen, vb + f.start, f.clen, win + fill + (o - vpos));
 					} else {
 						fsst_decode_to(fsym, flen, vb + f.start, f.clen, win + fill + (o - vpos));
 					}
@@ -438,6 +454,8 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 					uint8_t* dst = a.bytes + vbase + o;
 					if constexpr (KIND == STR_FSST) {
 						fsst_decode_to(fsym, flen, vb + f.start, f.clen, dst);
+					} else if constexpr (KIND == STR_FSST12) {
+						fsst12_decode_to(fsym, flen, vb + f.start, f.clen, dst);
 					} else {
 						const uint8_t* src = KIND == STR_DICT ? dict + f.start : vb + f.start;
 						for (uint32_t i = 0; i < f.len; ++i) { dst[i] = src[i]; }
@@ -529,6 +547,7 @@ cudaError_t launch_str_lengths(const StrArgs& a, int /*grid*/, cudaStream_t s) {
 		return a.ends_in_smem ? launch_str_kernel<STR_PASS_LENGTHS, STR_DICT, SM_ENDS>(a, w, sm + str_ends_smem(a), s)
 		                      : launch_str_kernel<STR_PASS_LENGTHS, STR_DICT, SM_NONE>(a, w, sm, s);
 	case STR_FSST: return launch_str_kernel<STR_PASS_LENGTHS, STR_FSST, SM_NONE>(a, w, sm, s);
+	case STR_FSST12: return launch_str_kernel<STR_PASS_LENGTHS, STR_FSST12, SM_NONE>(a, w, sm, s);
 	default: return launch_str_kernel<STR_PASS_LENGTHS, STR_BYTES, SM_NONE>(a, w, sm, s);
 	}
 }
@@ -549,6 +568,7 @@ cudaError_t launch_str_materialize(const StrArgs& a, int warps, uint32_t dyn_sme
 		return a.dict_in_smem ? launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, SM_BYTES>(a, warps, dyn_smem, s)
 		                      : launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, SM_NONE>(a, warps, dyn_smem, s);
 	case STR_FSST: return launch_str_kernel<STR_PASS_MATERIALIZE, STR_FSST, SM_NONE>(a, warps, dyn_smem, s);
+	case STR_FSST12: return launch_str_kernel<STR_PASS_MATERIALIZE, STR_FSST12, SM_NONE>(a, warps, dyn_smem, s);
 	default: return launch_str_kernel<STR_PASS_MATERIALIZE, STR_BYTES, SM_NONE>(a, warps, dyn_smem, s);
 	}
 }

@@ -11,6 +11,9 @@
 //     codes untransposed (and RLE-expanded for DICT_RLE).
 //   * FSST column (include/fls/encoder/assert_eq.hpp:166-210, src/cor/lyt/vec.cpp:162-207): per vector the
 //     compressed bytes and 1024 cumulative end offsets (transposed); row i decodes bytes [end[i-1], end[i]).
+//   * FSST12 (include/fls/cor/prm/fsst12/fsst12.h:130-177, src/cor/lyt/vec.cpp:208-248): the same column
+//     layout; every 3 compressed bytes hold two 12-bit codes (bits 0-11, 12-23, little-endian), a trailing
+//     2 bytes one code; no escapes.
 // Output is Arrow-style: n_rows + 1 u32 offsets and the concatenated bytes.
 #pragma once
 
@@ -52,6 +55,37 @@ __device__ __forceinline__ void fsst_decode_to(const uint64_t* sym, const uint8_
 			o += l;
 		}
 	}
+}
+
+// Decoded length of one FSST12-compressed string.  A trailing single byte (which the encoder never writes)
+// decodes as the code of its 8 bits; the reference's decoder reads the byte after the string there.
+__device__ __forceinline__ uint32_t fsst12_decoded_len(const uint8_t* len, const uint8_t* in, uint32_t n) {
+	uint32_t out = 0, i = 0;
+	for (; i + 3 <= n; i += 3) {
+		const uint32_t c = in[i] | (static_cast<uint32_t>(in[i + 1]) << 8) | (static_cast<uint32_t>(in[i + 2]) << 16);
+		out += len[c & 4095u] + len[c >> 12];
+	}
+	if (i < n) { out += len[(in[i] | (i + 1 < n ? static_cast<uint32_t>(in[i + 1]) << 8 : 0u)) & 4095u]; }
+	return out;
+}
+
+__device__ __forceinline__ uint32_t fsst12_emit(const uint64_t* sym, const uint8_t* len, uint32_t code, uint8_t* out) {
+	const uint64_t s = sym[code];
+	const uint32_t l = len[code];
+	for (uint32_t b = 0; b < l; ++b) { out[b] = static_cast<uint8_t>(s >> (8 * b)); }
+	return l;
+}
+
+// Decode one FSST12-compressed string to out (exactly the decoded length is written).
+__device__ __forceinline__ void fsst12_decode_to(const uint64_t* sym, const uint8_t* len, const uint8_t* in,
+                                                 uint32_t n, uint8_t* out) {
+	uint32_t o = 0, i = 0;
+	for (; i + 3 <= n; i += 3) {
+		const uint32_t c = in[i] | (static_cast<uint32_t>(in[i + 1]) << 8) | (static_cast<uint32_t>(in[i + 2]) << 16);
+		o += fsst12_emit(sym, len, c & 4095u, out + o);
+		o += fsst12_emit(sym, len, c >> 12, out + o);
+	}
+	if (i < n) { fsst12_emit(sym, len, (in[i] | (i + 1 < n ? static_cast<uint32_t>(in[i + 1]) << 8 : 0u)) & 4095u, out + o); }
 }
 
 // Inclusive warp scan (Kogge-Stone over shuffles).

@@ -13,15 +13,25 @@ struct FsstTable {
 	uint8_t  len[256];
 };
 
+// FSST12 symbol table (include/fls/cor/prm/fsst12/fsst12.h:74-79): 4096 codes of 12 bits, symbol c
+// (little-endian) and its length.
+struct Fsst12Table {
+	uint64_t sym[4096];
+	uint8_t  len[4096];
+};
+
 enum : uint8_t {
 	STR_DICT  = 0, // rows are dictionary codes (DICT / DICT_RLE pages), dictionary FSST-decoded once per plan
 	STR_FSST  = 1, // rows are FSST-compressed in the page (FSST pages)
 	STR_BYTES = 2, // rows are plain bytes in the page (BYTE_ARR pages)
+	STR_FSST12 = 3, // rows are FSST12-compressed in the page (FSST12 pages)
 };
 
 constexpr int      kStrMaxWarps   = 32;        // warps per CTA of the string kernels (at most)
 constexpr int      kStrLenWarps   = 16;        // warps per CTA of the lengths pass
 constexpr uint32_t kStrEndsSmemMax = 64 * 1024; // largest dictionary end-offset array copied to shared memory
+// static shared memory of the FSST12 string kernels (the symbol table), taken from the dynamic budget
+constexpr uint32_t kStrFsst12Smem = sizeof(Fsst12Table);
 
 struct StrArgs {
 	ColDesc          col; // the row stream: codes or cumulative end offsets, page layout
@@ -34,6 +44,7 @@ struct StrArgs {
 	const uint8_t*   dict_bytes;
 	uint64_t         dict_bytes_n;
 	const FsstTable* table;
+	const Fsst12Table* table12; // FSST12 pages
 	uint64_t*        vec_total;
 	const uint64_t*  vec_base;
 	uint32_t*        offsets;

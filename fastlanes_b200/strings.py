@@ -1,4 +1,4 @@
-"""String columns (DICT / DICT_RLE with FSST dictionaries, FSST, BYTE_ARR pages) decoded on the GPU into
+"""String columns (DICT / DICT_RLE / DICT_FRQ with FSST dictionaries, FSST, FSST12, BYTE_ARR pages) decoded on the GPU into
 Arrow-style offsets + bytes (fls_string_plan_* of include/fls_b200.h)."""
 import ctypes
 

@@ -290,9 +290,10 @@ int fls_file_read(fls_file* file, const uint32_t* cols, uint32_t n, void* const*
 int fls_file_close(fls_file* file);
 
 /* ---------------------------------------------------------------------------------------------------------
- * String columns.  d_page: a string page (DICT: str expressions 2, 3, 8; DICT_RLE: 15, 16; FSST: 13, 14;
- * BYTE_ARR: 0 of src/cor/exp_pool.cpp:66-101); d_dict: its dictionary bytes (DICT / DICT_RLE: the FSST-
- * compressed dictionary page; FSST: the exported symbol table; BYTE_ARR: none).  Creating a plan decodes the
+ * String columns.  d_page: a string page (BYTE_ARR: str expressions 0, 1; DICT: 2-12; FSST: 13, 14;
+ * DICT_RLE: 15, 16; DICT_FRQ: 17-27; FSST12: 28, 29 of src/cor/exp_pool.cpp:66-101); d_dict: its dictionary
+ * bytes (DICT / DICT_RLE / DICT_FRQ: the FSST-compressed dictionary page; FSST / FSST12: the exported symbol
+ * table; BYTE_ARR: none).  Creating a plan decodes the
  * dictionary once on the GPU (TColDecoder::ExtInitDict, src/encoder/col_encoder.cpp:198-201); decoding emits
  * Arrow-style output: n_rows + 1 u32 offsets and the concatenated bytes, rows in original order
  * (include/fls/encoder/assert_eq.hpp:166-210, :257-400).  The page and dictionary buffers must outlive the plan.

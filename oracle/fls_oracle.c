@@ -206,6 +206,55 @@ uint64_t fls_o_fsst_decode(const uint64_t* sym, const uint8_t* len, const uint8_
 	return pout;
 }
 
+/* fsst12_import (src/cor/prm/fsst12/libfsst12.cpp:363-389): version word, 8 u16 symbol counts at byte 8, then
+ * every symbol as a length byte and its bytes; unused codes are the 8 bytes "corrupt". */
+uint32_t fls_o_fsst12_import(const uint8_t* buf, uint64_t avail, uint64_t* sym, uint8_t* len) {
+	uint64_t version = 0, count = 0;
+	if (avail < 24) { return 0; }
+	memcpy(&version, buf, 8);
+	if ((version >> 32) != 20190218ull) { return 0; }
+	uint16_t hist[8];
+	memcpy(hist, buf + 8, 16);
+	for (int i = 0; i < 8; ++i) { count += hist[i]; }
+	if (count > 4096) { return 0; }
+	uint64_t pos = 24;
+	for (uint64_t c = 0; c < count; ++c) {
+		if (pos >= avail || buf[pos] > 8 || pos + 1 + buf[pos] > avail) { return 0; }
+		len[c] = buf[pos++];
+		sym[c] = 0;
+		for (uint32_t j = 0; j < len[c]; ++j) { sym[c] |= (uint64_t)buf[pos++] << (8 * j); }
+	}
+	for (uint64_t c = count; c < 4096; ++c) {
+		sym[c] = 32774747032022883ull;
+		len[c] = 8;
+	}
+	return (uint32_t)pos;
+}
+
+static uint64_t fsst12_emit(const uint64_t* sym, const uint8_t* len, uint32_t code, uint8_t* out, uint64_t pout,
+                            uint64_t cap) {
+	for (uint32_t j = 0; j < len[code]; ++j) {
+		if (pout + j < cap) { out[pout + j] = (uint8_t)(sym[code] >> (8 * j)); }
+	}
+	return pout + len[code];
+}
+
+uint64_t fls_o_fsst12_decode(const uint64_t* sym, const uint8_t* len, const uint8_t* in, uint64_t in_len, uint8_t* out,
+                             uint64_t cap) {
+	uint64_t pin = 0, pout = 0;
+	for (; pin + 3 <= in_len; pin += 3) {
+		const uint32_t code = in[pin] | ((uint32_t)in[pin + 1] << 8) | ((uint32_t)in[pin + 2] << 16);
+		pout = fsst12_emit(sym, len, code & 4095u, out, pout, cap);
+		pout = fsst12_emit(sym, len, (code >> 12) & 4095u, out, pout, cap);
+	}
+	if (pin < in_len) {
+		/* the encoder writes a lone code as 2 bytes; a lone trailing byte decodes as its own 8 bits */
+		const uint32_t code = in[pin] | (pin + 1 < in_len ? (uint32_t)in[pin + 1] << 8 : 0u);
+		pout = fsst12_emit(sym, len, code & 4095u, out, pout, cap);
+	}
+	return pout;
+}
+
 /* CPU baseline in the oracle port: the same batch decode as fls_o_unffor_batch_*, transposed order, for a
  * caller that splits vector ranges over threads itself. */
 void fls_o_unffor_batch_bytes(int w, const uint8_t* packed, const uint64_t* byte_off, const uint8_t* bw,

@@ -50,6 +50,16 @@ uint64_t fls_o_fsst_decode(const uint64_t* sym, const uint8_t* len, const uint8_
  * Returns the number of header bytes consumed, 0 on a malformed header. */
 uint32_t fls_o_fsst_import(const uint8_t* buf, uint64_t* sym, uint8_t* len);
 
+/* FSST12 decode of one string, restating fsst12_decompress (include/fls/cor/prm/fsst12/fsst12.h:130-177):
+ * every 3 input bytes hold two 12-bit codes (little-endian), a trailing 2 bytes one code; no escapes.
+ * sym/len hold 4096 codes.  Returns the decoded length (only cap bytes are written). */
+uint64_t fls_o_fsst12_decode(const uint64_t* sym, const uint8_t* len, const uint8_t* in, uint64_t in_len,
+                             uint8_t* out, uint64_t cap);
+
+/* Import an FSST12 symbol table written by fsst12_export (src/cor/prm/fsst12/libfsst12.cpp:363-389).
+ * Returns the number of header bytes consumed, 0 on a malformed header. */
+uint32_t fls_o_fsst12_import(const uint8_t* buf, uint64_t avail, uint64_t* sym, uint8_t* len);
+
 #ifdef __cplusplus
 }
 #endif

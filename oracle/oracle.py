@@ -137,3 +137,22 @@ def fsst_decode(sym, ln, data):
     n = lib().fls_o_fsst_decode(_ptr(sym), _ptr(ln), _ptr(data), ctypes.c_uint64(data.size), _ptr(out),
                                 ctypes.c_uint64(cap))
     return out[:n].copy()
+
+
+def fsst12_decode_table(table_bytes):
+    """FSST12 symbol table (4096 codes) from fsst12_export's bytes: (bytes used, symbols, lengths)."""
+    t = np.ascontiguousarray(table_bytes, np.uint8)
+    sym = np.zeros(4096, np.uint64)
+    ln = np.zeros(4096, np.uint8)
+    used = lib().fls_o_fsst12_import(_ptr(t), ctypes.c_uint64(t.size), _ptr(sym), _ptr(ln))
+    return int(used), sym, ln
+
+
+def fsst12_decode(sym, ln, data):
+    data = np.ascontiguousarray(data, np.uint8)
+    cap = max(8 * data.size, 1)
+    out = np.zeros(cap, np.uint8)
+    lib().fls_o_fsst12_decode.restype = ctypes.c_uint64
+    n = lib().fls_o_fsst12_decode(_ptr(sym), _ptr(ln), _ptr(data), ctypes.c_uint64(data.size), _ptr(out),
+                                  ctypes.c_uint64(cap))
+    return out[:n].copy()

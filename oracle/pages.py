@@ -35,6 +35,8 @@ ARR_C = {
     (6, 5): 5,  # RLE DELTA_NO_PATCH_REC2: run values and the u16 rsum bases rec-compressed (rle_exp.hpp:99-110)
     (7, 1): 2,  # FSST: bytes, end offsets
     (7, 2): 5,  # FSST DELTA_NO_PATCH: bytes, lane bases, bw, base, packed (u32 end offsets)
+    (20, 1): 2,  # FSST12: bytes, end offsets (src/cor/lyt/vec.cpp:208-248)
+    (20, 2): 5,  # FSST12 DELTA_NO_PATCH: as FSST DELTA_NO_PATCH
     (8, 1): 1,  # DICT UNCOMPRESSED: u32 codes
     (8, 2): 3,  # DICT FFOR_NO_PATCH
     (8, 7): 4,  # DICT DELTA_NO_PATCH

@@ -15,6 +15,7 @@
 #include "fls/cor/lyt/dic/dic.hpp"
 #include "fls/cor/lyt/vec.hpp"
 #include "fls/cor/prm/fsst/fsst.h"
+#include "fls/cor/prm/fsst12/fsst12.h"
 #include "fls/api/engine.hpp"
 #include "fls/cor/eng/decompressor.hpp"
 #include "fls/cor/eng/engine.hpp"
@@ -238,6 +239,25 @@ int ref_decode_str(const uint8_t* data,
 					const uint32_t len = un[i] - start;
 					size_t         got = fsst_decompress(vec->fsst_decoder_up.get(), len, str_p + start, tmp.size(),
 					                                     reinterpret_cast<unsigned char*>(tmp.data()));
+					if (pos + got > bytes_cap) { return -2; }
+					std::memcpy(out_bytes + pos, tmp.data(), got);
+					pos += got;
+					out_offsets[v * 1024 + i + 1] = pos;
+					start                         = un[i];
+				}
+				break;
+			}
+			case ExpT::FSST12: {
+				// as the FSST case, with the 12-bit decoder (include/fls/encoder/assert_eq.hpp:211-250)
+				auto*    str_p   = vec->buf_arr[vec->arr_c + 0].mutable_data();
+				auto*    off_arr = vec->buf_arr[vec->arr_c + 1].mutable_data<uint32_t>();
+				uint32_t un[1024];
+				gen::untranspose::fallback::scalar::untranspose_i(off_arr, un);
+				uint32_t start = 0;
+				for (int i = 0; i < 1024; ++i) {
+					const uint32_t len = un[i] - start;
+					size_t got = fsst12_decompress(vec->fsst12_decoder_up.get(), len, str_p + start, tmp.size(),
+					                               reinterpret_cast<unsigned char*>(tmp.data()));
 					if (pos + got > bytes_cap) { return -2; }
 					std::memcpy(out_bytes + pos, tmp.data(), got);
 					pos += got;

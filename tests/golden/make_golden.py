@@ -49,10 +49,10 @@ DPATCH_IDS = [18, 19, 20, 21, 22, 23, 24, 25, 26]
 # built in frequency order; the same columns as the patched DICT ones.
 FRQ_IDS = [28, 29, 30, 31, 32, 33, 34, 35, 36, 37, 38]
 STR_IDS = [0, 2, 3, 8, 13, 14, 15, 16]
-# the rest of the string pool (src/cor/exp_pool.cpp:70-99) but FSST12: BYTE_ARR DELTA_NO_PATCH (1), DICT with
-# patched codes (4-7, 9-12) and DICT_FRQ (17-27), the dictionary ones on columns whose rare strings' codes
+# the rest of the string pool (src/cor/exp_pool.cpp:70-99): BYTE_ARR DELTA_NO_PATCH (1), DICT with patched codes
+# (4-7, 9-12), DICT_FRQ (17-27) and FSST12 (28, 29); the dictionary ones on columns whose rare strings' codes
 # become the patches' exceptions
-STR_MORE_IDS = [1, 4, 5, 6, 7, 9, 10, 11, 12] + list(range(17, 28))
+STR_MORE_IDS = [1, 4, 5, 6, 7, 9, 10, 11, 12] + list(range(17, 28)) + [28, 29]  # 28, 29: FSST12
 
 
 def ptr(a):
@@ -169,7 +169,7 @@ def str_column(eid, rng, n):
     if eid in (15, 16):
         runs = rng.geometric(1 / 5, n)
         col = [distinct[k] for k in np.repeat(rng.integers(0, 300, runs.size), runs)[:n]]
-    elif eid in STR_MORE_IDS and eid != 1:
+    elif eid in STR_MORE_IDS and eid not in (1, 28, 29):
         k = rng.integers(0, 16, n)
         rare = rng.random(n) < 0.03
         k[rare] = rng.integers(16, 300, rare.sum())

@@ -154,3 +154,34 @@ def test_page_oracle_decodes_reference_dict_frq_pages(col_golden, eid):
     page, dic = col_golden[f"i64frq_{eid}_page"], col_golden[f"i64frq_{eid}_dict"]
     got = pages.decode_int(page, dic, np.uint64).view(np.int64)
     assert np.array_equal(got, col_golden[f"i64frq_{eid}_input"])
+
+
+@pytest.mark.parametrize("eid", [28, 29])
+def test_fsst12_import_and_decode_golden(col_golden, eid):
+    """FSST12 columns of the reference (string pool ids 28, 29: end offsets plain or DELTA-coded) decode every
+    row of their page through the FSST12 restatement."""
+    from oracle import pages
+
+    page, dic = col_golden[f"str_{eid}_page"], col_golden[f"str_{eid}_dict"]
+    used, sym, ln = oracle.fsst12_decode_table(dic[8:])
+    assert used > 24 and used <= dic.size - 8
+    assert sym[4095] == 32774747032022883 and ln[4095] == 8  # unused codes decode as "corrupt"
+    pg = pages.parse_page(page)
+    assert (pg.exp_t, pg.var) == (20, 1 if eid == 28 else 2)
+    exp_bytes, exp_offs = col_golden[f"str_{eid}_input_bytes"], col_golden[f"str_{eid}_input_offsets"]
+    row = 0
+    for v in range(pg.vec_c):
+        data = pg.vector_slice(v, 0)
+        if eid == 28:
+            ends_t = np.frombuffer(pg.vector_slice(v, 1, 4096).tobytes(), np.uint32).copy()
+        else:
+            ends_t = pages._stream(pg, v, 1, 32, "delta", np.uint32)
+        ends = oracle.untranspose_i(ends_t)
+        start = 0
+        for i in range(1024):
+            got = oracle.fsst12_decode(sym, ln, data[start:ends[i]])
+            assert (ends[i] - start) % 3 != 1  # codes come in 3-byte pairs and 2-byte singles
+            assert np.array_equal(got, exp_bytes[exp_offs[row]:exp_offs[row + 1]]), row
+            start = ends[i]
+            row += 1
+    assert row == exp_offs.size - 1

@@ -6,8 +6,9 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 STR_IDS = [0, 2, 3, 8, 13, 14, 15, 16]
-# the rest of the string pool but FSST12: BYTE_ARR DELTA (1), DICT with patched codes (4-7, 9-12), DICT_FRQ (17-27)
-STR_MORE_IDS = [1, 4, 5, 6, 7, 9, 10, 11, 12] + list(range(17, 28))
+# the rest of the string pool: BYTE_ARR DELTA (1), DICT with patched codes (4-7, 9-12), DICT_FRQ (17-27), FSST12
+# (28, 29)
+STR_MORE_IDS = [1, 4, 5, 6, 7, 9, 10, 11, 12] + list(range(17, 28)) + [28, 29]
 
 
 def _dev(a, dev, shift=0):
