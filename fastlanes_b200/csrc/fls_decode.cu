@@ -299,6 +299,36 @@ __device__ __forceinline__ void decode_stream(const Plan& p, const uint32_t* S, 
                                               int* status = nullptr) {
 	using T = typename StreamT<WS>::T;
 	if constexpr (WS == 64) {
+		if (p.enc == ENC_DELTA && p.bw <= 26 && p.for_base < (1ull << 26) &&
+		    !(PATCH && scratch && post_is_patch(p.post))) {
+			// small deltas (the common case of sorted 64-bit keys): every delta + FOR base is below 2^27, so a
+			// half-lane's running sum of 32 of them fits 32 bits; the 64-bit add happens once per value
+			const uint32_t l   = t & 15u;
+			const uint32_t h   = t >> 4;
+			const uint32_t mlo = (1u << p.bw) - 1u;
+			const uint32_t b32 = static_cast<uint32_t>(p.for_base);
+			uint32_t       x[32];
+#pragma unroll
+			for (uint32_t m = 0; m < 32; ++m) {
+				const uint32_t b  = (2 * m + h) * p.bw;
+				const uint32_t h2 = b >> 5;
+				const uint32_t lo = S[2 * (l + 16 * (h2 >> 1)) + (h2 & 1u)];
+				const uint32_t h3 = h2 + 1;
+				const uint32_t hi = S[2 * (l + 16 * (h3 >> 1)) + (h3 & 1u)];
+				x[run32_pos(m)]   = __funnelshift_r(lo, hi, b & 31u) & mlo;
+			}
+			uint32_t acc = 0;
+#pragma unroll
+			for (int i = 0; i < 32; ++i) {
+				acc += x[i] + b32;
+				x[i] = acc;
+			}
+			const uint32_t lower = __shfl_sync(0xFFFFFFFFu, acc, l); // total of the lane's first half
+			const T        add   = static_cast<T>(ld_le(p.lane_bases + 8 * l, 8)) + (h ? lower : 0u);
+#pragma unroll
+			for (int i = 0; i < 32; ++i) { v[i] = add + x[i]; }
+			return;
+		}
 		extract_w64(S, t, p.bw, v);
 	} else if constexpr (WS == 32) {
 		extract_w32(S, t, p.bw, v);
