@@ -292,6 +292,61 @@ __device__ __forceinline__ void apply_patch(const Plan& p, typename StreamT<WS>:
 	}
 }
 
+// The 32 values of half-lane h of lane l (values 2m + h, m = 0..31, in run order) of a 64-bit stream of bit
+// width BW <= 16, as 32-bit words.  The thread's values sit at bits h*BW + 2m*BW of the lane: the lane's
+// 32-bit words are first shifted by h*BW (one funnel shift each, every word read once), after which every
+// value's word and shift are compile-time constants.
+template <uint32_t BW>
+__device__ __forceinline__ void extract_w64_small_bw(const uint32_t* __restrict__ S, uint32_t l, uint32_t h,
+                                                     uint32_t (&x)[32]) {
+	constexpr uint32_t mask = BW == 0 ? 0u : (1u << BW) - 1u;
+	if constexpr (BW == 0) {
+#pragma unroll
+		for (int i = 0; i < 32; ++i) { x[i] = 0; }
+	} else {
+		const uint32_t hb  = h * BW;
+		// lane word k (k = 0, 1, ...: the low and high halves of the lane's 64-bit words in order)
+		auto           raw = [&](uint32_t k) { return S[2 * (l + 16 * (k >> 1)) + (k & 1u)]; };
+#pragma unroll
+		for (uint32_t m = 0; m < 32; ++m) {
+			const uint32_t b  = 2 * m * BW;
+			const uint32_t k  = b >> 5;
+			const uint32_t sh = b & 31u;
+			const uint32_t s0 = __funnelshift_r(raw(k), raw(k + 1), hb);
+			if (sh + BW <= 32) {
+				x[run32_pos(m)] = (s0 >> sh) & mask;
+			} else {
+				const uint32_t s1 = __funnelshift_r(raw(k + 1), raw(k + 2), hb);
+				x[run32_pos(m)]   = __funnelshift_r(s0, s1, sh) & mask;
+			}
+		}
+	}
+}
+
+// Bit widths up to 26 (values below 2^26): compile-time layouts up to 16 bits, computed offsets above.
+__device__ __forceinline__ void extract_w64_small(const uint32_t* __restrict__ S, uint32_t l, uint32_t h,
+                                                  uint32_t bw, uint32_t (&x)[32]) {
+	switch (bw) {
+#define FLS_W64_SMALL(B)                                                                                               \
+	case B: extract_w64_small_bw<B>(S, l, h, x); return;
+		FLS_W64_SMALL(0) FLS_W64_SMALL(1) FLS_W64_SMALL(2) FLS_W64_SMALL(3) FLS_W64_SMALL(4) FLS_W64_SMALL(5)
+		FLS_W64_SMALL(6) FLS_W64_SMALL(7) FLS_W64_SMALL(8) FLS_W64_SMALL(9) FLS_W64_SMALL(10) FLS_W64_SMALL(11)
+		FLS_W64_SMALL(12) FLS_W64_SMALL(13) FLS_W64_SMALL(14) FLS_W64_SMALL(15) FLS_W64_SMALL(16)
+#undef FLS_W64_SMALL
+	default: break;
+	}
+	const uint32_t mlo = (1u << bw) - 1u;
+#pragma unroll
+	for (uint32_t m = 0; m < 32; ++m) {
+		const uint32_t b  = (2 * m + h) * bw;
+		const uint32_t h2 = b >> 5;
+		const uint32_t lo = S[2 * (l + 16 * (h2 >> 1)) + (h2 & 1u)];
+		const uint32_t h3 = h2 + 1;
+		const uint32_t hi = S[2 * (l + 16 * (h3 >> 1)) + (h3 & 1u)];
+		x[run32_pos(m)]   = __funnelshift_r(lo, hi, b & 31u) & mlo;
+	}
+}
+
 // PATCH: the kernel may meet patched items (plain-stream kernels and the catch-all one; gather kernels never do)
 template <int WS, bool PATCH = true>
 __device__ __forceinline__ void decode_stream(const Plan& p, const uint32_t* S, uint32_t t,
@@ -305,18 +360,9 @@ __device__ __forceinline__ void decode_stream(const Plan& p, const uint32_t* S, 
 			// half-lane's running sum of 32 of them fits 32 bits; the 64-bit add happens once per value
 			const uint32_t l   = t & 15u;
 			const uint32_t h   = t >> 4;
-			const uint32_t mlo = (1u << p.bw) - 1u;
 			const uint32_t b32 = static_cast<uint32_t>(p.for_base);
 			uint32_t       x[32];
-#pragma unroll
-			for (uint32_t m = 0; m < 32; ++m) {
-				const uint32_t b  = (2 * m + h) * p.bw;
-				const uint32_t h2 = b >> 5;
-				const uint32_t lo = S[2 * (l + 16 * (h2 >> 1)) + (h2 & 1u)];
-				const uint32_t h3 = h2 + 1;
-				const uint32_t hi = S[2 * (l + 16 * (h3 >> 1)) + (h3 & 1u)];
-				x[run32_pos(m)]   = __funnelshift_r(lo, hi, b & 31u) & mlo;
-			}
+			extract_w64_small(S, l, h, p.bw, x);
 			uint32_t acc = 0;
 #pragma unroll
 			for (int i = 0; i < 32; ++i) {

@@ -89,6 +89,21 @@ def test_emulated_rsum_and_delta(emu, w, order):
     assert np.array_equal(got, oracle.delta_batch(packed, off, bw, base, lb, order == 1))
 
 
+@pytest.mark.parametrize("order", [0, 1])
+def test_emulated_delta_u64_small_widths(emu, order):
+    """64-bit DELTA vectors of every bit width 0..27 with FOR bases below and at 2^26: the 32-bit running-sum
+    path (widths up to 26, compile-time layouts up to 16) and the general one on either side of its bounds."""
+    rng = np.random.default_rng(77)
+    bw = np.array(list(range(28)) + [7, 16, 26], np.uint8)
+    base = rng.integers(0, 1 << 26, bw.size, dtype=np.uint64)
+    base[-3:] = [(1 << 26) - 1, 1 << 26, 0]
+    lb = rng.integers(0, np.iinfo(np.uint64).max, bw.size * 16, dtype=np.uint64, endpoint=True)
+    packed, off, _, _ = _rebuild(64, bw, base, rng)
+    got, st = run(emu, 64, 2, order, packed, off, bw, base, lb, bw.size)
+    assert st == 0
+    assert np.array_equal(got, oracle.delta_batch(packed, off, bw, base, lb, order == 1))
+
+
 @pytest.mark.parametrize("w", [8, 16, 32, 64])
 def test_emulated_untranspose(emu, w):
     T = TYPES[w]
