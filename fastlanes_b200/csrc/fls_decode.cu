@@ -384,7 +384,11 @@ __device__ __forceinline__ void decode_stream(const Plan& p, const uint32_t* S, 
 		extract_w8(S, t, p.bw, v);
 	}
 	constexpr T wmask = WS == 64 ? ~T(0) : static_cast<T>((1ull << WS) - 1ull);
-	if (p.enc != ENC_RAW) {
+	// 16- and 8-bit DELTA streams without patches add the FOR base inside the running sum: sums of at most 16
+	// terms below 2^16 stay exact in 32 bits, so the wrap to the stream width comes once per value, off the
+	// chain of dependent adds
+	const bool fold = WS <= 16 && p.enc == ENC_DELTA && !(PATCH && scratch && post_is_patch(p.post));
+	if (p.enc != ENC_RAW && !fold) {
 		const T base = static_cast<T>(p.for_base);
 #pragma unroll
 		for (int i = 0; i < 32; ++i) { v[i] = (v[i] + base) & wmask; }
@@ -416,25 +420,31 @@ __device__ __forceinline__ void decode_stream(const Plan& p, const uint32_t* S, 
 #pragma unroll
 			for (int i = 0; i < 32; ++i) { v[i] += add; }
 		} else if constexpr (WS == 16) {
+			const T base = fold ? static_cast<T>(p.for_base) & wmask : T(0);
 #pragma unroll
 			for (int q = 0; q < 2; ++q) {
 				T acc = static_cast<T>(ld_le(p.lane_bases + 2 * (2 * t + q), 2));
 #pragma unroll
 				for (int i = 0; i < 16; ++i) {
-					acc          = (acc + v[16 * q + i]) & wmask;
+					acc += v[16 * q + i] + base;
 					v[16 * q + i] = acc;
 				}
 			}
+#pragma unroll
+			for (int i = 0; i < 32; ++i) { v[i] &= wmask; }
 		} else {
+			const T base = fold ? static_cast<T>(p.for_base) & wmask : T(0);
 #pragma unroll
 			for (int q = 0; q < 4; ++q) {
 				T acc = p.lane_bases[4 * t + q];
 #pragma unroll
 				for (int i = 0; i < 8; ++i) {
-					acc         = (acc + v[8 * q + i]) & wmask;
+					acc += v[8 * q + i] + base;
 					v[8 * q + i] = acc;
 				}
 			}
+#pragma unroll
+			for (int i = 0; i < 32; ++i) { v[i] &= wmask; }
 		}
 	}
 }
