@@ -145,6 +145,7 @@ struct fls_string_plan {
 	DevArr<FsstTable>        table;
 	DevArr<Fsst12Table>      table12;
 	DevArr<uint32_t>         dict_ends;
+	DevArr<uint32_t>         dict_rows; // packed start | length << 24 of every entry, when they fit
 	DevArr<uint8_t>          dict_bytes;
 	DevArr<uint64_t>         vec_total;
 	DevArr<uint64_t>         vec_base;
@@ -261,6 +262,27 @@ int fls_string_plan_create(const uint8_t* d_page, uint64_t page_size, const uint
 			uint32_t last = 0;
 			if (cudaMemcpy(&last, p->dict_ends.p + entry_c - 1, 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
 				return FLS_ERR_CUDA;
+			}
+			if (last < (1u << 24)) {
+				// the row table of the materialising pass: start | length << 24 when every entry is < 256 bytes
+				std::vector<uint32_t> ends(entry_c);
+				if (cudaMemcpy(ends.data(), p->dict_ends.p, 4ull * entry_c, cudaMemcpyDeviceToHost) != cudaSuccess) {
+					return FLS_ERR_CUDA;
+				}
+				bool     fits  = true;
+				uint32_t start = 0;
+				for (uint32_t c = 0; c < entry_c && fits; ++c) {
+					fits    = ends[c] >= start && ends[c] - start < 256;
+					ends[c] = start | ((ends[c] - start) << 24);
+					start   = static_cast<uint32_t>(ends[c] & 0xFFFFFFu) + (ends[c] >> 24);
+				}
+				if (fits) {
+					if (!p->dict_rows.alloc(entry_c) ||
+					    cudaMemcpy(p->dict_rows.p, ends.data(), 4ull * entry_c, cudaMemcpyHostToDevice) != cudaSuccess) {
+						return FLS_ERR_CUDA;
+					}
+					a.dict_rows = p->dict_rows.p;
+				}
 			}
 			a.entry_c      = entry_c;
 			a.dict_ends    = p->dict_ends.p;

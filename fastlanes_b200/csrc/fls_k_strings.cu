@@ -245,12 +245,19 @@ struct RowRef {
 
 template <int KIND, bool R16>
 __device__ __forceinline__ RowRef row_ref(const StrArgs& a, const uint32_t* ends, const uint8_t* rows, uint32_t r,
-                                          const uint8_t* vb, uint32_t vn, const uint8_t* flen, bool* bad) {
+                                          const uint8_t* vb, uint32_t vn, const uint8_t* flen, bool* bad,
+                                          const uint32_t* packed = nullptr) {
 	RowRef f {0, 0, 0};
 	if constexpr (KIND == STR_DICT) {
 		const uint32_t code = row_at<R16>(rows, r);
 		if (code >= a.entry_c) {
 			*bad = true;
+			return f;
+		}
+		if (packed) {
+			const uint32_t e = __ldg(packed + code);
+			f.start          = e & 0xFFFFFFu;
+			f.len            = e >> 24;
 			return f;
 		}
 		f.start = code ? ends[code - 1] : 0u;
@@ -419,11 +426,11 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 			uint32_t  vpos = 0; // bytes of this vector emitted so far
 			uint32_t* offs = a.offsets + v * kVec + lane;
 			// the next batch's row is looked up while the current one is copied
-			RowRef next = row_ref<KIND, R16>(a, ends, rows, lane, vb, vn, flen, &bad);
+			RowRef next = row_ref<KIND, R16>(a, ends, rows, lane, vb, vn, flen, &bad, a.dict_rows);
 			for (uint32_t b = 0; b < kVec / 32; ++b) {
 				const uint32_t r = 32 * b + lane;
 				const RowRef   f = next;
-				if (b + 1 < kVec / 32) { next = row_ref<KIND, R16>(a, ends, rows, r + 32, vb, vn, flen, &bad); }
+				if (b + 1 < kVec / 32) { next = row_ref<KIND, R16>(a, ends, rows, r + 32, vb, vn, flen, &bad, a.dict_rows); }
 				const uint32_t inc = warp_inclusive_scan(f.len, lane);
 				const uint32_t o   = vpos + inc - f.len;
 				const uint32_t T   = __shfl_sync(0xFFFFFFFFu, inc, 31);

@@ -41,6 +41,9 @@ struct StrArgs {
 	bool             rows16;       // DICT with fewer than 65535 entries: codes kept as 16-bit rows
 	uint32_t         entry_c;
 	const uint32_t*  dict_ends;
+	// materialising pass: entry c as start | length << 24 (dictionaries of < 16 MiB decoded bytes whose
+	// entries are all < 256 bytes), one load per row instead of two end offsets; null otherwise
+	const uint32_t*  dict_rows;
 	const uint8_t*   dict_bytes;
 	uint64_t         dict_bytes_n;
 	const FsstTable* table;
