@@ -98,15 +98,17 @@ __device__ __forceinline__ const uint8_t* vector_bytes(const ColDesc& c, uint32_
 	return *n ? c.buf[0] + o : c.buf[0];
 }
 
-// OR the n bytes at byte offset `start` of the 4-byte aligned word array `base` into the window at byte offset
-// d, whose bytes there are zero.  Window words wholly inside the row are plain stores; the first and last
-// (shared with the neighbouring rows, which other lanes may be writing at the same time) are atomic ORs of the
-// row's bytes.  Only the source words that hold bytes of the row are read.
-__device__ __forceinline__ void or_row(uint32_t* __restrict__ win, uint32_t d, const uint32_t* __restrict__ base,
-                                       uint32_t start, uint32_t n) {
+// Write the n bytes at byte offset `start` of the 4-byte aligned word array `base` to the window at byte offset
+// d.  Every window word is stored whole by the row that owns its first byte (bytes past that row's end are
+// zero in the store); a row that starts inside a word instead returns its bytes of that word (*head, word
+// *hk), for an atomic OR once every lane's stores are done.  So the window needs no zeroing, only the word
+// that the first row of a run of batches starts inside must hold zeros past the filled bytes.  Only the source
+// words that hold bytes of the row are read.  Returns whether a head is left to OR.
+__device__ __forceinline__ bool put_row(uint32_t* __restrict__ win, uint32_t d, const uint32_t* __restrict__ base,
+                                        uint32_t start, uint32_t n, uint32_t* hk, uint32_t* head) {
 	// the row is bytes [start, start + n) of the word array `base`; word indices (not pointers) keep the array's
 	// address space (shared memory for a dictionary held there)
-	if (n == 0) { return; }
+	if (n == 0) { return false; }
 	const int32_t  a    = static_cast<int32_t>(start) - static_cast<int32_t>(d & 3u); // lands on window byte 4*(d/4)
 	const uint32_t sh   = 8u * (static_cast<uint32_t>(a) & 3u);
 	const int32_t  s    = a >> 2;
@@ -116,13 +118,14 @@ __device__ __forceinline__ void or_row(uint32_t* __restrict__ win, uint32_t d, c
 	const uint32_t hm = 0xFFFFFFFFu << (8u * (d & 3u));
 	const uint32_t tm = 0xFFFFFFFFu >> (8u * (3u - ((d + n - 1) & 3u)));
 	// a clamped word only feeds bytes outside the row, which the masks drop
-	uint32_t w0 = base[s < s_lo ? s_lo : s];
-	uint32_t w1 = base[s + 1 > s_hi ? s_hi : s + 1];
-	if (k0 == k1) {
-		atomicOr(win + k0, __funnelshift_r(w0, w1, sh) & hm & tm);
-		return;
-	}
-	atomicOr(win + k0, __funnelshift_r(w0, w1, sh) & hm);
+	uint32_t       w0  = base[s < s_lo ? s_lo : s];
+	uint32_t       w1  = base[s + 1 > s_hi ? s_hi : s + 1];
+	const uint32_t h   = __funnelshift_r(w0, w1, sh) & hm & (k0 == k1 ? tm : 0xFFFFFFFFu);
+	const bool     mid = (d & 3u) != 0;
+	if (!mid) { win[k0] = h; }
+	*hk   = k0;
+	*head = h;
+	if (k0 == k1) { return mid; }
 	const uint32_t m = k1 - k0; // words k0 + 1 .. k1 - 1 are whole row words
 	uint32_t       j = 1;
 #pragma unroll 4
@@ -134,7 +137,8 @@ __device__ __forceinline__ void or_row(uint32_t* __restrict__ win, uint32_t d, c
 	w0                = w1;
 	const int32_t lst = s + static_cast<int32_t>(m) + 1;
 	w1                = base[lst > s_hi ? s_hi : lst];
-	atomicOr(win + k1, __funnelshift_r(w0, w1, sh) & tm);
+	win[k1]           = __funnelshift_r(w0, w1, sh) & tm;
+	return mid;
 }
 
 // ---------------------------------------------------------------------------------------------------------
@@ -145,8 +149,9 @@ __device__ __forceinline__ void or_row(uint32_t* __restrict__ win, uint32_t d, c
 //           conflict-free both by run and by row).  Dictionaries of fewer than 65535 entries keep their codes
 //           as 16-bit values (row r at half-word r + 2 * (r / 32), as conflict-free) in half the space: their
 //           packed codes are at most 16 bits wide
-//   window  (materialize only) 2 KB of output bytes starting at a 16-byte aligned output position; for the
-//           copied kinds (DICT, BYTE_ARR) its bytes past the filled part are kept zero, so rows are OR-ed in
+//   window  (materialize only) 2 KB of output bytes starting at a 16-byte aligned output position; the copied
+//           kinds (DICT, BYTE_ARR) store whole words (put_row), so only the partly filled word is kept zero
+//           past the filled bytes
 // The work per vector (1024 row copies) is long next to the latency of its loads, so the packed words are
 // read synchronously: occupancy, not prefetch depth, is what hides latency here.
 // ---------------------------------------------------------------------------------------------------------
@@ -331,10 +336,8 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 	PlanS*   plans = reinterpret_cast<PlanS*>(wbase);
 	uint8_t* buf   = wbase + kStrPB * 64;
 	uint8_t* win   = buf + str_rows_bytes(R16);
-	constexpr bool kOr = PASS == STR_PASS_MATERIALIZE && KIND != STR_FSST && KIND != STR_FSST12;
-	if constexpr (kOr) {
-		for (uint32_t i = lane; i < kStrWindow / 16; i += 32) { reinterpret_cast<uint4*>(win)[i] = make_uint4(0, 0, 0, 0); }
-	}
+	constexpr bool kOr  = PASS == STR_PASS_MATERIALIZE && KIND != STR_FSST && KIND != STR_FSST12;
+	uint32_t*      win32 = reinterpret_cast<uint32_t*>(win);
 	__syncthreads();
 
 	const uint64_t gw = static_cast<uint64_t>(blockIdx.x) * nwarps + warp;
@@ -390,6 +393,11 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 			uint64_t W    = vbase & ~15ull; // output position of win[0]
 			uint32_t fill = static_cast<uint32_t>(vbase & 15u);
 			uint64_t lo   = vbase; // first output byte the window may write
+			if constexpr (kOr) {
+				// the first row may start inside this word: it ORs its bytes in
+				if (lane == 0) { win32[fill >> 2] = 0; }
+				__syncwarp();
+			}
 			auto flush = [&](bool all) {
 				const uint32_t full = fill & ~15u;
 				const uint32_t upto = all ? fill : full;
@@ -402,15 +410,14 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 							if (g + i >= lo) { a.bytes[g + i] = win[c + i]; }
 						}
 					}
-					if constexpr (kOr) { *reinterpret_cast<uint4*>(win + c) = make_uint4(0, 0, 0, 0); }
 				}
 				__syncwarp();
 				if (!all) {
 					// the partial chunk [full, fill) moves to the window start
 					if constexpr (kOr) {
+						// (its bytes past `fill` are zero: every word was stored whole, zeros past the row's end)
 						if (lane == 0 && full != 0 && (fill & 15u) != 0) {
 							*reinterpret_cast<uint4*>(win) = *reinterpret_cast<const uint4*>(win + full);
-							*reinterpret_cast<uint4*>(win + full) = make_uint4(0, 0, 0, 0);
 						}
 					} else {
 						const uint8_t t = lane < (fill & 15u) ? win[full + lane] : 0;
@@ -438,16 +445,19 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 				if (fill + T > kStrWindow) { flush(false); }
 				if (fill + T <= kStrWindow) {
 					if constexpr (kOr) {
+						uint32_t hk = 0, head = 0;
+						bool     mid;
 						if constexpr (KIND == STR_DICT) {
 							// the decoded dictionary starts 16-byte aligned (shared or global memory)
-							or_row(reinterpret_cast<uint32_t*>(win), fill + (o - vpos),
-							       reinterpret_cast<const uint32_t*>(dict), f.start, f.len);
+							mid = put_row(win32, fill + (o - vpos), reinterpret_cast<const uint32_t*>(dict), f.start,
+							              f.len, &hk, &head);
 						} else {
 							const uintptr_t va = reinterpret_cast<uintptr_t>(vb);
-							or_row(reinterpret_cast<uint32_t*>(win), fill + (o - vpos),
-							       reinterpret_cast<const uint32_t*>(va & ~uintptr_t(3)),
-							       f.start + static_cast<uint32_t>(va & 3u), f.len);
+							mid = put_row(win32, fill + (o - vpos), reinterpret_cast<const uint32_t*>(va & ~uintptr_t(3)),
+							              f.start + static_cast<uint32_t>(va & 3u), f.len, &hk, &head);
 						}
+						__syncwarp(); // every word's whole store lands before the rows that start inside it OR in
+						if (mid) { atomicOr(win32 + hk, head); }
 					} else if constexpr (KIND == STR_FSST12) {
 						fsst12_decode_to(fsym, flen, vb + f.start, f.clen, win + fill + (o - vpos));
 					} else {
@@ -471,6 +481,10 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 					W    = pos & ~15ull;
 					fill = static_cast<uint32_t>(pos & 15u);
 					lo   = pos;
+					if constexpr (kOr) {
+						__syncwarp();
+						if (lane == 0) { win32[fill >> 2] = 0; }
+					}
 				}
 				vpos += T;
 				__syncwarp();
