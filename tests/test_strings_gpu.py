@@ -105,3 +105,45 @@ def test_string_dict_shared_memory_modes(cuda, n_dict):
     assert np.array_equal(offs.cpu().numpy().astype(np.int64), want_off)
     idx = np.concatenate([np.arange(int(doffs[c]), int(doffs[c + 1])) for c in codes])
     assert np.array_equal(data.cpu().numpy(), dbytes[idx])
+
+
+def _oracle_fsst12_rows(page, table):
+    """Rows of an FSST12 page (plain end offsets) decoded by the oracle's FSST12 restatement."""
+    from oracle import oracle, pages
+
+    _, sym, ln = oracle.fsst12_decode_table(table)
+    pg = pages.parse_page(page)
+    rows = []
+    for v in range(pg.vec_c):
+        data = pg.vector_slice(v, 0)
+        ends = oracle.untranspose_i(np.frombuffer(pg.vector_slice(v, 1, 4096).tobytes(), np.uint32).copy())
+        start = 0
+        for i in range(1024):
+            rows.append(oracle.fsst12_decode(sym, ln, data[start:ends[i]]))
+            start = ends[i]
+    return rows
+
+
+def test_fsst12_codes_past_the_symbol_count_decode_as_corrupt(cuda, col_golden):
+    """A reference FSST12 page read with a table cut to its first 100 symbols: every code past them decodes as
+    the 8 bytes "corrupt" (fsst12_import's fill), on the GPU as in the oracle."""
+    from fastlanes_b200 import primitives as P
+    from fastlanes_b200.strings import StringPlan
+
+    page, dic = col_golden["str_28_page"], col_golden["str_28_dict"].copy()
+    hist = np.frombuffer(dic[16:32].tobytes(), np.uint16)
+    assert int(hist.sum()) > 100
+    dic[16:32] = np.frombuffer(np.array([100, 0, 0, 0, 0, 0, 0, 0], np.uint16).tobytes(), np.uint8)
+    rows = _oracle_fsst12_rows(page, dic[8:])
+    want_b = np.concatenate(rows)
+    assert b"corrupt" in want_b.tobytes()
+    want_o = np.zeros(len(rows) + 1, np.uint64)
+    want_o[1:] = np.cumsum([r.size for r in rows])
+    pb, pp = _dev(page, cuda, 0)
+    db, dp = _dev(dic, cuda, 0)
+    plan = StringPlan(pp, page.size, dp, dic.size)
+    offs, data = plan.decode(cuda)
+    plan.close()
+    assert np.array_equal(offs.cpu().numpy().astype(np.uint64), want_o)
+    assert np.array_equal(data.cpu().numpy(), want_b)
+    assert P.device_status() == 0
