@@ -259,11 +259,14 @@ HostPipe* host_pipe() {
 int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_t out_cap, uint8_t dt,
                      uint64_t* n_values) {
 	const int w = value_width_of(dt);
-	if (!page || w == 0 || dt == DOUBLE) { return FLS_ERR_UNSUPPORTED; }
+	if (!page || w == 0) { return FLS_ERR_UNSUPPORTED; }
 	PageInfo pi;
 	uint64_t computed = 0;
 	int      rc       = page_size_of(page, &pi, &computed, w);
 	if (rc != FLS_OK) { return rc; }
+	// doubles: their 64-bit patterns, through every layout but RLE's rec-compressed run values (the reference
+	// has no rec buffers of doubles) and ALP (no layout here: the ALP library is not part of the reference snapshot)
+	if (dt == DOUBLE && pi.layout->ib_rec != kNoBuf && pi.layout->post == POST_RLE) { return FLS_ERR_UNSUPPORTED; }
 	if (page_size == 0) { page_size = computed; }
 	if (computed > page_size) { return FLS_ERR_FORMAT; }
 	rc = finish_page_info(&pi, page_size);
@@ -410,6 +413,10 @@ int fls_encode_from_memory_status(void* in, uint64_t n, uint64_t cap, uint8_t* o
 	case UINT64: return encode_t(static_cast<const uint64_t*>(in), n, cap, out, out_size, mtd_size, false, expr);
 	case INT32: return encode_t(static_cast<const uint32_t*>(in), n, cap, out, out_size, mtd_size, true, expr);
 	case UINT32: return encode_t(static_cast<const uint32_t*>(in), n, cap, out, out_size, mtd_size, false, expr);
+	case DOUBLE:
+		// the double pool's UNCOMPRESSED (src/cor/exp_pool.cpp:107): the values' bit patterns, transposed
+		if (expr != 0) { return FLS_ERR_UNSUPPORTED; }
+		return encode_t(static_cast<const uint64_t*>(in), n, cap, out, out_size, mtd_size, false, expr);
 	default: return FLS_ERR_UNSUPPORTED;
 	}
 }

@@ -297,10 +297,16 @@ static int describe_pages(const fls_page_column* cols, uint32_t n_cols, std::vec
 		const uint8_t* dvals   = nullptr;
 		uint32_t       entries = 0;
 		if (pi.layout->post == POST_DICT || pi.layout->post == POST_RLE_DICT || pi.layout->dict_codes) {
-			if (!pc.d_dict || pc.dict_size < 20) { return FLS_ERR_FORMAT; }
+			if (!pc.d_dict || pc.dict_size < (pc.data_type == DOUBLE ? 8u : 20u)) { return FLS_ERR_FORMAT; }
 			uint8_t dh[20];
-			if (read_on(dh, pc.d_dict, 20, stream) != FLS_OK) { return FLS_ERR_CUDA; }
-			if (dh[8] == 255) {
+			if (read_on(dh, pc.d_dict, pc.data_type == DOUBLE ? 8 : 20, stream) != FLS_OK) { return FLS_ERR_CUDA; }
+			if (pc.data_type == DOUBLE) {
+				// a double dictionary is its entry_c values, raw, after dict_hdr_t (TDic<dbl_pt>::Decompress,
+				// src/cor/lyt/dic/dic.cpp:150-153)
+				std::memcpy(&entries, dh + 4, 4);
+				if (8 + 8ull * entries > pc.dict_size) { return FLS_ERR_FORMAT; }
+				dvals = pc.d_dict + 8;
+			} else if (dh[8] == 255) {
 				uint64_t voff = 0;
 				rc            = int_dictionary_values(dh, pc.dict_size, w, &voff, &entries);
 				if (rc != FLS_OK) { return rc; }
@@ -317,6 +323,11 @@ static int describe_pages(const fls_page_column* cols, uint32_t n_cols, std::vec
 		}
 		const uint8_t* rvals = nullptr;
 		uint64_t       rsize = 0;
+		// the reference has no rec buffers of doubles (THzlDeCmp<double>::decompress_buf aborts,
+		// src/cor/eng/hzl_de_cmp.cpp:37-40): RLE _REC pages of a double column are not a format
+		if (pc.data_type == DOUBLE && pi.layout->ib_rec != kNoBuf && pi.layout->post == POST_RLE) {
+			return FLS_ERR_UNSUPPORTED;
+		}
 		if (pi.layout->ib_rec != kNoBuf) {
 			const uint32_t b = pi.layout->ib_rec;
 			rc = decode_rec_on(pc.d_page + pi.off[b], pi.size[b], rec_elem_bytes(pi.layout, w), owned, &rvals, &rsize,

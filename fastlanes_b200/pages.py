@@ -9,9 +9,9 @@ _p = ctypes.c_void_p
 _u64 = ctypes.c_uint64
 
 # data_t values of include/fastlanes.h
-INT64, UINT64, INT32, UINT32, INT16, UINT16 = 5, 9, 4, 8, 3, 7
+INT64, UINT64, INT32, UINT32, INT16, UINT16, DOUBLE = 5, 9, 4, 8, 3, 7, 1
 DTYPE_OF = {INT64: np.int64, UINT64: np.uint64, INT32: np.int32, UINT32: np.uint32, INT16: np.int16,
-            UINT16: np.uint16}
+            UINT16: np.uint16, DOUBLE: np.float64}
 
 
 class PageColumn(ctypes.Structure):

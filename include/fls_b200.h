@@ -200,7 +200,8 @@ typedef struct {
 	uint64_t       page_size;
 	const uint8_t* d_dict; /* NULL unless the expression has a dictionary */
 	uint64_t       dict_size;
-	uint8_t        data_type; /* enum data_t of fastlanes.h: INT64, UINT64, INT32, UINT32, INT16, UINT16 */
+	uint8_t        data_type; /* enum data_t of fastlanes.h: INT64, UINT64, INT32, UINT32, INT16, UINT16, DOUBLE
+	                             (bit patterns; a DOUBLE dictionary page holds its values raw) */
 	uint8_t        order;     /* fls_order_code; FLS_ORIGINAL is what the reference materialises */
 	uint8_t        reserved[6];
 	void*          d_out; /* vec_c * 1024 values of data_type */

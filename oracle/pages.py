@@ -201,14 +201,22 @@ def _patched_stream(pg, v, T, rec_exc, kind=None, delta=None):
     return vals
 
 
-def decode_int(page, dict_bytes=None, value_dtype=np.uint64):
-    """Materialised (original-order) values of an integer page, as assert_eq.hpp:50-400 reconstructs them."""
+def decode_int(page, dict_bytes=None, value_dtype=np.uint64, raw_dict=False):
+    """Materialised (original-order) values of an integer page, as assert_eq.hpp:50-400 reconstructs them.
+    raw_dict: the dictionary page holds its entry_c values raw after dict_hdr_t, as a double column's does
+    (TDic<dbl_pt>::Decompress, src/cor/lyt/dic/dic.cpp:150-153); decode a double page with value_dtype uint64
+    (the values' bit patterns)."""
     pg = parse_page(page)
     VT = np.dtype(value_dtype)
     W = VT.itemsize * 8
     dic = None
     if dict_bytes is not None and len(dict_bytes) > 8:
-        dic = _le(rec_buffer(np.asarray(dict_bytes, np.uint8)[8:], np.uint64 if W == 64 else np.uint32)[0], VT)
+        db = np.asarray(dict_bytes, np.uint8)
+        if raw_dict:
+            entry_c = int(np.frombuffer(db[4:8].tobytes(), np.uint32)[0])
+            dic = _le(db[8:8 + entry_c * VT.itemsize], VT)
+        else:
+            dic = _le(rec_buffer(db[8:], np.uint64 if W == 64 else np.uint32)[0], VT)
     out = np.empty(pg.vec_c * 1024, VT)
     et, var = (8 if pg.exp_t == 9 else pg.exp_t), pg.var
     rec_vals = None

@@ -72,6 +72,76 @@ int copy_out(const Buf& b, uint8_t* dst, uint64_t cap, uint64_t* sz) {
 	if (b.Size() > 0) { std::memcpy(dst, b.data(), b.Size()); }
 	return 0;
 }
+
+template <class PT>
+int encode_col(const PT* data, uint64_t n, uint8_t expr_id, int verify, uint8_t* data_out, uint64_t data_cap,
+               uint64_t* data_sz, uint8_t* dict_out, uint64_t dict_cap, uint64_t* dict_sz) {
+	try {
+		bool       ok  = false;
+		Expression exp = expression_of(ExpPool<PT>::get_pool(), expr_id, &ok);
+		if (!ok) { return -3; }
+		std::vector<PT>   col(data, data + n);
+		ExpColEncoder<PT> enc(verify != 0);
+		ExpEncodedCol     res = enc.encode_pointer(col.data(), n, exp);
+		int               rc  = copy_out(*res.data_buf, data_out, data_cap, data_sz);
+		if (rc != 0) { return rc; }
+		return copy_out(*res.dictionary_buf, dict_out, dict_cap, dict_sz);
+	} catch (const std::exception&) { return -1; }
+}
+
+// Values come out as their 64-bit patterns, original order.
+template <class PT>
+int decode_col(const uint8_t* data, const uint8_t* dict, uint64_t dict_sz, uint64_t* out, uint64_t out_cap_vec,
+               uint64_t* n_vec) {
+	try {
+		TColDecoder<PT> dec;
+		if (dict_sz > 0) { dec.ExtInitDict(dict); }
+		dec.InitDecompress(data);
+		const n_t vc = dec.NVector();
+		*n_vec       = vc;
+		if (vc > out_cap_vec) { return -2; }
+		const ExpT exp_t = static_cast<ExpT>(data[0]);
+		for (n_t v = 0; v < vc; ++v) {
+			Vec*      vec = dec.Decompress();
+			uint64_t* o   = out + v * 1024;
+			switch (exp_t) {
+			case ExpT::UNCOMPRESSED:
+			case ExpT::FFOR:
+			case ExpT::DELTA:
+				gen::untranspose::fallback::scalar::untranspose_i(
+				    reinterpret_cast<const uint64_t*>(vec->buf_arr[0].data()), o);
+				break;
+			case ExpT::RLE: {
+				uint64_t tr[1024];
+				vec->flatten_to(tr);
+				gen::untranspose::fallback::scalar::untranspose_i(tr, o);
+				break;
+			}
+			case ExpT::DICT:
+			case ExpT::DICT_FRQ:
+			case ExpT::DICT_VAL: {
+				auto*    idx_arr = reinterpret_cast<uint32_t*>(vec->buf_arr[vec->arr_c + 0].mutable_data());
+				auto*    dic     = reinterpret_cast<const uint64_t*>(vec->dict_up->data_buf.mutable_data());
+				uint32_t un[1024];
+				gen::untranspose::fallback::scalar::untranspose_i(idx_arr, un);
+				for (int i = 0; i < 1024; ++i) { o[i] = dic[un[i]]; }
+				break;
+			}
+			case ExpT::DICT_RLE: {
+				uint32_t tr[1024], un[1024];
+				vec->flatten_to(tr);
+				gen::untranspose::fallback::scalar::untranspose_i(tr, un);
+				auto* dic = reinterpret_cast<const uint64_t*>(vec->dict_up->data_buf.mutable_data());
+				for (int i = 0; i < 1024; ++i) { o[i] = dic[un[i]]; }
+				break;
+			}
+			default:
+				return -4;
+			}
+		}
+		return 0;
+	} catch (const std::exception&) { return -1; }
+}
 } // namespace
 
 extern "C" {
@@ -92,17 +162,21 @@ int ref_encode_i64(const int64_t* data,
                    uint8_t*       dict_out,
                    uint64_t       dict_cap,
                    uint64_t*      dict_sz) {
-	try {
-		bool       ok  = false;
-		Expression exp = expression_of(ExpPool<i64_pt>::get_pool(), expr_id, &ok);
-		if (!ok) { return -3; }
-		std::vector<int64_t>   col(data, data + n);
-		ExpColEncoder<i64_pt>  enc(verify != 0);
-		ExpEncodedCol          res = enc.encode_pointer(col.data(), n, exp);
-		int                    rc  = copy_out(*res.data_buf, data_out, data_cap, data_sz);
-		if (rc != 0) { return rc; }
-		return copy_out(*res.dictionary_buf, dict_out, dict_cap, dict_sz);
-	} catch (const std::exception&) { return -1; }
+	return encode_col<i64_pt>(data, n, expr_id, verify, data_out, data_cap, data_sz, dict_out, dict_cap, dict_sz);
+}
+
+/* The same for a double column (double pool, src/cor/exp_pool.cpp:104-137). */
+int ref_encode_f64(const double* data,
+                   uint64_t      n,
+                   uint8_t       expr_id,
+                   int           verify,
+                   uint8_t*      data_out,
+                   uint64_t      data_cap,
+                   uint64_t*     data_sz,
+                   uint8_t*      dict_out,
+                   uint64_t      dict_cap,
+                   uint64_t*     dict_sz) {
+	return encode_col<dbl_pt>(data, n, expr_id, verify, data_out, data_cap, data_sz, dict_out, dict_cap, dict_sz);
 }
 
 /* Decode a reference-encoded int64 column to original order; *n_vec receives the vector count. */
@@ -112,54 +186,17 @@ int ref_decode_i64(const uint8_t* data,
                    int64_t*       out,
                    uint64_t       out_cap_vec,
                    uint64_t*      n_vec) {
-	try {
-		TColDecoder<i64_pt> dec;
-		if (dict_sz > 0) { dec.ExtInitDict(dict); }
-		dec.InitDecompress(data);
-		const n_t vc = dec.NVector();
-		*n_vec       = vc;
-		if (vc > out_cap_vec) { return -2; }
-		const ExpT exp_t = static_cast<ExpT>(data[0]);
-		for (n_t v = 0; v < vc; ++v) {
-			Vec*      vec = dec.Decompress();
-			uint64_t* o   = reinterpret_cast<uint64_t*>(out + v * 1024);
-			switch (exp_t) {
-			case ExpT::UNCOMPRESSED:
-			case ExpT::FFOR:
-			case ExpT::DELTA:
-				gen::untranspose::fallback::scalar::untranspose_i(
-				    reinterpret_cast<const uint64_t*>(vec->buf_arr[0].data()), o);
-				break;
-			case ExpT::RLE: {
-				uint64_t tr[1024];
-				vec->flatten_to(tr);
-				gen::untranspose::fallback::scalar::untranspose_i(tr, o);
-				break;
-			}
-			case ExpT::DICT:
-			case ExpT::DICT_FRQ:
-			case ExpT::DICT_VAL: {
-				auto*    idx_arr = reinterpret_cast<uint32_t*>(vec->buf_arr[vec->arr_c + 0].mutable_data());
-				auto*    dic     = reinterpret_cast<int64_t*>(vec->dict_up->data_buf.mutable_data());
-				uint32_t un[1024];
-				gen::untranspose::fallback::scalar::untranspose_i(idx_arr, un);
-				for (int i = 0; i < 1024; ++i) { out[v * 1024 + i] = dic[un[i]]; }
-				break;
-			}
-			case ExpT::DICT_RLE: {
-				uint32_t tr[1024], un[1024];
-				vec->flatten_to(tr);
-				gen::untranspose::fallback::scalar::untranspose_i(tr, un);
-				auto* dic = reinterpret_cast<int64_t*>(vec->dict_up->data_buf.mutable_data());
-				for (int i = 0; i < 1024; ++i) { out[v * 1024 + i] = dic[un[i]]; }
-				break;
-			}
-			default:
-				return -4;
-			}
-		}
-		return 0;
-	} catch (const std::exception&) { return -1; }
+	return decode_col<i64_pt>(data, dict, dict_sz, reinterpret_cast<uint64_t*>(out), out_cap_vec, n_vec);
+}
+
+/* The same for a double column (the values' bit patterns). */
+int ref_decode_f64(const uint8_t* data,
+                   const uint8_t* dict,
+                   uint64_t       dict_sz,
+                   double*        out,
+                   uint64_t       out_cap_vec,
+                   uint64_t*      n_vec) {
+	return decode_col<dbl_pt>(data, dict, dict_sz, reinterpret_cast<uint64_t*>(out), out_cap_vec, n_vec);
 }
 
 /* Encode n strings given as Arrow-style (offsets[n+1], bytes) with string pool expression expr_id

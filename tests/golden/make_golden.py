@@ -48,6 +48,11 @@ DPATCH_IDS = [18, 19, 20, 21, 22, 23, 24, 25, 26]
 # DICT_FRQ (exp_t 9): the DICT expressions (dict_frq_exp derives dict_exp, dict_exp.hpp:208) over a dictionary
 # built in frequency order; the same columns as the patched DICT ones.
 FRQ_IDS = [28, 29, 30, 31, 32, 33, 34, 35, 36, 37, 38]
+# The double pool (src/cor/exp_pool.cpp:104-137) through every expression the reference encodes and decodes for
+# doubles: UNCOMPRESSED, RLE without rec buffers, DICT (a raw double dictionary, src/cor/lyt/dic/dic.cpp:150-153)
+# with every code variant, DICT_RLE and DICT_FRQ.  Its RLE _REC variants (8-10) have no double form in the
+# reference (THzlDeCmp<double>::decompress_buf aborts) and ALP (1) needs the ALP library, absent here.
+F64_IDS = [0, 6, 7] + list(range(16, 39))
 STR_IDS = [0, 2, 3, 8, 13, 14, 15, 16]
 # the rest of the string pool (src/cor/exp_pool.cpp:70-99): BYTE_ARR DELTA_NO_PATCH (1), DICT with patched codes
 # (4-7, 9-12), DICT_FRQ (17-27) and FSST12 (28, 29); the dictionary ones on columns whose rare strings' codes
@@ -162,6 +167,18 @@ def dpatch_column(eid, rng, n):
     return x.astype(np.int64)
 
 
+def f64_column(eid, rng, n):
+    """Doubles with the equality structure of the int64 columns of the same expression (x / 4 is exact and
+    one-to-one below 2^53); UNCOMPRESSED also carries infinities, NaNs, signed zeros and subnormals."""
+    if eid == 0:
+        x = rng.normal(0, 1e6, n)
+        x[rng.integers(0, n, 64)] = [np.inf, -np.inf, np.nan, -0.0, 5e-324, -2.2250738585072014e-308, 1e308,
+                                     0.1] * 8
+        return x
+    src = i64_column(eid, rng, n) if eid in (6, 7, 16, 17, 22, 27) else dpatch_column(eid, rng, n)
+    return src.astype(np.float64) / 4
+
+
 def str_column(eid, rng, n):
     alphabet = np.frombuffer(b"abcdefghijklmnopqrstuvwxyzABCDEFGHIJKLMNOPQRSTUVWXYZ0123456789-_", np.uint8)
     tokens = [bytes(alphabet[rng.integers(0, 64, rng.integers(2, 7))]) for _ in range(64)]
@@ -253,6 +270,23 @@ def columns(ref):
         res[f"i64frq_{eid}_input"] = col
         res[f"i64frq_{eid}_page"] = page[: ps.value].copy()
         res[f"i64frq_{eid}_dict"] = dic[: ds.value].copy()
+    for eid in F64_IDS:
+        rng = np.random.default_rng(8000 + eid)
+        m = 4 * 1024
+        col = f64_column(eid, rng, m)
+        page, dic = np.zeros(cap, np.uint8), np.zeros(cap, np.uint8)
+        ps, ds = ctypes.c_uint64(), ctypes.c_uint64()
+        rc = ref.ref_encode_f64(ptr(col), ctypes.c_uint64(m), ctypes.c_uint8(eid), 1, ptr(page), ctypes.c_uint64(cap),
+                                ctypes.byref(ps), ptr(dic), ctypes.c_uint64(cap), ctypes.byref(ds))
+        assert rc == 0, (eid, rc)
+        out = np.zeros(m, np.float64)
+        nv = ctypes.c_uint64()
+        rc = ref.ref_decode_f64(ptr(page), ptr(dic), ds, ptr(out), ctypes.c_uint64(m // 1024), ctypes.byref(nv))
+        assert rc == 0 and nv.value == m // 1024, (eid, rc)
+        assert np.array_equal(out.view(np.uint64), col.view(np.uint64)), eid
+        res[f"f64_{eid}_input"] = col
+        res[f"f64_{eid}_page"] = page[: ps.value].copy()
+        res[f"f64_{eid}_dict"] = dic[: ds.value].copy()
     for eid in STR_IDS + STR_MORE_IDS:
         rng = np.random.default_rng(2000 + eid if eid in STR_IDS else 7000 + eid)
         byts, offs = str_column(eid, rng, n)

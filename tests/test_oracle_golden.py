@@ -185,3 +185,14 @@ def test_fsst12_import_and_decode_golden(col_golden, eid):
             start = ends[i]
             row += 1
     assert row == exp_offs.size - 1
+
+
+@pytest.mark.parametrize("eid", [0, 6, 7] + list(range(16, 39)))
+def test_page_oracle_decodes_reference_double_pages(col_golden, eid):
+    """Double columns of the reference (double pool ids 0, 6, 7, 16-38: raw double dictionaries): the page
+    restatement reproduces the values' bit patterns, NaNs, infinities and signed zeros included."""
+    from oracle import pages
+
+    page, dic = col_golden[f"f64_{eid}_page"], col_golden[f"f64_{eid}_dict"]
+    got = pages.decode_int(page, dic if dic.size else None, np.uint64, raw_dict=True)
+    assert np.array_equal(got, col_golden[f"f64_{eid}_input"].view(np.uint64))

@@ -325,3 +325,49 @@ def test_reference_patched_dict_pages(cuda, col_golden, eid, shift):
     assert np.array_equal(outs[2].cpu().numpy(), col_golden["i64_6_input"])
     plan.close()
     assert P.device_status() == 0
+
+
+F64_IDS = [0, 6, 7] + list(range(16, 39))
+
+
+@pytest.mark.parametrize("eid", F64_IDS)
+@pytest.mark.parametrize("shift", [0, 3])
+def test_reference_double_pages(cuda, col_golden, eid, shift):
+    """Double columns written by the reference (double pool: UNCOMPRESSED, RLE, DICT with every code variant over
+    a raw double dictionary, DICT_RLE, DICT_FRQ) decode to the input's exact bit patterns, through the page
+    decoder and through a plan."""
+    import torch
+
+    from fastlanes_b200 import pages
+    from fastlanes_b200 import primitives as P
+
+    page, dic = col_golden[f"f64_{eid}_page"], col_golden[f"f64_{eid}_dict"]
+    want = col_golden[f"f64_{eid}_input"].view(np.uint64)
+    pbuf, pptr = _dev_bytes(page, cuda, shift)
+    dbuf, dptr = _dev_bytes(dic, cuda, (shift * 5) % 8) if dic.size else (None, 0)
+    col = dict(d_page=pptr, page_size=page.size, d_dict=dptr, dict_size=dic.size, data_type=pages.DOUBLE, order=1)
+    out = torch.zeros(want.size, dtype=torch.float64, device=cuda)
+    pages.decode_pages([dict(col, d_out=out.data_ptr())])
+    assert np.array_equal(out.cpu().numpy().view(np.uint64), want), (eid, shift)
+    out2 = torch.zeros_like(out)
+    plan = pages.PagePlan([dict(col, d_out=out2.data_ptr())])
+    plan.decode()
+    torch.cuda.synchronize()
+    plan.close()
+    assert np.array_equal(out2.cpu().numpy().view(np.uint64), want), (eid, shift)
+    assert P.device_status() == 0
+
+
+def test_c_api_doubles(cuda, col_golden):
+    """decode_to_memory reads the reference's double UNCOMPRESSED and RLE pages; encode_from_memory writes the
+    UNCOMPRESSED one byte for byte; ALP (expression 1) is refused: the ALP library is not part of the reference."""
+    from fastlanes_b200 import pages
+
+    for eid in (0, 6, 7):
+        want = col_golden[f"f64_{eid}_input"]
+        got = pages.decode_to_memory(col_golden[f"f64_{eid}_page"], pages.DOUBLE)
+        assert np.array_equal(got.view(np.uint64), want.view(np.uint64)), eid
+    page, _ = pages.encode_from_memory(col_golden["f64_0_input"], pages.DOUBLE, 0)
+    assert np.array_equal(page, col_golden["f64_0_page"])
+    with pytest.raises(Exception):
+        pages.encode_from_memory(col_golden["f64_0_input"], pages.DOUBLE, 1)
