@@ -263,6 +263,56 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def cpu_column_leg(kind, values=None, strings=None, seconds=2.0):
+    """The reference's own column decoder (TColDecoder + materialisation, oracle/_ref compiled from its sources)
+    on one core, over a bounded sample of a leg's workload that the reference's own encoder wrote: decoded bytes
+    per second.  kind: ("i64", expr) or ("str", expr).  None where the reference library is absent."""
+    import ctypes
+
+    from oracle import oracle as orc
+
+    ref = orc.reference
+    if ref is None:
+        return None
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    cap = 1 << 28
+    page, dic = np.zeros(cap, np.uint8), np.zeros(1 << 24, np.uint8)
+    ps, ds = ctypes.c_uint64(), ctypes.c_uint64()
+    if kind[0] == "i64":
+        col = np.ascontiguousarray(values, np.int64)
+        rc = ref.ref_encode_i64(P(col), ctypes.c_uint64(col.size), ctypes.c_uint8(kind[1]), 0, P(page),
+                                ctypes.c_uint64(cap), ctypes.byref(ps), P(dic), ctypes.c_uint64(dic.size),
+                                ctypes.byref(ds))
+        out = np.zeros(col.size, np.int64)
+        nv = ctypes.c_uint64()
+        run = lambda: ref.ref_decode_i64(P(page), P(dic), ds, P(out), ctypes.c_uint64(col.size // 1024),
+                                         ctypes.byref(nv))
+        n_rows, out_bytes = col.size, col.nbytes
+    else:
+        byts, offs = strings
+        offs = np.ascontiguousarray(offs, np.uint64)
+        n_rows = offs.size - 1
+        rc = ref.ref_encode_str(P(byts), P(offs), ctypes.c_uint64(n_rows), ctypes.c_uint8(kind[1]), 0, P(page),
+                                ctypes.c_uint64(cap), ctypes.byref(ps), P(dic), ctypes.c_uint64(dic.size),
+                                ctypes.byref(ds))
+        ob = np.zeros(int(offs[-1]) + 4096, np.uint8)
+        oo = np.zeros(n_rows + 1, np.uint64)
+        nr = ctypes.c_uint64()
+        run = lambda: ref.ref_decode_str(P(page), P(dic), ds, P(ob), ctypes.c_uint64(ob.size), P(oo),
+                                         ctypes.c_uint64(oo.size), ctypes.byref(nr))
+        out_bytes = int(offs[-1]) + 4 * (n_rows + 1)
+    if rc != 0 or run() != 0:
+        return None
+    reps, t = 0, 0.0
+    while t < seconds:
+        t0 = time.perf_counter()
+        run()
+        t += time.perf_counter() - t0
+        reps += 1
+    return {"value": round(out_bytes * reps / t / 1e9, 3), "unit": "GB/s", "cores": 1, "kind": "reference",
+            "sample": f"{n_rows} rows written by the reference's encoder (expression {kind[1]}), decoded {reps} times"}
+
+
 def device_timed(fn, steps, warm):
     """Mean device time of fn() in ms: CUDA events on the current stream, synchronised on both sides."""
     import torch
@@ -353,10 +403,18 @@ def other_configs(dev, args):
         # roofline fraction counts the bytes it moves (page + bitmaps)
         out[name + "_filter"]["value"] = round(values.nbytes / (fms * 1e-3) / 1e9, 2)
 
+    ts = W.delta_timestamps()
     page_leg("3a_delta_i64", "32Mi sorted int64 timestamps from 1.6e18, geometric(mean 10) gaps, DELTA (id 11)",
-             W.delta_timestamps(), PG.INT64, 11)
+             ts, PG.INT64, 11)
+    out["3a_delta_i64"]["cpu_baseline"] = cpu_column_leg(("i64", 11), values=ts[:1 << 20])
+    runs = W.rle_int32()
     page_leg("3b_rle_i32", "32Mi int32 run values~U[0,1e6), geometric(mean 8) runs, RLE DELTA_NO_PATCH (id 6)",
-             W.rle_int32(), PG.INT32, 6)
+             runs, PG.INT32, 6)
+    # the reference has no int32 column encoder: its int64 RLE of the same values
+    cb = cpu_column_leg(("i64", 6), values=runs[:1 << 20])
+    if cb:
+        cb["sample"] += " (as int64: the reference has no int32 column encoder)"
+    out["3b_rle_i32"]["cpu_baseline"] = cb
 
     # 4: DICT + FSST strings, 16Mi rows
     dbytes, doffs = W.string_dictionary()
@@ -385,6 +443,13 @@ def other_configs(dev, args):
     leg("4_dict_fsst_str", "16Mi rows, 4096-entry FSST dictionary (5-40 B strings), Zipf(1.1) codes at 12 bits",
         ms, page.size + dic.size, 4 * (codes.size + 1) + n_bytes, codes.size, ok, 3)
     plan.close()
+    # the reference: its DICT FFOR string expression (string pool id 3) over the first 256 Ki rows
+    sc = codes[:1 << 18]
+    sl = np.diff(doffs).astype(np.int64)[sc]
+    so = np.zeros(sc.size + 1, np.uint64)
+    so[1:] = np.cumsum(sl)
+    sb = np.concatenate([dbytes[int(doffs[c]):int(doffs[c + 1])] for c in sc])
+    out["4_dict_fsst_str"]["cpu_baseline"] = cpu_column_leg(("str", 3), strings=(sb, so))
     out["5_mixed_select"] = mixed_rowgroups(dev, peak, steps)
     return out
 
