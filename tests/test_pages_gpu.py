@@ -371,3 +371,20 @@ def test_c_api_doubles(cuda, col_golden):
     assert np.array_equal(page, col_golden["f64_0_page"])
     with pytest.raises(Exception):
         pages.encode_from_memory(col_golden["f64_0_input"], pages.DOUBLE, 1)
+
+
+def test_double_dictionary_too_short_is_refused(cuda, col_golden):
+    """A double DICT page whose dictionary holds fewer bytes than entry_c values is a format error."""
+    import torch
+
+    from fastlanes_b200 import pages
+    from fastlanes_b200._lib import FlsError
+
+    page, dic = col_golden["f64_17_page"], col_golden["f64_17_dict"]
+    pbuf, pptr = _dev_bytes(page, cuda)
+    short = dic[:-8].copy()
+    dbuf, dptr = _dev_bytes(short, cuda)
+    out = torch.zeros(col_golden["f64_17_input"].size, dtype=torch.float64, device=cuda)
+    with pytest.raises(FlsError):
+        pages.decode_pages([dict(d_page=pptr, page_size=page.size, d_dict=dptr, dict_size=short.size,
+                                 data_type=pages.DOUBLE, order=1, d_out=out.data_ptr())])

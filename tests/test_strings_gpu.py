@@ -147,3 +147,28 @@ def test_fsst12_codes_past_the_symbol_count_decode_as_corrupt(cuda, col_golden):
     assert np.array_equal(offs.cpu().numpy().astype(np.uint64), want_o)
     assert np.array_equal(data.cpu().numpy(), want_b)
     assert P.device_status() == 0
+
+
+def test_fsst12_malformed_tables_are_refused(cuda, col_golden):
+    """An FSST12 symbol table whose counts exceed 4096 codes, with a symbol longer than 8 bytes, cut short, or
+    with another version word is a format error at plan creation (the reference would write past its table)."""
+    from fastlanes_b200._lib import FlsError
+    from fastlanes_b200.strings import StringPlan
+
+    page, dic = col_golden["str_28_page"], col_golden["str_28_dict"]
+    pb, pp = _dev(page, cuda, 0)
+    bad = []
+    d = dic.copy()
+    d[16:32] = np.frombuffer(np.array([4000, 97, 0, 0, 0, 0, 0, 0], np.uint16).tobytes(), np.uint8)
+    bad.append(d)
+    d = dic.copy()
+    d[32] = 9  # the first symbol's length byte
+    bad.append(d)
+    bad.append(dic[:40].copy())
+    d = dic.copy()
+    d[12] ^= 1  # the version word's upper half
+    bad.append(d)
+    for d in bad:
+        db, dp = _dev(d, cuda, 0)
+        with pytest.raises(FlsError):
+            StringPlan(pp, page.size, dp, d.size)
