@@ -153,6 +153,9 @@ struct fls_string_plan {
 	uint32_t                 dyn_smem = 0;
 	int                      warps    = 0; // warps per CTA of the materialising kernel
 	uint64_t                 n_rows   = 0;
+	// a measure() whose per-vector totals and bases the next decode() takes over (the usual measure, allocate,
+	// decode sequence runs the lengths pass once)
+	mutable bool             measured = false;
 };
 
 extern "C" {
@@ -337,6 +340,7 @@ static int run_totals(const fls_string_plan* p, cudaStream_t s) {
 int fls_string_plan_measure(fls_string_plan* p, uint64_t* n_bytes, fls_stream_t stream) {
 	if (!p || !n_bytes) { return FLS_ERR_ARG; }
 	cudaStream_t s  = static_cast<cudaStream_t>(stream);
+	p->measured     = false;
 	const int    rc = run_totals(p, s);
 	if (rc != FLS_OK) { return rc; }
 	*n_bytes = 0;
@@ -344,7 +348,9 @@ int fls_string_plan_measure(fls_string_plan* p, uint64_t* n_bytes, fls_stream_t 
 	if (cudaMemcpyAsync(n_bytes, p->vec_base.p + p->args.col.n_vec, 8, cudaMemcpyDeviceToHost, s) != cudaSuccess) {
 		return FLS_ERR_CUDA;
 	}
-	return cudaStreamSynchronize(s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
+	if (cudaStreamSynchronize(s) != cudaSuccess) { return FLS_ERR_CUDA; }
+	p->measured = true;
+	return FLS_OK;
 }
 
 int fls_string_plan_decode(const fls_string_plan* p, uint32_t* d_offsets, uint8_t* d_bytes, uint64_t bytes_cap,
@@ -352,7 +358,12 @@ int fls_string_plan_decode(const fls_string_plan* p, uint32_t* d_offsets, uint8_
 	if (!p || !d_offsets || (!d_bytes && bytes_cap)) { return FLS_ERR_ARG; }
 	if ((reinterpret_cast<uintptr_t>(d_bytes) & 15u) != 0 || bytes_cap >= (1ull << 32)) { return FLS_ERR_ARG; }
 	cudaStream_t s  = static_cast<cudaStream_t>(stream);
-	int          rc = run_totals(p, s);
+	// the totals of a measure() just before (complete: measure synchronised its stream) are still valid; a
+	// decode captured into a graph always computes its own (each replay must)
+	cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+	if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) { return FLS_ERR_CUDA; }
+	int rc      = p->measured && cs == cudaStreamCaptureStatusNone ? FLS_OK : run_totals(p, s);
+	p->measured = false;
 	if (rc != FLS_OK) { return rc; }
 	if (p->args.col.n_vec == 0) {
 		return cudaMemsetAsync(d_offsets, 0, 4, s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;

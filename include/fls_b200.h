@@ -305,7 +305,8 @@ int fls_string_plan_create(const uint8_t* d_page, uint64_t page_size, const uint
 int fls_string_plan_rows(const fls_string_plan* plan, uint64_t* n_rows);
 /* Total decoded bytes (runs the length pass; synchronises the stream). */
 int fls_string_plan_measure(fls_string_plan* plan, uint64_t* n_bytes, fls_stream_t stream);
-/* d_offsets: n_rows + 1 entries; d_bytes: 16-byte aligned, bytes_cap < 4 GiB.  Asynchronous, no allocation. */
+/* d_offsets: n_rows + 1 entries; d_bytes: 16-byte aligned, bytes_cap < 4 GiB.  Asynchronous, no allocation.
+ * Runs the length pass itself unless a measure() came just before (whose totals it then takes over). */
 int fls_string_plan_decode(const fls_string_plan* plan, uint32_t* d_offsets, uint8_t* d_bytes, uint64_t bytes_cap,
                            fls_stream_t stream);
 int fls_string_plan_destroy(fls_string_plan* plan);

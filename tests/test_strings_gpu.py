@@ -172,3 +172,26 @@ def test_fsst12_malformed_tables_are_refused(cuda, col_golden):
         db, dp = _dev(d, cuda, 0)
         with pytest.raises(FlsError):
             StringPlan(pp, page.size, dp, d.size)
+
+
+def test_decode_after_measure_and_alone_agree(cuda, col_golden):
+    """decode() straight after measure() reuses the measured vector totals; decode() alone recomputes them; both
+    give the reference's rows (DICT FFOR page, string pool id 3)."""
+    import torch
+
+    from fastlanes_b200.strings import StringPlan
+
+    page, dic = col_golden["str_3_page"], col_golden["str_3_dict"]
+    want_o, want_b = _expected(col_golden, 3)
+    pb, pp = _dev(page, cuda, 0)
+    db, dp = _dev(dic, cuda, 0)
+    plan = StringPlan(pp, page.size, dp, dic.size)
+    n = plan.measure()
+    assert n == want_b.size
+    for _ in range(3):  # after measure, then twice without
+        offs = torch.empty(plan.n_rows + 1, dtype=torch.int32, device=cuda)
+        data = torch.empty(n + 16, dtype=torch.uint8, device=cuda)
+        plan.decode_into(offs, data)
+        assert np.array_equal(offs.cpu().numpy().astype(np.uint64), want_o)
+        assert np.array_equal(data[:n].cpu().numpy(), want_b)
+    plan.close()
