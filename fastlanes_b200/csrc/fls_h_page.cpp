@@ -406,27 +406,16 @@ static int describe_pages(const fls_page_column* cols, uint32_t n_cols, std::vec
 	return FLS_OK;
 }
 
-int fls_gpu_decode_pages(const fls_page_column* cols, uint32_t n_cols, fls_stream_t stream) {
-	std::vector<ColDesc>  descs;
-	std::vector<uint32_t> queue;
-	Family                fam = Family::NUM;
-	cudaStream_t          s   = static_cast<cudaStream_t>(stream);
-	std::vector<void*>    owned;
-	struct Free {
-		std::vector<void*>& v;
-		cudaStream_t        s;
-		~Free() {
-			for (void* p : v) { cudaFreeAsync(p, s); }
-		}
-	} free_owned {owned, s};
-	int rc = describe_pages(cols, n_cols, &descs, &queue, &fam, s, &owned);
-	if (rc != FLS_OK) { return rc; }
+// One decode of described work items: one launch per item class (plain, patched, gathers) on its own kernel,
+// the descriptors and the queue copied in on the stream (a single descriptor needs neither).
+static int launch_described(const std::vector<ColDesc>& descs, const std::vector<uint32_t>& queue, cudaStream_t s) {
 	if (queue.empty()) { return FLS_OK; }
 	DecodeArgs a {};
 	a.col_shift = kPageShift;
-	Segments sg; // the queue is class-ordered above; an unordered one would run on the catch-all kernel
+	Segments sg; // the queue is class-ordered by describe_pages; an unordered one runs on the catch-all kernel
 	plan_segments(descs, queue, kPageShift, &sg);
-	if (descs.size() == 1) {
+	if (descs.size() == 1 && queue.front() == 0 && queue.back() + 1 == queue.size()) {
+		// one descriptor, every vector: the queue is implicit (item v = vector v)
 		a.col0    = descs[0];
 		a.n_items = queue.size();
 		return launch_decode(sg.fam[0], a, s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
@@ -449,6 +438,61 @@ int fls_gpu_decode_pages(const fls_page_column* cols, uint32_t n_cols, fls_strea
 	cudaFreeAsync(d_queue, s);
 	return e == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
 }
+
+int fls_gpu_decode_pages(const fls_page_column* cols, uint32_t n_cols, fls_stream_t stream) {
+	std::vector<ColDesc>  descs;
+	std::vector<uint32_t> queue;
+	Family                fam = Family::NUM;
+	cudaStream_t          s   = static_cast<cudaStream_t>(stream);
+	std::vector<void*>    owned;
+	struct Free {
+		std::vector<void*>& v;
+		cudaStream_t        s;
+		~Free() {
+			for (void* p : v) { cudaFreeAsync(p, s); }
+		}
+	} free_owned {owned, s};
+	int rc = describe_pages(cols, n_cols, &descs, &queue, &fam, s, &owned);
+	if (rc != FLS_OK) { return rc; }
+	return launch_described(descs, queue, s);
+}
+
+// Vectors [first_vec, first_vec + n_vec) of one page (random access by vector, as the reference's
+// Reader::get_chunk, src/reader/reader.cpp:19-61, and its declared random_access, include/fastlanes.h:88-106):
+// the page's metadata and any whole-page buffer (rec buffers, a patched DICT's code stream) are decoded as for
+// the whole page, then only the range's work items run; vector first_vec + i lands at d_out + i * 1024 values.
+int fls_gpu_decode_page_vectors(const fls_page_column* col, uint32_t first_vec, uint32_t n_vec, fls_stream_t stream) {
+	if (!col) { return FLS_ERR_ARG; }
+	std::vector<ColDesc>  descs;
+	std::vector<uint32_t> queue, col_desc(1);
+	Family                fam = Family::NUM;
+	cudaStream_t          s   = static_cast<cudaStream_t>(stream);
+	std::vector<void*>    owned;
+	struct Free {
+		std::vector<void*>& v;
+		cudaStream_t        s;
+		~Free() {
+			for (void* p : v) { cudaFreeAsync(p, s); }
+		}
+	} free_owned {owned, s};
+	int rc = describe_pages(col, 1, &descs, &queue, &fam, s, &owned, &col_desc);
+	if (rc != FLS_OK) { return rc; }
+	ColDesc&       out = descs[col_desc[0]];
+	const uint64_t end = static_cast<uint64_t>(first_vec) + n_vec;
+	if (end > out.n_vec) { return FLS_ERR_ARG; }
+	// the output descriptor writes vector v at out + v * 1024 * e: shift its base so that first_vec lands at
+	// d_out (only addresses of the range are ever formed from it)
+	out.out = reinterpret_cast<uint8_t*>(reinterpret_cast<uintptr_t>(out.out) -
+	                                     static_cast<uintptr_t>(first_vec) * 1024u * out.e);
+	std::vector<uint32_t> part;
+	part.reserve(static_cast<size_t>(n_vec) * 2);
+	for (const uint32_t it : queue) {
+		const uint32_t v = it & ((1u << kPageShift) - 1u);
+		if (v >= first_vec && v < end) { part.push_back(it); }
+	}
+	return launch_described(descs, part, s);
+}
+
 
 int fls_plan_create_filter(const fls_page_column* cols, uint32_t n_cols, const fls_predicate* pred,
                            fls_plan** out_plan) {

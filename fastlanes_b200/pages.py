@@ -20,6 +20,8 @@ class PageColumn(ctypes.Structure):
 
 
 _decode_pages = declare("fls_gpu_decode_pages", ctypes.c_int, [ctypes.POINTER(PageColumn), ctypes.c_uint32, _p])
+_decode_vectors = declare("fls_gpu_decode_page_vectors", ctypes.c_int, [ctypes.POINTER(PageColumn), ctypes.c_uint32,
+                                                                        ctypes.c_uint32, _p])
 _page_info = declare("fls_page_info", ctypes.c_int, [_p, _u64, ctypes.POINTER(ctypes.c_uint32),
                                                      ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32),
                                                      ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(_u64)])
@@ -182,6 +184,14 @@ def decode_pages(columns, stream=None):
         a.data_type, a.order, a.d_out = c["data_type"], c.get("order", 1), c["d_out"]
     s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
     check(_decode_pages(arr, len(columns), s), "fls_gpu_decode_pages")
+
+
+def decode_page_vectors(column, first_vec, n_vec, stream=None):
+    """Vectors [first_vec, first_vec + n_vec) of one page into column["d_out"] (fls_gpu_decode_page_vectors)."""
+    import torch
+
+    s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    check(_decode_vectors(_columns([column]), first_vec, n_vec, s), "fls_gpu_decode_page_vectors")
 
 
 def encode_from_memory(values, data_type, expr_id, capacity=None):

@@ -214,6 +214,11 @@ int fls_page_info(const uint8_t* page_prefix, uint64_t prefix_size, uint32_t* ex
  * 16-byte boundary. */
 int fls_page_placement(const uint8_t* page_prefix, uint64_t prefix_size, uint32_t* shift);
 int fls_gpu_decode_pages(const fls_page_column* cols, uint32_t n_cols, fls_stream_t stream);
+/* Random access by vector: vectors [first_vec, first_vec + n_vec) of one page, vector first_vec + i written at
+ * col->d_out + i * 1024 values (the reference's Reader::get_chunk, src/reader/reader.cpp:19-61, and the
+ * random_access it declares but never defines, include/fastlanes.h:88-106).  Page-wide buffers (rec buffers,
+ * a patched DICT's code stream) are decoded whole; FLS_ERR_ARG for a range past the page's vectors. */
+int fls_gpu_decode_page_vectors(const fls_page_column* col, uint32_t first_vec, uint32_t n_vec, fls_stream_t stream);
 /* fls_gpu_decode_pages reads each page header in stream order on `stream` (it synchronises that stream once).
  * The same decode as a plan: page metadata is read once here (on the legacy default stream, so the pages must
  * already be in place); fls_plan_decode then only launches.  Replaces

@@ -388,3 +388,34 @@ def test_double_dictionary_too_short_is_refused(cuda, col_golden):
     with pytest.raises(FlsError):
         pages.decode_pages([dict(d_page=pptr, page_size=page.size, d_dict=dptr, dict_size=short.size,
                                  data_type=pages.DOUBLE, order=1, d_out=out.data_ptr())])
+
+
+@pytest.mark.parametrize("key", ["i64_11", "i64_6", "i64_17", "i64_27", "i64rec_9", "i64rec_16", "i64patch_13",
+                                 "i64dpatch_25", "i64frq_33", "f64_22"])
+def test_page_vector_ranges(cuda, col_golden, key):
+    """Random access by vector: every range decodes to the same values as the whole page, for plain, DELTA,
+    RLE, DICT, DICT_RLE, rec-compressed, patched and two-step (patched DICT codes) pages."""
+    import torch
+
+    from fastlanes_b200 import pages
+    from fastlanes_b200 import primitives as P
+    from fastlanes_b200._lib import FlsError
+
+    page = col_golden[f"{key}_page"]
+    dic = col_golden[f"{key}_dict"] if f"{key}_dict" in col_golden.files else np.zeros(0, np.uint8)
+    want = col_golden[f"{key}_input"].view(np.uint64)
+    dt = pages.DOUBLE if key.startswith("f64") else pages.INT64
+    pbuf, pptr = _dev_bytes(page, cuda, 3)
+    dbuf, dptr = _dev_bytes(dic, cuda, 1) if dic.size else (None, 0)
+    n_vec = want.size // 1024
+    for first, n in [(0, n_vec), (n_vec - 1, 1), (1, n_vec - 2), (n_vec // 2, 1), (0, 0)]:
+        out = torch.full((max(n, 1) * 1024 + 1024,), 7, dtype=torch.int64, device=cuda)
+        pages.decode_page_vectors(dict(d_page=pptr, page_size=page.size, d_dict=dptr, dict_size=dic.size,
+                                       data_type=dt, order=1, d_out=out.data_ptr()), first, n)
+        got = out.cpu().numpy().view(np.uint64)
+        assert np.array_equal(got[:n * 1024], want[first * 1024:(first + n) * 1024]), (key, first, n)
+        assert np.all(got[n * 1024:] == 7)  # nothing written past the range
+    with pytest.raises(FlsError):
+        pages.decode_page_vectors(dict(d_page=pptr, page_size=page.size, d_dict=dptr, dict_size=dic.size,
+                                       data_type=dt, order=1, d_out=out.data_ptr()), n_vec - 1, 2)
+    assert P.device_status() == 0
