@@ -509,8 +509,9 @@ def mixed_rowgroups(dev, peak, steps):
     graph = torch.cuda.CUDAGraph()
     side = [torch.cuda.Stream() for _ in range(8)]
     with torch.cuda.graph(graph):
-        ss.decode(side)  # the string columns on eight branches of the graph
-        rg.decode(graph=False)
+        ss.decode(side, join=False)  # the string columns on eight branches of the graph ...
+        rg.decode(graph=False)  # ... beside the integer plan's segments on the capturing stream
+        ss.join(side)
     graph.replay()
     torch.cuda.synchronize()
     ok = ok and all(torch.equal(o, t) for o, (t, _) in zip(rg.outputs, cols)) and ss.check(str_cols, 64, 9)
@@ -528,7 +529,7 @@ def mixed_rowgroups(dev, peak, steps):
         "decoded_values_per_s": round(n_vals / (ms * 1e-3), 1), "bytes_per_step": read_b + write_b,
         "roofline_frac": round((read_b + write_b) / (ms * 1e-3) / 1e9 / peak, 4), "parity": bool(ok),
         "gpu_launches_per_step": len(tuned) + 3 * len(str_cols), "graph_launches_per_step": 1, "autotuned": tuned,
-        "graph": "integer plan segments + the string columns' launches on eight parallel branches",
+        "graph": "integer plan segments beside the string columns' launches on eight parallel branches",
         "integer_part": {"values": rg.values, "read_bytes": rg.page_bytes + rg.dict_bytes,
                          "written_bytes": rg.value_bytes},
         "string_part": {"rows": ss.rows, "read_bytes": ss.page_bytes + ss.dict_bytes, "written_bytes": ss.value_bytes,

@@ -154,10 +154,11 @@ class StringColumnSet:
             self.rows += plan.n_rows
             self.value_bytes += 4 * (plan.n_rows + 1) + n
 
-    def decode(self, streams=None):
+    def decode(self, streams=None, join=True):
         """Every column's decode; with `streams`, column i runs on streams[i % len(streams)], each stream
-        ordered after the current one and the current one after all of them (so the columns overlap, also
-        inside a CUDA graph capture)."""
+        ordered after the current one and (with `join`) the current one after all of them, so the columns
+        overlap, also inside a CUDA graph capture.  join=False leaves the current stream free for other work
+        that then overlaps the columns; join(streams) closes the fork."""
         if not streams:
             for plan, (offs, data, _) in zip(self.plans, self.outputs):
                 plan.decode_into(offs, data)
@@ -169,6 +170,12 @@ class StringColumnSet:
             s = streams[i % len(streams)]
             with torch.cuda.stream(s):
                 plan.decode_into(offs, data, stream=s.cuda_stream)
+        if join:
+            self.join(streams)
+
+    @staticmethod
+    def join(streams):
+        cur = torch.cuda.current_stream()
         for s in streams:
             cur.wait_stream(s)
 
