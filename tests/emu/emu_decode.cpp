@@ -4,6 +4,7 @@
 #define FLS_HOST_EMULATION 1
 #include "fls_decode.cu"
 #include "fls_page.h"
+#include "fls_strings.cuh"
 #include "fls_b200.h"
 
 #include <thread>
@@ -142,4 +143,16 @@ extern "C" int emu_filter_page(const uint8_t* page, uint64_t page_size, const ui
 	int st   = 0;
 	for (uint32_t v = 0; v < c.n_vec; ++v) { st |= emu_vector(c, v, &pr); }
 	return st;
+}
+
+// One string through the device FSST / FSST12 row decoders (fls_strings.cuh): its decoded length, and the bytes
+// written to out (the length the length pass counts must be what the materialising pass writes).
+extern "C" uint64_t emu_fsst_row(int twelve, const uint64_t* sym, const uint8_t* len, const uint8_t* in, uint32_t n,
+                                 uint8_t* out) {
+	if (twelve) {
+		fsst12_decode_to(sym, len, in, n, out);
+		return fsst12_decoded_len(len, in, n);
+	}
+	fsst_decode_to(sym, len, in, n, out);
+	return fsst_decoded_len(len, in, n);
 }

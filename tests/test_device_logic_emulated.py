@@ -169,3 +169,40 @@ def test_emulated_reference_patched_pages(emu, col_golden, eid, order):
         tw = np.concatenate([oracle.transpose_i(want.view(np.uint64)[v * 1024:(v + 1) * 1024]) for v in
                              range(want.size // 1024)]).view(np.int64)
         assert np.array_equal(out, tw)
+
+
+def _emu_row(emu, twelve, sym, ln, data):
+    data = np.ascontiguousarray(data, np.uint8)
+    out = np.zeros(8 * data.size + 16, np.uint8)
+    emu.emu_fsst_row.restype = ctypes.c_uint64
+    n = emu.emu_fsst_row(int(twelve), P(sym), P(ln), P(data if data.size else np.zeros(1, np.uint8)),
+                         ctypes.c_uint32(data.size), P(out))
+    return out[:n].copy()
+
+
+@pytest.mark.parametrize("eid", [13, 28])
+def test_emulated_fsst_rows_match_oracle(emu, col_golden, eid):
+    """The device FSST (pool id 13) and FSST12 (id 28) row decoders, compiled as host code: every row of the
+    reference's page, and random byte strings of every length 0..40 (escapes, trailing lone FSST12 bytes,
+    codes past the symbol count), decode as the oracle does; the length the lengths pass counts equals the
+    bytes written."""
+    from oracle import pages
+
+    twelve = eid == 28
+    page, dic = col_golden[f"str_{eid}_page"], col_golden[f"str_{eid}_dict"]
+    table = oracle.fsst12_decode_table if twelve else oracle.fsst_decode_table
+    dec = oracle.fsst12_decode if twelve else oracle.fsst_decode
+    _, sym, ln = table(dic[8:])
+    pg = pages.parse_page(page)
+    for v in range(pg.vec_c):
+        data = pg.vector_slice(v, 0)
+        ends = oracle.untranspose_i(np.frombuffer(pg.vector_slice(v, 1, 4096).tobytes(), np.uint32).copy())
+        start = 0
+        for i in range(1024):
+            row = data[start:ends[i]]
+            assert np.array_equal(_emu_row(emu, twelve, sym, ln, row), dec(sym, ln, row)), (v, i)
+            start = ends[i]
+    rng = np.random.default_rng(eid)
+    for n in list(range(41)) * 20:
+        row = rng.integers(0, 256, n, dtype=np.uint8)
+        assert np.array_equal(_emu_row(emu, twelve, sym, ln, row), dec(sym, ln, row)), n
