@@ -450,8 +450,43 @@ def other_configs(dev, args):
     so[1:] = np.cumsum(sl)
     sb = np.concatenate([dbytes[int(doffs[c]):int(doffs[c + 1])] for c in sc])
     out["4_dict_fsst_str"]["cpu_baseline"] = cpu_column_leg(("str", 3), strings=(sb, so))
+    del data_t, offs_t, pb, db
+
+    # 4b: the same rows as an FSST column (string pool id 13): every row FSST-decoded from the page (row a10)
+    try:
+        fsst_leg(dev, codes.size, steps, leg, out)
+    except Exception as e:  # a failed leg is reported, the other legs still count
+        out["4b_fsst_str"] = {"error": f"{type(e).__name__}: {e}"}
     out["5_mixed_select"] = mixed_rowgroups(dev, peak, steps)
     return out
+
+
+def fsst_leg(dev, n_rows, steps, leg, out):
+    import torch
+
+    from fastlanes_b200 import strings as S
+    from fastlanes_b200 import workloads as W
+
+    codes_n = n_rows
+    table, cb, co, pbytes, poffs = W.fsst_rows(codes_n)
+    page, dic = S.fsst_page(table, cb, co)
+    pg_d = torch.from_numpy(page).to(dev)
+    dc_d = torch.from_numpy(dic).to(dev)
+    plan = S.StringPlan(pg_d.data_ptr(), page.size, dc_d.data_ptr(), dic.size)
+    n_bytes = plan.measure()
+    offs_t = torch.empty(plan.n_rows + 1, dtype=torch.int32, device=dev)
+    data_t = torch.empty(n_bytes + 16, dtype=torch.uint8, device=dev)
+    plan.decode_into(offs_t, data_t)
+    ok = n_bytes == pbytes.size and torch.equal(offs_t.long().cpu(), torch.from_numpy(poffs.astype(np.int64)))
+    ok = ok and torch.equal(data_t[:n_bytes], torch.from_numpy(pbytes).to(dev))
+    ms = device_timed(lambda: plan.decode_into(offs_t, data_t), steps, 3)
+    leg("4b_fsst_str", f"the same {codes_n} rows as an FSST column (string pool id 13), one symbol table",
+        ms, page.size + dic.size, 4 * (codes_n + 1) + n_bytes, codes_n, ok, 3)
+    plan.close()
+    del data_t, offs_t, pg_d, dc_d
+    fo = np.zeros((1 << 18) + 1, np.uint64)
+    fo[1:] = poffs[1:(1 << 18) + 1]
+    out["4b_fsst_str"]["cpu_baseline"] = cpu_column_leg(("str", 13), strings=(pbytes[:int(fo[-1])], fo))
 
 
 def mixed_rowgroups(dev, peak, steps):

@@ -106,3 +106,52 @@ def encode_string_dict(dict_bytes, dict_offsets, codes):
                     _np_ptr(page), page.size, ctypes.byref(ps), _np_ptr(dic), dic.size, ctypes.byref(ds)),
           "fls_encode_string_dict")
     return page[: ps.value].copy(), dic[: ds.value].copy()
+
+
+def _transposed_order():
+    """Index array of the unified transposed layout: transposed[k] = original[idx[k]]."""
+    import numpy as np
+
+    k = np.arange(1024)
+    order = np.array([0, 4, 2, 6, 1, 5, 3, 7])
+    return (k % 16) * 64 + order[(k // 16) % 8] * 8 + k // 128
+
+
+def encode_fsst_page(byts, offsets):
+    """FSST column page (string pool expression 13, FSST UNCOMPRESSED) of n strings, n a multiple of 1024, and its
+    dictionary page (dict_hdr_t + the exported symbol table).  Layout as the reference writes it
+    (src/cor/lyt/vec.cpp:162-207): per vector its compressed bytes (buffer 0) and its 1024 cumulative END offsets
+    within them, u32, transposed (buffer 1); entry points per vector after the first."""
+    import numpy as np
+
+    table, comp, coffs = fsst_compress(byts, offsets)
+    return fsst_page(table, comp, coffs)
+
+
+def fsst_page(table, comp, coffs):
+    """The FSST column page and dictionary page of strings already compressed with `table` (fsst_compress's
+    outputs: compressed bytes and their offsets[n + 1], n a multiple of 1024)."""
+    import numpy as np
+
+    coffs = np.ascontiguousarray(coffs, np.uint64)
+    n = coffs.size - 1
+    if n % 1024:
+        raise ValueError("fsst_page: whole vectors only")
+    vec_c = n // 1024
+    if vec_c >= 1 << 16:
+        raise ValueError("fsst_page: at most 65535 vectors")
+    starts = coffs[0:n:1024]
+    ends = (coffs[1:].reshape(vec_c, 1024) - starts[:, None]).astype(np.uint32)
+    ends_t = ends[:, _transposed_order()]
+    meta = 8 + 2 * 4 + 2 * 4 * max(vec_c - 1, 0)
+    b0 = comp.size
+    hdr = np.zeros(meta, np.uint8)
+    hdr[0], hdr[1] = 7, 1
+    hdr[4:6] = np.frombuffer(np.uint16(vec_c).tobytes(), np.uint8)
+    hdr[8:16] = np.frombuffer(np.array([meta, meta + b0], np.uint32).tobytes(), np.uint8)
+    if vec_c > 1:
+        ep = np.stack([starts[1:].astype(np.uint32), (np.arange(1, vec_c) * 4096).astype(np.uint32)], axis=1)
+        hdr[16:] = np.frombuffer(ep.astype("<u4").tobytes(), np.uint8)
+    page = np.concatenate([hdr, comp, np.frombuffer(ends_t.astype("<u4").tobytes(), np.uint8)])
+    dic = np.concatenate([np.array([7, 0, 0, 0, 0, 0, 0, 0], np.uint8), table])
+    return page, dic

@@ -297,3 +297,27 @@ def mixed_rowgroup_columns(rng, n_cols=256, device="cuda", min_vec=64, max_vec=4
                "dict": "dict_i32"}[kind]
         ints.append(selection_column(rng, n_vec, device, fam))
     return ints, strs
+
+
+def fsst_rows(n_rows=8 << 20, seed=0):
+    """The string column of the DICT+FSST configuration (dictionary strings picked by Zipf(1.1) codes) as an FSST
+    column: every row FSST-compressed with one symbol table, built as the dictionary entries compressed once and
+    gathered by code (the same bytes as compressing each row with that table).  Returns (table, compressed
+    bytes, compressed offsets[n + 1], plain bytes, plain offsets[n + 1])."""
+    from .strings import fsst_compress
+
+    dbytes, doffs = string_dictionary(seed)
+    codes = zipf_codes(n_rows, seed=seed)
+    table, comp, coffs = fsst_compress(dbytes, doffs)
+
+    def gather(src, offs):
+        lens = np.diff(offs).astype(np.int64)[codes]
+        out_offs = np.zeros(codes.size + 1, np.uint64)
+        out_offs[1:] = np.cumsum(lens)
+        idx = np.repeat(offs[:-1][codes].astype(np.int64) - out_offs[:-1].astype(np.int64), lens)
+        idx += np.arange(idx.size, dtype=np.int64)
+        return src[idx], out_offs
+
+    cb, co = gather(comp, coffs.astype(np.uint64))
+    pb, po = gather(dbytes, doffs.astype(np.uint64))
+    return table, cb, co, pb, po

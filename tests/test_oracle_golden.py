@@ -196,3 +196,29 @@ def test_page_oracle_decodes_reference_double_pages(col_golden, eid):
     page, dic = col_golden[f"f64_{eid}_page"], col_golden[f"f64_{eid}_dict"]
     got = pages.decode_int(page, dic if dic.size else None, np.uint64, raw_dict=True)
     assert np.array_equal(got, col_golden[f"f64_{eid}_input"].view(np.uint64))
+
+
+def test_fsst_column_page_writer_round_trips(col_golden):
+    """The engine's FSST column page writer (strings.encode_fsst_page, host only) lays pages out as the
+    reference does: same header and buffer structure as the reference's FSST page of the same strings, and
+    every row decodes back through the oracle's restatement of the reference decoder."""
+    from fastlanes_b200 import strings as S
+    from oracle import pages
+
+    byts, offs = col_golden["str_13_input_bytes"], col_golden["str_13_input_offsets"]
+    page, dic = S.encode_fsst_page(byts, offs)
+    ref = pages.parse_page(col_golden["str_13_page"])
+    pg = pages.parse_page(page)
+    assert (pg.exp_t, pg.var, pg.vec_c, pg.arr_c) == (ref.exp_t, ref.var, ref.vec_c, ref.arr_c)
+    assert dic[0] == col_golden["str_13_dict"][0]
+    _, sym, ln = oracle.fsst_decode_table(dic[8:])
+    row = 0
+    for v in range(pg.vec_c):
+        assert pg.vector_slice(v, 1).size == 4096
+        data = pg.vector_slice(v, 0)
+        ends = oracle.untranspose_i(np.frombuffer(pg.vector_slice(v, 1, 4096).tobytes(), np.uint32).copy())
+        start = 0
+        for i in range(1024):
+            assert np.array_equal(oracle.fsst_decode(sym, ln, data[start:ends[i]]), byts[offs[row]:offs[row + 1]])
+            start = ends[i]
+            row += 1
