@@ -154,8 +154,31 @@ def case_select(a):
     return res
 
 
+def case_fsst(a):
+    """The DICT+FSST configuration's rows as an FSST column (string pool id 13)."""
+    from . import strings as S
+    from . import workloads as W
+
+    table, cb, co, pbytes, poffs = W.fsst_rows(a.rows)
+    page, dic = S.fsst_page(table, cb, co)
+    pg = torch.from_numpy(page).cuda()
+    dc = torch.from_numpy(dic).cuda()
+    plan = S.StringPlan(pg.data_ptr(), page.size, dc.data_ptr(), dic.size)
+    n = plan.measure()
+    offs = torch.empty(plan.n_rows + 1, dtype=torch.int32, device="cuda")
+    data = torch.empty(n + 16, dtype=torch.uint8, device="cuda")
+    plan.decode_into(offs, data)
+    if n != pbytes.size or not np.array_equal(offs.cpu().numpy().astype(np.int64), poffs.astype(np.int64)):
+        raise SystemExit("fsst: offsets mismatch")
+    if not torch.equal(data[:n], torch.from_numpy(pbytes).cuda()):
+        raise SystemExit("fsst: bytes mismatch")
+    ms = _timed(lambda: plan.decode_into(offs, data), a.reps)
+    plan.close()
+    return f"fsst rows={a.rows} bytes={n} compressed={cb.size} ms={ms:.4f}"
+
+
 CASES = {"strings": case_strings, "rle": case_rle, "delta": case_delta, "mixed": case_mixed, "select": case_select,
-         "filter": case_filter}
+         "filter": case_filter, "fsst": case_fsst}
 
 
 def main(argv=None):
