@@ -336,7 +336,8 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 	PlanS*   plans = reinterpret_cast<PlanS*>(wbase);
 	uint8_t* buf   = wbase + kStrPB * 64;
 	uint8_t* win   = buf + str_rows_bytes(R16);
-	constexpr bool kOr  = PASS == STR_PASS_MATERIALIZE && KIND != STR_FSST && KIND != STR_FSST12;
+	// kOr: rows go to the window as whole words (put_row, fsst_put_row); FSST12 rows as bytes
+	constexpr bool kOr  = PASS == STR_PASS_MATERIALIZE && KIND != STR_FSST12;
 	uint32_t*      win32 = reinterpret_cast<uint32_t*>(win);
 	__syncthreads();
 
@@ -451,6 +452,8 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 							// the decoded dictionary starts 16-byte aligned (shared or global memory)
 							mid = put_row(win32, fill + (o - vpos), reinterpret_cast<const uint32_t*>(dict), f.start,
 							              f.len, &hk, &head);
+						} else if constexpr (KIND == STR_FSST) {
+							mid = fsst_put_row(win32, fill + (o - vpos), fsym, flen, vb + f.start, f.clen, &hk, &head);
 						} else {
 							const uintptr_t va = reinterpret_cast<uintptr_t>(vb);
 							mid = put_row(win32, fill + (o - vpos), reinterpret_cast<const uint32_t*>(va & ~uintptr_t(3)),
@@ -458,10 +461,8 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 						}
 						__syncwarp(); // every word's whole store lands before the rows that start inside it OR in
 						if (mid) { atomicOr(win32 + hk, head); }
-					} else if constexpr (KIND == STR_FSST12) {
-						fsst12_decode_to(fsym, flen, vb + f.start, f.clen, win + fill + (o - vpos));
 					} else {
-						fsst_decode_to(fsym, flen, vb + f.start, f.clen, win + fill + (o - vpos));
+						fsst12_decode_to(fsym, flen, vb + f.start, f.clen, win + fill + (o - vpos));
 					}
 					fill += T;
 				} else {

@@ -57,6 +57,59 @@ __device__ __forceinline__ void fsst_decode_to(const uint64_t* sym, const uint8_
 	}
 }
 
+// Decode one FSST-compressed string into the word array `win` at byte offset d, whole 32-bit words: the
+// decoded bytes gather in a bit accumulator and leave as word stores, every word stored by the row that owns
+// its first byte, bytes past the row's end zero (the protocol of the string kernels' window).  A row that
+// starts inside a word returns its bytes of that word instead (*hk, *head) for an atomic OR once every lane's
+// stores are done.  The bytes are those of fsst_decode_to, an escape at the string's end giving a zero byte.
+__device__ __forceinline__ bool fsst_put_row(uint32_t* win, uint32_t d, const uint64_t* sym, const uint8_t* len,
+                                             const uint8_t* in, uint32_t n, uint32_t* hk, uint32_t* head) {
+	const uint32_t k0  = d >> 2;
+	const bool     mid = (d & 3u) != 0;
+	uint32_t       k   = k0;
+	uint32_t       nb  = 8u * (d & 3u); // bits of word k below the next byte (earlier rows' bytes stay zero)
+	uint64_t       acc = 0;             // bits of words k, k + 1 (byte 4k at bit 0)
+	uint32_t       hi  = 0;             // bits of word k + 2
+	bool           any = false, held = false;
+	auto emit = [&](uint32_t w) {
+		if (k == k0 && mid) {
+			*hk  = k;
+			*head = w;
+			held  = true;
+		} else {
+			win[k] = w;
+		}
+		++k;
+	};
+	for (uint32_t i = 0; i < n; ++i) {
+		const uint8_t c = in[i];
+		uint64_t      s;
+		uint32_t      l;
+		if (c == 255) {
+			s = i + 1 < n ? in[i + 1] : 0u;
+			l = 1;
+			++i;
+		} else {
+			s = sym[c];
+			l = len[c];
+		}
+		if (l == 0) { continue; }
+		any = true;
+		// nb < 32 here: the symbol's up to 64 bits land in bits [nb, nb + 8l) of acc and hi
+		acc |= s << nb;
+		if (nb) { hi |= static_cast<uint32_t>(s >> (64u - nb)); }
+		nb += 8u * l;
+		while (nb >= 32u) {
+			emit(static_cast<uint32_t>(acc));
+			acc = (acc >> 32) | (static_cast<uint64_t>(hi) << 32);
+			hi  = 0;
+			nb -= 32u;
+		}
+	}
+	if (any && nb > 8u * ((k == k0) ? (d & 3u) : 0u)) { emit(static_cast<uint32_t>(acc)); }
+	return held;
+}
+
 // Decoded length of one FSST12-compressed string.  A trailing single byte (which the encoder never writes)
 // decodes as the code of its 8 bits; the reference's decoder reads the byte after the string there.
 __device__ __forceinline__ uint32_t fsst12_decoded_len(const uint8_t* len, const uint8_t* in, uint32_t n) {

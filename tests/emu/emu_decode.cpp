@@ -156,3 +156,22 @@ extern "C" uint64_t emu_fsst_row(int twelve, const uint64_t* sym, const uint8_t*
 	fsst_decode_to(sym, len, in, n, out);
 	return fsst_decoded_len(len, in, n);
 }
+
+// A run of FSST rows written to a word window with the string kernels' protocol: the word the first row
+// starts in is zeroed, every row's whole words are stored, then the held heads are OR-ed in.  Returns the
+// bytes written (the sum of the rows' decoded lengths).
+extern "C" uint64_t emu_fsst_put_rows(const uint64_t* sym, const uint8_t* len, const uint8_t* comp,
+                                      const uint64_t* coffs, uint32_t n, uint32_t d0, uint32_t* win) {
+	win[d0 >> 2]   = 0;
+	uint32_t d     = d0;
+	std::vector<std::pair<uint32_t, uint32_t>> heads;
+	for (uint32_t r = 0; r < n; ++r) {
+		const uint8_t* in = comp + coffs[r];
+		const uint32_t cn = static_cast<uint32_t>(coffs[r + 1] - coffs[r]);
+		uint32_t       hk = 0, head = 0;
+		if (fsst_put_row(win, d, sym, len, in, cn, &hk, &head)) { heads.emplace_back(hk, head); }
+		d += fsst_decoded_len(len, in, cn);
+	}
+	for (const auto& h : heads) { win[h.first] |= h.second; }
+	return d - d0;
+}

@@ -206,3 +206,39 @@ def test_emulated_fsst_rows_match_oracle(emu, col_golden, eid):
     for n in list(range(41)) * 20:
         row = rng.integers(0, 256, n, dtype=np.uint8)
         assert np.array_equal(_emu_row(emu, twelve, sym, ln, row), dec(sym, ln, row)), n
+
+
+@pytest.mark.parametrize("d0", [0, 1, 2, 3, 6])
+def test_emulated_fsst_whole_word_rows(emu, col_golden, d0):
+    """fsst_put_row (the FSST materialising pass's row writer) on a window full of garbage: a vector's rows
+    written one after another from byte d0 reproduce the oracle's bytes exactly, nothing before d0 in the first
+    word but zeros, and the last word zero past the end (the next rows OR into it)."""
+    from oracle import pages
+
+    page, dic = col_golden["str_13_page"], col_golden["str_13_dict"]
+    _, sym, ln = oracle.fsst_decode_table(dic[8:])
+    pg = pages.parse_page(page)
+    rng = np.random.default_rng(d0)
+    for v in range(pg.vec_c):
+        data = np.ascontiguousarray(pg.vector_slice(v, 0))
+        ends = oracle.untranspose_i(np.frombuffer(pg.vector_slice(v, 1, 4096).tobytes(), np.uint32).copy())
+        starts = np.concatenate([[0], ends[:-1]])
+        rows = [oracle.fsst_decode(sym, ln, data[s:e]) for s, e in zip(starts, ends)]
+        # plus rows with escapes, an escape at the very end, and empty rows
+        extra = [np.array([255, 65, 1, 255], np.uint8), np.zeros(0, np.uint8), np.array([255], np.uint8)]
+        comp = np.concatenate([data[s:e] for s, e in zip(starts, ends)] + extra)
+        lens = np.concatenate([np.asarray(ends) - np.asarray(starts), [e.size for e in extra]]).astype(np.uint64)
+        coffs = np.zeros(lens.size + 1, np.uint64)
+        coffs[1:] = np.cumsum(lens)
+        rows += [oracle.fsst_decode(sym, ln, e) for e in extra]
+        want = np.concatenate(rows)
+        win = rng.integers(0, 1 << 32, (d0 + want.size) // 4 + 64, dtype=np.uint64).astype(np.uint32)
+        emu.emu_fsst_put_rows.restype = ctypes.c_uint64
+        n = emu.emu_fsst_put_rows(P(sym), P(ln), P(comp), P(coffs), ctypes.c_uint32(lens.size), ctypes.c_uint32(d0),
+                                  P(win))
+        got = win.view(np.uint8)
+        assert n == want.size
+        assert np.array_equal(got[d0:d0 + n], want), v
+        assert not got[(d0 // 4) * 4:d0].any()
+        end = d0 + n
+        assert not got[end:(end + 3) // 4 * 4].any()
