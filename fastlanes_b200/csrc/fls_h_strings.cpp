@@ -150,6 +150,7 @@ struct fls_string_plan {
 	DevArr<uint64_t>         vec_total;
 	DevArr<uint64_t>         vec_base;
 	DevArr<uint32_t>         codes; // patched DICT pages: their decoded code stream
+	DevArr<uint32_t>         row_len; // FSST / FSST12 pages: every row's decoded length
 	uint32_t                 dyn_smem = 0;
 	int                      warps    = 0; // warps per CTA of the materialising kernel
 	uint64_t                 n_rows   = 0;
@@ -223,6 +224,10 @@ int fls_string_plan_create(const uint8_t* d_page, uint64_t page_size, const uint
 	if (!p->vec_total.alloc(pi.vec_c + 1) || !p->vec_base.alloc(pi.vec_c + 1)) { return FLS_ERR_CUDA; }
 	a.vec_total = p->vec_total.p;
 	a.vec_base  = p->vec_base.p;
+	if (L->kind == STR_FSST || L->kind == STR_FSST12) {
+		if (!p->row_len.alloc(static_cast<size_t>(pi.vec_c) * 1024)) { return FLS_ERR_CUDA; }
+		a.row_len = p->row_len.p;
+	}
 	if (!p->table.alloc(1)) { return FLS_ERR_CUDA; }
 	FsstTable tab {};
 	if (L->kind == STR_FSST12) {

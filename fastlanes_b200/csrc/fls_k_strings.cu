@@ -251,7 +251,7 @@ struct RowRef {
 template <int KIND, bool R16>
 __device__ __forceinline__ RowRef row_ref(const StrArgs& a, const uint32_t* ends, const uint8_t* rows, uint32_t r,
                                           const uint8_t* vb, uint32_t vn, const uint8_t* flen, bool* bad,
-                                          const uint32_t* packed = nullptr) {
+                                          const uint32_t* packed = nullptr, const uint32_t* known_len = nullptr) {
 	RowRef f {0, 0, 0};
 	if constexpr (KIND == STR_DICT) {
 		const uint32_t code = row_at<R16>(rows, r);
@@ -279,6 +279,8 @@ __device__ __forceinline__ RowRef row_ref(const StrArgs& a, const uint32_t* ends
 		f.clen  = e - s;
 		if constexpr (KIND == STR_BYTES) {
 			f.len = f.clen;
+		} else if (known_len) {
+			f.len = known_len[r];
 		} else if constexpr (KIND == STR_FSST12) {
 			f.len = fsst12_decoded_len(flen, vb + s, f.clen);
 		} else {
@@ -374,7 +376,11 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 		bool            bad  = false;
 		if constexpr (PASS == STR_PASS_LENGTHS) {
 			uint32_t sum = 0;
-			for (uint32_t b = 0; b < kVec / 32; ++b) { sum += row_ref<KIND, R16>(a, ends, rows, 32 * b + lane, vb, vn, flen, &bad).len; }
+			for (uint32_t b = 0; b < kVec / 32; ++b) {
+				const uint32_t l = row_ref<KIND, R16>(a, ends, rows, 32 * b + lane, vb, vn, flen, &bad).len;
+				if (KIND != STR_DICT && KIND != STR_BYTES && a.row_len) { a.row_len[v * kVec + 32 * b + lane] = l; }
+				sum += l;
+			}
 			sum = warp_sum(sum);
 			if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) { atomicOr(a.status, STATUS_BAD_INDEX); }
 			if (lane == 0) { a.vec_total[v] = sum; }
@@ -434,11 +440,14 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 			uint32_t  vpos = 0; // bytes of this vector emitted so far
 			uint32_t* offs = a.offsets + v * kVec + lane;
 			// the next batch's row is looked up while the current one is copied
-			RowRef next = row_ref<KIND, R16>(a, ends, rows, lane, vb, vn, flen, &bad, a.dict_rows);
+			const uint32_t* known = a.row_len ? a.row_len + v * kVec : nullptr;
+			RowRef next = row_ref<KIND, R16>(a, ends, rows, lane, vb, vn, flen, &bad, a.dict_rows, known);
 			for (uint32_t b = 0; b < kVec / 32; ++b) {
 				const uint32_t r = 32 * b + lane;
 				const RowRef   f = next;
-				if (b + 1 < kVec / 32) { next = row_ref<KIND, R16>(a, ends, rows, r + 32, vb, vn, flen, &bad, a.dict_rows); }
+				if (b + 1 < kVec / 32) {
+					next = row_ref<KIND, R16>(a, ends, rows, r + 32, vb, vn, flen, &bad, a.dict_rows, known);
+				}
 				const uint32_t inc = warp_inclusive_scan(f.len, lane);
 				const uint32_t o   = vpos + inc - f.len;
 				const uint32_t T   = __shfl_sync(0xFFFFFFFFu, inc, 31);

@@ -44,6 +44,9 @@ struct StrArgs {
 	// materialising pass: entry c as start | length << 24 (dictionaries of < 16 MiB decoded bytes whose
 	// entries are all < 256 bytes), one load per row instead of two end offsets; null otherwise
 	const uint32_t*  dict_rows;
+	// FSST / FSST12 pages: every row's decoded length, written by the lengths pass and read by the materialising
+	// pass instead of walking the row's codes a second time (null: both walk them)
+	uint32_t*        row_len;
 	const uint8_t*   dict_bytes;
 	uint64_t         dict_bytes_n;
 	const FsstTable* table;
