@@ -303,6 +303,9 @@ int fls_file_close(fls_file* file);
  * dictionary once on the GPU (TColDecoder::ExtInitDict, src/encoder/col_encoder.cpp:198-201); decoding emits
  * Arrow-style output: n_rows + 1 u32 offsets and the concatenated bytes, rows in original order
  * (include/fls/encoder/assert_eq.hpp:166-210, :257-400).  The page and dictionary buffers must outlive the plan.
+ * Device memory a plan holds: 16 bytes per vector, the decoded dictionary (DICT kinds), a decoded code stream
+ * of 4 bytes per row (DICT pages with patched codes) or every row's decoded length, 4 bytes per row (FSST and
+ * FSST12 pages).
  * ------------------------------------------------------------------------------------------------------- */
 typedef struct fls_string_plan fls_string_plan;
 int fls_string_plan_create(const uint8_t* d_page, uint64_t page_size, const uint8_t* d_dict, uint64_t dict_size,
