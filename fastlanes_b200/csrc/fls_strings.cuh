@@ -57,6 +57,49 @@ __device__ __forceinline__ void fsst_decode_to(const uint64_t* sym, const uint8_
 	}
 }
 
+// Write the n bytes at byte offset `start` of the 4-byte aligned word array `base` to the window at byte offset
+// d.  Every window word is stored whole by the row that owns its first byte (bytes past that row's end are
+// zero in the store); a row that starts inside a word instead returns its bytes of that word (*head, word
+// *hk), for an atomic OR once every lane's stores are done.  So the window needs no zeroing, only the word
+// that the first row of a run of batches starts inside must hold zeros past the filled bytes.  Only the source
+// words that hold bytes of the row are read.  Returns whether a head is left to OR.
+__device__ __forceinline__ bool put_row(uint32_t* __restrict__ win, uint32_t d, const uint32_t* __restrict__ base,
+                                        uint32_t start, uint32_t n, uint32_t* hk, uint32_t* head) {
+	// the row is bytes [start, start + n) of the word array `base`; word indices (not pointers) keep the array's
+	// address space (shared memory for a dictionary held there)
+	if (n == 0) { return false; }
+	const int32_t  a    = static_cast<int32_t>(start) - static_cast<int32_t>(d & 3u); // lands on window byte 4*(d/4)
+	const uint32_t sh   = 8u * (static_cast<uint32_t>(a) & 3u);
+	const int32_t  s    = a >> 2;
+	const int32_t  s_lo = static_cast<int32_t>(start >> 2);
+	const int32_t  s_hi = static_cast<int32_t>((start + n - 1) >> 2);
+	const uint32_t k0 = d >> 2, k1 = (d + n - 1) >> 2;
+	const uint32_t hm = 0xFFFFFFFFu << (8u * (d & 3u));
+	const uint32_t tm = 0xFFFFFFFFu >> (8u * (3u - ((d + n - 1) & 3u)));
+	// a clamped word only feeds bytes outside the row, which the masks drop
+	uint32_t       w0  = base[s < s_lo ? s_lo : s];
+	uint32_t       w1  = base[s + 1 > s_hi ? s_hi : s + 1];
+	const uint32_t h   = __funnelshift_r(w0, w1, sh) & hm & (k0 == k1 ? tm : 0xFFFFFFFFu);
+	const bool     mid = (d & 3u) != 0;
+	if (!mid) { win[k0] = h; }
+	*hk   = k0;
+	*head = h;
+	if (k0 == k1) { return mid; }
+	const uint32_t m = k1 - k0; // words k0 + 1 .. k1 - 1 are whole row words
+	uint32_t       j = 1;
+#pragma unroll 4
+	for (; j < m; ++j) {
+		w0          = w1;
+		w1          = base[s + static_cast<int32_t>(j) + 1];
+		win[k0 + j] = __funnelshift_r(w0, w1, sh);
+	}
+	w0                = w1;
+	const int32_t lst = s + static_cast<int32_t>(m) + 1;
+	w1                = base[lst > s_hi ? s_hi : lst];
+	win[k1]           = __funnelshift_r(w0, w1, sh) & tm;
+	return mid;
+}
+
 // Decode one FSST-compressed string into the word array `win` at byte offset d, whole 32-bit words: the
 // decoded bytes gather in a bit accumulator and leave as word stores, every word stored by the row that owns
 // its first byte, bytes past the row's end zero (the protocol of the string kernels' window).  A row that

@@ -175,3 +175,19 @@ extern "C" uint64_t emu_fsst_put_rows(const uint64_t* sym, const uint8_t* len, c
 	for (const auto& h : heads) { win[h.first] |= h.second; }
 	return d - d0;
 }
+
+// A run of rows copied from the 4-byte aligned word array `base` (row r: bytes [start[r], start[r] + len[r]))
+// to a word window with the string kernels' protocol (put_row): returns the bytes written.
+extern "C" uint64_t emu_put_rows(const uint32_t* base, const uint32_t* start, const uint32_t* len, uint32_t n,
+                                 uint32_t d0, uint32_t* win) {
+	win[d0 >> 2] = 0;
+	uint32_t d   = d0;
+	std::vector<std::pair<uint32_t, uint32_t>> heads;
+	for (uint32_t r = 0; r < n; ++r) {
+		uint32_t hk = 0, head = 0;
+		if (put_row(win, d, base, start[r], len[r], &hk, &head)) { heads.emplace_back(hk, head); }
+		d += len[r];
+	}
+	for (const auto& h : heads) { win[h.first] |= h.second; }
+	return d - d0;
+}

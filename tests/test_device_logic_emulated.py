@@ -242,3 +242,27 @@ def test_emulated_fsst_whole_word_rows(emu, col_golden, d0):
         assert not got[(d0 // 4) * 4:d0].any()
         end = d0 + n
         assert not got[end:(end + 3) // 4 * 4].any()
+
+
+@pytest.mark.parametrize("d0", [0, 1, 2, 3, 5])
+def test_emulated_put_row_window_protocol(emu, d0):
+    """put_row (the DICT / BYTE_ARR materialising pass's row writer) on a window full of garbage: rows of 0..9
+    bytes (many empty or shorter than a word) and some long ones, from any source offset, written one after
+    another from byte d0 reproduce the source bytes, zeros before d0 in the first word and past the end."""
+    rng = np.random.default_rng(100 + d0)
+    src = rng.integers(0, 256, 1 << 14, dtype=np.uint8)
+    n = 2000
+    lens = rng.choice([0, 1, 2, 3, 4, 5, 7, 9, 40, 300], n, p=[.2, .15, .15, .1, .1, .1, .05, .05, .05, .05])
+    lens = lens.astype(np.uint32)
+    starts = rng.integers(0, src.size - 301, n).astype(np.uint32)
+    want = np.concatenate([src[s:s + l] for s, l in zip(starts, lens)])
+    win = rng.integers(0, 1 << 32, (d0 + want.size) // 4 + 64, dtype=np.uint64).astype(np.uint32)
+    emu.emu_put_rows.restype = ctypes.c_uint64
+    got_n = emu.emu_put_rows(P(src.view(np.uint32)), P(starts), P(lens), ctypes.c_uint32(n), ctypes.c_uint32(d0),
+                             P(win))
+    got = win.view(np.uint8)
+    assert got_n == want.size
+    assert np.array_equal(got[d0:d0 + want.size], want)
+    assert not got[(d0 // 4) * 4:d0].any()
+    end = d0 + want.size
+    assert not got[end:(end + 3) // 4 * 4].any()
