@@ -22,6 +22,7 @@ _i = ctypes.c_int
 _SIGS = {
     "fls_gpu_status": (_i, [_i]),
     "fls_gpu_launch_count": (_u64, [_i]),
+    "fls_gpu_test_stalled_copy": (_i, [_p, _p, _p, _p, _p, _u64, _u64, ctypes.c_uint32, _p]),
 }
 for w in (8, 16, 32, 64):
     _SIGS[f"fls_gpu_unpack_u{w}"] = (_i, [_p, _p, _p, _p, _u64, _i, _p])

@@ -330,6 +330,33 @@ int run_primitive(const void* in, void* out, const uint8_t* bw, uint8_t bw_const
 	return to_status(launch_decode(Family::NUM, a, static_cast<cudaStream_t>(stream)));
 }
 
+// The unffor primitive with failure injection (fls_gpu_test_stalled_copy).
+int run_stalled(const uint32_t* in, uint32_t* out, const uint8_t* bw, const uint32_t* base, const uint64_t* byte_off,
+                uint64_t n_vec, uint64_t stall_vector, uint32_t spin_limit, fls_stream_t stream) {
+	if (!in || !out || !bw || !base || !byte_off || n_vec == 0 || n_vec >= (1ull << 32) || stall_vector >= n_vec ||
+	    spin_limit == 0 || (reinterpret_cast<uintptr_t>(in) & 15u) != 0) {
+		return FLS_ERR_ARG;
+	}
+	DecodeArgs a {};
+	ColDesc&   c = a.col0;
+	c.ws         = 32;
+	c.e          = 4;
+	c.enc        = ENC_FFOR;
+	c.post       = POST_NONE;
+	c.order      = FLS_TRANSPOSED;
+	c.layout     = LAYOUT_ARRAYS;
+	c.n_vec      = static_cast<uint32_t>(n_vec);
+	c.packed     = reinterpret_cast<const uint8_t*>(in);
+	c.byte_off   = byte_off;
+	c.bw_arr     = bw;
+	c.base_arr   = reinterpret_cast<const uint8_t*>(base);
+	c.out        = reinterpret_cast<uint8_t*>(out);
+	a.n_items    = n_vec;
+	a.test_stall = stall_vector + 1;
+	a.spin_limit = spin_limit;
+	return to_status(launch_decode(Family::NUM, a, static_cast<cudaStream_t>(stream)));
+}
+
 template <typename T>
 int run_permute(const T* in, T* out, uint64_t n_vec, bool to_transposed, fls_stream_t stream) {
 	if (n_vec == 0) { return FLS_OK; }
@@ -391,6 +418,12 @@ uint64_t fls_gpu_launch_count(int reset) {
 	const uint64_t n = launch_counter();
 	if (reset) { launch_counter() = 0; }
 	return n;
+}
+
+int fls_gpu_test_stalled_copy(const uint32_t* d_in, uint32_t* d_out, const uint8_t* d_bw, const uint32_t* d_base,
+                              const uint64_t* d_byte_off, uint64_t n_vec, uint64_t stall_vector, uint32_t spin_limit,
+                              fls_stream_t stream) {
+	return run_stalled(d_in, d_out, d_bw, d_base, d_byte_off, n_vec, stall_vector, spin_limit, stream);
 }
 
 #define FLS_PRIM(T, W)                                                                                                \

@@ -174,7 +174,7 @@ constexpr uint32_t kLaneWindow = 256;
 
 template <uint32_t GSTAGE>
 __device__ __forceinline__ void issue(const Plan& p, uint8_t* stage, uint8_t* gstage, uint8_t* lbstage, uint64_t* bar,
-                                      uint32_t lane) {
+                                      uint32_t lane, bool stall = false) {
 	uint32_t       tx     = 0;
 	const uint32_t lbhead = static_cast<uint32_t>(reinterpret_cast<uintptr_t>(p.lane_bases) & 15u);
 	// 16-byte aligned lane bases: exactly their 128 bytes by TMA; inside a page: the aligned 144-byte window by
@@ -204,9 +204,10 @@ __device__ __forceinline__ void issue(const Plan& p, uint8_t* stage, uint8_t* gs
 		tx += gwindow;
 		if (lbtma) { tx += lbbytes; }
 		mbar_arrive_expect_tx(bar, tx);
-		if (tma_pk) { bulk_g2s(stage, p.src, p.bytes, bar); }
-		if (gwindow) { bulk_g2s(gstage, p.gsrc - p.ghead, gwindow, bar); }
-		if (lbtma) { bulk_g2s(lbstage, p.lane_bases - lbhead, lbbytes, bar); }
+		// stall (failure injection): the byte count is armed, no copy is issued, so the wait runs out
+		if (tma_pk && !stall) { bulk_g2s(stage, p.src, p.bytes, bar); }
+		if (gwindow && !stall) { bulk_g2s(gstage, p.gsrc - p.ghead, gwindow, bar); }
+		if (lbtma && !stall) { bulk_g2s(lbstage, p.lane_bases - lbhead, lbbytes, bar); }
 		// without a staging area the run values are gathered from global memory: start them towards L2 now
 		if (GSTAGE == 0 && p.ok && p.gbytes > 0) { bulk_prefetch_l2(p.gsrc - p.ghead, (p.ghead + p.gbytes + 15u) & ~15u); }
 	}
@@ -912,9 +913,11 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_decode(const DecodeArgs a) {
 	auto issue_k = [&](uint64_t k, uint32_t s) {
 		const PlanS& ps = plans[k % (2 * PB)];
 		if (ps.flags & 4u) {
-			issue<GSTAGE>(unpack_plan(ps), stage_ptr(s), gstage_ptr(s), lb_ptr(s), &bars[s], lane);
+			const bool stall = a.test_stall != 0 && gw + k * nw == a.test_stall - 1;
+			issue<GSTAGE>(unpack_plan(ps), stage_ptr(s), gstage_ptr(s), lb_ptr(s), &bars[s], lane, stall);
 		}
 	};
+	const uint32_t limit = a.spin_limit ? a.spin_limit : kMbarSpinLimit;
 
 	fill(0);
 	fill(1);
@@ -931,7 +934,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_decode(const DecodeArgs a) {
 		const uint32_t s      = k % STAGES;
 		const uint32_t parity = (k / STAGES) & 1u;
 		Plan           p      = unpack_plan(plans[k % (2 * PB)]);
-		if (!mbar_wait(&bars[s], parity)) {
+		if (!mbar_wait(&bars[s], parity, limit)) {
 			if (lane == 0) { atomicOr(a.status, STATUS_TIMEOUT); }
 			aborted = true;
 			break;
@@ -947,7 +950,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) k_decode(const DecodeArgs a) {
 		issue_k(k + STAGES, s);
 	}
 	if (aborted) {
-		// Drain: every later stage this warp armed must land before the block's shared memory goes away.
+		// Drain: every later stage this warp armed must land before the block's shared memory goes away (full
+		// bound: these copies were issued)
 		for (uint32_t j = k + 1; j < k + STAGES; ++j) {
 			const uint64_t item = gw + static_cast<uint64_t>(j) * nw;
 			if (item >= n) { break; }

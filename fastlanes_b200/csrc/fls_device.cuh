@@ -69,8 +69,8 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 // so the bound below is far beyond any legitimate copy latency.
 constexpr uint32_t kMbarSpinLimit = 1u << 20;
 
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-	for (uint32_t i = 0; i < kMbarSpinLimit; ++i) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit = kMbarSpinLimit) {
+	for (uint32_t i = 0; i < limit; ++i) {
 		if (mbar_try_wait(bar, parity)) { return true; }
 	}
 	return false;

@@ -437,6 +437,106 @@ void decode_to_memory(uint8_t* enc, void* out, enum data_t dt) {
 	(void)decode_host_page(enc, 0, out, ~0ull, dt, nullptr);
 }
 
+// init_random_access / random_access (include/fastlanes.h:88-108 of the reference, declared there and defined
+// nowhere).  They serve the pages whose buffers are all per vector -- the C API's own expressions (UNCOMPRESSED,
+// FFOR, DELTA, RLE, patched FFOR / DELTA without rec buffers) -- of INT64 columns (the functions carry no type).
+// The byte range of buffer i of vector v is [off[i] + ep(v, i), off[i] + ep(v + 1, i)); the last vector's
+// ranges end at the next buffer's offset, and its packed buffer at the page end, which the metadata alone does
+// not give: init_random_access reports the largest packed vector there (64 * 128 bytes) and random_access takes
+// the exact size from the vector's bit-width byte.
+static const ExprLayout* random_access_layout(const uint8_t* page, PageInfo* pi) {
+	if (!page || parse_page_header(page, 8 + 4 * 6, pi) != FLS_OK) { return nullptr; }
+	const ExprLayout* L = pi->layout;
+	if (L->ib_rec != kNoBuf || L->ib_rec2 != kNoBuf || L->post == POST_DICT || L->post == POST_RLE_DICT) {
+		return nullptr;
+	}
+	return L;
+}
+
+static uint64_t ep_at(const uint8_t* page, const PageInfo& pi, uint64_t v, uint32_t i) {
+	if (v == 0) { return 0; }
+	uint32_t x;
+	std::memcpy(&x, page + pi.ep_off + 4ull * ((v - 1) * pi.arr_c + i), 4);
+	return x;
+}
+
+static constexpr uint64_t kMaxPackedVector = 64 * 128;
+
+int fls_random_access_ranges(const uint8_t* page, uint64_t v, uint64_t* n_buf, uint64_t* pairs) {
+	PageInfo          pi;
+	const ExprLayout* L = random_access_layout(page, &pi);
+	if (!L) { return FLS_ERR_UNSUPPORTED; }
+	if (!n_buf || !pairs || v >= pi.vec_c) { return FLS_ERR_ARG; }
+	*n_buf = pi.arr_c;
+	for (uint32_t i = 0; i < pi.arr_c; ++i) {
+		const uint64_t start = pi.off[i] + ep_at(page, pi, v, i);
+		uint64_t       end;
+		if (v + 1 < pi.vec_c) {
+			end = pi.off[i] + ep_at(page, pi, v + 1, i);
+		} else {
+			end = i + 1 < pi.arr_c ? pi.off[i + 1] : start + kMaxPackedVector;
+		}
+		if (end < start) { return FLS_ERR_FORMAT; }
+		pairs[2 * i]     = start;
+		pairs[2 * i + 1] = end - start;
+	}
+	return FLS_OK;
+}
+
+int fls_random_access_decode(const uint8_t* page, uint64_t v, uint64_t n_buf, const uint64_t* pairs,
+                             const uint8_t* const* buffers, int64_t* out) {
+	PageInfo          pi;
+	const ExprLayout* L = random_access_layout(page, &pi);
+	if (!L) { return FLS_ERR_UNSUPPORTED; }
+	if (!pairs || !buffers || !out || v >= pi.vec_c || n_buf != pi.arr_c) { return FLS_ERR_ARG; }
+	// a one-vector page of the same expression: header with vec_c = 1, the buffer offsets, the vector's slices
+	uint64_t size[6];
+	uint64_t total = 8 + 4ull * pi.arr_c;
+	for (uint32_t i = 0; i < pi.arr_c; ++i) {
+		if (!buffers[i]) { return FLS_ERR_ARG; }
+		size[i] = pairs[2 * i + 1];
+	}
+	const uint32_t last = pi.arr_c - 1;
+	const uint64_t ws   = L->ws ? L->ws : 64;
+	if (L->enc == ENC_RAW) {
+		size[last] = ws * 128;
+	} else {
+		if (size[L->ib_bw] < 1) { return FLS_ERR_FORMAT; }
+		const uint64_t bw = buffers[L->ib_bw][0];
+		if (bw > ws) { return FLS_ERR_BW; }
+		size[last] = bw * 128;
+	}
+	if (size[last] > pairs[2 * last + 1]) { return FLS_ERR_FORMAT; }
+	for (uint32_t i = 0; i < pi.arr_c; ++i) { total += size[i]; }
+	std::vector<uint8_t> one(total);
+	std::memcpy(one.data(), page, 8);
+	const uint16_t one_vec = 1;
+	std::memcpy(one.data() + 4, &one_vec, 2);
+	uint64_t pos = 8 + 4ull * pi.arr_c;
+	for (uint32_t i = 0; i < pi.arr_c; ++i) {
+		const uint32_t o = static_cast<uint32_t>(pos);
+		std::memcpy(one.data() + 8 + 4 * i, &o, 4);
+		if (size[i]) { std::memcpy(one.data() + pos, buffers[i], size[i]); }
+		pos += size[i];
+	}
+	return decode_host_page(one.data(), total, out, 1024 * sizeof(int64_t), INT64, nullptr);
+}
+
+void init_random_access(uint8_t* in_encoded_data, uint64_t in_vector_id, uint64_t* output_n_buffer,
+                        uint64_t* output_buffer) {
+	if (fls_random_access_ranges(in_encoded_data, in_vector_id, output_n_buffer, output_buffer) != FLS_OK &&
+	    output_n_buffer) {
+		*output_n_buffer = 0;
+	}
+}
+
+void random_access(uint8_t* in_encoded_data, uint64_t in_vector_id, uint64_t* output_n_buffer,
+                   uint64_t* output_pair_offset_and_size, uint8_t** output_buffers, uint8_t* out_deencoded_vector) {
+	(void)fls_random_access_decode(in_encoded_data, in_vector_id, output_n_buffer ? *output_n_buffer : 0,
+	                               output_pair_offset_and_size, output_buffers,
+	                               reinterpret_cast<int64_t*>(out_deencoded_vector));
+}
+
 int fls_page_placement(const uint8_t* page_prefix, uint64_t prefix_size, uint32_t* shift) {
 	PageInfo pi;
 	const int rc = parse_page_header(page_prefix, prefix_size, &pi);

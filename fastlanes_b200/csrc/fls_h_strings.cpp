@@ -7,6 +7,7 @@
 #include "fls_runtime.h"
 #include "fls_strplan.h"
 
+#include <algorithm>
 #include <cstring>
 #include <cuda_runtime.h>
 #include <memory>
@@ -150,10 +151,16 @@ struct fls_string_plan {
 	DevArr<uint64_t>         vec_total;
 	DevArr<uint64_t>         vec_base;
 	DevArr<uint32_t>         codes; // patched DICT pages: their decoded code stream
-	DevArr<uint32_t>         row_len; // FSST / FSST12 pages: every row's decoded length
+	DevArr<uint32_t>         row_len; // FSST12 pages: every row's decoded length
 	uint32_t                 dyn_smem = 0;
 	int                      warps    = 0; // warps per CTA of the materialising kernel
 	uint64_t                 n_rows   = 0;
+	// single-pass DICT decode (k_dict_pass): DICT pages whose dictionary has a packed row table
+	bool                     single   = false;
+	DevArr<StrArgs>          dargs;    // the plan's arguments in device memory (item_base 0)
+	DevArr<uint64_t>         lb;       // ticket + one look-back word per vector, zeroed before every decode
+	int                      sp_warps = 0;
+	uint32_t                 sp_smem  = 0, sp_dict_cap = 0, sp_tab_cap = 0;
 	// a measure() whose per-vector totals and bases the next decode() takes over (the usual measure, allocate,
 	// decode sequence runs the lengths pass once)
 	mutable bool             measured = false;
@@ -224,7 +231,7 @@ int fls_string_plan_create(const uint8_t* d_page, uint64_t page_size, const uint
 	if (!p->vec_total.alloc(pi.vec_c + 1) || !p->vec_base.alloc(pi.vec_c + 1)) { return FLS_ERR_CUDA; }
 	a.vec_total = p->vec_total.p;
 	a.vec_base  = p->vec_base.p;
-	if (L->kind == STR_FSST || L->kind == STR_FSST12) {
+	if (L->kind == STR_FSST12) {
 		if (!p->row_len.alloc(static_cast<size_t>(pi.vec_c) * 1024)) { return FLS_ERR_CUDA; }
 		a.row_len = p->row_len.p;
 	}
@@ -325,6 +332,25 @@ int fls_string_plan_create(const uint8_t* d_page, uint64_t page_size, const uint
 	}
 	p->warps    = static_cast<int>(w < kStrMaxWarps ? w : kStrMaxWarps);
 	p->dyn_smem = static_cast<uint32_t>(p->warps * per_warp + (a.dict_in_smem ? dict_sm : 0u));
+	if (a.kind == STR_DICT && a.dict_rows && pi.vec_c > 0) {
+		// single-pass decode: the dictionary and its row table in shared memory when at least 8 warps still fit
+		p->single            = true;
+		const uint32_t   pw  = dict_pass_smem_per_warp(a.rows16);
+		const uint64_t   tab = (4ull * a.entry_c + 15) & ~15ull;
+		const uint64_t   all = 224 * 1024;
+		uint64_t         sw  = all / pw;
+		if (dict_sm + tab < all && (all - dict_sm - tab) / pw >= 8) {
+			p->sp_dict_cap = static_cast<uint32_t>(dict_sm);
+			p->sp_tab_cap  = a.entry_c;
+			sw             = (all - dict_sm - tab) / pw;
+		}
+		p->sp_warps = static_cast<int>(sw < kStrMaxWarps ? sw : kStrMaxWarps);
+		p->sp_smem  = static_cast<uint32_t>(p->sp_warps * pw + (p->sp_dict_cap ? dict_sm + tab : 0u));
+		if (!p->dargs.alloc(1) || !p->lb.alloc(1ull + pi.vec_c) ||
+		    cudaMemcpy(p->dargs.p, &a, sizeof(StrArgs), cudaMemcpyHostToDevice) != cudaSuccess) {
+			return FLS_ERR_CUDA;
+		}
+	}
 	*out                    = p.release();
 	return FLS_OK;
 }
@@ -358,11 +384,34 @@ int fls_string_plan_measure(fls_string_plan* p, uint64_t* n_bytes, fls_stream_t 
 	return FLS_OK;
 }
 
+// The single-pass DICT decode of one plan: one memset of its look-back words and one launch.
+static int single_pass_decode(const fls_string_plan* p, uint32_t* d_offsets, uint8_t* d_bytes, uint64_t cap,
+                              cudaStream_t s) {
+	const uint32_t n_vec = p->args.col.n_vec;
+	if (cudaMemsetAsync(p->lb.p, 0, 8ull * (1 + n_vec), s) != cudaSuccess) { return FLS_ERR_CUDA; }
+	StrSetArgs x {};
+	x.cols        = p->dargs.p;
+	x.chunk_w     = static_cast<uint32_t>(p->sp_warps);
+	x.n_chunks    = (n_vec + x.chunk_w - 1) / x.chunk_w;
+	x.flags       = p->lb.p;
+	x.status      = p->args.status;
+	x.out_offsets = d_offsets;
+	x.out_bytes   = d_bytes;
+	x.out_cap     = cap;
+	x.dict_cap    = p->sp_dict_cap;
+	x.tab_cap     = p->sp_tab_cap;
+	return launch_dict_pass(x, p->args.rows16, p->sp_warps, p->sp_smem, s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
+}
+
 int fls_string_plan_decode(const fls_string_plan* p, uint32_t* d_offsets, uint8_t* d_bytes, uint64_t bytes_cap,
                            fls_stream_t stream) {
 	if (!p || !d_offsets || (!d_bytes && bytes_cap)) { return FLS_ERR_ARG; }
 	if ((reinterpret_cast<uintptr_t>(d_bytes) & 15u) != 0 || bytes_cap >= (1ull << 32)) { return FLS_ERR_ARG; }
 	cudaStream_t s  = static_cast<cudaStream_t>(stream);
+	if (p->single) {
+		p->measured = false;
+		return single_pass_decode(p, d_offsets, d_bytes, bytes_cap, s);
+	}
 	// the totals of a measure() just before (complete: measure synchronised its stream) are still valid; a
 	// decode captured into a graph always computes its own (each replay must)
 	cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -380,8 +429,119 @@ int fls_string_plan_decode(const fls_string_plan* p, uint32_t* d_offsets, uint8_
 	return launch_str_materialize(a, p->warps, p->dyn_smem, s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
 }
 
+
+
 int fls_string_plan_destroy(fls_string_plan* p) {
 	delete p;
+	return FLS_OK;
+}
+
+} // extern "C"
+
+// A set of single-pass DICT string plans decoded by one launch (k_dict_pass over every column's vectors).
+struct fls_string_set {
+	std::vector<StrArgs> args;     // every column's arguments: item_base, and the outputs once bound
+	DevArr<StrArgs>      cols;     // the same in device memory
+	DevArr<uint32_t>     chunk_col, chunk_v0;
+	DevArr<uint64_t>     lb;       // ticket + one look-back word per vector of every column
+	uint64_t             n_items  = 0;
+	uint32_t             n_chunks = 0;
+	int                  warps    = 0;
+	uint32_t             smem = 0, dict_cap = 0, tab_cap = 0;
+	bool                 rows16 = true, bound = false;
+	int*                 status = nullptr;
+};
+
+extern "C" {
+
+int fls_string_set_create(const fls_string_plan* const* plans, uint32_t n, fls_string_set** out) {
+	if (!out || !plans || n == 0) { return FLS_ERR_ARG; }
+	*out = nullptr;
+	std::unique_ptr<fls_string_set> set(new fls_string_set());
+	uint64_t dict_max = 0, tab_max = 0;
+	for (uint32_t i = 0; i < n; ++i) {
+		if (!plans[i]) { return FLS_ERR_ARG; }
+		if (!plans[i]->single) { return FLS_ERR_UNSUPPORTED; } // DICT pages with a packed row table only
+		StrArgs a   = plans[i]->args;
+		a.item_base = set->n_items;
+		set->args.push_back(a);
+		set->n_items += a.col.n_vec;
+		set->rows16 = set->rows16 && a.rows16;
+		dict_max    = std::max<uint64_t>(dict_max, (a.dict_bytes_n + 15) & ~15ull);
+		tab_max     = std::max<uint64_t>(tab_max, a.entry_c);
+		set->status = a.status;
+	}
+	const uint32_t pw  = dict_pass_smem_per_warp(set->rows16);
+	const uint64_t tab = (4 * tab_max + 15) & ~15ull;
+	const uint64_t all = 224 * 1024;
+	uint64_t       w   = all / pw;
+	if (dict_max + tab < all && (all - dict_max - tab) / pw >= 8) {
+		set->dict_cap = static_cast<uint32_t>(dict_max);
+		set->tab_cap  = static_cast<uint32_t>(tab_max);
+		w             = (all - dict_max - tab) / pw;
+	}
+	set->warps = static_cast<int>(w < kStrMaxWarps ? w : kStrMaxWarps);
+	set->smem  = static_cast<uint32_t>(set->warps * pw + (set->dict_cap ? dict_max + tab : 0u));
+	// chunks of `warps` vectors that never cross a column, in column order
+	std::vector<uint32_t> cc, cv;
+	for (uint32_t i = 0; i < n; ++i) {
+		for (uint32_t v = 0; v < set->args[i].col.n_vec; v += static_cast<uint32_t>(set->warps)) {
+			cc.push_back(i);
+			cv.push_back(v);
+		}
+	}
+	set->n_chunks = static_cast<uint32_t>(cc.size());
+	if (!set->cols.alloc(n) || !set->lb.alloc(1 + set->n_items) || !set->chunk_col.alloc(cc.size()) ||
+	    !set->chunk_v0.alloc(cv.size())) {
+		return FLS_ERR_CUDA;
+	}
+	if (!cc.empty() && (cudaMemcpy(set->chunk_col.p, cc.data(), 4 * cc.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+	                    cudaMemcpy(set->chunk_v0.p, cv.data(), 4 * cv.size(), cudaMemcpyHostToDevice) != cudaSuccess)) {
+		return FLS_ERR_CUDA;
+	}
+	*out = set.release();
+	return FLS_OK;
+}
+
+int fls_string_set_bind(fls_string_set* set, uint32_t* const* d_offsets, uint8_t* const* d_bytes,
+                        const uint64_t* bytes_caps) {
+	if (!set || !d_offsets || !d_bytes || !bytes_caps) { return FLS_ERR_ARG; }
+	for (size_t i = 0; i < set->args.size(); ++i) {
+		if (!d_offsets[i] || (!d_bytes[i] && bytes_caps[i]) || (reinterpret_cast<uintptr_t>(d_bytes[i]) & 15u) != 0 ||
+		    bytes_caps[i] >= (1ull << 32)) {
+			return FLS_ERR_ARG;
+		}
+		set->args[i].offsets   = d_offsets[i];
+		set->args[i].bytes     = d_bytes[i];
+		set->args[i].bytes_cap = bytes_caps[i];
+	}
+	if (cudaMemcpy(set->cols.p, set->args.data(), sizeof(StrArgs) * set->args.size(), cudaMemcpyHostToDevice) !=
+	    cudaSuccess) {
+		return FLS_ERR_CUDA;
+	}
+	set->bound = true;
+	return FLS_OK;
+}
+
+int fls_string_set_decode(const fls_string_set* set, fls_stream_t stream) {
+	if (!set || !set->bound) { return FLS_ERR_ARG; }
+	cudaStream_t s = static_cast<cudaStream_t>(stream);
+	if (cudaMemsetAsync(set->lb.p, 0, 8ull * (1 + set->n_items), s) != cudaSuccess) { return FLS_ERR_CUDA; }
+	StrSetArgs x {};
+	x.cols      = set->cols.p;
+	x.chunk_col = set->chunk_col.p;
+	x.chunk_v0  = set->chunk_v0.p;
+	x.n_chunks  = set->n_chunks;
+	x.chunk_w   = static_cast<uint32_t>(set->warps);
+	x.flags     = set->lb.p;
+	x.status    = set->status;
+	x.dict_cap  = set->dict_cap;
+	x.tab_cap   = set->tab_cap;
+	return launch_dict_pass(x, set->rows16, set->warps, set->smem, s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
+}
+
+int fls_string_set_destroy(fls_string_set* set) {
+	delete set;
 	return FLS_OK;
 }
 

@@ -465,6 +465,297 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_str_pass(const StrArgs a)
 	}
 }
 
+// One pass over an FSST or BYTE_ARR column, warp per vector, the vector's compressed bytes decoded as one
+// stream (stream_vector: code-parallel, a lane per 4 bytes).  LENGTHS: per-vector decoded byte totals.
+// MATERIALIZE: Arrow offsets and bytes at the first output byte of every vector computed from the totals.
+template <int PASS, int KIND>
+__global__ void __launch_bounds__(kStrMaxWarps * 32) k_stream_pass(const StrArgs a) {
+	extern __shared__ __align__(128) uint8_t smem[];
+	constexpr bool      kFsst = KIND == STR_FSST;
+	__shared__ uint64_t fsym[kFsst ? 256 : 1];
+	__shared__ uint8_t  flen[kFsst ? 256 : 1];
+	const uint32_t      lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+	constexpr uint32_t  kPerWarp = str_per_warp(PASS, false);
+	if constexpr (kFsst) {
+		for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) {
+			fsym[i] = a.table->sym[i];
+			flen[i] = a.table->len[i];
+		}
+	}
+	uint8_t*        wbase  = smem + warp * kPerWarp;
+	PlanS*          plans  = reinterpret_cast<PlanS*>(wbase);
+	uint8_t*        buf    = wbase + kStrPB * 64;
+	const uint32_t* rows32 = reinterpret_cast<const uint32_t*>(buf);
+	uint8_t*        win    = buf + kStrRows;
+	__syncthreads();
+
+	const uint64_t gw = static_cast<uint64_t>(blockIdx.x) * nwarps + warp;
+	const uint64_t nw = static_cast<uint64_t>(gridDim.x) * nwarps;
+	const uint64_t n  = a.col.n_vec;
+	uint32_t       k  = 0;
+	for (uint64_t v = gw; v < n; v += nw, ++k) {
+		if (k % kStrPB == 0) {
+			if (lane < kStrPB) {
+				const uint64_t u = v + lane * nw;
+				Plan           q {};
+				if (u < n) { q = make_plan(a.col, static_cast<uint32_t>(u)); }
+				plans[lane] = pack_plan(q, u < n);
+			}
+			__syncwarp();
+		}
+		const Plan p = unpack_plan(plans[k % kStrPB]);
+		if (!p.ok) {
+			if (lane == 0) {
+				atomicOr(a.status, p.bw > p.ws ? STATUS_BAD_BW : STATUS_BAD_LAYOUT);
+				if (PASS == STR_PASS_LENGTHS) { a.vec_total[v] = 0; }
+			}
+			continue;
+		}
+		load_rows<false>(p, buf, lane, a.status);
+		uint32_t       vn  = 0;
+		const uint8_t* vb  = vector_bytes(a.col, static_cast<uint32_t>(v), &vn);
+		bool           bad = false;
+		StreamOut      o {};
+		if constexpr (PASS == STR_PASS_LENGTHS) {
+			const uint32_t tot = stream_vector<false, kFsst, kStrWindow>(rows32, vb, vn, fsym, flen, lane, o, &bad);
+			if (lane == 0) {
+				a.vec_total[v] = tot;
+				if (bad) { atomicOr(a.status, STATUS_BAD_INDEX); }
+			}
+		} else {
+			const uint64_t vbase = a.vec_base[v];
+			const uint64_t vend  = a.vec_base[v + 1];
+			if (vend < vbase || vend > a.bytes_cap) {
+				if (lane == 0) { atomicOr(a.status, STATUS_BAD_LAYOUT); }
+				__syncwarp();
+				continue;
+			}
+			o.offsets          = a.offsets + v * kVec;
+			o.bytes            = a.bytes;
+			o.vbase            = vbase;
+			o.win              = win;
+			const uint32_t tot = stream_vector<true, kFsst, kStrWindow>(rows32, vb, vn, fsym, flen, lane, o, &bad);
+			if (lane == 0) {
+				if (v + 1 == n) { a.offsets[n * kVec] = static_cast<uint32_t>(vbase + tot); }
+				if (bad || vbase + tot != vend) { atomicOr(a.status, STATUS_BAD_INDEX); }
+			}
+		}
+		__syncwarp();
+	}
+}
+
+// ---------------------------------------------------------------------------------------------------------
+// Single-pass DICT decode (k_dict_pass): no lengths pass.  A vector's rows resolve to (dictionary start,
+// length) through the packed row table; their lengths sum to the vector's total, which the warp publishes as
+// soon as it has it; its first output byte is the sum of its column's earlier totals, read back from the
+// earlier vectors' look-back words (a predecessor that has its inclusive prefix ends the walk).  Tickets hand
+// out work in vector order, so every vector a warp waits for was taken by a warp that is already running and
+// publishes without waiting on anything: the walk always ends.  Its spin is bounded all the same.
+// ---------------------------------------------------------------------------------------------------------
+constexpr uint64_t kLbAgg = 1ull << 62, kLbInc = 2ull << 62, kLbVal = (1ull << 62) - 1;
+constexpr uint32_t kLookbackSpinLimit = 1u << 20;
+
+__device__ __forceinline__ uint64_t ld_acquire_u64(const uint64_t* p) {
+	uint64_t v;
+	asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+	return v;
+}
+__device__ __forceinline__ void st_release_u64(uint64_t* p, uint64_t v) {
+	asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Exclusive prefix of vector v's column (words: the column's look-back words, vector 0 first): walk back 32
+// words at a time until a word with an inclusive prefix.  STATUS_TIMEOUT (and a partial sum) if a predecessor
+// never publishes.
+__device__ __forceinline__ uint64_t lookback(const uint64_t* words, uint32_t v, uint32_t lane, int* status) {
+	uint64_t P     = 0;
+	int64_t  j     = static_cast<int64_t>(v) - 1;
+	uint32_t spins = 0;
+	while (true) {
+		const int64_t  idx  = j - static_cast<int64_t>(lane);
+		const uint64_t f    = idx >= 0 ? ld_acquire_u64(words + idx) : kLbInc; // before vector 0: prefix 0
+		const uint32_t inc  = __ballot_sync(0xFFFFFFFFu, (f >> 62) == 2u);
+		const uint32_t emp  = __ballot_sync(0xFFFFFFFFu, (f >> 62) == 0u);
+		const uint32_t upto = inc ? (((inc & (0u - inc)) << 1) - 1u) : 0xFFFFFFFFu; // lanes up to the nearest prefix
+		if (emp & upto) {
+			if (++spins > kLookbackSpinLimit) {
+				if (lane == 0) { atomicOr(status, STATUS_TIMEOUT); }
+				return P;
+			}
+			__nanosleep(64);
+			continue;
+		}
+		P += warp_sum<uint64_t>(((upto >> lane) & 1u) ? (f & kLbVal) : 0ull);
+		if (inc) { return P; }
+		j -= 32;
+	}
+}
+
+// Rows of one DICT vector into Arrow offsets and bytes from the first output byte vbase: 32 rows at a time (a
+// row per lane, positions by a warp scan) into the warp's output window (put_row), which leaves in 16-byte
+// stores.  tab: the packed row table (start | length << 24) of the dictionary's entry_c entries.  Returns the
+// bytes written; *bad for codes outside the dictionary (such rows are empty).
+template <bool R16>
+__device__ __forceinline__ uint32_t dict_vector_out(const uint8_t* rows, const uint32_t* tab, uint32_t entry_c,
+                                                    const uint8_t* dict, uint8_t* win, uint32_t* offs, uint8_t* bytes,
+                                                    uint64_t vbase, uint32_t lane, bool* bad) {
+	uint32_t* win32 = reinterpret_cast<uint32_t*>(win);
+	uint64_t  W     = vbase & ~15ull; // output position of win[0]
+	uint32_t  fill  = static_cast<uint32_t>(vbase & 15u);
+	uint64_t  lo    = vbase; // first output byte the window may write
+	if (lane == 0) { win32[fill >> 2] = 0; }
+	__syncwarp();
+	auto flush = [&](bool all) {
+		const uint32_t full = fill & ~15u;
+		const uint32_t upto = all ? fill : full;
+		for (uint32_t c = 16 * lane; c < upto; c += 512) {
+			const uint64_t g = W + c;
+			if (g >= lo && c + 16 <= upto) {
+				*reinterpret_cast<uint4*>(bytes + g) = *reinterpret_cast<const uint4*>(win + c);
+			} else {
+				for (uint32_t i = 0; i < 16 && c + i < upto; ++i) {
+					if (g + i >= lo) { bytes[g + i] = win[c + i]; }
+				}
+			}
+		}
+		__syncwarp();
+		if (!all) {
+			if (lane == 0 && full != 0 && (fill & 15u) != 0) {
+				*reinterpret_cast<uint4*>(win) = *reinterpret_cast<const uint4*>(win + full);
+			}
+			__syncwarp();
+			W += full;
+			fill &= 15u;
+			lo = lo > W ? lo : W;
+		}
+	};
+	auto ref = [&](uint32_t r, uint32_t* start, uint32_t* len) {
+		const uint32_t code = row_at<R16>(rows, r);
+		if (code >= entry_c) {
+			*bad   = true;
+			*start = 0;
+			*len   = 0;
+		} else {
+			const uint32_t e = tab[code];
+			*start           = e & 0xFFFFFFu;
+			*len             = e >> 24;
+		}
+	};
+	uint32_t vpos = 0, ns, nl;
+	ref(lane, &ns, &nl);
+	for (uint32_t b = 0; b < kVec / 32; ++b) {
+		const uint32_t fs = ns, fl = nl;
+		if (b + 1 < kVec / 32) { ref(32 * (b + 1) + lane, &ns, &nl); }
+		const uint32_t inc = warp_inclusive_scan(fl, lane);
+		const uint32_t o   = vpos + inc - fl;
+		const uint32_t T   = __shfl_sync(0xFFFFFFFFu, inc, 31);
+		offs[32 * b + lane] = static_cast<uint32_t>(vbase + o);
+		if (fill + T > kStrWindow) { flush(false); }
+		if (fill + T <= kStrWindow) {
+			uint32_t   hk = 0, head = 0;
+			const bool mid = put_row(win32, fill + (o - vpos), reinterpret_cast<const uint32_t*>(dict), fs, fl, &hk, &head);
+			__syncwarp(); // every word's whole store lands before the rows that start inside it OR in
+			if (mid) { atomicOr(win32 + hk, head); }
+			fill += T;
+		} else {
+			// a batch larger than the window: straight to global memory after the window's pending bytes
+			flush(true);
+			uint8_t* dst = bytes + vbase + o;
+			for (uint32_t i = 0; i < fl; ++i) { dst[i] = dict[fs + i]; }
+			const uint64_t pos = vbase + vpos + T;
+			W                  = pos & ~15ull;
+			fill               = static_cast<uint32_t>(pos & 15u);
+			lo                 = pos;
+			__syncwarp();
+			if (lane == 0) { win32[fill >> 2] = 0; }
+		}
+		vpos += T;
+		__syncwarp();
+	}
+	flush(true);
+	return vpos;
+}
+
+template <bool R16, bool SMDICT>
+__global__ void __launch_bounds__(kStrMaxWarps * 32) k_dict_pass(const StrSetArgs s) {
+	extern __shared__ __align__(128) uint8_t smem[];
+	__shared__ uint32_t s_chunk;
+	const uint32_t      lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+	constexpr uint32_t  kPerWarp = str_rows_bytes(R16) + kStrWindow;
+	uint8_t*            rows     = smem + warp * kPerWarp;
+	uint8_t*            win      = rows + str_rows_bytes(R16);
+	uint8_t*            sdict    = smem + nwarps * kPerWarp;
+	uint32_t*           stab     = reinterpret_cast<uint32_t*>(sdict + s.dict_cap);
+	int64_t             loaded   = -1;
+	for (;;) {
+		if (threadIdx.x == 0) {
+			s_chunk = static_cast<uint32_t>(atomicAdd(reinterpret_cast<unsigned long long*>(s.flags), 1ull));
+		}
+		__syncthreads();
+		const uint32_t ch = s_chunk;
+		if (ch >= s.n_chunks) { break; }
+		const uint32_t col = s.chunk_col ? __ldg(s.chunk_col + ch) : 0u;
+		const StrArgs& A   = s.cols[col];
+		if constexpr (SMDICT) {
+			if (static_cast<int64_t>(col) != loaded) {
+				// the column's decoded dictionary (cudaMalloc'd, 16 bytes of slack) and row table
+				const uint32_t nb16 = static_cast<uint32_t>((A.dict_bytes_n + 15) / 16);
+				const uint4*   src  = reinterpret_cast<const uint4*>(A.dict_bytes);
+				for (uint32_t i = threadIdx.x; i < nb16; i += blockDim.x) { reinterpret_cast<uint4*>(sdict)[i] = __ldg(src + i); }
+				for (uint32_t i = threadIdx.x; i < A.entry_c; i += blockDim.x) { stab[i] = __ldg(A.dict_rows + i); }
+				loaded = col;
+			}
+		}
+		__syncthreads(); // also: every thread has read s_chunk before thread 0 overwrites it
+		const uint32_t v0    = s.chunk_v0 ? __ldg(s.chunk_v0 + ch) : ch * s.chunk_w;
+		const uint32_t n_vec = A.col.n_vec;
+		const uint32_t v     = v0 + warp;
+		if (warp >= s.chunk_w || v >= n_vec || v >= v0 + s.chunk_w) { continue; }
+		const uint8_t*  dict    = SMDICT ? sdict : A.dict_bytes;
+		const uint32_t* tab     = SMDICT ? stab : A.dict_rows;
+		const uint32_t  entry_c = A.entry_c;
+		uint64_t*       words   = s.flags + 1 + A.item_base;
+		const Plan      p       = make_plan(A.col, v);
+		bool            bad     = false;
+		bool            ok      = p.ok;
+		if (!ok && lane == 0) { atomicOr(s.status, p.bw > p.ws ? STATUS_BAD_BW : STATUS_BAD_LAYOUT); }
+		if (ok) { ok = load_rows<R16>(p, rows, lane, s.status); }
+		// the vector's total: every row's length
+		uint32_t T = 0;
+		if (ok) {
+			uint32_t sum = 0;
+			for (uint32_t b = 0; b < kVec / 32; ++b) {
+				const uint32_t code = row_at<R16>(rows, 32 * b + lane);
+				if (code < entry_c) {
+					sum += tab[code] >> 24;
+				} else {
+					bad = true;
+				}
+			}
+			T = warp_sum(sum);
+		}
+		// every vector publishes (also one that failed: its successors wait for it)
+		if (lane == 0) { st_release_u64(words + v, (v == 0 ? kLbInc : kLbAgg) | T); }
+		const uint64_t P = v == 0 ? 0ull : lookback(words, v, lane, s.status);
+		if (lane == 0 && v > 0) { st_release_u64(words + v, kLbInc | (P + T)); }
+		uint32_t*      offsets = s.out_offsets ? s.out_offsets : A.offsets;
+		uint8_t*       bytes   = s.out_offsets ? s.out_bytes : A.bytes;
+		const uint64_t cap     = s.out_offsets ? s.out_cap : A.bytes_cap;
+		uint32_t*      offs    = offsets + static_cast<uint64_t>(v) * kVec;
+		if (P + T > cap || P + T >= (1ull << 32)) {
+			if (lane == 0) { atomicOr(s.status, STATUS_BAD_LAYOUT); }
+		} else if (!ok) {
+			for (uint32_t r = lane; r < kVec; r += 32) { offs[r] = static_cast<uint32_t>(P); }
+		} else {
+			const uint32_t got = dict_vector_out<R16>(rows, tab, entry_c, dict, win, offs, bytes, P, lane, &bad);
+			if (got != T) { bad = true; }
+		}
+		if (lane == 0 && v + 1 == n_vec) { offsets[static_cast<uint64_t>(n_vec) * kVec] = static_cast<uint32_t>(P + T); }
+		if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) { atomicOr(s.status, STATUS_BAD_INDEX); }
+		__syncwarp();
+	}
+}
+
 __global__ void __launch_bounds__(1024) k_scan_totals(const uint64_t* total, uint64_t* base, uint64_t n) {
 	__shared__ uint64_t wt[33];
 	uint64_t            carry = 0;
@@ -493,11 +784,74 @@ cudaError_t launch_fsst_dict(const uint8_t* lens, const uint8_t* comp, uint64_t 
 	return cudaGetLastError();
 }
 
-// Launch one pass over the column's vectors with `warps` warps per CTA and as many CTAs per SM as shared
-// memory allows (no more CTAs than there are vectors for their warps).
+// Launch one pass of kernel fn over the column's vectors with `warps` warps per CTA and as many CTAs per SM as
+// shared memory allows (no more CTAs than there are vectors for their warps).  *set / *mu: the kernel's dynamic
+// shared-memory limit set so far and its lock.  sm_count 0: the SM count of the library's per-device state.
+template <class F>
+static cudaError_t launch_pass(F fn, uint32_t* set, std::mutex* mu, const StrArgs& a, int warps, uint32_t dyn_smem,
+                               cudaStream_t s, int sm_count) {
+	{
+		std::lock_guard<std::mutex> lk(*mu);
+		if (dyn_smem > *set) {
+			const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_smem);
+			if (e != cudaSuccess) { return e; }
+			*set = dyn_smem;
+		}
+	}
+	if (sm_count <= 0) {
+		const Device* dev = current_device();
+		if (!dev) { return cudaErrorUnknown; }
+		sm_count = dev->sm_count;
+	}
+	int         per_sm = 0;
+	cudaError_t e      = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, warps * 32, dyn_smem);
+	if (e != cudaSuccess) { return e; }
+	if (per_sm < 1) { return cudaErrorInvalidConfiguration; }
+	const uint64_t need = (a.col.n_vec + warps - 1) / warps;
+	uint64_t       grid = static_cast<uint64_t>(sm_count) * per_sm;
+	grid                = grid < need ? grid : need;
+	if (grid == 0) { return cudaSuccess; }
+	fn<<<static_cast<unsigned>(grid), warps * 32, dyn_smem, s>>>(a);
+	++launch_counter();
+	return cudaGetLastError();
+}
+
 template <int PASS, int KIND, int SM, bool R16 = false>
-static cudaError_t launch_str_kernel(const StrArgs& a, int warps, uint32_t dyn_smem, cudaStream_t s) {
-	auto* const       fn = k_str_pass<PASS, KIND, SM, R16>;
+static cudaError_t launch_str_kernel(const StrArgs& a, int warps, uint32_t dyn_smem, cudaStream_t s, int sm_count) {
+	static std::mutex mu;
+	static uint32_t   set = 0;
+	return launch_pass(k_str_pass<PASS, KIND, SM, R16>, &set, &mu, a, warps, dyn_smem, s, sm_count);
+}
+
+template <int PASS, int KIND>
+static cudaError_t launch_stream_kernel(const StrArgs& a, int warps, uint32_t dyn_smem, cudaStream_t s, int sm_count) {
+	static std::mutex mu;
+	static uint32_t   set = 0;
+	return launch_pass(k_stream_pass<PASS, KIND>, &set, &mu, a, warps, dyn_smem, s, sm_count);
+}
+
+cudaError_t launch_str_lengths(const StrArgs& a, int sm_count, cudaStream_t s) {
+	constexpr int      w  = kStrLenWarps;
+	const uint32_t     sm = w * str_per_warp(STR_PASS_LENGTHS, a.rows16);
+	switch (a.kind) {
+	case STR_DICT:
+		if (a.rows16) {
+			return a.ends_in_smem ? launch_str_kernel<STR_PASS_LENGTHS, STR_DICT, SM_ENDS, true>(a, w, sm + str_ends_smem(a), s, sm_count)
+			                      : launch_str_kernel<STR_PASS_LENGTHS, STR_DICT, SM_NONE, true>(a, w, sm, s, sm_count);
+		}
+		return a.ends_in_smem ? launch_str_kernel<STR_PASS_LENGTHS, STR_DICT, SM_ENDS>(a, w, sm + str_ends_smem(a), s, sm_count)
+		                      : launch_str_kernel<STR_PASS_LENGTHS, STR_DICT, SM_NONE>(a, w, sm, s, sm_count);
+	case STR_FSST: return launch_stream_kernel<STR_PASS_LENGTHS, STR_FSST>(a, w, sm, s, sm_count);
+	case STR_FSST12: return launch_str_kernel<STR_PASS_LENGTHS, STR_FSST12, SM_NONE>(a, w, sm, s, sm_count);
+	default: return launch_stream_kernel<STR_PASS_LENGTHS, STR_BYTES>(a, w, sm, s, sm_count);
+	}
+}
+
+uint32_t dict_pass_smem_per_warp(bool rows16) { return str_rows_bytes(rows16) + kStrWindow; }
+
+template <bool R16, bool SMDICT>
+static cudaError_t launch_dict_pass_t(const StrSetArgs& a, int warps, uint32_t dyn_smem, cudaStream_t s, int sm_count) {
+	auto* const       fn = k_dict_pass<R16, SMDICT>;
 	static std::mutex mu;
 	static uint32_t   set = 0;
 	{
@@ -508,36 +862,35 @@ static cudaError_t launch_str_kernel(const StrArgs& a, int warps, uint32_t dyn_s
 			set = dyn_smem;
 		}
 	}
-	Device* dev = current_device();
-	if (!dev) { return cudaErrorUnknown; }
+	if (sm_count <= 0) {
+		const Device* dev = current_device();
+		if (!dev) { return cudaErrorUnknown; }
+		sm_count = dev->sm_count;
+	}
 	int         per_sm = 0;
 	cudaError_t e      = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, warps * 32, dyn_smem);
 	if (e != cudaSuccess) { return e; }
 	if (per_sm < 1) { return cudaErrorInvalidConfiguration; }
-	const uint64_t need = (a.col.n_vec + warps - 1) / warps;
-	uint64_t       grid = static_cast<uint64_t>(dev->sm_count) * per_sm;
-	grid                = grid < need ? grid : need;
+	uint64_t grid = static_cast<uint64_t>(sm_count) * per_sm;
+	grid          = grid < a.n_chunks ? grid : a.n_chunks;
 	if (grid == 0) { return cudaSuccess; }
 	fn<<<static_cast<unsigned>(grid), warps * 32, dyn_smem, s>>>(a);
 	++launch_counter();
 	return cudaGetLastError();
 }
 
-cudaError_t launch_str_lengths(const StrArgs& a, int /*grid*/, cudaStream_t s) {
-	constexpr int      w  = kStrLenWarps;
-	const uint32_t     sm = w * str_per_warp(STR_PASS_LENGTHS, a.rows16);
-	switch (a.kind) {
-	case STR_DICT:
-		if (a.rows16) {
-			return a.ends_in_smem ? launch_str_kernel<STR_PASS_LENGTHS, STR_DICT, SM_ENDS, true>(a, w, sm + str_ends_smem(a), s)
-			                      : launch_str_kernel<STR_PASS_LENGTHS, STR_DICT, SM_NONE, true>(a, w, sm, s);
-		}
-		return a.ends_in_smem ? launch_str_kernel<STR_PASS_LENGTHS, STR_DICT, SM_ENDS>(a, w, sm + str_ends_smem(a), s)
-		                      : launch_str_kernel<STR_PASS_LENGTHS, STR_DICT, SM_NONE>(a, w, sm, s);
-	case STR_FSST: return launch_str_kernel<STR_PASS_LENGTHS, STR_FSST, SM_NONE>(a, w, sm, s);
-	case STR_FSST12: return launch_str_kernel<STR_PASS_LENGTHS, STR_FSST12, SM_NONE>(a, w, sm, s);
-	default: return launch_str_kernel<STR_PASS_LENGTHS, STR_BYTES, SM_NONE>(a, w, sm, s);
+cudaError_t launch_dict_pass(const StrSetArgs& a, bool rows16, int warps, uint32_t dyn_smem, cudaStream_t s,
+                             int sm_count) {
+	if (warps < 1 || warps > kStrMaxWarps || a.chunk_w != static_cast<uint32_t>(warps)) {
+		return cudaErrorInvalidValue;
 	}
+	const bool sm = a.dict_cap != 0;
+	if (rows16) {
+		return sm ? launch_dict_pass_t<true, true>(a, warps, dyn_smem, s, sm_count)
+		          : launch_dict_pass_t<true, false>(a, warps, dyn_smem, s, sm_count);
+	}
+	return sm ? launch_dict_pass_t<false, true>(a, warps, dyn_smem, s, sm_count)
+	          : launch_dict_pass_t<false, false>(a, warps, dyn_smem, s, sm_count);
 }
 
 cudaError_t launch_scan_totals(const uint64_t* total, uint64_t* base, uint64_t n, cudaStream_t s) {
@@ -546,18 +899,18 @@ cudaError_t launch_scan_totals(const uint64_t* total, uint64_t* base, uint64_t n
 	return cudaGetLastError();
 }
 
-cudaError_t launch_str_materialize(const StrArgs& a, int warps, uint32_t dyn_smem, cudaStream_t s) {
+cudaError_t launch_str_materialize(const StrArgs& a, int warps, uint32_t dyn_smem, cudaStream_t s, int sm_count) {
 	switch (a.kind) {
 	case STR_DICT:
 		if (a.rows16) {
-			return a.dict_in_smem ? launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, SM_BYTES, true>(a, warps, dyn_smem, s)
-			                      : launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, SM_NONE, true>(a, warps, dyn_smem, s);
+			return a.dict_in_smem ? launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, SM_BYTES, true>(a, warps, dyn_smem, s, sm_count)
+			                      : launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, SM_NONE, true>(a, warps, dyn_smem, s, sm_count);
 		}
-		return a.dict_in_smem ? launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, SM_BYTES>(a, warps, dyn_smem, s)
-		                      : launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, SM_NONE>(a, warps, dyn_smem, s);
-	case STR_FSST: return launch_str_kernel<STR_PASS_MATERIALIZE, STR_FSST, SM_NONE>(a, warps, dyn_smem, s);
-	case STR_FSST12: return launch_str_kernel<STR_PASS_MATERIALIZE, STR_FSST12, SM_NONE>(a, warps, dyn_smem, s);
-	default: return launch_str_kernel<STR_PASS_MATERIALIZE, STR_BYTES, SM_NONE>(a, warps, dyn_smem, s);
+		return a.dict_in_smem ? launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, SM_BYTES>(a, warps, dyn_smem, s, sm_count)
+		                      : launch_str_kernel<STR_PASS_MATERIALIZE, STR_DICT, SM_NONE>(a, warps, dyn_smem, s, sm_count);
+	case STR_FSST: return launch_stream_kernel<STR_PASS_MATERIALIZE, STR_FSST>(a, warps, dyn_smem, s, sm_count);
+	case STR_FSST12: return launch_str_kernel<STR_PASS_MATERIALIZE, STR_FSST12, SM_NONE>(a, warps, dyn_smem, s, sm_count);
+	default: return launch_stream_kernel<STR_PASS_MATERIALIZE, STR_BYTES>(a, warps, dyn_smem, s, sm_count);
 	}
 }
 
@@ -566,31 +919,35 @@ cudaError_t launch_str_materialize(const StrArgs& a, int warps, uint32_t dyn_sme
 // =========================================================================================================
 // Allocation-free decode of FSST / BYTE_ARR string pages (fls_gpu_decode_fsst_page_noalloc).
 //
-// The string plan keeps its scratch (per-vector byte totals and first-byte bases, the FSST table, a status
-// word) in cudaMalloc'd buffers.  This variant keeps the same scratch in one array compiled into the library,
-// so the call allocates nothing; in exchange the page may hold at most kNoAllocMaxVectors vectors.
+// The string plan keeps its scratch (per-vector byte totals and first-byte bases, the FSST table) in
+// cudaMalloc'd buffers and reports device errors through the library's per-device status word, which is
+// cudaMalloc'd on a device's first use.  This variant keeps the same scratch in one array compiled into the
+// library and reports errors through the caller's status word, so nothing on its path allocates: it reads the
+// SM count itself instead of going through current_device().  In exchange a page may hold at most
+// kNoAllocMaxVectors vectors.
 // =========================================================================================================
 namespace flsgpu {
 
 constexpr uint32_t kNoAllocMaxVectors = 8192; // 8,388,608 rows per call
 
 struct NoAllocLayout {
-	static constexpr size_t kStatus = 0;                                      // int, OR-ed device status
-	static constexpr size_t kTable  = 256;                                    // FsstTable (2304 B)
-	static constexpr size_t kTotal  = kTable + ((sizeof(FsstTable) + 255) & ~size_t(255));
-	static constexpr size_t kBase   = kTotal + 8 * (kNoAllocMaxVectors + 1);
-	static constexpr size_t kBytes  = kBase + 8 * (kNoAllocMaxVectors + 1);   // 133,376 B in all
+	static constexpr size_t kTable = 0;                                        // FsstTable (2304 B)
+	static constexpr size_t kTotal = kTable + ((sizeof(FsstTable) + 255) & ~size_t(255));
+	static constexpr size_t kBase  = kTotal + 8 * (kNoAllocMaxVectors + 1);
+	static constexpr size_t kBytes = kBase + 8 * (kNoAllocMaxVectors + 1);
 };
+static_assert(NoAllocLayout::kBytes == FLS_NOALLOC_SCRATCH_BYTES, "the header states the scratch size");
+static_assert(kNoAllocMaxVectors == FLS_NOALLOC_MAX_VECTORS, "the header states the vector limit");
 
 // Every GPU that loads the library holds this array until the process exits.
 static __device__ __align__(256) uint8_t g_noalloc_scratch[NoAllocLayout::kBytes];
 
-// Device address of g_noalloc_scratch on the current device, looked up once per device on the first call.
-static uint8_t* noalloc_scratch() {
+// Device address of g_noalloc_scratch on the current device, looked up once per device on the first call
+// (host code cannot use the symbol itself: on the host it names a stand-in, not device memory).
+static uint8_t* noalloc_scratch(int dev) {
 	static uint8_t*   addr[64] = {};
 	static std::mutex mu;
-	int               dev      = 0;
-	if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) { return nullptr; }
+	if (dev < 0 || dev >= 64) { return nullptr; }
 	std::lock_guard<std::mutex> lk(mu);
 	if (!addr[dev]) {
 		void* p = nullptr;
@@ -602,20 +959,28 @@ static uint8_t* noalloc_scratch() {
 
 int fsst_import_table(const uint8_t* buf, uint64_t avail, FsstTable* t, uint64_t* used);
 
+// n bytes from device memory into host memory in the stream's order (after the work queued on it before).
+static bool read_in_stream_order(void* dst, const void* src, uint64_t n, cudaStream_t s) {
+	return cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+	       cudaStreamSynchronize(s) == cudaSuccess;
+}
+
 } // namespace flsgpu
 
 extern "C" int fls_gpu_decode_fsst_page_noalloc(const uint8_t* d_page, uint64_t page_size, const uint8_t* d_dict,
                                                 uint64_t dict_size, uint32_t* d_offsets, uint8_t* d_bytes,
                                                 uint64_t bytes_cap, int* d_status, void* stream) {
 	using namespace flsgpu;
-	if (!d_page || !d_offsets || (!d_bytes && bytes_cap) || (reinterpret_cast<uintptr_t>(d_bytes) & 15u) != 0 ||
-	    bytes_cap >= (1ull << 32)) {
+	if (!d_page || !d_offsets || !d_status || (!d_bytes && bytes_cap) ||
+	    (reinterpret_cast<uintptr_t>(d_bytes) & 15u) != 0 || bytes_cap >= (1ull << 32)) {
 		return FLS_ERR_ARG;
 	}
-	cudaStream_t s = static_cast<cudaStream_t>(stream);
-	uint8_t      hdr[8 + 4 * 5];
+	cudaStream_t   s = static_cast<cudaStream_t>(stream);
+	uint8_t        hdr[8 + 4 * 5];
 	const uint64_t take = page_size < sizeof(hdr) ? page_size : sizeof(hdr);
-	if (take < 8 || cudaMemcpy(hdr, d_page, take, cudaMemcpyDeviceToHost) != cudaSuccess) { return FLS_ERR_FORMAT; }
+	if (take < 8) { return FLS_ERR_FORMAT; }
+	// the page may have been written by work the caller queued on this stream: read it in the stream's order
+	if (!read_in_stream_order(hdr, d_page, take, s)) { return FLS_ERR_CUDA; }
 	uint8_t kind = 0, arr_c = 0, ws = 32, enc = ENC_RAW, ib_packed = 1, ib_bw = kNoBuf, ib_base = kNoBuf,
 	        ib_lane = kNoBuf;
 	if (hdr[0] == 7 && hdr[1] == 1) {
@@ -641,24 +1006,22 @@ extern "C" int fls_gpu_decode_fsst_page_noalloc(const uint8_t* d_page, uint64_t 
 		c.buf[i]      = d_page + off[i];
 		c.buf_size[i] = end - off[i];
 	}
-	uint8_t* scratch = noalloc_scratch();
+	int dev = 0, sms = 0;
+	if (cudaGetDevice(&dev) != cudaSuccess ||
+	    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) {
+		return FLS_ERR_CUDA;
+	}
+	uint8_t* scratch = noalloc_scratch(dev);
 	if (!scratch) { return FLS_ERR_CUDA; }
 	FsstTable tab {};
 	if (kind == STR_FSST) {
 		// dict_hdr_t followed by the exported symbol table (at most FSST_MAXHEADER = 2066 bytes)
 		uint8_t        h[8 + 2066];
 		const uint64_t n = dict_size < sizeof(h) ? dict_size : sizeof(h);
-		if (!d_dict || n < 8 + 17 || cudaMemcpy(h, d_dict, n, cudaMemcpyDeviceToHost) != cudaSuccess) {
-			return FLS_ERR_FORMAT;
-		}
+		if (!d_dict || n < 8 + 17) { return FLS_ERR_FORMAT; }
+		if (!read_in_stream_order(h, d_dict, n, s)) { return FLS_ERR_CUDA; }
 		const int rc = fsst_import_table(h + 8, n - 8, &tab, nullptr);
 		if (rc != FLS_OK) { return rc; }
-	}
-	// the table and a zero status are the only scratch contents a call relies on; totals and bases are
-	// rewritten in full by every call
-	if (cudaMemcpyAsync(scratch + NoAllocLayout::kTable, &tab, sizeof(tab), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-	    cudaMemsetAsync(scratch + NoAllocLayout::kStatus, 0, sizeof(int), s) != cudaSuccess) {
-		return FLS_ERR_CUDA;
 	}
 	c.ws            = ws;
 	c.e             = 4;
@@ -675,6 +1038,13 @@ extern "C" int fls_gpu_decode_fsst_page_noalloc(const uint8_t* d_page, uint64_t 
 	c.ib_vals       = kNoBuf;
 	c.ep            = reinterpret_cast<const uint32_t*>(d_page + 8 + 4 * arr_c);
 	if (vec_c == 0) { return cudaMemsetAsync(d_offsets, 0, 4, s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA; }
+	// the table is the only scratch content a call relies on; totals and bases are rewritten in full by every
+	// call.  A copy from pageable host memory has read its source when cudaMemcpyAsync returns, so the table may
+	// live in this stack frame.
+	if (kind == STR_FSST &&
+	    cudaMemcpyAsync(scratch + NoAllocLayout::kTable, &tab, sizeof(tab), cudaMemcpyHostToDevice, s) != cudaSuccess) {
+		return FLS_ERR_CUDA;
+	}
 	StrArgs a {};
 	a.col       = c;
 	a.kind      = kind;
@@ -684,16 +1054,11 @@ extern "C" int fls_gpu_decode_fsst_page_noalloc(const uint8_t* d_page, uint64_t 
 	a.offsets   = d_offsets;
 	a.bytes     = d_bytes;
 	a.bytes_cap = bytes_cap;
-	a.status    = d_status ? d_status : reinterpret_cast<int*>(scratch + NoAllocLayout::kStatus);
-	int sms = 0, dev = 0;
-	if (cudaGetDevice(&dev) != cudaSuccess ||
-	    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) {
-		return FLS_ERR_CUDA;
-	}
+	a.status    = d_status;
 	if (launch_str_lengths(a, sms, s) != cudaSuccess ||
 	    launch_scan_totals(a.vec_total, reinterpret_cast<uint64_t*>(scratch + NoAllocLayout::kBase), vec_c, s) !=
 	        cudaSuccess ||
-	    launch_str_materialize(a, kStrLenWarps, kStrLenWarps * str_smem_per_warp(false), s) != cudaSuccess) {
+	    launch_str_materialize(a, kStrLenWarps, kStrLenWarps * str_smem_per_warp(false), s, sms) != cudaSuccess) {
 		return FLS_ERR_CUDA;
 	}
 	return FLS_OK;

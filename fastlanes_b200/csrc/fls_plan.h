@@ -102,6 +102,11 @@ struct DecodeArgs {
 	uint32_t        col_shift; // 24 for batch plans (256 batches), 16 for page plans (65,535 pages)
 	ColDesc         col0;
 	Pred            pred; // filter launches (KIND_FILTER kernels) only
+	// failure injection (fls_gpu_test_stalled_copy only; 0 otherwise): work item test_stall - 1 arms its copies'
+	// byte count without issuing them, so nothing is in flight and its wait runs out; spin_limit bounds the
+	// decode loop's waits (0: kMbarSpinLimit)
+	uint64_t        test_stall;
+	uint32_t        spin_limit;
 };
 
 enum : int {

@@ -202,4 +202,312 @@ __device__ __forceinline__ T warp_sum(T x) {
 	return x;
 }
 
+// ---------------------------------------------------------------------------------------------------------
+// Code-parallel decode of one vector of an FSST (or BYTE_ARR) column, one warp.
+//
+// The rows of a vector are consecutive in its compressed bytes (row r is [end[r-1], end[r])), and FSST is
+// context-free except for escapes, so the vector's bytes [0, end[1023]) decode as ONE stream whose output is the
+// rows' bytes concatenated; row r's output offset is the decoded length of the stream before byte end[r-1].
+// The warp walks the stream 128 bytes at a time, 4 bytes per lane:
+//   * which bytes start a code: a byte is an escaped literal when the code before it is an escape (255); rows
+//     restart the decoder (a row's first byte always starts a code).  Each lane composes the 2-state transfer
+//     function of its 4 bytes (state 1 = "the next byte is a literal"), a warp scan of the functions gives every
+//     lane its entry state.  Chunks without a 255 (nearly all of them) skip this: every byte starts a code.
+//   * decoded lengths (symbol length; 1 for an escape; 0 for its literal) are prefix-summed across the warp;
+//   * every lane writes its symbols at its offset into the warp's output window as whole words
+//     (put_syms: the put_row protocol), and rows starting in the chunk take their offsets from the sums.
+// An escape as a row's last byte decodes as one zero byte (as the oracle's row decoder does).
+// ---------------------------------------------------------------------------------------------------------
+constexpr uint32_t kStreamChunk = 128; // stream bytes per warp step
+
+__device__ __forceinline__ uint32_t stream_row_start(const uint32_t* rows32, uint32_t r) {
+	return r == 0 ? 0u : rows32[(r - 1) + ((r - 1) >> 5)];
+}
+
+// Escape-state transfer of one lane's bytes (bit j of esc: byte j is 255; of rs: a row starts at byte j; nv
+// valid bytes): the state after them for entry state st.
+__device__ __forceinline__ uint32_t esc_transfer(uint32_t st, uint32_t esc, uint32_t rs, uint32_t nv) {
+#pragma unroll
+	for (uint32_t j = 0; j < 4; ++j) {
+		if (j < nv) {
+			if ((rs >> j) & 1u) { st = 0; }
+			st = st ? 0u : ((esc >> j) & 1u);
+		}
+	}
+	return st;
+}
+
+// transfer functions as 2 bits, f(0) | f(1) << 1
+__device__ __forceinline__ uint32_t fn_apply(uint32_t f, uint32_t x) { return (f >> x) & 1u; }
+__device__ __forceinline__ uint32_t fn_compose(uint32_t later, uint32_t earlier) {
+	return fn_apply(later, fn_apply(earlier, 0)) | (fn_apply(later, fn_apply(earlier, 1)) << 1);
+}
+
+// Row starts inside [cb, cb + 128): the 128-bit mask m (bit i: a row starts at byte cb + i) and whether a row
+// starts at cb + 128.  *rc: on entry a row index at or before the first row starting at or after cb (rows
+// before cb are skipped); on return the first row starting at or after cb + 128.
+__device__ __forceinline__ void stream_row_mask(const uint32_t* rows32, uint32_t cb, uint32_t lane, uint32_t* rc,
+                                                uint32_t m[4], bool* at_end) {
+	m[0] = m[1] = m[2] = m[3] = 0;
+	*at_end  = false;
+	uint32_t r = *rc;
+	while (r < kVec) {
+		const uint32_t rr  = r + lane;
+		const uint32_t s   = rr < kVec ? stream_row_start(rows32, rr) : 0xFFFFFFFFu;
+		const bool     in  = s >= cb && s < cb + kStreamChunk;
+		const uint32_t rel = s - cb;
+#pragma unroll
+		for (uint32_t k = 0; k < 4; ++k) {
+			m[k] |= __reduce_or_sync(0xFFFFFFFFu, (in && (rel >> 5) == k) ? 1u << (rel & 31u) : 0u);
+		}
+		const uint32_t n = __popc(__ballot_sync(0xFFFFFFFFu, s < cb + kStreamChunk));
+		r += n;
+		if (n < 32) {
+			*at_end = __any_sync(0xFFFFFFFFu, s == cb + kStreamChunk);
+			break;
+		}
+	}
+	*rc = r;
+}
+
+// A lane's decoded bytes -- up to 4 symbols (value, length; length 0 = nothing) in order -- into the word
+// window at byte d, whole words: every word is stored by the lane owning its first byte, bytes past the lane's
+// end zero; a lane starting inside a word returns its bytes of that word (*hk, *head) for an atomic OR after a
+// warp sync (the protocol of put_row).  Returns whether such a head is left.
+__device__ __forceinline__ bool put_syms(uint32_t* win, uint32_t d, const uint64_t (&sv)[4], const uint32_t (&sl)[4],
+                                         uint32_t* hk, uint32_t* head) {
+	const uint32_t k0   = d >> 2;
+	const bool     mid  = (d & 3u) != 0;
+	uint32_t       k    = k0;
+	uint32_t       nb   = 8u * (d & 3u);
+	uint64_t       acc  = 0;
+	uint32_t       hi   = 0;
+	bool           any  = false, held = false;
+	auto           emit = [&](uint32_t w) {
+        if (k == k0 && mid) {
+            *hk   = k;
+            *head = w;
+            held  = true;
+        } else {
+            win[k] = w;
+        }
+        ++k;
+	};
+#pragma unroll
+	for (int j = 0; j < 4; ++j) {
+		const uint32_t l = sl[j];
+		if (l == 0) { continue; }
+		any = true;
+		acc |= sv[j] << nb; // nb < 32 here
+		if (nb) { hi |= static_cast<uint32_t>(sv[j] >> (64u - nb)); }
+		nb += 8u * l;
+		while (nb >= 32u) {
+			emit(static_cast<uint32_t>(acc));
+			acc = (acc >> 32) | (static_cast<uint64_t>(hi) << 32);
+			hi  = 0;
+			nb -= 32u;
+		}
+	}
+	if (any && nb > 8u * ((k == k0) ? (d & 3u) : 0u)) { emit(static_cast<uint32_t>(acc)); }
+	return held;
+}
+
+// Per-vector output of the materialising pass.
+struct StreamOut {
+	uint32_t* offsets;   // the vector's 1024 row offsets
+	uint8_t*  bytes;     // output bytes (global)
+	uint64_t  vbase;     // the vector's first output byte
+	uint8_t*  win;       // the warp's kWindow-byte output window (shared memory, 16-byte aligned)
+};
+
+// One vector of an FSST (KIND_FSST = true) or BYTE_ARR column: rows32 its 1024 cumulative row end offsets in
+// original order (row r at word r + r / 32), vb / vn its compressed bytes (vn 0 and rows all zero for none).
+// Returns the decoded byte total; MAT also writes the offsets and bytes (o).  *bad: the rows are not
+// non-decreasing within vn (the vector then decodes as 1024 empty rows).
+template <bool MAT, bool KIND_FSST, uint32_t kWindow>
+__device__ __forceinline__ uint32_t stream_vector(const uint32_t* rows32, const uint8_t* vb, uint32_t vn,
+                                                  const uint64_t* sym, const uint8_t* len, uint32_t lane,
+                                                  const StreamOut& o, bool* bad) {
+	// rows must be non-decreasing and end inside the vector's bytes
+	{
+		uint32_t prev = lane == 0 ? 0u : rows32[(32 * lane - 1) + lane - 1];
+		bool     b    = false;
+#pragma unroll 8
+		for (uint32_t i = 0; i < 32; ++i) {
+			const uint32_t e = rows32[32 * lane + i + lane];
+			b |= e < prev;
+			prev = e;
+		}
+		b |= lane == 31 && prev > vn;
+		*bad = __any_sync(0xFFFFFFFFu, b);
+	}
+	const uint32_t  L     = *bad ? 0u : rows32[kVec - 1 + (kVec - 1) / 32];
+	if constexpr (!KIND_FSST && !MAT) { return L; } // a plain-bytes vector decodes to its own bytes
+	const uintptr_t va    = reinterpret_cast<uintptr_t>(vb);
+	const uint32_t  off   = static_cast<uint32_t>(va & 3u);
+	const uint32_t* base  = reinterpret_cast<const uint32_t*>(va - off);
+	const uint32_t  nw    = (off + L + 3u) >> 2; // words holding a byte of the stream [0, L)
+	uint32_t*       win32 = reinterpret_cast<uint32_t*>(o.win);
+	uint32_t        carry = 0; // 1: the chunk's first byte is an escaped literal
+	uint32_t        vdec  = 0; // decoded bytes before the chunk
+	uint32_t        rc    = 0; // first row whose offset is not written (MAT) / a row at or before cb (lengths)
+
+	// window of the materialising pass: W = output position of win[0], fill bytes in it, lo = first output byte
+	// it may write (the previous vector owns the bytes before vbase)
+	uint64_t W    = o.vbase & ~15ull;
+	uint32_t fill = static_cast<uint32_t>(o.vbase & 15u);
+	uint64_t lo   = o.vbase;
+	if constexpr (MAT) {
+		// the first lane may start inside this word: it ORs its bytes in
+		if (lane == 0) { win32[fill >> 2] = 0; }
+		__syncwarp();
+	}
+	auto flush = [&](bool all) {
+		const uint32_t full = fill & ~15u;
+		const uint32_t upto = all ? fill : full;
+		for (uint32_t c = 16 * lane; c < upto; c += 512) {
+			const uint64_t g = W + c;
+			if (g >= lo && c + 16 <= upto) {
+				*reinterpret_cast<uint4*>(o.bytes + g) = *reinterpret_cast<const uint4*>(o.win + c);
+			} else {
+				for (uint32_t i = 0; i < 16 && c + i < upto; ++i) {
+					if (g + i >= lo) { o.bytes[g + i] = o.win[c + i]; }
+				}
+			}
+		}
+		__syncwarp();
+		if (!all) {
+			// the partial chunk [full, fill) moves to the window start (its bytes past `fill` are zero: every word
+			// was stored whole, zeros past its writer's end)
+			if (lane == 0 && full != 0 && (fill & 15u) != 0) {
+				*reinterpret_cast<uint4*>(o.win) = *reinterpret_cast<const uint4*>(o.win + full);
+			}
+			__syncwarp();
+			W += full;
+			fill &= 15u;
+			lo = lo > W ? lo : W;
+		}
+	};
+
+	for (uint32_t cb = 0; cb < L; cb += kStreamChunk) {
+		const uint32_t q  = (cb >> 2) + lane;
+		const uint32_t w0 = q < nw ? __ldg(base + q) : 0u;
+		uint32_t       w1 = __shfl_down_sync(0xFFFFFFFFu, w0, 1);
+		if (lane == 31) { w1 = q + 1 < nw ? __ldg(base + q + 1) : 0u; }
+		const uint32_t b4    = off ? __funnelshift_r(w0, w1, 8u * off) : w0; // stream bytes cb+4l .. +3
+		const uint32_t bnext = (w1 >> (8u * off)) & 0xFFu;                   // stream byte cb+4l+4
+		const uint32_t pos0  = cb + 4 * lane;
+		const uint32_t nv    = pos0 >= L ? 0u : (L - pos0 < 4u ? L - pos0 : 4u);
+		uint64_t       sv[4];
+		uint32_t       sl[4];
+		if constexpr (!KIND_FSST) {
+#pragma unroll
+			for (uint32_t j = 0; j < 4; ++j) {
+				sv[j] = (b4 >> (8 * j)) & 0xFFu;
+				sl[j] = j < nv ? 1u : 0u;
+			}
+		} else {
+			uint32_t esc = 0;
+#pragma unroll
+			for (uint32_t j = 0; j < 4; ++j) { esc |= (j < nv && ((b4 >> (8 * j)) & 0xFFu) == 255u) ? 1u << j : 0u; }
+			if (!__any_sync(0xFFFFFFFFu, esc != 0 || carry != 0)) {
+				// no escape anywhere in the chunk: every byte starts a code
+#pragma unroll
+				for (uint32_t j = 0; j < 4; ++j) {
+					const uint32_t c = (b4 >> (8 * j)) & 0xFFu;
+					sv[j]            = sym[c];
+					sl[j]            = j < nv ? len[c] : 0u;
+				}
+			} else {
+				uint32_t m[4];
+				bool     at_end;
+				uint32_t r = rc;
+				stream_row_mask(rows32, cb, lane, &r, m, &at_end);
+				if constexpr (!MAT) { rc = r; }
+				const uint32_t mk = (lane >> 3) == 0 ? m[0] : (lane >> 3) == 1 ? m[1] : (lane >> 3) == 2 ? m[2] : m[3];
+				const uint32_t rs = (mk >> ((4 * lane) & 31u)) & 0xFu;
+				uint32_t       rs4;
+				if ((lane & 7u) != 7u) {
+					rs4 = (mk >> ((4 * lane + 4) & 31u)) & 1u;
+				} else {
+					const uint32_t mn = (lane >> 3) == 0 ? m[1] : (lane >> 3) == 1 ? m[2] : m[3];
+					rs4               = lane == 31 ? (at_end ? 1u : 0u) : (mn & 1u);
+				}
+				// entry state of every lane: warp scan of the transfer functions
+				const uint32_t f    = esc_transfer(0, esc, rs, nv) | (esc_transfer(1, esc, rs, nv) << 1);
+				uint32_t       incl = f;
+#pragma unroll
+				for (int d = 1; d < 32; d <<= 1) {
+					const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+					if (lane >= static_cast<uint32_t>(d)) { incl = fn_compose(incl, y); }
+				}
+				uint32_t excl = __shfl_up_sync(0xFFFFFFFFu, incl, 1);
+				if (lane == 0) { excl = 2u; } // identity
+				uint32_t       st  = fn_apply(excl, carry);
+				const uint32_t all = __shfl_sync(0xFFFFFFFFu, incl, 31);
+				carry              = fn_apply(all, carry);
+#pragma unroll
+				for (uint32_t j = 0; j < 4; ++j) {
+					const uint32_t c = (b4 >> (8 * j)) & 0xFFu;
+					sv[j]            = 0;
+					sl[j]            = 0;
+					if (j < nv) {
+						if ((rs >> j) & 1u) { st = 0; }
+						if (st) {
+							st = 0; // the escaped literal: emitted with its escape
+						} else if (c == 255u) {
+							// the literal: the next byte unless the row (or the stream) ends first
+							const uint32_t nb    = j < 3 ? (b4 >> (8 * (j + 1))) & 0xFFu : bnext;
+							const bool     nvld  = j < 3 ? j + 1 < nv : pos0 + 4 < L;
+							const bool     nrow  = j < 3 ? ((rs >> (j + 1)) & 1u) != 0 : rs4 != 0;
+							sv[j]                = (nvld && !nrow) ? nb : 0u;
+							sl[j]                = 1;
+							st                   = 1;
+						} else {
+							sv[j] = sym[c];
+							sl[j] = len[c];
+						}
+					}
+				}
+			}
+		}
+		// decoded offsets: lane sum, warp exclusive scan, chunk total
+		const uint32_t e   = sl[0] + sl[1] + sl[2] + sl[3];
+		const uint32_t inc = warp_inclusive_scan(e, lane);
+		const uint32_t X   = inc - e;
+		const uint32_t T   = __shfl_sync(0xFFFFFFFFu, inc, 31);
+		if constexpr (MAT) {
+			// offsets of the rows starting in this chunk (before cb + 128): from the owner lane of their first byte
+			const uint32_t part = sl[0] | ((sl[0] + sl[1]) << 8) | ((sl[0] + sl[1] + sl[2]) << 16);
+			while (rc < kVec) {
+				const uint32_t rr  = rc + lane;
+				const uint32_t s   = rr < kVec ? stream_row_start(rows32, rr) : 0xFFFFFFFFu;
+				const bool     in  = s < cb + kStreamChunk;
+				const uint32_t rel = s - cb;
+				const uint32_t own = (rel >> 2) & 31u, sub = rel & 3u;
+				const uint32_t xo  = __shfl_sync(0xFFFFFFFFu, X, own);
+				const uint32_t po  = __shfl_sync(0xFFFFFFFFu, part, own);
+				if (in) { o.offsets[rr] = static_cast<uint32_t>(o.vbase + vdec + xo + (sub ? (po >> (8 * (sub - 1))) & 0xFFu : 0u)); }
+				const uint32_t n = __popc(__ballot_sync(0xFFFFFFFFu, in));
+				rc += n;
+				if (n < 32) { break; }
+			}
+			if (fill + T > kWindow) { flush(false); }
+			uint32_t hk = 0, head = 0;
+			const bool mid = put_syms(win32, fill + X, sv, sl, &hk, &head);
+			__syncwarp(); // every word's whole store lands before the lanes that start inside it OR in
+			if (mid) { atomicOr(win32 + hk, head); }
+			__syncwarp();
+			fill += T;
+		}
+		vdec += T;
+	}
+	if constexpr (MAT) {
+		// rows starting at the stream's end (and every row of an empty or bad vector)
+		for (uint32_t r = rc + lane; r < kVec; r += 32) { o.offsets[r] = static_cast<uint32_t>(o.vbase + vdec); }
+		flush(true);
+	}
+	return vdec;
+}
+
 } // namespace flsgpu

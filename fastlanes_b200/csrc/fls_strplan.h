@@ -44,8 +44,8 @@ struct StrArgs {
 	// materialising pass: entry c as start | length << 24 (dictionaries of < 16 MiB decoded bytes whose
 	// entries are all < 256 bytes), one load per row instead of two end offsets; null otherwise
 	const uint32_t*  dict_rows;
-	// FSST / FSST12 pages: every row's decoded length, written by the lengths pass and read by the materialising
-	// pass instead of walking the row's codes a second time (null: both walk them)
+	// FSST12 pages: every row's decoded length, written by the lengths pass and read by the materialising pass
+	// instead of walking the row's codes a second time (null: both walk them)
 	uint32_t*        row_len;
 	const uint8_t*   dict_bytes;
 	uint64_t         dict_bytes_n;
@@ -57,16 +57,45 @@ struct StrArgs {
 	uint8_t*         bytes;
 	uint64_t         bytes_cap;
 	int*             status;
+	uint64_t         item_base; // single-pass DICT decode: index of the column's vector 0 among the look-back words
 };
+
+// One launch of the single-pass DICT decode (k_dict_pass) over the vectors of one or more DICT string columns.
+// Work is taken in chunks of chunk_w vectors of one column (a chunk per CTA, by an atomic ticket); every vector
+// publishes its decoded byte total and, once its predecessors' totals are known, its inclusive prefix (a
+// decoupled look-back within its column), so each vector learns its first output byte without a separate
+// lengths pass.
+struct StrSetArgs {
+	const StrArgs*  cols;      // per-column arguments in device memory (each with dict_rows: start | length << 24)
+	const uint32_t* chunk_col; // column of every chunk (null: one column, chunk c = its vectors [c * chunk_w, ...))
+	const uint32_t* chunk_v0;  // first vector of every chunk (null: as above)
+	uint32_t        n_chunks;
+	uint32_t        chunk_w;   // vectors per chunk = warps per CTA
+	uint64_t*       flags;     // [0] the chunk ticket, [1 + item_base + v] the look-back word of vector v; zeroed
+	                           // before every launch
+	int*            status;
+	uint32_t*       out_offsets; // one-column launches: the outputs (null: each column's own)
+	uint8_t*        out_bytes;
+	uint64_t        out_cap;
+	uint32_t        dict_cap; // shared memory held for a dictionary's bytes (16-byte multiple; 0: dictionaries in
+	                          // global memory)
+	uint32_t        tab_cap;  // entries held for the packed row table (with dict_cap)
+};
+
+// per-warp shared memory of k_dict_pass: the vector's rows and the output window
+uint32_t dict_pass_smem_per_warp(bool rows16);
+cudaError_t launch_dict_pass(const StrSetArgs& a, bool rows16, int warps, uint32_t dyn_smem, cudaStream_t s,
+                             int sm_count = 0);
 
 cudaError_t launch_fsst_dict(const uint8_t* lens, const uint8_t* comp, uint64_t comp_size, uint32_t entry_c,
                              const FsstTable* tab, uint32_t* ends, uint8_t* bytes, uint64_t cap, int* status,
                              cudaStream_t s);
-cudaError_t launch_str_lengths(const StrArgs& a, int grid, cudaStream_t s);
+// sm_count: the device's SM count, or 0 to take it from the library's per-device state (current_device())
+cudaError_t launch_str_lengths(const StrArgs& a, int sm_count, cudaStream_t s);
 cudaError_t launch_scan_totals(const uint64_t* total, uint64_t* base, uint64_t n, cudaStream_t s);
 // warps: warps per CTA (at most kStrMaxWarps); dyn_smem: warps * str_smem_per_warp(a.rows16) plus the
 // 16-byte rounded dictionary bytes when a.dict_in_smem
-cudaError_t launch_str_materialize(const StrArgs& a, int warps, uint32_t dyn_smem, cudaStream_t s);
+cudaError_t launch_str_materialize(const StrArgs& a, int warps, uint32_t dyn_smem, cudaStream_t s, int sm_count = 0);
 uint32_t    str_smem_per_warp(bool rows16);
 // shared-memory bytes of the dictionary end offsets (16-byte rounded)
 __host__ __device__ inline uint32_t str_ends_smem(const StrArgs& a) { return (a.entry_c * 4u + 15u) & ~15u; }

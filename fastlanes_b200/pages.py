@@ -34,6 +34,10 @@ _dec_checked = declare("fls_decode_to_memory_checked", ctypes.c_int, [_p, _u64, 
 declare("encode_from_memory", ctypes.c_bool, [_p, _u64, _u64, _p, ctypes.POINTER(_u64), ctypes.POINTER(_u64),
                                               ctypes.c_uint8, ctypes.c_uint8])
 declare("decode_to_memory", None, [_p, _p, ctypes.c_uint8])
+_ra_ranges = declare("fls_random_access_ranges", ctypes.c_int, [_p, _u64, ctypes.POINTER(_u64), _p])
+_ra_decode = declare("fls_random_access_decode", ctypes.c_int, [_p, _u64, _u64, _p, _p, _p])
+declare("init_random_access", None, [_p, _u64, ctypes.POINTER(_u64), _p])
+declare("random_access", None, [_p, _u64, ctypes.POINTER(_u64), _p, _p, _p])
 declare("fls_cpi_connection_open", _p, [])
 declare("fls_cpi_connection_close", None, [_p])
 
@@ -235,4 +239,26 @@ def decode_to_memory(page, data_type, size=None):
     n = _u64()
     check(_dec_checked(_ptr(page), page.size if size is None else size, _ptr(out), out.nbytes, data_type,
                        ctypes.byref(n)), "decode_to_memory")
+    return out
+
+
+def random_access_ranges(page, vector):
+    """fastlanes.h init_random_access: the [offset, size] byte ranges of the buffers one vector of an INT64 page
+    needs (host only; reads the page's metadata)."""
+    page = np.ascontiguousarray(page, np.uint8)
+    n = _u64()
+    pairs = np.zeros(12, np.uint64)
+    check(_ra_ranges(_ptr(page), vector, ctypes.byref(n), _ptr(pairs)), "init_random_access")
+    return pairs[: 2 * n.value].reshape(-1, 2)
+
+
+def random_access(page, vector, buffers, ranges):
+    """fastlanes.h random_access: vector `vector` of an INT64 page from its loaded buffers (host arrays, one per
+    range of random_access_ranges); returns its 1024 values in original order."""
+    bufs = [np.ascontiguousarray(b, np.uint8) for b in buffers]
+    ptrs = (_p * len(bufs))(*[b.ctypes.data for b in bufs])
+    pairs = np.ascontiguousarray(ranges, np.uint64).reshape(-1)
+    out = np.zeros(1024, np.int64)
+    page = np.ascontiguousarray(page, np.uint8)
+    check(_ra_decode(_ptr(page), vector, len(bufs), _ptr(pairs), ctypes.cast(ptrs, _p), _ptr(out)), "random_access")
     return out

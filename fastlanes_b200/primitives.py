@@ -139,3 +139,14 @@ def analyze(x, signed=False):
 def device_status(reset=True):
     """OR of device-side error bits since the last reset (synchronises)."""
     return lib.fls_gpu_status(int(reset))
+
+
+def stalled_unffor(packed, bw, base, byte_off, stall_vector, spin_limit):
+    """fls_gpu_test_stalled_copy (failure injection): unffor u32 where vector `stall_vector`'s staging copy is
+    armed but never issued, so its bounded wait runs out.  Returns (output, call status); the device status
+    word then carries FLS_DEV_TIMEOUT."""
+    n = bw.numel()
+    out = torch.zeros(n * 1024, dtype=torch.uint32, device=base.device)
+    rc = lib.fls_gpu_test_stalled_copy(_ptr(packed), _ptr(out), _ptr(bw), _ptr(base), _ptr(byte_off), n, stall_vector,
+                                       spin_limit, _stream())
+    return out, rc

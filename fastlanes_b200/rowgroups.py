@@ -126,10 +126,10 @@ class RowGroupSet:
 
 class StringColumnSet:
     """String columns of a row-group set, each a DICT page (the string pool's DICT FFOR_NO_PATCH, id 3) over an
-    FSST-compressed dictionary page, decoded by one string plan per column into Arrow offsets + bytes.
+    FSST-compressed dictionary, all decoded by one string set (one kernel launch) into Arrow offsets + bytes.
 
     columns: list of (dictionary bytes, dictionary offsets, codes) host arrays.  decode() only launches
-    kernels (capturable in a CUDA graph together with the integer plan)."""
+    (capturable in a CUDA graph together with the integer plan)."""
 
     def __init__(self, columns, device="cuda"):
         from . import strings as S
@@ -153,48 +153,36 @@ class StringColumnSet:
             self.dict_bytes += dic.size
             self.rows += plan.n_rows
             self.value_bytes += 4 * (plan.n_rows + 1) + n
+        self.set = S.StringSet(self.plans)
+        self.set.bind([o for o, _, _ in self.outputs], [d for _, d, _ in self.outputs])
 
     def decode(self, streams=None, join=True):
-        """Every column's decode; with `streams`, column i runs on streams[i % len(streams)], each stream
-        ordered after the current one and (with `join`) the current one after all of them, so the columns
-        overlap, also inside a CUDA graph capture.  join=False leaves the current stream free for other work
-        that then overlaps the columns; join(streams) closes the fork."""
+        """Every column's decode (one launch); with `streams`, on streams[0], ordered after the current stream
+        and (with `join`) the current stream after it, so it overlaps other work on the current stream, also
+        inside a CUDA graph capture.  join(streams) closes the fork."""
         if not streams:
-            for plan, (offs, data, _) in zip(self.plans, self.outputs):
-                plan.decode_into(offs, data)
+            self.set.decode()
             return
         cur = torch.cuda.current_stream()
-        for s in streams:
-            s.wait_stream(cur)
-        for i, (plan, (offs, data, _)) in enumerate(zip(self.plans, self.outputs)):
-            s = streams[i % len(streams)]
-            with torch.cuda.stream(s):
-                plan.decode_into(offs, data, stream=s.cuda_stream)
+        streams[0].wait_stream(cur)
+        with torch.cuda.stream(streams[0]):
+            self.set.decode(stream=streams[0].cuda_stream)
         if join:
             self.join(streams)
 
     @staticmethod
     def join(streams):
-        cur = torch.cuda.current_stream()
-        for s in streams:
-            cur.wait_stream(s)
+        torch.cuda.current_stream().wait_stream(streams[0])
 
-    def check(self, columns, samples=256, seed=7):
-        """Offsets equal to the dictionary lengths' prefix sums, and a sample of rows byte-exact."""
-        rng = np.random.default_rng(seed)
-        for (dbytes, doffs, codes), (offs, data, n) in zip(columns, self.outputs):
-            lens = np.diff(doffs).astype(np.int64)
-            want = np.zeros(codes.size + 1, np.int64)
-            want[1:] = np.cumsum(lens[codes])
-            if not np.array_equal(offs.cpu().numpy().astype(np.int64), want):
-                return False
-            host = data[:n].cpu().numpy()
-            for r in rng.integers(0, codes.size, samples):
-                c = int(codes[r])
-                if not np.array_equal(host[want[r]:want[r + 1]], dbytes[int(doffs[c]):int(doffs[c + 1])]):
-                    return False
-        return True
+    def check(self, columns):
+        """Every column's offsets and every byte against the generator's rows (row r is dictionary entry
+        codes[r]), compared whole on the device."""
+        from .workloads import dict_rows_match
+
+        return all(dict_rows_match(offs, data[:n], dbytes, doffs, codes)
+                   for (dbytes, doffs, codes), (offs, data, n) in zip(columns, self.outputs))
 
     def close(self):
+        self.set.close()
         for p in self.plans:
             p.close()

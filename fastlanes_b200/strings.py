@@ -15,11 +15,16 @@ _measure = declare("fls_string_plan_measure", ctypes.c_int, [_p, ctypes.POINTER(
 _decode = declare("fls_string_plan_decode", ctypes.c_int, [_p, _p, _p, _u64, _p])
 _destroy = declare("fls_string_plan_destroy", ctypes.c_int, [_p])
 _noalloc = declare("fls_gpu_decode_fsst_page_noalloc", ctypes.c_int, [_p, _u64, _p, _u64, _p, _p, _u64, _p, _p])
+_set_create = declare("fls_string_set_create", ctypes.c_int, [_p, ctypes.c_uint32, ctypes.POINTER(_p)])
+_set_bind = declare("fls_string_set_bind", ctypes.c_int, [_p, _p, _p, _p])
+_set_decode = declare("fls_string_set_decode", ctypes.c_int, [_p, _p])
+_set_destroy = declare("fls_string_set_destroy", ctypes.c_int, [_p])
 
 
-def decode_fsst_page_noalloc(d_page, page_size, d_dict, dict_size, offsets, data, status=None, stream=None):
+def decode_fsst_page_noalloc(d_page, page_size, d_dict, dict_size, offsets, data, status, stream=None):
     """Allocation-free decode of an FSST / BYTE_ARR page into caller-owned offsets (int32, n_rows + 1) and data
-    (uint8) tensors; returns the status code (0 = ok, -6 = page beyond the fixed scratch)."""
+    (uint8) tensors.  status: a zeroed int32 device tensor that receives the device-detected errors (FLS_DEV_*);
+    returns the call's status code (0 = ok, -6 = page beyond the fixed scratch)."""
     s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
     return _noalloc(d_page, page_size, d_dict, dict_size, offsets.data_ptr(), data.data_ptr(), data.numel(),
                     status.data_ptr() if status is not None else None, s)
@@ -56,6 +61,44 @@ class StringPlan:
     def close(self):
         if self.handle:
             _destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class StringSet:
+    """Many DICT string plans decoded by one kernel launch (fls_string_set_*).  The plans and the bound output
+    tensors must outlive the set; decode() only launches (capturable in a CUDA graph)."""
+
+    def __init__(self, plans):
+        arr = (_p * len(plans))(*[p.handle.value for p in plans])
+        h = _p()
+        check(_set_create(ctypes.cast(arr, _p), len(plans), ctypes.byref(h)), "fls_string_set_create")
+        self.handle = h
+        self.n = len(plans)
+
+    def bind(self, offsets, data):
+        """offsets / data: one int32 (n_rows + 1) and one uint8 tensor per plan."""
+        import numpy as np
+
+        offs = (_p * self.n)(*[o.data_ptr() for o in offsets])
+        byts = (_p * self.n)(*[d.data_ptr() for d in data])
+        caps = np.array([d.numel() for d in data], np.uint64)
+        check(_set_bind(self.handle, ctypes.cast(offs, _p), ctypes.cast(byts, _p), caps.ctypes.data_as(_p)),
+              "fls_string_set_bind")
+        self._bound = (offsets, data)
+
+    def decode(self, stream=None):
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        check(_set_decode(self.handle, s), "fls_string_set_decode")
+
+    def close(self):
+        if self.handle:
+            _set_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -206,6 +206,33 @@ def zipf_codes(n_rows=16 << 20, n_dict=4096, a=1.1, seed=0):
     return ((rng.zipf(a, n_rows) - 1) % n_dict).astype(np.uint32)
 
 
+def dict_rows_match(offsets, data, dict_bytes, dict_offsets, codes, chunk_rows=1 << 22):
+    """Whole-buffer parity of decoded DICT string rows: `offsets` (int32, n + 1) and `data` (uint8) on the device
+    against the rows the generator meant -- row r is dictionary entry codes[r] -- built on the device by a
+    gather over the dictionary, chunk by chunk, every byte compared.  dict_bytes / dict_offsets / codes: host
+    arrays."""
+    dev = data.device
+    db = torch.from_numpy(np.ascontiguousarray(dict_bytes, np.uint8)).to(dev)
+    do = torch.from_numpy(np.asarray(dict_offsets).astype(np.int64)).to(dev)
+    cd = torch.from_numpy(np.asarray(codes).astype(np.int64)).to(dev)
+    n = cd.numel()
+    lens = (do[1:] - do[:-1])[cd]
+    want = torch.zeros(n + 1, dtype=torch.int64, device=dev)
+    want[1:] = torch.cumsum(lens, 0)
+    if offsets.numel() != n + 1 or not torch.equal(offsets.to(torch.int64) & 0xFFFFFFFF, want):
+        return False
+    if data.numel() < int(want[-1]):
+        return False
+    for a in range(0, n, chunk_rows):
+        b = min(n, a + chunk_rows)
+        o0, o1 = int(want[a]), int(want[b])
+        rows = torch.repeat_interleave(torch.arange(a, b, device=dev), lens[a:b])
+        src = do[cd[rows]] + (torch.arange(o0, o1, device=dev) - want[rows])
+        if not torch.equal(data[o0:o1], db[src]):
+            return False
+    return True
+
+
 # ---- integer columns for expression selection ------------------------------------------------------------
 SELECTION_FAMILIES = ("for_u32", "for_i64", "delta_i64", "rle", "dict_i32", "dict_rle", "noise")
 

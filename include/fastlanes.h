@@ -76,7 +76,27 @@ bool encode_from_memory(void*       in_data,
 /* include/fastlanes.h:84-86: decode a page into vec_c * 1024 values (original order). */
 void decode_to_memory(uint8_t* in_encoded_data, void* out_data, enum data_t in_datatype);
 
-/* Status-returning forms of the two calls above (0 = ok, fls_status_code of fls_b200.h otherwise).
+/* include/fastlanes.h:88-108 (declared by the reference, defined nowhere there).  Random access to one vector
+ * of an INT64 page whose buffers are all per vector (expressions 0, 1, 11, RLE 6, patched FFOR / DELTA without
+ * rec buffers); other pages report no buffers / leave the output untouched.
+ * init_random_access: with the page's metadata (header, buffer offsets, entry points) loaded at
+ *   in_encoded_data, the buffers vector in_vector_id needs: *output_n_buffer pairs [offset, size] (bytes from
+ *   the page start) in output_buffer (room for 2 * 6 values).  The last vector's packed buffer is reported with
+ *   the largest size a vector can take (8192 bytes); a caller clips it to the page.
+ * random_access: decodes vector in_vector_id into out_deencoded_vector (1024 int64 values, original order)
+ *   from the loaded buffers output_buffers[i] (the ranges init_random_access gave). */
+void init_random_access(uint8_t* in_encoded_data, uint64_t in_vector_id, uint64_t* output_n_buffer,
+                        uint64_t* output_buffer);
+void random_access(uint8_t* in_encoded_data, uint64_t in_vector_id, uint64_t* output_n_buffer,
+                   uint64_t* output_pair_offset_and_size, uint8_t** output_buffers, uint8_t* out_deencoded_vector);
+
+/* Status-returning forms of the two random-access calls (0 = ok, fls_status_code of fls_b200.h otherwise). */
+int fls_random_access_ranges(const uint8_t* in_encoded_data, uint64_t in_vector_id, uint64_t* n_buffer,
+                             uint64_t* pairs);
+int fls_random_access_decode(const uint8_t* in_encoded_data, uint64_t in_vector_id, uint64_t n_buffer,
+                             const uint64_t* pairs, const uint8_t* const* buffers, int64_t* out);
+
+/* Status-returning forms of encode_from_memory / decode_to_memory (0 = ok, fls_status_code of fls_b200.h otherwise).
  * fls_decode_to_memory_checked also bounds the input by in_encoded_size and reports the vector count. */
 int fls_encode_from_memory_status(void* in_data, uint64_t in_n_input, uint64_t in_capacity, uint8_t* out_encoded_data,
                                   uint64_t* out_encoded_size, uint64_t* out_metadadata_size, enum data_t in_datatype,

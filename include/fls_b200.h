@@ -48,6 +48,15 @@ int fls_gpu_status(int reset);
 /* Number of kernels this library has launched since the last reset (for launch accounting in benchmarks). */
 uint64_t fls_gpu_launch_count(int reset);
 
+/* Failure injection for tests of the bounded waits (no counterpart in the reference): fls_gpu_unffor_u32 over
+ * n_vec vectors (d_in 16-byte aligned) in which vector stall_vector's staging copy has its byte count armed on
+ * the mbarrier but is never issued, so nothing is in flight and that wait runs out after spin_limit polls (> 0);
+ * the warp then raises FLS_DEV_TIMEOUT, waits for the copies it did issue and leaves; every other vector decodes.
+ * No GPU fault is involved and the context stays usable. */
+int fls_gpu_test_stalled_copy(const uint32_t* d_in, uint32_t* d_out, const uint8_t* d_bw, const uint32_t* d_base,
+                              const uint64_t* d_byte_off, uint64_t n_vec, uint64_t stall_vector, uint32_t spin_limit,
+                              fls_stream_t stream);
+
 /* ---------------------------------------------------------------------------------------------------------
  * Primitives, batched over n_vec vectors.
  *   d_bw[v]        bit width of vector v (0..W)
@@ -304,8 +313,8 @@ int fls_file_close(fls_file* file);
  * Arrow-style output: n_rows + 1 u32 offsets and the concatenated bytes, rows in original order
  * (include/fls/encoder/assert_eq.hpp:166-210, :257-400).  The page and dictionary buffers must outlive the plan.
  * Device memory a plan holds: 16 bytes per vector, the decoded dictionary (DICT kinds), a decoded code stream
- * of 4 bytes per row (DICT pages with patched codes) or every row's decoded length, 4 bytes per row (FSST and
- * FSST12 pages).
+ * of 4 bytes per row (DICT pages with patched codes) or every row's decoded length, 4 bytes per row (FSST12
+ * pages).
  * ------------------------------------------------------------------------------------------------------- */
 typedef struct fls_string_plan fls_string_plan;
 int fls_string_plan_create(const uint8_t* d_page, uint64_t page_size, const uint8_t* d_dict, uint64_t dict_size,
@@ -319,21 +328,44 @@ int fls_string_plan_decode(const fls_string_plan* plan, uint32_t* d_offsets, uin
                            fls_stream_t stream);
 int fls_string_plan_destroy(fls_string_plan* plan);
 
+/* ---------------------------------------------------------------------------------------------------------
+ * String sets: many DICT string columns (string pool DICT / DICT_RLE / DICT_FRQ pages, each with its own
+ * FSST-compressed dictionary whose entries are < 256 bytes) decoded by ONE kernel launch (after one memset of the
+ * set's scratch), the multi-column form of fls_string_plan_decode for a row group's string columns
+ * (the reference decodes them column by column: TColDecoder<str_pt>, src/encoder/col_encoder.cpp:198-217).
+ * create: from plans made by fls_string_plan_create (they must outlive the set; FLS_ERR_UNSUPPORTED for a plan of
+ *   another kind).  bind: each column's outputs (as fls_string_plan_decode's: n_rows + 1 u32 offsets, 16-byte
+ *   aligned bytes, capacity < 4 GiB); synchronous, once.  decode: asynchronous, no allocation, capturable in a
+ *   CUDA graph.  Device memory a set holds: 8 bytes per vector and per CTA-sized chunk of vectors.
+ * ------------------------------------------------------------------------------------------------------- */
+typedef struct fls_string_set fls_string_set;
+int fls_string_set_create(const fls_string_plan* const* plans, uint32_t n, fls_string_set** out_set);
+int fls_string_set_bind(fls_string_set* set, uint32_t* const* d_offsets, uint8_t* const* d_bytes,
+                        const uint64_t* bytes_caps);
+int fls_string_set_decode(const fls_string_set* set, fls_stream_t stream);
+int fls_string_set_destroy(fls_string_set* set);
+
 /* Allocation-free decode of an FSST (str expressions 13, 14) or BYTE_ARR (0) page.  No counterpart in the
  * reference.  Some callers cannot allocate device memory: an engine whose buffer manager owns all of HBM and
  * forbids plugins to call cudaMalloc, or a caller on a path where allocating is not allowed.  This call needs no
- * allocation: its scratch (per-vector byte totals and bases, the FSST table, a status word) is one fixed array
- * of 133,376 bytes compiled into the library, which every GPU that loads the library holds until the process
- * exits.  Limits and rules:
- *   - at most 8192 vectors (8,388,608 rows) per page; larger pages return FLS_ERR_TOO_LARGE before any work;
+ * allocation: its scratch (per-vector byte totals and bases, the FSST table) is one fixed array of
+ * FLS_NOALLOC_SCRATCH_BYTES compiled into the library, which every GPU that loads the library holds until the
+ * process exits, and it never touches the library's per-device state (which is allocated on first use).
+ * Limits and rules:
+ *   - at most FLS_NOALLOC_MAX_VECTORS vectors (8,388,608 rows) per page; larger pages return FLS_ERR_TOO_LARGE
+ *     before any work;
  *   - the first call on a device looks up the array's device address (cudaGetSymbolAddress); make that first
  *     call before any stream capture;
+ *   - every call reads the page header and the symbol table back to the host in `stream`'s order (after the
+ *     work queued on it before) and waits for those reads;
  *   - all calls share the array, so calls whose work overlaps on the GPU (other streams, other threads) race;
  *     serialise them;
- *   - device-detected errors are OR-ed into *d_status when it is given (the caller zeroes it), else into the
- *     array's own status word, which every call clears.
+ *   - d_status is required (FLS_ERR_ARG when null): device-detected errors (FLS_DEV_*) are OR-ed into it, and
+ *     the caller zeroes it before the call.
  * Inputs and outputs are as for fls_string_plan_decode: d_offsets n_rows + 1 u32, d_bytes 16-byte aligned with
  * room for the decoded bytes (bytes_cap < 4 GiB); d_dict holds the FSST table bytes for FSST pages. */
+#define FLS_NOALLOC_MAX_VECTORS 8192
+#define FLS_NOALLOC_SCRATCH_BYTES 133392
 int fls_gpu_decode_fsst_page_noalloc(const uint8_t* d_page, uint64_t page_size, const uint8_t* d_dict,
                                      uint64_t dict_size, uint32_t* d_offsets, uint8_t* d_bytes, uint64_t bytes_cap,
                                      int* d_status, fls_stream_t stream);

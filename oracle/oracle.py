@@ -13,6 +13,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 RESTATED_PATH = os.path.join(HERE, "libfls_oracle.so")
 REFERENCE_PATH = os.path.join(HERE, "_ref", "libfls_ref.so")
+# the same sources built with -march=x86-64-v4 (AVX-512), for hosts that have those extensions
+REFERENCE_V4_PATH = os.path.join(HERE, "_ref", "libfls_ref_v4.so")
 TYPES = {8: np.uint8, 16: np.uint16, 32: np.uint32, 64: np.uint64}
 
 
@@ -24,8 +26,18 @@ def _load(path):
     return ctypes.CDLL(path) if os.path.exists(path) else None
 
 
+def _has_avx512():
+    try:
+        with open("/proc/cpuinfo") as f:
+            flags = next((ln for ln in f if ln.startswith("flags")), "").split()
+    except OSError:
+        return False
+    return all(x in flags for x in ("avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"))
+
+
 restated = _load(RESTATED_PATH)
-reference = _load(REFERENCE_PATH)
+REFERENCE_MARCH = "x86-64-v4" if os.path.exists(REFERENCE_V4_PATH) and _has_avx512() else "x86-64-v3"
+reference = _load(REFERENCE_V4_PATH if REFERENCE_MARCH == "x86-64-v4" else REFERENCE_PATH)
 
 
 def lib():

@@ -191,3 +191,49 @@ extern "C" uint64_t emu_put_rows(const uint32_t* base, const uint32_t* start, co
 	for (const auto& h : heads) { win[h.first] |= h.second; }
 	return d - d0;
 }
+
+// One vector of an FSST (fsst = 1) or BYTE_ARR column through the code-parallel device decoder (stream_vector of
+// fls_strings.cuh) on an emulated warp: ends = the 1024 cumulative row end offsets (original order), comp / n
+// the vector's compressed bytes (at any alignment).  Both passes run: the lengths pass's total is returned in
+// *len_total; offsets (1025 values, output positions from vbase) and bytes are written as the materialising
+// pass writes them.  Returns the materialising pass's total, *bad whether the rows were refused.
+extern "C" uint64_t emu_stream_vector(int fsst, const uint64_t* sym, const uint8_t* len, const uint32_t* ends,
+                                      const uint8_t* comp, uint32_t n, uint64_t vbase, uint32_t* offsets, uint8_t* out,
+                                      uint64_t* len_total, int* bad_out) {
+	std::vector<uint32_t> rows(kVec + kVec / 32 + 32, 0);
+	for (uint32_t r = 0; r < kVec; ++r) { rows[r + r / 32] = ends[r]; }
+	std::vector<uint8_t> win_buf(2048 + 64, 0xA5);
+	uint8_t*             win = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(win_buf.data()) + 15) & ~uintptr_t(15));
+	uint64_t             tot[2] = {0, 0};
+	bool                 bad[2] = {false, false};
+	for (int pass = 0; pass < 2; ++pass) {
+		std::barrier<>           bar(32);
+		EmuWarp                  w {&bar, {}, {}};
+		std::vector<std::thread> th;
+		for (int t = 0; t < 32; ++t) {
+			th.emplace_back([&, t] {
+				g_emu_warp = &w;
+				g_emu_lane = t;
+				StreamOut o {offsets, out, vbase, win};
+				bool      b = false;
+				uint32_t  r;
+				if (pass == 0) {
+					r = fsst ? stream_vector<false, true, 2048>(rows.data(), comp, n, sym, len, t, o, &b)
+					         : stream_vector<false, false, 2048>(rows.data(), comp, n, sym, len, t, o, &b);
+				} else {
+					r = fsst ? stream_vector<true, true, 2048>(rows.data(), comp, n, sym, len, t, o, &b)
+					         : stream_vector<true, false, 2048>(rows.data(), comp, n, sym, len, t, o, &b);
+				}
+				if (t == 0) {
+					tot[pass] = r;
+					bad[pass] = b;
+				}
+			});
+		}
+		for (auto& x : th) { x.join(); }
+	}
+	offsets[kVec] = static_cast<uint32_t>(vbase + tot[1]);
+	*len_total    = tot[0];
+	*bad_out      = (bad[0] ? 1 : 0) | (bad[1] ? 2 : 0);
+	return tot[1];
+}

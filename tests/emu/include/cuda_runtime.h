@@ -65,6 +65,23 @@ T __shfl_up_sync(unsigned, T v, unsigned d) {
 	__syncwarp();
 	return r;
 }
+template <class T>
+T __shfl_down_sync(unsigned, T v, unsigned d) {
+	g_emu_warp->xch[g_emu_lane] = static_cast<uint64_t>(v);
+	__syncwarp();
+	const T r = g_emu_lane + static_cast<int>(d) < 32 ? static_cast<T>(g_emu_warp->xch[g_emu_lane + d]) : v;
+	__syncwarp();
+	return r;
+}
+inline unsigned __reduce_or_sync(unsigned, unsigned v) {
+	g_emu_warp->xch[g_emu_lane] = v;
+	__syncwarp();
+	unsigned r = 0;
+	for (int i = 0; i < 32; ++i) { r |= static_cast<unsigned>(g_emu_warp->xch[i]); }
+	__syncwarp();
+	return r;
+}
+inline int __popc(unsigned x) { return __builtin_popcount(x); }
 inline int __popcll(unsigned long long x) { return __builtin_popcountll(x); }
 inline int __ffsll(long long x) { return __builtin_ffsll(x); }
 inline bool __any_sync(unsigned, bool p) {

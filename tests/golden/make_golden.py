@@ -30,7 +30,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FLS_REFERENCE", "/root/reference")
 PRIM = os.path.join(REF, "primitives/fls_generated/fallback/scalar_aav_uf1")
 TYPES = {8: np.uint8, 16: np.uint16, 32: np.uint32, 64: np.uint64}
 

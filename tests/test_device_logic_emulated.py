@@ -266,3 +266,91 @@ def test_emulated_put_row_window_protocol(emu, d0):
     assert not got[(d0 // 4) * 4:d0].any()
     end = d0 + want.size
     assert not got[end:(end + 3) // 4 * 4].any()
+
+
+def _aligned(n, fill, align=16):
+    raw = np.full(n + align, fill, np.uint8)
+    off = (-raw.ctypes.data) % align
+    return raw[off:off + n]
+
+
+def _emu_stream(emu, fsst, sym, ln, ends, comp, shift, vbase):
+    """stream_vector (both passes) on an emulated warp: comp placed at byte `shift` of a 16-byte aligned buffer,
+    output at byte vbase of a sentinel-filled buffer.  Returns (lengths total, offsets, output buffer, bad)."""
+    buf = _aligned(comp.size + shift + 16, 0x5A)
+    buf[shift:shift + comp.size] = comp
+    ends = np.ascontiguousarray(ends, np.uint32)
+    cap = vbase + 8 * max(comp.size, 1) + 64
+    out = _aligned(cap, 0xEE)
+    offs = np.zeros(1025, np.uint32)
+    tot_len = ctypes.c_uint64()
+    bad = ctypes.c_int()
+    emu.emu_stream_vector.restype = ctypes.c_uint64
+    tot = emu.emu_stream_vector(int(fsst), P(sym), P(ln), P(ends), ctypes.c_void_p(buf.ctypes.data + shift),
+                                ctypes.c_uint32(comp.size), ctypes.c_uint64(vbase), P(offs), P(out),
+                                ctypes.byref(tot_len), ctypes.byref(bad))
+    return tot, tot_len.value, offs, out, bad.value
+
+
+def _check_stream(emu, fsst, sym, ln, rows, shift, vbase):
+    comp = np.concatenate(rows) if rows else np.zeros(0, np.uint8)
+    ends = np.cumsum([r.size for r in rows]).astype(np.uint32)
+    dec = [oracle.fsst_decode(sym, ln, r) if fsst else r for r in rows]
+    want = np.concatenate(dec)
+    want_off = vbase + np.concatenate([[0], np.cumsum([d.size for d in dec])])
+    tot, tot_len, offs, out, bad = _emu_stream(emu, fsst, sym, ln, ends, comp.astype(np.uint8), shift, vbase)
+    assert bad == 0
+    assert tot == tot_len == want.size
+    assert np.array_equal(offs, want_off.astype(np.uint32))
+    assert np.array_equal(out[vbase:vbase + want.size], want)
+    assert (out[:vbase] == 0xEE).all() and (out[vbase + want.size:] == 0xEE).all()
+
+
+@pytest.mark.parametrize("shift,vbase", [(0, 0), (1, 5), (2, 16), (3, 13)])
+def test_emulated_stream_decode_reference_vectors(emu, col_golden, shift, vbase):
+    """The code-parallel FSST column decoder (stream_vector, both passes) on every vector of the reference's FSST
+    page and on the same rows as a BYTE_ARR vector: offsets and bytes equal the oracle's row-by-row decode, at
+    any source alignment and output position, and nothing outside the vector's output range is written."""
+    from oracle import pages
+
+    page, dic = col_golden["str_13_page"], col_golden["str_13_dict"]
+    _, sym, ln = oracle.fsst_decode_table(dic[8:])
+    pg = pages.parse_page(page)
+    for v in range(pg.vec_c):
+        data = np.ascontiguousarray(pg.vector_slice(v, 0))
+        ends = oracle.untranspose_i(np.frombuffer(pg.vector_slice(v, 1, 4096).tobytes(), np.uint32).copy())
+        starts = np.concatenate([[0], ends[:-1]])
+        rows = [data[s:e] for s, e in zip(starts, ends)]
+        _check_stream(emu, True, sym, ln, rows, shift, vbase)
+        _check_stream(emu, False, sym, ln, rows, shift, vbase)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_emulated_stream_decode_escapes_and_ragged_rows(emu, col_golden, seed):
+    """Rows full of escapes (runs of 255, an escape as a row's last byte, a literal 255), empty rows, rows of
+    one byte and rows of hundreds, so that chunk boundaries fall inside escapes and rows: the stream decoder
+    equals the oracle's row decoder."""
+    dic = col_golden["str_13_dict"]
+    _, sym, ln = oracle.fsst_decode_table(dic[8:])
+    rng = np.random.default_rng(1000 + seed)
+    lens = rng.choice([0, 1, 2, 3, 4, 7, 12, 40, 300], 1024, p=[.2, .1, .1, .1, .1, .1, .1, .15, .05])
+    p255 = [0.0, 0.05, 0.3, 0.7][seed % 4]
+    rows = []
+    for n in lens:
+        r = rng.integers(0, 256, n, dtype=np.uint8)
+        r[rng.random(n) < p255] = 255
+        rows.append(r)
+    _check_stream(emu, True, sym, ln, rows, seed % 4, (7 * seed) % 17)
+    _check_stream(emu, False, sym, ln, rows, seed % 4, (7 * seed) % 17)
+
+
+def test_emulated_stream_decode_refuses_bad_rows(emu, col_golden):
+    """Row ends that decrease, or end past the vector's bytes: the vector is refused (every row empty, total 0)
+    by both passes."""
+    dic = col_golden["str_13_dict"]
+    _, sym, ln = oracle.fsst_decode_table(dic[8:])
+    comp = np.arange(200, dtype=np.uint8)
+    for ends in (np.r_[np.arange(1, 101), np.full(924, 50)], np.r_[np.arange(1, 1024), [201]]):
+        tot, tot_len, offs, out, bad = _emu_stream(emu, True, sym, ln, ends.astype(np.uint32), comp, 1, 3)
+        assert bad == 3 and tot == tot_len == 0
+        assert (offs == 3).all()

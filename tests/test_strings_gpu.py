@@ -195,3 +195,103 @@ def test_decode_after_measure_and_alone_agree(cuda, col_golden):
         assert np.array_equal(offs.cpu().numpy().astype(np.uint64), want_o)
         assert np.array_equal(data[:n].cpu().numpy(), want_b)
     plan.close()
+
+
+DICT_KIND_IDS = [2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 15, 16] + list(range(17, 28))
+
+
+@pytest.mark.parametrize("n_dict", [600, 20000, 70000])
+def test_single_pass_dict_decode_every_size_class(cuda, n_dict):
+    """The single-pass DICT decode (entries below 256 bytes: the packed row table exists): dictionary and row table
+    in shared memory (600 entries) or read from global memory (20000, 70000), 16-bit code rows below 65535
+    entries and 32-bit ones at 70000, empty and 1-3-byte entries, batches of long rows larger than the window."""
+    from fastlanes_b200 import strings
+    from fastlanes_b200 import workloads as W
+
+    rng = np.random.default_rng(n_dict + 1)
+    kind = rng.choice(4, n_dict, p=[0.1, 0.2, 0.5, 0.2])
+    lens = rng.integers(np.array([0, 1, 4, 41])[kind], np.array([0, 3, 40, 255])[kind] + 1)
+    doffs = np.zeros(n_dict + 1, np.uint64)
+    doffs[1:] = np.cumsum(lens)
+    dbytes = rng.integers(0, 256, int(doffs[-1]), dtype=np.uint8)
+    codes = rng.integers(0, n_dict, 41 * 1024).astype(np.uint32)
+    codes[7 * 1024:8 * 1024] = int(np.argmax(np.diff(doffs)))
+    page, dic = strings.encode_string_dict(dbytes, doffs, codes)
+    pb, pp = _dev(page, cuda, 3)
+    db, dp = _dev(dic, cuda, 0)
+    plan = strings.StringPlan(pp, page.size, dp, dic.size)
+    offs, data = plan.decode(cuda)
+    plan.close()
+    assert W.dict_rows_match(offs, data, dbytes, doffs, codes)
+
+
+def test_string_set_decodes_every_dict_page_in_one_launch(cuda, col_golden):
+    """Every DICT-kind page of the reference's string pool (DICT with plain / FFOR / DELTA / patched codes,
+    DICT_RLE, DICT_FRQ; each with its own dictionary) plus two columns of the DICT+FSST configuration's shape,
+    decoded by one string set: one kernel launch, every column equal to the reference decoder's rows, twice in
+    a row and as a CUDA graph replay."""
+    import torch
+
+    from fastlanes_b200 import _lib
+    from fastlanes_b200 import primitives as P
+    from fastlanes_b200 import strings
+    from fastlanes_b200 import workloads as W
+
+    keep, plans, wants = [], [], []
+    for eid in DICT_KIND_IDS:
+        page, dic = col_golden[f"str_{eid}_page"], col_golden[f"str_{eid}_dict"]
+        pb, pp = _dev(page, cuda, eid % 4)
+        db, dp = _dev(dic, cuda, 0)
+        keep += [pb, db]
+        plans.append(strings.StringPlan(pp, page.size, dp, dic.size))
+        wants.append(("ref", _expected(col_golden, eid)))
+    for seed in (11, 12):
+        dbytes, doffs = W.string_dictionary(seed=seed)
+        codes = W.zipf_codes(50 * 1024, seed=seed)
+        page, dic = strings.encode_string_dict(dbytes, doffs, codes)
+        pb, pp = _dev(page, cuda, 0)
+        db, dp = _dev(dic, cuda, 0)
+        keep += [pb, db]
+        plans.append(strings.StringPlan(pp, page.size, dp, dic.size))
+        wants.append(("gen", (dbytes, doffs, codes)))
+    sizes = [p.measure() for p in plans]
+    offs = [torch.full((p.n_rows + 1,), -1, dtype=torch.int32, device=cuda) for p in plans]
+    data = [torch.full((n + 16,), 0xEE, dtype=torch.uint8, device=cuda) for n in sizes]
+    sset = strings.StringSet(plans)
+    sset.bind(offs, data)
+
+    def check():
+        torch.cuda.synchronize()
+        for (kind, w), o, d, n in zip(wants, offs, data, sizes):
+            if kind == "ref":
+                assert np.array_equal(o.cpu().numpy().astype(np.uint64), w[0])
+                assert np.array_equal(d[:n].cpu().numpy(), w[1])
+            else:
+                assert W.dict_rows_match(o, d[:n], *w)
+            assert (d[n:] == 0xEE).all()
+
+    _lib.lib.fls_gpu_launch_count(1)
+    sset.decode()
+    assert _lib.lib.fls_gpu_launch_count(1) == 1
+    check()
+    for o in offs:
+        o.fill_(-1)
+    sset.decode()
+    check()
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            sset.decode()
+    torch.cuda.current_stream().wait_stream(s)
+    for _ in range(2):
+        for o in offs:
+            o.fill_(-1)
+        g.replay()
+        check()
+    del g
+    sset.close()
+    for p in plans:
+        p.close()
+    assert P.device_status() == 0
