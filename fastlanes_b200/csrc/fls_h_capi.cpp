@@ -224,8 +224,13 @@ int encode_t(const T* in, uint64_t n, uint64_t cap, uint8_t* out, uint64_t* out_
 }
 
 // The three streams of the host decode pipeline of the current device: copies in, decode, copies out.
+constexpr uint32_t kPipeEvents = 256;    // three per chunk: enough for a 65,535-vector page of 8-byte values
+constexpr uint32_t kPipeIds     = 65536; // the identity work queue of a page's vectors, uploaded once
 struct HostPipe {
 	cudaStream_t in = nullptr, dec = nullptr, out = nullptr;
+	cudaEvent_t  ev[kPipeEvents] {};
+	uint32_t*    ids = nullptr; // device: ids[v] = v
+	std::mutex   call;          // one host-page decode at a time per device (the events are shared)
 };
 HostPipe* host_pipe() {
 	static HostPipe   p[64];
@@ -238,6 +243,19 @@ HostPipe* host_pipe() {
 		if (cudaStreamCreateWithFlags(&h.in, cudaStreamNonBlocking) != cudaSuccess ||
 		    cudaStreamCreateWithFlags(&h.dec, cudaStreamNonBlocking) != cudaSuccess ||
 		    cudaStreamCreateWithFlags(&h.out, cudaStreamNonBlocking) != cudaSuccess) {
+			h.in = nullptr;
+			return nullptr;
+		}
+		for (auto& e : h.ev) {
+			if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+				h.in = nullptr;
+				return nullptr;
+			}
+		}
+		std::vector<uint32_t> ids(kPipeIds);
+		for (uint32_t v = 0; v < kPipeIds; ++v) { ids[v] = v; }
+		if (cudaMalloc(&h.ids, 4ull * kPipeIds) != cudaSuccess ||
+		    cudaMemcpy(h.ids, ids.data(), 4ull * kPipeIds, cudaMemcpyHostToDevice) != cudaSuccess) {
 			h.in = nullptr;
 			return nullptr;
 		}
@@ -280,11 +298,10 @@ int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_
 	if (pi.vec_c == 0) { return FLS_OK; }
 	HostPipe* hp = host_pipe();
 	if (!hp) { return FLS_ERR_CUDA; }
+	std::lock_guard<std::mutex> call_lock(hp->call);
 	const uint32_t shift = static_cast<uint32_t>((16 - pi.off[pi.layout->ib_packed] % 16) % 16);
-	DevBuf         d_page(hp->in), d_out(hp->in), d_queue(hp->in);
-	if (!d_page.alloc(page_size + 32) || !d_out.alloc(out_bytes) || !d_queue.alloc(4ull * pi.vec_c)) {
-		return FLS_ERR_CUDA;
-	}
+	DevBuf         d_page(hp->in), d_out(hp->in);
+	if (!d_page.alloc(page_size + 32) || !d_out.alloc(out_bytes)) { return FLS_ERR_CUDA; }
 	uint8_t* dp = d_page.as<uint8_t>() + shift;
 	// _REC variants: the rec-compressed value buffer goes over whole and is decoded first (on the copy stream,
 	// so every chunk's decode is ordered after it)
@@ -320,41 +337,38 @@ int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_
 	rc = build_page_column(pi, dp, w, nullptr, 0, FLS_ORIGINAL, d_out.as<uint8_t>(), &c, d_rec.as<uint8_t>(), rec_n,
 	                       d_rec2.as<uint8_t>(), rec2_n);
 	if (rc != FLS_OK) { return rc; }
-	// work items: vector ids (the single column is the plan's inline column)
-	std::vector<uint32_t> ids(pi.vec_c);
-	for (uint32_t v = 0; v < pi.vec_c; ++v) { ids[v] = v; }
 	auto ep = [&](uint32_t v, uint32_t b) -> uint64_t {
 		if (v == 0) { return 0; }
 		uint32_t x;
 		std::memcpy(&x, page + pi.ep_off + 4ull * ((v - 1) * pi.arr_c + b), 4);
 		return x;
 	};
-	const uint64_t chunk_vec = std::max<uint64_t>(1, (8ull << 20) / (1024 * sz));
-	const uint32_t n_chunks  = static_cast<uint32_t>((pi.vec_c + chunk_vec - 1) / chunk_vec);
-	std::vector<cudaEvent_t> ev(2 * n_chunks, nullptr);
-	for (auto& e : ev) {
-		if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) { return FLS_ERR_CUDA; }
+	// chunks of about 8 MB of output, the first of about 1 MB so that the copies out start early
+	const uint64_t         chunk_vec = std::max<uint64_t>(1, (8ull << 20) / (1024 * sz));
+	const uint64_t         first_vec = std::max<uint64_t>(1, (1ull << 20) / (1024 * sz));
+	std::vector<uint32_t>  bounds {0};
+	while (bounds.back() < pi.vec_c) {
+		const uint64_t step = bounds.size() == 1 ? first_vec : chunk_vec;
+		bounds.push_back(static_cast<uint32_t>(std::min<uint64_t>(pi.vec_c, bounds.back() + step)));
 	}
-	struct EvGuard {
-		std::vector<cudaEvent_t>& ev;
-		~EvGuard() {
-			for (auto e : ev) {
-				if (e) { cudaEventDestroy(e); }
-			}
-		}
-	} guard {ev};
+	const uint32_t n_chunks = static_cast<uint32_t>(bounds.size() - 1);
+	if (3ull * n_chunks > kPipeEvents) { return FLS_ERR_TOO_LARGE; }
+	cudaEvent_t* ev = hp->ev;
 	const Family fam = post_is_patch(pi.layout->post)    ? Family::NUM_PATCH
 	                   : !post_is_gather(pi.layout->post) ? Family::NUM
 	                   : c.e <= 4                         ? Family::GATHER_NARROW
 	                                                      : Family::GATHER;
-	// page header, buffer offsets and entry points first, with the queue
-	if (cudaMemcpyAsync(dp, page, pi.meta_sz, cudaMemcpyHostToDevice, hp->in) != cudaSuccess ||
-	    cudaMemcpyAsync(d_queue.p, ids.data(), 4ull * pi.vec_c, cudaMemcpyHostToDevice, hp->in) != cudaSuccess) {
-		return FLS_ERR_CUDA;
-	}
+	// page header, buffer offsets and entry points first
+	if (cudaMemcpyAsync(dp, page, pi.meta_sz, cudaMemcpyHostToDevice, hp->in) != cudaSuccess) { return FLS_ERR_CUDA; }
+	// the copies in run at most kLead chunks ahead of the copies out: the link's two directions share its
+	// bandwidth, and the larger outbound transfer should not wait behind inbound bytes needed only later
+	constexpr uint32_t kLead = 2;
 	for (uint32_t k = 0; k < n_chunks; ++k) {
-		const uint32_t v0 = static_cast<uint32_t>(k * chunk_vec);
-		const uint32_t v1 = static_cast<uint32_t>(std::min<uint64_t>(pi.vec_c, v0 + chunk_vec));
+		const uint32_t v0 = bounds[k];
+		const uint32_t v1 = bounds[k + 1];
+		if (k >= kLead && cudaStreamWaitEvent(hp->in, ev[2 * n_chunks + k - kLead], 0) != cudaSuccess) {
+			return FLS_ERR_CUDA;
+		}
 		for (uint32_t b = 0; b < pi.arr_c; ++b) {
 			if (static_cast<int>(b) == rec_b) { continue; } // already in place (and decoded)
 			const uint64_t lo = pi.off[b] + ep(v0, b);
@@ -369,7 +383,7 @@ int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_
 		}
 		DecodeArgs a {};
 		a.col0      = c;
-		a.queue     = d_queue.as<uint32_t>() + v0;
+		a.queue     = hp->ids + v0;
 		a.n_items   = v1 - v0;
 		a.col_shift = 16;
 		if (launch_decode(fam, a, hp->dec) != cudaSuccess) { return FLS_ERR_CUDA; }
@@ -379,7 +393,8 @@ int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_
 		}
 		const uint64_t o0 = static_cast<uint64_t>(v0) * 1024 * sz, ob = static_cast<uint64_t>(v1 - v0) * 1024 * sz;
 		if (cudaMemcpyAsync(static_cast<uint8_t*>(out) + o0, d_out.as<uint8_t>() + o0, ob, cudaMemcpyDeviceToHost,
-		                    hp->out) != cudaSuccess) {
+		                    hp->out) != cudaSuccess ||
+		    cudaEventRecord(ev[2 * n_chunks + k], hp->out) != cudaSuccess) {
 			return FLS_ERR_CUDA;
 		}
 	}

@@ -14,6 +14,7 @@
 #include "fls_b200.h"
 #include "fls_select.h"
 #include "fls_strings.cuh"
+#include "fls_strplan.h"
 
 #include <algorithm>
 #include <cmath>
@@ -29,8 +30,7 @@ namespace sel {
 constexpr int      K        = FLS_SEL_K;
 constexpr int      NF       = FLS_SEL_FEATURES;
 constexpr int      H        = FLS_SEL_HIDDEN;
-constexpr uint32_t kTable   = 1u << 17;   // hash slots per chunk (chunks hold at most 65,536 values)
-constexpr uint64_t kEmpty   = ~0ull;      // empty key; the value ~0 itself lives in slot kTable
+constexpr uint64_t kEmpty   = ~0ull;      // empty key of the hash tables; the value ~0 itself has a slot of its own
 constexpr uint32_t kNoPos   = 0xFFFFFFFFu;
 constexpr uint32_t kMaxVecPerChunk = 64;
 constexpr int      kWarps   = 8;
@@ -411,145 +411,441 @@ __global__ void __launch_bounds__(kWarps * 32) k_features(ItemArgs a, float* fea
 }
 
 // ---------------------------------------------------------------------------------------------------------
-// Dictionary of a chunk (wizard): open-addressing table per chunk of the group, first occurrence by
-// atomicMin, codes in first-occurrence order.
-//   A insert       every value claims or finds its slot; first[slot] = min position
-//   B count        per vector, values that are their slot's first occurrence
-//   S scan         (per chunk) first-occurrence counts -> vector bases, distinct count
-//   C assign       code[slot] = rank of the first occurrence; the slot joins the chunk's list of used slots
-//   D codes        per vector, FFOR bit width of its codes
-//   E reset        the listed slots return to empty
+// Dictionary of a chunk (wizard), one CTA per chunk, in shared memory: the chunk's distinct values, numbered in
+// first-occurrence order (src/cor/lyt/dic/dic_fac.cpp:19-40), give the dictionary size and every vector's code
+// bit width.  A 16 Ki-slot open-addressing table holds the keys of one hash partition at a time (1 partition; a
+// chunk with more than kCdCap distinct values in a partition is redone with kCdParts of them):
+//   sweep 1   per partition: insert its keys, first position by atomicMin; every key's first position sets a bit
+//             in the chunk's position bitmap (64 Ki bits);
+//   prefix    popcounts of the bitmap words, scanned: the code of a first position is its rank among them;
+//   sweep 2   per partition: insert its keys again, then every value's code = rank(first position); each warp
+//             keeps the code range of its vectors.
+// Exact for every chunk; no global atomics, no table in global memory.
 // ---------------------------------------------------------------------------------------------------------
-struct DictArgs {
-	ItemArgs  it;
-	uint32_t  group_chunk0; // chunk index of the group's first chunk
-	uint64_t* keys;         // [group][kTable + 1]
-	uint32_t* first;        // [group][kTable + 1]
-	uint32_t* code;         // [group][kTable + 1]
-	uint32_t* used;         // [group][kMaxVecPerChunk * 1024] slots in rank order
-	uint32_t* vec_cnt;      // per item
-	uint32_t* vec_base;     // per item
-	uint32_t* dict_n;       // per chunk (global chunk index)
-	uint32_t* bw_code;      // per item
-	int*      status;
+constexpr uint32_t kCdSlots = 1u << 14;
+constexpr uint32_t kCdCap   = 12288; // keys of one partition (a load of 3/4)
+constexpr uint32_t kCdParts = 8;     // partitions of a chunk that exceeds kCdCap (8 x 12288 > 65,536 values)
+constexpr int      kCdWarps = 16;
+constexpr uint32_t kCdWords = kMaxVecPerChunk * 1024 / 32;
+constexpr uint32_t kCdSmem  = kCdSlots * 8 + (kCdSlots + 1) * 4 + 2 * kCdWords * 4;
+static_assert(kCdSmem <= 227 * 1024, "chunk dictionary tables fit one CTA");
+static_assert(kMaxVecPerChunk <= 4 * kCdWarps, "at most 4 vectors of a chunk per warp");
+
+struct ChunkDictArgs {
+	const Col*      cols;
+	const Item*     items;       // the chunks' vectors, chunk by chunk
+	const uint32_t* chunk_items; // item range of every chunk (n_chunks + 1)
+	uint32_t        n_chunks;
+	uint32_t*       dict_n;  // per chunk: distinct values
+	uint32_t*       bw_code; // per item: FFOR bit width of its codes
+	int*            status;
+	// string columns (optional): per-row weights of every column (row = vector * 1024 + position), summed over
+	// the first occurrences of a chunk's distinct values into dict_w[chunk][0..1] (the dictionary's raw and
+	// FSST-compressed bytes)
+	const uint32_t* const* w0;
+	const uint32_t* const* w1;
+	uint64_t*       dict_w;
 };
 
-__device__ __forceinline__ uint32_t dict_slot(uint64_t* keys, uint64_t x, bool insert, int* status) {
-	if (x == kEmpty) { return kTable; }
-	uint32_t h = hash_slot(x, 17);
-	for (uint32_t probe = 0; probe < kTable; ++probe) {
-		const uint64_t k = *reinterpret_cast<volatile uint64_t*>(keys + h);
-		if (k == x) { return h; }
+// 64-bit finaliser of MurmurHash3 (Appleby): slot from the low bits, partition from the high ones.
+__device__ __forceinline__ uint64_t cd_mix(uint64_t x) {
+	x ^= x >> 33;
+	x *= 0xff51afd7ed558ccdull;
+	x ^= x >> 33;
+	x *= 0xc4ceb9fe1a85ec53ull;
+	x ^= x >> 33;
+	return x;
+}
+__device__ __forceinline__ uint32_t cd_part(uint64_t h, uint32_t parts) { return static_cast<uint32_t>(h >> 48) & (parts - 1); }
+
+// Slot of x (inserted when absent; *count counts new keys): kCdSlots for the key ~0 (its own slot), kCdSlots + 1
+// when the table is full.
+__device__ __forceinline__ uint32_t cd_insert(uint64_t* keys, uint64_t x, uint64_t h, uint32_t* count) {
+	if (x == kEmpty) { return kCdSlots; }
+	uint32_t s = static_cast<uint32_t>(h) & (kCdSlots - 1);
+	for (uint32_t probe = 0; probe < kCdSlots; ++probe) {
+		const uint64_t k = *reinterpret_cast<volatile uint64_t*>(keys + s);
+		if (k == x) { return s; }
 		if (k == kEmpty) {
-			if (!insert) { break; }
-			const uint64_t old = atomicCAS(reinterpret_cast<unsigned long long*>(keys + h), kEmpty, x);
-			if (old == kEmpty || old == x) { return h; }
+			const uint64_t old = atomicCAS(reinterpret_cast<unsigned long long*>(keys + s), kEmpty, x);
+			if (old == kEmpty) {
+				atomicAdd(count, 1u);
+				return s;
+			}
+			if (old == x) { return s; }
 		}
-		h = (h + 1) & (kTable - 1);
+		s = (s + 1) & (kCdSlots - 1);
 	}
-	atomicOr(status, STATUS_BAD_INDEX);
-	return kTable;
+	return kCdSlots + 1;
 }
 
-template <int PASS, int W>
-__device__ __forceinline__ void dict_pass_vector(const DictArgs& a, uint64_t it, const Item& m, const Col& c,
-                                                 uint32_t lane) {
-	using T = typename UT<W>::T;
-	T x[32];
-	load_run<W>(c, m.vec, lane, x);
-	const uint64_t g     = m.chunk - a.group_chunk0;
-	uint64_t*      keys  = a.keys + g * (kTable + 1);
-	uint32_t*      first = a.first + g * (kTable + 1);
-	uint32_t*      code  = a.code + g * (kTable + 1);
-	const uint32_t pos0  = m.cpos * 1024 + thread_run(lane);
-	if constexpr (PASS == 0) {
-#pragma unroll
-		for (int i = 0; i < 32; ++i) {
-			const uint32_t s = dict_slot(keys, x[i], true, a.status);
-			atomicMin(first + s, pos0 + i);
+__device__ __forceinline__ uint32_t cd_find(const uint64_t* keys, uint64_t x, uint64_t h) {
+	if (x == kEmpty) { return kCdSlots; }
+	uint32_t s = static_cast<uint32_t>(h) & (kCdSlots - 1);
+	for (uint32_t probe = 0; probe < kCdSlots; ++probe) {
+		const uint64_t k = keys[s];
+		if (k == x) { return s; }
+		if (k == kEmpty) { break; }
+		s = (s + 1) & (kCdSlots - 1);
+	}
+	return kCdSlots + 1;
+}
+
+template <int W>
+__device__ __forceinline__ void chunk_dict(const ChunkDictArgs& a, const Col& col, uint32_t c, uint64_t* keys,
+                                           uint32_t* first, uint32_t* bits, uint32_t* pref, uint32_t* s_count,
+                                           uint32_t* s_over, uint32_t* s_wsum, uint64_t* s_dw) {
+	using T             = typename UT<W>::T;
+	const uint32_t tid  = threadIdx.x, nt = blockDim.x, lane = tid & 31u, warp = tid >> 5, nw = nt >> 5;
+	const uint32_t i0   = a.chunk_items[c], i1 = a.chunk_items[c + 1];
+	const Item     m0   = a.items[i0];
+	const uint32_t v0   = m0.vec - m0.cpos; // the chunk's first vector
+	if (tid == 0) { s_dw[0] = s_dw[1] = 0; }
+	// insert the keys of partition p of the chunk (first positions by atomicMin); false on overflow
+	auto insert_part = [&](uint32_t p, uint32_t parts) {
+		if (tid == 0) {
+			*s_count = 0;
+			*s_over  = 0;
 		}
-	} else if constexpr (PASS == 1 || PASS == 2) {
-		uint32_t fm = 0, sl[32];
-#pragma unroll
-		for (int i = 0; i < 32; ++i) {
-			sl[i] = dict_slot(keys, x[i], false, a.status);
-			fm |= (first[sl[i]] == pos0 + i ? 1u : 0u) << i;
-		}
-		const uint32_t cnt = __popc(fm);
-		if constexpr (PASS == 1) {
-			const uint32_t tot = warp_sum(cnt);
-			if (lane == 0) { a.vec_cnt[it] = tot; }
-		} else {
-			const uint32_t base = a.vec_base[it] + run_exclusive(cnt, lane);
-			uint32_t*      used = a.used + g * (kMaxVecPerChunk * 1024);
+		__syncthreads();
+		for (uint32_t j = i0 + warp; j < i1; j += nw) {
+			if (*reinterpret_cast<volatile uint32_t*>(s_count) > kCdCap) { break; } // redone with more partitions
+			const Item m = a.items[j];
+			T          x[32];
+			load_run<W>(col, m.vec, lane, x);
+			const uint32_t pos0 = m.cpos * 1024 + thread_run(lane);
 #pragma unroll
 			for (int i = 0; i < 32; ++i) {
-				if ((fm >> i) & 1u) {
-					const uint32_t r = base + __popc(fm & ((1u << i) - 1u));
-					code[sl[i]]      = r;
-					used[r]          = sl[i];
+				const uint64_t h = cd_mix(static_cast<uint64_t>(x[i]));
+				if (cd_part(h, parts) != p && static_cast<uint64_t>(x[i]) != kEmpty) { continue; }
+				if (static_cast<uint64_t>(x[i]) == kEmpty && p != 0) { continue; } // the key ~0 belongs to partition 0
+				const uint32_t s = cd_insert(keys, x[i], h, s_count);
+				if (s > kCdSlots) {
+					*s_over = 1;
+				} else if (pos0 + i < first[s]) {
+					atomicMin(first + s, pos0 + i);
 				}
 			}
 		}
-	} else {
-		uint32_t mn = 0xFFFFFFFFu, mx = 0;
+		__syncthreads();
+		return *s_over == 0 && *s_count <= kCdCap;
+	};
+	auto clear_table = [&]() {
+		for (uint32_t k = tid; k < kCdSlots; k += nt) { keys[k] = kEmpty; }
+		for (uint32_t k = tid; k <= kCdSlots; k += nt) { first[k] = kNoPos; }
+		__syncthreads();
+	};
+	for (uint32_t k = tid; k < kCdWords; k += nt) { bits[k] = 0; }
+	clear_table();
+	// sweep 1: every partition's first positions into the bitmap
+	uint32_t parts = 1;
+	for (;;) {
+		bool ok = true;
+		for (uint32_t p = 0; p < parts && ok; ++p) {
+			ok = insert_part(p, parts);
+			if (ok) {
+				uint64_t sw0 = 0, sw1 = 0;
+				for (uint32_t k = tid; k <= kCdSlots; k += nt) {
+					const uint32_t f = first[k];
+					if (f != kNoPos) {
+						atomicOr(bits + (f >> 5), 1u << (f & 31u));
+						if (a.w0) {
+							const uint64_t row = static_cast<uint64_t>(v0) * 1024 + f;
+							sw0 += a.w0[m0.col][row];
+							sw1 += a.w1[m0.col][row];
+						}
+					}
+				}
+				if (a.w0) {
+					sw0 = warp_sum(sw0);
+					sw1 = warp_sum(sw1);
+					if (lane == 0) {
+						atomicAdd(reinterpret_cast<unsigned long long*>(s_dw), static_cast<unsigned long long>(sw0));
+						atomicAdd(reinterpret_cast<unsigned long long*>(s_dw + 1), static_cast<unsigned long long>(sw1));
+					}
+				}
+				__syncthreads();
+			}
+			clear_table();
+		}
+		if (ok) { break; }
+		if (parts == kCdParts) {
+			if (tid == 0) { atomicOr(a.status, STATUS_BAD_INDEX); } // cannot happen for 65,536 values
+			break;
+		}
+		parts = kCdParts;
+		for (uint32_t k = tid; k < kCdWords; k += nt) { bits[k] = 0; }
+		if (tid == 0) { s_dw[0] = s_dw[1] = 0; }
+		__syncthreads();
+	}
+	// ranks: exclusive prefix of the bitmap words' popcounts (thread t: words [t * per, (t + 1) * per))
+	const uint32_t per = kCdWords / nt;
+	uint32_t       loc = 0;
+	for (uint32_t k = 0; k < per; ++k) { loc += __popc(bits[tid * per + k]); }
+	const uint32_t inc = warp_inclusive_scan(loc, lane);
+	if (lane == 31) { s_wsum[warp] = inc; }
+	__syncthreads();
+	if (warp == 0) {
+		const uint32_t w  = lane < nw ? s_wsum[lane] : 0u;
+		const uint32_t wi = warp_inclusive_scan(w, lane);
+		s_wsum[lane]      = wi - w;
+		if (lane == 31) { s_wsum[32] = wi; }
+	}
+	__syncthreads();
+	uint32_t run = s_wsum[warp] + inc - loc;
+	for (uint32_t k = 0; k < per; ++k) {
+		pref[tid * per + k] = run;
+		run += __popc(bits[tid * per + k]);
+	}
+	const uint32_t total = s_wsum[32];
+	__syncthreads();
+	// sweep 2: codes of every value, the code range of each of the warp's vectors
+	uint32_t mn[4] = {~0u, ~0u, ~0u, ~0u}, mx[4] = {0u, 0u, 0u, 0u};
+	for (uint32_t p = 0; p < parts; ++p) {
+		insert_part(p, parts);
 #pragma unroll
-		for (int i = 0; i < 32; ++i) {
-			const uint32_t r = code[dict_slot(keys, x[i], false, a.status)];
-			mn               = min(mn, r);
-			mx               = max(mx, r);
+		for (uint32_t q = 0; q < 4; ++q) {
+			const uint32_t j = i0 + warp + q * nw;
+			if (j >= i1) { continue; }
+			const Item m = a.items[j];
+			T          x[32];
+			load_run<W>(col, m.vec, lane, x);
+#pragma unroll
+			for (int i = 0; i < 32; ++i) {
+				const uint64_t h = cd_mix(static_cast<uint64_t>(x[i]));
+				if (static_cast<uint64_t>(x[i]) == kEmpty ? p != 0 : cd_part(h, parts) != p) { continue; }
+				const uint32_t s = cd_find(keys, x[i], h);
+				if (s > kCdSlots) { continue; }
+				const uint32_t f    = first[s];
+				const uint32_t code = pref[f >> 5] + __popc(bits[f >> 5] & ((1u << (f & 31u)) - 1u));
+				mn[q]               = min(mn[q], code);
+				mx[q]               = max(mx[q], code);
+			}
 		}
-		mn = warp_min(mn);
-		mx = warp_max(mx);
-		if (lane == 0) { a.bw_code[it] = bits_of(mx - mn); }
+		__syncthreads();
+		clear_table();
 	}
+#pragma unroll
+	for (uint32_t q = 0; q < 4; ++q) {
+		const uint32_t j  = i0 + warp + q * nw;
+		const uint32_t lo = warp_min(mn[q]), hi = warp_max(mx[q]);
+		if (j < i1 && lane == 0) { a.bw_code[j] = hi >= lo ? bits_of(hi - lo) : 0u; }
+	}
+	if (tid == 0) {
+		a.dict_n[c] = total;
+		if (a.dict_w) {
+			a.dict_w[2ull * c]     = s_dw[0];
+			a.dict_w[2ull * c + 1] = s_dw[1];
+		}
+	}
+	__syncthreads();
 }
 
-template <int PASS>
-__global__ void __launch_bounds__(kWarps * 32) k_dict(DictArgs a) {
-	const uint32_t lane = threadIdx.x & 31u;
-	for (uint64_t it = blockIdx.x * static_cast<uint64_t>(kWarps) + (threadIdx.x >> 5); it < a.it.n_items;
-	     it += static_cast<uint64_t>(gridDim.x) * kWarps) {
-		const Item m = a.it.items[it];
-		const Col  c = a.it.cols[m.col];
-		if (c.width == 64) {
-			dict_pass_vector<PASS, 64>(a, it, m, c, lane);
+__global__ void __launch_bounds__(kCdWarps * 32) k_chunk_dict(ChunkDictArgs a) {
+	extern __shared__ __align__(16) uint8_t smem[];
+	__shared__ uint32_t s_count, s_over, s_wsum[33];
+	__shared__ uint64_t s_dw[2];
+	uint64_t*           keys  = reinterpret_cast<uint64_t*>(smem);
+	uint32_t*           first = reinterpret_cast<uint32_t*>(keys + kCdSlots);
+	uint32_t*           bits  = first + kCdSlots + 1;
+	uint32_t*           pref  = bits + kCdWords;
+	for (uint32_t c = blockIdx.x; c < a.n_chunks; c += gridDim.x) {
+		const Col col = a.cols[a.items[a.chunk_items[c]].col];
+		if (col.width == 64) {
+			chunk_dict<64>(a, col, c, keys, first, bits, pref, &s_count, &s_over, s_wsum, s_dw);
 		} else {
-			dict_pass_vector<PASS, 32>(a, it, m, c, lane);
+			chunk_dict<32>(a, col, c, keys, first, bits, pref, &s_count, &s_over, s_wsum, s_dw);
 		}
 	}
 }
 
-// Chunk-level steps: chunk_items[c] .. chunk_items[c + 1] are chunk (group_chunk0 + c)'s items.
-__global__ void k_dict_scan(DictArgs a, const uint32_t* chunk_items, uint32_t n_chunks) {
+// ---------------------------------------------------------------------------------------------------------
+// String columns.  The selection works on a 64-bit hash of every row (distinct rows, runs and first-occurrence
+// codes come from the integer machinery run on the hashes), the row's length and its FSST-compressed length
+// under the column's symbol table (the encoder's greedy longest match; a byte no symbol starts with costs an
+// escape and itself, 2 bytes).  Candidates (string pool, no patches; src/cor/exp_pool.cpp:66-101):
+//   0 BYTE_ARR (pool id 0)   1 DICT FFOR over an FSST dictionary (id 3)   2 FSST (id 13)
+//   3 DICT_RLE with raw run codes and a raw u16 run index (id 15)
+// ---------------------------------------------------------------------------------------------------------
+constexpr int kStrK = FLS_SEL_STR_K;
+
+// An FSST symbol table arranged for greedy matching: symbols grouped by their first byte, longest first.
+struct StrTab {
+	uint64_t val[256];
+	uint8_t  len[256];
+	uint16_t start[257]; // symbols starting with byte b: [start[b], start[b + 1])
+};
+
+struct StrCol {
+	const uint8_t*  bytes;
+	const uint64_t* offsets; // n_rows + 1
+	uint64_t        n_bytes; // offsets[n_rows]
+	const StrTab*   tab;
+	uint32_t        tab_bytes; // the exported table's size (the FSST page's dictionary slot)
+	uint64_t*       hash;      // per row
+	uint32_t*       len;
+	uint32_t*       clen;
+};
+
+__device__ __forceinline__ uint64_t str_mix(uint64_t h) {
+	h ^= h >> 33;
+	h *= 0xff51afd7ed558ccdull;
+	h ^= h >> 33;
+	h *= 0xc4ceb9fe1a85ec53ull;
+	h ^= h >> 33;
+	return h;
+}
+
+// 8 bytes of a string from byte position p (bytes past the column's last byte read as the last word's)
+__device__ __forceinline__ uint64_t str_load8(const StrCol& c, uint64_t p) {
+	const uint32_t* w    = reinterpret_cast<const uint32_t*>(reinterpret_cast<uintptr_t>(c.bytes) & ~uintptr_t(3));
+	const uint64_t  a    = (reinterpret_cast<uintptr_t>(c.bytes) & 3u) + p; // byte index from w
+	const uint64_t  last = ((reinterpret_cast<uintptr_t>(c.bytes) & 3u) + (c.n_bytes ? c.n_bytes - 1 : 0)) >> 2;
+	const uint64_t  q    = a >> 2;
+	const uint32_t  x0 = __ldg(w + (q < last ? q : last)), x1 = __ldg(w + (q + 1 < last ? q + 1 : last)),
+	               x2  = __ldg(w + (q + 2 < last ? q + 2 : last));
+	const uint32_t  sh = 8u * static_cast<uint32_t>(a & 3u);
+	const uint32_t  lo = sh ? __funnelshift_r(x0, x1, sh) : x0, hi = sh ? __funnelshift_r(x1, x2, sh) : x1;
+	return (static_cast<uint64_t>(hi) << 32) | lo;
+}
+
+// warp per item: hash, length and compressed length of the vector's 1024 rows; the vector's sums
+__global__ void __launch_bounds__(kWarps * 32) k_str_rows(const StrCol* cols, const Item* items, uint64_t n_items,
+                                                          uint64_t* vlen, uint64_t* vclen) {
 	const uint32_t lane = threadIdx.x & 31u;
-	for (uint32_t c = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); c < n_chunks; c += gridDim.x * (blockDim.x / 32)) {
-		const uint32_t i0 = chunk_items[c], i1 = chunk_items[c + 1];
-		uint32_t       carry = 0;
-		for (uint32_t b = i0; b < i1; b += 32) {
-			const uint32_t i   = b + lane;
-			const uint32_t x   = i < i1 ? a.vec_cnt[i] : 0u;
-			const uint32_t inc = warp_inclusive_scan(x, lane);
-			if (i < i1) { a.vec_base[i] = carry + inc - x; }
-			carry += __shfl_sync(0xFFFFFFFFu, inc, 31);
+	for (uint64_t it = blockIdx.x * static_cast<uint64_t>(kWarps) + (threadIdx.x >> 5); it < n_items;
+	     it += static_cast<uint64_t>(gridDim.x) * kWarps) {
+		const Item   m = items[it];
+		const StrCol c = cols[m.col];
+		uint64_t     sl = 0, sc = 0;
+		for (uint32_t i = 0; i < 32; ++i) {
+			const uint64_t r = static_cast<uint64_t>(m.vec) * 1024 + lane + 32 * i;
+			const uint64_t s = c.offsets[r], e = c.offsets[r + 1];
+			const uint64_t n = e >= s ? e - s : 0;
+			uint64_t       h = 0x243F6A8885A308D3ull ^ n;
+			for (uint64_t p = 0; p < n; p += 8) {
+				const uint64_t x = str_load8(c, s + p);
+				const uint64_t k = n - p >= 8 ? x : (x & ((1ull << (8 * (n - p))) - 1));
+				h                = str_mix(h ^ k) + 0x9E3779B97F4A7C15ull;
+			}
+			uint64_t cl = 0;
+			for (uint64_t p = 0; p < n;) {
+				const uint64_t x    = str_load8(c, s + p);
+				const uint32_t b    = static_cast<uint32_t>(x & 0xFFu);
+				const uint64_t left = n - p;
+				uint32_t       step = 0;
+				for (uint32_t k = c.tab->start[b]; k < c.tab->start[b + 1]; ++k) {
+					const uint32_t l = c.tab->len[k];
+					if (l <= left && (l == 8 ? x : (x & ((1ull << (8 * l)) - 1))) == c.tab->val[k]) {
+						step = l;
+						break;
+					}
+				}
+				cl += step ? 1 : 2;
+				p += step ? step : 1;
+			}
+			c.hash[r] = h;
+			c.len[r]  = static_cast<uint32_t>(n);
+			c.clen[r] = static_cast<uint32_t>(cl);
+			sl += n;
+			sc += cl;
 		}
-		if (lane == 0) { a.dict_n[a.group_chunk0 + c] = carry; }
+		sl = warp_sum(sl);
+		sc = warp_sum(sc);
+		if (lane == 0) {
+			if (vlen) { vlen[it] = sl; }
+			if (vclen) { vclen[it] = sc; }
+		}
 	}
 }
 
-__global__ void k_dict_reset(DictArgs a, const uint32_t* chunk_items, uint32_t n_chunks) {
-	for (uint32_t c = blockIdx.x; c < n_chunks; c += gridDim.x) {
-		const uint32_t gc    = a.group_chunk0 + c;
-		const uint32_t n     = a.dict_n[gc];
-		uint64_t*      keys  = a.keys + static_cast<uint64_t>(c) * (kTable + 1);
-		uint32_t*      first = a.first + static_cast<uint64_t>(c) * (kTable + 1);
-		const uint32_t* used = a.used + static_cast<uint64_t>(c) * (kMaxVecPerChunk * 1024);
-		for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-			const uint32_t s = used[i];
-			if (s < kTable) { keys[s] = kEmpty; }
-			first[s] = kNoPos;
+// The features of a string vector: those of its row hashes (distinct rows, runs, multiplicities), with the
+// slots that mean nothing for hashes replaced by the rows' lengths and compressibility.
+__global__ void __launch_bounds__(kWarps * 32) k_str_features(const StrCol* cols, const Item* items, uint64_t n_items,
+                                                              float* feat) {
+	const uint32_t lane = threadIdx.x & 31u;
+	for (uint64_t it = blockIdx.x * static_cast<uint64_t>(kWarps) + (threadIdx.x >> 5); it < n_items;
+	     it += static_cast<uint64_t>(gridDim.x) * kWarps) {
+		const Item   m  = items[it];
+		const StrCol c  = cols[m.col];
+		float        sl = 0, sc = 0, sq = 0, mx = 0, mn = 1e30f;
+		for (uint32_t i = 0; i < 32; ++i) {
+			const uint64_t r = static_cast<uint64_t>(m.vec) * 1024 + lane + 32 * i;
+			const float    l = static_cast<float>(c.len[r]);
+			sl += l;
+			sq += l * l;
+			sc += static_cast<float>(c.clen[r]);
+			mx = fmaxf(mx, l);
+			mn = fminf(mn, l);
 		}
-		(void)chunk_items;
+		sl = warp_sum(sl);
+		sq = warp_sum(sq);
+		sc = warp_sum(sc);
+		mx = warp_max(mx);
+		mn = warp_min(mn);
+		const float mean = sl / 1024.0f;
+		const float var  = fmaxf(sq / 1024.0f - mean * mean, 0.0f);
+		float*      f    = feat + it * NF;
+		if (lane == 0) {
+			f[0]  = mean / 64.0f;
+			f[1]  = sl > 0 ? sc / sl : 1.0f;
+			f[9]  = sqrtf(var) / 64.0f;
+			f[14] = mx / 256.0f;
+			f[15] = mn / 64.0f;
+			f[16] = 1.0f; // a string column
+			f[22] = log2f(mean + 1.0f) / 8.0f;
+			f[29] = sc / (1024.0f * 64.0f);
+		}
+	}
+}
+
+struct StrSizeArgs {
+	const uint32_t* chunk_col;
+	const uint32_t* chunk_items; // item range of every chunk (n_chunks + 1)
+	const uint32_t* parts;       // per item: runs of the row hashes in bits 19..
+	const uint32_t* bw_code;     // per item
+	const uint64_t* vlen;        // per item
+	const uint64_t* vclen;       // per item
+	const uint32_t* dict_n;      // per chunk
+	const uint64_t* dict_w;      // per chunk: the dictionary's raw and compressed bytes
+	const StrCol*   cols;
+	uint32_t        n_chunks;
+	uint64_t*       sizes; // n_chunks x FLS_SEL_K (the string candidates in 0..3, the rest ~0)
+	uint8_t*        best;
+};
+
+// Exact page bytes of the string candidates (page = header, buffer offsets, per-vector entry points, buffers;
+// the dictionary page of DICT and DICT_RLE = dict_hdr_t, the FSST_MAXHEADER table slot, u32 compressed lengths
+// and the compressed entries, src/cor/lyt/dic/dic.cpp:88-111; the FSST column's = dict_hdr_t and the table).
+__global__ void k_str_sizes(StrSizeArgs a) {
+	const uint32_t lane = threadIdx.x & 31u;
+	for (uint32_t c = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); c < a.n_chunks; c += gridDim.x * (blockDim.x / 32)) {
+		const uint32_t i0 = a.chunk_items[c], i1 = a.chunk_items[c + 1];
+		uint64_t       L = 0, C = 0, R = 0, B = 0;
+		for (uint32_t i = i0 + lane; i < i1; i += 32) {
+			L += a.vlen[i];
+			C += a.vclen[i];
+			R += a.parts[i] >> 19;
+			B += a.bw_code[i];
+		}
+		L = warp_sum(L), C = warp_sum(C), R = warp_sum(R), B = warp_sum(B);
+		if (lane == 0) {
+			const uint64_t nv    = i1 - i0;
+			auto           frame = [&](uint64_t arr) { return 8 + 4 * arr + 4 * arr * (nv ? nv - 1 : 0); };
+			const uint64_t dpage = 8 + 2066 + 4ull * a.dict_n[c] + a.dict_w[2ull * c + 1];
+			uint64_t       z[FLS_SEL_K];
+			z[0] = frame(2) + L + 4096 * nv;
+			z[1] = frame(3) + nv + 4 * nv + 128 * B + dpage;
+			z[2] = frame(2) + C + 4096 * nv + 8 + a.cols[a.chunk_col[c]].tab_bytes;
+			z[3] = frame(2) + 4 * R + 2048 * nv + dpage;
+			for (int k = kStrK; k < FLS_SEL_K; ++k) { z[k] = ~0ull; }
+			uint32_t b = 0;
+			for (int k = 0; k < FLS_SEL_K; ++k) {
+				a.sizes[static_cast<uint64_t>(c) * FLS_SEL_K + k] = z[k];
+				if (z[k] < z[b]) { b = k; }
+			}
+			a.best[c] = static_cast<uint8_t>(b);
+		}
 	}
 }
 
@@ -602,7 +898,8 @@ __global__ void k_chunk_sizes(SizeArgs a) {
 
 // Per-chunk vote of the learned selector over its sampled rows: mean log-probability, argmax, mean top
 // probability as the confidence.
-__global__ void k_vote(const float* prob, const uint32_t* chunk_rows, uint32_t n_chunks, uint8_t* choice, float* conf) {
+__global__ void k_vote(const float* prob, const uint32_t* chunk_rows, uint32_t n_chunks, uint8_t* choice, float* conf,
+                       int k_use) {
 	const uint32_t lane = threadIdx.x & 31u;
 	for (uint32_t c = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); c < n_chunks; c += gridDim.x * (blockDim.x / 32)) {
 		const uint32_t r0 = chunk_rows[c], r1 = chunk_rows[c + 1];
@@ -620,7 +917,7 @@ __global__ void k_vote(const float* prob, const uint32_t* chunk_rows, uint32_t n
 		for (int k = 0; k < K; ++k) {
 			lp[k] = warp_sum(lp[k]);
 			pp[k] = warp_sum(pp[k]);
-			if (lp[k] > lp[b]) { b = k; }
+			if (k < k_use && lp[k] > lp[b]) { b = k; }
 		}
 		if (lane == 0) {
 			choice[c] = static_cast<uint8_t>(b);
@@ -918,8 +1215,11 @@ struct fls_sel_plan {
 	uint64_t              n_chunks = 0;
 	uint32_t              chunk_vectors = 64;
 	// wizard scratch
-	uint32_t group = 0;
-	DevMem   keys, first, code, used, vec_cnt, vec_base, bw_code, parts, dict_n;
+	DevMem   bw_code, parts, dict_n;
+	// string columns (fls_sel_plan_create_strings): the plan's columns are the row hashes; these are the strings
+	bool                str = false;
+	std::vector<StrCol> scols;
+	DevMem              scols_d, tabs_d, hash_d, len_d, clen_d, wptr_d;
 	std::map<uint32_t, ItemSet> samples; // stride -> sampled items
 };
 
@@ -990,43 +1290,44 @@ int wizard_run(fls_sel_plan* p, const std::vector<uint32_t>& subset, uint64_t* d
 	if ((rc = upload(items_d, it.data(), it.size() * sizeof(Item))) != FLS_OK) { return rc; }
 	if ((rc = upload(ranges_d, ranges.data(), ranges.size() * 4)) != FLS_OK) { return rc; }
 	if ((rc = upload(ccol_d, ccol.data(), ccol.size() * 4)) != FLS_OK) { return rc; }
-	if (!p->parts.alloc(it.size() * 4) || !p->vec_cnt.alloc(it.size() * 4) || !p->vec_base.alloc(it.size() * 4) ||
-	    !p->bw_code.alloc(it.size() * 4) || !p->dict_n.alloc(chunks.size() * 4)) {
+	if (!p->parts.alloc(it.size() * 4) || !p->bw_code.alloc(it.size() * 4) || !p->dict_n.alloc(chunks.size() * 4)) {
 		return FLS_ERR_CUDA;
+	}
+	DevMem vlen, vclen, dict_w;
+	if (p->str) {
+		// the rows of every vector: hashes (the columns the integer passes read), lengths, compressed lengths
+		if (!vlen.alloc(it.size() * 8) || !vclen.alloc(it.size() * 8) || !dict_w.alloc(chunks.size() * 16)) {
+			return FLS_ERR_CUDA;
+		}
+		k_str_rows<<<grid_for(it.size()), kWarps * 32, 0, s>>>(p->scols_d.as<StrCol>(), items_d.as<Item>(), it.size(),
+		                                                       vlen.as<uint64_t>(), vclen.as<uint64_t>());
+		++launch_counter();
 	}
 	ItemArgs ia {p->cols_d.as<Col>(), items_d.as<Item>(), it.size()};
 	k_parts<<<grid_for(it.size()), kWarps * 32, 0, s>>>(ia, p->parts.as<uint32_t>());
 	++launch_counter();
-	// dictionary, one group of chunks at a time
-	for (size_t g0 = 0; g0 < chunks.size(); g0 += p->group) {
-		const uint32_t ng = static_cast<uint32_t>(std::min<size_t>(p->group, chunks.size() - g0));
-		DictArgs       a {};
-		a.it           = ItemArgs {p->cols_d.as<Col>(), items_d.as<Item>() + ranges[g0], ranges[g0 + ng] - ranges[g0]};
-		a.group_chunk0 = static_cast<uint32_t>(g0);
-		a.keys         = p->keys.as<uint64_t>();
-		a.first        = p->first.as<uint32_t>();
-		a.code         = p->code.as<uint32_t>();
-		a.used         = p->used.as<uint32_t>();
-		a.vec_cnt      = p->vec_cnt.as<uint32_t>() + ranges[g0];
-		a.vec_base     = p->vec_base.as<uint32_t>() + ranges[g0];
-		a.dict_n       = p->dict_n.as<uint32_t>();
-		a.bw_code      = p->bw_code.as<uint32_t>() + ranges[g0];
-		a.status       = dev->status;
-		// chunk ranges relative to the group's first item
-		std::vector<uint32_t> rel(ng + 1);
-		for (uint32_t i = 0; i <= ng; ++i) { rel[i] = ranges[g0 + i] - ranges[g0]; }
-		DevMem rel_d;
-		if ((rc = upload(rel_d, rel.data(), rel.size() * 4)) != FLS_OK) { return rc; }
-		const int gi = grid_for(a.it.n_items);
-		k_dict<0><<<gi, kWarps * 32, 0, s>>>(a);
-		k_dict<1><<<gi, kWarps * 32, 0, s>>>(a);
-		k_dict_scan<<<(ng + 7) / 8, 256, 0, s>>>(a, rel_d.as<uint32_t>(), ng);
-		k_dict<2><<<gi, kWarps * 32, 0, s>>>(a);
-		k_dict<3><<<gi, kWarps * 32, 0, s>>>(a);
-		k_dict_reset<<<std::min<uint32_t>(ng, 4096), 256, 0, s>>>(a, rel_d.as<uint32_t>(), ng);
-		launch_counter() += 6;
+	// dictionary of every chunk: one CTA per chunk, tables in shared memory
+	{
+		static bool attr[64] = {};
+		if (dev->ordinal < 0 || dev->ordinal >= 64) { return FLS_ERR_CUDA; }
+		if (!attr[dev->ordinal]) {
+			if (cudaFuncSetAttribute(k_chunk_dict, cudaFuncAttributeMaxDynamicSharedMemorySize, kCdSmem) != cudaSuccess) {
+				return FLS_ERR_CUDA;
+			}
+			attr[dev->ordinal] = true;
+		}
+		ChunkDictArgs a {p->cols_d.as<Col>(), items_d.as<Item>(), ranges_d.as<uint32_t>(),
+		                 static_cast<uint32_t>(chunks.size()), p->dict_n.as<uint32_t>(), p->bw_code.as<uint32_t>(),
+		                 dev->status, nullptr, nullptr, nullptr};
+		if (p->str) {
+			const uint32_t* const* wp = p->wptr_d.as<const uint32_t*>();
+			a.w0                      = wp;
+			a.w1                      = wp + p->scols.size();
+			a.dict_w                  = dict_w.as<uint64_t>();
+		}
+		k_chunk_dict<<<static_cast<unsigned>(std::min<size_t>(chunks.size(), 65535)), kCdWarps * 32, kCdSmem, s>>>(a);
+		++launch_counter();
 		if (cudaGetLastError() != cudaSuccess) { return FLS_ERR_CUDA; }
-		if (cudaStreamSynchronize(s) != cudaSuccess) { return FLS_ERR_CUDA; } // rel_d is freed on return
 	}
 	uint64_t* sizes = d_sizes;
 	uint8_t*  best  = d_best;
@@ -1035,9 +1336,16 @@ int wizard_run(fls_sel_plan* p, const std::vector<uint32_t>& subset, uint64_t* d
 		sizes = sizes_tmp.as<uint64_t>();
 		best  = best_tmp.as<uint8_t>();
 	}
-	SizeArgs sa {p->cols_d.as<Col>(), ccol_d.as<uint32_t>(), ranges_d.as<uint32_t>(), p->parts.as<uint32_t>(),
-	             p->bw_code.as<uint32_t>(), p->dict_n.as<uint32_t>(), static_cast<uint32_t>(chunks.size()), sizes, best};
-	k_chunk_sizes<<<static_cast<unsigned>((chunks.size() + 7) / 8), 256, 0, s>>>(sa);
+	if (p->str) {
+		StrSizeArgs sa {ccol_d.as<uint32_t>(), ranges_d.as<uint32_t>(), p->parts.as<uint32_t>(), p->bw_code.as<uint32_t>(),
+		                vlen.as<uint64_t>(), vclen.as<uint64_t>(), p->dict_n.as<uint32_t>(), dict_w.as<uint64_t>(),
+		                p->scols_d.as<StrCol>(), static_cast<uint32_t>(chunks.size()), sizes, best};
+		k_str_sizes<<<static_cast<unsigned>((chunks.size() + 7) / 8), 256, 0, s>>>(sa);
+	} else {
+		SizeArgs sa {p->cols_d.as<Col>(), ccol_d.as<uint32_t>(), ranges_d.as<uint32_t>(), p->parts.as<uint32_t>(),
+		             p->bw_code.as<uint32_t>(), p->dict_n.as<uint32_t>(), static_cast<uint32_t>(chunks.size()), sizes, best};
+		k_chunk_sizes<<<static_cast<unsigned>((chunks.size() + 7) / 8), 256, 0, s>>>(sa);
+	}
 	++launch_counter();
 	if (cudaGetLastError() != cudaSuccess) { return FLS_ERR_CUDA; }
 	if (!all) {
@@ -1091,18 +1399,111 @@ int fls_sel_plan_create(const fls_sel_column* cols, uint32_t n_cols, uint32_t ch
 	int rc;
 	if ((rc = upload(p->cols_d, p->cols.data(), p->cols.size() * sizeof(Col))) != FLS_OK) { return rc; }
 	if ((rc = upload(p->items_d, p->items.data(), p->items.size() * sizeof(Item))) != FLS_OK) { return rc; }
-	// wizard hash tables: up to 1024 chunks at a time, empty once here (each run leaves them empty)
-	p->group             = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(p->n_chunks, 1024)));
-	const uint64_t slots = static_cast<uint64_t>(p->group) * (kTable + 1);
-	if (!p->keys.alloc(slots * 8) || !p->first.alloc(slots * 4) || !p->code.alloc(slots * 4) ||
-	    !p->used.alloc(static_cast<uint64_t>(p->group) * kMaxVecPerChunk * 1024 * 4)) {
-		return FLS_ERR_CUDA;
-	}
-	if (cudaMemset(p->keys.p, 0xFF, slots * 8) != cudaSuccess || cudaMemset(p->first.p, 0xFF, slots * 4) != cudaSuccess ||
-	    cudaDeviceSynchronize() != cudaSuccess) {
-		return FLS_ERR_CUDA;
-	}
 	*out = p.release();
+	return FLS_OK;
+}
+
+} // extern "C"
+
+namespace flsgpu {
+int fsst_import_table(const uint8_t* buf, uint64_t avail, FsstTable* t, uint64_t* used);
+}
+
+namespace {
+// An exported FSST table (fsst_export format) arranged for greedy matching: its symbols grouped by first byte,
+// longest first (the codes past the table's symbol count, which decode as "corrupt", are not symbols).
+int arrange_table(const uint8_t* tab, uint64_t n, StrTab* out) {
+	FsstTable t {};
+	const int rc = fsst_import_table(tab, n, &t, nullptr);
+	if (rc != FLS_OK) { return rc; }
+	const uint32_t zt = tab[8] & 1u;
+	uint32_t       count = 0;
+	for (uint32_t l = 0; l < 8; ++l) { count += tab[9 + l]; }
+	if (zt && count) { --count; }
+	std::vector<uint32_t> codes;
+	for (uint32_t c = zt; c < zt + count && c < 255; ++c) { codes.push_back(c); }
+	std::stable_sort(codes.begin(), codes.end(), [&](uint32_t x, uint32_t y) {
+		const uint32_t bx = static_cast<uint32_t>(t.sym[x] & 0xFFu), by = static_cast<uint32_t>(t.sym[y] & 0xFFu);
+		return bx != by ? bx < by : t.len[x] > t.len[y];
+	});
+	std::memset(out, 0, sizeof(*out));
+	uint32_t k = 0;
+	for (uint32_t b = 0; b < 256; ++b) {
+		out->start[b] = static_cast<uint16_t>(k);
+		while (k < codes.size() && (t.sym[codes[k]] & 0xFFu) == b) {
+			out->val[k] = t.sym[codes[k]];
+			out->len[k] = t.len[codes[k]];
+			++k;
+		}
+	}
+	out->start[256] = static_cast<uint16_t>(k);
+	return FLS_OK;
+}
+} // namespace
+
+extern "C" {
+
+int fls_sel_plan_create_strings(const fls_sel_str_column* cols, uint32_t n_cols, uint32_t chunk_vectors,
+                                fls_sel_plan** out) {
+	if (!out || (!cols && n_cols)) { return FLS_ERR_ARG; }
+	*out = nullptr;
+	uint64_t rows = 0;
+	for (uint32_t c = 0; c < n_cols; ++c) {
+		if (cols[c].n_rows % 1024 || (cols[c].n_rows && (!cols[c].d_offsets || !cols[c].table)) ||
+		    cols[c].n_rows >= (1ull << 41)) {
+			return FLS_ERR_ARG;
+		}
+		rows += cols[c].n_rows;
+	}
+	DevMem hash, len, clen, tabs;
+	if (!hash.alloc(rows * 8 + 16) || !len.alloc(rows * 4 + 16) || !clen.alloc(rows * 4 + 16) ||
+	    !tabs.alloc(sizeof(StrTab) * (n_cols ? n_cols : 1))) {
+		return FLS_ERR_CUDA;
+	}
+	// the plan's integer columns are the row hashes
+	std::vector<fls_sel_column> hc(n_cols);
+	std::vector<StrCol>         sc(n_cols);
+	std::vector<StrTab>         st(n_cols);
+	uint64_t                    r0 = 0;
+	for (uint32_t c = 0; c < n_cols; ++c) {
+		const fls_sel_str_column& x = cols[c];
+		if (x.n_rows) {
+			const int rc = arrange_table(x.table, x.table_size, &st[c]);
+			if (rc != FLS_OK) { return rc; }
+		}
+		uint64_t nb = 0;
+		if (x.n_rows && cudaMemcpy(&nb, x.d_offsets + x.n_rows, 8, cudaMemcpyDeviceToHost) != cudaSuccess) {
+			return FLS_ERR_CUDA;
+		}
+		hc[c]          = fls_sel_column {};
+		hc[c].d_values = hash.as<uint64_t>() + r0;
+		hc[c].n_vec    = x.n_rows / 1024;
+		hc[c].width    = 64;
+		sc[c] = StrCol {x.d_bytes, x.d_offsets, nb, tabs.as<StrTab>() + c, static_cast<uint32_t>(x.table_size),
+		                hash.as<uint64_t>() + r0, len.as<uint32_t>() + r0, clen.as<uint32_t>() + r0};
+		r0 += x.n_rows;
+	}
+	fls_sel_plan* p  = nullptr;
+	int           rc = fls_sel_plan_create(hc.data(), n_cols, chunk_vectors, &p);
+	if (rc != FLS_OK) { return rc; }
+	std::unique_ptr<fls_sel_plan> own(p);
+	std::vector<const uint32_t*>  wp(2 * n_cols);
+	for (uint32_t c = 0; c < n_cols; ++c) {
+		wp[c]          = sc[c].len;
+		wp[n_cols + c] = sc[c].clen;
+	}
+	if (n_cols && (cudaMemcpy(tabs.p, st.data(), sizeof(StrTab) * n_cols, cudaMemcpyHostToDevice) != cudaSuccess ||
+	               (rc = upload(own->scols_d, sc.data(), sizeof(StrCol) * n_cols)) != FLS_OK ||
+	               (rc = upload(own->wptr_d, wp.data(), sizeof(void*) * wp.size())) != FLS_OK)) {
+		return rc != FLS_OK ? rc : FLS_ERR_CUDA;
+	}
+	own->str   = true;
+	own->scols = sc;
+	own->hash_d.p = hash.p, hash.p = nullptr;
+	own->len_d.p  = len.p, len.p = nullptr;
+	own->clen_d.p = clen.p, clen.p = nullptr;
+	own->tabs_d.p = tabs.p, tabs.p = nullptr;
+	*out          = own.release();
 	return FLS_OK;
 }
 
@@ -1143,6 +1544,27 @@ int fls_sel_wizard(fls_sel_plan* p, uint64_t* d_sizes, uint8_t* d_best, uint32_t
 	return wizard_run(p, {}, d_sizes, d_best, d_dict_n, static_cast<cudaStream_t>(stream));
 }
 
+} // extern "C"
+
+namespace {
+// Statistics of the items of a: for a string plan, the sampled vectors' rows first (hashes, lengths, compressed
+// lengths), then the hash features with the string slots filled in.
+cudaError_t sample_features(fls_sel_plan* p, const ItemArgs& a, float* feat, cudaStream_t s) {
+	if (p->str) {
+		k_str_rows<<<grid_for(a.n_items), kWarps * 32, 0, s>>>(p->scols_d.as<StrCol>(), a.items, a.n_items, nullptr,
+		                                                      nullptr);
+		++launch_counter();
+	}
+	cudaError_t e = launch_features(a, feat, s);
+	if (e != cudaSuccess || !p->str) { return e; }
+	k_str_features<<<grid_for(a.n_items), kWarps * 32, 0, s>>>(p->scols_d.as<StrCol>(), a.items, a.n_items, feat);
+	++launch_counter();
+	return cudaGetLastError();
+}
+} // namespace
+
+extern "C" {
+
 int fls_sel_features(fls_sel_plan* p, uint32_t stride, float* d_feat, uint32_t* d_row_chunk, uint64_t* n_rows,
                      void* stream) {
 	if (!p || stride == 0 || !n_rows) { return FLS_ERR_ARG; }
@@ -1153,7 +1575,7 @@ int fls_sel_features(fls_sel_plan* p, uint32_t stride, float* d_feat, uint32_t* 
 	if (!d_feat || set->n == 0) { return FLS_OK; }
 	cudaStream_t s = static_cast<cudaStream_t>(stream);
 	ItemArgs     a {p->cols_d.as<Col>(), set->items.as<Item>(), set->n};
-	if (launch_features(a, d_feat, s) != cudaSuccess) { return FLS_ERR_CUDA; }
+	if (sample_features(p, a, d_feat, s) != cudaSuccess) { return FLS_ERR_CUDA; }
 	if (d_row_chunk && cudaMemcpyAsync(d_row_chunk, set->row_chunk.p, set->n * 4, cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
 		return FLS_ERR_CUDA;
 	}
@@ -1178,13 +1600,13 @@ int fls_sel_learned(fls_sel_plan* p, const float* d_params, uint32_t stride, flo
 	float*   z    = h2 + n * H;
 	float*   prob = z + n * K;
 	ItemArgs a {p->cols_d.as<Col>(), set->items.as<Item>(), n};
-	if (launch_features(a, feat, s) != cudaSuccess) { return FLS_ERR_CUDA; }
+	if (sample_features(p, a, feat, s) != cudaSuccess) { return FLS_ERR_CUDA; }
 	if (forward(s, d_params, feat, n, h1, h2, z) != cudaSuccess) { return FLS_ERR_CUDA; }
 	k_softmax<<<static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 4096)), 256, 0, s>>>(z, n, prob, nullptr, nullptr,
 	                                                                                            nullptr, nullptr, nullptr);
 	k_vote<<<static_cast<unsigned>((p->n_chunks + 7) / 8), 256, 0, s>>>(prob, set->chunk_items.as<uint32_t>(),
 	                                                                     static_cast<uint32_t>(p->n_chunks), d_choice,
-	                                                                     conf.as<float>());
+	                                                                     conf.as<float>(), p->str ? kStrK : K);
 	launch_counter() += 2;
 	if (cudaGetLastError() != cudaSuccess) { return FLS_ERR_CUDA; }
 	if (d_conf && cudaMemcpyAsync(d_conf, conf.p, p->n_chunks * 4, cudaMemcpyDeviceToDevice, s) != cudaSuccess) {

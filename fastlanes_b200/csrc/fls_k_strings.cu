@@ -511,11 +511,26 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_stream_pass(const StrArgs
 			}
 			continue;
 		}
+		if (lane == 0 && (k + 1) % kStrPB != 0) {
+			// the next vector's packed row offsets towards L2
+			const Plan q = unpack_plan(plans[(k + 1) % kStrPB]);
+			const uintptr_t lo = (reinterpret_cast<uintptr_t>(q.src) + 15) & ~uintptr_t(15);
+			const uintptr_t hi = (reinterpret_cast<uintptr_t>(q.src) + q.bytes) & ~uintptr_t(15);
+			if (q.ok && hi > lo) { bulk_prefetch_l2(reinterpret_cast<const void*>(lo), static_cast<uint32_t>(hi - lo)); }
+		}
 		load_rows<false>(p, buf, lane, a.status);
 		uint32_t       vn  = 0;
 		const uint8_t* vb  = vector_bytes(a.col, static_cast<uint32_t>(v), &vn);
 		bool           bad = false;
 		StreamOut      o {};
+		if (lane == 0 && v + nw < n) {
+			// the warp's next vector's bytes towards L2 (the 16-byte aligned part inside them)
+			uint32_t       nn = 0;
+			const uint8_t* nb = vector_bytes(a.col, static_cast<uint32_t>(v + nw), &nn);
+			const uintptr_t lo = (reinterpret_cast<uintptr_t>(nb) + 15) & ~uintptr_t(15);
+			const uintptr_t hi = (reinterpret_cast<uintptr_t>(nb) + nn) & ~uintptr_t(15);
+			if (hi > lo) { bulk_prefetch_l2(reinterpret_cast<const void*>(lo), static_cast<uint32_t>(hi - lo)); }
+		}
 		if constexpr (PASS == STR_PASS_LENGTHS) {
 			const uint32_t tot = stream_vector<false, kFsst, kStrWindow>(rows32, vb, vn, fsym, flen, lane, o, &bad);
 			if (lane == 0) {
@@ -652,10 +667,7 @@ __device__ __forceinline__ uint32_t dict_vector_out(const uint8_t* rows, const u
 		offs[32 * b + lane] = static_cast<uint32_t>(vbase + o);
 		if (fill + T > kStrWindow) { flush(false); }
 		if (fill + T <= kStrWindow) {
-			uint32_t   hk = 0, head = 0;
-			const bool mid = put_row(win32, fill + (o - vpos), reinterpret_cast<const uint32_t*>(dict), fs, fl, &hk, &head);
-			__syncwarp(); // every word's whole store lands before the rows that start inside it OR in
-			if (mid) { atomicOr(win32 + hk, head); }
+			put_rows_coop(win32, fill + (o - vpos), reinterpret_cast<const uint32_t*>(dict), fs, fl, lane);
 			fill += T;
 		} else {
 			// a batch larger than the window: straight to global memory after the window's pending bytes

@@ -48,6 +48,18 @@ _train = declare("fls_sel_train", _i, [_p, _p, _p, _p, _u32, _u32, _f, _p, _p])
 
 _WIDTH = {torch.int32: (32, 1), torch.int64: (64, 1)}
 
+STR_CANDIDATES = ("BYTE_ARR", "DICT", "FSST", "DICT_RLE")
+STR_POOL_IDS = (0, 3, 13, 15)  # reference string pool ids (src/cor/exp_pool.cpp:66-101)
+STR_K = len(STR_CANDIDATES)
+
+
+class SelStrColumn(ctypes.Structure):
+    _fields_ = [("d_bytes", _p), ("d_offsets", _p), ("n_rows", _u64), ("table", _p), ("table_size", _u64)]
+
+
+_plan_create_str = declare("fls_sel_plan_create_strings", _i, [ctypes.POINTER(SelStrColumn), _u32, _u32,
+                                                                ctypes.POINTER(_p)])
+
 
 def _stream(stream):
     return stream if stream is not None else torch.cuda.current_stream().cuda_stream
@@ -128,6 +140,33 @@ class SelectionPlan:
             pass
 
 
+class StrSelectionPlan(SelectionPlan):
+    """Chunks of a set of string columns: list of (bytes uint8 CUDA tensor, offsets int64 CUDA tensor of
+    n_rows + 1, the column's FSST table as host bytes).  wizard(): sizes n_chunks x 6 with the string
+    candidates (``STR_CANDIDATES``) in 0..3; features / learned as for integer columns."""
+
+    def __init__(self, columns, chunk_vectors=64):
+        cols = (SelStrColumn * max(len(columns), 1))()
+        self._keep = []
+        for i, (byts, offs, table) in enumerate(columns):
+            offs = offs.contiguous()
+            table = np.ascontiguousarray(table, np.uint8)
+            if offs.dtype != torch.int64 or not offs.is_cuda or (offs.numel() - 1) % 1024:
+                raise ValueError("offsets: int64 CUDA tensor of n_rows + 1, n_rows whole vectors")
+            self._keep += [byts, offs, table]
+            cols[i].d_bytes = byts.data_ptr()
+            cols[i].d_offsets = offs.data_ptr()
+            cols[i].n_rows = offs.numel() - 1
+            cols[i].table = table.ctypes.data
+            cols[i].table_size = table.size
+        h = _p()
+        check(_plan_create_str(cols, len(columns), chunk_vectors, ctypes.byref(h)), "fls_sel_plan_create_strings")
+        self.handle = h
+        nc, nv = _u64(), _u64()
+        check(_plan_info(h, ctypes.byref(nc), ctypes.byref(nv)), "plan_info")
+        self.n_chunks, self.n_vectors = nc.value, nv.value
+
+
 # ---- the MLP ----------------------------------------------------------------------------------------------
 def param_count():
     return int(_param_count())
@@ -197,6 +236,24 @@ def train_selector(n_chunks=3125, seed=0, epochs=10, batch=1024, lr=2e-3):
     params = mlp_init(seed)
     hist = train(params, feat, y, epochs=epochs, batch=batch, lr=lr, seed=seed)
     return params, hist
+
+
+def labelled_string_vectors(n_chunks=400, seed=0, chunk_vectors=16):
+    """Features and wizard labels of n_chunks seeded synthetic string chunks (one column each, families of
+    ``workloads.string_selection_column``); every vector carries its chunk's best string candidate."""
+    from . import workloads as W
+    rng = np.random.default_rng(seed)
+    cols = []
+    for _ in range(n_chunks):
+        byts, offs, table = W.string_selection_column(rng, chunk_vectors)
+        cols.append((torch.from_numpy(byts).cuda(), torch.from_numpy(offs.astype(np.int64)).cuda(), table))
+    plan = StrSelectionPlan(cols, chunk_vectors)
+    sizes, best, _ = plan.wizard()
+    feat, row_chunk = plan.features(1)
+    y = best.long()[row_chunk.long()]
+    out = (feat, y.to(torch.int32), sizes, best)
+    plan.close()
+    return out
 
 
 def ratio_loss(sizes, choice):

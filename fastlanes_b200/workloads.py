@@ -206,6 +206,76 @@ def zipf_codes(n_rows=16 << 20, n_dict=4096, a=1.1, seed=0):
     return ((rng.zipf(a, n_rows) - 1) % n_dict).astype(np.uint32)
 
 
+STRING_SELECTION_FAMILIES = ("dict_tokens", "dict_runs", "unique_tokens", "random_bytes", "few_long")
+
+
+def _gather_rows(dbytes, doffs, codes):
+    """Arrow (bytes, offsets) of rows = dictionary entries codes[r]."""
+    lens = np.diff(doffs).astype(np.int64)[codes]
+    offs = np.zeros(codes.size + 1, np.uint64)
+    offs[1:] = np.cumsum(lens)
+    idx = np.repeat(doffs[:-1][codes].astype(np.int64) - offs[:-1].astype(np.int64), lens)
+    idx += np.arange(idx.size, dtype=np.int64)
+    return dbytes[idx], offs
+
+
+def dict_rows_device(dict_bytes, dict_offsets, codes, device="cuda", chunk_rows=1 << 22):
+    """Arrow rows = dictionary entries codes[r], built on the device chunk by chunk: (bytes uint8, offsets
+    int64[n + 1]) tensors."""
+    db = torch.from_numpy(np.ascontiguousarray(dict_bytes, np.uint8)).to(device)
+    do = torch.from_numpy(np.asarray(dict_offsets).astype(np.int64)).to(device)
+    cd = torch.from_numpy(np.asarray(codes).astype(np.int64)).to(device)
+    lens = (do[1:] - do[:-1])[cd]
+    offs = torch.zeros(cd.numel() + 1, dtype=torch.int64, device=device)
+    offs[1:] = torch.cumsum(lens, 0)
+    out = torch.empty(int(offs[-1]) + 16, dtype=torch.uint8, device=device)
+    for a in range(0, cd.numel(), chunk_rows):
+        b = min(cd.numel(), a + chunk_rows)
+        o0, o1 = int(offs[a]), int(offs[b])
+        rows = torch.repeat_interleave(torch.arange(a, b, device=device), lens[a:b])
+        out[o0:o1] = db[do[cd[rows]] + (torch.arange(o0, o1, device=device) - offs[rows])]
+    return out, offs
+
+
+def string_selection_column(rng, n_vec, family=None):
+    """A seeded string column of n_vec vectors for expression selection: (bytes, offsets[n + 1] uint64, FSST
+    table bytes trained on a sample of its rows).  Families: token dictionaries with Zipf codes (DICT), the same
+    in runs (DICT_RLE), every row a fresh token string (FSST), random bytes (BYTE_ARR), a few long strings."""
+    from .strings import fsst_compress
+
+    n = n_vec * 1024
+    family = family or STRING_SELECTION_FAMILIES[rng.integers(0, len(STRING_SELECTION_FAMILIES))]
+    seed = int(rng.integers(0, 2 ** 31))
+    if family in ("dict_tokens", "dict_runs"):
+        dbytes, doffs = string_dictionary(seed=seed, n_dict=int(rng.integers(16, 4097)))
+        d = doffs.size - 1
+        if family == "dict_tokens":
+            codes = _zipf_codes(n, d, float(rng.uniform(0.8, 1.5)), torch.Generator().manual_seed(seed), "cpu").numpy()
+        else:
+            runs = rng.geometric(1.0 / float(rng.uniform(2, 64)), n)
+            codes = np.repeat(rng.integers(0, d, runs.size), runs)[:n]
+        byts, offs = _gather_rows(dbytes, doffs, codes)
+    elif family == "unique_tokens":
+        dbytes, doffs = string_dictionary(seed=seed, n_dict=n)
+        byts, offs = dbytes, doffs
+    elif family == "random_bytes":
+        lens = rng.integers(1, 41, n)
+        offs = np.zeros(n + 1, np.uint64)
+        offs[1:] = np.cumsum(lens)
+        byts = rng.integers(0, 256, int(offs[-1]), dtype=np.uint8)
+    else:  # few_long
+        d = int(rng.integers(4, 17))
+        lens = rng.integers(100, 256, d)
+        doffs = np.zeros(d + 1, np.uint64)
+        doffs[1:] = np.cumsum(lens)
+        dbytes = rng.integers(97, 123, int(doffs[-1]), dtype=np.uint8)
+        codes = _zipf_codes(n, d, 1.2, torch.Generator().manual_seed(seed), "cpu").numpy()
+        byts, offs = _gather_rows(dbytes, doffs, codes)
+    m = min(n, 4096)  # the table is trained on the column's first rows
+    table, _, _ = fsst_compress(byts[:int(offs[m])], offs[:m + 1])
+    return np.ascontiguousarray(byts, np.uint8), offs, table
+
+
 def dict_rows_match(offsets, data, dict_bytes, dict_offsets, codes, chunk_rows=1 << 22):
     """Whole-buffer parity of decoded DICT string rows: `offsets` (int32, n + 1) and `data` (uint8) on the device
     against the rows the generator meant -- row r is dictionary entry codes[r] -- built on the device by a

@@ -42,12 +42,37 @@ typedef struct fls_sel_column {
 typedef struct fls_sel_plan fls_sel_plan;
 
 /* Chunks: every column splits into chunks of chunk_vectors vectors (the last one may be shorter), numbered
- * column by column.  Synchronous (uploads the descriptors, allocates the wizard's hash tables). */
+ * column by column.  Synchronous (uploads the descriptors). */
 int fls_sel_plan_create(const fls_sel_column* cols, uint32_t n_cols, uint32_t chunk_vectors, fls_sel_plan** out);
 int fls_sel_plan_info(const fls_sel_plan* plan, uint64_t* n_chunks, uint64_t* n_vectors);
 /* host arrays of n_chunks entries: column, first vector, vector count of every chunk */
 int fls_sel_plan_chunks(const fls_sel_plan* plan, uint32_t* h_col, uint64_t* h_first, uint32_t* h_count);
 int fls_sel_plan_destroy(fls_sel_plan* plan);
+
+/* String columns (no counterpart in the reference's selection code, which picks per column by trial encoding:
+ * src/encoder/exp_col_encoder.cpp:18-28 over the string pool, src/cor/exp_pool.cpp:66-101).  Rows: Arrow
+ * offsets (n_rows + 1, u64, device) into d_bytes (device); n_rows whole vectors.  table: HOST bytes of the
+ * column's FSST symbol table in fsst_export's format, the one its DICT and FSST pages use.  A plan over string
+ * columns chooses among FLS_SEL_STR_K candidates (the string pool's no-patch expressions):
+ *
+ *   index  0 BYTE_ARR (pool id 0)   1 DICT FFOR over an FSST dictionary (id 3)   2 FSST (id 13)
+ *          3 DICT_RLE, raw run codes and a raw u16 run index (id 15)
+ *
+ * The wizard's sizes are exact for those pages, the dictionary holding a chunk's distinct rows in
+ * first-occurrence order compressed with the column's table (distinct rows are told apart by a 64-bit hash of
+ * their bytes); sizes 4 and 5 of a string chunk are UINT64_MAX.  fls_sel_wizard, fls_sel_features and
+ * fls_sel_learned take the plan as they take an integer one; the learned vote chooses among the 4.
+ * Synchronous. */
+#define FLS_SEL_STR_K 4
+typedef struct fls_sel_str_column {
+	const uint8_t*  d_bytes;
+	const uint64_t* d_offsets;
+	uint64_t        n_rows;
+	const uint8_t*  table;
+	uint64_t        table_size;
+} fls_sel_str_column;
+int fls_sel_plan_create_strings(const fls_sel_str_column* cols, uint32_t n_cols, uint32_t chunk_vectors,
+                                fls_sel_plan** out);
 
 /* Per vector (plan order: columns in order, vectors in order): bwF | bwD << 7 | bwI << 14 | runs << 19, where
  * bwF / bwD are the FFOR bit widths of the values / of their DELTA deltas, runs the runs in original order and

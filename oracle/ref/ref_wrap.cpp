@@ -457,3 +457,41 @@ extern "C" int ref_unffor_batch(int w, const uint8_t* packed, const uint64_t* by
 	for (auto& t : ts) { t.join(); }
 	return 0;
 }
+
+// The reference's column decode of FFOR vectors as decode_to_memory runs it (src/encoder/exp_col_decoder.cpp:13-26):
+// per vector, the generated unffor into the vector buffer (ffor_decompress, src/cor/prm/ffor/ffor_decompress.cpp)
+// then Materializer::Materialize's untranspose_i into the output (src/encoder/materializer.cpp:13-21): values in
+// original order.  Vector ranges split over n_threads threads (the reference itself runs one).
+template <typename T>
+static void decode_ffor_range(const uint8_t* packed, const uint64_t* byte_off, const uint8_t* bw, const uint8_t* base,
+                              uint64_t lo, uint64_t hi, uint8_t* out) {
+	alignas(64) T vec[1024];
+	for (uint64_t v = lo; v < hi; ++v) {
+		gen::unffor::fallback::scalar::unffor(reinterpret_cast<const T*>(packed + byte_off[v]), vec, bw[v],
+		                                      reinterpret_cast<const T*>(base) + v);
+		gen::untranspose::fallback::scalar::untranspose_i(vec, reinterpret_cast<T*>(out) + v * 1024);
+	}
+}
+
+extern "C" int ref_decode_ffor_batch(int w, const uint8_t* packed, const uint64_t* byte_off, const uint8_t* bw,
+                                     const uint8_t* base, uint64_t n_vec, uint8_t* out, int n_threads) {
+	if (w != 32 && w != 64) { return -1; }
+	if (n_threads < 1) { n_threads = 1; }
+	auto work = [&](uint64_t lo, uint64_t hi) {
+		if (w == 32) {
+			decode_ffor_range<uint32_t>(packed, byte_off, bw, base, lo, hi, out);
+		} else {
+			decode_ffor_range<uint64_t>(packed, byte_off, bw, base, lo, hi, out);
+		}
+	};
+	std::vector<std::thread> ts;
+	const uint64_t           per = (n_vec + n_threads - 1) / n_threads;
+	for (int t = 0; t < n_threads; ++t) {
+		const uint64_t lo = t * per;
+		const uint64_t hi = lo + per < n_vec ? lo + per : n_vec;
+		if (lo >= hi) { break; }
+		ts.emplace_back(work, lo, hi);
+	}
+	for (auto& t : ts) { t.join(); }
+	return 0;
+}

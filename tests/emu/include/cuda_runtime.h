@@ -30,6 +30,10 @@ inline uint32_t __funnelshift_r(uint32_t lo, uint32_t hi, uint32_t s) {
 	const uint64_t x = (static_cast<uint64_t>(hi) << 32) | lo;
 	return static_cast<uint32_t>(x >> (s & 31u));
 }
+inline uint32_t __funnelshift_l(uint32_t lo, uint32_t hi, uint32_t s) {
+	const uint64_t x = (static_cast<uint64_t>(hi) << 32) | lo;
+	return static_cast<uint32_t>((x << (s & 31u)) >> 32);
+}
 inline uint32_t __byte_perm(uint32_t x, uint32_t y, uint32_t s) {
 	uint8_t b[8];
 	std::memcpy(b, &x, 4);
