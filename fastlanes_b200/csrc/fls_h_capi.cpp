@@ -224,7 +224,7 @@ int encode_t(const T* in, uint64_t n, uint64_t cap, uint8_t* out, uint64_t* out_
 }
 
 // The three streams of the host decode pipeline of the current device: copies in, decode, copies out.
-constexpr uint32_t kPipeEvents = 256;    // three per chunk: enough for a 65,535-vector page of 8-byte values
+constexpr uint32_t kPipeEvents = 256;    // two per chunk: enough for a 65,535-vector page of 8-byte values
 constexpr uint32_t kPipeIds     = 65536; // the identity work queue of a page's vectors, uploaded once
 struct HostPipe {
 	cudaStream_t in = nullptr, dec = nullptr, out = nullptr;
@@ -352,7 +352,7 @@ int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_
 		bounds.push_back(static_cast<uint32_t>(std::min<uint64_t>(pi.vec_c, bounds.back() + step)));
 	}
 	const uint32_t n_chunks = static_cast<uint32_t>(bounds.size() - 1);
-	if (3ull * n_chunks > kPipeEvents) { return FLS_ERR_TOO_LARGE; }
+	if (2ull * n_chunks > kPipeEvents) { return FLS_ERR_TOO_LARGE; }
 	cudaEvent_t* ev = hp->ev;
 	const Family fam = post_is_patch(pi.layout->post)    ? Family::NUM_PATCH
 	                   : !post_is_gather(pi.layout->post) ? Family::NUM
@@ -360,15 +360,9 @@ int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_
 	                                                      : Family::GATHER;
 	// page header, buffer offsets and entry points first
 	if (cudaMemcpyAsync(dp, page, pi.meta_sz, cudaMemcpyHostToDevice, hp->in) != cudaSuccess) { return FLS_ERR_CUDA; }
-	// the copies in run at most kLead chunks ahead of the copies out: the link's two directions share its
-	// bandwidth, and the larger outbound transfer should not wait behind inbound bytes needed only later
-	constexpr uint32_t kLead = 2;
 	for (uint32_t k = 0; k < n_chunks; ++k) {
 		const uint32_t v0 = bounds[k];
 		const uint32_t v1 = bounds[k + 1];
-		if (k >= kLead && cudaStreamWaitEvent(hp->in, ev[2 * n_chunks + k - kLead], 0) != cudaSuccess) {
-			return FLS_ERR_CUDA;
-		}
 		for (uint32_t b = 0; b < pi.arr_c; ++b) {
 			if (static_cast<int>(b) == rec_b) { continue; } // already in place (and decoded)
 			const uint64_t lo = pi.off[b] + ep(v0, b);
@@ -393,8 +387,7 @@ int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_
 		}
 		const uint64_t o0 = static_cast<uint64_t>(v0) * 1024 * sz, ob = static_cast<uint64_t>(v1 - v0) * 1024 * sz;
 		if (cudaMemcpyAsync(static_cast<uint8_t*>(out) + o0, d_out.as<uint8_t>() + o0, ob, cudaMemcpyDeviceToHost,
-		                    hp->out) != cudaSuccess ||
-		    cudaEventRecord(ev[2 * n_chunks + k], hp->out) != cudaSuccess) {
+		                    hp->out) != cudaSuccess) {
 			return FLS_ERR_CUDA;
 		}
 	}

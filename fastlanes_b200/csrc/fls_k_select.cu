@@ -411,23 +411,26 @@ __global__ void __launch_bounds__(kWarps * 32) k_features(ItemArgs a, float* fea
 }
 
 // ---------------------------------------------------------------------------------------------------------
-// Dictionary of a chunk (wizard), one CTA per chunk, in shared memory: the chunk's distinct values, numbered in
-// first-occurrence order (src/cor/lyt/dic/dic_fac.cpp:19-40), give the dictionary size and every vector's code
-// bit width.  A 16 Ki-slot open-addressing table holds the keys of one hash partition at a time (1 partition; a
-// chunk with more than kCdCap distinct values in a partition is redone with kCdParts of them):
-//   sweep 1   per partition: insert its keys, first position by atomicMin; every key's first position sets a bit
-//             in the chunk's position bitmap (64 Ki bits);
-//   prefix    popcounts of the bitmap words, scanned: the code of a first position is its rank among them;
-//   sweep 2   per partition: insert its keys again, then every value's code = rank(first position); each warp
-//             keeps the code range of its vectors.
-// Exact for every chunk; no global atomics, no table in global memory.
+// Dictionary of a chunk (wizard), one CTA per chunk: the chunk's distinct values, numbered in first-occurrence
+// order (src/cor/lyt/dic/dic_fac.cpp:19-40), give the dictionary size and every vector's code bit width.
+//   table     open addressing in shared memory (16 Ki slots), first position of every key by atomicMin.  A
+//             chunk with more than kCdCap distinct values is split by hash into kCdParts buckets instead: one
+//             read of the values scatters (key, position) pairs into the CTA's bucket scratch in global memory
+//             (each bucket has room for the whole chunk), and every bucket (about 1/8 of the keys) goes
+//             through the shared-memory table in turn, read back coalesced;
+//   ranks     every key's first position sets a bit in the chunk's position bitmap (64 Ki bits, shared memory);
+//             popcounts of the bitmap words, scanned, rank the first positions: a value's code;
+//   codes     every value's code (the values again, or the buckets again), the code range of each vector.
+// Exact for every chunk.
 // ---------------------------------------------------------------------------------------------------------
-constexpr uint32_t kCdSlots = 1u << 14;
-constexpr uint32_t kCdCap   = 12288; // keys of one partition (a load of 3/4)
-constexpr uint32_t kCdParts = 8;     // partitions of a chunk that exceeds kCdCap (8 x 12288 > 65,536 values)
-constexpr int      kCdWarps = 16;
-constexpr uint32_t kCdWords = kMaxVecPerChunk * 1024 / 32;
-constexpr uint32_t kCdSmem  = kCdSlots * 8 + (kCdSlots + 1) * 4 + 2 * kCdWords * 4;
+constexpr uint32_t kCdSlots  = 1u << 14;
+constexpr uint32_t kCdCap    = 12288; // distinct values the shared-memory table takes (a load of 3/4)
+constexpr uint32_t kCdParts  = 8;     // buckets of a chunk of more distinct values (8 x 12288 > 65,536)
+constexpr uint32_t kCdBucket = kMaxVecPerChunk * 1024;  // room of a bucket: the whole chunk
+constexpr int      kCdWarps  = 16;
+constexpr uint32_t kCdWords  = kMaxVecPerChunk * 1024 / 32;
+constexpr uint32_t kCdSmem   = kCdSlots * 8 + (kCdSlots + 1) * 4 + 2 * kCdWords * 4 + 2 * kMaxVecPerChunk * 4;
+constexpr uint64_t kCdGBytes = static_cast<uint64_t>(kCdParts) * kCdBucket * 12; // per CTA: keys, then positions
 static_assert(kCdSmem <= 227 * 1024, "chunk dictionary tables fit one CTA");
 static_assert(kMaxVecPerChunk <= 4 * kCdWarps, "at most 4 vectors of a chunk per warp");
 
@@ -445,9 +448,10 @@ struct ChunkDictArgs {
 	const uint32_t* const* w0;
 	const uint32_t* const* w1;
 	uint64_t*       dict_w;
+	uint8_t*        gtab; // gridDim.x regions of kCdGBytes: the CTAs' bucket scratch
 };
 
-// 64-bit finaliser of MurmurHash3 (Appleby): slot from the low bits, partition from the high ones.
+// 64-bit finaliser of MurmurHash3 (Appleby): the slot from the low bits.
 __device__ __forceinline__ uint64_t cd_mix(uint64_t x) {
 	x ^= x >> 33;
 	x *= 0xff51afd7ed558ccdull;
@@ -456,14 +460,14 @@ __device__ __forceinline__ uint64_t cd_mix(uint64_t x) {
 	x ^= x >> 33;
 	return x;
 }
-__device__ __forceinline__ uint32_t cd_part(uint64_t h, uint32_t parts) { return static_cast<uint32_t>(h >> 48) & (parts - 1); }
 
-// Slot of x (inserted when absent; *count counts new keys): kCdSlots for the key ~0 (its own slot), kCdSlots + 1
-// when the table is full.
-__device__ __forceinline__ uint32_t cd_insert(uint64_t* keys, uint64_t x, uint64_t h, uint32_t* count) {
-	if (x == kEmpty) { return kCdSlots; }
-	uint32_t s = static_cast<uint32_t>(h) & (kCdSlots - 1);
-	for (uint32_t probe = 0; probe < kCdSlots; ++probe) {
+// Slot of x in a table of mask + 1 slots (inserted when absent; *count counts new keys): mask + 1 for the key
+// ~0 (a slot of its own), mask + 2 when `limit` probes found neither x nor an empty slot.
+__device__ __forceinline__ uint32_t cd_insert(uint64_t* keys, uint32_t mask, uint64_t x, uint32_t* count,
+                                              uint32_t limit) {
+	if (x == kEmpty) { return mask + 1; }
+	uint32_t s = static_cast<uint32_t>(cd_mix(x)) & mask;
+	for (uint32_t probe = 0; probe < limit; ++probe) {
 		const uint64_t k = *reinterpret_cast<volatile uint64_t*>(keys + s);
 		if (k == x) { return s; }
 		if (k == kEmpty) {
@@ -474,109 +478,149 @@ __device__ __forceinline__ uint32_t cd_insert(uint64_t* keys, uint64_t x, uint64
 			}
 			if (old == x) { return s; }
 		}
-		s = (s + 1) & (kCdSlots - 1);
+		s = (s + 1) & mask;
 	}
-	return kCdSlots + 1;
+	return mask + 2;
 }
 
-__device__ __forceinline__ uint32_t cd_find(const uint64_t* keys, uint64_t x, uint64_t h) {
-	if (x == kEmpty) { return kCdSlots; }
-	uint32_t s = static_cast<uint32_t>(h) & (kCdSlots - 1);
-	for (uint32_t probe = 0; probe < kCdSlots; ++probe) {
+__device__ __forceinline__ uint32_t cd_find(const uint64_t* keys, uint32_t mask, uint64_t x) {
+	if (x == kEmpty) { return mask + 1; }
+	uint32_t s = static_cast<uint32_t>(cd_mix(x)) & mask;
+	for (uint32_t probe = 0; probe <= mask; ++probe) {
 		const uint64_t k = keys[s];
 		if (k == x) { return s; }
 		if (k == kEmpty) { break; }
-		s = (s + 1) & (kCdSlots - 1);
+		s = (s + 1) & mask;
 	}
-	return kCdSlots + 1;
+	return mask + 2;
 }
 
 template <int W>
 __device__ __forceinline__ void chunk_dict(const ChunkDictArgs& a, const Col& col, uint32_t c, uint64_t* keys,
-                                           uint32_t* first, uint32_t* bits, uint32_t* pref, uint32_t* s_count,
-                                           uint32_t* s_over, uint32_t* s_wsum, uint64_t* s_dw) {
+                                           uint32_t* first, uint32_t* bits, uint32_t* pref, uint32_t* vrange,
+                                           uint32_t* s_count, uint32_t* s_over, uint32_t* s_wsum, uint64_t* s_dw) {
 	using T             = typename UT<W>::T;
 	const uint32_t tid  = threadIdx.x, nt = blockDim.x, lane = tid & 31u, warp = tid >> 5, nw = nt >> 5;
 	const uint32_t i0   = a.chunk_items[c], i1 = a.chunk_items[c + 1];
 	const Item     m0   = a.items[i0];
 	const uint32_t v0   = m0.vec - m0.cpos; // the chunk's first vector
-	if (tid == 0) { s_dw[0] = s_dw[1] = 0; }
-	// insert the keys of partition p of the chunk (first positions by atomicMin); false on overflow
-	auto insert_part = [&](uint32_t p, uint32_t parts) {
+	constexpr uint32_t mask = kCdSlots - 1;
+	uint64_t* bkeys = reinterpret_cast<uint64_t*>(a.gtab + blockIdx.x * kCdGBytes);
+	uint32_t* bpos  = reinterpret_cast<uint32_t*>(bkeys + static_cast<uint64_t>(kCdParts) * kCdBucket);
+	auto begin_insert = [&]() {
 		if (tid == 0) {
 			*s_count = 0;
 			*s_over  = 0;
 		}
 		__syncthreads();
-		for (uint32_t j = i0 + warp; j < i1; j += nw) {
-			if (*reinterpret_cast<volatile uint32_t*>(s_count) > kCdCap) { break; } // redone with more partitions
-			const Item m = a.items[j];
-			T          x[32];
-			load_run<W>(col, m.vec, lane, x);
-			const uint32_t pos0 = m.cpos * 1024 + thread_run(lane);
-#pragma unroll
-			for (int i = 0; i < 32; ++i) {
-				const uint64_t h = cd_mix(static_cast<uint64_t>(x[i]));
-				if (cd_part(h, parts) != p && static_cast<uint64_t>(x[i]) != kEmpty) { continue; }
-				if (static_cast<uint64_t>(x[i]) == kEmpty && p != 0) { continue; } // the key ~0 belongs to partition 0
-				const uint32_t s = cd_insert(keys, x[i], h, s_count);
-				if (s > kCdSlots) {
-					*s_over = 1;
-				} else if (pos0 + i < first[s]) {
-					atomicMin(first + s, pos0 + i);
-				}
-			}
+	};
+	// limit: probes before an insert gives up (the first attempt gives up early: its table must never fill,
+	// or every insert into it walks all slots)
+	auto insert_one = [&](uint64_t key, uint32_t pos, uint32_t limit) {
+		const uint32_t sl = cd_insert(keys, mask, key, s_count, limit);
+		if (sl > mask + 1) {
+			*s_over = 1;
+		} else if (pos < first[sl]) {
+			atomicMin(first + sl, pos);
 		}
-		__syncthreads();
-		return *s_over == 0 && *s_count <= kCdCap;
 	};
 	auto clear_table = [&]() {
 		for (uint32_t k = tid; k < kCdSlots; k += nt) { keys[k] = kEmpty; }
 		for (uint32_t k = tid; k <= kCdSlots; k += nt) { first[k] = kNoPos; }
 		__syncthreads();
 	};
-	for (uint32_t k = tid; k < kCdWords; k += nt) { bits[k] = 0; }
-	clear_table();
-	// sweep 1: every partition's first positions into the bitmap
-	uint32_t parts = 1;
-	for (;;) {
-		bool ok = true;
-		for (uint32_t p = 0; p < parts && ok; ++p) {
-			ok = insert_part(p, parts);
-			if (ok) {
-				uint64_t sw0 = 0, sw1 = 0;
-				for (uint32_t k = tid; k <= kCdSlots; k += nt) {
-					const uint32_t f = first[k];
-					if (f != kNoPos) {
-						atomicOr(bits + (f >> 5), 1u << (f & 31u));
-						if (a.w0) {
-							const uint64_t row = static_cast<uint64_t>(v0) * 1024 + f;
-							sw0 += a.w0[m0.col][row];
-							sw1 += a.w1[m0.col][row];
-						}
-					}
-				}
+	// every key's first position into the bitmap (and, for strings, its row's weights); the table emptied
+	auto harvest = [&]() {
+		uint64_t sw0 = 0, sw1 = 0;
+		for (uint32_t k = tid; k <= mask + 1; k += nt) {
+			const uint32_t f = first[k];
+			if (f != kNoPos) {
+				atomicOr(bits + (f >> 5), 1u << (f & 31u));
 				if (a.w0) {
-					sw0 = warp_sum(sw0);
-					sw1 = warp_sum(sw1);
-					if (lane == 0) {
-						atomicAdd(reinterpret_cast<unsigned long long*>(s_dw), static_cast<unsigned long long>(sw0));
-						atomicAdd(reinterpret_cast<unsigned long long*>(s_dw + 1), static_cast<unsigned long long>(sw1));
-					}
+					const uint64_t row = static_cast<uint64_t>(v0) * 1024 + f;
+					sw0 += a.w0[m0.col][row];
+					sw1 += a.w1[m0.col][row];
 				}
-				__syncthreads();
 			}
+		}
+		if (a.w0) {
+			sw0 = warp_sum(sw0);
+			sw1 = warp_sum(sw1);
+			if (lane == 0) {
+				atomicAdd(reinterpret_cast<unsigned long long*>(s_dw), static_cast<unsigned long long>(sw0));
+				atomicAdd(reinterpret_cast<unsigned long long*>(s_dw + 1), static_cast<unsigned long long>(sw1));
+			}
+		}
+		__syncthreads();
+	};
+	auto code_of = [&](uint32_t f) { return pref[f >> 5] + __popc(bits[f >> 5] & ((1u << (f & 31u)) - 1u)); };
+	for (uint32_t k = tid; k < kCdWords; k += nt) { bits[k] = 0; }
+	for (uint32_t k = tid; k < 2 * kMaxVecPerChunk; k += nt) { vrange[k] = (k & 1u) ? 0u : ~0u; }
+	if (tid == 0) { s_dw[0] = s_dw[1] = 0; }
+	// first attempt: every key of the chunk in the shared-memory table.  A thread stops within 4 inserts of
+	// the count passing kCdCap (the table then holds at most kCdCap + 4 * 512 keys, 7/8 of its slots).
+	begin_insert();
+	volatile uint32_t* v_count = s_count;
+	volatile uint32_t* v_over  = s_over;
+	for (uint32_t j = i0 + warp; j < i1; j += nw) {
+		if (*v_over != 0 || *v_count > kCdCap) { break; } // too many: the buckets instead
+		const Item m = a.items[j];
+		T          x[32];
+		load_run<W>(col, m.vec, lane, x);
+		const uint32_t pos0 = m.cpos * 1024 + thread_run(lane);
+#pragma unroll
+		for (int i = 0; i < 32; ++i) {
+			if ((i & 3) == 0 && (*v_over != 0 || *v_count > kCdCap)) { break; }
+			insert_one(static_cast<uint64_t>(x[i]), pos0 + i, 256);
+		}
+	}
+	__syncthreads();
+	const bool small = *s_over == 0 && *s_count <= kCdCap;
+	__syncthreads();
+	uint32_t bcount[kCdParts];
+	if (small) {
+		harvest();
+	} else {
+		clear_table();
+		// one read of the values: (key, position) pairs into kCdParts buckets by hash
+		if (tid < kCdParts) { s_wsum[tid] = 0; }
+		__syncthreads();
+		for (uint32_t j = i0 + warp; j < i1; j += nw) {
+			const Item m = a.items[j];
+			T          x[32];
+			load_run<W>(col, m.vec, lane, x);
+			const uint32_t pos0 = m.cpos * 1024 + thread_run(lane);
+#pragma unroll
+			for (int i = 0; i < 32; ++i) {
+				const uint64_t key  = static_cast<uint64_t>(x[i]);
+				const uint32_t b    = static_cast<uint32_t>(cd_mix(key) >> 61);
+				const uint32_t peer = __match_any_sync(0xFFFFFFFFu, b);
+				const uint32_t lead = __ffs(peer) - 1;
+				uint32_t       base = 0;
+				if (lane == lead) { base = atomicAdd(s_wsum + b, static_cast<uint32_t>(__popc(peer))); }
+				base                 = __shfl_sync(peer, base, lead);
+				const uint32_t slot  = base + __popc(peer & ((1u << lane) - 1u));
+				const uint64_t where = static_cast<uint64_t>(b) * kCdBucket + slot;
+				bkeys[where]         = key;
+				bpos[where]          = pos0 + i;
+			}
+		}
+		__syncthreads();
+#pragma unroll
+		for (uint32_t b = 0; b < kCdParts; ++b) { bcount[b] = s_wsum[b]; }
+		__syncthreads();
+		// every bucket through the table
+		for (uint32_t b = 0; b < kCdParts; ++b) {
+			begin_insert();
+			for (uint32_t k = tid; k < bcount[b]; k += nt) {
+				const uint64_t where = static_cast<uint64_t>(b) * kCdBucket + k;
+				insert_one(bkeys[where], bpos[where], kCdSlots);
+			}
+			__syncthreads();
+			if ((*s_over != 0 || *s_count > mask) && tid == 0) { atomicOr(a.status, STATUS_BAD_INDEX); } // never
+			harvest();
 			clear_table();
 		}
-		if (ok) { break; }
-		if (parts == kCdParts) {
-			if (tid == 0) { atomicOr(a.status, STATUS_BAD_INDEX); } // cannot happen for 65,536 values
-			break;
-		}
-		parts = kCdParts;
-		for (uint32_t k = tid; k < kCdWords; k += nt) { bits[k] = 0; }
-		if (tid == 0) { s_dw[0] = s_dw[1] = 0; }
-		__syncthreads();
 	}
 	// ranks: exclusive prefix of the bitmap words' popcounts (thread t: words [t * per, (t + 1) * per))
 	const uint32_t per = kCdWords / nt;
@@ -599,37 +643,58 @@ __device__ __forceinline__ void chunk_dict(const ChunkDictArgs& a, const Col& co
 	}
 	const uint32_t total = s_wsum[32];
 	__syncthreads();
-	// sweep 2: codes of every value, the code range of each of the warp's vectors
-	uint32_t mn[4] = {~0u, ~0u, ~0u, ~0u}, mx[4] = {0u, 0u, 0u, 0u};
-	for (uint32_t p = 0; p < parts; ++p) {
-		insert_part(p, parts);
+	// codes: the code range of every vector of the chunk
+	if (small) {
 #pragma unroll
 		for (uint32_t q = 0; q < 4; ++q) {
-			const uint32_t j = i0 + warp + q * nw;
-			if (j >= i1) { continue; }
-			const Item m = a.items[j];
-			T          x[32];
-			load_run<W>(col, m.vec, lane, x);
+			const uint32_t j  = i0 + warp + q * nw;
+			uint32_t       mn = ~0u, mx = 0u;
+			if (j < i1) {
+				const Item m = a.items[j];
+				T          x[32];
+				load_run<W>(col, m.vec, lane, x);
 #pragma unroll
-			for (int i = 0; i < 32; ++i) {
-				const uint64_t h = cd_mix(static_cast<uint64_t>(x[i]));
-				if (static_cast<uint64_t>(x[i]) == kEmpty ? p != 0 : cd_part(h, parts) != p) { continue; }
-				const uint32_t s = cd_find(keys, x[i], h);
-				if (s > kCdSlots) { continue; }
-				const uint32_t f    = first[s];
-				const uint32_t code = pref[f >> 5] + __popc(bits[f >> 5] & ((1u << (f & 31u)) - 1u));
-				mn[q]               = min(mn[q], code);
-				mx[q]               = max(mx[q], code);
+				for (int i = 0; i < 32; ++i) {
+					const uint32_t sl = cd_find(keys, mask, static_cast<uint64_t>(x[i]));
+					if (sl > mask + 1) { continue; }
+					const uint32_t code = code_of(first[sl]);
+					mn                  = min(mn, code);
+					mx                  = max(mx, code);
+				}
+			}
+			mn = warp_min(mn);
+			mx = warp_max(mx);
+			if (j < i1 && lane == 0) {
+				vrange[2 * (j - i0)]     = mn;
+				vrange[2 * (j - i0) + 1] = mx;
 			}
 		}
 		__syncthreads();
 		clear_table();
+	} else {
+		for (uint32_t b = 0; b < kCdParts; ++b) {
+			begin_insert();
+			for (uint32_t k = tid; k < bcount[b]; k += nt) {
+				const uint64_t where = static_cast<uint64_t>(b) * kCdBucket + k;
+				insert_one(bkeys[where], bpos[where], kCdSlots);
+			}
+			__syncthreads();
+			for (uint32_t k = tid; k < bcount[b]; k += nt) {
+				const uint64_t where = static_cast<uint64_t>(b) * kCdBucket + k;
+				const uint32_t sl    = cd_find(keys, mask, bkeys[where]);
+				if (sl > mask + 1) { continue; }
+				const uint32_t code = code_of(first[sl]);
+				const uint32_t vi   = bpos[where] >> 10; // the vector inside the chunk
+				atomicMin(vrange + 2 * vi, code);
+				atomicMax(vrange + 2 * vi + 1, code);
+			}
+			__syncthreads();
+			clear_table();
+		}
 	}
-#pragma unroll
-	for (uint32_t q = 0; q < 4; ++q) {
-		const uint32_t j  = i0 + warp + q * nw;
-		const uint32_t lo = warp_min(mn[q]), hi = warp_max(mx[q]);
-		if (j < i1 && lane == 0) { a.bw_code[j] = hi >= lo ? bits_of(hi - lo) : 0u; }
+	for (uint32_t j = i0 + tid; j < i1; j += nt) {
+		const uint32_t lo = vrange[2 * (j - i0)], hi = vrange[2 * (j - i0) + 1];
+		a.bw_code[j]      = hi >= lo ? bits_of(hi - lo) : 0u;
 	}
 	if (tid == 0) {
 		a.dict_n[c] = total;
@@ -645,16 +710,20 @@ __global__ void __launch_bounds__(kCdWarps * 32) k_chunk_dict(ChunkDictArgs a) {
 	extern __shared__ __align__(16) uint8_t smem[];
 	__shared__ uint32_t s_count, s_over, s_wsum[33];
 	__shared__ uint64_t s_dw[2];
-	uint64_t*           keys  = reinterpret_cast<uint64_t*>(smem);
-	uint32_t*           first = reinterpret_cast<uint32_t*>(keys + kCdSlots);
-	uint32_t*           bits  = first + kCdSlots + 1;
-	uint32_t*           pref  = bits + kCdWords;
+	uint64_t*           keys   = reinterpret_cast<uint64_t*>(smem);
+	uint32_t*           first  = reinterpret_cast<uint32_t*>(keys + kCdSlots);
+	uint32_t*           bits   = first + kCdSlots + 1;
+	uint32_t*           pref   = bits + kCdWords;
+	uint32_t*           vrange = pref + kCdWords;
+	for (uint32_t k = threadIdx.x; k < kCdSlots; k += blockDim.x) { keys[k] = kEmpty; }
+	for (uint32_t k = threadIdx.x; k <= kCdSlots; k += blockDim.x) { first[k] = kNoPos; }
+	__syncthreads();
 	for (uint32_t c = blockIdx.x; c < a.n_chunks; c += gridDim.x) {
 		const Col col = a.cols[a.items[a.chunk_items[c]].col];
 		if (col.width == 64) {
-			chunk_dict<64>(a, col, c, keys, first, bits, pref, &s_count, &s_over, s_wsum, s_dw);
+			chunk_dict<64>(a, col, c, keys, first, bits, pref, vrange, &s_count, &s_over, s_wsum, s_dw);
 		} else {
-			chunk_dict<32>(a, col, c, keys, first, bits, pref, &s_count, &s_over, s_wsum, s_dw);
+			chunk_dict<32>(a, col, c, keys, first, bits, pref, vrange, &s_count, &s_over, s_wsum, s_dw);
 		}
 	}
 }
@@ -1214,8 +1283,9 @@ struct fls_sel_plan {
 	std::vector<uint64_t> chunk_first;
 	uint64_t              n_chunks = 0;
 	uint32_t              chunk_vectors = 64;
-	// wizard scratch
-	DevMem   bw_code, parts, dict_n;
+	// wizard scratch (gtab: the chunk dictionary's global-memory tables, one per CTA)
+	DevMem   bw_code, parts, dict_n, gtab;
+	uint64_t gtab_bytes = 0;
 	// string columns (fls_sel_plan_create_strings): the plan's columns are the row hashes; these are the strings
 	bool                str = false;
 	std::vector<StrCol> scols;
@@ -1316,16 +1386,22 @@ int wizard_run(fls_sel_plan* p, const std::vector<uint32_t>& subset, uint64_t* d
 			}
 			attr[dev->ordinal] = true;
 		}
+		// one CTA per SM, each with its own bucket scratch for chunks of many distinct values
+		const uint32_t grid = static_cast<uint32_t>(std::min<size_t>(chunks.size(), static_cast<size_t>(dev->sm_count)));
+		if (p->gtab_bytes < kCdGBytes * grid) {
+			if (!p->gtab.alloc(kCdGBytes * grid)) { return FLS_ERR_CUDA; }
+			p->gtab_bytes = kCdGBytes * grid;
+		}
 		ChunkDictArgs a {p->cols_d.as<Col>(), items_d.as<Item>(), ranges_d.as<uint32_t>(),
 		                 static_cast<uint32_t>(chunks.size()), p->dict_n.as<uint32_t>(), p->bw_code.as<uint32_t>(),
-		                 dev->status, nullptr, nullptr, nullptr};
+		                 dev->status, nullptr, nullptr, nullptr, p->gtab.as<uint8_t>()};
 		if (p->str) {
 			const uint32_t* const* wp = p->wptr_d.as<const uint32_t*>();
 			a.w0                      = wp;
 			a.w1                      = wp + p->scols.size();
 			a.dict_w                  = dict_w.as<uint64_t>();
 		}
-		k_chunk_dict<<<static_cast<unsigned>(std::min<size_t>(chunks.size(), 65535)), kCdWarps * 32, kCdSmem, s>>>(a);
+		k_chunk_dict<<<grid, kCdWarps * 32, kCdSmem, s>>>(a);
 		++launch_counter();
 		if (cudaGetLastError() != cudaSuccess) { return FLS_ERR_CUDA; }
 	}

@@ -667,7 +667,10 @@ __device__ __forceinline__ uint32_t dict_vector_out(const uint8_t* rows, const u
 		offs[32 * b + lane] = static_cast<uint32_t>(vbase + o);
 		if (fill + T > kStrWindow) { flush(false); }
 		if (fill + T <= kStrWindow) {
-			put_rows_coop(win32, fill + (o - vpos), reinterpret_cast<const uint32_t*>(dict), fs, fl, lane);
+			uint32_t   hk = 0, head = 0;
+			const bool mid = put_row(win32, fill + (o - vpos), reinterpret_cast<const uint32_t*>(dict), fs, fl, &hk, &head);
+			__syncwarp(); // every word's whole store lands before the rows that start inside it OR in
+			if (mid) { atomicOr(win32 + hk, head); }
 			fill += T;
 		} else {
 			// a batch larger than the window: straight to global memory after the window's pending bytes

@@ -100,54 +100,6 @@ __device__ __forceinline__ bool put_row(uint32_t* __restrict__ win, uint32_t d, 
 	return mid;
 }
 
-// The 32 rows of a batch (lane i: row i, dictionary bytes [fs, fs + fl) of the word array D, window byte d)
-// into the window, 4 rows at a time with 8 lanes per row (lane 8g + j: words j, j + 8, ... of row 4 * step + g).
-// A row's words are consecutive in the dictionary and in the window, so the lanes of a step fall on few banks
-// (a lane per row would read 32 random entries).  The put_row protocol: every window word is stored whole by the
-// row owning its first byte (zeros past the row's end), a row's head word (the one it starts inside) is kept and
-// OR-ed in after a warp sync, once every whole word of the batch is stored.
-__device__ __forceinline__ void put_rows_coop(uint32_t* win, uint32_t d, const uint32_t* D, uint32_t fs, uint32_t fl,
-                                              uint32_t lane) {
-	const uint32_t g = lane >> 3, j0 = lane & 7u;
-	uint32_t       hk[8], hv[8];
-#pragma unroll
-	for (int step = 0; step < 8; ++step) {
-		const uint32_t r  = 4 * step + g;
-		const uint32_t rs = __shfl_sync(0xFFFFFFFFu, fs, r);
-		const uint32_t rl = __shfl_sync(0xFFFFFFFFu, fl, r);
-		const uint32_t rd = __shfl_sync(0xFFFFFFFFu, d, r);
-		hk[step]          = ~0u;
-		hv[step]          = 0;
-		if (rl == 0) { continue; }
-		const uint32_t k0   = rd >> 2, nw = ((rd + rl - 1) >> 2) - k0; // words k0 .. k0 + nw
-		const int32_t  s_lo = static_cast<int32_t>(rs >> 2), s_hi = static_cast<int32_t>((rs + rl - 1) >> 2);
-		const uint32_t hm   = 0xFFFFFFFFu << (8u * (rd & 3u));
-		const uint32_t tm   = 0xFFFFFFFFu >> (8u * (3u - ((rd + rl - 1) & 3u)));
-		for (uint32_t j = j0; j <= nw; j += 8) {
-			// window word k0 + j holds the row's bytes from dictionary byte rs - (rd & 3) + 4j on
-			const int32_t  a  = static_cast<int32_t>(rs) - static_cast<int32_t>(rd & 3u) + 4 * static_cast<int32_t>(j);
-			const int32_t  sw = a >> 2;
-			// a clamped word only feeds bytes outside the row, which the masks drop
-			const uint32_t w0 = D[sw < s_lo ? s_lo : (sw > s_hi ? s_hi : sw)];
-			const uint32_t w1 = D[sw + 1 > s_hi ? s_hi : (sw + 1 < s_lo ? s_lo : sw + 1)];
-			uint32_t       x  = __funnelshift_r(w0, w1, 8u * (static_cast<uint32_t>(a) & 3u));
-			if (j == 0) { x &= hm; }
-			if (j == nw) { x &= tm; }
-			if (j == 0 && (rd & 3u) != 0) {
-				hk[step] = k0;
-				hv[step] = x;
-			} else {
-				win[k0 + j] = x;
-			}
-		}
-	}
-	__syncwarp();
-#pragma unroll
-	for (int step = 0; step < 8; ++step) {
-		if (hk[step] != ~0u) { atomicOr(win + hk[step], hv[step]); }
-	}
-}
-
 // Decode one FSST-compressed string into the word array `win` at byte offset d, whole 32-bit words: the
 // decoded bytes gather in a bit accumulator and leave as word stores, every word stored by the row that owns
 // its first byte, bytes past the row's end zero (the protocol of the string kernels' window).  A row that

@@ -149,7 +149,8 @@ def case_select(a):
     plan.wizard()
     plan.learned(params, 8)
     ms = _timed(lambda: plan.learned(params, 8), a.reps)
-    res = f"select chunks={plan.n_chunks} ms={ms:.4f}"
+    wms = _timed(plan.wizard, a.reps)
+    res = f"select chunks={plan.n_chunks} ms={ms:.4f} wizard_ms={wms:.4f}"
     plan.close()
     return res
 

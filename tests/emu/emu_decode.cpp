@@ -237,33 +237,3 @@ extern "C" uint64_t emu_stream_vector(int fsst, const uint64_t* sym, const uint8
 	*bad_out      = (bad[0] ? 1 : 0) | (bad[1] ? 2 : 0);
 	return tot[1];
 }
-
-// A run of rows copied with put_rows_coop (the DICT materialising pass's batch writer) on an emulated warp,
-// 32 rows per batch: the word the first row starts in is zeroed, then every batch goes in.  Returns the bytes
-// written.
-extern "C" uint64_t emu_put_rows_coop(const uint32_t* base, const uint32_t* start, const uint32_t* len, uint32_t n,
-                                      uint32_t d0, uint32_t* win) {
-	win[d0 >> 2] = 0;
-	uint32_t d   = d0;
-	for (uint32_t b0 = 0; b0 < n; b0 += 32) {
-		uint32_t dd[32], ss[32], ll[32];
-		for (uint32_t i = 0; i < 32; ++i) {
-			ss[i] = b0 + i < n ? start[b0 + i] : 0;
-			ll[i] = b0 + i < n ? len[b0 + i] : 0;
-			dd[i] = d;
-			d += ll[i];
-		}
-		std::barrier<>           bar(32);
-		EmuWarp                  w {&bar, {}, {}};
-		std::vector<std::thread> th;
-		for (int t = 0; t < 32; ++t) {
-			th.emplace_back([&, t] {
-				g_emu_warp = &w;
-				g_emu_lane = t;
-				put_rows_coop(win, dd[t], base, ss[t], ll[t], static_cast<uint32_t>(t));
-			});
-		}
-		for (auto& x : th) { x.join(); }
-	}
-	return d - d0;
-}

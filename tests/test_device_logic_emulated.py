@@ -354,27 +354,3 @@ def test_emulated_stream_decode_refuses_bad_rows(emu, col_golden):
         tot, tot_len, offs, out, bad = _emu_stream(emu, True, sym, ln, ends.astype(np.uint32), comp, 1, 3)
         assert bad == 3 and tot == tot_len == 0
         assert (offs == 3).all()
-
-
-@pytest.mark.parametrize("d0", [0, 1, 2, 3, 5])
-def test_emulated_cooperative_row_copy_window_protocol(emu, d0):
-    """put_rows_coop (the single-pass DICT decode's batch writer: 8 lanes per row) on a window full of garbage:
-    rows of 0..255 bytes from any dictionary offset, in batches of 32, reproduce the source bytes, zeros before d0
-    in the first word and past the end."""
-    rng = np.random.default_rng(300 + d0)
-    src = rng.integers(0, 256, 1 << 14, dtype=np.uint8)
-    n = 32 * 40 + 7
-    lens = rng.choice([0, 1, 2, 3, 4, 5, 7, 9, 31, 33, 40, 255], n,
-                      p=[.15, .1, .1, .1, .1, .1, .05, .05, .05, .05, .1, .05]).astype(np.uint32)
-    starts = rng.integers(0, src.size - 256, n).astype(np.uint32)
-    want = np.concatenate([src[s:s + l] for s, l in zip(starts, lens)])
-    win = rng.integers(0, 1 << 32, (d0 + want.size) // 4 + 64, dtype=np.uint64).astype(np.uint32)
-    emu.emu_put_rows_coop.restype = ctypes.c_uint64
-    got_n = emu.emu_put_rows_coop(P(src.view(np.uint32)), P(starts), P(lens), ctypes.c_uint32(n), ctypes.c_uint32(d0),
-                                  P(win))
-    got = win.view(np.uint8)
-    assert got_n == want.size
-    assert np.array_equal(got[d0:d0 + want.size], want)
-    assert not got[(d0 // 4) * 4:d0].any()
-    end = d0 + want.size
-    assert not got[end:(end + 3) // 4 * 4].any()

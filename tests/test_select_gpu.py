@@ -84,6 +84,58 @@ def test_wizard_sizes_exact(cuda, chunk_vectors):
     plan.close()
 
 
+def _many_distinct_cols():
+    """Full 64-vector chunks around the chunk dictionary's shared-memory capacity (12,288 distinct values):
+    exactly at it and one past it, 13,000 and 40,000 values spread over the chunk, 65,536 distinct full-range
+    values with the all-ones key among them, and a chunk whose second half brings 20,000 new values after a
+    first half of 6,000.  Each column is 84 vectors: a full chunk and a partial one."""
+    import torch
+
+    rng = np.random.default_rng(17)
+    n = 84 * 1024
+
+    def spread(d, dtype):
+        pool = rng.permutation(np.arange(d, dtype=np.int64) * 7919 + 11).astype(dtype)
+        return pool[np.concatenate([np.arange(d), rng.integers(0, d, n - d)])[rng.permutation(n)]]
+
+    full = rng.integers(-2 ** 63, 2 ** 63 - 1, n, dtype=np.int64)
+    full[[5, 4097, 70000]] = -1
+    half = np.concatenate([rng.integers(0, 6000, 32 * 1024), rng.integers(6000, 26000, n - 32 * 1024)])
+    h = [
+        (spread(12288, np.int64), True),
+        (spread(12289, np.int64), False),
+        (spread(13000, np.int32), True),
+        (spread(40000, np.int32), False),
+        (full, True),
+        (half.astype(np.int64), True),
+    ]
+    return [(torch.from_numpy(x).cuda(), s) for x, s in h], h
+
+
+def test_wizard_sizes_exact_for_chunks_of_many_distinct_values(cuda):
+    """64-vector chunks past the shared-memory dictionary's capacity go through the hash buckets: the same exact
+    dictionary sizes, code widths and candidate sizes as the oracle's."""
+    from fastlanes_b200 import select as S
+
+    dcols, hcols = _many_distinct_cols()
+    plan = S.SelectionPlan(dcols, 64)
+    sizes, best, dn = plan.wizard()
+    sizes, best, dn = sizes.cpu().numpy(), best.cpu().numpy(), dn.cpu().numpy()
+    col, first, count = plan.chunks()
+    assert plan.n_chunks == 2 * len(hcols)
+    for c in range(plan.n_chunks):
+        x, sgn = hcols[col[c]]
+        u = _unsigned(x)[int(first[c]) * 1024:(int(first[c]) + int(count[c])) * 1024]
+        want = SEL.chunk_sizes(u, sgn)
+        assert dn[c] == SEL.chunk_dictionary(u)[0], (c, x.dtype, sgn)
+        assert sizes[c].tolist() == want.astype(np.int64).tolist(), (c, x.dtype, sgn)
+        assert best[c] == int(np.argmin(want))
+    from fastlanes_b200 import primitives as P
+
+    assert P.device_status() == 0
+    plan.close()
+
+
 def test_wizard_sizes_equal_encoded_page_sizes(cuda):
     """Candidates 0 / 1 / 2 / 3 are exactly the pages fastlanes.h's encoder writes (ids 0, 1, 6, 11)."""
     from fastlanes_b200 import pages as PG

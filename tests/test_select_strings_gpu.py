@@ -20,17 +20,49 @@ def _plan(cuda, byts, offs, table):
     return SL.StrSelectionPlan([(b, o, np.asarray(table, np.uint8))], 64), (b, o)
 
 
-@pytest.mark.parametrize("eid", [0, 3, 13, 15])
+def _distinct_first_occurrence(byts, offs):
+    rows = [bytes(byts[int(offs[i]):int(offs[i + 1])]) for i in range(offs.size - 1)]
+    seen, dist = {}, []
+    for r in rows:
+        if r not in seen:
+            seen[r] = len(dist)
+            dist.append(r)
+    d_offs = np.zeros(len(dist) + 1, np.uint64)
+    d_offs[1:] = np.cumsum([len(x) for x in dist])
+    return np.frombuffer(b"".join(dist), np.uint8).copy(), d_offs, np.array([seen[r] for r in rows], np.uint32)
+
+
+@pytest.mark.parametrize("eid", [0, 13])
 def test_string_wizard_size_is_the_reference_page_size(cuda, col_golden, eid):
+    """BYTE_ARR and FSST: the size of the reference's page (and, for FSST, its exported table) for the same
+    rows, with the reference's own symbol table."""
     byts, offs = col_golden[f"str_{eid}_input_bytes"], col_golden[f"str_{eid}_input_offsets"]
     page, dic = col_golden[f"str_{eid}_page"], col_golden[f"str_{eid}_dict"]
-    # the symbol table the reference's pages use (BYTE_ARR has none: its size does not depend on one)
-    table = dic[8:] if dic.size else col_golden["str_13_dict"][8:]
+    table = dic[8:] if dic.size else col_golden["str_13_dict"][8:]  # BYTE_ARR's size needs no table
     plan, keep = _plan(cuda, byts, offs, table)
     sizes, best, dn = plan.wizard()
     plan.close()
     assert int(sizes[0, CAND[eid]].item()) == page.size + dic.size
     assert int(sizes[0, 4].item()) == -1 and int(sizes[0, 5].item()) == -1  # UINT64_MAX: no such candidate
+
+
+@pytest.mark.parametrize("eid", [3, 15])
+def test_string_wizard_dictionary_sizes(cuda, col_golden, eid):
+    """DICT and DICT_RLE: the codes page as the reference writes it for the same rows, plus the dictionary page
+    with every entry's true compressed length, as this engine's encoder writes it (the reference's encoder
+    compresses entry i with the length of entry i - 1, so its dictionary pages hold other bytes)."""
+    from fastlanes_b200 import strings as S
+
+    byts, offs = col_golden[f"str_{eid}_input_bytes"], col_golden[f"str_{eid}_input_offsets"]
+    page = col_golden[f"str_{eid}_page"]
+    dbytes, doffs, codes = _distinct_first_occurrence(byts, offs)
+    table, _, _ = S.fsst_compress(dbytes, doffs)
+    _, own_dict = S.encode_string_dict(dbytes, doffs, codes)
+    plan, keep = _plan(cuda, byts, offs, table)
+    sizes, best, dn = plan.wizard()
+    plan.close()
+    assert int(dn[0].item()) == doffs.size - 1
+    assert int(sizes[0, CAND[eid]].item()) == page.size + own_dict.size
 
 
 def test_string_wizard_picks_the_family_winner_and_the_learned_selector_agrees(cuda):
