@@ -161,6 +161,8 @@ struct fls_string_plan {
 	DevArr<uint64_t>         lb;       // ticket + one look-back word per vector, zeroed before every decode
 	int                      sp_warps = 0;
 	uint32_t                 sp_smem  = 0, sp_dict_cap = 0, sp_tab_cap = 0;
+	// single-pass FSST / BYTE_ARR decode (k_stream_single), look-back words in lb
+	bool                     stream_single = false;
 	// a measure() whose per-vector totals and bases the next decode() takes over (the usual measure, allocate,
 	// decode sequence runs the lengths pass once)
 	mutable bool             measured = false;
@@ -351,6 +353,10 @@ int fls_string_plan_create(const uint8_t* d_page, uint64_t page_size, const uint
 			return FLS_ERR_CUDA;
 		}
 	}
+	if ((a.kind == STR_FSST || a.kind == STR_BYTES) && pi.vec_c > 0) {
+		p->stream_single = true;
+		if (!p->lb.alloc(1ull + pi.vec_c)) { return FLS_ERR_CUDA; }
+	}
 	*out                    = p.release();
 	return FLS_OK;
 }
@@ -411,6 +417,16 @@ int fls_string_plan_decode(const fls_string_plan* p, uint32_t* d_offsets, uint8_
 	if (p->single) {
 		p->measured = false;
 		return single_pass_decode(p, d_offsets, d_bytes, bytes_cap, s);
+	}
+	if (p->stream_single) {
+		// one memset of the look-back words and one launch
+		p->measured = false;
+		StrArgs a   = p->args;
+		a.offsets   = d_offsets;
+		a.bytes     = d_bytes;
+		a.bytes_cap = bytes_cap;
+		if (cudaMemsetAsync(p->lb.p, 0, 8ull * (1 + a.col.n_vec), s) != cudaSuccess) { return FLS_ERR_CUDA; }
+		return launch_stream_single(a, p->lb.p, s) == cudaSuccess ? FLS_OK : FLS_ERR_CUDA;
 	}
 	// the totals of a measure() just before (complete: measure synchronised its stream) are still valid; a
 	// decode captured into a graph always computes its own (each replay must)

@@ -119,6 +119,9 @@ constexpr uint32_t kStrWindow  = 2048;
 
 enum : int { STR_PASS_LENGTHS = 0, STR_PASS_MATERIALIZE = 1 };
 
+// per-warp shared memory of the single-pass FSST / BYTE_ARR kernel: rows, then the window (no plan ring)
+constexpr uint32_t kStreamSinglePerWarp = kStrRows + kStrWindow;
+
 __host__ __device__ constexpr uint32_t str_rows_bytes(bool r16) { return r16 ? kStrRows16 : kStrRows; }
 
 __host__ __device__ constexpr uint32_t str_per_warp(int pass, bool r16) {
@@ -477,9 +480,10 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_stream_pass(const StrArgs
 	const uint32_t      lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
 	constexpr uint32_t  kPerWarp = str_per_warp(PASS, false);
 	if constexpr (kFsst) {
+		// code 255 (the escape) keeps an empty entry: stream_vector reads bytes past a stream's end as code 255
 		for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) {
-			fsym[i] = a.table->sym[i];
-			flen[i] = a.table->len[i];
+			fsym[i] = i == 255 ? 0ull : a.table->sym[i];
+			flen[i] = i == 255 ? 0u : a.table->len[i];
 		}
 	}
 	uint8_t*        wbase  = smem + warp * kPerWarp;
@@ -771,6 +775,79 @@ __global__ void __launch_bounds__(kStrMaxWarps * 32) k_dict_pass(const StrSetArg
 	}
 }
 
+// Single-pass FSST / BYTE_ARR decode (no lengths pass, no scan).  A warp takes vectors by ticket (lb[0]), in
+// vector order, so every vector it waits for was taken by a running warp that publishes without waiting.  Per
+// vector: its rows; its decoded total -- the sum of its codes' symbol lengths when no escape is among its bytes,
+// else the escape-aware walk of stream_vector (a BYTE_ARR vector's total is its compressed length) -- published
+// in its look-back word lb[1 + v]; its first output byte from the earlier vectors' words (lookback); then its
+// offsets and bytes (stream_vector), whose total must match.
+template <int KIND>
+__global__ void __launch_bounds__(kStrMaxWarps * 32) k_stream_single(const StrArgs a, uint64_t* lb) {
+	extern __shared__ __align__(128) uint8_t smem[];
+	constexpr bool      kFsst = KIND == STR_FSST;
+	__shared__ uint64_t fsym[kFsst ? 256 : 1];
+	__shared__ uint8_t  flen[kFsst ? 256 : 1];
+	const uint32_t      lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+	if constexpr (kFsst) {
+		// code 255 (the escape) keeps an empty entry: stream_vector reads bytes past a stream's end as code 255
+		for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) {
+			fsym[i] = i == 255 ? 0ull : a.table->sym[i];
+			flen[i] = i == 255 ? 0u : a.table->len[i];
+		}
+	}
+	uint8_t*        buf    = smem + warp * kStreamSinglePerWarp;
+	const uint32_t* rows32 = reinterpret_cast<const uint32_t*>(buf);
+	uint8_t*        win    = buf + kStrRows;
+	__syncthreads();
+	const uint64_t n     = a.col.n_vec;
+	uint64_t*      words = lb + 1;
+	for (;;) {
+		unsigned long long t = 0;
+		if (lane == 0) { t = atomicAdd(reinterpret_cast<unsigned long long*>(lb), 1ull); }
+		const uint64_t v = __shfl_sync(0xFFFFFFFFu, t, 0);
+		if (v >= n) { break; }
+		const Plan     p  = make_plan(a.col, static_cast<uint32_t>(v));
+		uint32_t       vn = 0;
+		const uint8_t* vb = vector_bytes(a.col, static_cast<uint32_t>(v), &vn);
+		if (lane == 0) {
+			// the vector's bytes towards L2 while its rows decode (the 16-byte aligned part inside them)
+			const uintptr_t lo = (reinterpret_cast<uintptr_t>(vb) + 15) & ~uintptr_t(15);
+			const uintptr_t hi = (reinterpret_cast<uintptr_t>(vb) + vn) & ~uintptr_t(15);
+			if (hi > lo) { bulk_prefetch_l2(reinterpret_cast<const void*>(lo), static_cast<uint32_t>(hi - lo)); }
+		}
+		const bool ok  = p.ok;
+		bool       bad = false;
+		if (!ok && lane == 0) { atomicOr(a.status, p.bw > p.ws ? STATUS_BAD_BW : STATUS_BAD_LAYOUT); }
+		uint32_t T = 0;
+		if (ok) {
+			load_rows<false>(p, buf, lane, a.status);
+			const uint32_t L = stream_rows_length(rows32, vn, lane, &bad);
+			T                = L;
+			if (kFsst && !fsst_plain_total(vb, L, flen, lane, &T)) {
+				StreamOut o {};
+				T = stream_vector<false, true, kStrWindow>(rows32, vb, vn, fsym, flen, lane, o, &bad);
+			}
+		}
+		// every vector publishes (also one that failed: its successors wait for it)
+		if (lane == 0) { st_release_u64(words + v, (v == 0 ? kLbInc : kLbAgg) | T); }
+		const uint64_t P = v == 0 ? 0ull : lookback(words, static_cast<uint32_t>(v), lane, a.status);
+		if (lane == 0 && v > 0) { st_release_u64(words + v, kLbInc | (P + T)); }
+		uint32_t* offs = a.offsets + v * kVec;
+		if (P + T > a.bytes_cap || P + T >= (1ull << 32)) {
+			if (lane == 0) { atomicOr(a.status, STATUS_BAD_LAYOUT); }
+		} else if (!ok) {
+			for (uint32_t r = lane; r < kVec; r += 32) { offs[r] = static_cast<uint32_t>(P); }
+		} else {
+			StreamOut o {offs, a.bytes, P, win};
+			const uint32_t got = stream_vector<true, kFsst, kStrWindow>(rows32, vb, vn, fsym, flen, lane, o, &bad);
+			if (got != T) { bad = true; }
+		}
+		if (lane == 0 && v + 1 == n) { a.offsets[n * kVec] = static_cast<uint32_t>(P + T); }
+		if (__any_sync(0xFFFFFFFFu, bad) && lane == 0) { atomicOr(a.status, STATUS_BAD_INDEX); }
+		__syncwarp();
+	}
+}
+
 __global__ void __launch_bounds__(1024) k_scan_totals(const uint64_t* total, uint64_t* base, uint64_t n) {
 	__shared__ uint64_t wt[33];
 	uint64_t            carry = 0;
@@ -906,6 +983,43 @@ cudaError_t launch_dict_pass(const StrSetArgs& a, bool rows16, int warps, uint32
 	}
 	return sm ? launch_dict_pass_t<false, true>(a, warps, dyn_smem, s, sm_count)
 	          : launch_dict_pass_t<false, false>(a, warps, dyn_smem, s, sm_count);
+}
+
+template <int KIND>
+static cudaError_t launch_stream_single_t(const StrArgs& a, uint64_t* lb, cudaStream_t s, int sm_count) {
+	auto* const        fn    = k_stream_single<KIND>;
+	constexpr int      warps = kStrMaxWarps;
+	constexpr uint32_t smem  = warps * kStreamSinglePerWarp;
+	static std::mutex  mu;
+	static bool        set = false;
+	{
+		std::lock_guard<std::mutex> lk(mu);
+		if (!set) {
+			const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+			if (e != cudaSuccess) { return e; }
+			set = true;
+		}
+	}
+	if (sm_count <= 0) {
+		const Device* dev = current_device();
+		if (!dev) { return cudaErrorUnknown; }
+		sm_count = dev->sm_count;
+	}
+	// one CTA per SM (its 32 warps take vectors by ticket); no more warps than vectors
+	const uint64_t need = (static_cast<uint64_t>(a.col.n_vec) + warps - 1) / warps;
+	const uint64_t grid = need < static_cast<uint64_t>(sm_count) ? need : static_cast<uint64_t>(sm_count);
+	if (grid == 0) { return cudaSuccess; }
+	fn<<<static_cast<unsigned>(grid), warps * 32, smem, s>>>(a, lb);
+	++launch_counter();
+	return cudaGetLastError();
+}
+
+cudaError_t launch_stream_single(const StrArgs& a, uint64_t* lb, cudaStream_t s, int sm_count) {
+	switch (a.kind) {
+	case STR_FSST: return launch_stream_single_t<STR_FSST>(a, lb, s, sm_count);
+	case STR_BYTES: return launch_stream_single_t<STR_BYTES>(a, lb, s, sm_count);
+	default: return cudaErrorInvalidValue;
+	}
 }
 
 cudaError_t launch_scan_totals(const uint64_t* total, uint64_t* base, uint64_t n, cudaStream_t s) {

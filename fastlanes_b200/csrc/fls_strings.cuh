@@ -270,48 +270,125 @@ __device__ __forceinline__ void stream_row_mask(const uint32_t* rows32, uint32_t
 	*rc = r;
 }
 
-// A lane's decoded bytes -- up to 4 symbols (value, length; length 0 = nothing) in order -- into the word
-// window at byte d, whole words: every word is stored by the lane owning its first byte, bytes past the lane's
-// end zero; a lane starting inside a word returns its bytes of that word (*hk, *head) for an atomic OR after a
-// warp sync (the protocol of put_row).  Returns whether such a head is left.
+// A lane's decoded bytes -- up to 4 symbols (value, length; length 0 = nothing, its value then 0) in order --
+// into the word window at byte d, whole words: every word is stored by the lane owning its first byte, bytes
+// past the lane's end zero; a lane starting inside a word returns its bytes of that word (*hk, *head) for an
+// atomic OR after a warp sync (the protocol of put_row).  Returns whether such a head is left.
+// The bytes gather in a 128-bit accumulator a0..a3 (word k at a0) holding nb < 64 bits before every symbol, so
+// a symbol (at most 64 bits) leaves at most one pair of whole words behind it: one predicated two-word emit
+// per symbol, and no branch on where a word goes.
 __device__ __forceinline__ bool put_syms(uint32_t* win, uint32_t d, const uint64_t (&sv)[4], const uint32_t (&sl)[4],
                                          uint32_t* hk, uint32_t* head) {
-	const uint32_t k0   = d >> 2;
-	const bool     mid  = (d & 3u) != 0;
-	uint32_t       k    = k0;
-	uint32_t       nb   = 8u * (d & 3u); // bits of word k already placed (< 32 before every symbol)
-	uint32_t       a0 = 0, a1 = 0, a2 = 0; // words k, k + 1, k + 2 being built
-	bool           any  = false, held = false;
-	auto           emit = [&]() {
-        if (k == k0 && mid) {
-            *hk   = k;
-            *head = a0;
-            held  = true;
-        } else {
-            win[k] = a0;
-        }
-        ++k;
-        a0 = a1;
-        a1 = a2;
-        a2 = 0;
-        nb -= 32u;
+	const uint32_t k0  = d >> 2;
+	const bool     mid = (d & 3u) != 0;
+	uint32_t       k   = k0;
+	uint32_t       nb  = 8u * (d & 3u);
+	uint32_t       a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+	uint32_t       hv   = 0;
+	bool           held = false;
+	// words k, k + 1 leave: the first word of a lane that starts inside it is its head instead
+	auto emit2 = [&]() {
+		const bool h = mid && k == k0;
+		if (!h) { win[k] = a0; }
+		win[k + 1] = a1;
+		hv         = h ? a0 : hv;
+		held       = held || h;
 	};
 #pragma unroll
 	for (int j = 0; j < 4; ++j) {
-		const uint32_t l = sl[j];
-		if (l == 0) { continue; }
-		any               = true;
 		const uint32_t lo = static_cast<uint32_t>(sv[j]), hi = static_cast<uint32_t>(sv[j] >> 32);
-		// the symbol's up to 64 bits at bit nb of the 96-bit accumulator a0:a1:a2
-		a0 |= lo << nb;
-		a1 |= __funnelshift_l(lo, hi, nb);
-		a2 |= nb ? (hi >> (32u - nb)) : 0u;
-		nb += 8u * l;
-		if (nb >= 32u) { emit(); }
-		if (nb >= 32u) { emit(); } // a symbol adds at most 64 bits: two words at most
+		const uint32_t sh = nb & 31u;
+		const uint32_t t0 = lo << sh;
+		const uint32_t t1 = __funnelshift_l(lo, hi, sh);
+		const uint32_t t2 = __funnelshift_l(hi, 0u, sh); // hi >> (32 - sh), 0 for sh = 0
+		const bool     lw = nb < 32u;
+		a0 |= lw ? t0 : 0u;
+		a1 |= lw ? t1 : t0;
+		a2 |= lw ? t2 : t1;
+		a3 |= lw ? 0u : t2;
+		nb += 8u * sl[j];
+		if (nb >= 64u) {
+			emit2();
+			a0 = a2;
+			a1 = a3;
+			a2 = 0;
+			a3 = 0;
+			k += 2;
+			nb -= 64u;
+		}
 	}
-	if (any && nb > 8u * ((k == k0) ? (d & 3u) : 0u)) { emit(); }
+	// what is left: bits [0, nb) of a0, a1 (nb > 8 * (d & 3) when the lane wrote nothing yet and has bytes)
+	const bool any = (sl[0] | sl[1] | sl[2] | sl[3]) != 0;
+	if (any && nb > 0u) {
+		const bool h = mid && k == k0;
+		if (!h) { win[k] = a0; }
+		hv   = h ? a0 : hv;
+		held = held || h;
+		if (nb > 32u) { win[k + 1] = a1; }
+	}
+	*hk   = k0;
+	*head = hv;
 	return held;
+}
+
+// Compressed length of a vector's rows (rows32: its 1024 cumulative row end offsets, row r at word r + r / 32;
+// vn: its compressed bytes): the last row's end.  *bad, and length 0, when the rows are not non-decreasing or
+// end past vn.
+__device__ __forceinline__ uint32_t stream_rows_length(const uint32_t* rows32, uint32_t vn, uint32_t lane, bool* bad) {
+	uint32_t prev = lane == 0 ? 0u : rows32[(32 * lane - 1) + lane - 1];
+	bool     b    = false;
+#pragma unroll 8
+	for (uint32_t i = 0; i < 32; ++i) {
+		const uint32_t e = rows32[32 * lane + i + lane];
+		b |= e < prev;
+		prev = e;
+	}
+	b |= lane == 31 && prev > vn;
+	*bad = __any_sync(0xFFFFFFFFu, b);
+	return *bad ? 0u : rows32[kVec - 1 + (kVec - 1) / 32];
+}
+
+// Decoded byte total of an FSST vector's compressed bytes [0, L) when none of them is an escape (255): every
+// byte is then a code and the total is the sum of their symbol lengths (len: the symbol lengths, code 255's 0).
+// Returns false when a byte 255 may be among them -- the escape-aware walk (stream_vector) decides then; the
+// zero-byte test can also fire on a byte 254 just above a 255 outside the range, which costs only that walk.
+__device__ __forceinline__ bool fsst_plain_total(const uint8_t* vb, uint32_t L, const uint8_t* len, uint32_t lane,
+                                                 uint32_t* total) {
+	const uintptr_t va   = reinterpret_cast<uintptr_t>(vb);
+	const uint32_t  off  = static_cast<uint32_t>(va & 3u);
+	const uint32_t* base = reinterpret_cast<const uint32_t*>(va - off);
+	const uint32_t  nw   = (off + L + 3u) >> 2; // words holding a byte of [0, L)
+	uint32_t        sum = 0, esc = 0;
+	// 8 words per lane in flight per round: the walk is one read of the bytes, bound by load latency otherwise
+	constexpr uint32_t kU = 8;
+	for (uint32_t q0 = lane; q0 < nw; q0 += 32 * kU) {
+		uint32_t w[kU];
+#pragma unroll
+		for (uint32_t u = 0; u < kU; ++u) { w[u] = q0 + 32 * u < nw ? __ldg(base + q0 + 32 * u) : 0u; }
+#pragma unroll
+		for (uint32_t u = 0; u < kU; ++u) {
+			const uint32_t q = q0 + 32 * u;
+			if (q >= nw) { break; }
+			const int64_t p0 = 4ll * q - off; // stream position of the word's byte 0
+			uint32_t      vm;                 // 0x80 in every byte inside [0, L)
+			if (p0 >= 0 && p0 + 4 <= static_cast<int64_t>(L)) {
+				sum += len[w[u] & 0xFFu] + len[(w[u] >> 8) & 0xFFu] + len[(w[u] >> 16) & 0xFFu] + len[w[u] >> 24];
+				vm = 0x80808080u;
+			} else {
+				vm = 0;
+#pragma unroll
+				for (uint32_t j = 0; j < 4; ++j) {
+					const bool in = p0 + j >= 0 && p0 + j < static_cast<int64_t>(L);
+					sum += in ? len[(w[u] >> (8 * j)) & 0xFFu] : 0u;
+					vm |= in ? 0x80u << (8 * j) : 0u;
+				}
+			}
+			const uint32_t x = ~w[u]; // escape bytes turn into zero bytes
+			esc |= (x - 0x01010101u) & ~x & vm;
+		}
+	}
+	*total = warp_sum(sum);
+	return !__any_sync(0xFFFFFFFFu, esc != 0);
 }
 
 // Per-vector output of the materialising pass.
@@ -330,20 +407,7 @@ template <bool MAT, bool KIND_FSST, uint32_t kWindow>
 __device__ __forceinline__ uint32_t stream_vector(const uint32_t* rows32, const uint8_t* vb, uint32_t vn,
                                                   const uint64_t* sym, const uint8_t* len, uint32_t lane,
                                                   const StreamOut& o, bool* bad) {
-	// rows must be non-decreasing and end inside the vector's bytes
-	{
-		uint32_t prev = lane == 0 ? 0u : rows32[(32 * lane - 1) + lane - 1];
-		bool     b    = false;
-#pragma unroll 8
-		for (uint32_t i = 0; i < 32; ++i) {
-			const uint32_t e = rows32[32 * lane + i + lane];
-			b |= e < prev;
-			prev = e;
-		}
-		b |= lane == 31 && prev > vn;
-		*bad = __any_sync(0xFFFFFFFFu, b);
-	}
-	const uint32_t  L     = *bad ? 0u : rows32[kVec - 1 + (kVec - 1) / 32];
+	const uint32_t  L     = stream_rows_length(rows32, vn, lane, bad);
 	if constexpr (!KIND_FSST && !MAT) { return L; } // a plain-bytes vector decodes to its own bytes
 	const uintptr_t va    = reinterpret_cast<uintptr_t>(vb);
 	const uint32_t  off   = static_cast<uint32_t>(va & 3u);
@@ -415,7 +479,7 @@ __device__ __forceinline__ uint32_t stream_vector(const uint32_t* rows32, const 
 		if constexpr (!KIND_FSST) {
 #pragma unroll
 			for (uint32_t j = 0; j < 4; ++j) {
-				sv[j] = (b4 >> (8 * j)) & 0xFFu;
+				sv[j] = j < nv ? (b4 >> (8 * j)) & 0xFFu : 0u;
 				sl[j] = j < nv ? 1u : 0u;
 			}
 		} else {
@@ -426,9 +490,10 @@ __device__ __forceinline__ uint32_t stream_vector(const uint32_t* rows32, const 
 				// no escape anywhere in the chunk: every byte starts a code
 #pragma unroll
 				for (uint32_t j = 0; j < 4; ++j) {
-					const uint32_t c = (b4 >> (8 * j)) & 0xFFu;
+					// a byte past the stream's end reads as code 255, whose table entry is empty (symbol 0, length 0)
+					const uint32_t c = j < nv ? (b4 >> (8 * j)) & 0xFFu : 255u;
 					sv[j]            = sym[c];
-					sl[j]            = j < nv ? len[c] : 0u;
+					sl[j]            = len[c];
 				}
 			} else {
 				uint32_t m[4];

@@ -92,6 +92,9 @@ cudaError_t launch_fsst_dict(const uint8_t* lens, const uint8_t* comp, uint64_t 
                              cudaStream_t s);
 // sm_count: the device's SM count, or 0 to take it from the library's per-device state (current_device())
 cudaError_t launch_str_lengths(const StrArgs& a, int sm_count, cudaStream_t s);
+// Single-pass FSST / BYTE_ARR decode (k_stream_single): lb = a ticket word then one zeroed look-back word per
+// vector; writes a.offsets / a.bytes (capacity a.bytes_cap).
+cudaError_t launch_stream_single(const StrArgs& a, uint64_t* lb, cudaStream_t s, int sm_count = 0);
 cudaError_t launch_scan_totals(const uint64_t* total, uint64_t* base, uint64_t n, cudaStream_t s);
 // warps: warps per CTA (at most kStrMaxWarps); dyn_smem: warps * str_smem_per_warp(a.rows16) plus the
 // 16-byte rounded dictionary bytes when a.dict_in_smem

@@ -202,6 +202,17 @@ extern "C" uint64_t emu_stream_vector(int fsst, const uint64_t* sym, const uint8
                                       uint64_t* len_total, int* bad_out) {
 	std::vector<uint32_t> rows(kVec + kVec / 32 + 32, 0);
 	for (uint32_t r = 0; r < kVec; ++r) { rows[r + r / 32] = ends[r]; }
+	// the kernel's shared copy of the table: code 255 (the escape) with an empty entry
+	std::vector<uint64_t> tsym(256, 0);
+	std::vector<uint8_t>  tlen(256, 0);
+	if (fsst) {
+		for (int c = 0; c < 255; ++c) {
+			tsym[c] = sym[c];
+			tlen[c] = len[c];
+		}
+	}
+	sym = tsym.data();
+	len = tlen.data();
 	std::vector<uint8_t> win_buf(2048 + 64, 0xA5);
 	uint8_t*             win = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(win_buf.data()) + 15) & ~uintptr_t(15));
 	uint64_t             tot[2] = {0, 0};
@@ -236,4 +247,32 @@ extern "C" uint64_t emu_stream_vector(int fsst, const uint64_t* sym, const uint8
 	*len_total    = tot[0];
 	*bad_out      = (bad[0] ? 1 : 0) | (bad[1] ? 2 : 0);
 	return tot[1];
+}
+
+// fsst_plain_total (fls_strings.cuh) on an emulated warp: the bytes [0, L) at vb (any alignment), len the 256
+// symbol lengths (code 255's taken as 0, as the kernels' shared copy has it).  Returns 1 when the function
+// reports no escape (then *total is its sum), 0 otherwise.
+extern "C" int emu_fsst_plain_total(const uint8_t* len, const uint8_t* vb, uint32_t L, uint32_t* total) {
+	std::vector<uint8_t> tlen(256, 0);
+	for (int c = 0; c < 255; ++c) { tlen[c] = len[c]; }
+	std::barrier<>           bar(32);
+	EmuWarp                  w {&bar, {}, {}};
+	std::vector<std::thread> th;
+	int                      plain = 0;
+	uint32_t                 tot   = 0;
+	for (int t = 0; t < 32; ++t) {
+		th.emplace_back([&, t] {
+			g_emu_warp = &w;
+			g_emu_lane = t;
+			uint32_t   x  = 0;
+			const bool ok = fsst_plain_total(vb, L, tlen.data(), t, &x);
+			if (t == 0) {
+				plain = ok ? 1 : 0;
+				tot   = x;
+			}
+		});
+	}
+	for (auto& x : th) { x.join(); }
+	*total = tot;
+	return plain;
 }

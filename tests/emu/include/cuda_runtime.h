@@ -77,6 +77,14 @@ T __shfl_down_sync(unsigned, T v, unsigned d) {
 	__syncwarp();
 	return r;
 }
+template <class T>
+T __shfl_xor_sync(unsigned, T v, int m) {
+	g_emu_warp->xch[g_emu_lane] = static_cast<uint64_t>(v);
+	__syncwarp();
+	const T r = static_cast<T>(g_emu_warp->xch[(g_emu_lane ^ m) & 31]);
+	__syncwarp();
+	return r;
+}
 inline unsigned __reduce_or_sync(unsigned, unsigned v) {
 	g_emu_warp->xch[g_emu_lane] = v;
 	__syncwarp();

@@ -354,3 +354,40 @@ def test_emulated_stream_decode_refuses_bad_rows(emu, col_golden):
         tot, tot_len, offs, out, bad = _emu_stream(emu, True, sym, ln, ends.astype(np.uint32), comp, 1, 3)
         assert bad == 3 and tot == tot_len == 0
         assert (offs == 3).all()
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_emulated_fsst_plain_total(emu, col_golden, seed):
+    """The single-pass FSST kernel's total of a vector without escapes (fsst_plain_total): the sum of its codes'
+    symbol lengths, at every source alignment and length (empty, shorter than a word, ragged ends); any escape
+    inside [0, L) is reported, and so is nothing outside it except the documented false alarm (a 254 right above
+    an out-of-range 255 in the same word), which is always on the safe side."""
+    dic = col_golden["str_13_dict"]
+    _, sym, ln = oracle.fsst_decode_table(dic[8:])
+    lens = np.asarray(ln, np.int64).copy()
+    lens[255] = 0
+    rng = np.random.default_rng(77 + seed)
+    for L in [0, 1, 2, 3, 4, 5, 7, 127, 128, 129, 1000, 4099, int(rng.integers(1, 20000))]:
+        for shift in range(4):
+            buf = _aligned(L + 16, 0)
+            # the bytes around the range: 255 everywhere outside (the worst case for the zero-byte test)
+            buf[:] = 255
+            body = rng.integers(0, 255, L, dtype=np.uint8)  # no escape
+            buf[shift:shift + L] = body
+            tot = ctypes.c_uint32()
+            plain = emu.emu_fsst_plain_total(P(np.ascontiguousarray(ln, np.uint8)), ctypes.c_void_p(buf.ctypes.data + shift),
+                                             ctypes.c_uint32(L), ctypes.byref(tot))
+            # a false alarm needs a 254 as the range's first byte (right above the 255 before it)
+            false_alarm_possible = L > 0 and shift > 0 and body[0] == 254
+            if not false_alarm_possible:
+                assert plain == 1, (L, shift)
+            if plain:
+                assert tot.value == int(lens[body].sum()), (L, shift)
+            if L:
+                # one escape anywhere inside the range is always seen
+                pos = int(rng.integers(0, L))
+                buf[shift + pos] = 255
+                plain = emu.emu_fsst_plain_total(P(np.ascontiguousarray(ln, np.uint8)),
+                                                 ctypes.c_void_p(buf.ctypes.data + shift), ctypes.c_uint32(L),
+                                                 ctypes.byref(tot))
+                assert plain == 0, (L, shift, pos)
