@@ -778,17 +778,35 @@ __device__ __forceinline__ uint64_t str_load8(const StrCol& c, uint64_t p) {
 	return (static_cast<uint64_t>(hi) << 32) | lo;
 }
 
-// warp per item: hash, length and compressed length of the vector's 1024 rows; the vector's sums
+// Block per item: hash and length of each of the vector's 1024 rows, and the compressed length of every rs-th
+// row (rs = 1: every row, the exact figure the wizard's sizes need; rs > 1, the learned selector's features:
+// the other rows' compressed lengths are written as 0 and the vector's sum is scaled by rs).  The column's
+// symbol table is copied to shared memory for the greedy match; the vector's sums (vlen, vclen) by a block
+// reduction.
 __global__ void __launch_bounds__(kWarps * 32) k_str_rows(const StrCol* cols, const Item* items, uint64_t n_items,
-                                                          uint64_t* vlen, uint64_t* vclen) {
-	const uint32_t lane = threadIdx.x & 31u;
-	for (uint64_t it = blockIdx.x * static_cast<uint64_t>(kWarps) + (threadIdx.x >> 5); it < n_items;
-	     it += static_cast<uint64_t>(gridDim.x) * kWarps) {
+                                                          uint64_t* vlen, uint64_t* vclen, uint32_t rs) {
+	__shared__ uint64_t t_val[256];
+	__shared__ uint8_t  t_len[256];
+	__shared__ uint16_t t_start[257];
+	__shared__ uint64_t red[2][kWarps];
+	constexpr uint32_t  nt   = kWarps * 32;
+	const uint32_t      tid  = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+	for (uint64_t it = blockIdx.x; it < n_items; it += gridDim.x) {
 		const Item   m = items[it];
 		const StrCol c = cols[m.col];
-		uint64_t     sl = 0, sc = 0;
-		for (uint32_t i = 0; i < 32; ++i) {
-			const uint64_t r = static_cast<uint64_t>(m.vec) * 1024 + lane + 32 * i;
+		__syncthreads(); // the previous item's table reads and sums are done
+		for (uint32_t k = tid; k < 257; k += nt) {
+			if (k < 256) {
+				t_val[k] = c.tab->val[k];
+				t_len[k] = c.tab->len[k];
+			}
+			t_start[k] = c.tab->start[k];
+		}
+		__syncthreads();
+		const uint64_t r0 = static_cast<uint64_t>(m.vec) * 1024;
+		uint64_t       sl = 0, sc = 0;
+		for (uint32_t j = tid; j < 1024; j += nt) {
+			const uint64_t r = r0 + j;
 			const uint64_t s = c.offsets[r], e = c.offsets[r + 1];
 			const uint64_t n = e >= s ? e - s : 0;
 			uint64_t       h = 0x243F6A8885A308D3ull ^ n;
@@ -797,15 +815,25 @@ __global__ void __launch_bounds__(kWarps * 32) k_str_rows(const StrCol* cols, co
 				const uint64_t k = n - p >= 8 ? x : (x & ((1ull << (8 * (n - p))) - 1));
 				h                = str_mix(h ^ k) + 0x9E3779B97F4A7C15ull;
 			}
-			uint64_t cl = 0;
+			c.hash[r] = h;
+			c.len[r]  = static_cast<uint32_t>(n);
+			if (j % rs != 0) { c.clen[r] = 0; }
+			sl += n;
+		}
+		// compressed lengths: rows rs * (tid + nt * i), spread over every thread
+		for (uint32_t j = rs * tid; j < 1024; j += rs * nt) {
+			const uint64_t r = r0 + j;
+			const uint64_t s = c.offsets[r], e = c.offsets[r + 1];
+			const uint64_t n = e >= s ? e - s : 0;
+			uint64_t       cl = 0;
 			for (uint64_t p = 0; p < n;) {
 				const uint64_t x    = str_load8(c, s + p);
 				const uint32_t b    = static_cast<uint32_t>(x & 0xFFu);
 				const uint64_t left = n - p;
 				uint32_t       step = 0;
-				for (uint32_t k = c.tab->start[b]; k < c.tab->start[b + 1]; ++k) {
-					const uint32_t l = c.tab->len[k];
-					if (l <= left && (l == 8 ? x : (x & ((1ull << (8 * l)) - 1))) == c.tab->val[k]) {
+				for (uint32_t k = t_start[b]; k < t_start[b + 1]; ++k) {
+					const uint32_t l = t_len[k];
+					if (l <= left && (l == 8 ? x : (x & ((1ull << (8 * l)) - 1))) == t_val[k]) {
 						step = l;
 						break;
 					}
@@ -813,25 +841,40 @@ __global__ void __launch_bounds__(kWarps * 32) k_str_rows(const StrCol* cols, co
 				cl += step ? 1 : 2;
 				p += step ? step : 1;
 			}
-			c.hash[r] = h;
-			c.len[r]  = static_cast<uint32_t>(n);
 			c.clen[r] = static_cast<uint32_t>(cl);
-			sl += n;
 			sc += cl;
 		}
 		sl = warp_sum(sl);
 		sc = warp_sum(sc);
 		if (lane == 0) {
-			if (vlen) { vlen[it] = sl; }
-			if (vclen) { vclen[it] = sc; }
+			red[0][warp] = sl;
+			red[1][warp] = sc;
+		}
+		__syncthreads();
+		if (tid == 0) {
+			uint64_t a = 0, b = 0;
+			for (int w = 0; w < kWarps; ++w) {
+				a += red[0][w];
+				b += red[1][w];
+			}
+			if (vlen) { vlen[it] = a; }
+			if (vclen) { vclen[it] = b * rs; }
 		}
 	}
+}
+
+// blocks of k_str_rows (one item per block, at most 8 per SM)
+int str_rows_grid(uint64_t n_items) {
+	Device* d = current_device();
+	if (!d) { return 0; }
+	const uint64_t cap = static_cast<uint64_t>(d->sm_count) * 8;
+	return static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(n_items, cap)));
 }
 
 // The features of a string vector: those of its row hashes (distinct rows, runs, multiplicities), with the
 // slots that mean nothing for hashes replaced by the rows' lengths and compressibility.
 __global__ void __launch_bounds__(kWarps * 32) k_str_features(const StrCol* cols, const Item* items, uint64_t n_items,
-                                                              float* feat) {
+                                                              float* feat, uint32_t rs) {
 	const uint32_t lane = threadIdx.x & 31u;
 	for (uint64_t it = blockIdx.x * static_cast<uint64_t>(kWarps) + (threadIdx.x >> 5); it < n_items;
 	     it += static_cast<uint64_t>(gridDim.x) * kWarps) {
@@ -849,7 +892,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_str_features(const StrCol* cols
 		}
 		sl = warp_sum(sl);
 		sq = warp_sum(sq);
-		sc = warp_sum(sc);
+		sc = warp_sum(sc) * static_cast<float>(rs); // every rs-th row's compressed length, scaled
 		mx = warp_max(mx);
 		mn = warp_min(mn);
 		const float mean = sl / 1024.0f;
@@ -1174,6 +1217,25 @@ struct DevMem {
 	}
 };
 
+// Device scratch that only grows: a plan's calls reuse it instead of allocating (cudaFree synchronises the device).
+struct Scratch {
+	DevMem m;
+	size_t cap = 0;
+	bool   need(size_t n) {
+		if (n <= cap && m.p) { return true; }
+		if (!m.alloc(n)) {
+			cap = 0;
+			return false;
+		}
+		cap = n;
+		return true;
+	}
+	template <class T>
+	T* as() const {
+		return m.as<T>();
+	}
+};
+
 struct ItemSet {
 	DevMem   items, chunk_items, row_chunk;
 	uint64_t n = 0;
@@ -1283,9 +1345,10 @@ struct fls_sel_plan {
 	std::vector<uint64_t> chunk_first;
 	uint64_t              n_chunks = 0;
 	uint32_t              chunk_vectors = 64;
-	// wizard scratch (gtab: the chunk dictionary's global-memory tables, one per CTA)
-	DevMem   bw_code, parts, dict_n, gtab;
-	uint64_t gtab_bytes = 0;
+	// wizard scratch (gtab: the chunk dictionary's bucket scratch, one region per CTA; the subset lists of a
+	// wizard run over some chunks) and the learned selector's; all grow-only
+	Scratch bw_code, parts, dict_n, gtab, sub_items, sub_ranges, sub_ccol, sub_ids, sub_sizes, sub_best, vlen, vclen,
+	    dict_w, l_work, l_conf;
 	// string columns (fls_sel_plan_create_strings): the plan's columns are the row hashes; these are the strings
 	bool                str = false;
 	std::vector<StrCol> scols;
@@ -1340,41 +1403,56 @@ int wizard_run(fls_sel_plan* p, const std::vector<uint32_t>& subset, uint64_t* d
 	} else {
 		chunks = subset;
 	}
-	// item list of the selected chunks (in chunk order) and their ranges
-	std::vector<Item>     it;
-	std::vector<uint32_t> ranges(chunks.size() + 1), ccol(chunks.size());
-	for (size_t i = 0; i < chunks.size(); ++i) {
-		const uint32_t c = chunks[i];
-		ranges[i]        = static_cast<uint32_t>(it.size());
-		ccol[i]          = p->chunk_col[c];
-		for (uint32_t j = p->chunk_items[c]; j < p->chunk_items[c + 1]; ++j) {
-			Item m  = p->items[j];
-			m.chunk = static_cast<uint32_t>(i); // local chunk numbering for this run
-			it.push_back(m);
+	// item list of the selected chunks (in chunk order) and their ranges: the plan's own device lists for all
+	// chunks; for a subset, lists built here and copied in stream order into the plan's scratch
+	const Item*     items_d  = p->items_d.as<Item>();
+	const uint32_t* ranges_d = p->chunk_items_d.as<uint32_t>();
+	const uint32_t* ccol_d   = p->chunk_col_d.as<uint32_t>();
+	uint64_t        n_items  = p->items.size();
+	if (!all) {
+		std::vector<Item>     it;
+		std::vector<uint32_t> ranges(chunks.size() + 1), ccol(chunks.size());
+		for (size_t i = 0; i < chunks.size(); ++i) {
+			const uint32_t c = chunks[i];
+			ranges[i]        = static_cast<uint32_t>(it.size());
+			ccol[i]          = p->chunk_col[c];
+			for (uint32_t j = p->chunk_items[c]; j < p->chunk_items[c + 1]; ++j) {
+				Item m  = p->items[j];
+				m.chunk = static_cast<uint32_t>(i); // local chunk numbering for this run
+				it.push_back(m);
+			}
 		}
-	}
-	ranges[chunks.size()] = static_cast<uint32_t>(it.size());
-	if (it.empty()) { return FLS_OK; }
-	DevMem items_d, ranges_d, ccol_d, sizes_tmp, best_tmp;
-	int    rc;
-	if ((rc = upload(items_d, it.data(), it.size() * sizeof(Item))) != FLS_OK) { return rc; }
-	if ((rc = upload(ranges_d, ranges.data(), ranges.size() * 4)) != FLS_OK) { return rc; }
-	if ((rc = upload(ccol_d, ccol.data(), ccol.size() * 4)) != FLS_OK) { return rc; }
-	if (!p->parts.alloc(it.size() * 4) || !p->bw_code.alloc(it.size() * 4) || !p->dict_n.alloc(chunks.size() * 4)) {
-		return FLS_ERR_CUDA;
-	}
-	DevMem vlen, vclen, dict_w;
-	if (p->str) {
-		// the rows of every vector: hashes (the columns the integer passes read), lengths, compressed lengths
-		if (!vlen.alloc(it.size() * 8) || !vclen.alloc(it.size() * 8) || !dict_w.alloc(chunks.size() * 16)) {
+		ranges[chunks.size()] = static_cast<uint32_t>(it.size());
+		n_items               = it.size();
+		if (it.empty()) { return FLS_OK; }
+		if (!p->sub_items.need(it.size() * sizeof(Item)) || !p->sub_ranges.need(ranges.size() * 4) ||
+		    !p->sub_ccol.need(ccol.size() * 4) || !p->sub_ids.need(chunks.size() * 4) ||
+		    cudaMemcpyAsync(p->sub_items.m.p, it.data(), it.size() * sizeof(Item), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+		    cudaMemcpyAsync(p->sub_ranges.m.p, ranges.data(), ranges.size() * 4, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+		    cudaMemcpyAsync(p->sub_ccol.m.p, ccol.data(), ccol.size() * 4, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+		    cudaMemcpyAsync(p->sub_ids.m.p, chunks.data(), chunks.size() * 4, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+		    cudaStreamSynchronize(s) != cudaSuccess) { // the host lists go out of scope
 			return FLS_ERR_CUDA;
 		}
-		k_str_rows<<<grid_for(it.size()), kWarps * 32, 0, s>>>(p->scols_d.as<StrCol>(), items_d.as<Item>(), it.size(),
-		                                                       vlen.as<uint64_t>(), vclen.as<uint64_t>());
+		items_d  = p->sub_items.as<Item>();
+		ranges_d = p->sub_ranges.as<uint32_t>();
+		ccol_d   = p->sub_ccol.as<uint32_t>();
+	}
+	if (n_items == 0) { return FLS_OK; }
+	if (!p->parts.need(n_items * 4) || !p->bw_code.need(n_items * 4) || !p->dict_n.need(chunks.size() * 4)) {
+		return FLS_ERR_CUDA;
+	}
+	if (p->str) {
+		// the rows of every vector: hashes (the columns the integer passes read), lengths, compressed lengths
+		if (!p->vlen.need(n_items * 8) || !p->vclen.need(n_items * 8) || !p->dict_w.need(chunks.size() * 16)) {
+			return FLS_ERR_CUDA;
+		}
+		k_str_rows<<<str_rows_grid(n_items), kWarps * 32, 0, s>>>(p->scols_d.as<StrCol>(), items_d, n_items,
+		                                                          p->vlen.as<uint64_t>(), p->vclen.as<uint64_t>(), 1u);
 		++launch_counter();
 	}
-	ItemArgs ia {p->cols_d.as<Col>(), items_d.as<Item>(), it.size()};
-	k_parts<<<grid_for(it.size()), kWarps * 32, 0, s>>>(ia, p->parts.as<uint32_t>());
+	ItemArgs ia {p->cols_d.as<Col>(), items_d, n_items};
+	k_parts<<<grid_for(n_items), kWarps * 32, 0, s>>>(ia, p->parts.as<uint32_t>());
 	++launch_counter();
 	// dictionary of every chunk: one CTA per chunk, tables in shared memory
 	{
@@ -1388,18 +1466,15 @@ int wizard_run(fls_sel_plan* p, const std::vector<uint32_t>& subset, uint64_t* d
 		}
 		// one CTA per SM, each with its own bucket scratch for chunks of many distinct values
 		const uint32_t grid = static_cast<uint32_t>(std::min<size_t>(chunks.size(), static_cast<size_t>(dev->sm_count)));
-		if (p->gtab_bytes < kCdGBytes * grid) {
-			if (!p->gtab.alloc(kCdGBytes * grid)) { return FLS_ERR_CUDA; }
-			p->gtab_bytes = kCdGBytes * grid;
-		}
-		ChunkDictArgs a {p->cols_d.as<Col>(), items_d.as<Item>(), ranges_d.as<uint32_t>(),
+		if (!p->gtab.need(kCdGBytes * grid)) { return FLS_ERR_CUDA; }
+		ChunkDictArgs a {p->cols_d.as<Col>(), items_d, ranges_d,
 		                 static_cast<uint32_t>(chunks.size()), p->dict_n.as<uint32_t>(), p->bw_code.as<uint32_t>(),
 		                 dev->status, nullptr, nullptr, nullptr, p->gtab.as<uint8_t>()};
 		if (p->str) {
 			const uint32_t* const* wp = p->wptr_d.as<const uint32_t*>();
 			a.w0                      = wp;
 			a.w1                      = wp + p->scols.size();
-			a.dict_w                  = dict_w.as<uint64_t>();
+			a.dict_w                  = p->dict_w.as<uint64_t>();
 		}
 		k_chunk_dict<<<grid, kCdWarps * 32, kCdSmem, s>>>(a);
 		++launch_counter();
@@ -1408,17 +1483,17 @@ int wizard_run(fls_sel_plan* p, const std::vector<uint32_t>& subset, uint64_t* d
 	uint64_t* sizes = d_sizes;
 	uint8_t*  best  = d_best;
 	if (!all) {
-		if (!sizes_tmp.alloc(chunks.size() * K * 8) || !best_tmp.alloc(chunks.size())) { return FLS_ERR_CUDA; }
-		sizes = sizes_tmp.as<uint64_t>();
-		best  = best_tmp.as<uint8_t>();
+		if (!p->sub_sizes.need(chunks.size() * K * 8) || !p->sub_best.need(chunks.size())) { return FLS_ERR_CUDA; }
+		sizes = p->sub_sizes.as<uint64_t>();
+		best  = p->sub_best.as<uint8_t>();
 	}
 	if (p->str) {
-		StrSizeArgs sa {ccol_d.as<uint32_t>(), ranges_d.as<uint32_t>(), p->parts.as<uint32_t>(), p->bw_code.as<uint32_t>(),
-		                vlen.as<uint64_t>(), vclen.as<uint64_t>(), p->dict_n.as<uint32_t>(), dict_w.as<uint64_t>(),
+		StrSizeArgs sa {ccol_d, ranges_d, p->parts.as<uint32_t>(), p->bw_code.as<uint32_t>(),
+		                p->vlen.as<uint64_t>(), p->vclen.as<uint64_t>(), p->dict_n.as<uint32_t>(), p->dict_w.as<uint64_t>(),
 		                p->scols_d.as<StrCol>(), static_cast<uint32_t>(chunks.size()), sizes, best};
 		k_str_sizes<<<static_cast<unsigned>((chunks.size() + 7) / 8), 256, 0, s>>>(sa);
 	} else {
-		SizeArgs sa {p->cols_d.as<Col>(), ccol_d.as<uint32_t>(), ranges_d.as<uint32_t>(), p->parts.as<uint32_t>(),
+		SizeArgs sa {p->cols_d.as<Col>(), ccol_d, ranges_d, p->parts.as<uint32_t>(),
 		             p->bw_code.as<uint32_t>(), p->dict_n.as<uint32_t>(), static_cast<uint32_t>(chunks.size()), sizes, best};
 		k_chunk_sizes<<<static_cast<unsigned>((chunks.size() + 7) / 8), 256, 0, s>>>(sa);
 	}
@@ -1426,15 +1501,12 @@ int wizard_run(fls_sel_plan* p, const std::vector<uint32_t>& subset, uint64_t* d
 	if (cudaGetLastError() != cudaSuccess) { return FLS_ERR_CUDA; }
 	if (!all) {
 		// the subset's choices go to their chunks (sizes of a subset are not reported)
-		DevMem ids;
-		if ((rc = upload(ids, chunks.data(), chunks.size() * 4)) != FLS_OK) { return rc; }
 		if (d_best) {
-			k_scatter_best<<<64, 256, 0, s>>>(best, ids.as<uint32_t>(), static_cast<uint32_t>(chunks.size()), d_best);
+			k_scatter_best<<<64, 256, 0, s>>>(best, p->sub_ids.as<uint32_t>(), static_cast<uint32_t>(chunks.size()), d_best);
 			++launch_counter();
 		}
-		if (cudaStreamSynchronize(s) != cudaSuccess) { return FLS_ERR_CUDA; }
 	} else if (d_dict_n) {
-		if (cudaMemcpyAsync(d_dict_n, p->dict_n.p, chunks.size() * 4, cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+		if (cudaMemcpyAsync(d_dict_n, p->dict_n.m.p, chunks.size() * 4, cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
 			return FLS_ERR_CUDA;
 		}
 	}
@@ -1475,6 +1547,8 @@ int fls_sel_plan_create(const fls_sel_column* cols, uint32_t n_cols, uint32_t ch
 	int rc;
 	if ((rc = upload(p->cols_d, p->cols.data(), p->cols.size() * sizeof(Col))) != FLS_OK) { return rc; }
 	if ((rc = upload(p->items_d, p->items.data(), p->items.size() * sizeof(Item))) != FLS_OK) { return rc; }
+	if ((rc = upload(p->chunk_items_d, p->chunk_items.data(), p->chunk_items.size() * 4)) != FLS_OK) { return rc; }
+	if ((rc = upload(p->chunk_col_d, p->chunk_col.data(), p->chunk_col.size() * 4)) != FLS_OK) { return rc; }
 	*out = p.release();
 	return FLS_OK;
 }
@@ -1623,17 +1697,20 @@ int fls_sel_wizard(fls_sel_plan* p, uint64_t* d_sizes, uint8_t* d_best, uint32_t
 } // extern "C"
 
 namespace {
-// Statistics of the items of a: for a string plan, the sampled vectors' rows first (hashes, lengths, compressed
-// lengths), then the hash features with the string slots filled in.
-cudaError_t sample_features(fls_sel_plan* p, const ItemArgs& a, float* feat, cudaStream_t s) {
+// Statistics of the items of a: for a string plan, the sampled vectors' rows first (hashes and lengths of every
+// row, compressed lengths of every kStrFeatRowStride-th row), then the hash features with the string slots
+// filled in.
+constexpr uint32_t kStrFeatRowStride = 4;
+cudaError_t        sample_features(fls_sel_plan* p, const ItemArgs& a, float* feat, cudaStream_t s) {
 	if (p->str) {
-		k_str_rows<<<grid_for(a.n_items), kWarps * 32, 0, s>>>(p->scols_d.as<StrCol>(), a.items, a.n_items, nullptr,
-		                                                      nullptr);
+		k_str_rows<<<str_rows_grid(a.n_items), kWarps * 32, 0, s>>>(p->scols_d.as<StrCol>(), a.items, a.n_items,
+		                                                            nullptr, nullptr, kStrFeatRowStride);
 		++launch_counter();
 	}
 	cudaError_t e = launch_features(a, feat, s);
 	if (e != cudaSuccess || !p->str) { return e; }
-	k_str_features<<<grid_for(a.n_items), kWarps * 32, 0, s>>>(p->scols_d.as<StrCol>(), a.items, a.n_items, feat);
+	k_str_features<<<grid_for(a.n_items), kWarps * 32, 0, s>>>(p->scols_d.as<StrCol>(), a.items, a.n_items, feat,
+	                                                           kStrFeatRowStride);
 	++launch_counter();
 	return cudaGetLastError();
 }
@@ -1668,9 +1745,9 @@ int fls_sel_learned(fls_sel_plan* p, const float* d_params, uint32_t stride, flo
 	int          rc  = sample_set(p, stride, &set);
 	if (rc != FLS_OK) { return rc; }
 	const uint64_t n = set->n;
-	DevMem         work, conf;
-	if (!work.alloc(n * (NF + 2 * H + 2 * K) * 4) || !conf.alloc(p->n_chunks * 4)) { return FLS_ERR_CUDA; }
-	float*   feat = work.as<float>();
+	if (!p->l_work.need(n * (NF + 2 * H + 2 * K) * 4) || !p->l_conf.need(p->n_chunks * 4)) { return FLS_ERR_CUDA; }
+	Scratch& conf = p->l_conf;
+	float*   feat = p->l_work.as<float>();
 	float*   h1   = feat + n * NF;
 	float*   h2   = h1 + n * H;
 	float*   z    = h2 + n * H;
@@ -1685,12 +1762,12 @@ int fls_sel_learned(fls_sel_plan* p, const float* d_params, uint32_t stride, flo
 	                                                                     conf.as<float>(), p->str ? kStrK : K);
 	launch_counter() += 2;
 	if (cudaGetLastError() != cudaSuccess) { return FLS_ERR_CUDA; }
-	if (d_conf && cudaMemcpyAsync(d_conf, conf.p, p->n_chunks * 4, cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+	if (d_conf && cudaMemcpyAsync(d_conf, conf.m.p, p->n_chunks * 4, cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
 		return FLS_ERR_CUDA;
 	}
 	if (threshold > 0.0f) {
 		std::vector<float> hc(p->n_chunks);
-		if (cudaMemcpyAsync(hc.data(), conf.p, hc.size() * 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+		if (cudaMemcpyAsync(hc.data(), conf.m.p, hc.size() * 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
 		    cudaStreamSynchronize(s) != cudaSuccess) {
 			return FLS_ERR_CUDA;
 		}

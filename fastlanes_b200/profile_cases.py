@@ -6,6 +6,7 @@
     python -m fastlanes_b200.profile_cases mixed --columns 32 --reps 3
     python -m fastlanes_b200.profile_cases select --columns 32 --reps 3
     python -m fastlanes_b200.profile_cases filter --values 16777216 --reps 3
+    python -m fastlanes_b200.profile_cases select_strings --columns 12 --reps 3
 
 Each case builds its input, decodes (or selects) once and checks the result, then repeats the call `reps`
 times, and prints one line with the mean time of the repeats (CUDA events; not a benchmark number).
@@ -155,6 +156,34 @@ def case_select(a):
     return res
 
 
+def case_select_strings(a):
+    """Expression selection over string columns shaped as the mixed configuration's (4096-entry token
+    dictionaries, Zipf(1.1) codes; --columns columns of 64 vectors ... --max-vectors vectors): the wizard and the
+    learned path (an untrained network, no wizard fallback), each timed with CUDA events."""
+    from . import select as SL
+    from . import strings as S
+    from . import workloads as W
+
+    rng = np.random.default_rng(1)
+    cols = []
+    for _ in range(a.columns):
+        seed = int(rng.integers(0, 2 ** 31))
+        dbytes, doffs = W.string_dictionary(seed=seed)
+        codes = W.zipf_codes(int(rng.integers(64, a.max_vectors + 1)) * 1024, seed=seed + 1)
+        sb, so = W.dict_rows_device(dbytes, doffs, codes, "cuda")
+        table, _, _ = S.fsst_compress(dbytes, doffs)
+        cols.append((sb, so, table))
+    plan = SL.StrSelectionPlan(cols)
+    params = SL.mlp_init(0)
+    plan.wizard()
+    plan.learned(params, 8)
+    wms = _timed(plan.wizard, a.reps)
+    ms = _timed(lambda: plan.learned(params, 8), a.reps)
+    res = f"select_strings chunks={plan.n_chunks} ms={ms:.4f} wizard_ms={wms:.4f}"
+    plan.close()
+    return res
+
+
 def case_fsst(a):
     """The DICT+FSST configuration's rows as an FSST column (string pool id 13)."""
     from . import strings as S
@@ -179,7 +208,7 @@ def case_fsst(a):
 
 
 CASES = {"strings": case_strings, "rle": case_rle, "delta": case_delta, "mixed": case_mixed, "select": case_select,
-         "filter": case_filter, "fsst": case_fsst}
+         "filter": case_filter, "fsst": case_fsst, "select_strings": case_select_strings}
 
 
 def main(argv=None):
