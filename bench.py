@@ -461,10 +461,12 @@ def other_configs(dev, args):
     ms = device_timed(lambda: plan.decode_into(offs_t, data_t), steps, 3)
     offs_t.zero_()
     data_t.zero_()
+    L.lib.fls_gpu_launch_count(1)
     plan.decode_into(offs_t, data_t)
+    launches = int(L.lib.fls_gpu_launch_count(1))  # the library's kernel launches of one decode
     ok = ok and W.dict_rows_match(offs_t, data_t[:n_bytes], dbytes, doffs, codes)
     leg("4_dict_fsst_str", "16Mi rows, 4096-entry FSST dictionary (5-40 B strings), Zipf(1.1) codes at 12 bits",
-        ms, page.size + dic.size, 4 * (codes.size + 1) + n_bytes, codes.size, ok, 3)
+        ms, page.size + dic.size, 4 * (codes.size + 1) + n_bytes, codes.size, ok, launches)
     plan.close()
     # the reference: its DICT FFOR string expression (string pool id 3) over the first 256 Ki rows
     sc = codes[:1 << 18]
@@ -503,8 +505,11 @@ def fsst_leg(dev, n_rows, steps, leg, out):
     ok = n_bytes == pbytes.size and torch.equal(offs_t.long().cpu(), torch.from_numpy(poffs.astype(np.int64)))
     ok = ok and torch.equal(data_t[:n_bytes], torch.from_numpy(pbytes).to(dev))
     ms = device_timed(lambda: plan.decode_into(offs_t, data_t), steps, 3)
+    L.lib.fls_gpu_launch_count(1)
+    plan.decode_into(offs_t, data_t)
+    launches = int(L.lib.fls_gpu_launch_count(1))  # the library's kernel launches of one decode
     leg("4b_fsst_str", f"the same {codes_n} rows as an FSST column (string pool id 13), one symbol table",
-        ms, page.size + dic.size, 4 * (codes_n + 1) + n_bytes, codes_n, ok, 3)
+        ms, page.size + dic.size, 4 * (codes_n + 1) + n_bytes, codes_n, ok, launches)
     plan.close()
     del data_t, offs_t, pg_d, dc_d
     fo = np.zeros((1 << 18) + 1, np.uint64)

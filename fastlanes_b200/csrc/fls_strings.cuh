@@ -87,7 +87,17 @@ __device__ __forceinline__ bool put_row(uint32_t* __restrict__ win, uint32_t d, 
 	if (k0 == k1) { return mid; }
 	const uint32_t m = k1 - k0; // words k0 + 1 .. k1 - 1 are whole row words
 	uint32_t       j = 1;
-#pragma unroll 4
+	// four source words loaded before their four stores (more loads in flight); s + j + 4 <= s + m <= the
+	// row's last source word
+	for (; j + 3 < m; j += 4) {
+		const int32_t  q  = s + static_cast<int32_t>(j);
+		const uint32_t a1 = base[q + 1], a2 = base[q + 2], a3 = base[q + 3], a4 = base[q + 4];
+		win[k0 + j]       = __funnelshift_r(w1, a1, sh);
+		win[k0 + j + 1]   = __funnelshift_r(a1, a2, sh);
+		win[k0 + j + 2]   = __funnelshift_r(a2, a3, sh);
+		win[k0 + j + 3]   = __funnelshift_r(a3, a4, sh);
+		w1                = a4;
+	}
 	for (; j < m; ++j) {
 		w0          = w1;
 		w1          = base[s + static_cast<int32_t>(j) + 1];
