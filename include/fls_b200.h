@@ -323,7 +323,10 @@ int fls_string_plan_rows(const fls_string_plan* plan, uint64_t* n_rows);
 /* Total decoded bytes (runs the length pass; synchronises the stream). */
 int fls_string_plan_measure(fls_string_plan* plan, uint64_t* n_bytes, fls_stream_t stream);
 /* d_offsets: n_rows + 1 entries; d_bytes: 16-byte aligned, bytes_cap < 4 GiB.  Asynchronous, no allocation.
- * Runs the length pass itself unless a measure() came just before (whose totals it then takes over). */
+ * FSST and BYTE_ARR pages, and DICT pages whose dictionary entries are < 256 bytes, decode in one launch (after
+ * one memset): every vector finds its first output byte by a look-back over the earlier vectors' totals.  Other
+ * pages (FSST12, DICT with longer entries) run the length pass themselves unless a measure() came just before
+ * (whose totals they then take over). */
 int fls_string_plan_decode(const fls_string_plan* plan, uint32_t* d_offsets, uint8_t* d_bytes, uint64_t bytes_cap,
                            fls_stream_t stream);
 int fls_string_plan_destroy(fls_string_plan* plan);

@@ -61,7 +61,8 @@ int fls_sel_plan_destroy(fls_sel_plan* plan);
  * The wizard's sizes are exact for those pages, the dictionary holding a chunk's distinct rows in
  * first-occurrence order compressed with the column's table (distinct rows are told apart by a 64-bit hash of
  * their bytes); sizes 4 and 5 of a string chunk are UINT64_MAX.  fls_sel_wizard, fls_sel_features and
- * fls_sel_learned take the plan as they take an integer one; the learned vote chooses among the 4.
+ * fls_sel_learned take the plan as they take an integer one (their statistics take the compressed length of
+ * every 4th row of a sampled vector, scaled); the learned vote chooses among the 4.
  * Synchronous. */
 #define FLS_SEL_STR_K 4
 typedef struct fls_sel_str_column {
