@@ -343,8 +343,9 @@ int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_
 		std::memcpy(&x, page + pi.ep_off + 4ull * ((v - 1) * pi.arr_c + b), 4);
 		return x;
 	};
-	// chunks of about 8 MB of output, the first of about 1 MB so that the copies out start early
-	const uint64_t         chunk_vec = std::max<uint64_t>(1, (8ull << 20) / (1024 * sz));
+	// chunks of about 16 MB of output (fewer, larger copies: with both directions busy the link moves more in
+	// long copies), the first of about 1 MB so that the copies out start early
+	const uint64_t         chunk_vec = std::max<uint64_t>(1, (16ull << 20) / (1024 * sz));
 	const uint64_t         first_vec = std::max<uint64_t>(1, (1ull << 20) / (1024 * sz));
 	std::vector<uint32_t>  bounds {0};
 	while (bounds.back() < pi.vec_c) {
@@ -358,13 +359,25 @@ int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_
 	                   : !post_is_gather(pi.layout->post) ? Family::NUM
 	                   : c.e <= 4                         ? Family::GATHER_NARROW
 	                                                      : Family::GATHER;
-	// page header, buffer offsets and entry points first
+	// page header, buffer offsets and entry points first, then every buffer but the largest whole (a few bytes
+	// per vector: bit widths, bases, run counts), so that each chunk is one copy of the largest buffer's slice
 	if (cudaMemcpyAsync(dp, page, pi.meta_sz, cudaMemcpyHostToDevice, hp->in) != cudaSuccess) { return FLS_ERR_CUDA; }
+	int big = -1;
+	for (uint32_t b = 0; b < pi.arr_c; ++b) {
+		if (static_cast<int>(b) != rec_b && (big < 0 || pi.size[b] > pi.size[big])) { big = static_cast<int>(b); }
+	}
+	for (uint32_t b = 0; b < pi.arr_c; ++b) {
+		if (static_cast<int>(b) == rec_b || static_cast<int>(b) == big || pi.size[b] == 0) { continue; }
+		if (pi.off[b] + pi.size[b] <= page_size &&
+		    cudaMemcpyAsync(dp + pi.off[b], page + pi.off[b], pi.size[b], cudaMemcpyHostToDevice, hp->in) != cudaSuccess) {
+			return FLS_ERR_CUDA;
+		}
+	}
 	for (uint32_t k = 0; k < n_chunks; ++k) {
 		const uint32_t v0 = bounds[k];
 		const uint32_t v1 = bounds[k + 1];
 		for (uint32_t b = 0; b < pi.arr_c; ++b) {
-			if (static_cast<int>(b) == rec_b) { continue; } // already in place (and decoded)
+			if (static_cast<int>(b) != big) { continue; } // the others are in place (rec buffers also decoded)
 			const uint64_t lo = pi.off[b] + ep(v0, b);
 			const uint64_t hi = v1 < pi.vec_c ? pi.off[b] + ep(v1, b) : pi.off[b] + pi.size[b];
 			if (hi > lo && hi <= page_size &&
