@@ -489,6 +489,7 @@ def other_configs(dev, args):
 def fsst_leg(dev, n_rows, steps, leg, out):
     import torch
 
+    from fastlanes_b200 import _lib as L
     from fastlanes_b200 import strings as S
     from fastlanes_b200 import workloads as W
 

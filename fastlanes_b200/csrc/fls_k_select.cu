@@ -609,7 +609,8 @@ __device__ __forceinline__ void chunk_dict(const ChunkDictArgs& a, const Col& co
 #pragma unroll
 		for (uint32_t b = 0; b < kCdParts; ++b) { bcount[b] = s_wsum[b]; }
 		__syncthreads();
-		// every bucket through the table
+		// every bucket through the table; once a bucket's table is complete, every pair's key is replaced by its
+		// key's first position (high half) beside its own position, so the code pass needs no table
 		for (uint32_t b = 0; b < kCdParts; ++b) {
 			begin_insert();
 			for (uint32_t k = tid; k < bcount[b]; k += nt) {
@@ -618,7 +619,13 @@ __device__ __forceinline__ void chunk_dict(const ChunkDictArgs& a, const Col& co
 			}
 			__syncthreads();
 			if ((*s_over != 0 || *s_count > mask) && tid == 0) { atomicOr(a.status, STATUS_BAD_INDEX); } // never
-			harvest();
+			for (uint32_t k = tid; k < bcount[b]; k += nt) {
+				const uint64_t where = static_cast<uint64_t>(b) * kCdBucket + k;
+				const uint32_t sl    = cd_find(keys, mask, bkeys[where]);
+				const uint32_t f     = sl > mask + 1 ? kNoPos : first[sl];
+				bkeys[where]         = (static_cast<uint64_t>(f) << 32) | bpos[where];
+			}
+			harvest(); // reads the table only; its closing barrier orders the clear after every find
 			clear_table();
 		}
 	}
@@ -672,25 +679,34 @@ __device__ __forceinline__ void chunk_dict(const ChunkDictArgs& a, const Col& co
 		__syncthreads();
 		clear_table();
 	} else {
+		// codes from the recorded first positions; a warp whose pairs all belong to one vector (the usual case:
+		// a bucket keeps the scatter's order) folds them before one atomic pair
 		for (uint32_t b = 0; b < kCdParts; ++b) {
-			begin_insert();
-			for (uint32_t k = tid; k < bcount[b]; k += nt) {
-				const uint64_t where = static_cast<uint64_t>(b) * kCdBucket + k;
-				insert_one(bkeys[where], bpos[where], kCdSlots);
+			for (uint32_t kb = 0; kb < bcount[b]; kb += nt) {
+				const uint32_t k  = kb + tid;
+				uint32_t       vi = ~0u, code = 0;
+				if (k < bcount[b]) {
+					const uint64_t e = bkeys[static_cast<uint64_t>(b) * kCdBucket + k];
+					const uint32_t f = static_cast<uint32_t>(e >> 32);
+					if (f != kNoPos) {
+						vi   = static_cast<uint32_t>(e) >> 10; // the vector inside the chunk
+						code = code_of(f);
+					}
+				}
+				const uint32_t v0 = __shfl_sync(0xFFFFFFFFu, vi, 0);
+				if (__all_sync(0xFFFFFFFFu, vi == v0)) {
+					const uint32_t mn = warp_min(code), mx = warp_max(code);
+					if (lane == 0 && v0 != ~0u) {
+						atomicMin(vrange + 2 * v0, mn);
+						atomicMax(vrange + 2 * v0 + 1, mx);
+					}
+				} else if (vi != ~0u) {
+					atomicMin(vrange + 2 * vi, code);
+					atomicMax(vrange + 2 * vi + 1, code);
+				}
 			}
-			__syncthreads();
-			for (uint32_t k = tid; k < bcount[b]; k += nt) {
-				const uint64_t where = static_cast<uint64_t>(b) * kCdBucket + k;
-				const uint32_t sl    = cd_find(keys, mask, bkeys[where]);
-				if (sl > mask + 1) { continue; }
-				const uint32_t code = code_of(first[sl]);
-				const uint32_t vi   = bpos[where] >> 10; // the vector inside the chunk
-				atomicMin(vrange + 2 * vi, code);
-				atomicMax(vrange + 2 * vi + 1, code);
-			}
-			__syncthreads();
-			clear_table();
 		}
+		__syncthreads();
 	}
 	for (uint32_t j = i0 + tid; j < i1; j += nt) {
 		const uint32_t lo = vrange[2 * (j - i0)], hi = vrange[2 * (j - i0) + 1];
