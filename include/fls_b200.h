@@ -357,8 +357,7 @@ int fls_string_set_destroy(fls_string_set* set);
  * Limits and rules:
  *   - at most FLS_NOALLOC_MAX_VECTORS vectors (8,388,608 rows) per page; larger pages return FLS_ERR_TOO_LARGE
  *     before any work;
- *   - the first call on a device looks up the array's device address (cudaGetSymbolAddress); make that first
- *     call before any stream capture;
+ *   - the first call on a device looks up the array's device address (cudaGetSymbolAddress);
  *   - every call reads the page header and the symbol table back to the host in `stream`'s order (after the
  *     work queued on it before) and waits for those reads;
  *   - all calls share the array, so calls whose work overlaps on the GPU (other streams, other threads) race;
