@@ -295,3 +295,42 @@ def test_string_set_decodes_every_dict_page_in_one_launch(cuda, col_golden):
     for p in plans:
         p.close()
     assert P.device_status() == 0
+
+
+def test_fsst_column_with_and_without_escapes(cuda):
+    """The single-pass FSST decode on a page of our own encoder where some vectors hold escape codes (rare bytes
+    outside the symbol table: those vectors take the escape-aware total) and others none (their total is the sum
+    of their symbol lengths), with empty, one-byte and long rows: every offset and byte as the input's."""
+    from fastlanes_b200 import primitives as P
+    from fastlanes_b200 import strings as S
+
+    rng = np.random.default_rng(31)
+    common = np.frombuffer(b"abcdefghijklmnopqrstuvwxyz0123456789", np.uint8)
+    n_vec = 48
+    rows = []
+    for v in range(n_vec):
+        rare = v % 3 == 1  # every third vector: rows sprinkled with rare bytes
+        for _ in range(1024):
+            n = int(rng.choice([0, 1, 3, 9, 24, 200], p=[.1, .1, .2, .3, .25, .05]))
+            r = common[rng.integers(0, common.size, n)]
+            if rare and n:
+                m = rng.random(n) < 0.2
+                r = r.copy()
+                r[m] = rng.integers(128, 256, int(m.sum()), dtype=np.uint8)
+            rows.append(r)
+    byts = np.concatenate(rows).astype(np.uint8)
+    offs = np.zeros(len(rows) + 1, np.uint64)
+    offs[1:] = np.cumsum([r.size for r in rows])
+    table, comp, coffs = S.fsst_compress(byts, offs)
+    assert (comp == 255).any()  # the page does hold escapes
+    page, dic = S.fsst_page(table, comp, coffs)
+    pb, pp = _dev(page, cuda, 1)
+    db, dp = _dev(dic, cuda, 0)
+    plan = S.StringPlan(pp, page.size, dp, dic.size)
+    n = plan.measure()
+    assert n == byts.size
+    got_o, got_b = plan.decode(cuda)
+    assert np.array_equal(got_o.cpu().numpy().astype(np.uint64), offs)
+    assert np.array_equal(got_b.cpu().numpy(), byts)
+    plan.close()
+    assert P.device_status() == 0
