@@ -270,10 +270,11 @@ HostPipe* host_pipe() {
 	return &h;
 }
 
-// Decode a page held in host memory into host memory.  The header is parsed from the host copy; the vectors
-// go through in chunks of about 8 MB of output: each chunk's slice of every page buffer is copied in on one
-// stream, decoded on a second (a queue of the chunk's vector ids) and copied out on a third, so the copies in
-// both directions and the kernels overlap (with pinned host buffers).
+// Decode a page held in host memory into host memory.  The header is parsed from the host copy and the page's
+// small per-vector buffers go over whole; the vectors then go through in chunks of about 16 MB of output (the
+// first about 1 MB): each chunk's slice of the largest buffer is copied in on one stream, decoded on a second
+// (a queue of the chunk's vector ids) and copied out on a third, so the copies in both directions and the
+// kernels overlap (with pinned host buffers).
 int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_t out_cap, uint8_t dt,
                      uint64_t* n_values) {
 	const int w = value_width_of(dt);
