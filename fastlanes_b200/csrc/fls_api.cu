@@ -115,15 +115,16 @@ static const Variant* family_variants(Family fam, const DecodeArgs& a, int* n) {
 		default: return kFAny;
 		}
 	}
+	auto count = [](const auto& arr) { return static_cast<int>(sizeof(arr) / sizeof(arr[0])); };
 	switch (fam) {
-	case Family::NUM_NARROW: *n = 3; return kNum32;
+	case Family::NUM_NARROW: *n = count(kNum32); return kNum32;
 	case Family::NUM:
-		*n = 3;
+		*n = narrow ? count(kNum32) : count(kNum64);
 		return narrow ? kNum32 : kNum64;
-	case Family::NUM_PATCH: *n = 2; return kNumPatch;
-	case Family::GATHER: *n = 3; return kGather;
-	case Family::GATHER_NARROW: *n = 3; return kGather32;
-	default: *n = 1; return kAny;
+	case Family::NUM_PATCH: *n = count(kNumPatch); return kNumPatch;
+	case Family::GATHER: *n = count(kGather); return kGather;
+	case Family::GATHER_NARROW: *n = count(kGather32); return kGather32;
+	default: *n = count(kAny); return kAny;
 	}
 }
 
