@@ -334,3 +334,46 @@ def test_fsst_column_with_and_without_escapes(cuda):
     assert np.array_equal(got_b.cpu().numpy(), byts)
     plan.close()
     assert P.device_status() == 0
+
+
+def test_string_set_with_a_dictionary_too_large_for_shared_memory(cuda):
+    """A string set whose largest dictionary (70,000 entries: 32-bit code rows) does not fit in shared memory
+    decodes every column from global memory in one launch: a large-dictionary column, two small ones of 16-bit
+    codes and a one-vector column, every offset and byte against the generator's rows, twice in a row."""
+    import torch
+
+    from fastlanes_b200 import primitives as P
+    from fastlanes_b200 import strings
+    from fastlanes_b200 import workloads as W
+
+    rng = np.random.default_rng(77)
+    cols = []
+    for n_dict, n_vec in ((70000, 9), (300, 5), (4096, 12), (17, 1)):
+        lens = rng.integers(0, 60, n_dict)
+        doffs = np.zeros(n_dict + 1, np.uint64)
+        doffs[1:] = np.cumsum(lens)
+        dbytes = rng.integers(0, 256, int(doffs[-1]), dtype=np.uint8)
+        codes = rng.integers(0, n_dict, n_vec * 1024).astype(np.uint32)
+        cols.append((dbytes, doffs, codes))
+    keep, plans = [], []
+    for i, (dbytes, doffs, codes) in enumerate(cols):
+        page, dic = strings.encode_string_dict(dbytes, doffs, codes)
+        pb, pp = _dev(page, cuda, i % 4)
+        db, dp = _dev(dic, cuda, 0)
+        keep += [pb, db]
+        plans.append(strings.StringPlan(pp, page.size, dp, dic.size))
+    sizes = [p.measure() for p in plans]
+    offs = [torch.full((p.n_rows + 1,), -1, dtype=torch.int32, device=cuda) for p in plans]
+    data = [torch.full((n + 16,), 0xEE, dtype=torch.uint8, device=cuda) for n in sizes]
+    sset = strings.StringSet(plans)
+    sset.bind(offs, data)
+    for _ in range(2):
+        sset.decode()
+        torch.cuda.synchronize()
+        for (dbytes, doffs, codes), o, d, n in zip(cols, offs, data, sizes):
+            assert W.dict_rows_match(o, d[:n], dbytes, doffs, codes)
+            assert (d[n:] == 0xEE).all()
+    sset.close()
+    for p in plans:
+        p.close()
+    assert P.device_status() == 0
