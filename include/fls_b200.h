@@ -326,7 +326,8 @@ int fls_string_plan_measure(fls_string_plan* plan, uint64_t* n_bytes, fls_stream
  * FSST and BYTE_ARR pages, and DICT pages whose dictionary entries are < 256 bytes, decode in one launch (after
  * one memset): every vector finds its first output byte by a look-back over the earlier vectors' totals.  Other
  * pages (FSST12, DICT with longer entries) run the length pass themselves unless a measure() came just before
- * (whose totals they then take over). */
+ * (whose totals they then take over).  The plan keeps that scratch (look-back words, totals), so decodes of one
+ * plan whose work overlaps on the GPU (other streams) race: order them, or give each stream its own plan. */
 int fls_string_plan_decode(const fls_string_plan* plan, uint32_t* d_offsets, uint8_t* d_bytes, uint64_t bytes_cap,
                            fls_stream_t stream);
 int fls_string_plan_destroy(fls_string_plan* plan);
@@ -339,7 +340,8 @@ int fls_string_plan_destroy(fls_string_plan* plan);
  * create: from plans made by fls_string_plan_create (they must outlive the set; FLS_ERR_UNSUPPORTED for a plan of
  *   another kind).  bind: each column's outputs (as fls_string_plan_decode's: n_rows + 1 u32 offsets, 16-byte
  *   aligned bytes, capacity < 4 GiB); synchronous, once.  decode: asynchronous, no allocation, capturable in a
- *   CUDA graph.  Device memory a set holds: 8 bytes per vector and per CTA-sized chunk of vectors.
+ *   CUDA graph; decodes of one set whose work overlaps on the GPU race on its scratch.  Device memory a set
+ *   holds: 8 bytes per vector and per CTA-sized chunk of vectors.
  * ------------------------------------------------------------------------------------------------------- */
 typedef struct fls_string_set fls_string_set;
 int fls_string_set_create(const fls_string_plan* const* plans, uint32_t n, fls_string_set** out_set);
