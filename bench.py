@@ -560,7 +560,9 @@ def mixed_rowgroups(dev, peak, steps):
     rng = np.random.default_rng(1)
     cols, str_cols = W.mixed_rowgroup_columns(rng, 256, str(dev))
     plan = SL.SelectionPlan(cols)
-    stride, thr = 8, 0.7
+    # every 16th vector of a 64-vector chunk for the integer selector (every 8th chose the same expressions in a
+    # sweep of 8 / 12 / 16 / 32: 0.0 % ratio loss up to 16), every 8th for the string selector
+    stride, sstride, thr = 16, 8, 0.7
     ms_wiz, host_wiz, (sizes, best, _) = event_timed(plan.wizard)
     ms_sel, host_sel, (choice, conf, n_fb) = event_timed(lambda: plan.learned(params, stride, thr))
     value_bytes = sum(t.numel() * t.element_size() for t, _ in cols)
@@ -583,7 +585,7 @@ def mixed_rowgroups(dev, peak, steps):
         str_dev.append((sb, so, table))
     splan = SL.StrSelectionPlan(str_dev)
     ms_swiz, host_swiz, (ssizes, sbest, _) = event_timed(splan.wizard)
-    ms_ssel, host_ssel, (schoice, sconf, sn_fb) = event_timed(lambda: splan.learned(sparams, stride, thr))
+    ms_ssel, host_ssel, (schoice, sconf, sn_fb) = event_timed(lambda: splan.learned(sparams, sstride, thr))
     ssizes4 = ssizes[:, :SL.STR_K]
     sloss = SL.ratio_loss(ssizes4, schoice)
     sagree = float((schoice == sbest).float().mean())
@@ -664,7 +666,7 @@ def mixed_rowgroups(dev, peak, steps):
                 "speedup": round(ms_swiz / ms_ssel, 1),
                 "host_ms": {"learned": round(host_ssel, 3), "wizard": round(host_swiz, 3)},
                 "ratio_loss_pct": round(sloss * 100, 4), "agreement_with_wizard": round(sagree, 4),
-                "wizard_fallback_chunks": int(sn_fb),
+                "wizard_fallback_chunks": int(sn_fb), "sample_stride": sstride,
                 "candidates": dict(zip(SL.STR_CANDIDATES, np.bincount(schoice.cpu().numpy(), minlength=SL.STR_K)
                                        [:SL.STR_K].tolist())),
                 "training": {"vectors": int(sfeat.shape[0]), "label_s": round(t_slabel, 2),
