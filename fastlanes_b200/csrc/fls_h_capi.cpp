@@ -224,7 +224,11 @@ int encode_t(const T* in, uint64_t n, uint64_t cap, uint8_t* out, uint64_t* out_
 }
 
 // The three streams of the host decode pipeline of the current device: copies in, decode, copies out.
-constexpr uint32_t kPipeEvents = 256;    // two per chunk: enough for a 65,535-vector page of 8-byte values
+constexpr uint32_t kPipeEvents = 256;    // three per chunk: enough for a 65,535-vector page of 8-byte values
+// A chunk's copy in waits for the copy out of the chunk kPipeLead places before it.  Copies in are half the
+// bytes of copies out: issued all at once they take half the link for the first part of the call and the
+// copies out then run alone; paced, both directions stay busy for the whole call.
+constexpr uint32_t kPipeLead = 2;
 constexpr uint32_t kPipeIds     = 65536; // the identity work queue of a page's vectors, uploaded once
 struct HostPipe {
 	cudaStream_t in = nullptr, dec = nullptr, out = nullptr;
@@ -354,7 +358,7 @@ int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_
 		bounds.push_back(static_cast<uint32_t>(std::min<uint64_t>(pi.vec_c, bounds.back() + step)));
 	}
 	const uint32_t n_chunks = static_cast<uint32_t>(bounds.size() - 1);
-	if (2ull * n_chunks > kPipeEvents) { return FLS_ERR_TOO_LARGE; }
+	if (3ull * n_chunks > kPipeEvents) { return FLS_ERR_TOO_LARGE; }
 	cudaEvent_t* ev = hp->ev;
 	const Family fam = post_is_patch(pi.layout->post)    ? Family::NUM_PATCH
 	                   : !post_is_gather(pi.layout->post) ? Family::NUM
@@ -377,6 +381,9 @@ int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_
 	for (uint32_t k = 0; k < n_chunks; ++k) {
 		const uint32_t v0 = bounds[k];
 		const uint32_t v1 = bounds[k + 1];
+		if (k >= kPipeLead && cudaStreamWaitEvent(hp->in, ev[3 * (k - kPipeLead) + 2], 0) != cudaSuccess) {
+			return FLS_ERR_CUDA;
+		}
 		for (uint32_t b = 0; b < pi.arr_c; ++b) {
 			if (static_cast<int>(b) != big) { continue; } // the others are in place (rec buffers also decoded)
 			const uint64_t lo = pi.off[b] + ep(v0, b);
@@ -386,7 +393,7 @@ int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_
 				return FLS_ERR_CUDA;
 			}
 		}
-		if (cudaEventRecord(ev[2 * k], hp->in) != cudaSuccess || cudaStreamWaitEvent(hp->dec, ev[2 * k], 0) != cudaSuccess) {
+		if (cudaEventRecord(ev[3 * k], hp->in) != cudaSuccess || cudaStreamWaitEvent(hp->dec, ev[3 * k], 0) != cudaSuccess) {
 			return FLS_ERR_CUDA;
 		}
 		DecodeArgs a {};
@@ -395,13 +402,14 @@ int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_
 		a.n_items   = v1 - v0;
 		a.col_shift = 16;
 		if (launch_decode(fam, a, hp->dec) != cudaSuccess) { return FLS_ERR_CUDA; }
-		if (cudaEventRecord(ev[2 * k + 1], hp->dec) != cudaSuccess ||
-		    cudaStreamWaitEvent(hp->out, ev[2 * k + 1], 0) != cudaSuccess) {
+		if (cudaEventRecord(ev[3 * k + 1], hp->dec) != cudaSuccess ||
+		    cudaStreamWaitEvent(hp->out, ev[3 * k + 1], 0) != cudaSuccess) {
 			return FLS_ERR_CUDA;
 		}
 		const uint64_t o0 = static_cast<uint64_t>(v0) * 1024 * sz, ob = static_cast<uint64_t>(v1 - v0) * 1024 * sz;
 		if (cudaMemcpyAsync(static_cast<uint8_t*>(out) + o0, d_out.as<uint8_t>() + o0, ob, cudaMemcpyDeviceToHost,
-		                    hp->out) != cudaSuccess) {
+		                    hp->out) != cudaSuccess ||
+		    cudaEventRecord(ev[3 * k + 2], hp->out) != cudaSuccess) {
 			return FLS_ERR_CUDA;
 		}
 	}
