@@ -275,8 +275,8 @@ HostPipe* host_pipe() {
 }
 
 // Decode a page held in host memory into host memory.  The header is parsed from the host copy and the page's
-// small per-vector buffers go over whole; the vectors then go through in chunks of about 16 MB of output (the
-// first about 1 MB): each chunk's slice of the largest buffer is copied in on one stream, decoded on a second
+// small per-vector buffers go over whole; the vectors then go through in chunks of output growing from about
+// 1 MB to about 16 MB: each chunk's slice of the largest buffer is copied in on one stream, decoded on a second
 // (a queue of the chunk's vector ids) and copied out on a third, so the copies in both directions and the
 // kernels overlap (with pinned host buffers).
 int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_t out_cap, uint8_t dt,
@@ -352,10 +352,13 @@ int decode_host_page(const uint8_t* page, uint64_t page_size, void* out, uint64_
 	// long copies), the first of about 1 MB so that the copies out start early
 	const uint64_t         chunk_vec = std::max<uint64_t>(1, (16ull << 20) / (1024 * sz));
 	const uint64_t         first_vec = std::max<uint64_t>(1, (1ull << 20) / (1024 * sz));
-	std::vector<uint32_t>  bounds {0};
+	// chunk sizes double from the first up to the steady size, so that each chunk's copy in is done before the
+	// copies out ahead of it are (a 1 MB chunk then a 16 MB one left the copies out idle while it came in)
+	std::vector<uint32_t> bounds {0};
+	uint64_t              step = first_vec;
 	while (bounds.back() < pi.vec_c) {
-		const uint64_t step = bounds.size() == 1 ? first_vec : chunk_vec;
 		bounds.push_back(static_cast<uint32_t>(std::min<uint64_t>(pi.vec_c, bounds.back() + step)));
+		step = std::min<uint64_t>(2 * step, chunk_vec);
 	}
 	const uint32_t n_chunks = static_cast<uint32_t>(bounds.size() - 1);
 	if (3ull * n_chunks > kPipeEvents) { return FLS_ERR_TOO_LARGE; }

@@ -162,9 +162,9 @@ def test_page_plan_equals_direct_decode(cuda, col_golden):
 
 @pytest.mark.parametrize("expr", [1, 11, 6])
 def test_c_api_decode_pipelines_large_pages(cuda, expr):
-    """decode_to_memory of a page spanning several pipeline chunks (u64: a 128-vector first chunk, then 2048
-    vectors per chunk, so 3000 vectors make three chunks, the last partial, and the third chunk's copy in waits
-    for the first chunk's copy out), from pinned and from pageable host memory."""
+    """decode_to_memory of a page spanning several pipeline chunks (u64: chunks of 128, 256, 512, 1024 and then
+    2048 vectors, so 3000 vectors make five chunks, the last partial, and from the third on each chunk's copy in
+    waits for the copy out of the chunk two places before it), from pinned and from pageable host memory."""
     import torch
 
     from fastlanes_b200 import pages
